@@ -1,0 +1,237 @@
+"""ctypes front-end of the CPU oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: the checker and the CPU baseline. Imported by
+``tests/``, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` / reference
+legs of ``bench.py`` — never by the product package.
+
+Arrays follow the reference's C++ row-major layouts (compas-toolkit
+``include/compas/*``): tissue parameters float32 ``[9][V]`` (T1, T2, B1, B0,
+rho_x, rho_y, x, y, z), echos complex ``[R][V]``, coils ``[C][V]``, signal
+``[C][R][S]``, J·v input ``[4][V]``, Jᴴ·v input ``[C][R][S]``, output ``[4][V]``.
+``dtype='f64'`` returns the FP64 truth, ``'f32'`` the FP32 reference twin.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+_LIB = None
+
+_P, _I, _I64, _F = C.c_void_p, C.c_int, C.c_int64, C.c_float
+_SIGS = {
+    "oracle_fisp_f64": [_P, _I64, _P, _I64, _P, _P, _I, _I, _F, _F, _F, _F, _I, _I, _I, _I, _I, _P, _I],
+    "oracle_fisp_f32": [_P, _I64, _P, _I64, _P, _P, _I, _I, _F, _F, _F, _F, _I, _I, _I, _I, _I, _P, _I],
+    "oracle_pssfp_f64": [_P, _I64, _P, _I64, _P, _I, _P, _I, _F, _F, _F, _F, _F, _F, _P, _I, _P, _I],
+    "oracle_pssfp_f32": [_P, _I64, _P, _I64, _P, _I, _P, _I, _F, _F, _F, _F, _F, _F, _P, _I, _P, _I],
+    "oracle_phase_encoding_f64": [_P, _P, _I64, _I, _P, _P],
+    "oracle_signal_cartesian_f64": [_P, _P, _I64, _I, _I, _F, _P, _F, _F, _P, _I, _P, _I64, _P, _I],
+    "oracle_signal_cartesian_f32": [_P, _P, _I64, _I, _I, _F, _P, _F, _F, _P, _I, _P, _I64, _P, _I],
+    "oracle_signal_spiral_f64": [_P, _P, _I64, _I, _I, _F, _P, _P, _P, _I, _P, _I64, _P, _I],
+    "oracle_jacobian_f64": [_P, _P, _P, _P, _I64, _I, _I, _F, _F, _F, _P, _I, _P, _P, _I64, _P, _I],
+    "oracle_jacobian_hermitian_f64": [_P, _P, _P, _P, _I64, _I, _I, _F, _F, _F, _P, _I, _P, _P, _I64, _P, _I],
+    "oracle_residual_f64": [_P, _P, _I64, _P],
+    "oracle_cx_eval_f32": [_I, _P, _I64, _P],
+    "oracle_max_threads": [],
+}
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = _HERE / "liboracle.so"
+        if not path.exists():
+            raise RuntimeError(f"{path} missing: run `make -C oracle` (or __graft_entry__.build())")
+        L = C.CDLL(str(path))
+        for name, args in _SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = C.c_double if name == "oracle_residual_f64" else C.c_int
+        _LIB = L
+    return _LIB
+
+
+def nthreads_default() -> int:
+    return int(os.environ.get("COMPAS_ORACLE_THREADS", os.cpu_count() or 1))
+
+
+def _cf(a) -> np.ndarray:
+    """complex array -> contiguous interleaved float32 view."""
+    a = np.ascontiguousarray(a, dtype=np.complex64)
+    return a.view(np.float32)
+
+
+def _ff(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _ip(idx):
+    if idx is None:
+        return None, 0
+    idx = np.ascontiguousarray(idx, dtype=np.int32)
+    return idx, len(idx)
+
+
+def _iptr(idx):
+    return None if idx is None else idx.ctypes.data
+
+
+def _out(shape, dtype):
+    if dtype == "f64":
+        return np.zeros(shape + (2,), np.float64)
+    return np.zeros(shape + (2,), np.float32)
+
+
+def _as_complex(buf):
+    return buf[..., 0] + 1j * buf[..., 1] if buf.dtype == np.float64 else (buf[..., 0] + 1j * buf[..., 1]).astype(np.complex64)
+
+
+def fisp(params, seq, vidx=None, dtype="f64", nthreads=None):
+    """simulate_magnetization(FISP): echos [nTR*uf][n]."""
+    params = _ff(params)
+    nv = params.shape[1]
+    idx, nidx = _ip(vidx)
+    n = nidx if idx is not None else nv
+    rf = _cf(seq["rf"])
+    slices = _cf(seq["slices"])
+    nTR = len(seq["rf"])
+    P = seq["slices"].shape[0]
+    R = nTR * int(seq.get("uf", 1))
+    out = _out((R, n), dtype)
+    fn = lib().oracle_fisp_f64 if dtype == "f64" else lib().oracle_fisp_f32
+    rc = fn(params.ctypes.data, C.c_int64(nv), _iptr(idx), C.c_int64(nidx), rf.ctypes.data, slices.ctypes.data,
+            nTR, P, C.c_float(seq["TR"]), C.c_float(seq["TE"]), C.c_float(seq.get("TW", 0.0)),
+            C.c_float(seq["TI"]), int(seq["max_state"]), int(seq.get("uf", 1)), int(seq.get("reps", 1)),
+            int(seq.get("inversion", 1)), int(seq.get("wait_spoil", 1)), out.ctypes.data,
+            nthreads or nthreads_default())
+    if rc != 0:
+        raise ValueError("oracle_fisp rejected its arguments")
+    return _as_complex(out)
+
+
+def pssfp(params, seq, vidx=None, dtype="f64", nthreads=None):
+    """simulate_magnetization(pSSFP): echos [nTR][n]."""
+    params = _ff(params)
+    nv = params.shape[1]
+    idx, nidx = _ip(vidx)
+    n = nidx if idx is not None else nv
+    rf = _cf(seq["rf"])
+    g = _cf(seq["gdtrf"])
+    z = _ff(seq["z"])
+    nTR = len(seq["rf"])
+    out = _out((nTR, n), dtype)
+    fn = lib().oracle_pssfp_f64 if dtype == "f64" else lib().oracle_pssfp_f32
+    dt, gz = seq["dt"], seq["gz"]
+    rc = fn(params.ctypes.data, C.c_int64(nv), _iptr(idx), C.c_int64(nidx), rf.ctypes.data, nTR, g.ctypes.data,
+            len(seq["gdtrf"]), C.c_float(dt[0]), C.c_float(dt[1]), C.c_float(dt[2]), C.c_float(gz[0]),
+            C.c_float(gz[1]), C.c_float(gz[2]), z.ctypes.data, len(z), out.ctypes.data,
+            nthreads or nthreads_default())
+    if rc != 0:
+        raise ValueError("oracle_pssfp rejected its arguments")
+    return _as_complex(out)
+
+
+def phase_encoding(echo, params, k_start):
+    e, params, ks = _cf(echo), _ff(params), _cf(k_start)
+    R, V = echo.shape
+    out = np.zeros((R, V, 2), np.float64)
+    lib().oracle_phase_encoding_f64(e.ctypes.data, params.ctypes.data, C.c_int64(V), R, ks.ctypes.data,
+                                    out.ctypes.data)
+    return _as_complex(out)
+
+
+def _entries(entries):
+    if entries is None:
+        return None, 0
+    e = np.ascontiguousarray(entries, dtype=np.int32).reshape(-1, 3)
+    return e, len(e)
+
+
+def signal_cartesian(echo, params, traj, coils, entries=None, dtype="f64", nthreads=None):
+    e, params, ks, co = _cf(echo), _ff(params), _cf(traj["k_start"]), _cf(coils)
+    R, V = echo.shape
+    Cn = coils.shape[0]
+    ent, nent = _entries(entries)
+    shape = (nent,) if ent is not None else (Cn, traj["nr"], traj["ns"])
+    out = _out(shape, dtype)
+    dk = complex(traj["dk"])
+    fn = lib().oracle_signal_cartesian_f64 if dtype == "f64" else lib().oracle_signal_cartesian_f32
+    fn(e.ctypes.data, params.ctypes.data, C.c_int64(V), traj["nr"], traj["ns"], C.c_float(traj["dt"]),
+       ks.ctypes.data, C.c_float(dk.real), C.c_float(dk.imag), co.ctypes.data, Cn,
+       None if ent is None else ent.ctypes.data, C.c_int64(nent), out.ctypes.data, nthreads or nthreads_default())
+    return _as_complex(out)
+
+
+def signal_spiral(echo, params, traj, coils, entries=None, nthreads=None):
+    e, params, ks, dk, co = _cf(echo), _ff(params), _cf(traj["k_start"]), _cf(traj["dk"]), _cf(coils)
+    R, V = echo.shape
+    Cn = coils.shape[0]
+    ent, nent = _entries(entries)
+    shape = (nent,) if ent is not None else (Cn, traj["nr"], traj["ns"])
+    out = _out(shape, "f64")
+    lib().oracle_signal_spiral_f64(e.ctypes.data, params.ctypes.data, C.c_int64(V), traj["nr"], traj["ns"],
+                                   C.c_float(traj["dt"]), ks.ctypes.data, dk.ctypes.data, co.ctypes.data, Cn,
+                                   None if ent is None else ent.ctypes.data, C.c_int64(nent), out.ctypes.data,
+                                   nthreads or nthreads_default())
+    return _as_complex(out)
+
+
+def jacobian(echo, dT1, dT2, params, traj, coils, vec, entries=None, nthreads=None):
+    e, d1, d2, params, co, ve = _cf(echo), _cf(dT1), _cf(dT2), _ff(params), _cf(coils), _cf(vec)
+    R, V = echo.shape
+    Cn = coils.shape[0]
+    ent, nent = _entries(entries)
+    shape = (nent,) if ent is not None else (Cn, traj["nr"], traj["ns"])
+    out = _out(shape, "f64")
+    dk = complex(traj["dk"])
+    lib().oracle_jacobian_f64(e.ctypes.data, d1.ctypes.data, d2.ctypes.data, params.ctypes.data, C.c_int64(V),
+                              traj["nr"], traj["ns"], C.c_float(traj["dt"]), C.c_float(dk.real),
+                              C.c_float(dk.imag), co.ctypes.data, Cn, ve.ctypes.data,
+                              None if ent is None else ent.ctypes.data, C.c_int64(nent), out.ctypes.data,
+                              nthreads or nthreads_default())
+    return _as_complex(out)
+
+
+def jacobian_hermitian(echo, dT1, dT2, params, traj, coils, vec, vidx=None, nthreads=None):
+    e, d1, d2, params, co, ve = _cf(echo), _cf(dT1), _cf(dT2), _ff(params), _cf(coils), _cf(vec)
+    R, V = echo.shape
+    Cn = coils.shape[0]
+    idx, nidx = _ip(vidx)
+    n = nidx if idx is not None else V
+    out = _out((4, n), "f64")
+    dk = complex(traj["dk"])
+    lib().oracle_jacobian_hermitian_f64(e.ctypes.data, d1.ctypes.data, d2.ctypes.data, params.ctypes.data,
+                                        C.c_int64(V), traj["nr"], traj["ns"], C.c_float(traj["dt"]),
+                                        C.c_float(dk.real), C.c_float(dk.imag), co.ctypes.data, Cn,
+                                        ve.ctypes.data, _iptr(idx), C.c_int64(nidx), out.ctypes.data,
+                                        nthreads or nthreads_default())
+    return _as_complex(out)
+
+
+def residual(lhs, rhs):
+    a, b = _cf(lhs), _cf(rhs)
+    n = lhs.size
+    out = np.zeros(lhs.shape + (2,), np.float64)
+    obj = lib().oracle_residual_f64(a.ctypes.data, b.ctypes.data, C.c_int64(n), out.ctypes.data)
+    return float(obj), _as_complex(out)
+
+
+def cx_eval_f32(op: int, packed: np.ndarray) -> np.ndarray:
+    """Evaluate the FP32 twin's complex primitives (see oracle_capi.cpp)."""
+    packed = _ff(packed)
+    n = packed.shape[0]
+    out = np.zeros((n, 2), np.float32)
+    rc = lib().oracle_cx_eval_f32(op, packed.ctypes.data, C.c_int64(n), out.ctypes.data)
+    if rc != 0:
+        raise ValueError("unknown op")
+    return out
+
+
+def rel_l2(x, ref) -> float:
+    x = np.asarray(x, np.complex128)
+    ref = np.asarray(ref, np.complex128)
+    den = np.linalg.norm(ref.ravel())
+    return float(np.linalg.norm((x - ref).ravel()) / (den if den > 0 else 1.0))
