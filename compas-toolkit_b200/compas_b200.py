@@ -1,0 +1,449 @@
+"""Python front-end of libcompas_b200.so (the C ABI in include/compas_b200.h).
+
+Mirrors the reference's Julia module (CompasToolkit.jl/src/CompasToolkit.jl): a
+``Context``, device arrays (``CompasArray``), ``TissueParameters``,
+``FispSequence`` / ``pSSFPSequence``, ``CartesianTrajectory`` / ``SpiralTrajectory``
+and the operations ``simulate_magnetization``, ``simulate_magnetization_derivative(s)``,
+``magnetization_to_signal``, ``compute_jacobian``, ``compute_jacobian_hermitian``,
+``phase_encoding`` and ``compute_residual``. Every call goes through the C ABI
+symbols the Julia module binds; arrays use the C++ row-major layout (slowest
+dimension first), which is the reverse of the Julia view.
+
+The GPU library is required: importing works without it, but every operation raises
+``CompasError`` when libcompas_b200.so is missing — there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIBRARY_PATH = Path(os.environ.get("COMPAS_B200_LIBRARY", _HERE / "libcompas_b200.so"))
+
+# enum values of the reference (compas/trajectories/signal.h:14-44, compas/jacobian/product.h:10)
+SIGNAL_METHODS = {"Naive": 0, "Direct": 1, "MatmulPedantic": 2, "Matmul": 3, "MatmulFast": 4, "MatmulLow": 5}
+JACOBIAN_METHODS = {"Naive": 0, "Direct": 1, "Gemm": 2, "GemmFast": 3, "GemmLow": 4}
+FIELDS = {"T1": 0, "T2": 1, "B1": 2, "B0": 3, "rho_x": 4, "rho_y": 5, "x": 6, "y": 7, "z": 8}
+
+
+class CompasError(RuntimeError):
+    pass
+
+
+_P, _I, _I32, _I64, _F = C.c_void_p, C.c_int, C.c_int32, C.c_int64, C.c_float
+_SIGS = {
+    "compas_version": ([], C.c_char_p),
+    "compas_last_error": ([], C.c_char_p),
+    "compas_make_context": ([], _P),
+    "compas_copy_context_for_device": ([_P, _I], _P),
+    "compas_destroy_context": ([_P], None),
+    "compas_destroy_object": ([_P], None),
+    "compas_synchronize": ([_P], None),
+    "compas_make_array_float": ([_P, _P, _I, _P], _P),
+    "compas_read_array_float": ([_P, _P, _P, _I64], None),
+    "compas_make_array_complex": ([_P, _P, _I, _P], _P),
+    "compas_read_array_complex": ([_P, _P, _P, _I64], None),
+    "compas_destroy_array": ([_P], None),
+    "compas_make_tissue_parameters": ([_P, _I] + [_P] * 9, _P),
+    "compas_make_fisp_sequence": ([_P, _P, _F, _F, _F, _I, _F, _I, _I], _P),
+    "compas_make_pssfp_sequence": ([_P, _F, _P, _F, _F, _F, _F, _F, _F, _P], _P),
+    "compas_make_cartesian_trajectory": ([_I, _I, _F, _P, _F], _P),
+    "compas_make_spiral_trajectory": ([_I, _I, _F, _P, _P], _P),
+    "compas_simulate_magnetization_fisp": ([_P, _P, _P], _P),
+    "compas_simulate_magnetization_pssfp": ([_P, _P, _P], _P),
+    "compas_magnetization_to_signal_cartesian": ([_P, _I, _P, _P, _P, _P, _I32], _P),
+    "compas_magnetization_to_signal_spiral": ([_P, _I, _P, _P, _P, _P], _P),
+    "compas_compute_jacobian": ([_P, _I, _P, _P, _P, _P, _P, _P, _P, _I32], _P),
+    "compas_compute_jacobian_hermitian": ([_P, _I, _P, _P, _P, _P, _P, _P, _P, _I32], _P),
+    "phase_encoding": ([_P, _P, _P, _P], _P),
+    "compas_compute_residual": ([_P, _P, _P, _P], _P),
+    "compas_simulate_magnetization_derivative_pssfp": ([_P, _I, _P, _P, _F, _P], _P),
+    "compas_simulate_magnetization_derivative_fisp": ([_P, _I, _P, _P, _F, _P], _P),
+    "compas_b200_magnetization_to_signal": ([_P, _P, _P, _P, _P, _I], _P),
+    "compas_b200_compute_jacobian": ([_P, _P, _P, _P, _P, _P, _P, _P, _I], _P),
+    "compas_b200_compute_jacobian_hermitian": ([_P, _P, _P, _P, _P, _P, _P, _P, _I], _P),
+    "compas_b200_context_stream": ([_P], _P),
+    "compas_b200_array_device_ptr": ([_P], _P),
+    "compas_b200_array_rank": ([_P], _I),
+    "compas_b200_array_extent": ([_P, _I], _I64),
+    "compas_b200_launch_count": ([], C.c_uint64),
+    "compas_b200_set_fisp_launch": ([_I, _I], None),
+    "compas_b200_set_pssfp_launch": ([_I], None),
+    "compas_b200_fisp_config_count": ([], _I),
+    "compas_b200_fisp_config_info": ([_I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
+    "compas_b200_pssfp_config_count": ([], _I),
+    "compas_b200_pssfp_config_info": ([_I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
+}
+
+_LIB = None
+
+
+def library() -> C.CDLL:
+    """Load libcompas_b200.so (raises CompasError when it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        if not LIBRARY_PATH.exists():
+            raise CompasError(f"{LIBRARY_PATH} not found: build it with __graft_entry__.build() "
+                              "(make -C compas-toolkit_b200)")
+        lib = C.CDLL(str(LIBRARY_PATH))
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _LIB = lib
+    return _LIB
+
+
+def exported_symbols() -> list:
+    return list(_SIGS)
+
+
+def _check(result=None, what="compas call"):
+    err = library().compas_last_error()
+    if err is not None:
+        raise CompasError(err.decode(errors="replace"))
+    if result is None and what is not None and what.endswith("!"):
+        raise CompasError(f"{what[:-1]} returned NULL")
+    return result
+
+
+def version() -> str:
+    return library().compas_version().decode()
+
+
+class Context:
+    """A COMPAS context on one device (compas_make_context / compas_copy_context_for_device)."""
+
+    def __init__(self, device: int = 0):
+        lib = library()
+        base = lib.compas_make_context()
+        _check(base, "compas_make_context!")
+        if device != 0:
+            ptr = lib.compas_copy_context_for_device(base, device)
+            lib.compas_destroy_context(base)
+            _check(ptr, "compas_copy_context_for_device!")
+            base = ptr
+        self.ptr = base
+        self.device = device
+
+    def synchronize(self):
+        library().compas_synchronize(self.ptr)
+        _check()
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of this context (all its work is ordered on it)."""
+        return library().compas_b200_context_stream(self.ptr) or 0
+
+    def __del__(self):
+        if getattr(self, "ptr", None) and _LIB is not None:
+            _LIB.compas_destroy_context(self.ptr)
+            self.ptr = None
+
+
+class CompasArray:
+    """Device array handle (float32 or complex64, rank 1-3), row-major like the C++ side."""
+
+    def __init__(self, context: Context, ptr, dtype, shape):
+        self.context = context
+        self.ptr = ptr
+        self.dtype = np.dtype(dtype)
+        self.shape = tuple(int(s) for s in shape)
+
+    @staticmethod
+    def from_numpy(context: Context, arr) -> "CompasArray":
+        arr = np.asarray(arr)
+        if np.iscomplexobj(arr):
+            a = np.ascontiguousarray(arr, dtype=np.complex64)
+            fn = library().compas_make_array_complex
+        else:
+            a = np.ascontiguousarray(arr, dtype=np.float32)
+            fn = library().compas_make_array_float
+        if a.ndim < 1 or a.ndim > 3:
+            raise CompasError("cannot support rank > 3")
+        sizes = (C.c_int64 * a.ndim)(*a.shape)
+        ptr = fn(context.ptr, a.ctypes.data, a.ndim, sizes)
+        _check(ptr, "compas_make_array!")
+        return CompasArray(context, ptr, a.dtype, a.shape)
+
+    @property
+    def size(self) -> int:
+        return int(np.prod(self.shape)) if self.shape else 0
+
+    @property
+    def device_ptr(self) -> int:
+        return library().compas_b200_array_device_ptr(self.ptr) or 0
+
+    def to_numpy(self) -> np.ndarray:
+        out = np.empty(self.shape, self.dtype)
+        fn = library().compas_read_array_complex if self.dtype == np.complex64 else library().compas_read_array_float
+        fn(self.context.ptr, self.ptr, out.ctypes.data, out.size)
+        _check()
+        return out
+
+    def read_into(self, out: np.ndarray) -> np.ndarray:
+        """Blocking copy into a preallocated (e.g. pinned) host array of matching size/dtype."""
+        assert out.dtype == self.dtype and out.size == self.size and out.flags.c_contiguous
+        fn = library().compas_read_array_complex if self.dtype == np.complex64 else library().compas_read_array_float
+        fn(self.context.ptr, self.ptr, out.ctypes.data, out.size)
+        _check()
+        return out
+
+    collect = to_numpy
+
+    def __del__(self):
+        if getattr(self, "ptr", None) and _LIB is not None:
+            _LIB.compas_destroy_array(self.ptr)
+            self.ptr = None
+
+    def __repr__(self):
+        return f"CompasArray{{{self.dtype}}} of size {self.shape}"
+
+
+def _arr(context, a, dtype=None) -> CompasArray:
+    if isinstance(a, CompasArray):
+        return a
+    a = np.asarray(a)
+    if dtype is not None:
+        a = a.astype(dtype, copy=False)
+    return CompasArray.from_numpy(context, a)
+
+
+class _Object:
+    def __init__(self, ptr, keep=()):
+        _check(ptr, "constructor!")
+        self.ptr = ptr
+        self._keep = keep
+
+    def __del__(self):
+        if getattr(self, "ptr", None) and _LIB is not None:
+            _LIB.compas_destroy_object(self.ptr)
+            self.ptr = None
+
+
+class TissueParameters(_Object):
+    """compas_make_tissue_parameters; fields as host vectors of nvoxels floats."""
+
+    def __init__(self, context: Context, nvoxels: int, T1, T2, B1, B0, rho_x, rho_y, x, y, z=None):
+        cols = [np.ascontiguousarray(np.broadcast_to(np.asarray(c, np.float32), (nvoxels,)))
+                for c in (T1, T2, B1, B0, rho_x, rho_y, x, y)]
+        cols.append(np.zeros(nvoxels, np.float32) if z is None else
+                    np.ascontiguousarray(np.broadcast_to(np.asarray(z, np.float32), (nvoxels,))))
+        ptr = library().compas_make_tissue_parameters(context.ptr, int(nvoxels), *[c.ctypes.data for c in cols])
+        super().__init__(ptr)
+        self.nvoxels = int(nvoxels)
+
+    @staticmethod
+    def from_soa(context: Context, params: np.ndarray) -> "TissueParameters":
+        p = np.asarray(params, np.float32)
+        return TissueParameters(context, p.shape[1], *p)
+
+
+class FispSequence(_Object):
+    """compas_make_fisp_sequence: RF train [nTR] (deg, phase), slice profiles [npos][nTR]."""
+
+    def __init__(self, context: Context, RF_train, slice_profiles, TR: float, TE: float, max_state: int, TI: float,
+                 undersampling_factor: int = 1, repetitions: int = 1, TW: float = 0.0):
+        rf = _arr(context, np.asarray(RF_train, np.complex64))
+        sp = _arr(context, np.asarray(slice_profiles, np.complex64).reshape(-1, rf.shape[0]))
+        ptr = library().compas_make_fisp_sequence(rf.ptr, sp.ptr, TR, TE, TW, int(max_state), TI,
+                                                  int(undersampling_factor), int(repetitions))
+        super().__init__(ptr, (rf, sp))
+        self.nreadouts = rf.shape[0] * int(undersampling_factor)
+        self.max_state = int(max_state)
+        self.npositions = sp.shape[0]
+
+    @staticmethod
+    def from_dict(context: Context, s: dict) -> "FispSequence":
+        return FispSequence(context, s["rf"], s["slices"], s["TR"], s["TE"], s["max_state"], s["TI"],
+                            s.get("uf", 1), s.get("reps", 1), s.get("TW", 0.0))
+
+
+class pSSFPSequence(_Object):
+    """compas_make_pssfp_sequence. `z` is passed as float32 (the reference's Julia wrapper
+    converted it to ComplexF32, which disagrees with the C++ side)."""
+
+    def __init__(self, context: Context, RF_train, TR: float, gamma_dt_RF, dt: Sequence[float],
+                 gamma_dt_GRz: Sequence[float], z):
+        rf = _arr(context, np.asarray(RF_train, np.complex64))
+        g = _arr(context, np.asarray(gamma_dt_RF, np.complex64))
+        zz = _arr(context, np.asarray(z, np.float32))
+        ptr = library().compas_make_pssfp_sequence(rf.ptr, TR, g.ptr, dt[0], dt[1], dt[2], gamma_dt_GRz[0],
+                                                   gamma_dt_GRz[1], gamma_dt_GRz[2], zz.ptr)
+        super().__init__(ptr, (rf, g, zz))
+        self.nreadouts = rf.shape[0]
+
+    @staticmethod
+    def from_dict(context: Context, s: dict) -> "pSSFPSequence":
+        return pSSFPSequence(context, s["rf"], s["TR"], s["gdtrf"], s["dt"], s["gz"], s["z"])
+
+
+class CartesianTrajectory(_Object):
+    def __init__(self, context: Context, nreadouts: int, samples_per_readout: int, delta_t: float, k_start,
+                 delta_k: float):
+        ks = _arr(context, np.asarray(k_start, np.complex64))
+        ptr = library().compas_make_cartesian_trajectory(int(nreadouts), int(samples_per_readout), delta_t, ks.ptr,
+                                                         float(delta_k))
+        super().__init__(ptr, (ks,))
+        self.nreadouts, self.samples_per_readout = int(nreadouts), int(samples_per_readout)
+
+    @staticmethod
+    def from_dict(context: Context, t: dict) -> "CartesianTrajectory":
+        return CartesianTrajectory(context, t["nr"], t["ns"], t["dt"], t["k_start"], t["dk"])
+
+
+class SpiralTrajectory(_Object):
+    def __init__(self, context: Context, nreadouts: int, samples_per_readout: int, delta_t: float, k_start, delta_k):
+        ks = _arr(context, np.asarray(k_start, np.complex64))
+        dk = _arr(context, np.asarray(delta_k, np.complex64))
+        ptr = library().compas_make_spiral_trajectory(int(nreadouts), int(samples_per_readout), delta_t, ks.ptr,
+                                                      dk.ptr)
+        super().__init__(ptr, (ks, dk))
+        self.nreadouts, self.samples_per_readout = int(nreadouts), int(samples_per_readout)
+
+    @staticmethod
+    def from_dict(context: Context, t: dict) -> "SpiralTrajectory":
+        return SpiralTrajectory(context, t["nr"], t["ns"], t["dt"], t["k_start"], t["dk"])
+
+
+def trajectory_from_dict(context: Context, t: dict):
+    return (CartesianTrajectory if t.get("kind", "cartesian") == "cartesian" else SpiralTrajectory).from_dict(context, t)
+
+
+def _result(ptr, context, shape, what) -> CompasArray:
+    _check(ptr, what + "!")
+    return CompasArray(context, ptr, np.complex64, shape)
+
+
+def simulate_magnetization(context: Context, parameters: TissueParameters, sequence) -> CompasArray:
+    lib = library()
+    if isinstance(sequence, FispSequence):
+        ptr = lib.compas_simulate_magnetization_fisp(context.ptr, parameters.ptr, sequence.ptr)
+    elif isinstance(sequence, pSSFPSequence):
+        ptr = lib.compas_simulate_magnetization_pssfp(context.ptr, parameters.ptr, sequence.ptr)
+    else:
+        raise CompasError("unknown sequence type")
+    return _result(ptr, context, (sequence.nreadouts, parameters.nvoxels), "simulate_magnetization")
+
+
+def simulate_magnetization_derivative(context: Context, field, echos, parameters: TissueParameters, sequence,
+                                      delta: float = 1e-4) -> CompasArray:
+    field = FIELDS[field] if isinstance(field, str) else int(field)
+    e = _arr(context, echos, np.complex64)
+    lib = library()
+    fn = (lib.compas_simulate_magnetization_derivative_fisp if isinstance(sequence, FispSequence)
+          else lib.compas_simulate_magnetization_derivative_pssfp)
+    ptr = fn(context.ptr, field, e.ptr, parameters.ptr, delta, sequence.ptr)
+    return _result(ptr, context, e.shape, "simulate_magnetization_derivative")
+
+
+def simulate_magnetization_derivatives(context, echos, parameters, sequence, delta: float = 1e-4) -> dict:
+    return {"T1": simulate_magnetization_derivative(context, 0, echos, parameters, sequence, delta),
+            "T2": simulate_magnetization_derivative(context, 1, echos, parameters, sequence, delta)}
+
+
+def magnetization_to_signal(context: Context, echos, parameters: TissueParameters, trajectory, coils,
+                            method: Optional[str] = None, low_precision: bool = False) -> CompasArray:
+    """method=None uses the reference's C ABI entry point (MatmulFast, or MatmulLow when
+    low_precision); a method name from SIGNAL_METHODS selects it explicitly."""
+    e = _arr(context, echos, np.complex64)
+    c = _arr(context, coils, np.complex64)
+    lib = library()
+    shape = (c.shape[0], trajectory.nreadouts, trajectory.samples_per_readout)
+    if method is not None:
+        ptr = lib.compas_b200_magnetization_to_signal(context.ptr, e.ptr, parameters.ptr, trajectory.ptr, c.ptr,
+                                                      SIGNAL_METHODS[method])
+    elif isinstance(trajectory, CartesianTrajectory):
+        ptr = lib.compas_magnetization_to_signal_cartesian(context.ptr, c.shape[0], e.ptr, parameters.ptr, c.ptr,
+                                                           trajectory.ptr, int(bool(low_precision)))
+    else:
+        ptr = lib.compas_magnetization_to_signal_spiral(context.ptr, c.shape[0], e.ptr, parameters.ptr, c.ptr,
+                                                        trajectory.ptr)
+    return _result(ptr, context, shape, "magnetization_to_signal")
+
+
+def compute_jacobian(context: Context, echos, dechos: dict, parameters: TissueParameters, trajectory, coils, v,
+                     method: Optional[str] = None, low_precision: bool = False) -> CompasArray:
+    e, d1, d2 = (_arr(context, a, np.complex64) for a in (echos, dechos["T1"], dechos["T2"]))
+    c = _arr(context, coils, np.complex64)
+    vv = _arr(context, v, np.complex64)
+    lib = library()
+    shape = (c.shape[0], trajectory.nreadouts, trajectory.samples_per_readout)
+    if method is not None:
+        ptr = lib.compas_b200_compute_jacobian(context.ptr, e.ptr, d1.ptr, d2.ptr, parameters.ptr, trajectory.ptr,
+                                               c.ptr, vv.ptr, JACOBIAN_METHODS[method])
+    else:
+        ptr = lib.compas_compute_jacobian(context.ptr, c.shape[0], e.ptr, d1.ptr, d2.ptr, parameters.ptr, c.ptr,
+                                          trajectory.ptr, vv.ptr, int(bool(low_precision)))
+    return _result(ptr, context, shape, "compute_jacobian")
+
+
+def compute_jacobian_hermitian(context: Context, echos, dechos: dict, parameters: TissueParameters, trajectory,
+                               coils, v, method: Optional[str] = None, low_precision: bool = False) -> CompasArray:
+    e, d1, d2 = (_arr(context, a, np.complex64) for a in (echos, dechos["T1"], dechos["T2"]))
+    c = _arr(context, coils, np.complex64)
+    vv = _arr(context, v, np.complex64)
+    lib = library()
+    shape = (4, parameters.nvoxels)
+    if method is not None:
+        ptr = lib.compas_b200_compute_jacobian_hermitian(context.ptr, e.ptr, d1.ptr, d2.ptr, parameters.ptr,
+                                                         trajectory.ptr, c.ptr, vv.ptr, JACOBIAN_METHODS[method])
+    else:
+        ptr = lib.compas_compute_jacobian_hermitian(context.ptr, c.shape[0], e.ptr, d1.ptr, d2.ptr, parameters.ptr,
+                                                    trajectory.ptr, c.ptr, vv.ptr, int(bool(low_precision)))
+    return _result(ptr, context, shape, "compute_jacobian_hermitian")
+
+
+def phase_encoding(context: Context, echos, parameters: TissueParameters, trajectory) -> CompasArray:
+    e = _arr(context, echos, np.complex64)
+    ptr = library().phase_encoding(context.ptr, e.ptr, parameters.ptr, trajectory.ptr)
+    return _result(ptr, context, e.shape, "phase_encoding")
+
+
+def compute_residual(context: Context, lhs, rhs):
+    """Returns (Σ|lhs - rhs|², lhs - rhs) like the Julia wrapper."""
+    a = _arr(context, lhs, np.complex64)
+    b = _arr(context, rhs, np.complex64)
+    obj = np.zeros(1, np.float32)
+    ptr = library().compas_compute_residual(context.ptr, a.ptr, b.ptr, obj.ctypes.data)
+    diff = _result(ptr, context, a.shape, "compute_residual")
+    return float(obj[0]), diff
+
+
+def launch_count() -> int:
+    """Kernels launched by libcompas_b200.so so far in this process."""
+    return int(library().compas_b200_launch_count())
+
+
+def set_fisp_launch(config: int = -1, warps: int = -1):
+    library().compas_b200_set_fisp_launch(int(config), int(warps))
+    _check()
+
+
+def set_pssfp_launch(config: int = -1):
+    library().compas_b200_set_pssfp_launch(int(config))
+    _check()
+
+
+def fisp_configs() -> list:
+    lib = library()
+    out = []
+    for i in range(lib.compas_b200_fisp_config_count()):
+        k, g = C.c_int(), C.c_int()
+        lib.compas_b200_fisp_config_info(i, C.byref(k), C.byref(g))
+        out.append((k.value, g.value))
+    return out
+
+
+def pssfp_configs() -> list:
+    lib = library()
+    out = []
+    for i in range(lib.compas_b200_pssfp_config_count()):
+        k, g = C.c_int(), C.c_int()
+        lib.compas_b200_pssfp_config_info(i, C.byref(k), C.byref(g))
+        out.append((k.value, g.value))
+    return out

@@ -1,0 +1,474 @@
+// capi.cpp — the extern "C" boundary (include/compas_b200.h).
+//
+// Same symbols and parameter lists as the reference's Julia binding library
+// (julia-bindings/src/bindings.cpp:19-411). Handles are heap objects derived from
+// compas::Object; arrays are compas::Array<T, N>. Exceptions never cross the boundary:
+// they are turned into a Julia error when jl_errorf is resolvable in the process (the
+// reference's behaviour, julia-bindings/src/common.h:48-62) and otherwise recorded for
+// compas_last_error() while the call returns NULL.
+#include <dlfcn.h>
+
+#include <cstring>
+#include <string>
+
+#include "../../include/compas_b200.h"
+#include "compas/compas.h"
+#include "kernels.h"
+
+#ifndef COMPAS_B200_VERSION
+#define COMPAS_B200_VERSION "compas-b200-0.1.0"
+#endif
+
+using compas::cfloat;
+
+namespace {
+
+thread_local std::string t_last_error;
+thread_local bool t_has_error = false;
+
+using jl_errorf_t = void (*)(const char*, ...);
+
+jl_errorf_t julia_error_fn() {
+    static jl_errorf_t fn = reinterpret_cast<jl_errorf_t>(dlsym(RTLD_DEFAULT, "jl_errorf"));
+    return fn;
+}
+
+void record_error(const char* msg) {
+    t_last_error = msg;
+    t_has_error = true;
+    if (auto fn = julia_error_fn()) {
+        fn("COMPAS error occurred: %s\n", msg);  // does not return
+    }
+}
+
+template<typename F>
+auto guarded(F fun) -> decltype(fun()) {
+    t_has_error = false;
+    try {
+        return fun();
+    } catch (const std::exception& e) {
+        record_error(e.what());
+    } catch (...) {
+        record_error("unknown exception");
+    }
+    using R = decltype(fun());
+    if constexpr (std::is_void_v<R>) {
+        return;
+    } else {
+        return R {};
+    }
+}
+
+template<typename T>
+T* handle(const void* p) {
+    return reinterpret_cast<T*>(const_cast<void*>(p));
+}
+
+const compas::CompasContext& ctx_of(const compas_context* c) {
+    if (!c) throw compas::CompasException("null context");
+    return *handle<compas::CompasContext>(c);
+}
+
+template<typename T>
+const T& unwrap(const void* obj) {
+    if (!obj) throw compas::CompasException("null object handle");
+    const auto* base = handle<compas::Object>(obj);
+    if (const T* p = dynamic_cast<const T*>(base)) return *p;
+    throw compas::CompasException(std::string("invalid object (expecting: ") + typeid(T).name() +
+                                  ", gotten: " + base->name() + ")");
+}
+
+template<typename T, size_t N>
+const compas::Array<T, N>& array_of(const void* arr, const char* what) {
+    if (!arr) throw compas::CompasException(std::string("null array: ") + what);
+    const auto* base = handle<compas::Object>(arr);
+    if (const auto* p = dynamic_cast<const compas::Array<T, N>*>(base)) return *p;
+    throw compas::CompasException(std::string("array `") + what + "` has the wrong element type or rank");
+}
+
+template<typename T>
+compas_array* new_array(T&& a) {
+    return reinterpret_cast<compas_array*>(static_cast<compas::Object*>(new std::decay_t<T>(std::forward<T>(a))));
+}
+
+template<typename T>
+compas_object* new_obj(T&& a) {
+    return reinterpret_cast<compas_object*>(static_cast<compas::Object*>(new std::decay_t<T>(std::forward<T>(a))));
+}
+
+template<typename T>
+const compas_array* make_array(const compas_context* context, const T* data, int rank, int64_t* sizes) {
+    const auto& ctx = ctx_of(context);
+    if (!sizes) throw compas::CompasException("null sizes");
+    for (int i = 0; i < rank; i++)
+        if (sizes[i] < 0) throw compas::CompasException("negative array size");
+    int64_t n = 1;
+    for (int i = 0; i < rank; i++) n *= sizes[i];
+    if (n > 0 && !data) throw compas::CompasException("null data pointer");
+    if (rank == 1) return new_array(ctx.allocate(data, sizes[0]));
+    if (rank == 2) return new_array(ctx.allocate(data, sizes[0], sizes[1]));
+    if (rank == 3) return new_array(ctx.allocate(data, sizes[0], sizes[1], sizes[2]));
+    throw compas::CompasException("cannot support rank > 3");
+}
+
+void read_array(const compas_array* arr, void* dest, int64_t length, size_t elem) {
+    if (!arr) throw compas::CompasException("null array");
+    const auto* base = dynamic_cast<const compas::ArrayBase*>(handle<compas::Object>(arr));
+    if (!base) throw compas::CompasException("handle is not an array");
+    if (base->element_size() != elem) throw compas::CompasException("array element type mismatch");
+    if (length < 0) throw compas::CompasException("negative length");
+    if (length > 0 && !dest) throw compas::CompasException("null destination");
+    base->copy_bytes_to(dest, size_t(length) * elem);
+}
+
+compas::SimulateSignalMethod signal_method(int m) {
+    if (m < 0 || m > 5) throw compas::CompasException("invalid SimulateSignalMethod");
+    return compas::SimulateSignalMethod(m);
+}
+
+compas::JacobianComputeMethod jacobian_method(int m) {
+    if (m < 0 || m > 4) throw compas::CompasException("invalid JacobianComputeMethod");
+    return compas::JacobianComputeMethod(m);
+}
+
+}  // namespace
+
+namespace compas {
+unsigned long long launch_count();
+void set_fisp_override(int config, int warps);
+void set_pssfp_override(int config);
+}  // namespace compas
+
+extern "C" {
+
+const char* compas_version(void) {
+    return COMPAS_B200_VERSION;
+}
+
+const char* compas_last_error(void) {
+    return t_has_error ? t_last_error.c_str() : nullptr;
+}
+
+const compas_context* compas_make_context(void) {
+    return guarded([&]() -> const compas_context* {
+        return reinterpret_cast<const compas_context*>(new compas::CompasContext(compas::make_context()));
+    });
+}
+
+const compas_context* compas_copy_context_for_device(compas_context* ctx, int device) {
+    return guarded([&]() -> const compas_context* {
+        return reinterpret_cast<const compas_context*>(new compas::CompasContext(ctx_of(ctx).with_device(device)));
+    });
+}
+
+void compas_destroy_context(const compas_context* ctx) {
+    guarded([&] { delete handle<compas::CompasContext>(ctx); });
+}
+
+void compas_destroy_object(const compas_object* obj) {
+    guarded([&] { delete handle<compas::Object>(obj); });
+}
+
+void compas_synchronize(const compas_context* ctx) {
+    guarded([&] { ctx_of(ctx).synchronize(); });
+}
+
+const compas_array* compas_make_array_float(const compas_context* context, const float* data, int rank,
+                                            int64_t* sizes) {
+    return guarded([&] { return make_array(context, data, rank, sizes); });
+}
+
+void compas_read_array_float(const compas_context*, const compas_array* array, float* dest, int64_t length) {
+    guarded([&] { read_array(array, dest, length, sizeof(float)); });
+}
+
+const compas_array* compas_make_array_complex(const compas_context* context, const compas_cfloat* data, int rank,
+                                              int64_t* sizes) {
+    return guarded([&] { return make_array(context, reinterpret_cast<const cfloat*>(data), rank, sizes); });
+}
+
+void compas_read_array_complex(const compas_context*, const compas_array* array, compas_cfloat* dest,
+                               int64_t length) {
+    guarded([&] { read_array(array, dest, length, sizeof(cfloat)); });
+}
+
+void compas_destroy_array(const compas_array* array) {
+    guarded([&] { delete handle<compas::Object>(array); });
+}
+
+const compas_object* compas_make_tissue_parameters(const compas_context* context, int nvoxels, const float* T1,
+                                                   const float* T2, const float* B1, const float* B0,
+                                                   const float* rho_x, const float* rho_y, const float* x,
+                                                   const float* y, const float* z) {
+    return guarded([&]() -> const compas_object* {
+        if (nvoxels < 0) throw compas::CompasException("negative voxel count");
+        auto view = [&](const float* p) { return compas::View<float>(p, {p ? nvoxels : 0}); };
+        return new_obj(compas::make_tissue_parameters(ctx_of(context), nvoxels, nvoxels, view(T1), view(T2),
+                                                      view(B1), view(B0), view(rho_x), view(rho_y), view(x),
+                                                      view(y), view(z)));
+    });
+}
+
+compas_object* compas_make_fisp_sequence(const compas_array* RF_train, const compas_array* sliceprofiles, float TR,
+                                         float TE, float TW, int max_state, float TI, int undersampling_factor,
+                                         int repetitions) {
+    return guarded([&]() -> compas_object* {
+        const auto& rf = array_of<cfloat, 1>(RF_train, "RF_train");
+        const auto& sp = array_of<cfloat, 2>(sliceprofiles, "sliceprofiles");
+        if (sp.size(1) != rf.size(0)) throw compas::CompasException("sliceprofiles must be [npositions][nTR]");
+        if (max_state < 1 || max_state > 128) throw compas::CompasException("max_state must be in [1, 128]");
+        if (undersampling_factor < 1 || repetitions < 1)
+            throw compas::CompasException("undersampling_factor and repetitions must be >= 1");
+        return new_obj(compas::FISPSequence(rf, sp, TR, TE, TW, max_state, TI, undersampling_factor, repetitions));
+    });
+}
+
+compas_object* compas_make_pssfp_sequence(const compas_array* RF_train, float TR, const compas_array* gamma_dt_RF,
+                                          float dt_ex, float dt_inv, float dt_pr, float gamma_dt_GRz_ex,
+                                          float gamma_dt_GRz_inv, float gamma_dt_GRz_pr, const compas_array* z) {
+    return guarded([&]() -> compas_object* {
+        const auto& rf = array_of<cfloat, 1>(RF_train, "RF_train");
+        const auto& g = array_of<cfloat, 1>(gamma_dt_RF, "gamma_dt_RF");
+        const auto& zz = array_of<float, 1>(z, "z");
+        if (rf.size() == 0) throw compas::CompasException("empty RF train");
+        return new_obj(compas::pSSFPSequence(rf, TR, g, compas::RepetitionData {dt_ex, dt_inv, dt_pr},
+                                             compas::RepetitionData {gamma_dt_GRz_ex, gamma_dt_GRz_inv,
+                                                                     gamma_dt_GRz_pr},
+                                             zz));
+    });
+}
+
+compas_object* compas_make_cartesian_trajectory(int nreadouts, int samples_per_readout, float delta_t,
+                                                compas_array* k_start, float delta_k) {
+    return guarded([&]() -> compas_object* {
+        const auto& ks = array_of<cfloat, 1>(k_start, "k_start");
+        if (ks.size() != nreadouts) throw compas::CompasException("k_start must have nreadouts entries");
+        if (nreadouts < 0 || samples_per_readout < 0) throw compas::CompasException("negative trajectory size");
+        return new_obj(compas::CartesianTrajectory(nreadouts, samples_per_readout, delta_t, ks, cfloat(delta_k, 0)));
+    });
+}
+
+compas_object* compas_make_spiral_trajectory(int nreadouts, int samples_per_readout, float delta_t,
+                                             compas_array* k_start, compas_array* delta_k) {
+    return guarded([&]() -> compas_object* {
+        const auto& ks = array_of<cfloat, 1>(k_start, "k_start");
+        const auto& dk = array_of<cfloat, 1>(delta_k, "delta_k");
+        if (ks.size() != nreadouts || dk.size() != nreadouts)
+            throw compas::CompasException("k_start and delta_k must have nreadouts entries");
+        if (nreadouts < 0 || samples_per_readout < 0) throw compas::CompasException("negative trajectory size");
+        return new_obj(compas::SpiralTrajectory(nreadouts, samples_per_readout, delta_t, ks, dk));
+    });
+}
+
+compas_array* compas_simulate_magnetization_fisp(const compas_context* ctx, const compas_object* parameters,
+                                                 const compas_object* sequence) {
+    return guarded([&] {
+        return new_array(compas::simulate_magnetization(ctx_of(ctx), unwrap<compas::TissueParameters>(parameters),
+                                                        unwrap<compas::FISPSequence>(sequence)));
+    });
+}
+
+compas_array* compas_simulate_magnetization_pssfp(const compas_context* ctx, const compas_object* parameters,
+                                                  const compas_object* sequence) {
+    return guarded([&] {
+        return new_array(compas::simulate_magnetization(ctx_of(ctx), unwrap<compas::TissueParameters>(parameters),
+                                                        unwrap<compas::pSSFPSequence>(sequence)));
+    });
+}
+
+compas_array* compas_magnetization_to_signal_cartesian(const compas_context* ctx, int ncoils,
+                                                       const compas_array* echos, const compas_object* parameters,
+                                                       const compas_array* coils, const compas_object* trajectory,
+                                                       int32_t low_precision) {
+    return guarded([&] {
+        const auto& co = array_of<cfloat, 2>(coils, "coils");
+        if (co.size(0) != ncoils) throw compas::CompasException("ncoils does not match the coil array");
+        auto method = low_precision == 0 ? compas::SimulateSignalMethod::MatmulFast
+                                         : compas::SimulateSignalMethod::MatmulLow;
+        return new_array(compas::magnetization_to_signal(
+            ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"), unwrap<compas::TissueParameters>(parameters),
+            unwrap<compas::CartesianTrajectory>(trajectory), co, method));
+    });
+}
+
+compas_array* compas_magnetization_to_signal_spiral(const compas_context* ctx, int ncoils, const compas_array* echos,
+                                                    const compas_object* parameters, const compas_array* coils,
+                                                    const compas_object* trajectory) {
+    return guarded([&] {
+        const auto& co = array_of<cfloat, 2>(coils, "coils");
+        if (co.size(0) != ncoils) throw compas::CompasException("ncoils does not match the coil array");
+        return new_array(compas::magnetization_to_signal(ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"),
+                                                         unwrap<compas::TissueParameters>(parameters),
+                                                         unwrap<compas::SpiralTrajectory>(trajectory), co));
+    });
+}
+
+compas_array* compas_compute_jacobian(const compas_context* ctx, int ncoils, const compas_array* echos,
+                                      const compas_array* delta_echos_T1, const compas_array* delta_echos_T2,
+                                      const compas_object* parameters, const compas_array* coils,
+                                      const compas_object* trajectory, const compas_array* vector,
+                                      const int32_t low_precision) {
+    return guarded([&] {
+        const auto& co = array_of<cfloat, 2>(coils, "coils");
+        if (co.size(0) != ncoils) throw compas::CompasException("ncoils does not match the coil array");
+        auto method =
+            low_precision == 0 ? compas::JacobianComputeMethod::GemmFast : compas::JacobianComputeMethod::GemmLow;
+        return new_array(compas::compute_jacobian(
+            ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"), array_of<cfloat, 2>(delta_echos_T1, "delta_echos_T1"),
+            array_of<cfloat, 2>(delta_echos_T2, "delta_echos_T2"), unwrap<compas::TissueParameters>(parameters),
+            unwrap<compas::CartesianTrajectory>(trajectory), co, array_of<cfloat, 2>(vector, "vector"), method));
+    });
+}
+
+compas_array* compas_compute_jacobian_hermitian(const compas_context* ctx, int ncoils, const compas_array* echos,
+                                                const compas_array* delta_echos_T1,
+                                                const compas_array* delta_echos_T2, const compas_object* parameters,
+                                                const compas_object* trajectory, const compas_array* coils,
+                                                const compas_array* vector, const int32_t low_precision) {
+    return guarded([&] {
+        const auto& co = array_of<cfloat, 2>(coils, "coils");
+        if (co.size(0) != ncoils) throw compas::CompasException("ncoils does not match the coil array");
+        auto method =
+            low_precision == 0 ? compas::JacobianComputeMethod::GemmFast : compas::JacobianComputeMethod::GemmLow;
+        return new_array(compas::compute_jacobian_hermitian(
+            ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"), array_of<cfloat, 2>(delta_echos_T1, "delta_echos_T1"),
+            array_of<cfloat, 2>(delta_echos_T2, "delta_echos_T2"), unwrap<compas::TissueParameters>(parameters),
+            unwrap<compas::CartesianTrajectory>(trajectory), co, array_of<cfloat, 3>(vector, "vector"), method));
+    });
+}
+
+compas_array* phase_encoding(const compas_context* ctx, const compas_array* echos, const compas_object* parameters,
+                             const compas_object* trajectory) {
+    return guarded([&] {
+        return new_array(compas::phase_encoding(ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"),
+                                                unwrap<compas::TissueParameters>(parameters),
+                                                unwrap<compas::CartesianTrajectory>(trajectory)));
+    });
+}
+
+compas_array* compas_compute_residual(const compas_context* ctx, const compas_array* lhs, const compas_array* rhs,
+                                      float* sum) {
+    return guarded([&] {
+        return new_array(compas::compute_residual(ctx_of(ctx), array_of<cfloat, 3>(lhs, "lhs"),
+                                                  array_of<cfloat, 3>(rhs, "rhs"), sum));
+    });
+}
+
+compas_array* compas_simulate_magnetization_derivative_pssfp(const compas_context* ctx, int field,
+                                                             const compas_array* echos,
+                                                             const compas_object* parameters, float delta,
+                                                             const compas_object* sequence) {
+    return guarded([&] {
+        return new_array(compas::simulate_magnetization_derivative(
+            ctx_of(ctx), field, array_of<cfloat, 2>(echos, "echos"), unwrap<compas::TissueParameters>(parameters),
+            unwrap<compas::pSSFPSequence>(sequence), delta));
+    });
+}
+
+compas_array* compas_simulate_magnetization_derivative_fisp(const compas_context* ctx, int field,
+                                                            const compas_array* echos, const compas_object* parameters,
+                                                            float delta, const compas_object* sequence) {
+    return guarded([&] {
+        return new_array(compas::simulate_magnetization_derivative(
+            ctx_of(ctx), field, array_of<cfloat, 2>(echos, "echos"), unwrap<compas::TissueParameters>(parameters),
+            unwrap<compas::FISPSequence>(sequence), delta));
+    });
+}
+
+compas_array* compas_b200_magnetization_to_signal(const compas_context* ctx, const compas_array* echos,
+                                                  const compas_object* parameters, const compas_object* trajectory,
+                                                  const compas_array* coils, int method) {
+    return guarded([&] {
+        if (!trajectory) throw compas::CompasException("null trajectory");
+        return new_array(compas::magnetization_to_signal(
+            ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"), unwrap<compas::TissueParameters>(parameters),
+            unwrap<compas::Trajectory>(trajectory), array_of<cfloat, 2>(coils, "coils"), signal_method(method)));
+    });
+}
+
+compas_array* compas_b200_compute_jacobian(const compas_context* ctx, const compas_array* echos,
+                                           const compas_array* delta_echos_T1, const compas_array* delta_echos_T2,
+                                           const compas_object* parameters, const compas_object* trajectory,
+                                           const compas_array* coils, const compas_array* vector, int method) {
+    return guarded([&] {
+        return new_array(compas::compute_jacobian(
+            ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"), array_of<cfloat, 2>(delta_echos_T1, "delta_echos_T1"),
+            array_of<cfloat, 2>(delta_echos_T2, "delta_echos_T2"), unwrap<compas::TissueParameters>(parameters),
+            unwrap<compas::CartesianTrajectory>(trajectory), array_of<cfloat, 2>(coils, "coils"),
+            array_of<cfloat, 2>(vector, "vector"), jacobian_method(method)));
+    });
+}
+
+compas_array* compas_b200_compute_jacobian_hermitian(const compas_context* ctx, const compas_array* echos,
+                                                     const compas_array* delta_echos_T1,
+                                                     const compas_array* delta_echos_T2,
+                                                     const compas_object* parameters,
+                                                     const compas_object* trajectory, const compas_array* coils,
+                                                     const compas_array* vector, int method) {
+    return guarded([&] {
+        return new_array(compas::compute_jacobian_hermitian(
+            ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"), array_of<cfloat, 2>(delta_echos_T1, "delta_echos_T1"),
+            array_of<cfloat, 2>(delta_echos_T2, "delta_echos_T2"), unwrap<compas::TissueParameters>(parameters),
+            unwrap<compas::CartesianTrajectory>(trajectory), array_of<cfloat, 2>(coils, "coils"),
+            array_of<cfloat, 3>(vector, "vector"), jacobian_method(method)));
+    });
+}
+
+void* compas_b200_context_stream(const compas_context* ctx) {
+    return guarded([&]() -> void* { return reinterpret_cast<void*>(ctx_of(ctx).stream()); });
+}
+
+void* compas_b200_array_device_ptr(const compas_array* array) {
+    return guarded([&]() -> void* {
+        const auto* base = dynamic_cast<const compas::ArrayBase*>(handle<compas::Object>(array));
+        if (!base) throw compas::CompasException("handle is not an array");
+        return base->raw_data();
+    });
+}
+
+int compas_b200_array_rank(const compas_array* array) {
+    return guarded([&]() -> int {
+        const auto* base = dynamic_cast<const compas::ArrayBase*>(handle<compas::Object>(array));
+        if (!base) throw compas::CompasException("handle is not an array");
+        return base->rank();
+    });
+}
+
+int64_t compas_b200_array_extent(const compas_array* array, int axis) {
+    return guarded([&]() -> int64_t {
+        const auto* base = dynamic_cast<const compas::ArrayBase*>(handle<compas::Object>(array));
+        if (!base) throw compas::CompasException("handle is not an array");
+        if (axis < 0 || axis >= base->rank()) throw compas::CompasException("axis out of range");
+        return base->extent(axis);
+    });
+}
+
+void compas_b200_set_fisp_launch(int config, int warps) {
+    guarded([&] { compas::set_fisp_override(config, warps); });
+}
+
+void compas_b200_set_pssfp_launch(int config) {
+    guarded([&] { compas::set_pssfp_override(config); });
+}
+
+uint64_t compas_b200_launch_count(void) {
+    return compas::launch_count();
+}
+
+int compas_b200_fisp_config_count(void) {
+    return compas::fisp_config_count();
+}
+
+int compas_b200_fisp_config_info(int index, int* states_per_lane, int* lanes) {
+    return compas::fisp_config_info(index, states_per_lane, lanes) ? 1 : 0;
+}
+
+int compas_b200_pssfp_config_count(void) {
+    return compas::pssfp_config_count();
+}
+
+int compas_b200_pssfp_config_info(int index, int* iso_per_lane, int* lanes) {
+    return compas::pssfp_config_info(index, iso_per_lane, lanes) ? 1 : 0;
+}
+
+}  // extern "C"

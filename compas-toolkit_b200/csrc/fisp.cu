@@ -1,0 +1,450 @@
+// fisp.cu — FISP extended-phase-graph simulation on sm_100a.
+//
+// Restates the reference's FISP EPG recurrence (src/operators/epg.cuh:13-322,
+// src/simulate/fisp_kernels.cuh:99-223, src/simulate/fisp.cu:269-402) with a layout
+// chosen for B200:
+//
+// * Work unit: one (voxel, slice position) pair per group of G lanes; each lane keeps
+//   K consecutive EPG states (F+, F-, Z) in registers (G = 1: the whole state vector of
+//   a voxel/position lives in one thread — no shuffles at all). A CTA holds VB = 32/G
+//   voxels; its W warps sweep the slice positions round-robin and the per-TR samples of
+//   all positions are summed in shared memory in a fixed order (deterministic result).
+// * Algebra (exact rearrangement of the reference's per-TR sequence excite → decay(TE) →
+//   sample → decay(TR-TE) → dephase): decay and rotation commute with the dephasing shift,
+//   so the two relaxation steps of TR t are folded into the excitation matrix of TR t+1
+//   (M' = M·diag(c, c̄, E1), c = E2(TR)·e^{2πi·B0·TR}); the regrowth becomes one additive
+//   term on state 0. F+ and g = conj(F-) are stored; the update is done on
+//   P = F+ + conj(F-), Q = F+ - conj(F-), in which M' is 2×2-block structured. Per state
+//   and TR this is 26 FP32 operations against 48 for the reference's order.
+// * The per-(position, TR) RF angle and phase table is built once per sequence and kept
+//   resident with it.
+#include <cfloat>
+
+#include "common.cuh"
+#include "compas/compas.h"
+#include "kernels.h"
+
+namespace compas {
+namespace kernels {
+
+// table[p][t] = {½·(π/180)·|sliceprofile[p][t]·RF[t]|, cos φ, sin φ, 0}
+__global__ void fisp_table_kernel(const float2* __restrict__ rf, const float2* __restrict__ slices, int nTR,
+                                  int P, float4* __restrict__ table) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nTR * P) return;
+    int t = i % nTR;
+    float2 s = slices[i], r = rf[t];
+    double re = double(s.x) * r.x - double(s.y) * r.y;
+    double im = double(s.x) * r.y + double(s.y) * r.x;
+    double a = sqrt(re * re + im * im);
+    double cp = 1.0, sp = 0.0;
+    if (a > double(FLT_MIN)) {  // epg.cuh:64-67
+        cp = re / a;
+        sp = im / a;
+    }
+    table[i] = make_float4(float(0.5 * (M_PI / 180.0) * a), float(cp), float(sp), 0.0f);
+}
+
+struct FispArgs {
+    const float* params;   // [9][param_stride]
+    int64_t param_stride;
+    int voxel_begin;       // first voxel of this launch
+    int nvoxels;           // voxels in this launch
+    const float4* table;   // [P][nTR]
+    int nTR, P, N, uf, reps, inversion, wait_spoil;
+    float TR, TE, TW, TI;
+    float2* echo;          // [nTR*uf][echo_stride], column = voxel_begin + local voxel
+    int64_t echo_stride;
+};
+
+// Excitation coefficients of one TR, already multiplied by the preceding relaxation
+// D = diag(c, c̄, E1) (see file header). Halved where the P/Q update needs it.
+struct ExciteCoefs {
+    float A1, A2, A3, A4;   // ½(a ± b) combinations
+    float dre, dim;         // d = R13·E1
+    float ere, eim;         // e = R31·c
+    float f;                // R33·E1
+    float bre, bim, bz;     // β·R13 (added to F+0 and conj(F-0)), β·R33 (added to Z0)
+};
+
+__device__ __forceinline__ ExciteCoefs make_coefs(float4 tab, float B1, float2 c, float E1, float beta) {
+    float s, co;
+    __sincosf(tab.x * B1, &s, &co);  // x = α/2   (epg.cuh:41-51)
+    float s2 = s * s, c2 = co * co;
+    float sa = 2.0f * s * co;        // sin α
+    float ca = 2.0f * c2 - 1.0f;     // cos α
+    float cp = tab.y, sp = tab.z;
+    float cos2p = 2.0f * cp * cp - 1.0f, sin2p = 2.0f * cp * sp;
+    // R11 = cos²(α/2), R12 = e^{2iφ} sin²(α/2), R13 = -i e^{iφ} sin α, R31 = -½ conj(R13), R33 = cos α
+    float r12re = cos2p * s2, r12im = sin2p * s2;
+    float r13re = sp * sa, r13im = -cp * sa;
+    float r31re = -0.5f * r13re, r31im = 0.5f * r13im;
+    // a = R11·c, b = R12·c̄, d = R13·E1, e = R31·c, f = R33·E1
+    float are = c2 * c.x, aim = c2 * c.y;
+    float bre = r12re * c.x + r12im * c.y, bim = r12im * c.x - r12re * c.y;
+    ExciteCoefs k;
+    k.A1 = 0.5f * (are + bre);
+    k.A2 = 0.5f * (bim - aim);
+    k.A3 = 0.5f * (aim + bim);
+    k.A4 = 0.5f * (are - bre);
+    k.dre = r13re * E1;
+    k.dim = r13im * E1;
+    k.ere = r31re * c.x - r31im * c.y;
+    k.eim = r31re * c.y + r31im * c.x;
+    k.f = ca * E1;
+    k.bre = beta * r13re;
+    k.bim = beta * r13im;
+    k.bz = beta * ca;
+    return k;
+}
+
+// y ← M'·x for one state (F+ = u, conj(F-) = g, Z = z)
+__device__ __forceinline__ void excite_state(float2& u, float2& g, float2& z, const ExciteCoefs& k) {
+    float Pr = u.x + g.x, Pi = u.y + g.y;
+    float Qr = u.x - g.x, Qi = u.y - g.y;
+    float Phr = fmaf(k.A1, Pr, fmaf(k.A2, Pi, k.dre * z.x));
+    float Phi = fmaf(k.A3, Pr, fmaf(k.A4, Pi, k.dim * z.x));
+    float Qhr = fmaf(k.A4, Qr, fmaf(-k.A3, Qi, -k.dim * z.y));
+    float Qhi = fmaf(-k.A2, Qr, fmaf(k.A1, Qi, k.dre * z.y));
+    float zr = fmaf(k.ere, Pr, fmaf(-k.eim, Pi, k.f * z.x));
+    float zi = fmaf(k.ere, Qi, fmaf(k.eim, Qr, k.f * z.y));
+    u = make_float2(Phr + Qhr, Phi + Qhi);
+    g = make_float2(Phr - Qhr, Phi - Qhi);
+    z = make_float2(zr, zi);
+}
+
+template<int K, int G>
+struct EPG {
+    float2 u[K], g[K], z[K];
+
+    __device__ __forceinline__ void init(int sub) {
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            u[i] = g[i] = z[i] = make_float2(0.f, 0.f);
+        }
+        if (sub == 0) z[0].x = 1.0f;
+    }
+
+    // dephasing gradient (epg.cuh:229-298): F- one state down with zero at ≥ N-1,
+    // F+ one state up, F+0 = conj(F-0)
+    __device__ __forceinline__ void shift(int sub, int N) {
+        if constexpr (G == 1) {
+#pragma unroll
+            for (int i = 0; i < K - 1; i++) g[i] = g[i + 1];
+            g[K - 1] = make_float2(0.f, 0.f);
+            if (N < K) {
+#pragma unroll
+                for (int i = 0; i < K; i++)
+                    if (i == N - 1) g[i] = make_float2(0.f, 0.f);
+            }
+#pragma unroll
+            for (int i = K - 1; i > 0; i--) u[i] = u[i - 1];
+            u[0] = g[0];
+        } else {
+            const unsigned mask = 0xffffffffu;
+            float gx = __shfl_down_sync(mask, g[0].x, 1, G);
+            float gy = __shfl_down_sync(mask, g[0].y, 1, G);
+            float ux = __shfl_up_sync(mask, u[K - 1].x, 1, G);
+            float uy = __shfl_up_sync(mask, u[K - 1].y, 1, G);
+#pragma unroll
+            for (int i = 0; i < K - 1; i++) g[i] = g[i + 1];
+            g[K - 1] = (sub == G - 1) ? make_float2(0.f, 0.f) : make_float2(gx, gy);
+            const int lane_n = (N - 1) / K, slot_n = (N - 1) % K;
+            if (sub == lane_n) {
+#pragma unroll
+                for (int i = 0; i < K; i++)
+                    if (i == slot_n) g[i] = make_float2(0.f, 0.f);
+            }
+#pragma unroll
+            for (int i = K - 1; i > 0; i--) u[i] = u[i - 1];
+            u[0] = (sub == 0) ? g[0] : make_float2(ux, uy);
+        }
+    }
+
+    __device__ __forceinline__ void excite(const ExciteCoefs& k, int sub) {
+#pragma unroll
+        for (int i = 0; i < K; i++) excite_state(u[i], g[i], z[i], k);
+        if (sub == 0) {
+            u[0].x += k.bre;
+            u[0].y += k.bim;
+            g[0].x += k.bre;
+            g[0].y += k.bim;
+            z[0].x += k.bz;
+        }
+    }
+
+    // F *= c (F+ by c, F- by c̄ ⇒ conj(F-) by c), Z *= E1, Z0 += 1 - E1
+    __device__ __forceinline__ void relax(float2 c, float E1, int sub) {
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            u[i] = cmul(u[i], c);
+            g[i] = cmul(g[i], c);
+            z[i] = cscale(E1, z[i]);
+        }
+        if (sub == 0) z[0].x += 1.0f - E1;
+    }
+
+    __device__ __forceinline__ void invert_spoil() {
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            u[i] = g[i] = make_float2(0.f, 0.f);
+            z[i] = make_float2(-z[i].x, -z[i].y);
+        }
+    }
+
+    __device__ __forceinline__ void spoil() {
+#pragma unroll
+        for (int i = 0; i < K; i++) u[i] = g[i] = make_float2(0.f, 0.f);
+    }
+};
+
+template<int K, int G>
+__global__ void __launch_bounds__(256, 1) fisp_epg_kernel(FispArgs a) {
+    constexpr int VB = 32 / G;
+    extern __shared__ float2 samples[];  // [W][32][VB]
+    const int W = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane / G, sub = lane % G;
+    const int vloc = blockIdx.x * VB + grp;
+    const bool vok = vloc < a.nvoxels;
+    const int64_t vcol = a.voxel_begin + (vok ? vloc : a.nvoxels - 1);
+
+    const float T1 = a.params[0 * a.param_stride + vcol];
+    const float T2 = a.params[1 * a.param_stride + vcol];
+    const float B1 = a.params[2 * a.param_stride + vcol];
+    const float B0 = a.params[3 * a.param_stride + vcol];
+
+    // per-voxel relaxation factors (fisp_kernels.cuh:110-144)
+    const float R1 = 1.0f / T1, R2 = 1.0f / T2;
+    auto rot = [&](float dt) -> float2 {
+        if (B0 == 0.0f) return make_float2(1.f, 0.f);
+        float s, c;
+        sincospif(2.0f * dt * B0, &s, &c);
+        return make_float2(c, s);
+    };
+    const float E1_TR = expf(-a.TR * R1), E2_TR = expf(-a.TR * R2);
+    const float2 c_TR = cscale(E2_TR, rot(a.TR));
+    const float2 c_TE = cscale(expf(-a.TE * R2), rot(a.TE));
+    const float E1_TI = expf(-a.TI * R1);
+    const float E1_W = expf(-a.TW * R1);
+    const float2 c_W = cscale(expf(-a.TW * R2), rot(a.TW));
+    const float beta = 1.0f - E1_TR;
+
+    const int nrounds = (a.P + W - 1) / W;
+    for (int round = 0; round < nrounds; round++) {
+        const int p = round * W + warp;
+        const bool pok = p < a.P;  // warp-uniform
+        const float4* tab = a.table + int64_t(pok ? p : 0) * a.nTR;
+        EPG<K, G> st;
+        st.init(sub);
+        for (int rep = a.reps; rep >= 1; rep--) {
+            const bool sampled = (rep == 1);
+            if (a.inversion) {  // invert, spoil, decay(TI), regrowth (fisp_kernels.cuh:146-152)
+                st.invert_spoil();
+#pragma unroll
+                for (int i = 0; i < K; i++) st.z[i] = cscale(E1_TI, st.z[i]);
+                if (sub == 0) st.z[0].x += 1.0f - E1_TI;
+            }
+            for (int t0 = 0; t0 < a.nTR; t0 += 32) {
+                const int nt = min(32, a.nTR - t0);
+                if (pok) {
+                    for (int j = 0; j < nt; j++) {
+                        const int t = t0 + j;
+                        const float4 tv = __ldg(tab + t);
+                        if (t == 0) {
+                            st.excite(make_coefs(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), sub);
+                        } else {
+                            st.shift(sub, a.N);
+                            st.excite(make_coefs(tv, B1, c_TR, E1_TR, beta), sub);
+                        }
+                        if (sampled && sub == 0) samples[(warp * 32 + j) * VB + grp] = cmul(c_TE, st.u[0]);
+                    }
+                } else if (sampled && sub == 0) {
+                    for (int j = 0; j < nt; j++) samples[(warp * 32 + j) * VB + grp] = make_float2(0.f, 0.f);
+                }
+                if (sampled) {
+                    __syncthreads();
+                    // Σ over the warps' positions in fixed order, then write / accumulate the
+                    // undersampling-expanded rows (fisp_kernels.cuh:246-259)
+                    for (int e = threadIdx.x; e < nt * VB; e += blockDim.x) {
+                        const int j = e / VB, gv = e % VB;
+                        const int v = blockIdx.x * VB + gv;
+                        float2 acc = make_float2(0.f, 0.f);
+                        for (int w = 0; w < W; w++) acc = cadd(acc, samples[(w * 32 + j) * VB + gv]);
+                        if (v < a.nvoxels) {
+                            for (int q = 0; q < a.uf; q++) {
+                                float2* dst = a.echo + (int64_t(t0 + j) * a.uf + q) * a.echo_stride + a.voxel_begin + v;
+                                *dst = round == 0 ? acc : cadd(*dst, acc);
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+            if (rep > 1) {  // close the repetition: relax to TR, dephase, spoil, wait (fisp_kernels.cuh:195-200)
+                if (pok) {
+                    st.relax(c_TR, E1_TR, sub);
+                    st.shift(sub, a.N);
+                    if (a.wait_spoil) st.spoil();
+                    st.relax(c_W, E1_W, sub);
+                }
+            }
+        }
+    }
+}
+
+}  // namespace kernels
+
+// ------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------
+
+namespace {
+
+using FispKernel = void (*)(kernels::FispArgs);
+
+struct FispConfig {
+    int K, G;
+    FispKernel fn;
+};
+
+// Instantiated layouts: (states per lane K, lanes per voxel/position G). Coverage K·G ≥ N.
+const FispConfig kFispConfigs[] = {
+    {1, 1, kernels::fisp_epg_kernel<1, 1>},     {2, 1, kernels::fisp_epg_kernel<2, 1>},
+    {4, 1, kernels::fisp_epg_kernel<4, 1>},     {6, 1, kernels::fisp_epg_kernel<6, 1>},
+    {8, 1, kernels::fisp_epg_kernel<8, 1>},     {12, 1, kernels::fisp_epg_kernel<12, 1>},
+    {16, 1, kernels::fisp_epg_kernel<16, 1>},   {20, 1, kernels::fisp_epg_kernel<20, 1>},
+    {25, 1, kernels::fisp_epg_kernel<25, 1>},   {2, 4, kernels::fisp_epg_kernel<2, 4>},
+    {4, 2, kernels::fisp_epg_kernel<4, 2>},     {4, 4, kernels::fisp_epg_kernel<4, 4>},
+    {4, 8, kernels::fisp_epg_kernel<4, 8>},     {7, 4, kernels::fisp_epg_kernel<7, 4>},
+    {13, 2, kernels::fisp_epg_kernel<13, 2>},   {8, 4, kernels::fisp_epg_kernel<8, 4>},
+    {8, 8, kernels::fisp_epg_kernel<8, 8>},     {8, 16, kernels::fisp_epg_kernel<8, 16>},
+    {4, 32, kernels::fisp_epg_kernel<4, 32>},
+};
+
+}  // namespace
+
+int fisp_config_count() {
+    return int(sizeof(kFispConfigs) / sizeof(kFispConfigs[0]));
+}
+
+bool fisp_config_info(int index, int* K, int* G) {
+    if (index < 0 || index >= fisp_config_count()) return false;
+    *K = kFispConfigs[index].K;
+    *G = kFispConfigs[index].G;
+    return true;
+}
+
+// Default layout choice for `N` states: the smallest single-lane layout that covers N for
+// N ≤ 25 when there are enough (voxel, position) pairs to fill the GPU, otherwise a
+// lane-split layout. The autotuner (tuning.cpp) may override it per shape class.
+FispLaunch fisp_default_launch(int N, int64_t nvoxels, int P) {
+    FispLaunch L {-1, 1};
+    const int64_t pairs = nvoxels * P;
+    const bool wide = pairs >= 148LL * 32 * 8;
+    int best = -1;
+    for (int i = 0; i < fisp_config_count(); i++) {
+        const auto& c = kFispConfigs[i];
+        if (c.K * c.G < N) continue;
+        if (wide && c.G != 1) continue;
+        if (!wide && N > 1 && c.G == 1 && nvoxels < 148 * 64) continue;
+        if (best < 0) {
+            best = i;
+            continue;
+        }
+        const auto& b = kFispConfigs[best];
+        int waste_c = c.K * c.G - N, waste_b = b.K * b.G - N;
+        if (waste_c < waste_b || (waste_c == waste_b && c.G < b.G)) best = i;
+    }
+    if (best < 0) {  // nothing matched the width preference: any covering layout
+        for (int i = 0; i < fisp_config_count(); i++)
+            if (kFispConfigs[i].K * kFispConfigs[i].G >= N && (best < 0 || kFispConfigs[i].G > kFispConfigs[best].G))
+                best = i;
+    }
+    L.config = best;
+    L.warps = P >= 5 ? (P % 7 == 0 ? 7 : 5) : P;
+    if (L.warps < 1) L.warps = 1;
+    if (L.warps > 8) L.warps = 8;
+    return L;
+}
+
+const Array<float, 3>& fisp_excite_table(const CompasContext& ctx, const FISPSequence& seq) {
+    if (!seq.excite_table) {
+        int nTR = int(seq.RF_train.size());
+        int P = int(seq.sliceprofiles.size(0));
+        COMPAS_CHECK(int(seq.sliceprofiles.size(1)) == nTR);
+        auto tab = std::make_shared<Array<float, 3>>(std::array<int64_t, 3> {P, nTR, 4}, ctx.device());
+        DeviceGuard guard(ctx.device());
+        int n = nTR * P;
+        if (n > 0) {
+            kernels::fisp_table_kernel<<<div_ceil(n, 256), 256, 0, ctx.stream()>>>(
+                reinterpret_cast<const float2*>(seq.RF_train.data()),
+                reinterpret_cast<const float2*>(seq.sliceprofiles.data()), nTR, P,
+                reinterpret_cast<float4*>(tab->data()));
+            check_launch("fisp_table_kernel");
+        }
+        seq.excite_table = tab;
+    }
+    return *seq.excite_table;
+}
+
+void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
+                 const FISPSequence& seq, cfloat* echo, int64_t echo_stride, FispLaunch L) {
+    const int nTR = int(seq.RF_train.size());
+    const int P = int(seq.sliceprofiles.size(0));
+    const int N = seq.max_state;
+    if (N < 1 || N > 128) COMPAS_ERROR("max_state must be in [1, 128]");
+    COMPAS_CHECK(seq.undersampling_factor >= 1 && seq.repetitions >= 1);
+    COMPAS_CHECK(P >= 1 && int(seq.sliceprofiles.size(1)) == nTR);
+    if (nvoxels <= 0 || nTR <= 0) return;
+    if (L.config < 0) L = fisp_default_launch(N, nvoxels, P);
+    COMPAS_CHECK(L.config >= 0 && L.config < fisp_config_count());
+    const auto& cfg = kFispConfigs[L.config];
+    COMPAS_CHECK(cfg.K * cfg.G >= N);
+    const auto& tab = fisp_excite_table(ctx, seq);
+
+    kernels::FispArgs a;
+    a.params = params.data.data();
+    a.param_stride = params.data.size(1);
+    a.voxel_begin = voxel_begin;
+    a.nvoxels = nvoxels;
+    a.table = reinterpret_cast<const float4*>(tab.data());
+    a.nTR = nTR;
+    a.P = P;
+    a.N = N;
+    a.uf = seq.undersampling_factor;
+    a.reps = seq.repetitions;
+    a.inversion = seq.inversion_prepulse ? 1 : 0;
+    a.wait_spoil = seq.wait_spoiling ? 1 : 0;
+    a.TR = seq.TR;
+    a.TE = seq.TE;
+    a.TW = seq.TW;
+    a.TI = seq.TI;
+    a.echo = reinterpret_cast<float2*>(echo);
+    a.echo_stride = echo_stride;
+
+    const int VB = 32 / cfg.G;
+    const int W = std::max(1, std::min(L.warps, 8));
+    dim3 grid(div_ceil(nvoxels, VB)), block(32 * W);
+    size_t smem = size_t(W) * 32 * VB * sizeof(float2);  // ≤ 64 KB (W ≤ 8)
+    DeviceGuard guard(ctx.device());
+    if (smem > 48 * 1024) {
+        COMPAS_CUDA_CHECK(cudaFuncSetAttribute(reinterpret_cast<const void*>(cfg.fn),
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    }
+    cfg.fn<<<grid, block, smem, ctx.stream()>>>(a);
+    check_launch("fisp_epg_kernel");
+}
+
+Array<cfloat, 2> simulate_magnetization(const CompasContext& context, TissueParameters parameters,
+                                        FISPSequence sequence) {
+    const int nTR = int(sequence.RF_train.size());
+    const int nreadouts = nTR * sequence.undersampling_factor;
+    const int nvoxels = parameters.nvoxels;
+    COMPAS_CHECK(sequence.undersampling_factor >= 1);
+    Array<cfloat, 2> echos({nreadouts, nvoxels}, context.device());
+    launch_fisp(context, parameters, 0, nvoxels, sequence, echos.data(), nvoxels, tuned_fisp_launch(sequence.max_state, nvoxels, int(sequence.sliceprofiles.size(0))));
+    return echos;
+}
+
+}  // namespace compas

@@ -1,0 +1,69 @@
+// kernels.h — internal launch interfaces between the host operations, the batch /
+// graph / serving layers and the autotuner. Not part of the public API.
+#pragma once
+
+#include <cstdint>
+
+#include "compas/compas.h"
+
+namespace compas {
+
+// ---- FISP EPG -------------------------------------------------------------------------
+struct FispLaunch {
+    int config;  // index into the instantiated (K, G) layouts, -1 = default choice
+    int warps;   // warps per CTA (slice positions in flight per voxel tile)
+};
+int fisp_config_count();
+bool fisp_config_info(int index, int* K, int* G);
+FispLaunch fisp_default_launch(int N, int64_t nvoxels, int P);
+FispLaunch tuned_fisp_launch(int N, int64_t nvoxels, int P);
+const Array<float, 3>& fisp_excite_table(const CompasContext& ctx, const FISPSequence& seq);
+// simulates voxels [voxel_begin, voxel_begin + nvoxels) of `params` into echo columns
+// voxel_begin.. of a [nTR*uf][echo_stride] complex array
+void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
+                 const FISPSequence& seq, cfloat* echo, int64_t echo_stride, FispLaunch L);
+
+// ---- pSSFP ------------------------------------------------------------------------------
+struct PssfpLaunch {
+    int config;  // index into the instantiated (ZT, GZ) layouts, -1 = default
+};
+int pssfp_config_count();
+bool pssfp_config_info(int index, int* ZT, int* GZ);
+PssfpLaunch pssfp_default_launch(int nz, int64_t nvoxels);
+PssfpLaunch tuned_pssfp_launch(int nz, int64_t nvoxels);
+void launch_pssfp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
+                  const pSSFPSequence& seq, cfloat* echo, int64_t echo_stride, PssfpLaunch L);
+
+// ---- signal / Jacobian products ----------------------------------------------------------
+enum class Precision { FP32, SplitBF16 };
+
+struct CartesianGeom {
+    int nreadouts, ns;
+    float dt;
+    float dk_re, dk_im;
+};
+
+// s[c][r][k] = Σ_v coil[c][v]·ρ_v·m[r][v]·w_v·z_v^k  (Cartesian, signal_kernels.cuh:137-167)
+void launch_signal_cartesian(const CompasContext& ctx, const float* params, int64_t param_stride, int nvoxels,
+                             const cfloat* echos, const cfloat* coils, int ncoils, const CartesianGeom& g,
+                             cfloat* signal, Precision prec);
+void launch_signal_spiral(const CompasContext& ctx, const float* params, int64_t param_stride, int nvoxels,
+                          const cfloat* echos, const cfloat* coils, int ncoils, int nreadouts, int ns, float dt,
+                          const cfloat* k_start, const cfloat* delta_k, cfloat* signal);
+void launch_jacobian(const CompasContext& ctx, const float* params, int64_t param_stride, int nvoxels,
+                     const cfloat* echos, const cfloat* dT1, const cfloat* dT2, const cfloat* coils, int ncoils,
+                     const cfloat* vec, const CartesianGeom& g, cfloat* Jv, Precision prec);
+void launch_jacobian_hermitian(const CompasContext& ctx, const float* params, int64_t param_stride, int nvoxels,
+                               const cfloat* echos, const cfloat* dT1, const cfloat* dT2, const cfloat* coils,
+                               int ncoils, const cfloat* vec, const CartesianGeom& g, cfloat* JHv, Precision prec);
+
+// ---- elementwise -------------------------------------------------------------------------
+void launch_phase_encoding(const CompasContext& ctx, const cfloat* echos, const float* params, int64_t param_stride,
+                           int nvoxels, int nreadouts, const cfloat* k_start, cfloat* out);
+void launch_residual(const CompasContext& ctx, const cfloat* lhs, const cfloat* rhs, int64_t n, cfloat* out,
+                     float* partials, int npartials, float* objective);
+
+// ---- tcgen05 tensor-core complex GEMM support ---------------------------------------------
+bool tensor_cores_available(int device);
+
+}  // namespace compas

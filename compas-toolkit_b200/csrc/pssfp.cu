@@ -1,0 +1,277 @@
+// pssfp.cu — pSSFP isochromat (Bloch) simulation on sm_100a.
+//
+// Restates src/simulate/pssfp_kernels.cuh:14-129 and src/operators/isochromat.cuh:9-128:
+// per (voxel, z) an isochromat is inverted (cos πB1), relaxed, given an α/2 pulse, and then
+// for each TR excited by n_RF hard-pulse Rodrigues rotations (each followed by relaxation),
+// precessed, sampled (Σ_z m_x + i m_y) and precessed again.
+//
+// B200 layout: a thread owns ZT isochromats of one voxel and GZ lanes (a power of two)
+// cover the z positions; the per-TR sum over z is a register sum plus an xor-shuffle tree.
+// The RF rotation axis (Re, -Im)(RF[t]·γΔtRF[i])·B1 is the same for every z, so the
+// products RF[t]·γΔtRF[i] are tabulated once per sequence; the z-dependent axis component
+// and the precession angles are constant over the TR loop and hoisted out of it (the
+// precession sin/cos is evaluated once per z instead of twice per TR). The rotation uses
+// the unnormalised-axis Rodrigues form
+//     m' = cos θ·m + (sin θ/θ)·(a×m) + ((1-cos θ)/θ²)·(a·m)·a,   θ² = a·a,
+// whose three coefficients are Taylor polynomials in θ² (coefficients 1/n!) for θ ≤ 0.5 rad,
+// accurate to < 3e-10, so the hot loop runs on the FMA pipe; larger angles use sqrt/sincos.
+#include "common.cuh"
+#include "compas/compas.h"
+#include "kernels.h"
+
+namespace compas {
+namespace kernels {
+
+// zap[0][i] = -(RF[0]/2)·γΔtRF[i] (the α/2 pulse), zap[1+t][i] = RF[t]·γΔtRF[i]
+__global__ void pssfp_table_kernel(const float2* __restrict__ rf, int nTR, const float2* __restrict__ g, int nRF,
+                                   float2* __restrict__ zap) {
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (nTR + 1) * nRF) return;
+    int row = idx / nRF, i = idx % nRF;
+    float2 th = row == 0 ? make_float2(-rf[0].x / 2.0f, -rf[0].y / 2.0f) : rf[row - 1];
+    zap[idx] = cmul(th, g[i]);
+}
+
+struct PssfpArgs {
+    const float* params;
+    int64_t param_stride;
+    int voxel_begin, nvoxels;
+    const float2* zap;  // [nTR+1][nRF]
+    const float* z;     // [nz]
+    int nTR, nRF, nz;
+    float dt_ex, dt_inv, dt_pr, gz_ex, gz_pr;
+    float2* echo;  // [nTR][echo_stride]
+    int64_t echo_stride;
+};
+
+struct Iso {
+    float x, y, z;
+};
+
+// rotation about the unnormalised axis (ax, ay, az) by |a|   (isochromat.cuh:14-73)
+__device__ __forceinline__ void rodrigues(Iso& m, float ax, float ay, float az, float axy2) {
+    const float t2 = fmaf(az, az, axy2);
+    float c, s, h;
+    if (t2 <= 0.25f) {
+        // cos θ, sin θ/θ, (1-cos θ)/θ² as Taylor series in x = θ² through x⁴
+        const float x = t2;
+        c = fmaf(x, fmaf(x, fmaf(x, fmaf(x, 1.0f / 40320.0f, -1.0f / 720.0f), 1.0f / 24.0f), -0.5f), 1.0f);
+        s = fmaf(x, fmaf(x, fmaf(x, fmaf(x, 1.0f / 362880.0f, -1.0f / 5040.0f), 1.0f / 120.0f), -1.0f / 6.0f), 1.0f);
+        h = fmaf(x, fmaf(x, fmaf(x, fmaf(x, 1.0f / 3628800.0f, -1.0f / 40320.0f), 1.0f / 720.0f), -1.0f / 24.0f), 0.5f);
+    } else {
+        const float th = sqrtf(t2);
+        float sn, cs;
+        sincosf(th, &sn, &cs);
+        c = cs;
+        s = sn / th;
+        h = (1.0f - cs) / t2;
+    }
+    const float cx = ay * m.z - az * m.y;
+    const float cy = az * m.x - ax * m.z;
+    const float cz = ax * m.y - ay * m.x;
+    const float hd = h * fmaf(ax, m.x, fmaf(ay, m.y, az * m.z));
+    m.x = fmaf(c, m.x, fmaf(s, cx, hd * ax));
+    m.y = fmaf(c, m.y, fmaf(s, cy, hd * ay));
+    m.z = fmaf(c, m.z, fmaf(s, cz, hd * az));
+}
+
+template<int ZT, int GZ>
+__global__ void __launch_bounds__(128) pssfp_kernel(PssfpArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int sub = lane % GZ;
+    const int vloc = (blockIdx.x * blockDim.x + threadIdx.x) / GZ;
+    const bool vok = vloc < a.nvoxels;
+    const int64_t vcol = a.voxel_begin + (vok ? vloc : a.nvoxels - 1);
+    const float T1 = a.params[0 * a.param_stride + vcol];
+    const float T2 = a.params[1 * a.param_stride + vcol];
+    const float B1 = a.params[2 * a.param_stride + vcol];
+    const float B0 = a.params[3 * a.param_stride + vcol];
+    const float R1 = 1.0f / T1, R2 = 1.0f / T2;
+    const float E1_ex = expf(-a.dt_ex * R1), E2_ex = expf(-a.dt_ex * R2);
+    const float E1_pr = expf(-a.dt_pr * R1), E2_pr = expf(-a.dt_pr * R2);
+    const float E1_inv = expf(-a.dt_inv * R1), E2_inv = expf(-a.dt_inv * R2);
+    const float twopi = 6.28318530717958647692f;
+
+    Iso m[ZT];
+    float az[ZT], cpr[ZT], spr[ZT];
+    bool valid[ZT];
+    const float cinv = cospif(B1);  // invert(p): z·cos(πB1)   (isochromat.cuh:100-112)
+#pragma unroll
+    for (int k = 0; k < ZT; k++) {
+        const int zi = sub * ZT + k;
+        valid[k] = zi < a.nz;
+        const float z = valid[k] ? a.z[zi] : 0.0f;
+        az[k] = -(a.gz_ex * z) - a.dt_ex * twopi * B0;
+        sincosf(-(a.gz_pr * z) - a.dt_pr * twopi * B0, &spr[k], &cpr[k]);
+        m[k].x = 0.0f;
+        m[k].y = 0.0f;
+        m[k].z = cinv * E1_inv + (1.0f - E1_inv);
+        (void)E2_inv;
+    }
+
+    auto excite = [&](int row) {
+        const float2* zr = a.zap + int64_t(row) * a.nRF;
+        for (int i = 0; i < a.nRF; i++) {
+            const float2 zp = __ldg(zr + i);
+            const float ax = zp.x * B1, ay = -zp.y * B1;
+            const float axy2 = fmaf(ax, ax, ay * ay);
+#pragma unroll
+            for (int k = 0; k < ZT; k++) {
+                rodrigues(m[k], ax, ay, az[k], axy2);
+                m[k].x *= E2_ex;
+                m[k].y *= E2_ex;
+                m[k].z = fmaf(m[k].z, E1_ex, 1.0f - E1_ex);
+            }
+        }
+    };
+    auto precess = [&]() {
+#pragma unroll
+        for (int k = 0; k < ZT; k++) {
+            const float x = m[k].x, y = m[k].y;
+            m[k].x = E2_pr * (cpr[k] * x - spr[k] * y);
+            m[k].y = E2_pr * (cpr[k] * y + spr[k] * x);
+            m[k].z = fmaf(m[k].z, E1_pr, 1.0f - E1_pr);
+        }
+    };
+
+    // α/2 pulse, then re- and prephaser with twice the prephasing gradient (pssfp_kernels.cuh:73-80)
+    excite(0);
+#pragma unroll
+    for (int k = 0; k < ZT; k++) {
+        const int zi = sub * ZT + k;
+        const float z = valid[k] ? a.z[zi] : 0.0f;
+        float s2, c2;
+        sincosf(-(2.0f * a.gz_pr * z) - a.dt_pr * twopi * B0, &s2, &c2);
+        const float x = m[k].x, y = m[k].y;
+        m[k].x = E2_pr * (c2 * x - s2 * y);
+        m[k].y = E2_pr * (c2 * y + s2 * x);
+        m[k].z = fmaf(m[k].z, E1_pr, 1.0f - E1_pr);
+    }
+
+    for (int t = 0; t < a.nTR; t++) {  // pssfp_kernels.cuh:83-107
+        excite(t + 1);
+        precess();
+        float sx = 0.0f, sy = 0.0f;
+#pragma unroll
+        for (int k = 0; k < ZT; k++) {
+            if (valid[k]) {
+                sx += m[k].x;
+                sy += m[k].y;
+            }
+        }
+#pragma unroll
+        for (int d = GZ / 2; d > 0; d /= 2) {
+            sx += __shfl_xor_sync(0xffffffffu, sx, d, GZ);
+            sy += __shfl_xor_sync(0xffffffffu, sy, d, GZ);
+        }
+        if (sub == 0 && vok) a.echo[int64_t(t) * a.echo_stride + a.voxel_begin + vloc] = make_float2(sx, sy);
+        precess();
+    }
+}
+
+}  // namespace kernels
+
+namespace {
+using PssfpKernel = void (*)(kernels::PssfpArgs);
+struct PssfpConfig {
+    int ZT, GZ;
+    PssfpKernel fn;
+};
+const PssfpConfig kPssfpConfigs[] = {
+    {1, 1, kernels::pssfp_kernel<1, 1>},   {2, 1, kernels::pssfp_kernel<2, 1>},
+    {4, 1, kernels::pssfp_kernel<4, 1>},   {8, 1, kernels::pssfp_kernel<8, 1>},
+    {9, 4, kernels::pssfp_kernel<9, 4>},   {5, 8, kernels::pssfp_kernel<5, 8>},
+    {3, 16, kernels::pssfp_kernel<3, 16>}, {2, 32, kernels::pssfp_kernel<2, 32>},
+    {1, 32, kernels::pssfp_kernel<1, 32>}, {18, 2, kernels::pssfp_kernel<18, 2>},
+    {4, 4, kernels::pssfp_kernel<4, 4>},   {8, 4, kernels::pssfp_kernel<8, 4>},
+    {4, 8, kernels::pssfp_kernel<4, 8>},   {12, 4, kernels::pssfp_kernel<12, 4>},
+};
+}  // namespace
+
+int pssfp_config_count() {
+    return int(sizeof(kPssfpConfigs) / sizeof(kPssfpConfigs[0]));
+}
+
+bool pssfp_config_info(int index, int* ZT, int* GZ) {
+    if (index < 0 || index >= pssfp_config_count()) return false;
+    *ZT = kPssfpConfigs[index].ZT;
+    *GZ = kPssfpConfigs[index].GZ;
+    return true;
+}
+
+// Smallest covering layout (ZT·GZ ≥ nz) with at most 12 isochromats per thread; ties go
+// to more lanes when there are few voxels.
+PssfpLaunch pssfp_default_launch(int nz, int64_t nvoxels) {
+    int best = -1;
+    for (int i = 0; i < pssfp_config_count(); i++) {
+        const auto& c = kPssfpConfigs[i];
+        if (c.ZT * c.GZ < nz || c.ZT > 12) continue;
+        if (best < 0) {
+            best = i;
+            continue;
+        }
+        const auto& b = kPssfpConfigs[best];
+        int wc = c.ZT * c.GZ - nz, wb = b.ZT * b.GZ - nz;
+        bool few = nvoxels * c.GZ < 148LL * 256;
+        if (wc < wb || (wc == wb && (few ? c.GZ > b.GZ : c.GZ < b.GZ))) best = i;
+    }
+    if (best < 0) best = 7;  // 2 x 32 lanes covers nz ≤ 64
+    return PssfpLaunch {best};
+}
+
+void launch_pssfp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
+                  const pSSFPSequence& seq, cfloat* echo, int64_t echo_stride, PssfpLaunch L) {
+    const int nTR = int(seq.RF_train.size());
+    const int nRF = int(seq.gamma_dt_RF.size());
+    const int nz = int(seq.z.size());
+    COMPAS_CHECK(nTR > 0);
+    if (nz > 64) COMPAS_ERROR("pSSFP supports at most 64 z positions");
+    if (nvoxels <= 0) return;
+    DeviceGuard guard(ctx.device());
+    if (!seq.zap_table) {
+        auto tab = std::make_shared<Array<cfloat, 2>>(std::array<int64_t, 2> {nTR + 1, nRF}, ctx.device());
+        int n = (nTR + 1) * nRF;
+        if (n > 0) {
+            kernels::pssfp_table_kernel<<<div_ceil(n, 256), 256, 0, ctx.stream()>>>(
+                reinterpret_cast<const float2*>(seq.RF_train.data()), nTR,
+                reinterpret_cast<const float2*>(seq.gamma_dt_RF.data()), nRF, reinterpret_cast<float2*>(tab->data()));
+            check_launch("pssfp_table_kernel");
+        }
+        seq.zap_table = tab;
+    }
+    if (L.config < 0) L = pssfp_default_launch(nz, nvoxels);
+    const auto& cfg = kPssfpConfigs[L.config];
+    if (cfg.ZT * cfg.GZ < nz) COMPAS_ERROR("pSSFP layout does not cover the z positions");
+    kernels::PssfpArgs a;
+    a.params = params.data.data();
+    a.param_stride = params.data.size(1);
+    a.voxel_begin = voxel_begin;
+    a.nvoxels = nvoxels;
+    a.zap = reinterpret_cast<const float2*>(seq.zap_table->data());
+    a.z = seq.z.data();
+    a.nTR = nTR;
+    a.nRF = nRF;
+    a.nz = nz;
+    a.dt_ex = seq.dt.ex;
+    a.dt_inv = seq.dt.inv;
+    a.dt_pr = seq.dt.pr;
+    a.gz_ex = seq.gamma_dt_GRz.ex;
+    a.gz_pr = seq.gamma_dt_GRz.pr;
+    a.echo = reinterpret_cast<float2*>(echo);
+    a.echo_stride = echo_stride;
+    const int threads = 128;
+    const int64_t total = int64_t(nvoxels) * cfg.GZ;
+    cfg.fn<<<unsigned((total + threads - 1) / threads), threads, 0, ctx.stream()>>>(a);
+    check_launch("pssfp_kernel");
+}
+
+Array<cfloat, 2> simulate_magnetization(const CompasContext& context, TissueParameters parameters,
+                                        pSSFPSequence sequence) {
+    const int nTR = int(sequence.RF_train.size());
+    Array<cfloat, 2> echos({nTR, parameters.nvoxels}, context.device());
+    launch_pssfp(context, parameters, 0, parameters.nvoxels, sequence, echos.data(), parameters.nvoxels,
+                 tuned_pssfp_launch(int(sequence.z.size()), parameters.nvoxels));
+    return echos;
+}
+
+}  // namespace compas

@@ -1,0 +1,114 @@
+// tuning.cu — launch-layout selection for the simulation kernels.
+//
+// The FISP and pSSFP kernels are instantiated for several register layouts (states or
+// isochromats per lane × lanes per voxel). The choice is made, in order, from
+//   1. an explicit override (compas_b200_set_*_launch, used by the autotuner while timing),
+//   2. the autotuner's table (COMPAS_B200_TUNING file, one line per shape class:
+//      "fisp <N> <voxel-bucket> <P-bucket> <config> <warps>" or
+//      "pssfp <nz> <voxel-bucket> <config>"), written by compas_b200_autotune.py,
+//   3. the built-in heuristic (fisp_default_launch / pssfp_default_launch).
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <tuple>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace compas {
+
+namespace {
+std::atomic<int> g_fisp_cfg {-1}, g_fisp_warps {-1}, g_pssfp_cfg {-1};
+
+struct Table {
+    std::map<std::tuple<int, int, int>, std::pair<int, int>> fisp;  // (N, vbucket, pbucket) -> (cfg, warps)
+    std::map<std::tuple<int, int>, int> pssfp;                        // (nz, vbucket) -> cfg
+};
+
+int bucket(int64_t n) {  // log2 bucket
+    int b = 0;
+    while (n > 1) {
+        n >>= 1;
+        b++;
+    }
+    return b;
+}
+
+const Table& table() {
+    static Table t;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        const char* path = std::getenv("COMPAS_B200_TUNING");
+        if (!path || !*path) return;
+        std::ifstream in(path);
+        std::string line;
+        while (std::getline(in, line)) {
+            std::istringstream s(line);
+            std::string kind;
+            s >> kind;
+            if (kind == "fisp") {
+                int N, vb, pb, cfg, w;
+                if (s >> N >> vb >> pb >> cfg >> w) t.fisp[{N, vb, pb}] = {cfg, w};
+            } else if (kind == "pssfp") {
+                int nz, vb, cfg;
+                if (s >> nz >> vb >> cfg) t.pssfp[{nz, vb}] = cfg;
+            }
+        }
+    });
+    return t;
+}
+}  // namespace
+
+void set_fisp_override(int config, int warps) {
+    if (config >= fisp_config_count()) COMPAS_ERROR("FISP layout index out of range");
+    g_fisp_cfg = config;
+    g_fisp_warps = warps;
+}
+
+void set_pssfp_override(int config) {
+    if (config >= pssfp_config_count()) COMPAS_ERROR("pSSFP layout index out of range");
+    g_pssfp_cfg = config;
+}
+
+FispLaunch tuned_fisp_launch(int N, int64_t nvoxels, int P) {
+    FispLaunch d = fisp_default_launch(N, nvoxels, P);
+    int cfg = g_fisp_cfg.load();
+    if (cfg >= 0) {
+        int K = 0, G = 0;
+        fisp_config_info(cfg, &K, &G);
+        if (K * G >= N) {
+            int w = g_fisp_warps.load();
+            return FispLaunch {cfg, w > 0 ? w : d.warps};
+        }
+    }
+    const auto& t = table();
+    auto it = t.fisp.find({N, bucket(nvoxels), bucket(P)});
+    if (it != t.fisp.end()) {
+        int K = 0, G = 0;
+        if (fisp_config_info(it->second.first, &K, &G) && K * G >= N) return FispLaunch {it->second.first, it->second.second};
+    }
+    return d;
+}
+
+PssfpLaunch tuned_pssfp_launch(int nz, int64_t nvoxels) {
+    int cfg = g_pssfp_cfg.load();
+    if (cfg >= 0) {
+        int ZT = 0, GZ = 0;
+        pssfp_config_info(cfg, &ZT, &GZ);
+        if (ZT * GZ >= nz) return PssfpLaunch {cfg};
+    }
+    const auto& t = table();
+    auto it = t.pssfp.find({nz, bucket(nvoxels)});
+    if (it != t.pssfp.end()) {
+        int ZT = 0, GZ = 0;
+        if (pssfp_config_info(it->second, &ZT, &GZ) && ZT * GZ >= nz) return PssfpLaunch {it->second};
+    }
+    return pssfp_default_launch(nz, nvoxels);
+}
+
+}  // namespace compas

@@ -1,0 +1,420 @@
+// compas.h — C++ API of the B200 implementation of the compas-toolkit simulation hot path.
+//
+// Source-level drop-in for the reference's C++ API (namespace `compas`, same type and
+// function names and argument meaning; reference headers cited per declaration). The
+// runtime under it is a thin single-GPU one: one CUDA stream per device, stream-ordered
+// allocations from the device's memory pool, kernels written for sm_100a. There is no
+// CPU fallback: every operation runs on the GPU and throws `CompasException` on error.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace compas {
+
+using index_t = int;
+
+// ------------------------------------------------------------------------------------------
+// value types   (compas/core/complex_type.h:24-72, 324-325)
+// ------------------------------------------------------------------------------------------
+template<typename T>
+struct alignas(2 * sizeof(T)) complex_type {
+    T re, im;
+    complex_type(T r = T(0), T i = T(0)) : re(r), im(i) {}
+    T real() const { return re; }
+    T imag() const { return im; }
+};
+using cfloat = complex_type<float>;
+using cdouble = complex_type<double>;
+
+// ------------------------------------------------------------------------------------------
+// errors   (compas/core/assertion.h:35-66: COMPAS_CHECK throws CompasException)
+// ------------------------------------------------------------------------------------------
+class CompasException: public std::runtime_error {
+  public:
+    using std::runtime_error::runtime_error;
+};
+
+[[noreturn]] void throw_exception(const char* file, int line, const std::string& msg);
+
+#define COMPAS_CHECK(cond)                                                              \
+    do {                                                                                \
+        if (!(cond)) ::compas::throw_exception(__FILE__, __LINE__, "check failed: " #cond); \
+    } while (0)
+#define COMPAS_ERROR(msg) ::compas::throw_exception(__FILE__, __LINE__, (msg))
+#define COMPAS_CUDA_CHECK(expr)                                                               \
+    do {                                                                                      \
+        cudaError_t compas_err_ = (expr);                                                     \
+        if (compas_err_ != cudaSuccess)                                                       \
+            ::compas::throw_exception(__FILE__, __LINE__,                                     \
+                                      std::string(#expr ": ") + cudaGetErrorString(compas_err_)); \
+    } while (0)
+
+// ------------------------------------------------------------------------------------------
+// objects and arrays   (compas/core/object.h; kmm::Array used via compas/core/context.h:155-156)
+// ------------------------------------------------------------------------------------------
+class Object {
+  public:
+    virtual ~Object() = default;
+    virtual const char* name() const { return "compas::Object"; }
+};
+
+namespace detail {
+// One device allocation, released stream-ordered on the stream that made it.
+struct Buffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Buffer(size_t bytes, int device, cudaStream_t stream);
+    ~Buffer();
+    Buffer(const Buffer&) = delete;
+    Buffer& operator=(const Buffer&) = delete;
+};
+int current_device();
+cudaStream_t device_stream(int device);
+}  // namespace detail
+
+template<typename T, size_t N = 1>
+struct View {
+    const T* ptr = nullptr;
+    std::array<int64_t, N> dims {};
+    View() = default;
+    View(const T* p, std::array<int64_t, N> d) : ptr(p), dims(d) {}
+    const T* data() const { return ptr; }
+    int64_t size(size_t i) const { return dims[i]; }
+    int64_t size() const {
+        int64_t n = 1;
+        for (auto d : dims) n *= d;
+        return n;
+    }
+    bool is_empty() const { return ptr == nullptr || size() == 0; }
+};
+template<typename T, size_t N = 1>
+using HostView = View<T, N>;
+
+class ArrayBase: public Object {
+  public:
+    virtual int rank() const = 0;
+    virtual int64_t extent(int axis) const = 0;
+    virtual size_t element_size() const = 0;
+    virtual void* raw_data() const = 0;
+    virtual int device() const = 0;
+    int64_t numel() const {
+        int64_t n = 1;
+        for (int i = 0; i < rank(); i++) n *= extent(i);
+        return n;
+    }
+    size_t nbytes() const { return size_t(numel()) * element_size(); }
+    // blocking device-to-host copy of the first `nbytes` bytes
+    void copy_bytes_to(void* dst, size_t nbytes) const;
+};
+
+template<typename T, size_t N = 1>
+class Array: public ArrayBase {
+  public:
+    Array() { m_dims.fill(0); }
+    // allocates (uninitialised) device memory on the current device's stream
+    Array(std::array<int64_t, N> dims) : m_dims(dims) { allocate(detail::current_device()); }
+    Array(std::array<int64_t, N> dims, int device) : m_dims(dims) { allocate(device); }
+
+    const char* name() const override { return "compas::Array"; }
+    int rank() const override { return int(N); }
+    int64_t extent(int axis) const override { return m_dims[size_t(axis)]; }
+    size_t element_size() const override { return sizeof(T); }
+    void* raw_data() const override { return m_buf ? m_buf->ptr : nullptr; }
+    int device() const override { return m_buf ? m_buf->device : 0; }
+
+    T* data() const { return static_cast<T*>(raw_data()); }
+    int64_t size(size_t axis) const { return m_dims[axis]; }
+    std::array<int64_t, N> sizes() const { return m_dims; }
+    int64_t size() const { return numel(); }
+    int64_t chunk_size(size_t axis) const { return m_dims[axis]; }  // one chunk per array
+    bool is_valid() const { return bool(m_buf) || numel() == 0; }
+
+    void copy_to(T* dst) const { copy_bytes_to(dst, nbytes()); }
+    std::vector<T> copy_to_vector() const {
+        std::vector<T> out(static_cast<size_t>(numel()));
+        copy_to(out.data());
+        return out;
+    }
+
+  private:
+    void allocate(int device) {
+        int64_t n = 1;
+        for (auto d : m_dims) {
+            if (d < 0) throw CompasException("negative array dimension");
+            n *= d;
+        }
+        m_buf = std::make_shared<detail::Buffer>(size_t(n) * sizeof(T), device, detail::device_stream(device));
+    }
+    std::array<int64_t, N> m_dims;
+    std::shared_ptr<detail::Buffer> m_buf;
+};
+
+// ------------------------------------------------------------------------------------------
+// context   (compas/core/context.h:158-264)
+// ------------------------------------------------------------------------------------------
+class CompasContext {
+  public:
+    explicit CompasContext(int device = 0);
+    CompasContext with_device(int index) const;
+    int device() const { return m_device; }
+    cudaStream_t stream() const { return m_stream; }
+
+    template<typename T, size_t N>
+    Array<std::decay_t<T>, N> allocate(View<T, N> content) const {
+        Array<std::decay_t<T>, N> out(content.dims, m_device);
+        upload(out.data(), content.data(), size_t(content.size()) * sizeof(T));
+        return out;
+    }
+    template<typename T, typename... Sizes>
+    Array<std::decay_t<T>, sizeof...(Sizes)> allocate(const T* content, Sizes... sizes) const {
+        std::array<int64_t, sizeof...(Sizes)> dims = {int64_t(sizes)...};
+        return allocate(View<T, sizeof...(Sizes)>(content, dims));
+    }
+    template<typename T>
+    Array<std::decay_t<T>> allocate(const std::vector<T>& content) const {
+        return allocate(content.data(), int64_t(content.size()));
+    }
+
+    void synchronize() const;
+    // raises CompasException when a kernel recorded an error in the device status word
+    void check_device_status() const;
+
+  private:
+    void upload(void* dst, const void* src, size_t bytes) const;
+    int m_device;
+    cudaStream_t m_stream;
+};
+
+inline CompasContext make_context(int device = 0) {
+    return CompasContext(device);
+}
+
+// ------------------------------------------------------------------------------------------
+// tissue parameters   (compas/parameters/tissue.h:16-67, tissue_view.cuh:88-101)
+// ------------------------------------------------------------------------------------------
+namespace TissueParameterField {
+enum { T1 = 0, T2 = 1, B1 = 2, B0 = 3, RHO_X = 4, RHO_Y = 5, X = 6, Y = 7, Z = 8, NUM_FIELDS = 9 };
+}
+
+struct TissueParameters: public Object {
+    Array<float, 2> data;  // [NUM_FIELDS][nvoxels]
+    int nvoxels = 0;
+    int chunk_size = 0;
+    bool has_z = true;
+    bool has_b0 = true;
+    bool has_b1 = true;
+
+    TissueParameters() = default;
+    TissueParameters(Array<float, 2> parameters, bool has_z, bool has_b0, bool has_b1) :
+        data(parameters),
+        nvoxels(int(parameters.size(1))),
+        chunk_size(int(parameters.size(1))),
+        has_z(has_z),
+        has_b0(has_b0),
+        has_b1(has_b1) {}
+    const char* name() const override { return "compas::TissueParameters"; }
+};
+
+TissueParameters make_tissue_parameters(
+    const CompasContext& ctx,
+    int num_voxels,
+    int chunk_size,
+    View<float> T1,
+    View<float> T2,
+    View<float> B1,
+    View<float> B0,
+    View<float> rho_x,
+    View<float> rho_y,
+    View<float> x,
+    View<float> y,
+    View<float> z = {});
+
+// ------------------------------------------------------------------------------------------
+// sequences   (compas/sequences/fisp.h:10-60, pssfp.h:9-72, pssfp_view.h:7-11)
+// ------------------------------------------------------------------------------------------
+struct FISPSequence: public Object {
+    Array<cfloat> RF_train;             // [nTR] flip angle (deg) and phase
+    Array<cfloat, 2> sliceprofiles;     // [npositions][nTR]
+    float TR = 0;
+    float TE = 0;
+    float TW = 0;
+    int max_state = 0;
+    float TI = 0;
+    int undersampling_factor = 1;
+    int repetitions = 1;
+    bool inversion_prepulse = true;
+    bool wait_spoiling = true;
+
+    FISPSequence() = default;
+    FISPSequence(Array<cfloat> RF_train, Array<cfloat, 2> sliceprofiles, float TR, float TE, float TW,
+                 int max_state, float TI, int undersampling_factor = 1, int repetitions = 1,
+                 bool inversion_prepulse = true, bool wait_spoiling = true) :
+        RF_train(RF_train), sliceprofiles(sliceprofiles), TR(TR), TE(TE), TW(TW), max_state(max_state), TI(TI),
+        undersampling_factor(undersampling_factor), repetitions(repetitions),
+        inversion_prepulse(inversion_prepulse), wait_spoiling(wait_spoiling) {}
+    const char* name() const override { return "compas::FISPSequence"; }
+
+    // device-resident per-(position, TR) excitation table, built on first use and kept
+    // with the sequence so repeated simulations reuse it
+    mutable std::shared_ptr<Array<float, 3>> excite_table;
+};
+
+inline FISPSequence make_fisp_sequence(const CompasContext& context, View<cfloat> RF_train,
+                                       View<cfloat, 2> sliceprofiles, float TR, float TE, int max_state,
+                                       float TI) {
+    return FISPSequence(context.allocate(RF_train), context.allocate(sliceprofiles), TR, TE, 0.0F, max_state, TI);
+}
+
+struct RepetitionData {
+    float ex;
+    float inv;
+    float pr;
+};
+
+struct pSSFPSequence: public Object {
+    Array<cfloat> RF_train;
+    float TR = 0;
+    int nRF = 0;
+    int nTR = 0;
+    Array<cfloat> gamma_dt_RF;
+    RepetitionData dt {};
+    RepetitionData gamma_dt_GRz {};
+    int nz = 0;
+    Array<float> z;
+
+    pSSFPSequence() = default;
+    pSSFPSequence(Array<cfloat> RF_train, float TR, Array<cfloat> gamma_dt_RF, RepetitionData dt,
+                  RepetitionData gamma_dt_GRz, Array<float> z) :
+        RF_train(RF_train), TR(TR), nRF(int(gamma_dt_RF.size())), nTR(int(RF_train.size())),
+        gamma_dt_RF(gamma_dt_RF), dt(dt), gamma_dt_GRz(gamma_dt_GRz), nz(int(z.size())), z(z) {}
+    const char* name() const override { return "compas::pSSFPSequence"; }
+
+    // device-resident rotation table [nTR+1][nRF] (row 0: the α/2 pulse), built on first use
+    mutable std::shared_ptr<Array<cfloat, 2>> zap_table;
+};
+
+inline pSSFPSequence make_pssfp_sequence(const CompasContext& context, View<cfloat> RF_train, float TR,
+                                         View<cfloat> gamma_dt_RF, RepetitionData dt, RepetitionData gamma_dt_GRz,
+                                         View<float> z) {
+    COMPAS_CHECK(RF_train.size() > 0);
+    return pSSFPSequence(context.allocate(RF_train), TR, context.allocate(gamma_dt_RF), dt, gamma_dt_GRz,
+                         context.allocate(z));
+}
+
+// ------------------------------------------------------------------------------------------
+// trajectories   (compas/trajectories/trajectory.h:10-19, cartesian.h:17-58, spiral.h:14-57)
+// ------------------------------------------------------------------------------------------
+struct Trajectory: public Object {
+    int nreadouts = 0;
+    int samples_per_readout = 0;
+    float delta_t = 0;
+    Trajectory() = default;
+    Trajectory(int nreadouts, int samples_per_readout, float delta_t) :
+        nreadouts(nreadouts), samples_per_readout(samples_per_readout), delta_t(delta_t) {}
+};
+
+struct CartesianTrajectory: public Trajectory {
+    Array<cfloat> k_start;  // [nreadouts]
+    cfloat delta_k;
+    CartesianTrajectory() = default;
+    CartesianTrajectory(int nreadouts, int samples_per_readout, float delta_t, Array<cfloat> k_start,
+                        cfloat delta_k) :
+        Trajectory(nreadouts, samples_per_readout, delta_t), k_start(k_start), delta_k(delta_k) {}
+    const char* name() const override { return "compas::CartesianTrajectory"; }
+};
+
+inline CartesianTrajectory make_cartesian_trajectory(const CompasContext& context, int nreadouts,
+                                                     int samples_per_readout, float delta_t,
+                                                     HostView<cfloat> k_start, cfloat delta_k) {
+    COMPAS_CHECK(k_start.size() == nreadouts);
+    return CartesianTrajectory(nreadouts, samples_per_readout, delta_t, context.allocate(k_start), delta_k);
+}
+
+struct SpiralTrajectory: public Trajectory {
+    Array<cfloat> k_start;  // [nreadouts]
+    Array<cfloat> delta_k;  // [nreadouts]
+    SpiralTrajectory() = default;
+    SpiralTrajectory(int nreadouts, int samples_per_readout, float delta_t, Array<cfloat> k_start,
+                     Array<cfloat> delta_k) :
+        Trajectory(nreadouts, samples_per_readout, delta_t), k_start(k_start), delta_k(delta_k) {}
+    const char* name() const override { return "compas::SpiralTrajectory"; }
+};
+
+inline SpiralTrajectory make_spiral_trajectory(const CompasContext& context, int nreadouts,
+                                               int samples_per_readout, float delta_t, View<cfloat> k_start,
+                                               View<cfloat> delta_k) {
+    COMPAS_CHECK(k_start.size() == nreadouts);
+    COMPAS_CHECK(delta_k.size() == nreadouts);
+    return SpiralTrajectory(nreadouts, samples_per_readout, delta_t, context.allocate(k_start),
+                            context.allocate(delta_k));
+}
+
+// ------------------------------------------------------------------------------------------
+// operations
+// ------------------------------------------------------------------------------------------
+
+// FISP EPG simulation; echos [nTR*undersampling][nvoxels]   (compas/simulate/fisp.h:17-20)
+Array<cfloat, 2> simulate_magnetization(const CompasContext& context, TissueParameters parameters,
+                                        FISPSequence sequence);
+
+// pSSFP isochromat simulation; echos [nTR][nvoxels]   (compas/simulate/pssfp.h:17-20)
+Array<cfloat, 2> simulate_magnetization(const CompasContext& context, TissueParameters parameters,
+                                        pSSFPSequence sequence);
+
+static constexpr float DEFAULT_FINITE_DIFFERENCE_DELTA = 1e-4F;
+
+// forward finite difference (m(p + Δ e_field) - m(p)) / Δ   (compas/simulate/derivative.h:7-47)
+Array<cfloat, 2> simulate_magnetization_derivative(const CompasContext& context, int field, Array<cfloat, 2> echos,
+                                                   TissueParameters parameters, pSSFPSequence sequence,
+                                                   float delta = DEFAULT_FINITE_DIFFERENCE_DELTA);
+Array<cfloat, 2> simulate_magnetization_derivative(const CompasContext& context, int field, Array<cfloat, 2> echos,
+                                                   TissueParameters parameters, FISPSequence sequence,
+                                                   float delta = DEFAULT_FINITE_DIFFERENCE_DELTA);
+
+// echo[r][v] · exp(i y_v Im k_start[r])   (compas/trajectories/phase_encoding.h:19-23)
+Array<cfloat, 2> phase_encoding(const CompasContext& ctx, const Array<cfloat, 2>& echos,
+                                const TissueParameters& parameters, const CartesianTrajectory& trajectory);
+
+// (compas/trajectories/signal.h:14-44). Naive, Direct, MatmulPedantic and Matmul run the plain
+// FP32 SIMT kernels; MatmulFast and MatmulLow run the split-BF16 tcgen05 tensor-core kernels
+// (three BF16 products accumulated in FP32, relative error ≤1e-4 against FP64).
+enum struct SimulateSignalMethod { Naive, Direct, MatmulPedantic, Matmul, MatmulFast, MatmulLow };
+
+// MR signal [ncoils][nreadouts][samples_per_readout]   (compas/trajectories/signal.h:46-63)
+Array<cfloat, 3> magnetization_to_signal(const CompasContext& context, Array<cfloat, 2> echos,
+                                         TissueParameters parameters, const Trajectory& trajectory,
+                                         Array<cfloat, 2> coil_sensitivities,
+                                         SimulateSignalMethod method = SimulateSignalMethod::MatmulFast);
+
+// (compas/jacobian/product.h:10). Naive, Direct and Gemm: plain FP32; GemmFast and GemmLow:
+// split-BF16 tensor cores.
+enum struct JacobianComputeMethod { Naive, Direct, Gemm, GemmFast, GemmLow };
+
+// J·v, v [4][nvoxels] -> [ncoils][nreadouts][ns]   (compas/jacobian/product.h:12-34)
+Array<cfloat, 3> compute_jacobian(const CompasContext& ctx, Array<cfloat, 2> echos, Array<cfloat, 2> delta_echos_T1,
+                                  Array<cfloat, 2> delta_echos_T2, TissueParameters parameters,
+                                  CartesianTrajectory trajectory, Array<cfloat, 2> coil_sensitivities,
+                                  Array<cfloat, 2> vector, JacobianComputeMethod kind = JacobianComputeMethod::Direct);
+
+// Jᴴ·v, v [ncoils][nreadouts][ns] -> [4][nvoxels]   (compas/jacobian/hermitian.h:12-33)
+Array<cfloat, 2> compute_jacobian_hermitian(const CompasContext& ctx, Array<cfloat, 2> echos,
+                                            Array<cfloat, 2> delta_echos_T1, Array<cfloat, 2> delta_echos_T2,
+                                            TissueParameters parameters, CartesianTrajectory trajectory,
+                                            Array<cfloat, 2> coil_sensitivities, Array<cfloat, 3> vector,
+                                            JacobianComputeMethod kind = JacobianComputeMethod::Direct);
+
+// lhs - rhs and Σ|lhs - rhs|²   (compas/utils/residual.h:20-24)
+Array<cfloat, 3> compute_residual(CompasContext ctx, Array<cfloat, 3> lhs, Array<cfloat, 3> rhs,
+                                  float* objective_out = nullptr);
+
+}  // namespace compas

@@ -1,0 +1,174 @@
+/* compas_b200.h — C ABI of the B200 implementation of the compas-toolkit simulation hot path.
+ *
+ * Binary drop-in for the reference's Julia binding library (libcompas-julia.so): the first
+ * block declares the same 26 `extern "C"` symbols with the same parameter lists, in the
+ * order of compas-toolkit julia-bindings/src/bindings.cpp (file:line cited per symbol).
+ * Handles are opaque heap objects owned by the caller and released with
+ * compas_destroy_object / compas_destroy_array / compas_destroy_context.
+ * Complex arrays are interleaved {float re, im}; dimensions are given slowest first
+ * (C row-major), i.e. reversed with respect to Julia.
+ *
+ * Errors: inside a Julia process (symbol `jl_errorf` resolvable) a failing call raises a
+ * Julia error exactly like the reference (julia-bindings/src/common.h:48-62). Elsewhere the
+ * call returns NULL (or leaves outputs untouched) and compas_last_error() describes the
+ * failure; it returns NULL when the last call on this thread succeeded.
+ */
+#ifndef COMPAS_B200_H
+#define COMPAS_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define COMPAS_API __attribute__((visibility("default")))
+#else
+#define COMPAS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct compas_context compas_context; /* compas::CompasContext */
+typedef struct compas_object compas_object;   /* tissue parameters, sequences, trajectories */
+typedef struct compas_array compas_array;     /* compas::Array<T, N> */
+typedef struct {
+    float re, im;
+} compas_cfloat;
+
+/* ---- identical to the reference's C ABI ------------------------------------------------ */
+
+/* bindings.cpp:19-21 */
+COMPAS_API const char* compas_version(void);
+/* bindings.cpp:23-28 */
+COMPAS_API const compas_context* compas_make_context(void);
+/* bindings.cpp:30-36 */
+COMPAS_API const compas_context* compas_copy_context_for_device(compas_context* ctx, int device);
+/* bindings.cpp:38-40 */
+COMPAS_API void compas_destroy_context(const compas_context* ctx);
+/* bindings.cpp:42-44 */
+COMPAS_API void compas_destroy_object(const compas_object* obj);
+/* bindings.cpp:46-48 */
+COMPAS_API void compas_synchronize(const compas_context* ctx);
+/* bindings.cpp:50-67: rank 1..3, sizes slowest first */
+COMPAS_API const compas_array* compas_make_array_float(const compas_context* ctx, const float* data, int rank, int64_t* sizes);
+/* bindings.cpp:69-78: blocking copy of `length` elements */
+COMPAS_API void compas_read_array_float(const compas_context* ctx, const compas_array* array, float* dest, int64_t length);
+/* bindings.cpp:80-96 */
+COMPAS_API const compas_array* compas_make_array_complex(const compas_context* ctx, const compas_cfloat* data, int rank,
+                                              int64_t* sizes);
+/* bindings.cpp:98-107 */
+COMPAS_API void compas_read_array_complex(const compas_context* ctx, const compas_array* array, compas_cfloat* dest,
+                               int64_t length);
+/* bindings.cpp:109-111 */
+COMPAS_API void compas_destroy_array(const compas_array* array);
+/* bindings.cpp:117-149: nine host arrays of nvoxels floats (T1,T2,B1,B0,rho_x,rho_y,x,y,z) */
+COMPAS_API const compas_object* compas_make_tissue_parameters(const compas_context* ctx, int nvoxels, const float* T1,
+                                                   const float* T2, const float* B1, const float* B0,
+                                                   const float* rho_x, const float* rho_y, const float* x,
+                                                   const float* y, const float* z);
+/* bindings.cpp:151-174: RF_train [nTR] complex array, sliceprofiles [npos][nTR] complex array */
+COMPAS_API compas_object* compas_make_fisp_sequence(const compas_array* RF_train, const compas_array* sliceprofiles, float TR,
+                                         float TE, float TW, int max_state, float TI, int undersampling_factor,
+                                         int repetitions);
+/* bindings.cpp:176-196: z is a float array */
+COMPAS_API compas_object* compas_make_pssfp_sequence(const compas_array* RF_train, float TR, const compas_array* gamma_dt_RF,
+                                          float dt_ex, float dt_inv, float dt_pr, float gamma_dt_GRz_ex,
+                                          float gamma_dt_GRz_inv, float gamma_dt_GRz_pr, const compas_array* z);
+/* bindings.cpp:198-212 */
+COMPAS_API compas_object* compas_make_cartesian_trajectory(int nreadouts, int samples_per_readout, float delta_t,
+                                                compas_array* k_start, float delta_k);
+/* bindings.cpp:214-228 */
+COMPAS_API compas_object* compas_make_spiral_trajectory(int nreadouts, int samples_per_readout, float delta_t,
+                                             compas_array* k_start, compas_array* delta_k);
+/* bindings.cpp:230-241: echos [nreadouts][nvoxels] */
+COMPAS_API compas_array* compas_simulate_magnetization_fisp(const compas_context* ctx, const compas_object* parameters,
+                                                 const compas_object* sequence);
+/* bindings.cpp:243-254 */
+COMPAS_API compas_array* compas_simulate_magnetization_pssfp(const compas_context* ctx, const compas_object* parameters,
+                                                  const compas_object* sequence);
+/* bindings.cpp:256-276: signal [ncoils][nreadouts][ns]; low_precision selects MatmulLow instead
+ * of MatmulFast — both run the split-BF16 tensor-core kernels here */
+COMPAS_API compas_array* compas_magnetization_to_signal_cartesian(const compas_context* ctx, int ncoils,
+                                                       const compas_array* echos, const compas_object* parameters,
+                                                       const compas_array* coils, const compas_object* trajectory,
+                                                       int32_t low_precision);
+/* bindings.cpp:278-294 */
+COMPAS_API compas_array* compas_magnetization_to_signal_spiral(const compas_context* ctx, int ncoils, const compas_array* echos,
+                                                    const compas_object* parameters, const compas_array* coils,
+                                                    const compas_object* trajectory);
+/* bindings.cpp:296-322: vector [4][nvoxels] -> [ncoils][nreadouts][ns] */
+COMPAS_API compas_array* compas_compute_jacobian(const compas_context* ctx, int ncoils, const compas_array* echos,
+                                      const compas_array* delta_echos_T1, const compas_array* delta_echos_T2,
+                                      const compas_object* parameters, const compas_array* coils,
+                                      const compas_object* trajectory, const compas_array* vector,
+                                      const int32_t low_precision);
+/* bindings.cpp:324-350: note trajectory before coils; vector [ncoils][nreadouts][ns] -> [4][nvoxels] */
+COMPAS_API compas_array* compas_compute_jacobian_hermitian(const compas_context* ctx, int ncoils, const compas_array* echos,
+                                                const compas_array* delta_echos_T1,
+                                                const compas_array* delta_echos_T2, const compas_object* parameters,
+                                                const compas_object* trajectory, const compas_array* coils,
+                                                const compas_array* vector, const int32_t low_precision);
+/* bindings.cpp:352-365 (no compas_ prefix in the reference) */
+COMPAS_API compas_array* phase_encoding(const compas_context* ctx, const compas_array* echos, const compas_object* parameters,
+                             const compas_object* trajectory);
+/* bindings.cpp:367-374: returns lhs - rhs; *sum = Σ|lhs - rhs|² when sum != NULL */
+COMPAS_API compas_array* compas_compute_residual(const compas_context* ctx, const compas_array* lhs, const compas_array* rhs,
+                                      float* sum);
+/* bindings.cpp:376-393 */
+COMPAS_API compas_array* compas_simulate_magnetization_derivative_pssfp(const compas_context* ctx, int field,
+                                                             const compas_array* echos,
+                                                             const compas_object* parameters, float delta,
+                                                             const compas_object* sequence);
+/* bindings.cpp:395-411 */
+COMPAS_API compas_array* compas_simulate_magnetization_derivative_fisp(const compas_context* ctx, int field,
+                                                            const compas_array* echos, const compas_object* parameters,
+                                                            float delta, const compas_object* sequence);
+
+/* ---- additions (no counterpart in the reference) ----------------------------------------- */
+
+/* Message of the last failed call on this thread, or NULL. Needed outside Julia, where the
+ * reference's jl_errorf path is not available. */
+COMPAS_API const char* compas_last_error(void);
+
+/* Explicit-method variants of the signal and Jacobian entry points: `method` takes the
+ * reference's enum values SimulateSignalMethod {Naive=0, Direct, MatmulPedantic, Matmul,
+ * MatmulFast, MatmulLow} (compas/trajectories/signal.h:14-44) and JacobianComputeMethod
+ * {Naive=0, Direct, Gemm, GemmFast, GemmLow} (compas/jacobian/product.h:10). */
+COMPAS_API compas_array* compas_b200_magnetization_to_signal(const compas_context* ctx, const compas_array* echos,
+                                                  const compas_object* parameters, const compas_object* trajectory,
+                                                  const compas_array* coils, int method);
+COMPAS_API compas_array* compas_b200_compute_jacobian(const compas_context* ctx, const compas_array* echos,
+                                           const compas_array* delta_echos_T1, const compas_array* delta_echos_T2,
+                                           const compas_object* parameters, const compas_object* trajectory,
+                                           const compas_array* coils, const compas_array* vector, int method);
+COMPAS_API compas_array* compas_b200_compute_jacobian_hermitian(const compas_context* ctx, const compas_array* echos,
+                                                     const compas_array* delta_echos_T1,
+                                                     const compas_array* delta_echos_T2,
+                                                     const compas_object* parameters,
+                                                     const compas_object* trajectory, const compas_array* coils,
+                                                     const compas_array* vector, int method);
+
+/* The CUDA stream (cudaStream_t) all work of `ctx` is ordered on, and the device pointer,
+ * rank and extents of an array — for callers that time or chain work on the device. */
+COMPAS_API void* compas_b200_context_stream(const compas_context* ctx);
+COMPAS_API void* compas_b200_array_device_ptr(const compas_array* array);
+COMPAS_API int compas_b200_array_rank(const compas_array* array);
+COMPAS_API int64_t compas_b200_array_extent(const compas_array* array, int axis);
+
+/* Number of kernels this library has launched in this process (all devices). */
+COMPAS_API uint64_t compas_b200_launch_count(void);
+
+/* Launch-layout overrides used by the autotuner: FISP (config index, warps per CTA) and
+ * pSSFP (config index); -1 restores the built-in choice. Number/description of layouts. */
+COMPAS_API void compas_b200_set_fisp_launch(int config, int warps);
+COMPAS_API void compas_b200_set_pssfp_launch(int config);
+COMPAS_API int compas_b200_fisp_config_count(void);
+COMPAS_API int compas_b200_fisp_config_info(int index, int* states_per_lane, int* lanes);
+COMPAS_API int compas_b200_pssfp_config_count(void);
+COMPAS_API int compas_b200_pssfp_config_info(int index, int* iso_per_lane, int* lanes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* COMPAS_B200_H */

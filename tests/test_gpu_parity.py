@@ -1,0 +1,325 @@
+"""GPU parity tests: every operation runs on cuda:0 through the C ABI
+(libcompas_b200.so) and is compared with the CPU oracle on the same seeded inputs.
+
+Tolerances (relative L2 against the FP64 oracle):
+  * simulation (FISP EPG, pSSFP) and every plain-FP32 product:      1e-5
+  * split-BF16 tensor-core products (MatmulFast/Low, GemmFast/Low): 1e-4
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP32 = 1e-5
+TOL_BF16X3 = 1e-4
+PLAIN_SIGNAL = ["Naive", "Direct", "MatmulPedantic", "Matmul"]
+TC_SIGNAL = ["MatmulFast", "MatmulLow"]
+PLAIN_JAC = ["Naive", "Direct", "Gemm"]
+TC_JAC = ["GemmFast", "GemmLow"]
+
+
+@pytest.fixture(scope="module")
+def cb():
+    import compas_b200
+
+    compas_b200.library()
+    return compas_b200
+
+
+@pytest.fixture(scope="module")
+def ctx(cb):
+    return cb.Context(0)
+
+
+def _upload(cb, ctx, w):
+    params = cb.TissueParameters.from_soa(ctx, w["params"])
+    seq = cb.FispSequence.from_dict(ctx, w["seq"]) if "seq" in w else None
+    traj = cb.trajectory_from_dict(ctx, w["traj"])
+    return params, seq, traj
+
+
+# ------------------------------------------------------------------------------------------------
+# FISP EPG
+# ------------------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("max_state", [1, 2, 5, 8, 13, 25])
+def test_fisp_every_layout(cb, ctx, oracle, workloads, max_state):
+    w = workloads.tiny(n_side=7, ntr=41, P=3, max_state=max_state)
+    params, seq, _ = _upload(cb, ctx, w)
+    ref = oracle.fisp(w["params"], w["seq"])
+    tried = 0
+    try:
+        for i, (k, g) in enumerate(cb.fisp_configs()):
+            if k * g < max_state:
+                continue
+            for warps in (1, 2, 3):
+                cb.set_fisp_launch(i, warps)
+                got = cb.simulate_magnetization(ctx, params, seq).to_numpy()
+                assert oracle.rel_l2(got, ref) < TOL_FP32, (k, g, warps)
+                tried += 1
+    finally:
+        cb.set_fisp_launch(-1, -1)
+    assert tried > 0
+
+
+def test_fisp_large_state_counts(cb, ctx, oracle, workloads):
+    for n in (40, 64, 100, 128):
+        w = workloads.tiny(n_side=5, ntr=150, P=2, max_state=n, seed=n)
+        params, seq, _ = _upload(cb, ctx, w)
+        got = cb.simulate_magnetization(ctx, params, seq).to_numpy()
+        assert oracle.rel_l2(got, oracle.fisp(w["params"], w["seq"])) < TOL_FP32, n
+
+
+def test_fisp_repetitions_undersampling(cb, ctx, oracle, workloads):
+    w = workloads.tiny(n_side=6, ntr=29, P=5, max_state=7)
+    w["seq"]["reps"], w["seq"]["uf"], w["seq"]["TW"] = 3, 4, 0.05
+    params, seq, _ = _upload(cb, ctx, w)
+    got = cb.simulate_magnetization(ctx, params, seq).to_numpy()
+    assert got.shape == (29 * 4, 36)
+    assert np.array_equal(got[0::4], got[3::4])
+    assert oracle.rel_l2(got, oracle.fisp(w["params"], w["seq"])) < TOL_FP32
+
+
+def test_fisp_small_config_full(cb, ctx, oracle, workloads):
+    w = workloads.fisp_small()
+    params, seq, _ = _upload(cb, ctx, w)
+    got = cb.simulate_magnetization(ctx, params, seq).to_numpy()
+    ref = oracle.fisp(w["params"], w["seq"])
+    assert oracle.rel_l2(got, ref) < TOL_FP32
+    # FP32 twin of the reference's arithmetic sits in the same band
+    idx = np.arange(0, 4096, 41)
+    twin = oracle.fisp(w["params"], w["seq"], vidx=idx, dtype="f32")
+    assert oracle.rel_l2(got[:, idx], twin) < TOL_FP32
+
+
+def test_fisp_mrstat_scale_sampled(cb, ctx, oracle, workloads):
+    w = workloads.mrstat()
+    params, seq, _ = _upload(cb, ctx, w)
+    got = cb.simulate_magnetization(ctx, params, seq).to_numpy()
+    assert got.shape == (1120, 50176) and np.isfinite(got).all()
+    idx = np.sort(np.random.default_rng(11).choice(50176, 512, replace=False))
+    ref = oracle.fisp(w["params"], w["seq"], vidx=idx)
+    assert oracle.rel_l2(got[:, idx], ref) < TOL_FP32
+
+
+def test_fisp_deterministic(cb, ctx, workloads):
+    w = workloads.tiny(n_side=8, ntr=70, P=6, max_state=9)
+    params, seq, _ = _upload(cb, ctx, w)
+    a = cb.simulate_magnetization(ctx, params, seq).to_numpy()
+    b = cb.simulate_magnetization(ctx, params, seq).to_numpy()
+    assert np.array_equal(a, b)
+
+
+def test_fisp_rejects_bad_state_count(cb, ctx, workloads):
+    w = workloads.tiny()
+    with pytest.raises(cb.CompasError):
+        cb.FispSequence.from_dict(ctx, dict(w["seq"], max_state=129))
+    # context still usable afterwards
+    params, seq, _ = _upload(cb, ctx, w)
+    assert np.isfinite(cb.simulate_magnetization(ctx, params, seq).to_numpy()).all()
+
+
+# ------------------------------------------------------------------------------------------------
+# pSSFP
+# ------------------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("nz", [1, 5, 35])
+def test_pssfp_every_layout(cb, ctx, oracle, workloads, nz):
+    rng = np.random.default_rng(nz)
+    seq = workloads.pssfp_sequence(rng, 23, nrf=7, nz=nz)
+    p = workloads.tissue(rng, 5, 20.0)
+    params = cb.TissueParameters.from_soa(ctx, p)
+    s = cb.pSSFPSequence.from_dict(ctx, seq)
+    ref = oracle.pssfp(p, seq)
+    tried = 0
+    try:
+        for i, (zt, gz) in enumerate(cb.pssfp_configs()):
+            if zt * gz < nz:
+                continue
+            cb.set_pssfp_launch(i)
+            got = cb.simulate_magnetization(ctx, params, s).to_numpy()
+            assert oracle.rel_l2(got, ref) < TOL_FP32, (zt, gz)
+            tried += 1
+    finally:
+        cb.set_pssfp_launch(-1)
+    assert tried > 0
+
+
+def test_pssfp_large_rotations(cb, ctx, oracle, workloads):
+    # flip angles of 120° per TR and strong off-resonance exercise the sincos branch
+    rng = np.random.default_rng(4)
+    seq = workloads.pssfp_sequence(rng, 17, nrf=3, nz=9)
+    seq["rf"] = (seq["rf"] * 3).astype(np.complex64)
+    p = workloads.tissue(rng, 4, 20.0)
+    p[3] *= 20
+    got = cb.simulate_magnetization(ctx, cb.TissueParameters.from_soa(ctx, p), cb.pSSFPSequence.from_dict(ctx, seq))
+    assert oracle.rel_l2(got.to_numpy(), oracle.pssfp(p, seq)) < TOL_FP32
+
+
+# ------------------------------------------------------------------------------------------------
+# signal
+# ------------------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("method", PLAIN_SIGNAL + TC_SIGNAL)
+def test_signal_cartesian_methods(cb, ctx, oracle, workloads, method):
+    w = workloads.tiny(n_side=11, ntr=45, ns=33, nc=3)
+    params, _, traj = _upload(cb, ctx, w)
+    echo = workloads.cn(np.random.default_rng(2), (45, 121))
+    got = cb.magnetization_to_signal(ctx, echo, params, traj, w["coils"], method=method).to_numpy()
+    ref = oracle.signal_cartesian(echo, w["params"], w["traj"], w["coils"])
+    tol = TOL_BF16X3 if method in TC_SIGNAL else TOL_FP32
+    assert oracle.rel_l2(got, ref) < tol
+
+
+@pytest.mark.parametrize("low", [0, 1])
+def test_signal_cartesian_reference_entry_point(cb, ctx, oracle, workloads, low):
+    w = workloads.fisp_small()
+    params, seq, traj = _upload(cb, ctx, w)
+    echos = cb.simulate_magnetization(ctx, params, seq)
+    sig = cb.magnetization_to_signal(ctx, echos, params, traj, w["coils"], low_precision=bool(low)).to_numpy()
+    ref = oracle.signal_cartesian(echos.to_numpy(), w["params"], w["traj"], w["coils"])
+    assert oracle.rel_l2(sig, ref) < TOL_BF16X3
+
+
+@pytest.mark.parametrize("method", ["Direct", "MatmulFast"])
+def test_signal_mrstat_scale_sampled(cb, ctx, oracle, workloads, method):
+    w = workloads.mrstat()
+    params, seq, traj = _upload(cb, ctx, w)
+    rng = np.random.default_rng(5)
+    echo = cb.simulate_magnetization(ctx, params, seq)
+    sig = cb.magnetization_to_signal(ctx, echo, params, traj, w["coils"], method=method).to_numpy()
+    ent = np.stack([rng.integers(0, 4, 192), rng.integers(0, 1120, 192), rng.integers(0, 224, 192)], 1)
+    ref = oracle.signal_cartesian(echo.to_numpy(), w["params"], w["traj"], w["coils"], entries=ent)
+    got = sig[ent[:, 0], ent[:, 1], ent[:, 2]]
+    tol = TOL_BF16X3 if method == "MatmulFast" else TOL_FP32
+    assert oracle.rel_l2(got, ref) < tol
+
+
+def test_signal_spiral(cb, ctx, oracle, workloads):
+    rng = np.random.default_rng(8)
+    p = workloads.tissue(rng, 9, 22.4)
+    traj = workloads.spiral(rng, 13, 300, 22.4, 4e-6)
+    coils = workloads.cn(rng, (3, 81))
+    echo = workloads.cn(rng, (13, 81))
+    params = cb.TissueParameters.from_soa(ctx, p)
+    t = cb.trajectory_from_dict(ctx, traj)
+    got = cb.magnetization_to_signal(ctx, echo, params, t, coils).to_numpy()
+    ref = oracle.signal_spiral(echo, p, traj, coils)
+    assert oracle.rel_l2(got, ref) < TOL_FP32
+
+
+# ------------------------------------------------------------------------------------------------
+# Jacobian products
+# ------------------------------------------------------------------------------------------------
+
+def _jac_case(workloads, rng, n_side=9, nr=37, ns=29, nc=3):
+    p = workloads.tissue(rng, n_side, 22.4)
+    nv = n_side * n_side
+    traj = workloads.cartesian(nr, ns, 22.4, 5e-6, nr)
+    coils = workloads.cn(rng, (nc, nv))
+    e, d1, d2 = (workloads.cn(rng, (nr, nv)) for _ in range(3))
+    return p, traj, coils, e, d1, d2
+
+
+@pytest.mark.parametrize("method", PLAIN_JAC + TC_JAC)
+def test_jacobian(cb, ctx, oracle, workloads, method):
+    rng = np.random.default_rng(21)
+    p, traj, coils, e, d1, d2 = _jac_case(workloads, rng)
+    v = workloads.cn(rng, (4, p.shape[1]))
+    params = cb.TissueParameters.from_soa(ctx, p)
+    t = cb.trajectory_from_dict(ctx, traj)
+    got = cb.compute_jacobian(ctx, e, {"T1": d1, "T2": d2}, params, t, coils, v, method=method).to_numpy()
+    ref = oracle.jacobian(e, d1, d2, p, traj, coils, v)
+    assert oracle.rel_l2(got, ref) < (TOL_BF16X3 if method in TC_JAC else TOL_FP32)
+
+
+@pytest.mark.parametrize("method", PLAIN_JAC + TC_JAC)
+@pytest.mark.parametrize("nc", [1, 5])
+def test_jacobian_hermitian(cb, ctx, oracle, workloads, method, nc):
+    rng = np.random.default_rng(22 + nc)
+    p, traj, coils, e, d1, d2 = _jac_case(workloads, rng, nc=nc)
+    u = workloads.cn(rng, (nc, traj["nr"], traj["ns"]))
+    params = cb.TissueParameters.from_soa(ctx, p)
+    t = cb.trajectory_from_dict(ctx, traj)
+    got = cb.compute_jacobian_hermitian(ctx, e, {"T1": d1, "T2": d2}, params, t, coils, u, method=method).to_numpy()
+    ref = oracle.jacobian_hermitian(e, d1, d2, p, traj, coils, u)
+    assert oracle.rel_l2(got, ref) < (TOL_BF16X3 if method in TC_JAC else TOL_FP32)
+
+
+def test_jacobian_adjointness_on_gpu(cb, ctx, workloads):
+    rng = np.random.default_rng(31)
+    p, traj, coils, e, d1, d2 = _jac_case(workloads, rng, n_side=13, nr=50, ns=40, nc=4)
+    v = workloads.cn(rng, (4, p.shape[1]))
+    u = workloads.cn(rng, (4, 50, 40))
+    params = cb.TissueParameters.from_soa(ctx, p)
+    t = cb.trajectory_from_dict(ctx, traj)
+    for m in ("Direct", "GemmFast"):
+        jv = cb.compute_jacobian(ctx, e, {"T1": d1, "T2": d2}, params, t, coils, v, method=m).to_numpy()
+        jhu = cb.compute_jacobian_hermitian(ctx, e, {"T1": d1, "T2": d2}, params, t, coils, u, method=m).to_numpy()
+        lhs = np.vdot(u.astype(complex), jv.astype(complex))
+        rhs = np.vdot(jhu.astype(complex), v.astype(complex))
+        assert abs(lhs - rhs) / abs(lhs) < (1e-5 if m == "Direct" else 1e-4), m
+
+
+# ------------------------------------------------------------------------------------------------
+# phase encoding, residual, derivatives, edge cases
+# ------------------------------------------------------------------------------------------------
+
+def test_phase_encoding(cb, ctx, oracle, workloads):
+    w = workloads.fisp_small()
+    params, _, traj = _upload(cb, ctx, w)
+    echo = workloads.cn(np.random.default_rng(3), (400, 4096))
+    got = cb.phase_encoding(ctx, echo, params, traj).to_numpy()
+    assert oracle.rel_l2(got, oracle.phase_encoding(echo, w["params"], w["traj"]["k_start"])) < TOL_FP32
+
+
+def test_residual(cb, ctx, oracle):
+    rng = np.random.default_rng(12)
+    a = (rng.standard_normal((3, 70, 33)) + 1j * rng.standard_normal((3, 70, 33))).astype(np.complex64)
+    b = (rng.standard_normal((3, 70, 33)) + 1j * rng.standard_normal((3, 70, 33))).astype(np.complex64)
+    obj, d = cb.compute_residual(ctx, a, b)
+    obj_ref, d_ref = oracle.residual(a, b)
+    assert np.allclose(d.to_numpy(), d_ref, atol=1e-6)
+    assert abs(obj - obj_ref) / obj_ref < 1e-5
+
+
+@pytest.mark.parametrize("kind", ["fisp", "pssfp"])
+def test_derivative(cb, ctx, oracle, workloads, kind):
+    rng = np.random.default_rng(40)
+    if kind == "fisp":
+        w = workloads.tiny(n_side=5, ntr=31, P=2, max_state=6)
+        seqd, sim = w["seq"], oracle.fisp
+        p = w["params"]
+        seq = cb.FispSequence.from_dict(ctx, seqd)
+    else:
+        seqd = workloads.pssfp_sequence(rng, 19, nrf=5, nz=6)
+        p = workloads.tissue(rng, 5, 20.0)
+        seq, sim = cb.pSSFPSequence.from_dict(ctx, seqd), oracle.pssfp
+    params = cb.TissueParameters.from_soa(ctx, p)
+    echos = cb.simulate_magnetization(ctx, params, seq)
+    delta = 1e-3
+    for field in (0, 1):
+        got = cb.simulate_magnetization_derivative(ctx, field, echos, params, seq, delta).to_numpy()
+        q = p.copy()
+        q[field] = (p[field].astype(np.float32) + np.float32(delta)).astype(np.float32)
+        ref = (sim(q, seqd) - sim(p, seqd)) / np.float32(delta)
+        # FP32 forward differences: the GPU and oracle echoes differ by ~1e-7 relative, amplified by 1/Δ
+        assert oracle.rel_l2(got, ref) < 5e-3, field
+
+
+def test_single_voxel_single_readout(cb, ctx, oracle, workloads):
+    w = workloads.tiny(n_side=1, ntr=1, ns=1, nc=1, P=1, max_state=1)
+    params, seq, traj = _upload(cb, ctx, w)
+    e = cb.simulate_magnetization(ctx, params, seq)
+    assert oracle.rel_l2(e.to_numpy(), oracle.fisp(w["params"], w["seq"])) < TOL_FP32
+    for m in ("Direct", "MatmulFast"):
+        s = cb.magnetization_to_signal(ctx, e, params, traj, w["coils"], method=m).to_numpy()
+        ref = oracle.signal_cartesian(e.to_numpy(), w["params"], w["traj"], w["coils"])
+        assert oracle.rel_l2(s, ref) < TOL_BF16X3
+
+
+def test_shape_mismatch_raises(cb, ctx, workloads):
+    w = workloads.tiny()
+    params, _, traj = _upload(cb, ctx, w)
+    with pytest.raises(cb.CompasError):
+        cb.magnetization_to_signal(ctx, np.zeros((3, 3), np.complex64), params, traj, w["coils"])
