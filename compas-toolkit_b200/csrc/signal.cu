@@ -277,6 +277,14 @@ __global__ void __launch_bounds__(SP_THREADS) signal_spiral_kernel(SpiralArgs a)
 
 }  // namespace kernels
 
+void sum_partials(const CompasContext& ctx, const cfloat* partials, int nsplit, int64_t n, cfloat* out) {
+    DeviceGuard guard(ctx.device());
+    const int blocks = int(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)));
+    kernels::sum_partials_kernel<<<blocks, 256, 0, ctx.stream()>>>(reinterpret_cast<const float2*>(partials), nsplit,
+                                                                    n, reinterpret_cast<float2*>(out));
+    check_launch("sum_partials_kernel");
+}
+
 namespace {
 
 template<kernels::GenMode MODE>
@@ -295,12 +303,7 @@ void run_signal_gemm(const CompasContext& ctx, kernels::SignalArgs a, cfloat* ou
     dim3 grid(ktiles, rtiles, a.C * splits);
     kernels::signal_gemm_kernel<MODE><<<grid, kernels::SG_THREADS, 0, ctx.stream()>>>(a);
     check_launch("signal_gemm_kernel");
-    if (splits > 1) {
-        kernels::sum_partials_kernel<<<std::min<int64_t>(div_ceil(int(std::min<int64_t>(n, 1 << 30)), 256), 148 * 8), 256, 0,
-                                       ctx.stream()>>>(reinterpret_cast<const float2*>(partials.data()), splits, n,
-                                                       reinterpret_cast<float2*>(out));
-        check_launch("sum_partials_kernel");
-    }
+    if (splits > 1) sum_partials(ctx, partials.data(), splits, n, out);
 }
 
 }  // namespace
