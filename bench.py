@@ -196,6 +196,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-jacobian", action="store_true", help="skip the J·v / Jᴴ·v measurements")
+    ap.add_argument("--n-side", type=int, default=224,
+                    help="voxel grid side (224 = the MR-STAT workload; smaller values for profiler captures)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -214,7 +217,7 @@ def main():
     import workloads
 
     peaks, peak_kind = load_peaks()
-    w = workloads.mrstat(seed=2 + rank)
+    w = workloads.mrstat(seed=2 + rank, n_side=args.n_side)
     V = w["params"].shape[1]
     nTR = len(w["seq"]["rf"])
     P, N = w["seq"]["slices"].shape[0], w["seq"]["max_state"]
@@ -289,21 +292,24 @@ def main():
     sig_tf = sig_flops / (sig_ms / 1e3) / 1e12
     roofline_signal = {"bound": "tensor", "kernel": "signal (split-BF16 tcgen05)", "achieved": sig_tf,
                        "peak": peaks["bf16_tflops_sustained"], "unit": "TFLOP/s",
-                       "frac": sig_tf / peaks["bf16_tflops_sustained"], "traffic": profile_traffic("signal_mrstat"),
+                       "frac": sig_tf / peaks["bf16_tflops_sustained"], "traffic": profile_traffic("signal_tc_mrstat"),
                        "note": f"algorithmic 8·C·R·S·V flops; split-BF16 issues 3 BF16 MMAs per product, so the "
                                f"attainable algorithmic rate is 1/3 of the BF16 peak ({peak_kind})"}
 
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "fp32 (EPG), bf16x3->fp32 (signal)", "data": "synthetic",
-           "config": {"workload": "mrstat: 224x224=50176 voxels, FISP 1120 TR, 25 EPG states, 35 slice positions, "
-                                  "4 coils, Cartesian 1120x224 readouts; one independent slice per GPU",
+           "config": {"workload": f"mrstat: {args.n_side}x{args.n_side}={V} voxels, FISP 1120 TR, 25 EPG states, "
+                                  f"35 slice positions, 4 coils, Cartesian 1120x{args.n_side} readouts; one "
+                                  "independent slice per GPU",
                       "parallelism": f"voxel-independent, {world} rank(s), no collective",
                       "l2": "working set > L2 (echo array 450 MB per step)", "seed": 2},
            "gpu_launches": launches, "clocks": clocks, "roofline": roofline, "roofline_signal": roofline_signal,
            "stage_ms": {"simulate_fisp": sim_ms, "signal_cartesian": sig_ms},
            "signal_tflops": sig_tf, "peaks": peak_kind}
 
+    if not args.no_jacobian:
+        out["jacobian"] = jacobian_products(cb, ctx, stream, args, peaks, rank)
     if not args.no_e2e:
         out["e2e"] = e2e(cb, ctx, w, args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -314,6 +320,60 @@ def main():
     if rank == 0:
         print(json.dumps(out))
     return 0
+
+
+def jacobian_products(cb, ctx, stream, args, peaks, rank):
+    """J·v and Jᴴ·v on the Jacobian workload (224x224 voxels, 1120x224 Cartesian, 8 coils),
+    split-BF16 tensor cores, plus signal + Jᴴ·v on the plain FP32 path for comparison."""
+    import torch
+    import workloads
+
+    w = workloads.jacobian_inputs(seed=3 + rank, n_side=args.n_side)
+    V = w["params"].shape[1]
+    C_, R, S = w["coils"].shape[0], w["traj"]["nr"], w["traj"]["ns"]
+    params = cb.TissueParameters.from_soa(ctx, w["params"])
+    traj = cb.CartesianTrajectory.from_dict(ctx, w["traj"])
+    arr = {k: cb.CompasArray.from_numpy(ctx, w[k]) for k in ("echo", "dT1", "dT2", "v", "r", "coils")}
+    d = {"T1": arr["dT1"], "T2": arr["dT2"]}
+
+    def timed(fn, reps):
+        fn()
+        ctx.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    reps = max(2, min(args.steps, 5))
+    jv = timed(lambda: cb.compute_jacobian(ctx, arr["echo"], d, params, traj, arr["coils"], arr["v"],
+                                           method="GemmFast"), reps)
+    jhv = timed(lambda: cb.compute_jacobian_hermitian(ctx, arr["echo"], d, params, traj, arr["coils"], arr["r"],
+                                                      method="GemmFast"), reps)
+    sig = timed(lambda: cb.magnetization_to_signal(ctx, arr["echo"], params, traj, arr["coils"],
+                                                   method="MatmulFast"), reps)
+    sig_plain = timed(lambda: cb.magnetization_to_signal(ctx, arr["echo"], params, traj, arr["coils"],
+                                                         method="Direct"), 1)
+    jhv_plain = timed(lambda: cb.compute_jacobian_hermitian(ctx, arr["echo"], d, params, traj, arr["coils"],
+                                                            arr["r"], method="Direct"), 1)
+    f_sig = 8.0 * C_ * R * S * V
+    f_j = 16.0 * C_ * R * S * V
+    f_jh = 16.0 * C_ * R * S * V + 24.0 * C_ * R * V
+    peak = peaks["bf16_tflops_sustained"]
+    tf = lambda f, ms: f / (ms / 1e3) / 1e12
+    return {"workload": f"{args.n_side}x{args.n_side}={V} voxels, Cartesian {R}x{S}, {C_} coils, random echoes / "
+                        "∂echoes, v and residual CN(0,1)",
+            "jv_ms": jv, "jv_tflops": tf(f_j, jv), "jhv_ms": jhv, "jhv_tflops": tf(f_jh, jhv),
+            "signal_ms": sig, "signal_tflops": tf(f_sig, sig),
+            "signal_plus_jhv_tflops": tf(f_sig + f_jh, sig + jhv),
+            "signal_plus_jhv_frac_of_bf16": tf(f_sig + f_jh, sig + jhv) / peak,
+            "plain_fp32_signal_ms": sig_plain, "plain_fp32_jhv_ms": jhv_plain,
+            "tensor_vs_plain_signal_plus_jhv": (sig_plain + jhv_plain) / (sig + jhv),
+            "note": "algorithmic flops 8·C·R·S·V (signal), 16·C·R·S·V (J·v), 16·C·R·S·V + 24·C·R·V (Jᴴ·v); "
+                    "split-BF16 issues 3 MMAs per product; fraction of the sustained BF16 peak (measured)"}
 
 
 def e2e(cb, ctx, w, args, local):

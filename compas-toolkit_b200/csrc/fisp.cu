@@ -369,7 +369,9 @@ FispLaunch fisp_default_launch(int N, int64_t nvoxels, int P) {
 }
 
 const Array<float, 3>& fisp_excite_table(const CompasContext& ctx, const FISPSequence& seq) {
-    if (!seq.excite_table) {
+    auto& cache = *seq.cache;
+    std::lock_guard<std::mutex> lock(cache.mutex);
+    if (!cache.table || cache.key_rf != seq.RF_train.data() || cache.key_sp != seq.sliceprofiles.data()) {
         int nTR = int(seq.RF_train.size());
         int P = int(seq.sliceprofiles.size(0));
         COMPAS_CHECK(int(seq.sliceprofiles.size(1)) == nTR);
@@ -383,9 +385,11 @@ const Array<float, 3>& fisp_excite_table(const CompasContext& ctx, const FISPSeq
                 reinterpret_cast<float4*>(tab->data()));
             check_launch("fisp_table_kernel");
         }
-        seq.excite_table = tab;
+        cache.table = tab;
+        cache.key_rf = seq.RF_train.data();
+        cache.key_sp = seq.sliceprofiles.data();
     }
-    return *seq.excite_table;
+    return *cache.table;
 }
 
 void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,

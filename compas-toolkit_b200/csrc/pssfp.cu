@@ -228,16 +228,25 @@ void launch_pssfp(const CompasContext& ctx, const TissueParameters& params, int 
     if (nz > 64) COMPAS_ERROR("pSSFP supports at most 64 z positions");
     if (nvoxels <= 0) return;
     DeviceGuard guard(ctx.device());
-    if (!seq.zap_table) {
-        auto tab = std::make_shared<Array<cfloat, 2>>(std::array<int64_t, 2> {nTR + 1, nRF}, ctx.device());
-        int n = (nTR + 1) * nRF;
-        if (n > 0) {
-            kernels::pssfp_table_kernel<<<div_ceil(n, 256), 256, 0, ctx.stream()>>>(
-                reinterpret_cast<const float2*>(seq.RF_train.data()), nTR,
-                reinterpret_cast<const float2*>(seq.gamma_dt_RF.data()), nRF, reinterpret_cast<float2*>(tab->data()));
-            check_launch("pssfp_table_kernel");
+    std::shared_ptr<Array<cfloat, 2>> zap;
+    {
+        auto& cache = *seq.cache;
+        std::lock_guard<std::mutex> lock(cache.mutex);
+        if (!cache.table || cache.key_rf != seq.RF_train.data() || cache.key_g != seq.gamma_dt_RF.data()) {
+            auto tab = std::make_shared<Array<cfloat, 2>>(std::array<int64_t, 2> {nTR + 1, nRF}, ctx.device());
+            int n = (nTR + 1) * nRF;
+            if (n > 0) {
+                kernels::pssfp_table_kernel<<<div_ceil(n, 256), 256, 0, ctx.stream()>>>(
+                    reinterpret_cast<const float2*>(seq.RF_train.data()), nTR,
+                    reinterpret_cast<const float2*>(seq.gamma_dt_RF.data()), nRF,
+                    reinterpret_cast<float2*>(tab->data()));
+                check_launch("pssfp_table_kernel");
+            }
+            cache.table = tab;
+            cache.key_rf = seq.RF_train.data();
+            cache.key_g = seq.gamma_dt_RF.data();
         }
-        seq.zap_table = tab;
+        zap = cache.table;
     }
     if (L.config < 0) L = pssfp_default_launch(nz, nvoxels);
     const auto& cfg = kPssfpConfigs[L.config];
@@ -247,7 +256,7 @@ void launch_pssfp(const CompasContext& ctx, const TissueParameters& params, int 
     a.param_stride = params.data.size(1);
     a.voxel_begin = voxel_begin;
     a.nvoxels = nvoxels;
-    a.zap = reinterpret_cast<const float2*>(seq.zap_table->data());
+    a.zap = reinterpret_cast<const float2*>(zap->data());
     a.z = seq.z.data();
     a.nTR = nTR;
     a.nRF = nRF;

@@ -40,7 +40,7 @@ constexpr int TC_STAGES = 2;
 constexpr int TC_A_BYTES = TC_M * TC_K * 2;  // 16 KB per hi/lo plane
 constexpr int TC_B_BYTES = TC_N * TC_K * 2;  // 32 KB per hi/lo plane
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
-constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 128 /*barriers*/;
+constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 128 /*barriers*/ + 2 * 32 * 32 /*voxel constants*/;
 
 struct TcArgs {
     const float* params;
@@ -58,10 +58,20 @@ struct TcArgs {
     unsigned int* status;
 };
 
+// per-stage, per-voxel constants of the generated operand, shared by the B-producer warps
+struct VoxelGen {
+    double theta;  // Θ_v = Δk_re·x + Δk_im·y + 2πΔt·B0 (rad per sample)
+    float2 step;   // e^{-Δt/T2 + iΘ_v}
+    float2 w;      // ρ·e^{i(S/2)Δk_im·y} (signal) or 1 (J·v)
+    float decay;   // -Δt/T2
+    int pad;
+};
+
 template<bool JAC>
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
     constexpr int TERMS = JAC ? 2 : 1;            // complex terms per voxel along K
     constexpr int VPS = TC_K / (2 * TERMS);       // voxels per stage (32 or 16)
+    constexpr int VPC = 4 / TERMS;                // voxels per 16-byte chunk (4 or 2)
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + TC_STAGES * TC_STAGE_BYTES);
@@ -69,6 +79,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
     uint64_t* done = empty + TC_STAGES;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+    VoxelGen* vgen = reinterpret_cast<VoxelGen*>(smem + TC_STAGES * TC_STAGE_BYTES + 128);  // [VPS]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int n_pair0 = blockIdx.x * (TC_N / 2);          // first (c,k) pair of this tile
@@ -95,64 +106,77 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
     const uint32_t tmem = *tmem_slot;
 
     if (warp < 4) {
-        // ---------------- A producer: 128 readouts × VPS voxels → BF16 hi/lo, swizzled
-        const int t = threadIdx.x;          // 0..127
-        const int chunk = t & 7, rsub = t >> 3;  // 8 chunks per row, 16 rows per pass
+        // ---------------- A producer: 128 readouts × VPS voxels → BF16 hi/lo, swizzled.
+        // thread → (16-byte chunk along K, readouts rsub + 16·pass); global loads for a stage
+        // are issued before waiting for its buffer so they overlap the wait.
+        const int t = threadIdx.x;
+        const int chunk = t & 7, rsub = t >> 3;
         for (int it = 0; it < nstages; it++) {
             const int buf = it % TC_STAGES;
-            if (!tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status)) {
-                *abort_flag = 1;
-            }
-            if (*(volatile int*)abort_flag) break;
-            unsigned char* Ah = smem + buf * TC_STAGE_BYTES;
-            unsigned char* Al = Ah + TC_A_BYTES;
-            const int v0 = v_begin + it * VPS;
-#pragma unroll 2
-            for (int pass = 0; pass < TC_M / 16; pass++) {
-                const int rl = rsub + 16 * pass;
-                const int r = r0 + rl;
-                float x[8];
-                if constexpr (!JAC) {
-                    // chunk covers voxels 4·chunk .. 4·chunk+3 (re, im interleaved)
+            const int v0 = v_begin + it * VPS + VPC * chunk;
+            float x[TC_M / 16][8];
+            if constexpr (!JAC) {
+#pragma unroll
+                for (int pass = 0; pass < TC_M / 16; pass++) {
+                    const int r = r0 + rsub + 16 * pass;
 #pragma unroll
                     for (int q = 0; q < 4; q++) {
-                        const int v = v0 + 4 * chunk + q;
+                        const int v = v0 + q;
                         float2 e = make_float2(0.f, 0.f);
                         if (r < a.R && v < v_end) e = __ldg(a.echo + int64_t(r) * a.nvoxels + v);
-                        x[2 * q] = e.x;
-                        x[2 * q + 1] = e.y;
+                        x[pass][2 * q] = e.x;
+                        x[pass][2 * q + 1] = e.y;
                     }
-                } else {
-                    // chunk covers voxels 2·chunk, 2·chunk+1, each (P_re, P_im, Q'_re, Q'_im)
+                }
+            } else {
+                // P = v0 T1ρ ∂T1m + v1 T2ρ ∂T2m + (v2 + i v3) m,  Q' = ΔtR2² v1 T2ρ m
+                float2 c1[2], c2[2], cm[2], cq[2];
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    const int v = v0 + q;
+                    c1[q] = c2[q] = cm[q] = cq[q] = make_float2(0.f, 0.f);
+                    if (v < v_end) {
+                        const float T1 = a.params[v], T2 = a.params[a.pstride + v];
+                        const float2 rho = make_float2(a.params[4 * a.pstride + v], a.params[5 * a.pstride + v]);
+                        const float2 w0 = a.vec[v], w1 = a.vec[a.nvoxels + v];
+                        const float2 w2 = a.vec[2 * int64_t(a.nvoxels) + v], w3 = a.vec[3 * int64_t(a.nvoxels) + v];
+                        c1[q] = cmul(w0, cscale(T1, rho));
+                        c2[q] = cmul(w1, cscale(T2, rho));
+                        cm[q] = make_float2(w2.x - w3.y, w2.y + w3.x);
+                        const float R2 = 1.0f / T2;
+                        cq[q] = cscale(a.dt * R2 * R2, c2[q]);
+                    }
+                }
+#pragma unroll
+                for (int pass = 0; pass < TC_M / 16; pass++) {
+                    const int r = r0 + rsub + 16 * pass;
 #pragma unroll
                     for (int q = 0; q < 2; q++) {
-                        const int v = v0 + 2 * chunk + q;
+                        const int v = v0 + q;
                         float2 P = make_float2(0.f, 0.f), Q = P;
                         if (r < a.R && v < v_end) {
                             const int64_t idx = int64_t(r) * a.nvoxels + v;
-                            const float T1 = a.params[v], T2 = a.params[a.pstride + v];
-                            const float2 rho = make_float2(a.params[4 * a.pstride + v], a.params[5 * a.pstride + v]);
                             const float2 me = __ldg(a.echo + idx), d1 = __ldg(a.dT1 + idx), d2 = __ldg(a.dT2 + idx);
-                            const float2 w0 = a.vec[v], w1 = a.vec[a.nvoxels + v];
-                            const float2 w2 = a.vec[2 * int64_t(a.nvoxels) + v], w3 = a.vec[3 * int64_t(a.nvoxels) + v];
-                            const float2 t1r = cscale(T1, rho), t2r = cscale(T2, rho);
-                            P = cmul(cmul(w0, t1r), d1);
-                            P = cadd(P, cmul(cmul(w1, t2r), d2));
-                            P = cadd(P, cmul(w2, me));
-                            P = cadd(P, cmul(make_float2(-w3.y, w3.x), me));
-                            const float R2 = 1.0f / T2;
-                            Q = cscale(a.dt * R2 * R2, cmul(cmul(w1, t2r), me));
+                            P = cadd(cadd(cmul(c1[q], d1), cmul(c2[q], d2)), cmul(cm[q], me));
+                            Q = cmul(cq[q], me);
                         }
-                        x[4 * q] = P.x;
-                        x[4 * q + 1] = P.y;
-                        x[4 * q + 2] = Q.x;
-                        x[4 * q + 3] = Q.y;
+                        x[pass][4 * q] = P.x;
+                        x[pass][4 * q + 1] = P.y;
+                        x[pass][4 * q + 2] = Q.x;
+                        x[pass][4 * q + 3] = Q.y;
                     }
                 }
+            }
+            if (!tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status)) *abort_flag = 1;
+            if (*(volatile int*)abort_flag) break;
+            unsigned char* Ah = smem + buf * TC_STAGE_BYTES;
+            unsigned char* Al = Ah + TC_A_BYTES;
+#pragma unroll
+            for (int pass = 0; pass < TC_M / 16; pass++) {
                 uint32_t h[4], l[4];
 #pragma unroll
-                for (int q = 0; q < 4; q++) tc::split2(x[2 * q], x[2 * q + 1], h[q], l[q]);
-                const uint32_t off = tc::sw128_offset(rl, chunk);
+                for (int q = 0; q < 4; q++) tc::split2(x[pass][2 * q], x[pass][2 * q + 1], h[q], l[q]);
+                const uint32_t off = tc::sw128_offset(rsub + 16 * pass, chunk);
                 *reinterpret_cast<uint4*>(Ah + off) = make_uint4(h[0], h[1], h[2], h[3]);
                 *reinterpret_cast<uint4*>(Al + off) = make_uint4(l[0], l[1], l[2], l[3]);
             }
@@ -160,80 +184,113 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
             tc::mbar_arrive(&full[buf]);
         }
     } else if (warp < 8) {
-        // ---------------- B producer: 128 pairs × VPS voxels of F = factor·E_k
-        const int t = threadIdx.x - 128;          // 0..127
+        // ---------------- B producer: 128 pairs × VPS voxels of F = coil·w·E_k
+        // thread → (16-byte chunk q = VPC voxels, group of 8 consecutive pairs)
+        const int t = threadIdx.x - 128;
+        const int q = t & 7, pg = t >> 3;
         const double twopi = 6.283185307179586476925;
-        // thread → (voxel slot vs, pair group pg): VPS voxels × (128/VPS) groups of pairs
-        constexpr int GROUPS = 128 / VPS;         // 4 (signal) or 8 (J·v)
-        constexpr int PPG = (TC_N / 2) / GROUPS;  // pairs per group: 32 or 16
-        const int vs = t % VPS, pg = t / VPS;
+        // first pair of this thread's group: (coil, sample) by one division per CTA
+        const int n_first = n_pair0 + pg * 8;
+        const int c_first = n_first / a.S, k_first = n_first - c_first * a.S;
         for (int it = 0; it < nstages; it++) {
             const int buf = it % TC_STAGES;
-            if (!tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status)) {
-                *abort_flag = 1;
+            const int vs0 = it * VPS;
+            // per-voxel constants of this stage, one voxel per thread
+            if (t < VPS) {
+                const int v = v_begin + vs0 + t;
+                VoxelGen g;
+                g.theta = 0.0;
+                g.decay = 0.0f;
+                g.step = make_float2(0.f, 0.f);
+                g.w = make_float2(0.f, 0.f);
+                if (v < v_end) {
+                    const float T2 = a.params[a.pstride + v], B0 = a.params[3 * a.pstride + v];
+                    const float x = a.params[6 * a.pstride + v], y = a.params[7 * a.pstride + v];
+                    g.theta = double(a.dk_re) * x + double(a.dk_im) * y + double(a.dt) * twopi * B0;
+                    g.decay = -a.dt / T2;
+                    const float2 st = cis_rad(g.theta);
+                    const float sm = __expf(g.decay);
+                    g.step = make_float2(sm * st.x, sm * st.y);
+                    g.w = make_float2(1.f, 0.f);
+                    if constexpr (!JAC) {
+                        g.w = make_float2(a.params[4 * a.pstride + v], a.params[5 * a.pstride + v]);
+                        if (a.dk_im != 0.0f) g.w = cmul(g.w, cis_rad(0.5 * double(a.S) * double(a.dk_im) * y));
+                    }
+                }
+                // the previous stage's readers are done: the B warps passed its full-barrier arrive
+                // only after their last read, and this buffer alternates with the stage index
+                vgen[(it & 1) * VPS + t] = g;
             }
-            if (*(volatile int*)abort_flag) break;
+            // B warps only; the OR makes the stop decision identical for all 128 of them
+            if (tc::bar_red_or(1, 128, *(volatile int*)abort_flag)) break;
+            const VoxelGen* vg = vgen + (it & 1) * VPS + VPC * q;
+            double th[VPC];
+            float dec[VPC];
+            float2 stp[VPC], wv[VPC], G[VPC];
+            bool vok[VPC];
+#pragma unroll
+            for (int i = 0; i < VPC; i++) {
+                th[i] = vg[i].theta;
+                dec[i] = vg[i].decay;
+                stp[i] = vg[i].step;
+                wv[i] = vg[i].w;
+                vok[i] = (v_begin + vs0 + VPC * q + i) < v_end;
+            }
+            const bool have_buf = tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status);
+            if (!have_buf) *abort_flag = 1;  // leave at the next collective check, never mid-barrier
             unsigned char* Bh = smem + buf * TC_STAGE_BYTES + 2 * TC_A_BYTES;
             unsigned char* Bl = Bh + TC_B_BYTES;
-            const int v = v_begin + it * VPS + vs;
-            const bool vok = v < v_end;
-            const int vc = vok ? v : 0;
-            const float T2 = a.params[a.pstride + vc], B0 = a.params[3 * a.pstride + vc];
-            const float x = a.params[6 * a.pstride + vc], y = a.params[7 * a.pstride + vc];
-            const double theta = double(a.dk_re) * x + double(a.dk_im) * y + double(a.dt) * twopi * B0;
-            const float decay = -a.dt / T2;
-            float2 wv = make_float2(1.f, 0.f);
-            if constexpr (!JAC) {
-                wv = make_float2(a.params[4 * a.pstride + vc], a.params[5 * a.pstride + vc]);
-                if (a.dk_im != 0.0f) wv = cmul(wv, cis_rad(0.5 * double(a.S) * double(a.dk_im) * y));
-            }
-            const float2 st = cis_rad(theta);
-            const float sm = __expf(decay);
-            const float2 step = make_float2(sm * st.x, sm * st.y);
-            int cur_c = -1;
-            float2 e = make_float2(0.f, 0.f), wc = e;
-            for (int jj = 0; jj < PPG; jj++) {
-                const int j = pg * PPG + jj;       // pair within tile
-                const int n = n_pair0 + j;         // global pair
-                float2 F = make_float2(0.f, 0.f);
-                float ks = 0.0f;
-                if (vok && n < npairs) {
-                    const int c = n / a.S, k = n - c * a.S;
-                    ks = float(k) - 0.5f * float(a.S);
-                    if (c != cur_c || jj % 16 == 0) {  // exact restart (new coil, or every 16 samples)
-                        const float2 ph = cis_rad(double(ks) * theta);
-                        const float mg = __expf(ks * decay);
-                        e = make_float2(mg * ph.x, mg * ph.y);
-                        if (c != cur_c) {
-                            wc = cmul(a.coils[int64_t(c) * a.nvoxels + v], wv);
-                            cur_c = c;
+            int c = c_first, k = k_first;
+            bool restart = true;
+#pragma unroll 2
+            for (int jj = 0; jj < 8 && have_buf; jj++) {
+                const int j = pg * 8 + jj;
+                const bool pok = (n_first + jj) < npairs;
+                const float ks = float(k) - 0.5f * float(a.S);
+                if (restart) {
+#pragma unroll
+                    for (int i = 0; i < VPC; i++) {
+                        G[i] = make_float2(0.f, 0.f);
+                        if (pok && vok[i]) {
+                            const int v = v_begin + vs0 + VPC * q + i;
+                            const float2 ph = cis_rad(double(ks) * th[i]);
+                            const float mg = __expf(ks * dec[i]);
+                            G[i] = cmul(make_float2(mg * ph.x, mg * ph.y), cmul(a.coils[int64_t(c) * a.nvoxels + v], wv[i]));
                         }
-                    } else {
-                        e = cmul(e, step);
                     }
-                    F = cmul(e, wc);
                 }
-                // rows 2j: (F_re, -F_im), 2j+1: (F_im, F_re) at K' = TERMS·2·vs (+2 for the Q' term)
-                uint32_t h0, l0, h1, l1;
-                tc::split2(F.x, -F.y, h0, l0);
-                tc::split2(F.y, F.x, h1, l1);
-                const int kk = TERMS * 2 * vs;                     // bf16 index along K
-                const int chunk = kk >> 3, within = (kk & 7) * 2;  // byte offset inside the chunk
-                const uint32_t o0 = tc::sw128_offset(2 * j, chunk) + within;
-                const uint32_t o1 = tc::sw128_offset(2 * j + 1, chunk) + within;
+                uint32_t h0[4], l0[4], h1[4], l1[4];
                 if constexpr (!JAC) {
-                    *reinterpret_cast<uint32_t*>(Bh + o0) = h0;
-                    *reinterpret_cast<uint32_t*>(Bl + o0) = l0;
-                    *reinterpret_cast<uint32_t*>(Bh + o1) = h1;
-                    *reinterpret_cast<uint32_t*>(Bl + o1) = l1;
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const float2 F = pok ? G[i] : make_float2(0.f, 0.f);
+                        tc::split2(F.x, -F.y, h0[i], l0[i]);
+                        tc::split2(F.y, F.x, h1[i], l1[i]);
+                    }
                 } else {
-                    uint32_t h2, l2, h3, l3;
-                    tc::split2(ks * F.x, -ks * F.y, h2, l2);
-                    tc::split2(ks * F.y, ks * F.x, h3, l3);
-                    *reinterpret_cast<uint2*>(Bh + o0) = make_uint2(h0, h2);
-                    *reinterpret_cast<uint2*>(Bl + o0) = make_uint2(l0, l2);
-                    *reinterpret_cast<uint2*>(Bh + o1) = make_uint2(h1, h3);
-                    *reinterpret_cast<uint2*>(Bl + o1) = make_uint2(l1, l3);
+#pragma unroll
+                    for (int i = 0; i < 2; i++) {
+                        const float2 F = pok ? G[i] : make_float2(0.f, 0.f);
+                        tc::split2(F.x, -F.y, h0[2 * i], l0[2 * i]);
+                        tc::split2(ks * F.x, -ks * F.y, h0[2 * i + 1], l0[2 * i + 1]);
+                        tc::split2(F.y, F.x, h1[2 * i], l1[2 * i]);
+                        tc::split2(ks * F.y, ks * F.x, h1[2 * i + 1], l1[2 * i + 1]);
+                    }
+                }
+                const uint32_t o0 = tc::sw128_offset(2 * j, q), o1 = tc::sw128_offset(2 * j + 1, q);
+                *reinterpret_cast<uint4*>(Bh + o0) = make_uint4(h0[0], h0[1], h0[2], h0[3]);
+                *reinterpret_cast<uint4*>(Bl + o0) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
+                *reinterpret_cast<uint4*>(Bh + o1) = make_uint4(h1[0], h1[1], h1[2], h1[3]);
+                *reinterpret_cast<uint4*>(Bl + o1) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
+                // next pair: same coil → one recurrence step, new coil → exact restart
+                if (++k == a.S) {
+                    k = 0;
+                    ++c;
+                    restart = true;
+                } else {
+                    restart = false;
+#pragma unroll
+                    for (int i = 0; i < VPC; i++) G[i] = cmul(G[i], stp[i]);
                 }
             }
             tc::fence_async_shared();
@@ -245,9 +302,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
             constexpr uint32_t idesc = tc::idesc_bf16_f32(TC_M, TC_N);
             for (int it = 0; it < nstages; it++) {
                 const int buf = it % TC_STAGES;
-                if (!tc::mbar_wait(&full[buf], (it / TC_STAGES) & 1, a.status)) {
-                    *abort_flag = 1;
-                }
+                if (!tc::mbar_wait(&full[buf], (it / TC_STAGES) & 1, a.status)) *abort_flag = 1;
                 if (*(volatile int*)abort_flag) break;
                 tc::tc_fence_after();
                 const uint32_t base = tc::smem_u32(smem + buf * TC_STAGE_BYTES);
@@ -279,24 +334,25 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
             const int r = r0 + warp * 32 + lane;
             float2* outp = a.out + int64_t(split) * npairs * a.R;
 #pragma unroll 1
-            for (int q = 0; q < TC_N / 32; q++) {
+            for (int qq = 0; qq < TC_N / 32; qq++) {
                 float v[32];
-                tc::tmem_load32(tmem + (uint32_t(warp * 32) << 16) + uint32_t(q * 32), v);
+                tc::tmem_load32(tmem + (uint32_t(warp * 32) << 16) + uint32_t(qq * 32), v);
                 if (r < a.R) {
+                    int n = n_pair0 + qq * 16;
+                    int c = n / a.S, k = n - c * a.S;
 #pragma unroll
                     for (int i = 0; i < 16; i++) {
-                        const int n = n_pair0 + q * 16 + i;
-                        if (n < npairs) {
-                            const int c = n / a.S, k = n - c * a.S;
-                            outp[(int64_t(c) * a.R + r) * a.S + k] = make_float2(v[2 * i], v[2 * i + 1]);
+                        if (n + i < npairs) outp[(int64_t(c) * a.R + r) * a.S + k] = make_float2(v[2 * i], v[2 * i + 1]);
+                        if (++k == a.S) {
+                            k = 0;
+                            ++c;
                         }
                     }
                 }
             }
         }
     } else if (warp == 8) {
-        // the MMA lane waited for nothing after its last commit: make sure the MMAs finished
-        // before the TMEM is released (bounded)
+        // make sure the MMAs finished before the TMEM is released (bounded)
         if (lane == 0) tc::mbar_wait(done, 0, a.status);
         __syncwarp();
     }
@@ -319,9 +375,22 @@ bool run_tc(const CompasContext& ctx, kernels::TcArgs a, bool jac, cfloat* out) 
     const int ntiles = div_ceil(npairs, kernels::TC_N / 2), mtiles = div_ceil(a.R, kernels::TC_M);
     const int tiles = ntiles * mtiles;
     const int vps = jac ? 16 : 32;
-    // split the voxel range so that the grid fills ~3 waves of 148 SMs, ≥ 8 stages per split
-    int splits = std::max(1, (148 * 3 + tiles - 1) / tiles);
-    splits = std::min(splits, std::max(1, a.nvoxels / (8 * vps)));
+    // split the voxel range over CTAs: pick the split count (≥ 16 stages per split) whose grid
+    // leaves the least idle SM time in the last wave of one CTA per SM
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device());
+    const int max_splits = std::max(1, std::min(64, a.nvoxels / (16 * vps)));
+    int splits = 1;
+    double best = -1.0;
+    for (int sp = 1; sp <= max_splits; sp++) {
+        const int64_t ctas = int64_t(tiles) * sp;
+        const int64_t waves = (ctas + sms - 1) / sms;
+        const double eff = double(ctas) / double(waves * sms) - 0.002 * sp;  // mild preference for fewer partials
+        if (eff > best + 1e-9) {
+            best = eff;
+            splits = sp;
+        }
+    }
     a.vchunk = div_ceil(div_ceil(a.nvoxels, splits), vps) * vps;
     splits = std::max(1, div_ceil(a.nvoxels, a.vchunk));
     const int64_t n = int64_t(npairs) * a.R;
@@ -387,9 +456,5 @@ bool launch_jacobian_tc(const CompasContext& ctx, const float* params, int64_t p
     return run_tc(ctx, a, true, Jv);
 }
 
-bool launch_jacobian_hermitian_tc(const CompasContext&, const float*, int64_t, int, const cfloat*, const cfloat*,
-                                  const cfloat*, const cfloat*, int, const cfloat*, const CartesianGeom&, cfloat*) {
-    return false;
-}
 
 }  // namespace compas

@@ -13,6 +13,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -264,9 +265,15 @@ struct FISPSequence: public Object {
         inversion_prepulse(inversion_prepulse), wait_spoiling(wait_spoiling) {}
     const char* name() const override { return "compas::FISPSequence"; }
 
-    // device-resident per-(position, TR) excitation table, built on first use and kept
-    // with the sequence so repeated simulations reuse it
-    mutable std::shared_ptr<Array<float, 3>> excite_table;
+    // device-resident per-(position, TR) excitation table, built on first use; copies of the
+    // sequence share it, so repeated simulations reuse it
+    struct Cache {
+        std::mutex mutex;
+        const void* key_rf = nullptr;
+        const void* key_sp = nullptr;
+        std::shared_ptr<Array<float, 3>> table;
+    };
+    std::shared_ptr<Cache> cache = std::make_shared<Cache>();
 };
 
 inline FISPSequence make_fisp_sequence(const CompasContext& context, View<cfloat> RF_train,
@@ -300,7 +307,14 @@ struct pSSFPSequence: public Object {
     const char* name() const override { return "compas::pSSFPSequence"; }
 
     // device-resident rotation table [nTR+1][nRF] (row 0: the α/2 pulse), built on first use
-    mutable std::shared_ptr<Array<cfloat, 2>> zap_table;
+    // and shared by copies of the sequence
+    struct Cache {
+        std::mutex mutex;
+        const void* key_rf = nullptr;
+        const void* key_g = nullptr;
+        std::shared_ptr<Array<cfloat, 2>> table;
+    };
+    std::shared_ptr<Cache> cache = std::make_shared<Cache>();
 };
 
 inline pSSFPSequence make_pssfp_sequence(const CompasContext& context, View<cfloat> RF_train, float TR,
