@@ -13,12 +13,14 @@
 // product is accumulated in FP32 TMEM as hi·hi + hi·lo + lo·hi (three tcgen05.mma per K step);
 // the dropped lo·lo term is ≤ 2⁻¹⁶ relative, giving ~1e-5 relative L2 against FP64.
 //
-// CTA organisation (288 threads, 1 CTA/SM, 192 KB shared memory in 2 pipeline stages):
-//   warps 0-3  convert the A tile (128 readouts × 64 K) from the FP32 echoes into BF16 hi/lo,
-//              128-byte swizzled K-major, and afterwards drain the TMEM accumulator;
-//   warps 4-7  generate the B tile (256 rows × 64 K): E_k by an exact FP64-reduced start and a
-//              complex recurrence along k, times the per-voxel coil (and ρ) factor;
-//   warp 8     allocates 256 TMEM columns and one lane issues the 12 MMAs per stage.
+// CTA organisation (544 threads, 1 CTA/SM, 192 KB shared memory in 2 pipeline stages):
+//   warps 0-7   convert the A tile (128 readouts × 64 K) from the FP32 echoes into BF16 hi/lo,
+//               128-byte swizzled K-major (next stage's loads in flight during the stores);
+//               warps 0-3 afterwards drain the TMEM accumulator;
+//   warps 8-15  generate the B tile (256 rows × 64 K): E_k by an exact FP64-reduced start and a
+//               complex recurrence along k, times the per-voxel coil·w factor;
+//   warp 16     allocates 256 TMEM columns and one lane issues the 12 MMAs per stage.
+// Per-voxel constants (phase step, decay, coil·w, J·v coefficients) come from a small prep kernel.
 // Stages hand over through mbarriers (full: producers → MMA, empty: tcgen05.commit → producers).
 // The voxel range is split over CTAs (split-K); partial tiles are summed in a fixed order.
 #include <cuda_bf16.h>
@@ -35,12 +37,12 @@ void sum_partials(const CompasContext& ctx, const cfloat* partials, int nsplit, 
 namespace kernels {
 
 constexpr int TC_M = 128, TC_N = 256, TC_K = 64;  // real-ified tile; TC_N/2 = 128 complex pairs
-constexpr int TC_THREADS = 288;
+constexpr int TC_THREADS = 544;  // 8 A-producer + 8 B-producer warps + 1 MMA warp
 constexpr int TC_STAGES = 2;
 constexpr int TC_A_BYTES = TC_M * TC_K * 2;  // 16 KB per hi/lo plane
 constexpr int TC_B_BYTES = TC_N * TC_K * 2;  // 32 KB per hi/lo plane
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
-constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 128 /*barriers*/ + 2 * 32 * 32 /*voxel constants*/;
+constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 128 /*barriers*/;
 
 struct TcArgs {
     const float* params;
@@ -56,22 +58,62 @@ struct TcArgs {
     int vchunk;           // voxels per split
     float2* out;          // [splits][C][R][S]
     unsigned int* status;
+    const struct VoxelGen* vgen;  // [V] per-voxel generation constants (prep kernel)
+    const float2* coilw;          // [C][V] coil·w
+    const float4* jcoef;          // J·v only: [V][2] {T1ρv0, T2ρv1}, {v2 + i v3, ΔtR2²·T2ρv1}
 };
 
-// per-stage, per-voxel constants of the generated operand, shared by the B-producer warps
+// per-voxel constants of the generated operand (written by tc_prep_kernel)
 struct VoxelGen {
     double theta;  // Θ_v = Δk_re·x + Δk_im·y + 2πΔt·B0 (rad per sample)
     float2 step;   // e^{-Δt/T2 + iΘ_v}
-    float2 w;      // ρ·e^{i(S/2)Δk_im·y} (signal) or 1 (J·v)
     float decay;   // -Δt/T2
-    int pad;
+    int valid;
 };
+
+// one thread per voxel: generation constants, coil·w for every coil and (J·v) the four complex
+// coefficients of P and Q' — done once per call instead of once per CTA and stage
+template<bool JAC>
+__global__ void tc_prep_kernel(TcArgs a, VoxelGen* vgen, float2* coilw, float4* jcoef) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= a.nvoxels) return;
+    const double twopi = 6.283185307179586476925;
+    const float T1 = a.params[v], T2 = a.params[a.pstride + v], B0 = a.params[3 * a.pstride + v];
+    const float x = a.params[6 * a.pstride + v], y = a.params[7 * a.pstride + v];
+    const float2 rho = make_float2(a.params[4 * a.pstride + v], a.params[5 * a.pstride + v]);
+    VoxelGen g;
+    g.theta = double(a.dk_re) * x + double(a.dk_im) * y + double(a.dt) * twopi * B0;
+    g.decay = -a.dt / T2;
+    const float2 st = cis_rad(g.theta);
+    const float sm = __expf(g.decay);
+    g.step = make_float2(sm * st.x, sm * st.y);
+    g.valid = 1;
+    vgen[v] = g;
+    float2 w = make_float2(1.f, 0.f);
+    if constexpr (!JAC) {
+        w = rho;
+        if (a.dk_im != 0.0f) w = cmul(w, cis_rad(0.5 * double(a.S) * double(a.dk_im) * y));
+    }
+    for (int c = 0; c < a.C; c++) coilw[int64_t(c) * a.nvoxels + v] = cmul(a.coils[int64_t(c) * a.nvoxels + v], w);
+    if constexpr (JAC) {
+        // P = c1·∂T1m + c2·∂T2m + cm·m,  Q' = cq·m   (product_kernels.cuh:56-60, dE/dT2 folded)
+        const float2 w0 = a.vec[v], w1 = a.vec[a.nvoxels + v];
+        const float2 w2 = a.vec[2 * int64_t(a.nvoxels) + v], w3 = a.vec[3 * int64_t(a.nvoxels) + v];
+        const float2 c1 = cmul(w0, cscale(T1, rho)), c2 = cmul(w1, cscale(T2, rho));
+        const float2 cm = make_float2(w2.x - w3.y, w2.y + w3.x);
+        const float R2 = 1.0f / T2;
+        const float2 cq = cscale(a.dt * R2 * R2, c2);
+        jcoef[2 * int64_t(v)] = make_float4(c1.x, c1.y, c2.x, c2.y);
+        jcoef[2 * int64_t(v) + 1] = make_float4(cm.x, cm.y, cq.x, cq.y);
+    }
+}
 
 template<bool JAC>
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
     constexpr int TERMS = JAC ? 2 : 1;            // complex terms per voxel along K
     constexpr int VPS = TC_K / (2 * TERMS);       // voxels per stage (32 or 16)
     constexpr int VPC = 4 / TERMS;                // voxels per 16-byte chunk (4 or 2)
+    constexpr int VPH = VPC / 2;                  // voxels per 8-byte half chunk (2 or 1)
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + TC_STAGES * TC_STAGE_BYTES);
@@ -79,7 +121,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
     uint64_t* done = empty + TC_STAGES;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
-    VoxelGen* vgen = reinterpret_cast<VoxelGen*>(smem + TC_STAGES * TC_STAGE_BYTES + 128);  // [VPS]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int n_pair0 = blockIdx.x * (TC_N / 2);          // first (c,k) pair of this tile
@@ -92,33 +133,32 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_STAGES; s++) {
-            tc::mbar_init(&full[s], 256);
+            tc::mbar_init(&full[s], 512);
             tc::mbar_init(&empty[s], 1);
         }
         tc::mbar_init(done, 1);
         *abort_flag = 0;
         tc::fence_mbarrier_init();
     }
-    if (warp == 8) tc::tmem_alloc(tmem_slot, 256);
+    if (warp == 16) tc::tmem_alloc(tmem_slot, 256);
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp < 4) {
+    if (warp < 8) {
         // ---------------- A producer: 128 readouts × VPS voxels → BF16 hi/lo, swizzled.
-        // thread → (16-byte chunk along K, readouts rsub + 16·pass); global loads for a stage
-        // are issued before waiting for its buffer so they overlap the wait.
+        // thread → (16-byte chunk along K, readouts rsub + 32·pass); the next stage's global
+        // loads are issued before the current stage is converted and stored.
         const int t = threadIdx.x;
         const int chunk = t & 7, rsub = t >> 3;
-        for (int it = 0; it < nstages; it++) {
-            const int buf = it % TC_STAGES;
+        float x[TC_M / 32][8];
+        auto load_stage = [&](int it) {
             const int v0 = v_begin + it * VPS + VPC * chunk;
-            float x[TC_M / 16][8];
             if constexpr (!JAC) {
 #pragma unroll
-                for (int pass = 0; pass < TC_M / 16; pass++) {
-                    const int r = r0 + rsub + 16 * pass;
+                for (int pass = 0; pass < TC_M / 32; pass++) {
+                    const int r = r0 + rsub + 32 * pass;
 #pragma unroll
                     for (int q = 0; q < 4; q++) {
                         const int v = v0 + q;
@@ -129,27 +169,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
                     }
                 }
             } else {
-                // P = v0 T1ρ ∂T1m + v1 T2ρ ∂T2m + (v2 + i v3) m,  Q' = ΔtR2² v1 T2ρ m
-                float2 c1[2], c2[2], cm[2], cq[2];
+                float4 k0[2], k1[2];
 #pragma unroll
                 for (int q = 0; q < 2; q++) {
                     const int v = v0 + q;
-                    c1[q] = c2[q] = cm[q] = cq[q] = make_float2(0.f, 0.f);
+                    k0[q] = k1[q] = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (v < v_end) {
-                        const float T1 = a.params[v], T2 = a.params[a.pstride + v];
-                        const float2 rho = make_float2(a.params[4 * a.pstride + v], a.params[5 * a.pstride + v]);
-                        const float2 w0 = a.vec[v], w1 = a.vec[a.nvoxels + v];
-                        const float2 w2 = a.vec[2 * int64_t(a.nvoxels) + v], w3 = a.vec[3 * int64_t(a.nvoxels) + v];
-                        c1[q] = cmul(w0, cscale(T1, rho));
-                        c2[q] = cmul(w1, cscale(T2, rho));
-                        cm[q] = make_float2(w2.x - w3.y, w2.y + w3.x);
-                        const float R2 = 1.0f / T2;
-                        cq[q] = cscale(a.dt * R2 * R2, c2[q]);
+                        k0[q] = __ldg(a.jcoef + 2 * int64_t(v));
+                        k1[q] = __ldg(a.jcoef + 2 * int64_t(v) + 1);
                     }
                 }
 #pragma unroll
-                for (int pass = 0; pass < TC_M / 16; pass++) {
-                    const int r = r0 + rsub + 16 * pass;
+                for (int pass = 0; pass < TC_M / 32; pass++) {
+                    const int r = r0 + rsub + 32 * pass;
 #pragma unroll
                     for (int q = 0; q < 2; q++) {
                         const int v = v0 + q;
@@ -157,8 +189,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
                         if (r < a.R && v < v_end) {
                             const int64_t idx = int64_t(r) * a.nvoxels + v;
                             const float2 me = __ldg(a.echo + idx), d1 = __ldg(a.dT1 + idx), d2 = __ldg(a.dT2 + idx);
-                            P = cadd(cadd(cmul(c1[q], d1), cmul(c2[q], d2)), cmul(cm[q], me));
-                            Q = cmul(cq[q], me);
+                            P = cadd(cadd(cmul(make_float2(k0[q].x, k0[q].y), d1), cmul(make_float2(k0[q].z, k0[q].w), d2)),
+                                     cmul(make_float2(k1[q].x, k1[q].y), me));
+                            Q = cmul(make_float2(k1[q].z, k1[q].w), me);
                         }
                         x[pass][4 * q] = P.x;
                         x[pass][4 * q + 1] = P.y;
@@ -167,121 +200,100 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
                     }
                 }
             }
+        };
+        load_stage(0);
+        for (int it = 0; it < nstages; it++) {
+            const int buf = it % TC_STAGES;
             if (!tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status)) *abort_flag = 1;
             if (*(volatile int*)abort_flag) break;
             unsigned char* Ah = smem + buf * TC_STAGE_BYTES;
             unsigned char* Al = Ah + TC_A_BYTES;
+            uint32_t h[TC_M / 32][4], l[TC_M / 32][4];
 #pragma unroll
-            for (int pass = 0; pass < TC_M / 16; pass++) {
-                uint32_t h[4], l[4];
+            for (int pass = 0; pass < TC_M / 32; pass++)
 #pragma unroll
-                for (int q = 0; q < 4; q++) tc::split2(x[pass][2 * q], x[pass][2 * q + 1], h[q], l[q]);
-                const uint32_t off = tc::sw128_offset(rsub + 16 * pass, chunk);
-                *reinterpret_cast<uint4*>(Ah + off) = make_uint4(h[0], h[1], h[2], h[3]);
-                *reinterpret_cast<uint4*>(Al + off) = make_uint4(l[0], l[1], l[2], l[3]);
+                for (int q = 0; q < 4; q++) tc::split2(x[pass][2 * q], x[pass][2 * q + 1], h[pass][q], l[pass][q]);
+            if (it + 1 < nstages) load_stage(it + 1);  // in flight while the stores below run
+#pragma unroll
+            for (int pass = 0; pass < TC_M / 32; pass++) {
+                const uint32_t off = tc::sw128_offset(rsub + 32 * pass, chunk);
+                *reinterpret_cast<uint4*>(Ah + off) = make_uint4(h[pass][0], h[pass][1], h[pass][2], h[pass][3]);
+                *reinterpret_cast<uint4*>(Al + off) = make_uint4(l[pass][0], l[pass][1], l[pass][2], l[pass][3]);
             }
             tc::fence_async_shared();
             tc::mbar_arrive(&full[buf]);
         }
-    } else if (warp < 8) {
-        // ---------------- B producer: 128 pairs × VPS voxels of F = coil·w·E_k
-        // thread → (16-byte chunk q = VPC voxels, group of 8 consecutive pairs)
-        const int t = threadIdx.x - 128;
-        const int q = t & 7, pg = t >> 3;
-        const double twopi = 6.283185307179586476925;
-        // first pair of this thread's group: (coil, sample) by one division per CTA
+    } else if (warp < 16) {
+        // ---------------- B producer: 128 pairs × VPS voxels of F = coil·w·E_k.
+        // thread → (8-byte half chunk hq = VPH voxels, group pg of 8 consecutive pairs)
+        const int t = threadIdx.x - 256;
+        const int hq = t & 15, pg = t >> 4;
         const int n_first = n_pair0 + pg * 8;
         const int c_first = n_first / a.S, k_first = n_first - c_first * a.S;
+        VoxelGen vg[VPH], vg_next[VPH];
+        auto load_gen = [&](int it, VoxelGen (&dst)[VPH]) {
+#pragma unroll
+            for (int i = 0; i < VPH; i++) {
+                const int v = v_begin + it * VPS + VPH * hq + i;
+                if (v < v_end) {
+                    dst[i] = a.vgen[v];
+                } else {
+                    dst[i].theta = 0.0;
+                    dst[i].step = make_float2(0.f, 0.f);
+                    dst[i].decay = 0.0f;
+                    dst[i].valid = 0;
+                }
+            }
+        };
+        load_gen(0, vg);
         for (int it = 0; it < nstages; it++) {
             const int buf = it % TC_STAGES;
-            const int vs0 = it * VPS;
-            // per-voxel constants of this stage, one voxel per thread
-            if (t < VPS) {
-                const int v = v_begin + vs0 + t;
-                VoxelGen g;
-                g.theta = 0.0;
-                g.decay = 0.0f;
-                g.step = make_float2(0.f, 0.f);
-                g.w = make_float2(0.f, 0.f);
-                if (v < v_end) {
-                    const float T2 = a.params[a.pstride + v], B0 = a.params[3 * a.pstride + v];
-                    const float x = a.params[6 * a.pstride + v], y = a.params[7 * a.pstride + v];
-                    g.theta = double(a.dk_re) * x + double(a.dk_im) * y + double(a.dt) * twopi * B0;
-                    g.decay = -a.dt / T2;
-                    const float2 st = cis_rad(g.theta);
-                    const float sm = __expf(g.decay);
-                    g.step = make_float2(sm * st.x, sm * st.y);
-                    g.w = make_float2(1.f, 0.f);
-                    if constexpr (!JAC) {
-                        g.w = make_float2(a.params[4 * a.pstride + v], a.params[5 * a.pstride + v]);
-                        if (a.dk_im != 0.0f) g.w = cmul(g.w, cis_rad(0.5 * double(a.S) * double(a.dk_im) * y));
-                    }
-                }
-                // the previous stage's readers are done: the B warps passed its full-barrier arrive
-                // only after their last read, and this buffer alternates with the stage index
-                vgen[(it & 1) * VPS + t] = g;
-            }
-            // B warps only; the OR makes the stop decision identical for all 128 of them
-            if (tc::bar_red_or(1, 128, *(volatile int*)abort_flag)) break;
-            const VoxelGen* vg = vgen + (it & 1) * VPS + VPC * q;
-            double th[VPC];
-            float dec[VPC];
-            float2 stp[VPC], wv[VPC], G[VPC];
-            bool vok[VPC];
-#pragma unroll
-            for (int i = 0; i < VPC; i++) {
-                th[i] = vg[i].theta;
-                dec[i] = vg[i].decay;
-                stp[i] = vg[i].step;
-                wv[i] = vg[i].w;
-                vok[i] = (v_begin + vs0 + VPC * q + i) < v_end;
-            }
-            const bool have_buf = tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status);
-            if (!have_buf) *abort_flag = 1;  // leave at the next collective check, never mid-barrier
+            const int vbase = v_begin + it * VPS + VPH * hq;
+            if (it + 1 < nstages) load_gen(it + 1, vg_next);
+            if (!tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status)) *abort_flag = 1;
+            if (*(volatile int*)abort_flag) break;
             unsigned char* Bh = smem + buf * TC_STAGE_BYTES + 2 * TC_A_BYTES;
             unsigned char* Bl = Bh + TC_B_BYTES;
             int c = c_first, k = k_first;
             bool restart = true;
+            float2 G[VPH];
 #pragma unroll 2
-            for (int jj = 0; jj < 8 && have_buf; jj++) {
+            for (int jj = 0; jj < 8; jj++) {
                 const int j = pg * 8 + jj;
                 const bool pok = (n_first + jj) < npairs;
                 const float ks = float(k) - 0.5f * float(a.S);
                 if (restart) {
 #pragma unroll
-                    for (int i = 0; i < VPC; i++) {
+                    for (int i = 0; i < VPH; i++) {
                         G[i] = make_float2(0.f, 0.f);
-                        if (pok && vok[i]) {
-                            const int v = v_begin + vs0 + VPC * q + i;
-                            const float2 ph = cis_rad(double(ks) * th[i]);
-                            const float mg = __expf(ks * dec[i]);
-                            G[i] = cmul(make_float2(mg * ph.x, mg * ph.y), cmul(a.coils[int64_t(c) * a.nvoxels + v], wv[i]));
+                        if (pok && vg[i].valid) {
+                            const float2 ph = cis_rad(double(ks) * vg[i].theta);
+                            const float mg = __expf(ks * vg[i].decay);
+                            G[i] = cmul(make_float2(mg * ph.x, mg * ph.y), __ldg(a.coilw + int64_t(c) * a.nvoxels + vbase + i));
                         }
                     }
                 }
-                uint32_t h0[4], l0[4], h1[4], l1[4];
+                uint32_t h0[2], l0[2], h1[2], l1[2];
                 if constexpr (!JAC) {
 #pragma unroll
-                    for (int i = 0; i < 4; i++) {
+                    for (int i = 0; i < 2; i++) {
                         const float2 F = pok ? G[i] : make_float2(0.f, 0.f);
                         tc::split2(F.x, -F.y, h0[i], l0[i]);
                         tc::split2(F.y, F.x, h1[i], l1[i]);
                     }
                 } else {
-#pragma unroll
-                    for (int i = 0; i < 2; i++) {
-                        const float2 F = pok ? G[i] : make_float2(0.f, 0.f);
-                        tc::split2(F.x, -F.y, h0[2 * i], l0[2 * i]);
-                        tc::split2(ks * F.x, -ks * F.y, h0[2 * i + 1], l0[2 * i + 1]);
-                        tc::split2(F.y, F.x, h1[2 * i], l1[2 * i]);
-                        tc::split2(ks * F.y, ks * F.x, h1[2 * i + 1], l1[2 * i + 1]);
-                    }
+                    const float2 F = pok ? G[0] : make_float2(0.f, 0.f);
+                    tc::split2(F.x, -F.y, h0[0], l0[0]);
+                    tc::split2(ks * F.x, -ks * F.y, h0[1], l0[1]);
+                    tc::split2(F.y, F.x, h1[0], l1[0]);
+                    tc::split2(ks * F.y, ks * F.x, h1[1], l1[1]);
                 }
-                const uint32_t o0 = tc::sw128_offset(2 * j, q), o1 = tc::sw128_offset(2 * j + 1, q);
-                *reinterpret_cast<uint4*>(Bh + o0) = make_uint4(h0[0], h0[1], h0[2], h0[3]);
-                *reinterpret_cast<uint4*>(Bl + o0) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
-                *reinterpret_cast<uint4*>(Bh + o1) = make_uint4(h1[0], h1[1], h1[2], h1[3]);
-                *reinterpret_cast<uint4*>(Bl + o1) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
+                const uint32_t o0 = tc::sw128_offset(2 * j, hq >> 1) + (hq & 1) * 8;
+                const uint32_t o1 = tc::sw128_offset(2 * j + 1, hq >> 1) + (hq & 1) * 8;
+                *reinterpret_cast<uint2*>(Bh + o0) = make_uint2(h0[0], h0[1]);
+                *reinterpret_cast<uint2*>(Bl + o0) = make_uint2(l0[0], l0[1]);
+                *reinterpret_cast<uint2*>(Bh + o1) = make_uint2(h1[0], h1[1]);
+                *reinterpret_cast<uint2*>(Bl + o1) = make_uint2(l1[0], l1[1]);
                 // next pair: same coil → one recurrence step, new coil → exact restart
                 if (++k == a.S) {
                     k = 0;
@@ -290,14 +302,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
                 } else {
                     restart = false;
 #pragma unroll
-                    for (int i = 0; i < VPC; i++) G[i] = cmul(G[i], stp[i]);
+                    for (int i = 0; i < VPH; i++) G[i] = cmul(G[i], vg[i].step);
                 }
             }
             tc::fence_async_shared();
             tc::mbar_arrive(&full[buf]);
+#pragma unroll
+            for (int i = 0; i < VPH; i++) vg[i] = vg_next[i];
         }
     } else {
-        // ---------------- MMA issuer (warp 8, lane 0)
+        // ---------------- MMA issuer (warp 16, lane 0)
         if (lane == 0) {
             constexpr uint32_t idesc = tc::idesc_bf16_f32(TC_M, TC_N);
             for (int it = 0; it < nstages; it++) {
@@ -351,14 +365,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
                 }
             }
         }
-    } else if (warp == 8) {
+    } else if (warp == 16) {
         // make sure the MMAs finished before the TMEM is released (bounded)
         if (lane == 0) tc::mbar_wait(done, 0, a.status);
         __syncwarp();
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 8) {
+    if (warp == 16) {
         tc::tc_fence_after();
         tc::tmem_dealloc(tmem, 256);
     }
@@ -395,8 +409,24 @@ bool run_tc(const CompasContext& ctx, kernels::TcArgs a, bool jac, cfloat* out) 
     splits = std::max(1, div_ceil(a.nvoxels, a.vchunk));
     const int64_t n = int64_t(npairs) * a.R;
     Array<cfloat, 2> partials({splits > 1 ? splits : 0, n}, ctx.device());
+    // per-voxel tables: 24 B generation constants, C coil·w values, J·v coefficients
+    Array<float, 2> vgen({a.nvoxels, int64_t(sizeof(kernels::VoxelGen) / sizeof(float))}, ctx.device());
+    Array<cfloat, 2> coilw({a.C, a.nvoxels}, ctx.device());
+    Array<float, 2> jcoef({jac ? a.nvoxels : 0, 8}, ctx.device());
+    a.vgen = reinterpret_cast<const kernels::VoxelGen*>(vgen.data());
+    a.coilw = reinterpret_cast<const float2*>(coilw.data());
+    a.jcoef = reinterpret_cast<const float4*>(jcoef.data());
     a.out = reinterpret_cast<float2*>(splits > 1 ? partials.data() : out);
     a.status = detail::device_status_word(ctx.device());
+    if (jac) {
+        kernels::tc_prep_kernel<true><<<div_ceil(a.nvoxels, 128), 128, 0, ctx.stream()>>>(
+            a, reinterpret_cast<kernels::VoxelGen*>(vgen.data()), reinterpret_cast<float2*>(coilw.data()),
+            reinterpret_cast<float4*>(jcoef.data()));
+    } else {
+        kernels::tc_prep_kernel<false><<<div_ceil(a.nvoxels, 128), 128, 0, ctx.stream()>>>(
+            a, reinterpret_cast<kernels::VoxelGen*>(vgen.data()), reinterpret_cast<float2*>(coilw.data()), nullptr);
+    }
+    check_launch("tc_prep_kernel");
     auto fn = jac ? kernels::tc_contract_kernel<true> : kernels::tc_contract_kernel<false>;
     static bool attr_set[2] = {false, false};
     if (!attr_set[jac]) {

@@ -16,8 +16,9 @@
 //   B'[2·64 + p]     = (k-S/2)(u_re, -u_im) → Ỹ_re B'[3·64 + p] = (k-S/2)(u_im, u_re) → Ỹ_im
 // D[128 voxels][256] accumulates in TMEM; two accumulators (512 columns) alternate between
 // consecutive pair tiles so the epilogue of tile t overlaps the MMAs of tile t+1.
-// Warp roles: 0-3 epilogue (TMEM lanes 0-127 = voxels), 4-7 generate A, 8-11 convert u (B),
-// 12 allocates TMEM and issues the MMAs. All waits are bounded.
+// Warp roles: 0-7 epilogue (warps w and w+4 share TMEM lanes 32(w%4).. = voxels and split each
+// tile's pairs), 8-11 generate A, 12-15 convert u (B), 16 allocates TMEM and issues the MMAs.
+// All waits are bounded.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -32,7 +33,7 @@ void sum_partials(const CompasContext& ctx, const cfloat* partials, int nsplit, 
 namespace kernels {
 
 constexpr int TH_M = 128, TH_N = 256, TH_K = 64, TH_PAIRS = 64;
-constexpr int TH_THREADS = 416;  // 4 epilogue + 4 A + 4 B warps + 1 MMA warp
+constexpr int TH_THREADS = 544;  // 8 epilogue + 4 A + 4 B warps + 1 MMA warp
 constexpr int TH_STAGES = 2;
 constexpr int TH_A_BYTES = TH_M * TH_K * 2;
 constexpr int TH_B_BYTES = TH_N * TH_K * 2;
@@ -83,21 +84,21 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
         }
         for (int s = 0; s < 2; s++) {
             tc::mbar_init(&acc_full[s], 1);
-            tc::mbar_init(&acc_empty[s], 128);
+            tc::mbar_init(&acc_empty[s], 256);
         }
         tc::mbar_init(done, 1);
         *abort_flag = 0;
         tc::fence_mbarrier_init();
     }
-    if (warp == 12) tc::tmem_alloc(tmem_slot, 512);
+    if (warp == 16) tc::tmem_alloc(tmem_slot, 512);
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     const double twopi = 6.283185307179586476925;
 
-    if (warp < 8) {
-        // per-voxel constants: warps 0-3 (epilogue) and 4-7 (A producer) own voxel v0 + (tid & 127)
+    if (warp < 12) {
+        // per-voxel constants: warps 0-7 (epilogue) and 8-11 (A producer) own voxel v0 + (tid & 127)
         const int t = threadIdx.x & 127;
         const int v = v0 + t;
         const bool vok = v < a.nvoxels;
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
         const float x = a.params[6 * a.pstride + vc], y = a.params[7 * a.pstride + vc];
         const double theta = double(a.dk_re) * x + double(a.dk_im) * y + double(a.dt) * twopi * B0;
         const float decay = -a.dt / T2;
-        if (warp >= 4) {
+        if (warp >= 8) {
             // ---------------- A producer: 32 samples of conj(E_k(v)) per stage, row t
             const float2 st = cis_rad(theta);
             const float sm = __expf(decay);
@@ -147,10 +148,12 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
                 if (*(volatile int*)abort_flag) break;
             }
         } else {
-            // ---------------- epilogue: thread = voxel = TMEM lane 32·warp + lane
+            // ---------------- epilogue: thread = voxel = TMEM lane 32·(warp%4) + lane; warps w and
+            // w+4 take alternate 8-pair chunks of every tile
             const float2 rho = make_float2(a.params[4 * a.pstride + vc], a.params[5 * a.pstride + vc]);
             const float R2 = 1.0f / T2;
             const float dscale = a.dt * R2 * R2;
+            const int quarter = warp & 3, parity = warp >> 2;
             float2 acc[4];
 #pragma unroll
             for (int f = 0; f < 4; f++) acc[f] = make_float2(0.f, 0.f);
@@ -164,52 +167,72 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
                     ok = false;
                     break;
                 }
-                const uint32_t tbase = tmem + (uint32_t(warp * 32) << 16) + uint32_t(abuf * 256);
+                const uint32_t tbase = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(abuf * 256);
                 const int p0 = (tile_begin + tl) * TH_PAIRS;
 #pragma unroll 1
-                for (int pq = 0; pq < 4; pq++) {  // 16 pairs at a time
-                    float yr[16], yi[16], tr[16], ti[16];
-                    tc::tmem_load16(tbase + 0 * 64 + pq * 16, yr);
-                    tc::tmem_load16(tbase + 1 * 64 + pq * 16, yi);
-                    tc::tmem_load16(tbase + 2 * 64 + pq * 16, tr);
-                    tc::tmem_load16(tbase + 3 * 64 + pq * 16, ti);
-                    int p = p0 + pq * 16;
-                    int r = p / a.C, c = p - r * a.C;
-#pragma unroll 4
-                    for (int i = 0; i < 16; i++) {
-                        if (vok && p + i < npairs) {
-                            const int64_t idx = int64_t(r) * a.nvoxels + v;
-                            const float2 m = __ldg(a.echo + idx), m1 = __ldg(a.dT1 + idx), m2 = __ldg(a.dT2 + idx);
-                            const float2 Y = make_float2(yr[i], yi[i]), Yt = make_float2(tr[i], ti[i]);
-                            const float2 cc = __ldg(a.coils + int64_t(c) * a.nvoxels + v);
-                            const float2 mH = cmulc(Y, m);
-                            const float2 d0 = cmulc(Y, m1);
-                            const float2 dd1 = cadd(cmulc(Y, m2), cscale(dscale, cmulc(Yt, m)));
-                            const float2 rc = cmul(rho, cc);
-                            acc[0] = cadd(acc[0], cmulc(d0, cscale(T1, rc)));
-                            acc[1] = cadd(acc[1], cmulc(dd1, cscale(T2, rc)));
-                            const float2 cm = cmulc(mH, cc);
-                            acc[2] = cadd(acc[2], cm);
-                            acc[3] = cadd(acc[3], make_float2(cm.y, -cm.x));
+                for (int ch = parity; ch < TH_PAIRS / 8; ch += 2) {  // 8 pairs at a time
+                    const int pb = p0 + ch * 8;
+                    // loads first (echo, ∂echo, coil of the 8 pairs), then the TMEM reads and math
+                    float2 m[8], m1[8], m2[8], cc[8];
+                    {
+                        int r = pb / a.C, c = pb - r * a.C;
+#pragma unroll
+                        for (int i = 0; i < 8; i++) {
+                            if (vok && pb + i < npairs) {
+                                const int64_t idx = int64_t(r) * a.nvoxels + v;
+                                m[i] = __ldg(a.echo + idx);
+                                m1[i] = __ldg(a.dT1 + idx);
+                                m2[i] = __ldg(a.dT2 + idx);
+                                cc[i] = __ldg(a.coils + int64_t(c) * a.nvoxels + v);
+                            } else {
+                                m[i] = m1[i] = m2[i] = cc[i] = make_float2(0.f, 0.f);
+                            }
+                            if (++c == a.C) {
+                                c = 0;
+                                ++r;
+                            }
                         }
-                        if (++c == a.C) {
-                            c = 0;
-                            ++r;
-                        }
+                    }
+                    float yr[8], yi[8], tr[8], ti[8];
+                    tc::tmem_load8(tbase + 0 * 64 + ch * 8, yr);
+                    tc::tmem_load8(tbase + 1 * 64 + ch * 8, yi);
+                    tc::tmem_load8(tbase + 2 * 64 + ch * 8, tr);
+                    tc::tmem_load8(tbase + 3 * 64 + ch * 8, ti);
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const float2 Y = make_float2(yr[i], yi[i]), Yt = make_float2(tr[i], ti[i]);
+                        const float2 mH = cmulc(Y, m[i]);
+                        const float2 d0 = cmulc(Y, m1[i]);
+                        const float2 dd1 = cadd(cmulc(Y, m2[i]), cscale(dscale, cmulc(Yt, m[i])));
+                        const float2 rc = cmul(rho, cc[i]);
+                        acc[0] = cadd(acc[0], cmulc(d0, cscale(T1, rc)));
+                        acc[1] = cadd(acc[1], cmulc(dd1, cscale(T2, rc)));
+                        const float2 cm = cmulc(mH, cc[i]);
+                        acc[2] = cadd(acc[2], cm);
+                        acc[3] = cadd(acc[3], make_float2(cm.y, -cm.x));
                     }
                 }
                 tc::tc_fence_before();
                 tc::mbar_arrive(&acc_empty[abuf]);
             }
-            if (ok && vok && !*(volatile int*)abort_flag) {
+            // combine the two warps of each lane quarter through shared memory (stage buffer 0,
+            // free once every tile has been consumed) and write the four results
+            float2* red = reinterpret_cast<float2*>(smem);
+            asm volatile("bar.sync 2, 256;" ::: "memory");  // epilogue warps only: all MMAs consumed
+            if (parity == 1) {
+#pragma unroll
+                for (int f = 0; f < 4; f++) red[f * 128 + t] = acc[f];
+            }
+            asm volatile("bar.sync 2, 256;" ::: "memory");
+            if (parity == 0 && ok && vok && !*(volatile int*)abort_flag) {
                 float2* o = a.out + int64_t(split) * 4 * a.nvoxels;
 #pragma unroll
-                for (int f = 0; f < 4; f++) o[int64_t(f) * a.nvoxels + v] = acc[f];
+                for (int f = 0; f < 4; f++) o[int64_t(f) * a.nvoxels + v] = cadd(acc[f], red[f * 128 + t]);
             }
         }
-    } else if (warp < 12) {
+    } else if (warp < 16) {
         // ---------------- B producer: u → rows (u_re,-u_im), (u_im,u_re) and their (k-S/2)-scaled copies
-        const int t = threadIdx.x - 256;
+        const int t = threadIdx.x - 384;
         const int pl = t & 63, half = t >> 6;  // pair within tile, 16-sample half of the stage
         int g = 0;
         for (int tl = 0; tl < ntiles; tl++) {
@@ -298,7 +321,7 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 12) {
+    if (warp == 16) {
         tc::tc_fence_after();
         tc::tmem_dealloc(tmem, 512);
     }
