@@ -134,6 +134,8 @@ compas::JacobianComputeMethod jacobian_method(int m) {
 }  // namespace
 
 namespace compas {
+void residual_noalloc(int device, const cfloat* lhs, const cfloat* rhs, cfloat* diff, float* objective, int64_t n,
+                      cudaStream_t stream);
 unsigned long long launch_count();
 void set_fisp_override(int config, int warps);
 void set_pssfp_override(int config);
@@ -449,6 +451,17 @@ void compas_b200_set_fisp_launch(int config, int warps) {
 
 void compas_b200_set_pssfp_launch(int config) {
     guarded([&] { compas::set_pssfp_override(config); });
+}
+
+int compas_b200_compute_residual_noalloc(int device, const compas_cfloat* lhs, const compas_cfloat* rhs,
+                                         compas_cfloat* diff, float* objective, int64_t n, void* stream) {
+    int rc = -1;
+    guarded([&] {
+        compas::residual_noalloc(device, reinterpret_cast<const cfloat*>(lhs), reinterpret_cast<const cfloat*>(rhs),
+                                 reinterpret_cast<cfloat*>(diff), objective, n, reinterpret_cast<cudaStream_t>(stream));
+        rc = 0;
+    });
+    return rc;
 }
 
 uint64_t compas_b200_launch_count(void) {

@@ -155,6 +155,18 @@ COMPAS_API void* compas_b200_array_device_ptr(const compas_array* array);
 COMPAS_API int compas_b200_array_rank(const compas_array* array);
 COMPAS_API int64_t compas_b200_array_extent(const compas_array* array, int axis);
 
+/* Residual without any device allocation (no counterpart in the reference): diff = lhs - rhs
+ * over n complex values and *objective = Σ|lhs - rhs|², where lhs, rhs, diff and objective are
+ * device pointers on `device` supplied by the caller and the work is ordered on `stream`
+ * (a cudaStream_t; NULL is the legacy default stream). For callers that cannot let a library
+ * allocate device memory (a fixed, caller-owned memory budget, or a loop that must not trigger
+ * allocations). Its scratch is a fixed 256 KB device array inside the library, shared by all calls
+ * on a device: n is limited to 16,777,216 (larger n returns an error), and calls whose work
+ * overlaps on the GPU race on the scratch. The first call on a device resolves the scratch's
+ * address; make it before any stream capture. Returns 0, or -1 with compas_last_error() set. */
+COMPAS_API int compas_b200_compute_residual_noalloc(int device, const compas_cfloat* lhs, const compas_cfloat* rhs,
+                                                    compas_cfloat* diff, float* objective, int64_t n, void* stream);
+
 /* Number of kernels this library has launched in this process (all devices). */
 COMPAS_API uint64_t compas_b200_launch_count(void);
 

@@ -1,0 +1,69 @@
+"""The allocation-free residual entry point (compas_b200_compute_residual_noalloc).
+
+It serves callers that cannot let the library allocate device memory — e.g. an application that
+owns a fixed device-memory budget and passes the library pre-allocated buffers. The test hands it
+caller-owned device buffers, calls it through the C ABI twice in a row with different inputs
+(its scratch is shared between calls), and checks each result against the allocating entry point
+compas_compute_residual on the same inputs: the difference array exactly, the objective within the
+FP32 tolerance of the other GPU tests. It also checks that sizes beyond the stated limit are
+rejected with an error instead of running.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP32 = 1e-5
+
+
+@pytest.fixture(scope="module")
+def lib_and_ctx():
+    import compas_b200 as cb
+
+    lib = cb.library()
+    fn = lib.compas_b200_compute_residual_noalloc
+    fn.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+    fn.restype = C.c_int
+    return cb, fn, cb.Context(0)
+
+
+def _complex(rng, shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+
+def test_noalloc_residual_matches_allocating_entry_point_twice(lib_and_ctx):
+    import torch
+
+    cb, fn, ctx = lib_and_ctx
+    stream = torch.cuda.current_stream(0)
+    for call, shape in enumerate([(3, 257, 129), (2, 1120, 224)]):
+        rng = np.random.default_rng(100 + call)
+        a, b = _complex(rng, shape), _complex(rng, shape)
+        obj_ref, diff_ref = cb.compute_residual(ctx, a, b)
+        diff_ref = diff_ref.to_numpy()
+
+        # caller-owned device buffers (the entry point itself allocates nothing)
+        da = torch.from_numpy(a.view(np.float32).reshape(-1)).to("cuda:0")
+        db = torch.from_numpy(b.view(np.float32).reshape(-1)).to("cuda:0")
+        ddiff = torch.full_like(da, float("nan"))
+        dobj = torch.full((1,), float("nan"), device="cuda:0")
+        rc = fn(0, da.data_ptr(), db.data_ptr(), ddiff.data_ptr(), dobj.data_ptr(), a.size, stream.cuda_stream)
+        assert rc == 0, cb.library().compas_last_error()
+        stream.synchronize()
+        diff = ddiff.cpu().numpy().view(np.complex64).reshape(shape)
+        assert np.array_equal(diff, diff_ref)
+        obj = float(dobj.item())
+        assert abs(obj - obj_ref) <= TOL_FP32 * obj_ref, (call, obj, obj_ref)
+
+
+def test_noalloc_residual_rejects_sizes_beyond_its_scratch(lib_and_ctx):
+    import torch
+
+    cb, fn, _ = lib_and_ctx
+    d = torch.zeros(4, device="cuda:0")
+    limit = 1 << 24
+    rc = fn(0, d.data_ptr(), d.data_ptr(), d.data_ptr(), d.data_ptr(), limit + 1, None)
+    assert rc == -1
+    assert b"exceeds the limit" in cb.library().compas_last_error()
