@@ -335,36 +335,35 @@ bool fisp_config_info(int index, int* K, int* G) {
     return true;
 }
 
-// Default layout choice for `N` states: the smallest single-lane layout that covers N for
-// N ≤ 25 when there are enough (voxel, position) pairs to fill the GPU, otherwise a
-// lane-split layout. The autotuner (tuning.cpp) may override it per shape class.
+// Default layout choice for `N` states (from layout timings on B200):
+//  * many (voxel, position) pairs: all states of a voxel in one lane (G = 1, K ≥ N) — no shuffles;
+//    25 states × 35 positions at 25600 voxels: 38.6 ms vs 51 ms for the best split layout;
+//  * few pairs (e.g. 4096 voxels × 1 position): split the states over 4 lanes to get 4× more warps
+//    (8 states: K2·G4 0.155 ms vs 0.205 ms for K8·G1);
+//  * N > 25: the smallest covering split layout.
+// The autotuner (tuning.cu) may override it per shape class.
 FispLaunch fisp_default_launch(int N, int64_t nvoxels, int P) {
-    FispLaunch L {-1, 1};
     const int64_t pairs = nvoxels * P;
     const bool wide = pairs >= 148LL * 32 * 8;
     int best = -1;
+    auto waste = [&](int i) { return kFispConfigs[i].K * kFispConfigs[i].G - N; };
     for (int i = 0; i < fisp_config_count(); i++) {
         const auto& c = kFispConfigs[i];
         if (c.K * c.G < N) continue;
-        if (wide && c.G != 1) continue;
-        if (!wide && N > 1 && c.G == 1 && nvoxels < 148 * 64) continue;
-        if (best < 0) {
-            best = i;
-            continue;
-        }
-        const auto& b = kFispConfigs[best];
-        int waste_c = c.K * c.G - N, waste_b = b.K * b.G - N;
-        if (waste_c < waste_b || (waste_c == waste_b && c.G < b.G)) best = i;
+        bool preferred;
+        if (N <= 25 && wide) preferred = (c.G == 1);
+        else if (N <= 32 && !wide) preferred = (c.G == 4);
+        else preferred = true;
+        if (!preferred) continue;
+        if (best < 0 || waste(i) < waste(best) || (waste(i) == waste(best) && c.G < kFispConfigs[best].G)) best = i;
     }
-    if (best < 0) {  // nothing matched the width preference: any covering layout
+    if (best < 0) {  // nothing matched the preference: the covering layout with the least waste
         for (int i = 0; i < fisp_config_count(); i++)
-            if (kFispConfigs[i].K * kFispConfigs[i].G >= N && (best < 0 || kFispConfigs[i].G > kFispConfigs[best].G))
-                best = i;
+            if (kFispConfigs[i].K * kFispConfigs[i].G >= N && (best < 0 || waste(i) < waste(best))) best = i;
     }
-    L.config = best;
-    L.warps = P >= 5 ? (P % 7 == 0 ? 7 : 5) : P;
-    if (L.warps < 1) L.warps = 1;
-    if (L.warps > 8) L.warps = 8;
+    FispLaunch L {best, 1};
+    L.warps = P >= 5 ? (P % 7 == 0 || P > 35 ? 7 : 5) : P;
+    L.warps = std::max(1, std::min(L.warps, 8));
     return L;
 }
 
