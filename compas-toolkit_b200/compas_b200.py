@@ -77,6 +77,10 @@ _SIGS = {
     "compas_b200_fisp_config_info": ([_I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
     "compas_b200_pssfp_config_count": ([], _I),
     "compas_b200_pssfp_config_info": ([_I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
+    "compas_b200_make_batch": ([_P, _I, _P, _P, _P, _P, _I], _P),
+    "compas_b200_batch_run": ([_P], _I),
+    "compas_b200_batch_echos": ([_P, _I], _P),
+    "compas_b200_batch_signal": ([_P, _I], _P),
 }
 
 _LIB = None
@@ -412,6 +416,60 @@ def compute_residual(context: Context, lhs, rhs):
     ptr = library().compas_compute_residual(context.ptr, a.ptr, b.ptr, obj.ctypes.data)
     diff = _result(ptr, context, a.shape, "compute_residual")
     return float(obj[0]), diff
+
+
+def job_from_dict(context: Context, job: dict) -> tuple:
+    """(parameters, sequence, trajectory, coils) of a job dict as made by workloads.batch_jobs."""
+    params = TissueParameters.from_soa(context, job["params"])
+    seq = (FispSequence if job["kind"] == "fisp" else pSSFPSequence).from_dict(context, job["seq"])
+    traj = trajectory_from_dict(context, job["traj"]) if job.get("traj") is not None else None
+    coils = job.get("coils") if traj is not None else None
+    return params, seq, traj, coils
+
+
+class SimulationBatch(_Object):
+    """compas_b200_make_batch: independent simulate -> signal jobs planned into a few launches
+    (persistent work-queue simulation kernels, batched signal kernels).
+
+    jobs: sequence of (parameters, sequence, trajectory or None, coils or None). Each job's
+    echoes and signal equal those of simulate_magnetization + magnetization_to_signal(method)."""
+
+    def __init__(self, context: Context, jobs, method: str = "MatmulFast"):
+        lib = library()
+        n = len(jobs)
+        arr_t = C.c_void_p * max(n, 1)
+        coil_arrays = [None if j[3] is None else _arr(context, j[3], np.complex64) for j in jobs]
+        params = arr_t(*[j[0].ptr for j in jobs])
+        seqs = arr_t(*[j[1].ptr for j in jobs])
+        trajs = arr_t(*[None if j[2] is None else j[2].ptr for j in jobs])
+        coils = arr_t(*[None if c is None else c.ptr for c in coil_arrays])
+        ptr = lib.compas_b200_make_batch(context.ptr, n, C.cast(params, _P), C.cast(seqs, _P), C.cast(trajs, _P),
+                                         C.cast(coils, _P), SIGNAL_METHODS[method])
+        super().__init__(ptr, (list(jobs), coil_arrays))
+        self.context = context
+        self.jobs = list(jobs)
+        self.coil_arrays = coil_arrays
+
+    def __len__(self):
+        return len(self.jobs)
+
+    def run(self):
+        """Enqueue every job on the context's stream (returns without waiting)."""
+        if library().compas_b200_batch_run(self.ptr) != 0:
+            _check(None, "compas_b200_batch_run!")
+
+    def echos(self, job: int) -> CompasArray:
+        params, seq = self.jobs[job][0], self.jobs[job][1]
+        ptr = library().compas_b200_batch_echos(self.ptr, int(job))
+        return _result(ptr, self.context, (seq.nreadouts, params.nvoxels), "compas_b200_batch_echos")
+
+    def signal(self, job: int) -> CompasArray:
+        traj, coils = self.jobs[job][2], self.coil_arrays[job]
+        if traj is None:
+            raise CompasError("job has no trajectory")
+        ptr = library().compas_b200_batch_signal(self.ptr, int(job))
+        shape = (coils.shape[0], traj.nreadouts, traj.samples_per_readout)
+        return _result(ptr, self.context, shape, "compas_b200_batch_signal")
 
 
 def launch_count() -> int:

@@ -484,4 +484,51 @@ int compas_b200_pssfp_config_info(int index, int* iso_per_lane, int* lanes) {
     return compas::pssfp_config_info(index, iso_per_lane, lanes) ? 1 : 0;
 }
 
+compas_object* compas_b200_make_batch(const compas_context* context, int njobs, const compas_object* const* parameters,
+                                      const compas_object* const* sequences, const compas_object* const* trajectories,
+                                      const compas_array* const* coils, int method) {
+    return guarded([&] {
+        const auto& ctx = ctx_of(context);
+        if (njobs < 0) throw compas::CompasException("negative job count");
+        if (njobs > 0 && (!parameters || !sequences)) throw compas::CompasException("null job arrays");
+        std::vector<compas::SimulationJob> jobs;
+        jobs.reserve(size_t(njobs));
+        for (int i = 0; i < njobs; i++) {
+            compas::SimulationJob job;
+            job.parameters = unwrap<compas::TissueParameters>(parameters[i]);
+            if (!sequences[i]) throw compas::CompasException("null sequence");
+            const auto* seq = handle<compas::Object>(sequences[i]);
+            if (const auto* f = dynamic_cast<const compas::FISPSequence*>(seq)) job.sequence = *f;
+            else if (const auto* p = dynamic_cast<const compas::pSSFPSequence*>(seq)) job.sequence = *p;
+            else throw compas::CompasException(std::string("invalid sequence object: ") + seq->name());
+            const void* traj = trajectories ? trajectories[i] : nullptr;
+            if (traj) {
+                const auto* t = handle<compas::Object>(traj);
+                if (const auto* c = dynamic_cast<const compas::CartesianTrajectory*>(t)) job.trajectory = *c;
+                else if (const auto* sp = dynamic_cast<const compas::SpiralTrajectory*>(t)) job.trajectory = *sp;
+                else throw compas::CompasException(std::string("invalid trajectory object: ") + t->name());
+                if (!coils) throw compas::CompasException("null coils array");
+                job.coil_sensitivities = array_of<cfloat, 2>(coils[i], "coils");
+            }
+            jobs.push_back(std::move(job));
+        }
+        return new_obj(compas::SimulationBatch(ctx, std::move(jobs), signal_method(method)));
+    });
+}
+
+int compas_b200_batch_run(const compas_object* batch) {
+    t_has_error = false;
+    guarded([&] { unwrap<compas::SimulationBatch>(batch).run(); });
+    return t_has_error ? -1 : 0;
+}
+
+compas_array* compas_b200_batch_echos(const compas_object* batch, int job) {
+    return guarded([&] { return new_array(compas::Array<cfloat, 2>(unwrap<compas::SimulationBatch>(batch).echos(job))); });
+}
+
+compas_array* compas_b200_batch_signal(const compas_object* batch, int job) {
+    // a job without trajectory yields an empty [0][0][0] array
+    return guarded([&] { return new_array(compas::Array<cfloat, 3>(unwrap<compas::SimulationBatch>(batch).signal(job))); });
+}
+
 }  // extern "C"

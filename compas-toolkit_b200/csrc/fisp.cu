@@ -22,6 +22,7 @@
 
 #include "common.cuh"
 #include "compas/compas.h"
+#include "job_args.cuh"
 #include "kernels.h"
 
 namespace compas {
@@ -45,17 +46,6 @@ __global__ void fisp_table_kernel(const float2* __restrict__ rf, const float2* _
     table[i] = make_float4(float(0.5 * (M_PI / 180.0) * a), float(cp), float(sp), 0.0f);
 }
 
-struct FispArgs {
-    const float* params;   // [9][param_stride]
-    int64_t param_stride;
-    int voxel_begin;       // first voxel of this launch
-    int nvoxels;           // voxels in this launch
-    const float4* table;   // [P][nTR]
-    int nTR, P, N, uf, reps, inversion, wait_spoil;
-    float TR, TE, TW, TI;
-    float2* echo;          // [nTR*uf][echo_stride], column = voxel_begin + local voxel
-    int64_t echo_stride;
-};
 
 // Excitation coefficients of one TR, already multiplied by the preceding relaxation
 // D = diag(c, c̄, E1) (see file header). Halved where the P/Q update needs it.
@@ -198,14 +188,16 @@ struct EPG {
     }
 };
 
+// One voxel tile (VB = 32/G voxels, all slice positions) of a FISP simulation; the CTA's W
+// warps sweep the positions. Shared by the one-simulation kernel (tile = blockIdx.x) and the
+// batched work-queue kernel (tile taken from the queue), so both give bit-identical echoes.
 template<int K, int G>
-__global__ void __launch_bounds__(256, 1) fisp_epg_kernel(FispArgs a) {
+__device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, float2* samples) {
     constexpr int VB = 32 / G;
-    extern __shared__ float2 samples[];  // [W][32][VB]
     const int W = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grp = lane / G, sub = lane % G;
-    const int vloc = blockIdx.x * VB + grp;
+    const int vloc = tile * VB + grp;
     const bool vok = vloc < a.nvoxels;
     const int64_t vcol = a.voxel_begin + (vok ? vloc : a.nvoxels - 1);
 
@@ -268,7 +260,7 @@ __global__ void __launch_bounds__(256, 1) fisp_epg_kernel(FispArgs a) {
                     // undersampling-expanded rows (fisp_kernels.cuh:246-259)
                     for (int e = threadIdx.x; e < nt * VB; e += blockDim.x) {
                         const int j = e / VB, gv = e % VB;
-                        const int v = blockIdx.x * VB + gv;
+                        const int v = tile * VB + gv;
                         float2 acc = make_float2(0.f, 0.f);
                         for (int w = 0; w < W; w++) acc = cadd(acc, samples[(w * 32 + j) * VB + gv]);
                         if (v < a.nvoxels) {
@@ -293,6 +285,35 @@ __global__ void __launch_bounds__(256, 1) fisp_epg_kernel(FispArgs a) {
     }
 }
 
+template<int K, int G>
+__global__ void __launch_bounds__(256, 1) fisp_epg_kernel(FispArgs a) {
+    extern __shared__ float2 samples[];  // [W][32][VB]
+    fisp_tile<K, G>(a, blockIdx.x, samples);
+}
+
+// Persistent work-queue kernel for a batch of FISP simulations sharing one (K, G, W) layout:
+// each CTA takes (job, tile) items from `items` in order through an atomic counter until the
+// queue is empty. Items are ordered longest job first, so the last wave is short.
+template<int K, int G>
+__global__ void __launch_bounds__(256, 1) fisp_queue_kernel(const FispArgs* __restrict__ jobs,
+                                                            const int2* __restrict__ items, int nitems,
+                                                            int* __restrict__ head) {
+    extern __shared__ float2 samples[];
+    __shared__ FispArgs job;
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(head, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= nitems) break;
+        const int2 w = items[it];
+        if (threadIdx.x == 0) job = jobs[w.x];
+        __syncthreads();
+        fisp_tile<K, G>(job, w.y, samples);
+        __syncthreads();  // job and s_item are rewritten by the next item
+    }
+}
+
 }  // namespace kernels
 
 // ------------------------------------------------------------------------------------------
@@ -302,24 +323,35 @@ __global__ void __launch_bounds__(256, 1) fisp_epg_kernel(FispArgs a) {
 namespace {
 
 using FispKernel = void (*)(kernels::FispArgs);
+using FispQueueKernel = void (*)(const kernels::FispArgs*, const int2*, int, int*);
 
 struct FispConfig {
     int K, G;
     FispKernel fn;
+    FispQueueKernel queue;
 };
 
 // Instantiated layouts: (states per lane K, lanes per voxel/position G). Coverage K·G ≥ N.
 const FispConfig kFispConfigs[] = {
-    {1, 1, kernels::fisp_epg_kernel<1, 1>},     {2, 1, kernels::fisp_epg_kernel<2, 1>},
-    {4, 1, kernels::fisp_epg_kernel<4, 1>},     {6, 1, kernels::fisp_epg_kernel<6, 1>},
-    {8, 1, kernels::fisp_epg_kernel<8, 1>},     {12, 1, kernels::fisp_epg_kernel<12, 1>},
-    {16, 1, kernels::fisp_epg_kernel<16, 1>},   {20, 1, kernels::fisp_epg_kernel<20, 1>},
-    {25, 1, kernels::fisp_epg_kernel<25, 1>},   {2, 4, kernels::fisp_epg_kernel<2, 4>},
-    {4, 2, kernels::fisp_epg_kernel<4, 2>},     {4, 4, kernels::fisp_epg_kernel<4, 4>},
-    {4, 8, kernels::fisp_epg_kernel<4, 8>},     {7, 4, kernels::fisp_epg_kernel<7, 4>},
-    {13, 2, kernels::fisp_epg_kernel<13, 2>},   {8, 4, kernels::fisp_epg_kernel<8, 4>},
-    {8, 8, kernels::fisp_epg_kernel<8, 8>},     {8, 16, kernels::fisp_epg_kernel<8, 16>},
-    {4, 32, kernels::fisp_epg_kernel<4, 32>},
+    {1, 1, kernels::fisp_epg_kernel<1, 1>, kernels::fisp_queue_kernel<1, 1>},
+    {2, 1, kernels::fisp_epg_kernel<2, 1>, kernels::fisp_queue_kernel<2, 1>},
+    {4, 1, kernels::fisp_epg_kernel<4, 1>, kernels::fisp_queue_kernel<4, 1>},
+    {6, 1, kernels::fisp_epg_kernel<6, 1>, kernels::fisp_queue_kernel<6, 1>},
+    {8, 1, kernels::fisp_epg_kernel<8, 1>, kernels::fisp_queue_kernel<8, 1>},
+    {12, 1, kernels::fisp_epg_kernel<12, 1>, kernels::fisp_queue_kernel<12, 1>},
+    {16, 1, kernels::fisp_epg_kernel<16, 1>, kernels::fisp_queue_kernel<16, 1>},
+    {20, 1, kernels::fisp_epg_kernel<20, 1>, kernels::fisp_queue_kernel<20, 1>},
+    {25, 1, kernels::fisp_epg_kernel<25, 1>, kernels::fisp_queue_kernel<25, 1>},
+    {2, 4, kernels::fisp_epg_kernel<2, 4>, kernels::fisp_queue_kernel<2, 4>},
+    {4, 2, kernels::fisp_epg_kernel<4, 2>, kernels::fisp_queue_kernel<4, 2>},
+    {4, 4, kernels::fisp_epg_kernel<4, 4>, kernels::fisp_queue_kernel<4, 4>},
+    {4, 8, kernels::fisp_epg_kernel<4, 8>, kernels::fisp_queue_kernel<4, 8>},
+    {7, 4, kernels::fisp_epg_kernel<7, 4>, kernels::fisp_queue_kernel<7, 4>},
+    {13, 2, kernels::fisp_epg_kernel<13, 2>, kernels::fisp_queue_kernel<13, 2>},
+    {8, 4, kernels::fisp_epg_kernel<8, 4>, kernels::fisp_queue_kernel<8, 4>},
+    {8, 8, kernels::fisp_epg_kernel<8, 8>, kernels::fisp_queue_kernel<8, 8>},
+    {8, 16, kernels::fisp_epg_kernel<8, 16>, kernels::fisp_queue_kernel<8, 16>},
+    {4, 32, kernels::fisp_epg_kernel<4, 32>, kernels::fisp_queue_kernel<4, 32>},
 };
 
 }  // namespace
@@ -391,19 +423,14 @@ const Array<float, 3>& fisp_excite_table(const CompasContext& ctx, const FISPSeq
     return *cache.table;
 }
 
-void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
-                 const FISPSequence& seq, cfloat* echo, int64_t echo_stride, FispLaunch L) {
+kernels::FispArgs fisp_args(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
+                            const FISPSequence& seq, cfloat* echo, int64_t echo_stride) {
     const int nTR = int(seq.RF_train.size());
     const int P = int(seq.sliceprofiles.size(0));
     const int N = seq.max_state;
     if (N < 1 || N > 128) COMPAS_ERROR("max_state must be in [1, 128]");
     COMPAS_CHECK(seq.undersampling_factor >= 1 && seq.repetitions >= 1);
     COMPAS_CHECK(P >= 1 && int(seq.sliceprofiles.size(1)) == nTR);
-    if (nvoxels <= 0 || nTR <= 0) return;
-    if (L.config < 0) L = fisp_default_launch(N, nvoxels, P);
-    COMPAS_CHECK(L.config >= 0 && L.config < fisp_config_count());
-    const auto& cfg = kFispConfigs[L.config];
-    COMPAS_CHECK(cfg.K * cfg.G >= N);
     const auto& tab = fisp_excite_table(ctx, seq);
 
     kernels::FispArgs a;
@@ -425,18 +452,70 @@ void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int v
     a.TI = seq.TI;
     a.echo = reinterpret_cast<float2*>(echo);
     a.echo_stride = echo_stride;
+    return a;
+}
 
+namespace {
+
+const FispConfig& checked_config(FispLaunch L, int N) {
+    COMPAS_CHECK(L.config >= 0 && L.config < fisp_config_count());
+    const auto& cfg = kFispConfigs[L.config];
+    COMPAS_CHECK(cfg.K * cfg.G >= N);
+    return cfg;
+}
+
+size_t fisp_smem_bytes(const FispConfig& cfg, int W) {
+    return size_t(W) * 32 * (32 / cfg.G) * sizeof(float2);  // ≤ 64 KB (W ≤ 8)
+}
+
+void allow_smem(const void* fn, size_t smem) {
+    if (smem > 48 * 1024)
+        COMPAS_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+}
+
+}  // namespace
+
+int fisp_tile_voxels(FispLaunch L) {
+    COMPAS_CHECK(L.config >= 0 && L.config < fisp_config_count());
+    return 32 / kFispConfigs[L.config].G;
+}
+
+void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
+                 const FISPSequence& seq, cfloat* echo, int64_t echo_stride, FispLaunch L) {
+    const int nTR = int(seq.RF_train.size());
+    const int P = int(seq.sliceprofiles.size(0));
+    const int N = seq.max_state;
+    if (nvoxels <= 0 || nTR <= 0) {
+        (void)fisp_args(ctx, params, voxel_begin, nvoxels, seq, echo, echo_stride);  // validates
+        return;
+    }
+    if (L.config < 0) L = fisp_default_launch(N, nvoxels, P);
+    const kernels::FispArgs a = fisp_args(ctx, params, voxel_begin, nvoxels, seq, echo, echo_stride);
+    const auto& cfg = checked_config(L, N);
     const int VB = 32 / cfg.G;
     const int W = std::max(1, std::min(L.warps, 8));
     dim3 grid(div_ceil(nvoxels, VB)), block(32 * W);
-    size_t smem = size_t(W) * 32 * VB * sizeof(float2);  // ≤ 64 KB (W ≤ 8)
+    const size_t smem = fisp_smem_bytes(cfg, W);
     DeviceGuard guard(ctx.device());
-    if (smem > 48 * 1024) {
-        COMPAS_CUDA_CHECK(cudaFuncSetAttribute(reinterpret_cast<const void*>(cfg.fn),
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    }
+    allow_smem(reinterpret_cast<const void*>(cfg.fn), smem);
     cfg.fn<<<grid, block, smem, ctx.stream()>>>(a);
     check_launch("fisp_epg_kernel");
+}
+
+void launch_fisp_queue(cudaStream_t stream, int device, FispLaunch L, int max_state, const kernels::FispArgs* jobs,
+                       const int2* items, int nitems, int* head) {
+    if (nitems <= 0) return;
+    const auto& cfg = checked_config(L, max_state);
+    const int W = std::max(1, std::min(L.warps, 8));
+    const size_t smem = fisp_smem_bytes(cfg, W);
+    DeviceGuard guard(device);
+    allow_smem(reinterpret_cast<const void*>(cfg.queue), smem);
+    int per_sm = 1, sms = 148;
+    COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.queue, 32 * W, smem));
+    COMPAS_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int grid = std::max(1, std::min(nitems, std::max(1, per_sm) * sms));
+    cfg.queue<<<grid, 32 * W, smem, stream>>>(jobs, items, nitems, head);
+    check_launch("fisp_queue_kernel");
 }
 
 Array<cfloat, 2> simulate_magnetization(const CompasContext& context, TissueParameters parameters,

@@ -1,0 +1,88 @@
+// job_args.cuh — argument blocks of the simulation and signal kernels.
+//
+// One block describes one operation (a simulation, a signal or J·v contraction) on one set of
+// device arrays. The one-operation kernels take it as a kernel parameter; the batched work-queue
+// kernels (batch.cu) take an array of them, one per job, in device memory.
+#pragma once
+
+#include <cstdint>
+
+#include <vector_types.h>
+
+namespace compas {
+namespace kernels {
+
+struct FispArgs {
+    const float* params;   // [9][param_stride]
+    int64_t param_stride;
+    int voxel_begin;       // first voxel of this launch
+    int nvoxels;           // voxels in this launch
+    const float4* table;   // [P][nTR]
+    int nTR, P, N, uf, reps, inversion, wait_spoil;
+    float TR, TE, TW, TI;
+    float2* echo;          // [nTR*uf][echo_stride], column = voxel_begin + local voxel
+    int64_t echo_stride;
+};
+
+struct PssfpArgs {
+    const float* params;
+    int64_t param_stride;
+    int voxel_begin, nvoxels;
+    const float2* zap;  // [nTR+1][nRF]
+    const float* z;     // [nz]
+    int nTR, nRF, nz;
+    float dt_ex, dt_inv, dt_pr, gz_ex, gz_pr;
+    float2* echo;  // [nTR][echo_stride]
+    int64_t echo_stride;
+};
+
+struct SpiralArgs {
+    const float* params;
+    int64_t pstride;
+    int nvoxels;
+    const float2* echo;
+    const float2* coils;
+    int R, S, C;
+    float dt;
+    const float2* k_start;
+    const float2* delta_k;
+    float2* signal;  // [C][R][S]
+};
+
+// per-voxel constants of the generated operand (written by tc_prep_kernel)
+struct VoxelGen {
+    double theta;  // Θ_v = Δk_re·x + Δk_im·y + 2πΔt·B0 (rad per sample)
+    float2 step;   // e^{-Δt/T2 + iΘ_v}
+    float decay;   // -Δt/T2
+    int valid;
+};
+
+struct TcArgs {
+    const float* params;
+    int64_t pstride;
+    int nvoxels;
+    const float2* echo;   // [R][V]
+    const float2* dT1;    // J·v only
+    const float2* dT2;
+    const float2* vec;    // J·v only: [4][V]
+    const float2* coils;  // [C][V]
+    int R, S, C;
+    float dt, dk_re, dk_im;
+    int vchunk;           // voxels per split
+    float2* out;          // [splits][C][R][S]
+    unsigned int* status;
+    const VoxelGen* vgen;         // [V] per-voxel generation constants (prep kernel)
+    const float2* coilw;          // [C][V] coil·w
+    const float4* jcoef;          // J·v only: [V][2] {T1ρv0, T2ρv1}, {v2 + i v3, ΔtR2²·T2ρv1}
+};
+
+// one split-K reduction: out[i] = Σ_q partials[q·n + i], q = 0..nsplit-1 in order
+struct PartialSum {
+    const float2* partials;
+    float2* out;
+    int64_t n;
+    int nsplit;
+};
+
+}  // namespace kernels
+}  // namespace compas

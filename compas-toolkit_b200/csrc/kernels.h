@@ -5,6 +5,7 @@
 #include <cstdint>
 
 #include "compas/compas.h"
+#include "job_args.cuh"
 
 namespace compas {
 
@@ -22,6 +23,14 @@ const Array<float, 3>& fisp_excite_table(const CompasContext& ctx, const FISPSeq
 // voxel_begin.. of a [nTR*uf][echo_stride] complex array
 void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
                  const FISPSequence& seq, cfloat* echo, int64_t echo_stride, FispLaunch L);
+// argument block of one FISP simulation (validates the sequence, builds its table on first use)
+kernels::FispArgs fisp_args(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
+                            const FISPSequence& seq, cfloat* echo, int64_t echo_stride);
+int fisp_tile_voxels(FispLaunch L);  // voxels per work item (tile) of layout L
+// persistent work-queue launch over (job, tile) items of FISP jobs that all use layout L;
+// *head must be 0 when the kernel starts
+void launch_fisp_queue(cudaStream_t stream, int device, FispLaunch L, int max_state, const kernels::FispArgs* jobs,
+                       const int2* items, int nitems, int* head);
 
 // ---- pSSFP ------------------------------------------------------------------------------
 struct PssfpLaunch {
@@ -33,6 +42,11 @@ PssfpLaunch pssfp_default_launch(int nz, int64_t nvoxels);
 PssfpLaunch tuned_pssfp_launch(int nz, int64_t nvoxels);
 void launch_pssfp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
                   const pSSFPSequence& seq, cfloat* echo, int64_t echo_stride, PssfpLaunch L);
+kernels::PssfpArgs pssfp_args(const CompasContext& ctx, const TissueParameters& params, int voxel_begin,
+                              int nvoxels, const pSSFPSequence& seq, cfloat* echo, int64_t echo_stride);
+int pssfp_tile_voxels(PssfpLaunch L);
+void launch_pssfp_queue(cudaStream_t stream, int device, PssfpLaunch L, int nz, const kernels::PssfpArgs* jobs,
+                        const int2* items, int nitems, int* head);
 
 // ---- signal / Jacobian products ----------------------------------------------------------
 enum class Precision { FP32, SplitBF16 };
@@ -42,6 +56,8 @@ struct CartesianGeom {
     float dt;
     float dk_re, dk_im;
 };
+CartesianGeom cartesian_geom(const CartesianTrajectory& t);
+Precision signal_precision(SimulateSignalMethod m);
 
 // s[c][r][k] = Σ_v coil[c][v]·ρ_v·m[r][v]·w_v·z_v^k  (Cartesian, signal_kernels.cuh:137-167)
 void launch_signal_cartesian(const CompasContext& ctx, const float* params, int64_t param_stride, int nvoxels,
@@ -65,5 +81,26 @@ void launch_residual(const CompasContext& ctx, const cfloat* lhs, const cfloat* 
 
 // ---- tcgen05 tensor-core complex GEMM support ---------------------------------------------
 bool tensor_cores_available(int device);
+
+// tile grid and voxel split of one split-BF16 contraction (a function of its shape only, so a
+// job gives the same partial sums alone and inside a batch)
+struct TcPlan {
+    int ntiles, mtiles, splits, vchunk;
+};
+TcPlan tc_plan(int device, int nvoxels, int R, int S, int C, bool jac);
+// argument block of a Cartesian signal contraction; out / vchunk / status / tables set by the caller
+kernels::TcArgs tc_signal_args(const float* params, int64_t pstride, int nvoxels, const cfloat* echos,
+                               const cfloat* coils, int ncoils, const CartesianGeom& g);
+// batched prep (prep_blocks flattened 128-thread blocks) and contraction (ctas flattened CTAs)
+void launch_tc_batch(cudaStream_t stream, int device, bool jac, const kernels::TcArgs* jobs, int njobs,
+                     const int* prep_offsets, int prep_blocks, const int* cta_offsets, int ctas);
+
+// ---- batched spiral signal and split-K sums -----------------------------------------------
+int spiral_coil_group(int ncoils);  // coils per block (1 or 4) of the spiral kernel
+int spiral_block_count(int ncoils, int nreadouts, int ns);
+void launch_signal_spiral_batch(cudaStream_t stream, int device, int coil_group, const kernels::SpiralArgs* jobs,
+                                const int* cta_offsets, int njobs, int ctas);
+void launch_sum_partials_batch(cudaStream_t stream, int device, const kernels::PartialSum* jobs,
+                               const int* block_offsets, int njobs, int blocks);
 
 }  // namespace compas

@@ -211,7 +211,7 @@ bool tensor_cores_available(int device) {
     return cache[device] == 1;
 }
 
-static CartesianGeom geom(const CartesianTrajectory& t) {
+CartesianGeom cartesian_geom(const CartesianTrajectory& t) {
     return CartesianGeom {t.nreadouts, t.samples_per_readout, t.delta_t, t.delta_k.re, t.delta_k.im};
 }
 
@@ -242,7 +242,7 @@ void launch_jacobian_hermitian(const CompasContext& ctx, const float* params, in
     launch_jacobian_hermitian_simt(ctx, params, pstride, nvoxels, echos, dT1, dT2, coils, ncoils, vec, g, JHv);
 }
 
-static Precision signal_precision(SimulateSignalMethod m) {
+Precision signal_precision(SimulateSignalMethod m) {
     return (m == SimulateSignalMethod::MatmulFast || m == SimulateSignalMethod::MatmulLow) ? Precision::SplitBF16
                                                                                              : Precision::FP32;
 }
@@ -264,7 +264,7 @@ Array<cfloat, 3> magnetization_to_signal(const CompasContext& context, Array<cfl
     Array<cfloat, 3> signal({ncoils, nreadouts, ns}, context.device());
     if (const auto* cart = dynamic_cast<const CartesianTrajectory*>(&trajectory)) {
         launch_signal_cartesian(context, parameters.data.data(), parameters.data.size(1), nvoxels, echos.data(),
-                                coil_sensitivities.data(), ncoils, geom(*cart), signal.data(),
+                                coil_sensitivities.data(), ncoils, cartesian_geom(*cart), signal.data(),
                                 signal_precision(method));
     } else if (const auto* sp = dynamic_cast<const SpiralTrajectory*>(&trajectory)) {
         COMPAS_CHECK(sp->k_start.size() == nreadouts && sp->delta_k.size() == nreadouts);
@@ -296,7 +296,7 @@ Array<cfloat, 3> compute_jacobian(const CompasContext& ctx, Array<cfloat, 2> ech
     COMPAS_CHECK(vector.size(0) == 4 && vector.size(1) == nvoxels);  // product.cu:304-313
     Array<cfloat, 3> Jv({ncoils, nreadouts, ns}, ctx.device());
     launch_jacobian(ctx, parameters.data.data(), parameters.data.size(1), nvoxels, echos.data(), delta_echos_T1.data(),
-                    delta_echos_T2.data(), coil_sensitivities.data(), ncoils, vector.data(), geom(trajectory),
+                    delta_echos_T2.data(), coil_sensitivities.data(), ncoils, vector.data(), cartesian_geom(trajectory),
                     Jv.data(), jacobian_precision(kind));
     return Jv;
 }
@@ -313,7 +313,7 @@ Array<cfloat, 2> compute_jacobian_hermitian(const CompasContext& ctx, Array<cflo
     Array<cfloat, 2> JHv({4, nvoxels}, ctx.device());
     launch_jacobian_hermitian(ctx, parameters.data.data(), parameters.data.size(1), nvoxels, echos.data(),
                               delta_echos_T1.data(), delta_echos_T2.data(), coil_sensitivities.data(), ncoils,
-                              vector.data(), geom(trajectory), JHv.data(), jacobian_precision(kind));
+                              vector.data(), cartesian_geom(trajectory), JHv.data(), jacobian_precision(kind));
     return JHv;
 }
 

@@ -17,6 +17,7 @@
 // accurate to < 3e-10, so the hot loop runs on the FMA pipe; larger angles use sqrt/sincos.
 #include "common.cuh"
 #include "compas/compas.h"
+#include "job_args.cuh"
 #include "kernels.h"
 
 namespace compas {
@@ -32,17 +33,6 @@ __global__ void pssfp_table_kernel(const float2* __restrict__ rf, int nTR, const
     zap[idx] = cmul(th, g[i]);
 }
 
-struct PssfpArgs {
-    const float* params;
-    int64_t param_stride;
-    int voxel_begin, nvoxels;
-    const float2* zap;  // [nTR+1][nRF]
-    const float* z;     // [nz]
-    int nTR, nRF, nz;
-    float dt_ex, dt_inv, dt_pr, gz_ex, gz_pr;
-    float2* echo;  // [nTR][echo_stride]
-    int64_t echo_stride;
-};
 
 struct Iso {
     float x, y, z;
@@ -75,11 +65,13 @@ __device__ __forceinline__ void rodrigues(Iso& m, float ax, float ay, float az, 
     m.z = fmaf(c, m.z, fmaf(s, cz, hd * az));
 }
 
+// One tile (128/GZ voxels) of a pSSFP simulation. Shared by the one-simulation kernel
+// (tile = blockIdx.x) and the batched work-queue kernel, so both give bit-identical echoes.
 template<int ZT, int GZ>
-__global__ void __launch_bounds__(128) pssfp_kernel(PssfpArgs a) {
+__device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
     const int lane = threadIdx.x & 31;
     const int sub = lane % GZ;
-    const int vloc = (blockIdx.x * blockDim.x + threadIdx.x) / GZ;
+    const int vloc = (tile * blockDim.x + threadIdx.x) / GZ;
     const bool vok = vloc < a.nvoxels;
     const int64_t vcol = a.voxel_begin + (vok ? vloc : a.nvoxels - 1);
     const float T1 = a.params[0 * a.param_stride + vcol];
@@ -169,22 +161,57 @@ __global__ void __launch_bounds__(128) pssfp_kernel(PssfpArgs a) {
     }
 }
 
+template<int ZT, int GZ>
+__global__ void __launch_bounds__(128) pssfp_kernel(PssfpArgs a) {
+    pssfp_tile<ZT, GZ>(a, blockIdx.x);
+}
+
+// Persistent work-queue kernel for a batch of pSSFP simulations sharing one (ZT, GZ) layout:
+// CTAs of 128 threads take (job, tile) items, longest job first, through an atomic counter.
+template<int ZT, int GZ>
+__global__ void __launch_bounds__(128) pssfp_queue_kernel(const PssfpArgs* __restrict__ jobs,
+                                                          const int2* __restrict__ items, int nitems,
+                                                          int* __restrict__ head) {
+    __shared__ PssfpArgs job;
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(head, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= nitems) break;
+        const int2 w = items[it];
+        if (threadIdx.x == 0) job = jobs[w.x];
+        __syncthreads();
+        pssfp_tile<ZT, GZ>(job, w.y);
+        __syncthreads();
+    }
+}
+
 }  // namespace kernels
 
 namespace {
 using PssfpKernel = void (*)(kernels::PssfpArgs);
+using PssfpQueueKernel = void (*)(const kernels::PssfpArgs*, const int2*, int, int*);
 struct PssfpConfig {
     int ZT, GZ;
     PssfpKernel fn;
+    PssfpQueueKernel queue;
 };
 const PssfpConfig kPssfpConfigs[] = {
-    {1, 1, kernels::pssfp_kernel<1, 1>},   {2, 1, kernels::pssfp_kernel<2, 1>},
-    {4, 1, kernels::pssfp_kernel<4, 1>},   {8, 1, kernels::pssfp_kernel<8, 1>},
-    {9, 4, kernels::pssfp_kernel<9, 4>},   {5, 8, kernels::pssfp_kernel<5, 8>},
-    {3, 16, kernels::pssfp_kernel<3, 16>}, {2, 32, kernels::pssfp_kernel<2, 32>},
-    {1, 32, kernels::pssfp_kernel<1, 32>}, {18, 2, kernels::pssfp_kernel<18, 2>},
-    {4, 4, kernels::pssfp_kernel<4, 4>},   {8, 4, kernels::pssfp_kernel<8, 4>},
-    {4, 8, kernels::pssfp_kernel<4, 8>},   {12, 4, kernels::pssfp_kernel<12, 4>},
+    {1, 1, kernels::pssfp_kernel<1, 1>, kernels::pssfp_queue_kernel<1, 1>},
+    {2, 1, kernels::pssfp_kernel<2, 1>, kernels::pssfp_queue_kernel<2, 1>},
+    {4, 1, kernels::pssfp_kernel<4, 1>, kernels::pssfp_queue_kernel<4, 1>},
+    {8, 1, kernels::pssfp_kernel<8, 1>, kernels::pssfp_queue_kernel<8, 1>},
+    {9, 4, kernels::pssfp_kernel<9, 4>, kernels::pssfp_queue_kernel<9, 4>},
+    {5, 8, kernels::pssfp_kernel<5, 8>, kernels::pssfp_queue_kernel<5, 8>},
+    {3, 16, kernels::pssfp_kernel<3, 16>, kernels::pssfp_queue_kernel<3, 16>},
+    {2, 32, kernels::pssfp_kernel<2, 32>, kernels::pssfp_queue_kernel<2, 32>},
+    {1, 32, kernels::pssfp_kernel<1, 32>, kernels::pssfp_queue_kernel<1, 32>},
+    {18, 2, kernels::pssfp_kernel<18, 2>, kernels::pssfp_queue_kernel<18, 2>},
+    {4, 4, kernels::pssfp_kernel<4, 4>, kernels::pssfp_queue_kernel<4, 4>},
+    {8, 4, kernels::pssfp_kernel<8, 4>, kernels::pssfp_queue_kernel<8, 4>},
+    {4, 8, kernels::pssfp_kernel<4, 8>, kernels::pssfp_queue_kernel<4, 8>},
+    {12, 4, kernels::pssfp_kernel<12, 4>, kernels::pssfp_queue_kernel<12, 4>},
 };
 }  // namespace
 
@@ -222,14 +249,13 @@ PssfpLaunch pssfp_default_launch(int nz, int64_t nvoxels) {
     return PssfpLaunch {best};
 }
 
-void launch_pssfp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
-                  const pSSFPSequence& seq, cfloat* echo, int64_t echo_stride, PssfpLaunch L) {
+kernels::PssfpArgs pssfp_args(const CompasContext& ctx, const TissueParameters& params, int voxel_begin,
+                              int nvoxels, const pSSFPSequence& seq, cfloat* echo, int64_t echo_stride) {
     const int nTR = int(seq.RF_train.size());
     const int nRF = int(seq.gamma_dt_RF.size());
     const int nz = int(seq.z.size());
     COMPAS_CHECK(nTR > 0);
     if (nz > 64) COMPAS_ERROR("pSSFP supports at most 64 z positions");
-    if (nvoxels <= 0) return;
     DeviceGuard guard(ctx.device());
     std::shared_ptr<Array<cfloat, 2>> zap;
     {
@@ -251,9 +277,6 @@ void launch_pssfp(const CompasContext& ctx, const TissueParameters& params, int 
         }
         zap = cache.table;
     }
-    if (L.config < 0) L = pssfp_default_launch(nz, nvoxels);
-    const auto& cfg = kPssfpConfigs[L.config];
-    if (cfg.ZT * cfg.GZ < nz) COMPAS_ERROR("pSSFP layout does not cover the z positions");
     kernels::PssfpArgs a;
     a.params = params.data.data();
     a.param_stride = params.data.size(1);
@@ -271,10 +294,48 @@ void launch_pssfp(const CompasContext& ctx, const TissueParameters& params, int 
     a.gz_pr = seq.gamma_dt_GRz.pr;
     a.echo = reinterpret_cast<float2*>(echo);
     a.echo_stride = echo_stride;
-    const int threads = 128;
+    return a;
+}
+
+namespace {
+const PssfpConfig& checked_config(PssfpLaunch L, int nz) {
+    COMPAS_CHECK(L.config >= 0 && L.config < pssfp_config_count());
+    const auto& cfg = kPssfpConfigs[L.config];
+    if (cfg.ZT * cfg.GZ < nz) COMPAS_ERROR("pSSFP layout does not cover the z positions");
+    return cfg;
+}
+constexpr int kPssfpThreads = 128;
+}  // namespace
+
+int pssfp_tile_voxels(PssfpLaunch L) {
+    COMPAS_CHECK(L.config >= 0 && L.config < pssfp_config_count());
+    return kPssfpThreads / kPssfpConfigs[L.config].GZ;
+}
+
+void launch_pssfp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
+                  const pSSFPSequence& seq, cfloat* echo, int64_t echo_stride, PssfpLaunch L) {
+    const int nz = int(seq.z.size());
+    const kernels::PssfpArgs a = pssfp_args(ctx, params, voxel_begin, nvoxels, seq, echo, echo_stride);
+    if (nvoxels <= 0) return;
+    if (L.config < 0) L = pssfp_default_launch(nz, nvoxels);
+    const auto& cfg = checked_config(L, nz);
     const int64_t total = int64_t(nvoxels) * cfg.GZ;
-    cfg.fn<<<unsigned((total + threads - 1) / threads), threads, 0, ctx.stream()>>>(a);
+    DeviceGuard guard(ctx.device());
+    cfg.fn<<<unsigned((total + kPssfpThreads - 1) / kPssfpThreads), kPssfpThreads, 0, ctx.stream()>>>(a);
     check_launch("pssfp_kernel");
+}
+
+void launch_pssfp_queue(cudaStream_t stream, int device, PssfpLaunch L, int nz, const kernels::PssfpArgs* jobs,
+                        const int2* items, int nitems, int* head) {
+    if (nitems <= 0) return;
+    const auto& cfg = checked_config(L, nz);
+    DeviceGuard guard(device);
+    int per_sm = 1, sms = 148;
+    COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.queue, kPssfpThreads, 0));
+    COMPAS_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int grid = std::max(1, std::min(nitems, std::max(1, per_sm) * sms));
+    cfg.queue<<<grid, kPssfpThreads, 0, stream>>>(jobs, items, nitems, head);
+    check_launch("pssfp_queue_kernel");
 }
 
 Array<cfloat, 2> simulate_magnetization(const CompasContext& context, TissueParameters parameters,

@@ -18,6 +18,7 @@
 // kernel); 256 threads, 8×4 complex register micro-tile, 16-voxel shared-memory chunks.
 #include "common.cuh"
 #include "compas/compas.h"
+#include "job_args.cuh"
 #include "kernels.h"
 
 namespace compas {
@@ -185,28 +186,17 @@ __global__ void sum_partials_kernel(const float2* __restrict__ partials, int nsp
 // ---- spiral: per readout r, s[c][r][k] = Σ_v coil·A[r][v]·z_rv^k  (signal_kernels.cuh:274-345)
 constexpr int SP_THREADS = 128, SP_KPT = 8, SP_VCH = 64;
 
-struct SpiralArgs {
-    const float* params;
-    int64_t pstride;
-    int nvoxels;
-    const float2* echo;
-    const float2* coils;
-    int R, S, C;
-    float dt;
-    const float2* k_start;
-    const float2* delta_k;
-    float2* signal;  // [C][R][S]
-};
 
+// One block of the spiral signal: samples bx·SP_THREADS·SP_KPT.., readout r, coils cz·CT..
+// Shared by the one-operation kernel (blockIdx) and the batched kernel: bit-identical results.
 template<int CT>
-__global__ void __launch_bounds__(SP_THREADS) signal_spiral_kernel(SpiralArgs a) {
+__device__ __forceinline__ void spiral_tile(const SpiralArgs& a, const int bx, const int r, const int cz) {
     __shared__ float2 sA[SP_VCH];            // ρ·rewind·prephaser·m for this readout
     __shared__ double sTheta[SP_VCH];        // Θ_rv
     __shared__ float sDecay[SP_VCH];         // -Δt R2
     __shared__ float2 sCoil[CT][SP_VCH];
-    const int r = blockIdx.y;
-    const int c0 = blockIdx.z * CT;
-    const int k0 = (blockIdx.x * SP_THREADS + threadIdx.x) * SP_KPT;
+    const int c0 = cz * CT;
+    const int k0 = (bx * SP_THREADS + threadIdx.x) * SP_KPT;
     const double twopi = 6.283185307179586476925;
     const float2 ks = a.k_start[r], dkr = a.delta_k[r];
     float2 acc[CT][SP_KPT];
@@ -273,6 +263,53 @@ __global__ void __launch_bounds__(SP_THREADS) signal_spiral_kernel(SpiralArgs a)
             if (k < a.S) a.signal[(int64_t(c0 + c) * a.R + r) * a.S + k] = acc[c][j];
         }
     }
+}
+
+template<int CT>
+__global__ void __launch_bounds__(SP_THREADS) signal_spiral_kernel(SpiralArgs a) {
+    spiral_tile<CT>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+__device__ __forceinline__ int job_of_block(const int* __restrict__ offsets, int njobs, int b) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(offsets + mid) <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Batched spiral signal: flattened block b → job j (cta_offsets[j] ≤ b < cta_offsets[j+1]) and the
+// block (l % nx, (l / nx) % R, l / (nx·R)) of that job's own grid, l = b - cta_offsets[j].
+template<int CT>
+__global__ void __launch_bounds__(SP_THREADS) signal_spiral_batch_kernel(const SpiralArgs* __restrict__ jobs,
+                                                                        const int* __restrict__ cta_offsets,
+                                                                        int njobs) {
+    __shared__ SpiralArgs job;
+    __shared__ int3 blk;
+    if (threadIdx.x == 0) {
+        const int j = job_of_block(cta_offsets, njobs, blockIdx.x);
+        job = jobs[j];
+        const int nx = (job.S + SP_THREADS * SP_KPT - 1) / (SP_THREADS * SP_KPT);
+        const int l = blockIdx.x - cta_offsets[j];
+        blk = make_int3(l % nx, (l / nx) % job.R, l / (nx * job.R));
+    }
+    __syncthreads();
+    spiral_tile<CT>(job, blk.x, blk.y, blk.z);
+}
+
+// Batched sum of split-K partials: flattened 256-thread block b → job j, element
+// (b - block_offsets[j])·256 + t; same per-element order as sum_partials_kernel.
+__global__ void sum_partials_batch_kernel(const PartialSum* __restrict__ jobs, const int* __restrict__ block_offsets,
+                                          int njobs) {
+    const int j = job_of_block(block_offsets, njobs, blockIdx.x);
+    const PartialSum p = jobs[j];
+    const int64_t i = int64_t(blockIdx.x - block_offsets[j]) * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    float2 s = p.partials[i];
+    for (int q = 1; q < p.nsplit; q++) s = cadd(s, p.partials[int64_t(q) * p.n + i]);
+    p.out[i] = s;
 }
 
 }  // namespace kernels
@@ -384,6 +421,37 @@ void launch_signal_spiral(const CompasContext& ctx, const float* params, int64_t
         kernels::signal_spiral_kernel<4><<<grid, kernels::SP_THREADS, 0, ctx.stream()>>>(a);
     }
     check_launch("signal_spiral_kernel");
+}
+
+int spiral_coil_group(int ncoils) {
+    return ncoils <= 1 ? 1 : 4;
+}
+
+int spiral_block_count(int ncoils, int nreadouts, int ns) {
+    const int kper = kernels::SP_THREADS * kernels::SP_KPT;
+    const int ct = spiral_coil_group(ncoils);
+    return div_ceil(ns, kper) * nreadouts * div_ceil(ncoils, ct);
+}
+
+void launch_signal_spiral_batch(cudaStream_t stream, int device, int coil_group, const kernels::SpiralArgs* jobs,
+                                const int* cta_offsets, int njobs, int ctas) {
+    if (njobs <= 0 || ctas <= 0) return;
+    DeviceGuard guard(device);
+    if (coil_group == 1) {
+        kernels::signal_spiral_batch_kernel<1><<<ctas, kernels::SP_THREADS, 0, stream>>>(jobs, cta_offsets, njobs);
+    } else {
+        COMPAS_CHECK(coil_group == 4);
+        kernels::signal_spiral_batch_kernel<4><<<ctas, kernels::SP_THREADS, 0, stream>>>(jobs, cta_offsets, njobs);
+    }
+    check_launch("signal_spiral_batch_kernel");
+}
+
+void launch_sum_partials_batch(cudaStream_t stream, int device, const kernels::PartialSum* jobs,
+                               const int* block_offsets, int njobs, int blocks) {
+    if (njobs <= 0 || blocks <= 0) return;
+    DeviceGuard guard(device);
+    kernels::sum_partials_batch_kernel<<<blocks, 256, 0, stream>>>(jobs, block_offsets, njobs);
+    check_launch("sum_partials_batch_kernel");
 }
 
 }  // namespace compas

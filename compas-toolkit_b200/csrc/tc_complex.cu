@@ -25,8 +25,11 @@
 // The voxel range is split over CTAs (split-K); partial tiles are summed in a fixed order.
 #include <cuda_bf16.h>
 
+#include <mutex>
+
 #include "common.cuh"
 #include "compas/compas.h"
+#include "job_args.cuh"
 #include "kernels.h"
 #include "tc_common.cuh"
 
@@ -44,38 +47,13 @@ constexpr int TC_B_BYTES = TC_N * TC_K * 2;  // 32 KB per hi/lo plane
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
 constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 128 /*barriers*/;
 
-struct TcArgs {
-    const float* params;
-    int64_t pstride;
-    int nvoxels;
-    const float2* echo;   // [R][V]
-    const float2* dT1;    // J·v only
-    const float2* dT2;
-    const float2* vec;    // J·v only: [4][V]
-    const float2* coils;  // [C][V]
-    int R, S, C;
-    float dt, dk_re, dk_im;
-    int vchunk;           // voxels per split
-    float2* out;          // [splits][C][R][S]
-    unsigned int* status;
-    const struct VoxelGen* vgen;  // [V] per-voxel generation constants (prep kernel)
-    const float2* coilw;          // [C][V] coil·w
-    const float4* jcoef;          // J·v only: [V][2] {T1ρv0, T2ρv1}, {v2 + i v3, ΔtR2²·T2ρv1}
-};
 
-// per-voxel constants of the generated operand (written by tc_prep_kernel)
-struct VoxelGen {
-    double theta;  // Θ_v = Δk_re·x + Δk_im·y + 2πΔt·B0 (rad per sample)
-    float2 step;   // e^{-Δt/T2 + iΘ_v}
-    float decay;   // -Δt/T2
-    int valid;
-};
 
 // one thread per voxel: generation constants, coil·w for every coil and (J·v) the four complex
 // coefficients of P and Q' — done once per call instead of once per CTA and stage
 template<bool JAC>
-__global__ void tc_prep_kernel(TcArgs a, VoxelGen* vgen, float2* coilw, float4* jcoef) {
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void tc_prep_voxel(const TcArgs& a, const int v, VoxelGen* vgen, float2* coilw,
+                                              float4* jcoef) {
     if (v >= a.nvoxels) return;
     const double twopi = 6.283185307179586476925;
     const float T1 = a.params[v], T2 = a.params[a.pstride + v], B0 = a.params[3 * a.pstride + v];
@@ -109,12 +87,20 @@ __global__ void tc_prep_kernel(TcArgs a, VoxelGen* vgen, float2* coilw, float4* 
 }
 
 template<bool JAC>
-__global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
+__global__ void tc_prep_kernel(TcArgs a, VoxelGen* vgen, float2* coilw, float4* jcoef) {
+    tc_prep_voxel<JAC>(a, blockIdx.x * blockDim.x + threadIdx.x, vgen, coilw, jcoef);
+}
+
+// One output tile (pair tile bx, readout tile by, voxel split bz) of one contraction. Shared by
+// the one-operation kernel (tile = blockIdx) and the batched kernel, so both give bit-identical
+// results.
+template<bool JAC>
+__device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int by, const int bz,
+                                        unsigned char* smem_raw) {
     constexpr int TERMS = JAC ? 2 : 1;            // complex terms per voxel along K
     constexpr int VPS = TC_K / (2 * TERMS);       // voxels per stage (32 or 16)
     constexpr int VPC = 4 / TERMS;                // voxels per 16-byte chunk (4 or 2)
     constexpr int VPH = VPC / 2;                  // voxels per 8-byte half chunk (2 or 1)
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + TC_STAGES * TC_STAGE_BYTES);
     uint64_t* empty = full + TC_STAGES;
@@ -123,9 +109,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n_pair0 = blockIdx.x * (TC_N / 2);          // first (c,k) pair of this tile
-    const int r0 = blockIdx.y * TC_M;
-    const int split = blockIdx.z;
+    const int n_pair0 = bx * (TC_N / 2);                  // first (c,k) pair of this tile
+    const int r0 = by * TC_M;
+    const int split = bz;
     const int v_begin = split * a.vchunk;
     const int v_end = min(a.nvoxels, v_begin + a.vchunk);
     const int nstages = max(1, (v_end - v_begin + VPS - 1) / VPS);
@@ -378,22 +364,80 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
     }
 }
 
+template<bool JAC>
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    tc_tile<JAC>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+}
+
+// tile grid of one contraction: (pair tiles, readout tiles, voxel splits)
+__device__ __forceinline__ int3 tc_grid_of(const TcArgs& a) {
+    return make_int3((a.C * a.S + TC_N / 2 - 1) / (TC_N / 2), (a.R + TC_M - 1) / TC_M,
+                     (a.nvoxels + a.vchunk - 1) / a.vchunk);
+}
+
+// index of the job owning flattened block b: offsets[j] ≤ b < offsets[j + 1] (offsets ascending)
+__device__ __forceinline__ int job_of_block(const int* __restrict__ offsets, int njobs, int b) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(offsets + mid) <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Batched contraction: one launch for many jobs. Flattened CTA b belongs to job j
+// (cta_offsets[j] ≤ b < cta_offsets[j+1]) and takes the tile the one-operation grid of that job
+// would give blockIdx = (l % nx, (l / nx) % ny, l / (nx·ny)), l = b - cta_offsets[j]. Jobs are
+// ordered by decreasing work per CTA, so the block scheduler runs the longest tiles first.
+template<bool JAC>
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_batch_kernel(const TcArgs* __restrict__ jobs,
+                                                                         const int* __restrict__ cta_offsets,
+                                                                         int njobs) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ TcArgs job;
+    __shared__ int3 tile;
+    if (threadIdx.x == 0) {
+        const int j = job_of_block(cta_offsets, njobs, blockIdx.x);
+        job = jobs[j];
+        const int3 g = tc_grid_of(job);
+        const int l = blockIdx.x - cta_offsets[j];
+        tile = make_int3(l % g.x, (l / g.x) % g.y, l / (g.x * g.y));
+    }
+    __syncthreads();
+    tc_tile<JAC>(job, tile.x, tile.y, tile.z, smem_raw);
+}
+
+// batched tc_prep_kernel: flattened 128-thread block b → job j, voxel (b - offsets[j])·128 + t
+template<bool JAC>
+__global__ void tc_prep_batch_kernel(const TcArgs* __restrict__ jobs, const int* __restrict__ block_offsets,
+                                     int njobs) {
+    __shared__ TcArgs job;
+    __shared__ int local;
+    if (threadIdx.x == 0) {
+        const int j = job_of_block(block_offsets, njobs, blockIdx.x);
+        job = jobs[j];
+        local = blockIdx.x - block_offsets[j];
+    }
+    __syncthreads();
+    tc_prep_voxel<JAC>(job, local * blockDim.x + threadIdx.x, const_cast<VoxelGen*>(job.vgen),
+                       const_cast<float2*>(job.coilw), const_cast<float4*>(job.jcoef));
+}
+
 }  // namespace kernels
 
-namespace {
-
-bool run_tc(const CompasContext& ctx, kernels::TcArgs a, bool jac, cfloat* out) {
-    if (!tensor_cores_available(ctx.device())) return false;
-    DeviceGuard guard(ctx.device());
-    const int npairs = a.C * a.S;
-    const int ntiles = div_ceil(npairs, kernels::TC_N / 2), mtiles = div_ceil(a.R, kernels::TC_M);
-    const int tiles = ntiles * mtiles;
+TcPlan tc_plan(int device, int nvoxels, int R, int S, int C, bool jac) {
+    TcPlan p;
+    p.ntiles = div_ceil(C * S, kernels::TC_N / 2);
+    p.mtiles = div_ceil(R, kernels::TC_M);
+    const int tiles = p.ntiles * p.mtiles;
     const int vps = jac ? 16 : 32;
     // split the voxel range over CTAs: pick the split count (≥ 16 stages per split) whose grid
     // leaves the least idle SM time in the last wave of one CTA per SM
     int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device());
-    const int max_splits = std::max(1, std::min(64, a.nvoxels / (16 * vps)));
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const int max_splits = std::max(1, std::min(64, nvoxels / (16 * vps)));
     int splits = 1;
     double best = -1.0;
     for (int sp = 1; sp <= max_splits; sp++) {
@@ -405,8 +449,32 @@ bool run_tc(const CompasContext& ctx, kernels::TcArgs a, bool jac, cfloat* out) 
             splits = sp;
         }
     }
-    a.vchunk = div_ceil(div_ceil(a.nvoxels, splits), vps) * vps;
-    splits = std::max(1, div_ceil(a.nvoxels, a.vchunk));
+    p.vchunk = std::max(vps, div_ceil(div_ceil(std::max(nvoxels, 1), splits), vps) * vps);
+    p.splits = std::max(1, div_ceil(nvoxels, p.vchunk));
+    return p;
+}
+
+namespace {
+
+void set_tc_smem_attribute(bool jac, bool batch) {
+    static std::once_flag once[4];
+    std::call_once(once[int(jac) + 2 * int(batch)], [&] {
+        const void* fn = batch ? (jac ? reinterpret_cast<const void*>(kernels::tc_contract_batch_kernel<true>)
+                                      : reinterpret_cast<const void*>(kernels::tc_contract_batch_kernel<false>))
+                               : (jac ? reinterpret_cast<const void*>(kernels::tc_contract_kernel<true>)
+                                      : reinterpret_cast<const void*>(kernels::tc_contract_kernel<false>));
+        COMPAS_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kernels::TC_SMEM));
+    });
+}
+
+bool run_tc(const CompasContext& ctx, kernels::TcArgs a, bool jac, cfloat* out) {
+    if (!tensor_cores_available(ctx.device())) return false;
+    DeviceGuard guard(ctx.device());
+    const int npairs = a.C * a.S;
+    const TcPlan plan = tc_plan(ctx.device(), a.nvoxels, a.R, a.S, a.C, jac);
+    const int ntiles = plan.ntiles, mtiles = plan.mtiles;
+    int splits = plan.splits;
+    a.vchunk = plan.vchunk;
     const int64_t n = int64_t(npairs) * a.R;
     Array<cfloat, 2> partials({splits > 1 ? splits : 0, n}, ctx.device());
     // per-voxel tables: 24 B generation constants, C coil·w values, J·v coefficients
@@ -428,12 +496,7 @@ bool run_tc(const CompasContext& ctx, kernels::TcArgs a, bool jac, cfloat* out) 
     }
     check_launch("tc_prep_kernel");
     auto fn = jac ? kernels::tc_contract_kernel<true> : kernels::tc_contract_kernel<false>;
-    static bool attr_set[2] = {false, false};
-    if (!attr_set[jac]) {
-        COMPAS_CUDA_CHECK(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn),
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, kernels::TC_SMEM));
-        attr_set[jac] = true;
-    }
+    set_tc_smem_attribute(jac, false);
     dim3 grid(ntiles, mtiles, splits);
     fn<<<grid, kernels::TC_THREADS, kernels::TC_SMEM, ctx.stream()>>>(a);
     check_launch("tc_contract_kernel");
@@ -484,6 +547,29 @@ bool launch_jacobian_tc(const CompasContext& ctx, const float* params, int64_t p
     a.dT2 = reinterpret_cast<const float2*>(dT2);
     a.vec = reinterpret_cast<const float2*>(vec);
     return run_tc(ctx, a, true, Jv);
+}
+
+kernels::TcArgs tc_signal_args(const float* params, int64_t pstride, int nvoxels, const cfloat* echos,
+                               const cfloat* coils, int ncoils, const CartesianGeom& g) {
+    return common_args(params, pstride, nvoxels, echos, coils, ncoils, g);
+}
+
+void launch_tc_batch(cudaStream_t stream, int device, bool jac, const kernels::TcArgs* jobs, int njobs,
+                     const int* prep_offsets, int prep_blocks, const int* cta_offsets, int ctas) {
+    if (njobs <= 0) return;
+    DeviceGuard guard(device);
+    if (prep_blocks > 0) {
+        if (jac) kernels::tc_prep_batch_kernel<true><<<prep_blocks, 128, 0, stream>>>(jobs, prep_offsets, njobs);
+        else kernels::tc_prep_batch_kernel<false><<<prep_blocks, 128, 0, stream>>>(jobs, prep_offsets, njobs);
+        check_launch("tc_prep_batch_kernel");
+    }
+    if (ctas <= 0) return;
+    set_tc_smem_attribute(jac, true);
+    if (jac)
+        kernels::tc_contract_batch_kernel<true><<<ctas, kernels::TC_THREADS, kernels::TC_SMEM, stream>>>(jobs, cta_offsets, njobs);
+    else
+        kernels::tc_contract_batch_kernel<false><<<ctas, kernels::TC_THREADS, kernels::TC_SMEM, stream>>>(jobs, cta_offsets, njobs);
+    check_launch("tc_contract_batch_kernel");
 }
 
 

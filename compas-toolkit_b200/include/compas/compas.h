@@ -16,6 +16,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <variant>
 #include <vector>
 
 namespace compas {
@@ -430,5 +431,42 @@ Array<cfloat, 2> compute_jacobian_hermitian(const CompasContext& ctx, Array<cflo
 // lhs - rhs and Σ|lhs - rhs|²   (compas/utils/residual.h:20-24)
 Array<cfloat, 3> compute_residual(CompasContext ctx, Array<cfloat, 3> lhs, Array<cfloat, 3> rhs,
                                   float* objective_out = nullptr);
+
+// ------------------------------------------------------------------------------------------
+// batched execution (no counterpart in the reference, which runs one operation per call)
+// ------------------------------------------------------------------------------------------
+
+// One independent simulate → signal job: its own voxels, sequence, trajectory and coils.
+// Without a trajectory the job only simulates.
+struct SimulationJob {
+    TissueParameters parameters;
+    std::variant<FISPSequence, pSSFPSequence> sequence;
+    std::variant<std::monostate, CartesianTrajectory, SpiralTrajectory> trajectory;
+    Array<cfloat, 2> coil_sensitivities;  // [ncoils][nvoxels]
+};
+
+// Many jobs of uneven size in a handful of launches: every FISP job of one launch layout runs
+// in one persistent work-queue kernel, every pSSFP job likewise (on a second stream, so the two
+// families overlap), then the Cartesian signals of each family in one batched tensor-core
+// launch and the spiral signals in one batched launch per coil grouping. Each job gives the
+// same bits as simulate_magnetization + magnetization_to_signal called for it alone.
+// All buffers are allocated at construction; run() only enqueues kernels (and can be captured
+// into a CUDA graph).
+class SimulationBatch: public Object {
+  public:
+    SimulationBatch(const CompasContext& ctx, std::vector<SimulationJob> jobs,
+                    SimulateSignalMethod method = SimulateSignalMethod::MatmulFast);
+    // enqueue every job on the context's stream (returns without waiting)
+    void run() const;
+    int size() const;
+    const Array<cfloat, 2>& echos(int job) const;   // [nreadouts][nvoxels]
+    const Array<cfloat, 3>& signal(int job) const;  // [ncoils][nreadouts][ns]; empty without trajectory
+    const char* name() const override { return "compas::SimulationBatch"; }
+
+    struct Impl;
+
+  private:
+    std::shared_ptr<Impl> m_impl;
+};
 
 }  // namespace compas

@@ -50,6 +50,12 @@ def tissue(rng: np.random.Generator, n_side: int, fov: float) -> np.ndarray:
     return p
 
 
+def tissue_voxels(rng: np.random.Generator, nv: int, fov: float) -> np.ndarray:
+    """`tissue` for an arbitrary voxel count: the first nv points of a ceil(√nv)² grid."""
+    side = max(1, math.ceil(math.sqrt(nv)))
+    return np.ascontiguousarray(tissue(rng, side, fov)[:, :nv])
+
+
 def cartesian(nr: int, ns: int, fov: float, dt: float, nlines: int) -> dict:
     """k_start[r] = -S/2·Δkx + i·py[r]·Δky with py cycling -nlines/2 .. nlines/2-1; Δk = 2π/FOV."""
     dk = 2 * np.pi / fov
@@ -189,3 +195,37 @@ def tiny(seed: int = 7, n_side: int = 6, ntr: int = 13, ns: int = 7, nc: int = 3
     traj = cartesian(ntr, ns, fov, 1e-5, ns)
     coils = cn(rng, (nc, nv))
     return {"name": "tiny", "params": params, "seq": seq, "traj": traj, "coils": coils, "fov": fov}
+
+
+def batch_jobs(seed: int = 4, njobs: int = 256, vmin: int = 1000, vmax: int = 64000, ntr_min: int = 400,
+               ntr_max: int = 1120, cmax: int = 16, ns_spiral: int = 1000, P: int = 35, max_state: int = 25,
+               nz: int = 35, nrf: int = 15) -> list:
+    """Uneven independent jobs: V ~ logU[vmin, vmax], nTR ~ U{ntr_min..ntr_max}, C ~ U{1..cmax};
+    50/50 FISP (max_state states, P Gaussian slice positions, smooth random 0–70° train) vs pSSFP
+    (nz z positions, Gaussian RF of nrf samples); 50/50 Cartesian (S = round(√V), nTR readouts)
+    vs variable-density spiral (nTR interleaves × ns_spiral samples). FOV 22.4 cm."""
+    rng = np.random.default_rng(seed)
+    fov = 22.4
+    jobs = []
+    for i in range(njobs):
+        nv = int(round(math.exp(rng.uniform(math.log(vmin), math.log(vmax)))))
+        ntr = int(rng.integers(ntr_min, ntr_max + 1))
+        nc = int(rng.integers(1, cmax + 1))
+        jrng = np.random.default_rng([seed, i])
+        params = tissue_voxels(jrng, nv, fov)
+        if rng.uniform() < 0.5:
+            kind = "fisp"
+            seq = fisp_sequence(smooth_flip_train(jrng, ntr), gaussian_slice_profile(P, ntr), 8.7e-3, 4.35e-3,
+                                25e-3, max_state)
+        else:
+            kind = "pssfp"
+            seq = pssfp_sequence(jrng, ntr, nrf=nrf, nz=nz)
+        if rng.uniform() < 0.5:
+            ns = max(2, int(round(math.sqrt(nv))))
+            traj = cartesian(ntr, ns, fov, 5e-6, ns)
+        else:
+            traj = spiral(jrng, ntr, ns_spiral, fov, 4e-6)
+        coils = gaussian_coils(nc, params, fov)
+        jobs.append({"kind": kind, "params": params, "seq": seq, "traj": traj, "coils": coils,
+                     "nvoxels": nv, "ntr": ntr, "ncoils": nc})
+    return jobs

@@ -179,6 +179,25 @@ COMPAS_API int compas_b200_fisp_config_info(int index, int* states_per_lane, int
 COMPAS_API int compas_b200_pssfp_config_count(void);
 COMPAS_API int compas_b200_pssfp_config_info(int index, int* iso_per_lane, int* lanes);
 
+/* Batched jobs (no counterpart in the reference): njobs independent simulate -> signal jobs,
+ * job i = (parameters[i], sequences[i] (FISP or pSSFP), trajectories[i] (Cartesian, spiral, or
+ * NULL for simulate only), coils[i] ([ncoils][nvoxels] complex; NULL without trajectory)),
+ * planned once into a few persistent work-queue / batched launches. `method` is a
+ * SimulateSignalMethod value as in compas_b200_magnetization_to_signal. The handle is released
+ * with compas_destroy_object. Each job's echoes and signal equal, bit for bit, those of the
+ * one-job calls (compas_simulate_magnetization_* then compas_b200_magnetization_to_signal). */
+COMPAS_API compas_object* compas_b200_make_batch(const compas_context* ctx, int njobs,
+                                                 const compas_object* const* parameters,
+                                                 const compas_object* const* sequences,
+                                                 const compas_object* const* trajectories,
+                                                 const compas_array* const* coils, int method);
+/* Enqueue every job of the batch on the context's stream; 0 on success, -1 on error. */
+COMPAS_API int compas_b200_batch_run(const compas_object* batch);
+/* New array handles sharing the batch's result storage (valid while the batch exists or
+ * until released with compas_destroy_array; the next run overwrites them). */
+COMPAS_API compas_array* compas_b200_batch_echos(const compas_object* batch, int job);
+COMPAS_API compas_array* compas_b200_batch_signal(const compas_object* batch, int job);
+
 #ifdef __cplusplus
 }
 #endif
