@@ -203,7 +203,8 @@ void SimulationBatch::Impl::plan_simulation(Family& fam, bool fisp, const std::v
 
 void SimulationBatch::Impl::plan_signal(Family& fam, const std::vector<int>& members) {
     const int dev = ctx.device();
-    std::vector<int> tc_jobs, spiral1, spiral4;
+    std::vector<int> tc_jobs;
+    std::vector<int> spiral_by_group[4];  // coil groupings 1, 2, 4, 8
     for (int j : members) {
         const auto& job = jobs[size_t(j)];
         if (std::holds_alternative<std::monostate>(job.trajectory)) continue;
@@ -218,7 +219,8 @@ void SimulationBatch::Impl::plan_signal(Family& fam, const std::vector<int>& mem
             if (prec == Precision::SplitBF16 && tensor_cores_available(dev)) tc_jobs.push_back(j);
             else fam.simt_cartesian.push_back(j);
         } else {
-            (spiral_coil_group(C) == 1 ? spiral1 : spiral4).push_back(j);
+            const int cg = spiral_coil_group(C);
+            spiral_by_group[cg == 1 ? 0 : cg == 2 ? 1 : cg == 4 ? 2 : 3].push_back(j);
         }
     }
 
@@ -285,8 +287,9 @@ void SimulationBatch::Impl::plan_signal(Family& fam, const std::vector<int>& mem
     }
 
     // ---- spiral, one batched launch per coil grouping
-    for (int cg : {1, 4}) {
-        std::vector<int>& js = cg == 1 ? spiral1 : spiral4;
+    for (int gi = 0; gi < 4; gi++) {
+        const int cg = 1 << gi;
+        std::vector<int>& js = spiral_by_group[gi];
         if (js.empty()) continue;
         std::stable_sort(js.begin(), js.end(),
                          [&](int a, int b) { return jobs[size_t(a)].parameters.nvoxels > jobs[size_t(b)].parameters.nvoxels; });

@@ -267,7 +267,7 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
                         if (t == 0) {
                             st.excite(make_coefs(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), sub);
                         } else {
-                            st.shift<ONEHOT>(sub, a.N);
+                            st.template shift<ONEHOT>(sub, a.N);
                             st.excite(make_coefs(tv, B1, c_TR, E1_TR, beta), sub);
                         }
                         if (sampled && sub == 0) samples[(warp * 32 + j) * VB + grp] = cmul(c_TE, st.u[0]);
@@ -297,7 +297,7 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
             if (rep > 1) {  // close the repetition: relax to TR, dephase, spoil, wait (fisp_kernels.cuh:195-200)
                 if (pok) {
                     st.relax(c_TR, E1_TR, sub);
-                    st.shift<ONEHOT>(sub, a.N);
+                    st.template shift<ONEHOT>(sub, a.N);
                     if (a.wait_spoil) st.spoil();
                     st.relax(c_W, E1_W, sub);
                 }

@@ -96,7 +96,7 @@ void launch_tc_batch(cudaStream_t stream, int device, bool jac, const kernels::T
                      const int* prep_offsets, int prep_blocks, const int* cta_offsets, int ctas);
 
 // ---- batched spiral signal and split-K sums -----------------------------------------------
-int spiral_coil_group(int ncoils);  // coils per block (1 or 4) of the spiral kernel
+int spiral_coil_group(int ncoils);  // coils per block (1, 2, 4 or 8) of the spiral kernel
 int spiral_block_count(int ncoils, int nreadouts, int ns);
 void launch_signal_spiral_batch(cudaStream_t stream, int device, int coil_group, const kernels::SpiralArgs* jobs,
                                 const int* cta_offsets, int njobs, int ctas);

@@ -184,20 +184,29 @@ __global__ void sum_partials_kernel(const float2* __restrict__ partials, int nsp
 }
 
 // ---- spiral: per readout r, s[c][r][k] = Σ_v coil·A[r][v]·z_rv^k  (signal_kernels.cuh:274-345)
+//
+// A block owns one readout, SP_THREADS·SP_KPT consecutive samples and CT coils; each thread
+// keeps SP_KPT samples × CT coils of accumulators. Voxels are staged SP_VCH at a time in shared
+// memory with everything that depends on the voxel only: A = ρ·rewind·prephaser·m, Θ_rv in
+// turns (FP64), the decay -Δt R2, the per-sample step z_rv = e^{-Δt R2 + iΘ_rv} and the coil
+// values. Per voxel a thread then forms its start factor z^{k0} (FP64-reduced phase) once and
+// advances it by z along its samples, so the work per staged voxel is CT·SP_KPT complex FMAs
+// plus SP_KPT complex products. Every (coil, sample) accumulates the voxels in the same order
+// whatever CT is, so the result does not depend on the coil grouping.
 constexpr int SP_THREADS = 128, SP_KPT = 8, SP_VCH = 64;
-
 
 // One block of the spiral signal: samples bx·SP_THREADS·SP_KPT.., readout r, coils cz·CT..
 // Shared by the one-operation kernel (blockIdx) and the batched kernel: bit-identical results.
 template<int CT>
 __device__ __forceinline__ void spiral_tile(const SpiralArgs& a, const int bx, const int r, const int cz) {
-    __shared__ float2 sA[SP_VCH];            // ρ·rewind·prephaser·m for this readout
-    __shared__ double sTheta[SP_VCH];        // Θ_rv
-    __shared__ float sDecay[SP_VCH];         // -Δt R2
+    __shared__ float2 sA[SP_VCH];
+    __shared__ double sTurns[SP_VCH];
+    __shared__ float sDecay[SP_VCH];
+    __shared__ float2 sStep[SP_VCH];
     __shared__ float2 sCoil[CT][SP_VCH];
     const int c0 = cz * CT;
     const int k0 = (bx * SP_THREADS + threadIdx.x) * SP_KPT;
-    const double twopi = 6.283185307179586476925;
+    const double twopi = 6.283185307179586476925, inv_2pi = 0.15915494309189533577;
     const float2 ks = a.k_start[r], dkr = a.delta_k[r];
     float2 acc[CT][SP_KPT];
 #pragma unroll
@@ -208,8 +217,8 @@ __device__ __forceinline__ void spiral_tile(const SpiralArgs& a, const int bx, c
     for (int v0 = 0; v0 < a.nvoxels; v0 += SP_VCH) {
         for (int i = threadIdx.x; i < SP_VCH; i += SP_THREADS) {
             const int v = v0 + i;
-            float2 A = make_float2(0.f, 0.f);
-            double th = 0.0;
+            float2 A = make_float2(0.f, 0.f), step = make_float2(0.f, 0.f);
+            double turns = 0.0;
             float dec = 0.0f;
             if (v < a.nvoxels) {
                 const float T2 = a.params[1 * a.pstride + v], B0 = a.params[3 * a.pstride + v];
@@ -221,12 +230,14 @@ __device__ __forceinline__ void spiral_tile(const SpiralArgs& a, const int bx, c
                 const float2 rw = cis_rad(-half * twopi * double(B0) + double(ks.x) * double(x));
                 const float mag = expf(float(half) * R2);
                 A = cmul(cmul(a.echo[int64_t(r) * a.nvoxels + v], cscale(mag, rw)), rho);
-                th = double(dkr.x) * x + double(dkr.y) * y + double(a.dt) * twopi * B0;
+                turns = (double(dkr.x) * x + double(dkr.y) * y + double(a.dt) * twopi * B0) * inv_2pi;
                 dec = -a.dt * R2;
+                step = cscale(__expf(dec), cis_turns(turns));
             }
             sA[i] = A;
-            sTheta[i] = th;
+            sTurns[i] = turns;
             sDecay[i] = dec;
+            sStep[i] = step;
 #pragma unroll
             for (int c = 0; c < CT; c++)
                 sCoil[c][i] = (v < a.nvoxels && c0 + c < a.C) ? a.coils[int64_t(c0 + c) * a.nvoxels + v]
@@ -234,20 +245,19 @@ __device__ __forceinline__ void spiral_tile(const SpiralArgs& a, const int bx, c
         }
         __syncthreads();
         if (k0 < a.S) {
-            for (int i = 0; i < SP_VCH; i++) {
-                const float2 A = sA[i];
-                const double th = sTheta[i];
-                const float dec = sDecay[i];
-                const float2 ph = cis_rad(double(k0) * th);
-                const float m0 = __expf(float(k0) * dec);
-                float2 e = cmul(A, make_float2(m0 * ph.x, m0 * ph.y));
-                const float2 st = cis_rad(th);
-                const float sm = __expf(dec);
-                const float2 step = make_float2(sm * st.x, sm * st.y);
+            const int nv = min(SP_VCH, a.nvoxels - v0);
+            for (int i = 0; i < nv; i++) {
+                const float2 ph = cis_turns(double(k0) * sTurns[i]);
+                const float m0 = __expf(float(k0) * sDecay[i]);
+                float2 e = cmul(sA[i], make_float2(m0 * ph.x, m0 * ph.y));
+                const float2 step = sStep[i];
+                float2 coil[CT];
+#pragma unroll
+                for (int c = 0; c < CT; c++) coil[c] = sCoil[c][i];
 #pragma unroll
                 for (int j = 0; j < SP_KPT; j++) {
 #pragma unroll
-                    for (int c = 0; c < CT; c++) acc[c][j] = cfma(sCoil[c][i], e, acc[c][j]);
+                    for (int c = 0; c < CT; c++) acc[c][j] = cfma(coil[c], e, acc[c][j]);
                     e = cmul(e, step);
                 }
             }
@@ -412,36 +422,48 @@ void launch_signal_spiral(const CompasContext& ctx, const float* params, int64_t
     a.delta_k = reinterpret_cast<const float2*>(delta_k);
     a.signal = reinterpret_cast<float2*>(signal);
     DeviceGuard guard(ctx.device());
-    const int kper = kernels::SP_THREADS * kernels::SP_KPT;
-    if (ncoils <= 1) {
-        dim3 grid(div_ceil(ns, kper), nreadouts, ncoils);
-        kernels::signal_spiral_kernel<1><<<grid, kernels::SP_THREADS, 0, ctx.stream()>>>(a);
-    } else {
-        dim3 grid(div_ceil(ns, kper), nreadouts, div_ceil(ncoils, 4));
-        kernels::signal_spiral_kernel<4><<<grid, kernels::SP_THREADS, 0, ctx.stream()>>>(a);
+    const int ct = spiral_coil_group(ncoils);
+    dim3 grid(div_ceil(ns, kernels::SP_THREADS * kernels::SP_KPT), nreadouts, div_ceil(ncoils, ct));
+    switch (ct) {
+        case 1: kernels::signal_spiral_kernel<1><<<grid, kernels::SP_THREADS, 0, ctx.stream()>>>(a); break;
+        case 2: kernels::signal_spiral_kernel<2><<<grid, kernels::SP_THREADS, 0, ctx.stream()>>>(a); break;
+        case 4: kernels::signal_spiral_kernel<4><<<grid, kernels::SP_THREADS, 0, ctx.stream()>>>(a); break;
+        default: kernels::signal_spiral_kernel<8><<<grid, kernels::SP_THREADS, 0, ctx.stream()>>>(a); break;
     }
     check_launch("signal_spiral_kernel");
 }
 
+// Coils per block for `ncoils` coils: minimises (blocks per readout) × (modelled instructions
+// per staged voxel and thread), where a block of CT coils costs 4·CT·8 FMAs for the products,
+// 8 complex steps and ~50 instructions for the start factor and shared-memory loads.
 int spiral_coil_group(int ncoils) {
-    return ncoils <= 1 ? 1 : 4;
+    int best = 1;
+    double best_cost = 1e300;
+    for (int ct : {1, 2, 4, 8}) {
+        const double cost = double(div_ceil(std::max(ncoils, 1), ct)) * (32.0 * ct + 48.0 + 50.0);
+        if (cost < best_cost - 1e-9) {
+            best_cost = cost;
+            best = ct;
+        }
+    }
+    return best;
 }
 
 int spiral_block_count(int ncoils, int nreadouts, int ns) {
     const int kper = kernels::SP_THREADS * kernels::SP_KPT;
-    const int ct = spiral_coil_group(ncoils);
-    return div_ceil(ns, kper) * nreadouts * div_ceil(ncoils, ct);
+    return div_ceil(ns, kper) * nreadouts * div_ceil(ncoils, spiral_coil_group(ncoils));
 }
 
 void launch_signal_spiral_batch(cudaStream_t stream, int device, int coil_group, const kernels::SpiralArgs* jobs,
                                 const int* cta_offsets, int njobs, int ctas) {
     if (njobs <= 0 || ctas <= 0) return;
     DeviceGuard guard(device);
-    if (coil_group == 1) {
-        kernels::signal_spiral_batch_kernel<1><<<ctas, kernels::SP_THREADS, 0, stream>>>(jobs, cta_offsets, njobs);
-    } else {
-        COMPAS_CHECK(coil_group == 4);
-        kernels::signal_spiral_batch_kernel<4><<<ctas, kernels::SP_THREADS, 0, stream>>>(jobs, cta_offsets, njobs);
+    switch (coil_group) {
+        case 1: kernels::signal_spiral_batch_kernel<1><<<ctas, kernels::SP_THREADS, 0, stream>>>(jobs, cta_offsets, njobs); break;
+        case 2: kernels::signal_spiral_batch_kernel<2><<<ctas, kernels::SP_THREADS, 0, stream>>>(jobs, cta_offsets, njobs); break;
+        case 4: kernels::signal_spiral_batch_kernel<4><<<ctas, kernels::SP_THREADS, 0, stream>>>(jobs, cta_offsets, njobs); break;
+        case 8: kernels::signal_spiral_batch_kernel<8><<<ctas, kernels::SP_THREADS, 0, stream>>>(jobs, cta_offsets, njobs); break;
+        default: COMPAS_ERROR("invalid spiral coil grouping");
     }
     check_launch("signal_spiral_batch_kernel");
 }
