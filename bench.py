@@ -197,6 +197,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-jacobian", action="store_true", help="skip the J·v / Jᴴ·v measurements")
+    ap.add_argument("--no-gn", action="store_true", help="skip the Gauss-Newton iteration timings")
     ap.add_argument("--batch-jobs", type=int, default=256,
                     help="jobs of the batched uneven workload (0 skips it)")
     ap.add_argument("--n-side", type=int, default=224,
@@ -314,6 +315,8 @@ def main():
         out["jacobian"] = jacobian_products(cb, ctx, stream, args, peaks, rank)
     if args.batch_jobs > 0:
         out["batched"] = batched(cb, ctx, stream, args, rank)
+    if not args.no_gn:
+        out["gauss_newton"] = gauss_newton(cb, ctx, stream, args, rank)
     if not args.no_e2e:
         out["e2e"] = e2e(cb, ctx, w, args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -377,6 +380,50 @@ def batched(cb, ctx, stream, args, rank):
             "note": "simulation: one persistent work-queue launch per kernel layout (FISP and pSSFP families on "
                     "two streams); signal: one batched launch per kind and family; results bit-identical to "
                     "the one-job calls"}
+
+
+def gauss_newton(cb, ctx, stream, args, rank):
+    """One Gauss-Newton iteration (3 FISP simulations, signal, residual, 4 CGLS steps of J·d and
+    Jᴴ·b, update) per step, replayed as a CUDA graph vs issued kernel by kernel, on the MR-STAT
+    slice (fit of data simulated from the true parameters, start perturbed) and on the 64x64 case."""
+    import numpy as np
+    import torch
+    import workloads
+
+    res = {}
+    for name, w in (("mrstat", workloads.mrstat(seed=2 + rank, n_side=args.n_side)),
+                    ("fisp_small", workloads.fisp_small(seed=1 + rank))):
+        rng = np.random.default_rng(5)
+        truth = w["params"]
+        start = truth.copy()
+        start[0] *= rng.uniform(0.9, 1.1, truth.shape[1])
+        start[1] *= rng.uniform(0.9, 1.1, truth.shape[1])
+        seq = cb.FispSequence.from_dict(ctx, w["seq"])
+        traj = cb.CartesianTrajectory.from_dict(ctx, w["traj"])
+        p_true = cb.TissueParameters.from_soa(ctx, truth)
+        y = cb.magnetization_to_signal(ctx, cb.simulate_magnetization(ctx, p_true, seq), p_true, traj, w["coils"])
+        gn = cb.GaussNewtonStep(ctx, cb.TissueParameters.from_soa(ctx, start), seq, traj, w["coils"], y)
+        times = {}
+        for mode in (False, True):
+            gn.run(graph=mode)  # warm-up (captures the graph)
+            ctx.synchronize()
+            reps = 3
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                gn.run(graph=mode)
+            e1.record(stream)
+            ctx.synchronize()
+            times["graph" if mode else "eager"] = e0.elapsed_time(e1) / reps
+        objs = []
+        for _ in range(2):
+            gn.run(graph=True)
+            objs.append(gn.objective())
+        V = truth.shape[1]
+        res[name] = {"voxels": V, "coils": int(w["coils"].shape[0]), "cg_iterations": 4,
+                     "ms_per_iteration_graph": times["graph"], "ms_per_iteration_eager": times["eager"],
+                     "kernels_per_iteration": gn.graph_kernels(), "objective_last_two": objs}
+    return res
 
 
 def jacobian_products(cb, ctx, stream, args, peaks, rank):

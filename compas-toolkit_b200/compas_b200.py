@@ -81,6 +81,10 @@ _SIGS = {
     "compas_b200_batch_run": ([_P], _I),
     "compas_b200_batch_echos": ([_P, _I], _P),
     "compas_b200_batch_signal": ([_P, _I], _P),
+    "compas_b200_make_gauss_newton": ([_P, _P, _P, _P, _P, _P, _I, _F, _I], _P),
+    "compas_b200_gauss_newton_run": ([_P, _I], _I),
+    "compas_b200_gauss_newton_array": ([_P, _I], _P),
+    "compas_b200_gauss_newton_graph_kernels": ([_P], _I),
 }
 
 _LIB = None
@@ -470,6 +474,48 @@ class SimulationBatch(_Object):
         ptr = library().compas_b200_batch_signal(self.ptr, int(job))
         shape = (coils.shape[0], traj.nreadouts, traj.samples_per_readout)
         return _result(ptr, self.context, shape, "compas_b200_batch_signal")
+
+
+class GaussNewtonStep(_Object):
+    """compas_b200_make_gauss_newton: one Gauss-Newton iteration on the device (simulate, FD
+    derivatives, signal, residual against `data`, `cg_iterations` CGLS steps of J·v / Jᴴ·v,
+    parameter update), captured as a CUDA graph on the first graph run."""
+
+    ARRAYS = {"parameters": 0, "echos": 1, "dT1": 2, "dT2": 3, "signal": 4, "gradient": 5, "step": 6,
+              "scalars": 7}
+
+    def __init__(self, context: Context, parameters: TissueParameters, sequence, trajectory, coils, data,
+                 cg_iterations: int = 4, delta: float = 1e-4, method: str = "GemmFast"):
+        c = _arr(context, coils, np.complex64)
+        d = _arr(context, data, np.complex64)
+        ptr = library().compas_b200_make_gauss_newton(context.ptr, parameters.ptr, sequence.ptr, trajectory.ptr,
+                                                      c.ptr, d.ptr, int(cg_iterations), float(delta),
+                                                      JACOBIAN_METHODS[method])
+        super().__init__(ptr, (parameters, sequence, trajectory, c, d))
+        self.context = context
+        self.nvoxels = parameters.nvoxels
+        self.shapes = {"parameters": (9, self.nvoxels), "echos": (sequence.nreadouts, self.nvoxels),
+                       "dT1": (sequence.nreadouts, self.nvoxels), "dT2": (sequence.nreadouts, self.nvoxels),
+                       "signal": tuple(d.shape), "gradient": (4, self.nvoxels), "step": (4, self.nvoxels),
+                       "scalars": (8,)}
+
+    def run(self, graph: bool = True):
+        """Enqueue one iteration on the context's stream."""
+        if library().compas_b200_gauss_newton_run(self.ptr, int(bool(graph))) != 0:
+            _check(None, "compas_b200_gauss_newton_run!")
+
+    def array(self, name: str) -> CompasArray:
+        ptr = library().compas_b200_gauss_newton_array(self.ptr, self.ARRAYS[name])
+        _check(ptr, "compas_b200_gauss_newton_array!")
+        real = name in ("parameters", "step", "scalars")
+        return CompasArray(self.context, ptr, np.float32 if real else np.complex64, self.shapes[name])
+
+    def objective(self) -> float:
+        """‖y - s(p)‖² of the last iteration, before its update (blocks)."""
+        return float(self.array("scalars").to_numpy()[0])
+
+    def graph_kernels(self) -> int:
+        return int(library().compas_b200_gauss_newton_graph_kernels(self.ptr))
 
 
 def launch_count() -> int:

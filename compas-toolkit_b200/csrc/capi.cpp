@@ -526,6 +526,54 @@ compas_array* compas_b200_batch_echos(const compas_object* batch, int job) {
     return guarded([&] { return new_array(compas::Array<cfloat, 2>(unwrap<compas::SimulationBatch>(batch).echos(job))); });
 }
 
+compas_object* compas_b200_make_gauss_newton(const compas_context* context, const compas_object* parameters,
+                                             const compas_object* sequence, const compas_object* trajectory,
+                                             const compas_array* coils, const compas_array* data, int cg_iterations,
+                                             float delta, int method) {
+    return guarded([&] {
+        const auto& ctx = ctx_of(context);
+        if (!sequence) throw compas::CompasException("null sequence");
+        const auto* seq = handle<compas::Object>(sequence);
+        std::variant<compas::FISPSequence, compas::pSSFPSequence> s;
+        if (const auto* f = dynamic_cast<const compas::FISPSequence*>(seq)) s = *f;
+        else if (const auto* p = dynamic_cast<const compas::pSSFPSequence*>(seq)) s = *p;
+        else throw compas::CompasException(std::string("invalid sequence object: ") + seq->name());
+        return new_obj(compas::GaussNewtonStep(ctx, unwrap<compas::TissueParameters>(parameters), s,
+                                               unwrap<compas::CartesianTrajectory>(trajectory),
+                                               array_of<cfloat, 2>(coils, "coils"), array_of<cfloat, 3>(data, "data"),
+                                               cg_iterations, delta, jacobian_method(method)));
+    });
+}
+
+int compas_b200_gauss_newton_run(const compas_object* gn, int use_graph) {
+    t_has_error = false;
+    guarded([&] { const_cast<compas::GaussNewtonStep&>(unwrap<compas::GaussNewtonStep>(gn)).run(use_graph != 0); });
+    return t_has_error ? -1 : 0;
+}
+
+compas_array* compas_b200_gauss_newton_array(const compas_object* gn, int which) {
+    return guarded([&]() -> compas_array* {
+        const auto& g = unwrap<compas::GaussNewtonStep>(gn);
+        switch (which) {
+            case 0: return new_array(compas::Array<float, 2>(g.parameters().data));
+            case 1: return new_array(compas::Array<cfloat, 2>(g.echos()));
+            case 2: return new_array(compas::Array<cfloat, 2>(g.derivative(compas::TissueParameterField::T1)));
+            case 3: return new_array(compas::Array<cfloat, 2>(g.derivative(compas::TissueParameterField::T2)));
+            case 4: return new_array(compas::Array<cfloat, 3>(g.signal()));
+            case 5: return new_array(compas::Array<cfloat, 2>(g.gradient()));
+            case 6: return new_array(compas::Array<float, 2>(g.step()));
+            case 7: return new_array(compas::Array<float>(g.scalars()));
+            default: throw compas::CompasException("invalid Gauss-Newton array index");
+        }
+    });
+}
+
+int compas_b200_gauss_newton_graph_kernels(const compas_object* gn) {
+    t_has_error = false;
+    const int n = guarded([&] { return unwrap<compas::GaussNewtonStep>(gn).kernels_per_iteration(); });
+    return t_has_error ? -1 : n;
+}
+
 compas_array* compas_b200_batch_signal(const compas_object* batch, int job) {
     // a job without trajectory yields an empty [0][0][0] array
     return guarded([&] { return new_array(compas::Array<cfloat, 3>(unwrap<compas::SimulationBatch>(batch).signal(job))); });

@@ -78,6 +78,7 @@ void launch_phase_encoding(const CompasContext& ctx, const cfloat* echos, const 
                            int nvoxels, int nreadouts, const cfloat* k_start, cfloat* out);
 void launch_residual(const CompasContext& ctx, const cfloat* lhs, const cfloat* rhs, int64_t n, cfloat* out,
                      float* partials, int npartials, float* objective);
+int residual_partial_count(int64_t n);  // partial sums launch_residual uses for n values
 
 // ---- tcgen05 tensor-core complex GEMM support ---------------------------------------------
 bool tensor_cores_available(int device);

@@ -469,4 +469,38 @@ class SimulationBatch: public Object {
     std::shared_ptr<Impl> m_impl;
 };
 
+// One Gauss–Newton iteration of MR-STAT parameter fitting, on the device and captured as a CUDA
+// graph on first use (no counterpart in the reference, whose callers chain the operations):
+// simulate m(p), finite-difference ∂m/∂T1 and ∂m/∂T2, s = signal(m), b = y - s, then
+// `cg_iterations` CGLS iterations (one J·d and one Jᴴ·b each) on min ‖J δ - b‖² over real δ in
+// the Jacobian's scaled coordinates (δT1/T1, δT2/T2, δRe ρ, δIm ρ), and the update
+// T1·c(δ0), T2·c(δ1), ρ + δ2 + iδ3 with c(x) = clamp(1 + x, ½, 2). The estimate is a private
+// copy of `parameters`; every buffer is allocated at construction.
+class GaussNewtonStep: public Object {
+  public:
+    GaussNewtonStep(const CompasContext& ctx, TissueParameters parameters,
+                    std::variant<FISPSequence, pSSFPSequence> sequence, CartesianTrajectory trajectory,
+                    Array<cfloat, 2> coil_sensitivities, Array<cfloat, 3> data, int cg_iterations = 4,
+                    float delta = DEFAULT_FINITE_DIFFERENCE_DELTA,
+                    JacobianComputeMethod method = JacobianComputeMethod::GemmFast);
+    // enqueue one iteration on the context's stream: a replay of the captured graph (captured
+    // on the first call), or the kernels one by one
+    void run(bool use_graph = true);
+    const TissueParameters& parameters() const;       // current estimate
+    const Array<cfloat, 2>& echos() const;            // m(p) of the last iteration
+    const Array<cfloat, 2>& derivative(int field) const;  // ∂m/∂T1 or ∂m/∂T2
+    const Array<cfloat, 3>& signal() const;           // s(p)
+    const Array<cfloat, 2>& gradient() const;         // Jᴴ·b of the last CG iteration [4][V]
+    const Array<float, 2>& step() const;              // δ [4][V]
+    // device scalars: [0] ‖y - s(p)‖² before the update, [1] γ, [2] γ', [3] ‖q‖², [4] α, [5] β
+    const Array<float>& scalars() const;
+    int kernels_per_iteration() const;  // kernel nodes of the captured graph (-1 before capture)
+    const char* name() const override { return "compas::GaussNewtonStep"; }
+
+    struct Impl;
+
+  private:
+    std::shared_ptr<Impl> m_impl;
+};
+
 }  // namespace compas

@@ -198,6 +198,26 @@ COMPAS_API int compas_b200_batch_run(const compas_object* batch);
 COMPAS_API compas_array* compas_b200_batch_echos(const compas_object* batch, int job);
 COMPAS_API compas_array* compas_b200_batch_signal(const compas_object* batch, int job);
 
+/* One Gauss-Newton iteration of parameter fitting on the device (no counterpart in the
+ * reference): simulate, finite-difference dm/dT1 and dm/dT2, signal, residual against `data`
+ * ([ncoils][nreadouts][ns] complex), `cg_iterations` CGLS steps of J.v / J^H.v, parameter update.
+ * Captured as a CUDA graph on the first graph run. `method` is a JacobianComputeMethod value.
+ * The estimate starts as a copy of `parameters`. Released with compas_destroy_object. */
+COMPAS_API compas_object* compas_b200_make_gauss_newton(const compas_context* ctx, const compas_object* parameters,
+                                                        const compas_object* sequence,
+                                                        const compas_object* trajectory, const compas_array* coils,
+                                                        const compas_array* data, int cg_iterations, float delta,
+                                                        int method);
+/* Enqueue one iteration (graph replay when use_graph != 0); 0 on success, -1 on error. */
+COMPAS_API int compas_b200_gauss_newton_run(const compas_object* gn, int use_graph);
+/* New array handle sharing the iteration's device storage: 0 parameters [9][nvoxels] float,
+ * 1 echoes, 2 dm/dT1, 3 dm/dT2 ([nreadouts][nvoxels] complex), 4 signal [ncoils][nreadouts][ns],
+ * 5 J^H.b [4][nvoxels] complex, 6 step [4][nvoxels] float, 7 scalars [8] float
+ * (objective before the update, gamma, gamma', |q|^2, alpha, beta). */
+COMPAS_API compas_array* compas_b200_gauss_newton_array(const compas_object* gn, int which);
+/* Kernel nodes of the captured graph, -1 before the first graph run. */
+COMPAS_API int compas_b200_gauss_newton_graph_kernels(const compas_object* gn);
+
 #ifdef __cplusplus
 }
 #endif
