@@ -85,6 +85,14 @@ _SIGS = {
     "compas_b200_gauss_newton_run": ([_P, _I], _I),
     "compas_b200_gauss_newton_array": ([_P, _I], _P),
     "compas_b200_gauss_newton_graph_kernels": ([_P], _I),
+    "compas_b200_make_server": ([_P, C.c_double, _I, _I, C.c_double, _I, _F], _P),
+    "compas_b200_server_submit": ([_P, _P, _P, _P, _P, _P, C.c_uint64], _I64),
+    "compas_b200_server_wait": ([_P, _I64, C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int)], _I),
+    "compas_b200_server_result": ([_P, _I64, _I], _P),
+    "compas_b200_server_release": ([_P, _I64], _I),
+    "compas_b200_server_drain": ([_P], _I),
+    "compas_b200_server_stats": ([_P, C.POINTER(C.c_double), _I], _I),
+    "compas_b200_server_reset_stats": ([_P], None),
 }
 
 _LIB = None
@@ -516,6 +524,75 @@ class GaussNewtonStep(_Object):
 
     def graph_kernels(self) -> int:
         return int(library().compas_b200_gauss_newton_graph_kernels(self.ptr))
+
+
+class ServeEngine(_Object):
+    """compas_b200_make_server: continuous-batching request loop on one GPU.
+
+    submit() queues a reconstruction request (simulate -> signal -> residual against `data`, and
+    for Cartesian trajectories the gradient Jᴴ·r) and returns a ticket; wait() blocks for it.
+    Requests are admitted by estimated device footprint against the memory budget, run in
+    batches (persistent work-queue simulations, batched signals) on up to
+    `max_inflight_batches` streams at once, and give the same bits as the one-request calls."""
+
+    STATS = ("completed", "failed", "batches", "echo_cache_hits", "p50_ms", "p99_ms", "mean_ms", "max_ms",
+             "peak_bytes", "max_concurrent_batches")
+
+    def __init__(self, context: Context, memory_budget_gb: float = 150.0, max_inflight_batches: int = 4,
+                 max_batch_requests: int = 16, echo_cache_gb: float = 16.0, method: str = "MatmulFast",
+                 delta: float = 1e-4):
+        ptr = library().compas_b200_make_server(context.ptr, float(memory_budget_gb), int(max_inflight_batches),
+                                                int(max_batch_requests), float(echo_cache_gb),
+                                                SIGNAL_METHODS[method], float(delta))
+        super().__init__(ptr)
+        self.context = context
+        self._meta = {}
+
+    def submit(self, parameters: TissueParameters, sequence, trajectory, coils, data, echo_key: int = 0) -> int:
+        c = _arr(self.context, coils, np.complex64)
+        d = _arr(self.context, data, np.complex64)
+        t = library().compas_b200_server_submit(self.ptr, parameters.ptr, sequence.ptr, trajectory.ptr, c.ptr, d.ptr,
+                                                int(echo_key))
+        if t < 0:
+            _check(None, "compas_b200_server_submit!")
+        self._meta[t] = (tuple(d.shape), parameters.nvoxels, isinstance(trajectory, CartesianTrajectory))
+        return int(t)
+
+    def wait(self, ticket: int) -> dict:
+        obj = C.c_float()
+        times = (C.c_double * 3)()
+        batch = C.c_int()
+        if library().compas_b200_server_wait(self.ptr, int(ticket), C.byref(obj), times, C.byref(batch)) != 0:
+            _check(None, "compas_b200_server_wait!")
+        return {"objective": obj.value, "queued_ms": times[0], "device_ms": times[1], "latency_ms": times[2],
+                "batch": batch.value}
+
+    def result(self, ticket: int, which: str = "residual") -> CompasArray:
+        shape, nv, cart = self._meta[int(ticket)]
+        idx = {"residual": 0, "gradient": 1}[which]
+        if idx == 1 and not cart:
+            raise CompasError("spiral requests have no gradient")
+        ptr = library().compas_b200_server_result(self.ptr, int(ticket), idx)
+        return _result(ptr, self.context, shape if idx == 0 else (4, nv), "compas_b200_server_result")
+
+    def release(self, ticket: int):
+        self._meta.pop(int(ticket), None)
+        if library().compas_b200_server_release(self.ptr, int(ticket)) != 0:
+            _check(None, "compas_b200_server_release!")
+
+    def drain(self):
+        if library().compas_b200_server_drain(self.ptr) != 0:
+            _check(None, "compas_b200_server_drain!")
+
+    def stats(self) -> dict:
+        out = (C.c_double * len(self.STATS))()
+        n = library().compas_b200_server_stats(self.ptr, out, len(self.STATS))
+        if n < 0:
+            _check(None, "compas_b200_server_stats!")
+        return {k: out[i] for i, k in enumerate(self.STATS[:n])}
+
+    def reset_stats(self):
+        library().compas_b200_server_reset_stats(self.ptr)
 
 
 def launch_count() -> int:

@@ -33,7 +33,7 @@ namespace {
 
 template<typename T>
 Array<unsigned char> upload_table(const CompasContext& ctx, const std::vector<T>& v) {
-    Array<unsigned char> out({int64_t(v.size() * sizeof(T))}, ctx.device());
+    Array<unsigned char> out({int64_t(v.size() * sizeof(T))}, ctx.device(), ctx.stream());
     if (!v.empty()) {
         DeviceGuard guard(ctx.device());
         COMPAS_CUDA_CHECK(cudaMemcpyAsync(out.data(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice,
@@ -251,15 +251,15 @@ void SimulationBatch::Impl::plan_signal(Family& fam, const std::vector<int>& mem
                                                cartesian_geom(t));
             a.vchunk = e.plan.vchunk;
             a.status = detail::device_status_word(dev);
-            Array<unsigned char> vgen({int64_t(V) * int64_t(sizeof(kernels::VoxelGen))}, dev);
-            Array<unsigned char> coilw({int64_t(C) * V * int64_t(sizeof(float2))}, dev);
+            Array<unsigned char> vgen({int64_t(V) * int64_t(sizeof(kernels::VoxelGen))}, dev, ctx.stream());
+            Array<unsigned char> coilw({int64_t(C) * V * int64_t(sizeof(float2))}, dev, ctx.stream());
             a.vgen = reinterpret_cast<const kernels::VoxelGen*>(vgen.data());
             a.coilw = reinterpret_cast<const float2*>(coilw.data());
             a.jcoef = nullptr;
             const int64_t n = int64_t(C) * t.nreadouts * t.samples_per_readout;
             float2* out = reinterpret_cast<float2*>(signals[size_t(e.job)].data());
             if (e.plan.splits > 1) {
-                Array<unsigned char> partials({int64_t(e.plan.splits) * n * int64_t(sizeof(float2))}, dev);
+                Array<unsigned char> partials({int64_t(e.plan.splits) * n * int64_t(sizeof(float2))}, dev, ctx.stream());
                 a.out = reinterpret_cast<float2*>(partials.data());
                 sums.push_back({a.out, out, n, e.plan.splits});
                 sum_counts.push_back((n + 255) / 256);
@@ -370,7 +370,7 @@ SimulationBatch::SimulationBatch(const CompasContext& ctx, std::vector<Simulatio
         } else {
             nreadouts = int(std::get<pSSFPSequence>(job.sequence).RF_train.size());
         }
-        im.echos.emplace_back(std::array<int64_t, 2> {nreadouts, V}, dev);
+        im.echos.emplace_back(std::array<int64_t, 2> {nreadouts, V}, dev, ctx.stream());
         if (std::holds_alternative<std::monostate>(job.trajectory)) {
             im.signals.emplace_back();
         } else {
@@ -382,7 +382,7 @@ SimulationBatch::SimulationBatch(const CompasContext& ctx, std::vector<Simulatio
             COMPAS_CHECK(job.coil_sensitivities.size(1) == V);
             if (const auto* sp = std::get_if<SpiralTrajectory>(&job.trajectory))
                 COMPAS_CHECK(sp->k_start.size() == t.nreadouts && sp->delta_k.size() == t.nreadouts);
-            im.signals.emplace_back(std::array<int64_t, 3> {C, t.nreadouts, t.samples_per_readout}, dev);
+            im.signals.emplace_back(std::array<int64_t, 3> {C, t.nreadouts, t.samples_per_readout}, dev, ctx.stream());
         }
         members[fisp ? 0 : 1].push_back(int(j));
     }
@@ -393,7 +393,7 @@ SimulationBatch::SimulationBatch(const CompasContext& ctx, std::vector<Simulatio
     int nheads = 0;
     for (auto& fam : im.families)
         for (auto& g : fam.sims) g.head = nheads++;
-    im.heads = Array<int>({std::max(1, nheads)}, dev);
+    im.heads = Array<int>({std::max(1, nheads)}, dev, ctx.stream());
     COMPAS_CUDA_CHECK(cudaStreamCreateWithFlags(&im.side, cudaStreamNonBlocking));
     COMPAS_CUDA_CHECK(cudaEventCreateWithFlags(&im.fork, cudaEventDisableTiming));
     COMPAS_CUDA_CHECK(cudaEventCreateWithFlags(&im.join, cudaEventDisableTiming));

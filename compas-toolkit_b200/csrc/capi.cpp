@@ -568,6 +568,107 @@ compas_array* compas_b200_gauss_newton_array(const compas_object* gn, int which)
     });
 }
 
+namespace {
+compas::ServeEngine& server_of(const compas_object* server) {
+    return const_cast<compas::ServeEngine&>(unwrap<compas::ServeEngine>(server));
+}
+}  // namespace
+
+compas_object* compas_b200_make_server(const compas_context* context, double memory_budget_gb,
+                                       int max_inflight_batches, int max_batch_requests, double echo_cache_gb,
+                                       int method, float delta) {
+    return guarded([&] {
+        if (!(memory_budget_gb > 0) || echo_cache_gb < 0) throw compas::CompasException("invalid memory budget");
+        compas::ServeOptions o;
+        o.memory_budget_bytes = size_t(memory_budget_gb * double(size_t(1) << 30));
+        o.max_inflight_batches = max_inflight_batches;
+        o.max_batch_requests = max_batch_requests;
+        o.echo_cache_bytes = size_t(echo_cache_gb * double(size_t(1) << 30));
+        o.method = signal_method(method);
+        o.delta = delta;
+        return new_obj(compas::ServeEngine(ctx_of(context), o));
+    });
+}
+
+int64_t compas_b200_server_submit(const compas_object* server, const compas_object* parameters,
+                                  const compas_object* sequence, const compas_object* trajectory,
+                                  const compas_array* coils, const compas_array* data, uint64_t echo_key) {
+    t_has_error = false;
+    const int64_t id = guarded([&]() -> int64_t {
+        compas::ServeRequest r;
+        r.parameters = unwrap<compas::TissueParameters>(parameters);
+        if (!sequence) throw compas::CompasException("null sequence");
+        const auto* seq = handle<compas::Object>(sequence);
+        if (const auto* f = dynamic_cast<const compas::FISPSequence*>(seq)) r.sequence = *f;
+        else if (const auto* p = dynamic_cast<const compas::pSSFPSequence*>(seq)) r.sequence = *p;
+        else throw compas::CompasException(std::string("invalid sequence object: ") + seq->name());
+        if (!trajectory) throw compas::CompasException("null trajectory");
+        const auto* t = handle<compas::Object>(trajectory);
+        if (const auto* c = dynamic_cast<const compas::CartesianTrajectory*>(t)) r.trajectory = *c;
+        else if (const auto* sp = dynamic_cast<const compas::SpiralTrajectory*>(t)) r.trajectory = *sp;
+        else throw compas::CompasException(std::string("invalid trajectory object: ") + t->name());
+        r.coil_sensitivities = array_of<cfloat, 2>(coils, "coils");
+        r.data = array_of<cfloat, 3>(data, "data");
+        r.echo_key = echo_key;
+        return int64_t(server_of(server).submit(std::move(r)));
+    });
+    return t_has_error ? -1 : id;
+}
+
+int compas_b200_server_wait(const compas_object* server, int64_t ticket, float* objective, double* times, int* batch) {
+    t_has_error = false;
+    guarded([&] {
+        const compas::ServeResult r = server_of(server).wait(uint64_t(ticket));
+        if (objective) *objective = r.objective;
+        if (times) {
+            times[0] = r.queued_ms;
+            times[1] = r.device_ms;
+            times[2] = r.latency_ms;
+        }
+        if (batch) *batch = r.batch;
+    });
+    return t_has_error ? -1 : 0;
+}
+
+compas_array* compas_b200_server_result(const compas_object* server, int64_t ticket, int which) {
+    return guarded([&]() -> compas_array* {
+        const compas::ServeResult r = server_of(server).wait(uint64_t(ticket));
+        if (which == 0) return new_array(compas::Array<cfloat, 3>(r.residual));
+        if (which == 1) return new_array(compas::Array<cfloat, 2>(r.gradient));
+        throw compas::CompasException("invalid result index");
+    });
+}
+
+int compas_b200_server_release(const compas_object* server, int64_t ticket) {
+    t_has_error = false;
+    guarded([&] { server_of(server).release(uint64_t(ticket)); });
+    return t_has_error ? -1 : 0;
+}
+
+int compas_b200_server_drain(const compas_object* server) {
+    t_has_error = false;
+    guarded([&] { server_of(server).drain(); });
+    return t_has_error ? -1 : 0;
+}
+
+int compas_b200_server_stats(const compas_object* server, double* out, int n) {
+    t_has_error = false;
+    const int written = guarded([&] {
+        const compas::ServeStats s = server_of(server).stats();
+        const double v[10] = {double(s.completed), double(s.failed), double(s.batches), double(s.echo_cache_hits),
+                              s.p50_ms, s.p99_ms, s.mean_ms, s.max_ms, double(s.peak_bytes),
+                              double(s.max_concurrent_batches)};
+        int k = 0;
+        for (; k < n && k < 10; k++) out[k] = v[k];
+        return k;
+    });
+    return t_has_error ? -1 : written;
+}
+
+void compas_b200_server_reset_stats(const compas_object* server) {
+    guarded([&] { server_of(server).reset_stats(); });
+}
+
 int compas_b200_gauss_newton_graph_kernels(const compas_object* gn) {
     t_has_error = false;
     const int n = guarded([&] { return unwrap<compas::GaussNewtonStep>(gn).kernels_per_iteration(); });

@@ -433,7 +433,7 @@ const Array<float, 3>& fisp_excite_table(const CompasContext& ctx, const FISPSeq
         int nTR = int(seq.RF_train.size());
         int P = int(seq.sliceprofiles.size(0));
         COMPAS_CHECK(int(seq.sliceprofiles.size(1)) == nTR);
-        auto tab = std::make_shared<Array<float, 3>>(std::array<int64_t, 3> {P, nTR, 4}, ctx.device());
+        auto tab = std::make_shared<Array<float, 3>>(std::array<int64_t, 3> {P, nTR, 4}, ctx.device(), ctx.stream());
         DeviceGuard guard(ctx.device());
         int n = nTR * P;
         if (n > 0) {
@@ -551,7 +551,7 @@ Array<cfloat, 2> simulate_magnetization(const CompasContext& context, TissuePara
     const int nreadouts = nTR * sequence.undersampling_factor;
     const int nvoxels = parameters.nvoxels;
     COMPAS_CHECK(sequence.undersampling_factor >= 1);
-    Array<cfloat, 2> echos({nreadouts, nvoxels}, context.device());
+    Array<cfloat, 2> echos({nreadouts, nvoxels}, context.device(), context.stream());
     launch_fisp(context, parameters, 0, nvoxels, sequence, echos.data(), nvoxels, tuned_fisp_launch(sequence.max_state, nvoxels, int(sequence.sliceprofiles.size(0))));
     return echos;
 }

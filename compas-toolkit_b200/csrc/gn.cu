@@ -275,13 +275,13 @@ GaussNewtonStep::GaussNewtonStep(const CompasContext& ctx, TissueParameters para
     COMPAS_CHECK(V > 0);
 
     // the estimate is a private copy of the parameters (updated in place by every iteration)
-    Array<float, 2> own({TissueParameterField::NUM_FIELDS, V}, dev);
+    Array<float, 2> own({TissueParameterField::NUM_FIELDS, V}, dev, ctx.stream());
     DeviceGuard guard(dev);
     COMPAS_CUDA_CHECK(cudaMemcpy2DAsync(own.data(), size_t(V) * sizeof(float), parameters.data.data(),
                                         size_t(parameters.data.size(1)) * sizeof(float), size_t(V) * sizeof(float),
                                         TissueParameterField::NUM_FIELDS, cudaMemcpyDeviceToDevice, ctx.stream()));
     im.params = TissueParameters(own, parameters.has_z, parameters.has_b0, parameters.has_b1);
-    im.perturbed = Array<float, 2>({TissueParameterField::NUM_FIELDS, V}, dev);
+    im.perturbed = Array<float, 2>({TissueParameterField::NUM_FIELDS, V}, dev, ctx.stream());
     im.sequence = std::move(sequence);
     im.trajectory = std::move(trajectory);
     im.coils = std::move(coil_sensitivities);
@@ -291,18 +291,18 @@ GaussNewtonStep::GaussNewtonStep(const CompasContext& ctx, TissueParameters para
     im.prec = (method == JacobianComputeMethod::GemmFast || method == JacobianComputeMethod::GemmLow)
                   ? Precision::SplitBF16
                   : Precision::FP32;
-    im.echos = Array<cfloat, 2>({R, V}, dev);
-    im.dT1 = Array<cfloat, 2>({R, V}, dev);
-    im.dT2 = Array<cfloat, 2>({R, V}, dev);
-    im.signal = Array<cfloat, 3>({C, R, S}, dev);
-    im.b = Array<cfloat, 3>({C, R, S}, dev);
-    im.q = Array<cfloat, 3>({C, R, S}, dev);
-    im.g = Array<cfloat, 2>({4, V}, dev);
-    im.d = Array<cfloat, 2>({4, V}, dev);
-    im.x = Array<float, 2>({4, V}, dev);
-    im.scalars = Array<float>({kernels::kNumScalars}, dev);
+    im.echos = Array<cfloat, 2>({R, V}, dev, ctx.stream());
+    im.dT1 = Array<cfloat, 2>({R, V}, dev, ctx.stream());
+    im.dT2 = Array<cfloat, 2>({R, V}, dev, ctx.stream());
+    im.signal = Array<cfloat, 3>({C, R, S}, dev, ctx.stream());
+    im.b = Array<cfloat, 3>({C, R, S}, dev, ctx.stream());
+    im.q = Array<cfloat, 3>({C, R, S}, dev, ctx.stream());
+    im.g = Array<cfloat, 2>({4, V}, dev, ctx.stream());
+    im.d = Array<cfloat, 2>({4, V}, dev, ctx.stream());
+    im.x = Array<float, 2>({4, V}, dev, ctx.stream());
+    im.scalars = Array<float>({kernels::kNumScalars}, dev, ctx.stream());
     im.npartials = residual_partial_count(im.signal.numel());
-    im.partials = Array<float>({std::max(im.npartials, kernels::kRedBlocks)}, dev);
+    im.partials = Array<float>({std::max(im.npartials, kernels::kRedBlocks)}, dev, ctx.stream());
     COMPAS_CUDA_CHECK(cudaMemsetAsync(im.scalars.data(), 0, im.scalars.nbytes(), ctx.stream()));
     // build the sequence's device table now, so that no capture ever contains its construction
     if (const auto* f = std::get_if<FISPSequence>(&im.sequence)) (void)fisp_excite_table(ctx, *f);

@@ -123,7 +123,7 @@ Array<cfloat, 2> phase_encoding(const CompasContext& ctx, const Array<cfloat, 2>
     const int nreadouts = trajectory.nreadouts, nvoxels = parameters.nvoxels;
     COMPAS_CHECK(echos.size(0) == nreadouts && echos.size(1) == nvoxels);
     COMPAS_CHECK(trajectory.k_start.size() == nreadouts);
-    Array<cfloat, 2> out({nreadouts, nvoxels}, ctx.device());
+    Array<cfloat, 2> out({nreadouts, nvoxels}, ctx.device(), ctx.stream());
     launch_phase_encoding(ctx, echos.data(), parameters.data.data(), parameters.data.size(1), nvoxels, nreadouts,
                           trajectory.k_start.data(), out.data());
     return out;
@@ -149,8 +149,8 @@ Array<cfloat, 3> compute_residual(CompasContext ctx, Array<cfloat, 3> lhs, Array
     const int64_t n = lhs.numel();
     Array<cfloat, 3> out(lhs.sizes(), ctx.device());
     const int np = residual_partial_count(n);
-    Array<float> partials({np}, ctx.device());
-    Array<float> objective({1}, ctx.device());
+    Array<float> partials({np}, ctx.device(), ctx.stream());
+    Array<float> objective({1}, ctx.device(), ctx.stream());
     launch_residual(ctx, lhs.data(), rhs.data(), n, out.data(), partials.data(), np, objective.data());
     if (objective_out != nullptr) objective.copy_to(objective_out);
     return out;
@@ -164,7 +164,7 @@ Array<cfloat, 2> derivative_impl(const CompasContext& ctx, int field, Array<cflo
     COMPAS_CHECK(echos.size(1) == nvoxels);
     COMPAS_CHECK(field >= 0 && field < TissueParameterField::NUM_FIELDS);
     COMPAS_CHECK(delta != 0.0f);
-    Array<float, 2> data({TissueParameterField::NUM_FIELDS, nvoxels}, ctx.device());
+    Array<float, 2> data({TissueParameterField::NUM_FIELDS, nvoxels}, ctx.device(), ctx.stream());
     DeviceGuard guard(ctx.device());
     if (nvoxels > 0) {
         kernels::add_difference_kernel<<<div_ceil(nvoxels, 256), 256, 0, ctx.stream()>>>(
@@ -261,7 +261,7 @@ Array<cfloat, 3> magnetization_to_signal(const CompasContext& context, Array<cfl
     COMPAS_CHECK(nreadouts >= 0 && ns >= 0);
     COMPAS_CHECK(coil_sensitivities.size(1) == nvoxels);
     COMPAS_CHECK(echos.size(0) == nreadouts && echos.size(1) == nvoxels);
-    Array<cfloat, 3> signal({ncoils, nreadouts, ns}, context.device());
+    Array<cfloat, 3> signal({ncoils, nreadouts, ns}, context.device(), context.stream());
     if (const auto* cart = dynamic_cast<const CartesianTrajectory*>(&trajectory)) {
         launch_signal_cartesian(context, parameters.data.data(), parameters.data.size(1), nvoxels, echos.data(),
                                 coil_sensitivities.data(), ncoils, cartesian_geom(*cart), signal.data(),
@@ -294,7 +294,7 @@ Array<cfloat, 3> compute_jacobian(const CompasContext& ctx, Array<cfloat, 2> ech
     const int nvoxels = parameters.nvoxels, ncoils = int(coil_sensitivities.size(0));
     check_jacobian_shapes(nreadouts, nvoxels, echos, delta_echos_T1, delta_echos_T2, coil_sensitivities);
     COMPAS_CHECK(vector.size(0) == 4 && vector.size(1) == nvoxels);  // product.cu:304-313
-    Array<cfloat, 3> Jv({ncoils, nreadouts, ns}, ctx.device());
+    Array<cfloat, 3> Jv({ncoils, nreadouts, ns}, ctx.device(), ctx.stream());
     launch_jacobian(ctx, parameters.data.data(), parameters.data.size(1), nvoxels, echos.data(), delta_echos_T1.data(),
                     delta_echos_T2.data(), coil_sensitivities.data(), ncoils, vector.data(), cartesian_geom(trajectory),
                     Jv.data(), jacobian_precision(kind));
@@ -310,7 +310,7 @@ Array<cfloat, 2> compute_jacobian_hermitian(const CompasContext& ctx, Array<cflo
     const int nvoxels = parameters.nvoxels, ncoils = int(coil_sensitivities.size(0));
     check_jacobian_shapes(nreadouts, nvoxels, echos, delta_echos_T1, delta_echos_T2, coil_sensitivities);
     COMPAS_CHECK(vector.size(0) == ncoils && vector.size(1) == nreadouts && vector.size(2) == ns);  // hermitian.cu:265-275
-    Array<cfloat, 2> JHv({4, nvoxels}, ctx.device());
+    Array<cfloat, 2> JHv({4, nvoxels}, ctx.device(), ctx.stream());
     launch_jacobian_hermitian(ctx, parameters.data.data(), parameters.data.size(1), nvoxels, echos.data(),
                               delta_echos_T1.data(), delta_echos_T2.data(), coil_sensitivities.data(), ncoils,
                               vector.data(), cartesian_geom(trajectory), JHv.data(), jacobian_precision(kind));

@@ -262,7 +262,7 @@ kernels::PssfpArgs pssfp_args(const CompasContext& ctx, const TissueParameters& 
         auto& cache = *seq.cache;
         std::lock_guard<std::mutex> lock(cache.mutex);
         if (!cache.table || cache.key_rf != seq.RF_train.data() || cache.key_g != seq.gamma_dt_RF.data()) {
-            auto tab = std::make_shared<Array<cfloat, 2>>(std::array<int64_t, 2> {nTR + 1, nRF}, ctx.device());
+            auto tab = std::make_shared<Array<cfloat, 2>>(std::array<int64_t, 2> {nTR + 1, nRF}, ctx.device(), ctx.stream());
             int n = (nTR + 1) * nRF;
             if (n > 0) {
                 kernels::pssfp_table_kernel<<<div_ceil(n, 256), 256, 0, ctx.stream()>>>(
@@ -341,7 +341,7 @@ void launch_pssfp_queue(cudaStream_t stream, int device, PssfpLaunch L, int nz, 
 Array<cfloat, 2> simulate_magnetization(const CompasContext& context, TissueParameters parameters,
                                         pSSFPSequence sequence) {
     const int nTR = int(sequence.RF_train.size());
-    Array<cfloat, 2> echos({nTR, parameters.nvoxels}, context.device());
+    Array<cfloat, 2> echos({nTR, parameters.nvoxels}, context.device(), context.stream());
     launch_pssfp(context, parameters, 0, parameters.nvoxels, sequence, echos.data(), parameters.nvoxels,
                  tuned_pssfp_launch(int(sequence.z.size()), parameters.nvoxels));
     return echos;

@@ -113,10 +113,10 @@ void ArrayBase::copy_bytes_to(void* dst, size_t n) const {
     if (n > nbytes()) COMPAS_ERROR("read of more bytes than the array holds");
     if (n == 0) return;
     DeviceGuard guard(device());
-    cudaStream_t s = detail::device_stream(device());
+    cudaStream_t s = stream();
     COMPAS_CUDA_CHECK(cudaMemcpyAsync(dst, raw_data(), n, cudaMemcpyDeviceToHost, s));
     COMPAS_CUDA_CHECK(cudaStreamSynchronize(s));
-    CompasContext(device()).check_device_status();
+    CompasContext(device(), s).check_device_status();
 }
 
 CompasContext::CompasContext(int device) : m_device(device), m_stream(detail::device_stream(device)) {}
@@ -168,7 +168,7 @@ TissueParameters make_tissue_parameters(const CompasContext& ctx, int num_voxels
     COMPAS_CHECK(num_voxels >= 0);
     using F = int;
     namespace TF = TissueParameterField;
-    Array<float, 2> params({TF::NUM_FIELDS, num_voxels}, ctx.device());
+    Array<float, 2> params({TF::NUM_FIELDS, num_voxels}, ctx.device(), ctx.stream());
     DeviceGuard guard(ctx.device());
     cudaStream_t s = ctx.stream();
     size_t row = size_t(num_voxels) * sizeof(float);

@@ -345,7 +345,7 @@ void run_signal_gemm(const CompasContext& ctx, kernels::SignalArgs a, cfloat* ou
     a.vchunk = div_ceil(div_ceil(a.nvoxels, splits), kernels::SG_VT) * kernels::SG_VT;
     splits = div_ceil(a.nvoxels, a.vchunk);
     const int64_t n = int64_t(a.C) * a.R * a.S;
-    Array<cfloat, 2> partials({splits > 1 ? splits : 0, n}, ctx.device());
+    Array<cfloat, 2> partials({splits > 1 ? splits : 0, n}, ctx.device(), ctx.stream());
     a.out = reinterpret_cast<float2*>(splits > 1 ? partials.data() : out);
     dim3 grid(ktiles, rtiles, a.C * splits);
     kernels::signal_gemm_kernel<MODE><<<grid, kernels::SG_THREADS, 0, ctx.stream()>>>(a);

@@ -476,11 +476,11 @@ bool run_tc(const CompasContext& ctx, kernels::TcArgs a, bool jac, cfloat* out) 
     int splits = plan.splits;
     a.vchunk = plan.vchunk;
     const int64_t n = int64_t(npairs) * a.R;
-    Array<cfloat, 2> partials({splits > 1 ? splits : 0, n}, ctx.device());
+    Array<cfloat, 2> partials({splits > 1 ? splits : 0, n}, ctx.device(), ctx.stream());
     // per-voxel tables: 24 B generation constants, C coil·w values, J·v coefficients
-    Array<float, 2> vgen({a.nvoxels, int64_t(sizeof(kernels::VoxelGen) / sizeof(float))}, ctx.device());
-    Array<cfloat, 2> coilw({a.C, a.nvoxels}, ctx.device());
-    Array<float, 2> jcoef({jac ? a.nvoxels : 0, 8}, ctx.device());
+    Array<float, 2> vgen({a.nvoxels, int64_t(sizeof(kernels::VoxelGen) / sizeof(float))}, ctx.device(), ctx.stream());
+    Array<cfloat, 2> coilw({a.C, a.nvoxels}, ctx.device(), ctx.stream());
+    Array<float, 2> jcoef({jac ? a.nvoxels : 0, 8}, ctx.device(), ctx.stream());
     a.vgen = reinterpret_cast<const kernels::VoxelGen*>(vgen.data());
     a.coilw = reinterpret_cast<const float2*>(coilw.data());
     a.jcoef = reinterpret_cast<const float4*>(jcoef.data());

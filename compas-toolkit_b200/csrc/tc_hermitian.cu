@@ -374,7 +374,7 @@ bool launch_jacobian_hermitian_tc(const CompasContext& ctx, const float* params,
     a.tiles_per_split = div_ceil(ptiles, splits);
     splits = div_ceil(ptiles, a.tiles_per_split);
     const int64_t n = 4 * int64_t(nvoxels);
-    Array<cfloat, 2> partials({splits > 1 ? splits : 0, n}, ctx.device());
+    Array<cfloat, 2> partials({splits > 1 ? splits : 0, n}, ctx.device(), ctx.stream());
     a.out = reinterpret_cast<float2*>(splits > 1 ? partials.data() : JHv);
     static bool attr_set = false;
     if (!attr_set) {

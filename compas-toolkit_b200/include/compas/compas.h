@@ -109,6 +109,8 @@ class ArrayBase: public Object {
     virtual size_t element_size() const = 0;
     virtual void* raw_data() const = 0;
     virtual int device() const = 0;
+    // the stream the array was allocated on (its producer's stream); reads are ordered on it
+    virtual cudaStream_t stream() const = 0;
     int64_t numel() const {
         int64_t n = 1;
         for (int i = 0; i < rank(); i++) n *= extent(i);
@@ -124,8 +126,12 @@ class Array: public ArrayBase {
   public:
     Array() { m_dims.fill(0); }
     // allocates (uninitialised) device memory on the current device's stream
-    Array(std::array<int64_t, N> dims) : m_dims(dims) { allocate(detail::current_device()); }
-    Array(std::array<int64_t, N> dims, int device) : m_dims(dims) { allocate(device); }
+    Array(std::array<int64_t, N> dims) : m_dims(dims) {
+        allocate(detail::current_device(), detail::device_stream(detail::current_device()));
+    }
+    Array(std::array<int64_t, N> dims, int device) : m_dims(dims) { allocate(device, detail::device_stream(device)); }
+    // allocated and released stream-ordered on `stream` (a context's stream)
+    Array(std::array<int64_t, N> dims, int device, cudaStream_t stream) : m_dims(dims) { allocate(device, stream); }
 
     const char* name() const override { return "compas::Array"; }
     int rank() const override { return int(N); }
@@ -133,6 +139,13 @@ class Array: public ArrayBase {
     size_t element_size() const override { return sizeof(T); }
     void* raw_data() const override { return m_buf ? m_buf->ptr : nullptr; }
     int device() const override { return m_buf ? m_buf->device : 0; }
+    cudaStream_t stream() const override { return m_buf ? m_buf->stream : detail::device_stream(device()); }
+    // Order later reads and the release of this array on `s` instead of its allocation stream.
+    // Only valid once the host has seen every pending use of the array complete (an event or a
+    // synchronisation), since `s` is not ordered after that work.
+    void set_stream(cudaStream_t s) const {
+        if (m_buf) m_buf->stream = s;
+    }
 
     T* data() const { return static_cast<T*>(raw_data()); }
     int64_t size(size_t axis) const { return m_dims[axis]; }
@@ -149,13 +162,13 @@ class Array: public ArrayBase {
     }
 
   private:
-    void allocate(int device) {
+    void allocate(int device, cudaStream_t stream) {
         int64_t n = 1;
         for (auto d : m_dims) {
             if (d < 0) throw CompasException("negative array dimension");
             n *= d;
         }
-        m_buf = std::make_shared<detail::Buffer>(size_t(n) * sizeof(T), device, detail::device_stream(device));
+        m_buf = std::make_shared<detail::Buffer>(size_t(n) * sizeof(T), device, stream);
     }
     std::array<int64_t, N> m_dims;
     std::shared_ptr<detail::Buffer> m_buf;
@@ -167,13 +180,16 @@ class Array: public ArrayBase {
 class CompasContext {
   public:
     explicit CompasContext(int device = 0);
+    // a view of the device's context that issues work, and allocates, on `stream` (which the
+    // caller keeps alive while work or arrays made through this view exist)
+    CompasContext(int device, cudaStream_t stream) : m_device(device), m_stream(stream) {}
     CompasContext with_device(int index) const;
     int device() const { return m_device; }
     cudaStream_t stream() const { return m_stream; }
 
     template<typename T, size_t N>
     Array<std::decay_t<T>, N> allocate(View<T, N> content) const {
-        Array<std::decay_t<T>, N> out(content.dims, m_device);
+        Array<std::decay_t<T>, N> out(content.dims, m_device, m_stream);
         upload(out.data(), content.data(), size_t(content.size()) * sizeof(T));
         return out;
     }
@@ -462,6 +478,80 @@ class SimulationBatch: public Object {
     const Array<cfloat, 2>& echos(int job) const;   // [nreadouts][nvoxels]
     const Array<cfloat, 3>& signal(int job) const;  // [ncoils][nreadouts][ns]; empty without trajectory
     const char* name() const override { return "compas::SimulationBatch"; }
+
+    struct Impl;
+
+  private:
+    std::shared_ptr<Impl> m_impl;
+};
+
+// ------------------------------------------------------------------------------------------
+// serving (no counterpart in the reference)
+// ------------------------------------------------------------------------------------------
+
+// A reconstruction request: simulate the echoes of `parameters` under `sequence`, form the
+// signal on `trajectory` with `coil_sensitivities`, the residual b = data - s and its norm, and
+// (Cartesian trajectories: the reference's Jacobians accept no other) the gradient Jᴴ·b with
+// forward-difference ∂m/∂T1, ∂m/∂T2. Requests with the same nonzero `echo_key` share echoes and
+// derivatives: while an entry is resident, a request with its key skips the simulations (the
+// caller guarantees that equal keys mean equal parameters and sequence).
+struct ServeRequest {
+    TissueParameters parameters;
+    std::variant<FISPSequence, pSSFPSequence> sequence;
+    std::variant<CartesianTrajectory, SpiralTrajectory> trajectory;
+    Array<cfloat, 2> coil_sensitivities;  // [ncoils][nvoxels]
+    Array<cfloat, 3> data;                // measured signal [ncoils][nreadouts][ns]
+    uint64_t echo_key = 0;
+};
+
+struct ServeResult {
+    Array<cfloat, 3> residual;  // data - s
+    Array<cfloat, 2> gradient;  // Jᴴ·(data - s) [4][nvoxels]; empty for spiral trajectories
+    float objective = 0;        // ‖data - s‖²
+    double queued_ms = 0;       // submit → admitted to a batch
+    double device_ms = 0;       // admitted → results complete on the device
+    double latency_ms = 0;      // submit → complete
+    int batch = -1;             // batch it ran in
+    bool echo_cache_hit = false;
+};
+
+struct ServeOptions {
+    size_t memory_budget_bytes = size_t(150) << 30;  // admission budget for working sets and results
+    int max_inflight_batches = 4;                     // batches on the device at once, one stream each
+    int max_batch_requests = 16;                      // requests admitted into one batch
+    size_t echo_cache_bytes = size_t(16) << 30;      // resident echoes/derivatives (within the budget)
+    SimulateSignalMethod method = SimulateSignalMethod::MatmulFast;
+    float delta = DEFAULT_FINITE_DIFFERENCE_DELTA;
+};
+
+struct ServeStats {
+    uint64_t completed = 0, failed = 0, batches = 0, echo_cache_hits = 0;
+    double p50_ms = 0, p99_ms = 0, mean_ms = 0, max_ms = 0;
+    size_t peak_bytes = 0;        // peak of the admitted footprints plus cached echoes
+    int max_concurrent_batches = 0;
+};
+
+// Continuous-batching request loop on one GPU. submit() queues a request (thread-safe); a
+// worker thread admits queued requests in arrival order while their estimated device footprint
+// fits the memory budget and a batch slot is free, runs each admitted group as one
+// SimulationBatch (persistent work-queue simulations of all requests, their derivative
+// simulations and batched signals) followed by the per-request residuals and gradients, on the
+// slot's own stream, so batches admitted while others run overlap on the device. Each result is
+// the same, bit for bit, as the one-request operations give.
+class ServeEngine: public Object {
+  public:
+    explicit ServeEngine(const CompasContext& ctx, ServeOptions options = {});
+    ~ServeEngine() override;
+    uint64_t submit(ServeRequest request);
+    bool ready(uint64_t ticket) const;
+    // blocks until the request completed; throws CompasException if it failed. The result's
+    // arrays stay valid after release().
+    ServeResult wait(uint64_t ticket);
+    void release(uint64_t ticket);  // forget a completed request (frees its budget share)
+    void drain();                   // blocks until every submitted request completed
+    ServeStats stats() const;
+    void reset_stats();
+    const char* name() const override { return "compas::ServeEngine"; }
 
     struct Impl;
 

@@ -218,6 +218,36 @@ COMPAS_API compas_array* compas_b200_gauss_newton_array(const compas_object* gn,
 /* Kernel nodes of the captured graph, -1 before the first graph run. */
 COMPAS_API int compas_b200_gauss_newton_graph_kernels(const compas_object* gn);
 
+/* Continuous-batching serving engine (no counterpart in the reference). Requests (parameters,
+ * FISP or pSSFP sequence, Cartesian or spiral trajectory, coils [ncoils][nvoxels], measured data
+ * [ncoils][nreadouts][ns]) are admitted by estimated device footprint against
+ * `memory_budget_gb`, grouped into batches (at most `max_batch_requests` each, at most
+ * `max_inflight_batches` on the device at once) and give residual, objective and (Cartesian)
+ * gradient J^H.r. A nonzero echo_key lets requests with equal parameters and sequence share
+ * resident echoes (`echo_cache_gb`). `method` is a SimulateSignalMethod value. Released with
+ * compas_destroy_object, which finishes queued requests first. */
+COMPAS_API compas_object* compas_b200_make_server(const compas_context* ctx, double memory_budget_gb,
+                                                  int max_inflight_batches, int max_batch_requests,
+                                                  double echo_cache_gb, int method, float delta);
+/* Queue a request; returns its ticket (> 0) or -1 on error. */
+COMPAS_API int64_t compas_b200_server_submit(const compas_object* server, const compas_object* parameters,
+                                             const compas_object* sequence, const compas_object* trajectory,
+                                             const compas_array* coils, const compas_array* data,
+                                             uint64_t echo_key);
+/* Block until the request completed: objective, times[3] = queued, device, latency (ms), batch
+ * id; 0 on success, -1 if it failed (message in compas_last_error). */
+COMPAS_API int compas_b200_server_wait(const compas_object* server, int64_t ticket, float* objective,
+                                       double* times, int* batch);
+/* Result arrays of a completed request: 0 residual [ncoils][nreadouts][ns], 1 gradient [4][nvoxels]
+ * (empty for spiral trajectories). New handles, valid after release. */
+COMPAS_API compas_array* compas_b200_server_result(const compas_object* server, int64_t ticket, int which);
+COMPAS_API int compas_b200_server_release(const compas_object* server, int64_t ticket);
+COMPAS_API int compas_b200_server_drain(const compas_object* server);
+/* Statistics: out[0..9] = completed, failed, batches, echo cache hits, p50, p99, mean, max latency
+ * (ms), peak footprint (bytes), most batches in flight at once. Returns the count written. */
+COMPAS_API int compas_b200_server_stats(const compas_object* server, double* out, int n);
+COMPAS_API void compas_b200_server_reset_stats(const compas_object* server);
+
 #ifdef __cplusplus
 }
 #endif
