@@ -198,6 +198,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-jacobian", action="store_true", help="skip the J·v / Jᴴ·v measurements")
     ap.add_argument("--no-gn", action="store_true", help="skip the Gauss-Newton iteration timings")
+    ap.add_argument("--serve-rates", default="2,4,8",
+                    help="Poisson arrival rates (requests/s) of the served stream, empty to skip")
+    ap.add_argument("--serve-requests", type=int, default=32, help="requests per arrival rate")
     ap.add_argument("--batch-jobs", type=int, default=256,
                     help="jobs of the batched uneven workload (0 skips it)")
     ap.add_argument("--n-side", type=int, default=224,
@@ -317,6 +320,8 @@ def main():
         out["batched"] = batched(cb, ctx, stream, args, rank)
     if not args.no_gn:
         out["gauss_newton"] = gauss_newton(cb, ctx, stream, args, rank)
+    if args.serve_rates and rank == 0:
+        out["served"] = served(cb, ctx, args)
     if not args.no_e2e:
         out["e2e"] = e2e(cb, ctx, w, args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -380,6 +385,80 @@ def batched(cb, ctx, stream, args, rank):
             "note": "simulation: one persistent work-queue launch per kernel layout (FISP and pSSFP families on "
                     "two streams); signal: one batched launch per kind and family; results bit-identical to "
                     "the one-job calls"}
+
+
+def served(cb, ctx, args):
+    """Served request stream: Poisson arrivals at each rate of reconstruction requests (simulate +
+    signal + residual, and for Cartesian trajectories the FD derivatives and Jᴴ·r) drawn from 12
+    distinct requests (voxels logU[4k,200k], coils U{4..16}, FISP/pSSFP, Cartesian/spiral, TRs
+    U{400..1120}) whose sequences, trajectories, coils and data stay resident; HBM budget 150 GB.
+    Latency = submit -> results complete on the device, measured by the engine."""
+    import threading
+    import time
+
+    import numpy as np
+    import workloads
+
+    dicts = workloads.serve_requests(seed=5, n=12)
+    objs = []
+    for d in dicts:
+        p, s, t, _ = cb.job_from_dict(ctx, d)
+        objs.append((p, s, t, cb.CompasArray.from_numpy(ctx, d["coils"]), cb.CompasArray.from_numpy(ctx, d["data"])))
+    vtr = [d["nvoxels"] * d["ntr"] for d in dicts]
+    rng = np.random.default_rng(6)
+    out = {"workload": "12 distinct requests reused: voxels logU[4k,200k], coils U{4..16}, TRs U{400..1120}, "
+                       "FISP (25 states, 35 positions) / pSSFP (35 z), Cartesian (S=sqrt V) / spiral (TRs x 1000); "
+                       "request = simulate + signal + residual (+ FD derivatives + J^H r for Cartesian)",
+           "memory_budget_gb": 150, "max_inflight_batches": 4, "max_batch_requests": 16, "runs": []}
+
+    warmed = set()
+
+    def stream_run(rate, method, nreq, echo_keys):
+        eng = cb.ServeEngine(ctx, memory_budget_gb=150.0, max_inflight_batches=4, max_batch_requests=16,
+                             method=method)
+        if method not in warmed:  # first use of each kernel family and of every sequence table
+            for t in [eng.submit(*o) for o in objs]:
+                eng.wait(t)
+                eng.release(t)
+            eng.reset_stats()
+            warmed.add(method)
+        picks = rng.integers(0, len(objs), nreq)
+        gaps = rng.exponential(1.0 / rate, nreq)
+        tickets = [None] * nreq
+        t0 = time.perf_counter()
+
+        def client():
+            due = t0
+            for k in range(nreq):
+                due += gaps[k]
+                delay = due - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                i = int(picks[k])
+                tickets[k] = eng.submit(*objs[i], echo_key=(i + 1) if echo_keys else 0)
+
+        th = threading.Thread(target=client)
+        th.start()
+        th.join()
+        for t in tickets:
+            eng.wait(t)
+        wall = time.perf_counter() - t0
+        for t in tickets:
+            eng.release(t)
+        st = eng.stats()
+        done_vtr = float(sum(vtr[int(i)] for i in picks))
+        return {"rate_per_s": rate, "method": method, "requests": nreq, "echo_reuse": echo_keys,
+                "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
+                "voxel_tr_per_s": done_vtr / wall, "requests_per_s": nreq / wall, "batches": st["batches"],
+                "max_concurrent_batches": st["max_concurrent_batches"], "peak_gb": st["peak_bytes"] / 2 ** 30,
+                "echo_cache_hits": st["echo_cache_hits"], "failed": st["failed"]}
+
+    rates = [float(r) for r in args.serve_rates.split(",") if r]
+    for r in rates:
+        out["runs"].append(stream_run(r, "MatmulFast", args.serve_requests, False))
+    out["runs"].append(stream_run(rates[len(rates) // 2], "Direct", args.serve_requests, False))
+    out["runs"].append(stream_run(rates[-1], "MatmulFast", args.serve_requests, True))
+    return out
 
 
 def gauss_newton(cb, ctx, stream, args, rank):

@@ -229,3 +229,18 @@ def batch_jobs(seed: int = 4, njobs: int = 256, vmin: int = 1000, vmax: int = 64
         jobs.append({"kind": kind, "params": params, "seq": seq, "traj": traj, "coils": coils,
                      "nvoxels": nv, "ntr": ntr, "ncoils": nc})
     return jobs
+
+
+def serve_requests(seed: int = 5, n: int = 12, vmin: int = 4000, vmax: int = 200000, cmin: int = 4,
+                   cmax: int = 16, **kw) -> list:
+    """Distinct reconstruction requests for the served stream: the uneven jobs of `batch_jobs`
+    with voxels logU[vmin, vmax] and coils U{cmin..cmax}, each with measured data
+    y ~ 0.05·CN(0,1) of shape [C][R][S]."""
+    jobs = batch_jobs(seed=seed, njobs=n, vmin=vmin, vmax=vmax, **kw)
+    rng = np.random.default_rng([seed, 99])
+    for j in jobs:
+        c = int(rng.integers(cmin, cmax + 1))
+        j["ncoils"] = c
+        j["coils"] = gaussian_coils(c, j["params"], 22.4)
+        j["data"] = cn(rng, (c, j["traj"]["nr"], j["traj"]["ns"])) * 0.05
+    return jobs

@@ -96,14 +96,14 @@ def test_mixed_requests_from_threads_match_alone_bitwise(env):
 
 def test_budget_admission_and_oversized_request(env):
     cb, ctx, dicts, objs, data, alone = env
-    # a budget that fits roughly one request: batches of one, one at a time, same results
-    eng = cb.ServeEngine(ctx, memory_budget_gb=0.06, max_inflight_batches=4, max_batch_requests=8)
+    # a small budget: fewer requests admitted at once, the peak footprint within it, same results
+    eng = cb.ServeEngine(ctx, memory_budget_gb=0.02, max_inflight_batches=4, max_batch_requests=8)
     ts = [eng.submit(*objs[i], data[i]) for i in range(4)]
     for i, t in enumerate(ts):
         _check_same(cb, eng, t, alone[i], dicts[i]["traj"]["kind"] == "cartesian", i)
         eng.release(t)
     st = eng.stats()
-    assert st["peak_bytes"] <= 0.06 * 2 ** 30
+    assert st["peak_bytes"] <= 0.02 * 2 ** 30
     # a request larger than the whole budget fails with a clear error
     tiny = cb.ServeEngine(ctx, memory_budget_gb=1e-4)
     t = tiny.submit(*objs[0], data[0])
