@@ -77,6 +77,8 @@ _SIGS = {
     "compas_b200_fisp_config_info": ([_I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
     "compas_b200_pssfp_config_count": ([], _I),
     "compas_b200_pssfp_config_info": ([_I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
+    "compas_b200_fisp_launch_choice": ([_I, _I64, _I, C.POINTER(C.c_int), C.POINTER(C.c_int)], None),
+    "compas_b200_pssfp_launch_choice": ([_I, _I64], _I),
     "compas_b200_make_batch": ([_P, _I, _P, _P, _P, _P, _I], _P),
     "compas_b200_batch_run": ([_P], _I),
     "compas_b200_batch_echos": ([_P, _I], _P),
@@ -618,6 +620,17 @@ def fisp_configs() -> list:
         lib.compas_b200_fisp_config_info(i, C.byref(k), C.byref(g))
         out.append((k.value, g.value))
     return out
+
+
+def fisp_launch_choice(max_state: int, nvoxels: int, npositions: int) -> tuple:
+    """(layout index, warps) a FISP simulation of this shape runs with."""
+    cfg, w = C.c_int(), C.c_int()
+    library().compas_b200_fisp_launch_choice(int(max_state), int(nvoxels), int(npositions), C.byref(cfg), C.byref(w))
+    return cfg.value, w.value
+
+
+def pssfp_launch_choice(nz: int, nvoxels: int) -> int:
+    return int(library().compas_b200_pssfp_launch_choice(int(nz), int(nvoxels)))
 
 
 def pssfp_configs() -> list:

@@ -484,6 +484,18 @@ int compas_b200_pssfp_config_info(int index, int* iso_per_lane, int* lanes) {
     return compas::pssfp_config_info(index, iso_per_lane, lanes) ? 1 : 0;
 }
 
+void compas_b200_fisp_launch_choice(int max_state, int64_t nvoxels, int npositions, int* config, int* warps) {
+    compas::FispLaunch L = compas::tuned_fisp_launch(max_state, nvoxels, npositions);
+    if (L.config < 0) L = compas::fisp_default_launch(max_state, nvoxels, npositions);
+    if (config) *config = L.config;
+    if (warps) *warps = L.warps;
+}
+
+int compas_b200_pssfp_launch_choice(int nz, int64_t nvoxels) {
+    compas::PssfpLaunch L = compas::tuned_pssfp_launch(nz, nvoxels);
+    return L.config < 0 ? compas::pssfp_default_launch(nz, nvoxels).config : L.config;
+}
+
 compas_object* compas_b200_make_batch(const compas_context* context, int njobs, const compas_object* const* parameters,
                                       const compas_object* const* sequences, const compas_object* const* trajectories,
                                       const compas_array* const* coils, int method) {

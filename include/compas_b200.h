@@ -178,6 +178,10 @@ COMPAS_API int compas_b200_fisp_config_count(void);
 COMPAS_API int compas_b200_fisp_config_info(int index, int* states_per_lane, int* lanes);
 COMPAS_API int compas_b200_pssfp_config_count(void);
 COMPAS_API int compas_b200_pssfp_config_info(int index, int* iso_per_lane, int* lanes);
+/* The layout a simulation of this shape gets (override, tuning table, or built-in choice). */
+COMPAS_API void compas_b200_fisp_launch_choice(int max_state, int64_t nvoxels, int npositions, int* config,
+                                               int* warps);
+COMPAS_API int compas_b200_pssfp_launch_choice(int nz, int64_t nvoxels);
 
 /* Batched jobs (no counterpart in the reference): njobs independent simulate -> signal jobs,
  * job i = (parameters[i], sequences[i] (FISP or pSSFP), trajectories[i] (Cartesian, spiral, or

@@ -1,0 +1,70 @@
+"""Launch-layout selection: built-in choice, autotuner table (COMPAS_B200_TUNING) and overrides.
+
+The choice is host logic only, so it runs without a GPU. Each case runs in a fresh interpreter
+because the library reads the tuning table once per process.
+"""
+import json
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent.parent
+PKG = ROOT / "compas-toolkit_b200"
+
+PROBE = """
+import json, sys
+sys.path.insert(0, {pkg!r})
+import compas_b200 as cb
+out = {{"fisp": [cb.fisp_launch_choice(*s) for s in [(25, 50176, 35), (25, 4096, 1), (8, 4096, 1)]],
+       "pssfp": [cb.pssfp_launch_choice(*s) for s in [(35, 16384), (5, 4096)]],
+       "fisp_configs": cb.fisp_configs(), "pssfp_configs": cb.pssfp_configs()}}
+cb.set_fisp_launch(0, 2)
+out["override_uncovered"] = cb.fisp_launch_choice(25, 50176, 35)
+ok = [i for i, (k, g) in enumerate(cb.fisp_configs()) if k * g >= 25][-1]
+cb.set_fisp_launch(ok, 3)
+out["override"] = cb.fisp_launch_choice(25, 50176, 35)
+print(json.dumps(out))
+"""
+
+
+def _probe(env_extra=None):
+    env = dict(os.environ)
+    env.pop("COMPAS_B200_TUNING", None)
+    env.update(env_extra or {})
+    r = subprocess.run([sys.executable, "-c", PROBE.format(pkg=str(PKG))], capture_output=True, text=True, env=env,
+                       timeout=120)
+    assert r.returncode == 0, r.stderr
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def test_builtin_choice_covers_the_states():
+    out = _probe()
+    fc, pc = out["fisp_configs"], out["pssfp_configs"]
+    for (cfg, warps), n in zip(out["fisp"], (25, 25, 8)):
+        k, g = fc[cfg]
+        assert k * g >= n and 1 <= warps <= 8
+    assert tuple(fc[out["fisp"][0][0]]) == (25, 1) and out["fisp"][0][1] == 7  # 35 positions: 7 warps
+    assert fc[out["fisp"][2][0]][1] == 4  # few voxel/position pairs: states split over 4 lanes
+    for cfg, nz in zip(out["pssfp"], (35, 5)):
+        zt, gz = pc[cfg]
+        assert zt * gz >= nz
+    assert tuple(pc[out["pssfp"][0]]) == (5, 8)
+    # an override that does not cover the states is ignored; a covering one wins
+    assert out["override_uncovered"] == out["fisp"][0]
+    assert out["override"][1] == 3
+
+
+def test_tuning_table_is_used(tmp_path):
+    base = _probe()
+    fc, pc = base["fisp_configs"], base["pssfp_configs"]
+    fisp_cfg = next(i for i, (k, g) in enumerate(fc) if (k, g) == (7, 4))
+    pssfp_cfg = next(i for i, (z, g) in enumerate(pc) if (z, g) == (9, 4))
+    table = tmp_path / "tuning.txt"
+    table.write_text(f"# comment lines are ignored\nfisp 25 15 5 {fisp_cfg} 6\npssfp 35 14 {pssfp_cfg}\n"
+                     f"fisp 25 12 0 0 1\n")  # layout 0 cannot hold 25 states: ignored
+    out = _probe({"COMPAS_B200_TUNING": str(table)})
+    assert out["fisp"][0] == [fisp_cfg, 6]
+    assert out["fisp"][1] == base["fisp"][1]
+    assert out["pssfp"][0] == pssfp_cfg
+    assert out["pssfp"][1] == base["pssfp"][1]
