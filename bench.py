@@ -209,6 +209,12 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
 
+    # launch layouts from the committed autotuner table (compas_b200_autotune.py) unless the
+    # caller names another one
+    table = Path(__file__).resolve().parent / "compas-toolkit_b200" / "tuning" / "b200.txt"
+    if "COMPAS_B200_TUNING" not in os.environ and table.exists():
+        os.environ["COMPAS_B200_TUNING"] = str(table)
+
     import torch
 
     rank, world, local = dist_env()

@@ -51,38 +51,46 @@ def tune_fisp(ctx, N, nv, P, ntr, reps, warps=(4, 5, 6, 7, 8)):
     seq = cb.FispSequence.from_dict(ctx, W.fisp_sequence(W.smooth_flip_train(rng, ntr),
                                                         W.gaussian_slice_profile(P, ntr), 8.7e-3, 4.35e-3,
                                                         25e-3, N))
-    results = []
+    cb.set_fisp_launch(-1, -1)
+    default = cb.fisp_launch_choice(N, nv, P)
+    candidates = {default}
     for cfg, (K, G) in enumerate(cb.fisp_configs()):
         if K * G < N or K * G > max(2 * N, 32):
             continue
-        for w in sorted({min(P, w) for w in warps}):  # more warps than positions would idle
-            cb.set_fisp_launch(cfg, w)
-            ms = _time(ctx, lambda: cb.simulate_magnetization(ctx, params, seq), reps)
-            results.append((ms, cfg, w))
+        for w in {min(P, w) for w in warps}:  # more warps than positions would idle
+            candidates.add((cfg, w))
+    results = []
+    for cfg, w in sorted(candidates):
+        cb.set_fisp_launch(cfg, w)
+        ms = _time(ctx, lambda: cb.simulate_magnetization(ctx, params, seq), reps)
+        results.append((ms, cfg, w))
     cb.set_fisp_launch(-1, -1)
-    return sorted(results)
+    default_ms = next(ms for ms, cfg, w in results if (cfg, w) == default)
+    return sorted(results), default, default_ms
 
 
 def tune_pssfp(ctx, nz, nv, ntr, reps):
     rng = np.random.default_rng(nz)
     params = cb.TissueParameters.from_soa(ctx, W.tissue_voxels(rng, nv, 22.4))
     seq = cb.pSSFPSequence.from_dict(ctx, W.pssfp_sequence(rng, ntr, nrf=15, nz=nz))
+    cb.set_pssfp_launch(-1)
+    default = cb.pssfp_launch_choice(nz, nv)
+    candidates = {default} | {cfg for cfg, (ZT, GZ) in enumerate(cb.pssfp_configs()) if nz <= ZT * GZ <= 2 * nz + 30}
     results = []
-    for cfg, (ZT, GZ) in enumerate(cb.pssfp_configs()):
-        if ZT * GZ < nz or ZT * GZ > 2 * nz + 8:
-            continue
+    for cfg in sorted(candidates):
         cb.set_pssfp_launch(cfg)
         ms = _time(ctx, lambda: cb.simulate_magnetization(ctx, params, seq), reps)
         results.append((ms, cfg))
     cb.set_pssfp_launch(-1)
-    return sorted(results)
+    default_ms = next(ms for ms, cfg in results if cfg == default)
+    return sorted(results), default, default_ms
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--out", required=True, help="tuning table to write")
     ap.add_argument("--quick", action="store_true", help="fewer shape classes (a smoke run)")
-    ap.add_argument("--ntr", type=int, default=160, help="TRs of the timed sequences (cost is linear in it)")
+    ap.add_argument("--ntr", type=int, default=320, help="TRs of the timed sequences (cost is linear in it)")
     args = ap.parse_args(argv)
     ctx = cb.Context(0)
     voxel_classes = [4096, 50176] if args.quick else [4096, 16384, 50176, 200704]
@@ -90,19 +98,19 @@ def main(argv=None):
     lines, report = [], []
     for N, P in fisp_classes:
         for nv in voxel_classes:
-            res = tune_fisp(ctx, N, nv, P, args.ntr, reps=2 if args.quick else 3)
+            res, default, dms = tune_fisp(ctx, N, nv, P, args.ntr, reps=2 if args.quick else 3)
             ms, cfg, w = res[0]
-            default = cb.fisp_launch_choice(N, nv, P)
             lines.append(f"fisp {N} {int(math.log2(nv))} {int(math.log2(P))} {cfg} {w}")
-            report.append(f"# fisp N={N} P={P} V={nv}: best {cb.fisp_configs()[cfg]} W={w} {ms:.3f} ms "
-                          f"(default {cb.fisp_configs()[default[0]]} W={default[1]}; {len(res)} candidates)")
+            report.append(f"# fisp N={N} P={P} V={nv}: best {tuple(cb.fisp_configs()[cfg])} W={w} {ms:.3f} ms; "
+                          f"built-in {tuple(cb.fisp_configs()[default[0]])} W={default[1]} {dms:.3f} ms "
+                          f"({len(res)} candidates)")
     for nz in ([35] if args.quick else [9, 35]):
         for nv in voxel_classes:
-            res = tune_pssfp(ctx, nz, nv, args.ntr, reps=2 if args.quick else 3)
+            res, default, dms = tune_pssfp(ctx, nz, nv, args.ntr, reps=2 if args.quick else 3)
             ms, cfg = res[0]
             lines.append(f"pssfp {nz} {int(math.log2(nv))} {cfg}")
-            report.append(f"# pssfp nz={nz} V={nv}: best {cb.pssfp_configs()[cfg]} {ms:.3f} ms "
-                          f"(default {cb.pssfp_configs()[cb.pssfp_launch_choice(nz, nv)]}; {len(res)} candidates)")
+            report.append(f"# pssfp nz={nz} V={nv}: best {tuple(cb.pssfp_configs()[cfg])} {ms:.3f} ms; built-in "
+                          f"{tuple(cb.pssfp_configs()[default])} {dms:.3f} ms ({len(res)} candidates)")
     Path(args.out).write_text("\n".join(report + lines) + "\n")
     print("\n".join(report))
     return 0

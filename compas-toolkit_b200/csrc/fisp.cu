@@ -394,7 +394,7 @@ bool fisp_config_info(int index, int* K, int* G) {
     return true;
 }
 
-// Default layout choice for `N` states (from layout timings on B200):
+// Default layout choice for `N` states (from layout and autotuner timings on B200):
 //  * many (voxel, position) pairs: all states of a voxel in one lane (G = 1, K ≥ N) — no shuffles;
 //    25 states × 35 positions at 25600 voxels: 38.6 ms vs 51 ms for the best split layout;
 //  * few pairs (e.g. 4096 voxels × 1 position): split the states over 4 lanes to get 4× more warps
@@ -420,9 +420,13 @@ FispLaunch fisp_default_launch(int N, int64_t nvoxels, int P) {
         for (int i = 0; i < fisp_config_count(); i++)
             if (kFispConfigs[i].K * kFispConfigs[i].G >= N && (best < 0 || waste(i) < waste(best))) best = i;
     }
+    // warps (slice positions in flight per voxel tile), from the autotuner's B200 timings at
+    // 35 positions: 8 for 12+ states in one lane (25 states, 50176 voxels: 18.0 ms vs 19.8 ms
+    // with 7), 6 for fewer states in one lane, 4 for states split over lanes; never more than P
     FispLaunch L {best, 1};
-    L.warps = P >= 5 ? (P % 7 == 0 || P > 35 ? 7 : 5) : P;
-    L.warps = std::max(1, std::min(L.warps, 8));
+    const auto& c = kFispConfigs[best];
+    const int w = c.G == 1 ? (c.K >= 12 ? 8 : 6) : 4;
+    L.warps = std::max(1, std::min(w, P));
     return L;
 }
 

@@ -226,26 +226,27 @@ bool pssfp_config_info(int index, int* ZT, int* GZ) {
     return true;
 }
 
-// Default pSSFP layout (from layout timings on B200, 16384 voxels × 35 z × 760 TRs): 8 lanes per
-// voxel with ZT = ceil(nz/8) isochromats each (ZT5·GZ8: 11.2 ms vs 12.7 for ZT9·GZ4 and 19.1 for
-// ZT2·GZ32); for few z positions the smallest covering single-lane layout.
+// Default pSSFP layout (from the autotuner's timings on B200): 4 lanes per voxel with the
+// fewest isochromats per lane that cover nz (9 z: ZT4·GZ4 2.3 ms vs 3.9 ms for ZT4·GZ8 at 16384
+// voxels; 35 z: ZT9·GZ4 13.8 ms vs 14.0 ms for ZT5·GZ8 at 50176 voxels); 8 lanes when that
+// needs more than 12 per lane, one lane for nz ≤ 2.
 PssfpLaunch pssfp_default_launch(int nz, int64_t nvoxels) {
+    (void)nvoxels;
+    const int want_gz = nz <= 2 ? 1 : (div_ceil(nz, 4) <= 12 ? 4 : 8);
     int best = -1;
-    const int want_gz = nz > 8 ? 8 : 1;
     for (int i = 0; i < pssfp_config_count(); i++) {
         const auto& c = kPssfpConfigs[i];
-        if (c.ZT * c.GZ < nz || c.ZT > 12) continue;
-        if (best < 0) {
-            best = i;
-            continue;
+        if (c.GZ != want_gz || c.ZT * c.GZ < nz) continue;
+        if (best < 0 || c.ZT < kPssfpConfigs[best].ZT) best = i;
+    }
+    if (best < 0) {  // smallest covering layout of any shape
+        for (int i = 0; i < pssfp_config_count(); i++) {
+            const auto& c = kPssfpConfigs[i];
+            if (c.ZT * c.GZ >= nz && (best < 0 || c.ZT * c.GZ < kPssfpConfigs[best].ZT * kPssfpConfigs[best].GZ))
+                best = i;
         }
-        const auto& b = kPssfpConfigs[best];
-        const bool pc = c.GZ == want_gz, pb = b.GZ == want_gz;
-        const int wc = c.ZT * c.GZ - nz, wb = b.ZT * b.GZ - nz;
-        if ((pc && !pb) || (pc == pb && wc < wb)) best = i;
     }
     if (best < 0) best = 7;  // 2 x 32 lanes covers nz ≤ 64
-    (void)nvoxels;
     return PssfpLaunch {best};
 }
 

@@ -44,12 +44,12 @@ def test_builtin_choice_covers_the_states():
     for (cfg, warps), n in zip(out["fisp"], (25, 25, 8)):
         k, g = fc[cfg]
         assert k * g >= n and 1 <= warps <= 8
-    assert tuple(fc[out["fisp"][0][0]]) == (25, 1) and out["fisp"][0][1] == 7  # 35 positions: 7 warps
+    assert tuple(fc[out["fisp"][0][0]]) == (25, 1) and out["fisp"][0][1] == 8  # 35 positions: 8 warps
     assert fc[out["fisp"][2][0]][1] == 4  # few voxel/position pairs: states split over 4 lanes
     for cfg, nz in zip(out["pssfp"], (35, 5)):
         zt, gz = pc[cfg]
         assert zt * gz >= nz
-    assert tuple(pc[out["pssfp"][0]]) == (5, 8)
+    assert tuple(pc[out["pssfp"][0]]) == (9, 4)
     # an override that does not cover the states is ignored; a covering one wins
     assert out["override_uncovered"] == out["fisp"][0]
     assert out["override"][1] == 3
