@@ -203,6 +203,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=32, help="requests per arrival rate")
     ap.add_argument("--batch-jobs", type=int, default=256,
                     help="jobs of the batched uneven workload (0 skips it)")
+    ap.add_argument("--batch-vmax", type=int, default=64000,
+                    help="largest voxel count of a batched job (smaller values for profiler captures)")
     ap.add_argument("--n-side", type=int, default=224,
                     help="voxel grid side (224 = the MR-STAT workload; smaller values for profiler captures)")
     args = ap.parse_args()
@@ -347,7 +349,7 @@ def batched(cb, ctx, stream, args, rank):
     import torch
     import workloads
 
-    dicts = workloads.batch_jobs(seed=4 + rank, njobs=args.batch_jobs)
+    dicts = workloads.batch_jobs(seed=4 + rank, njobs=args.batch_jobs, vmax=args.batch_vmax)
     jobs = [cb.job_from_dict(ctx, d) for d in dicts]
     batch = cb.SimulationBatch(ctx, jobs)
     vtr = sum(d["nvoxels"] * d["ntr"] for d in dicts)
@@ -382,7 +384,7 @@ def batched(cb, ctx, stream, args, rank):
     for d in dicts:
         key = f'{d["kind"]}+{d["traj"]["kind"]}'
         kinds[key] = kinds.get(key, 0) + 1
-    return {"workload": f"{len(dicts)} jobs: voxels logU[1k,64k], TRs U{{400..1120}}, coils U{{1..16}}, FISP (25 "
+    return {"workload": f"{len(dicts)} jobs: voxels logU[1k,{args.batch_vmax}], TRs U{{400..1120}}, coils U{{1..16}}, FISP (25 "
                         "states, 35 positions) or pSSFP (35 z, 15 RF samples), Cartesian (S=sqrt V) or spiral "
                         f"(TRs x 1000), seed {4 + rank}",
             "mix": kinds, "voxel_tr": vtr, "batch_ms": t_batch, "voxel_tr_per_s": vtr / (t_batch / 1e3),
