@@ -203,6 +203,14 @@ class CompasArray:
         _check()
         return out
 
+    @property
+    def __cuda_array_interface__(self) -> dict:
+        """Zero-copy view for CUDA-aware libraries (e.g. torch.as_tensor(arr, device="cuda")); the
+        consumer orders its use after the context's stream, on which the array was produced."""
+        typestr = "<c8" if self.dtype == np.complex64 else "<f4"
+        return {"shape": self.shape, "typestr": typestr, "data": (self.device_ptr(), False), "version": 3,
+                "strides": None, "stream": int(self.context.stream) or None}
+
     def read_into(self, out: np.ndarray) -> np.ndarray:
         """Blocking copy into a preallocated (e.g. pinned) host array of matching size/dtype."""
         assert out.dtype == self.dtype and out.size == self.size and out.flags.c_contiguous

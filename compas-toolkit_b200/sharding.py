@@ -1,0 +1,95 @@
+"""Voxel sharding of the simulation hot path over torch.distributed ranks (one GPU per rank).
+
+Every operation of the path is either independent per voxel (simulation, derivatives, Jᴴ·v) or a
+sum over voxels (signal, J·v). So a slice is split into contiguous voxel ranges, one per rank:
+
+* signal and J·v: each rank contracts its voxels into a partial [C][R][S] and one all-reduce
+  (sum) over the ranks forms the full result (NCCL over NVLink on GPUs);
+* Jᴴ·r: each rank needs the full residual r (identical on every rank after the all-reduce) and
+  produces its own voxels of [4][V]; `gather_voxels` assembles the full vector when needed.
+
+This mirrors the reference's chunking of voxels across devices with a summing reduction of the
+signal (src/trajectories/signal.cu:289-300, compas/core/context.h:51-68). The functions below
+take the per-rank compute as callables, so the partition and reduction logic is the same whether
+the ranks run the GPU library (NCCL) or a CPU restatement (gloo).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass(frozen=True)
+class VoxelShard:
+    """Contiguous voxel range [begin, end) of `rank` among `world` ranks (sizes differ by ≤ 1)."""
+
+    nvoxels: int
+    rank: int
+    world: int
+
+    @property
+    def begin(self) -> int:
+        q, r = divmod(self.nvoxels, self.world)
+        return self.rank * q + min(self.rank, r)
+
+    @property
+    def end(self) -> int:
+        q, r = divmod(self.nvoxels, self.world)
+        return self.begin + q + (1 if self.rank < r else 0)
+
+    @property
+    def size(self) -> int:
+        return self.end - self.begin
+
+    def take(self, a: np.ndarray) -> np.ndarray:
+        """This rank's voxels of an array whose last axis is the voxel axis (tissue [9][V],
+        coils [C][V], echoes [R][V], J·v input [4][V])."""
+        return np.ascontiguousarray(a[..., self.begin:self.end])
+
+    def counts(self) -> list:
+        return [VoxelShard(self.nvoxels, r, self.world).size for r in range(self.world)]
+
+
+def allreduce_sum(tensor, group=None):
+    """Sum a partial signal / J·v over the ranks in place (torch.distributed, NCCL or gloo)."""
+    import torch.distributed as dist
+
+    dist.all_reduce(tensor, op=dist.ReduceOp.SUM, group=group)
+    return tensor
+
+
+def gather_voxels(local, shard: VoxelShard, group=None):
+    """Assemble [..., V] from every rank's [..., V_rank] (torch tensors on the backend's device)."""
+    import torch
+    import torch.distributed as dist
+
+    counts = shard.counts()
+    width = max(counts)
+    pad = torch.zeros(local.shape[:-1] + (width,), dtype=local.dtype, device=local.device)
+    pad[..., :local.shape[-1]] = local
+    parts = [torch.empty_like(pad) for _ in counts]
+    dist.all_gather(parts, pad, group=group)
+    return torch.cat([p[..., :c] for p, c in zip(parts, counts)], dim=-1)
+
+
+def sharded_signal(shard: VoxelShard, partial_signal, params: np.ndarray, coils: np.ndarray, echos_or_none,
+                   to_tensor, group=None):
+    """Full signal [C][R][S] on every rank: `partial_signal(params_local, coils_local, echos_local)`
+    contracts this rank's voxels (echos_local is None when the callable simulates them itself);
+    `to_tensor` turns its result into a torch tensor on the collective's device."""
+    local = partial_signal(shard.take(params), shard.take(coils),
+                           None if echos_or_none is None else shard.take(echos_or_none))
+    return allreduce_sum(to_tensor(local), group)
+
+
+def gpu_partial_signal(cb, ctx, sequence, trajectory, method: str = "MatmulFast"):
+    """Per-rank compute for `sharded_signal` on the GPU library: simulate this rank's voxels and
+    contract them; returns the device array (view it with torch.as_tensor(..., device="cuda"))."""
+
+    def fn(params_local, coils_local, echos_local):
+        p = cb.TissueParameters.from_soa(ctx, params_local)
+        e = cb.simulate_magnetization(ctx, p, sequence) if echos_local is None else echos_local
+        return cb.magnetization_to_signal(ctx, e, p, trajectory, coils_local, method=method)
+
+    return fn
