@@ -93,3 +93,22 @@ def gpu_partial_signal(cb, ctx, sequence, trajectory, method: str = "MatmulFast"
         return cb.magnetization_to_signal(ctx, e, p, trajectory, coils_local, method=method)
 
     return fn
+
+
+def gpu_to_tensor(ctx):
+    """`to_tensor` for `sharded_signal` on the GPU library: a torch copy of the library array on
+    torch's current stream, ordered after the context's stream that produced it (the collective
+    then runs on torch's stream)."""
+    import torch
+
+    def fn(arr):
+        lib_stream = torch.cuda.ExternalStream(ctx.stream)
+        torch.cuda.current_stream().wait_stream(lib_stream)
+        view = torch.as_tensor(arr, device="cuda")  # zero-copy view of the library's buffer
+        out = torch.view_as_real(view).clone()
+        # the library releases `arr` on its own stream: order that after the copy
+        lib_stream.wait_stream(torch.cuda.current_stream())
+        return out
+
+    return fn
+
