@@ -467,4 +467,65 @@ void jacobian_hermitian_voxel(const float* echo, const float* dT1, const float* 
     }
 }
 
+// ---- spiral J·v and Jᴴ·v ----------------------------------------------------------------
+// The reference's Jacobians accept only CartesianTrajectory (compas/jacobian/product.h:30,
+// hermitian.h:30). These differentiate the spiral signal model of signal_spiral_entry
+// (spiral_view.cuh:352-412, signal_kernels.cuh:274-345) with the column scaling of the Cartesian
+// products (product_kernels.cuh:44-63): the per-readout factor F_rvk = readout_rv · z_rv^k depends
+// on T2 through R2 = 1/T2 in the rewind exp((S/2)Δt R2) and in z^k = exp(k(-Δt R2 + iΘ)), so
+// dF/dT2 = (k - S/2)·Δt·R2²·F, the same form as the Cartesian dE/dT2.
+template<typename T>
+cx<T> spiral_factor(const Spiral& t, const Voxel<T>& p, int r, int k) {
+    const T R2 = T(1) / p.T2;
+    const T Theta = T(t.dk[2 * r]) * p.x + T(t.dk[2 * r + 1]) * p.y + T(t.dt) * two_pi<T>() * p.B0;
+    const cx<T> zk = cexp(cx<T>{T(k) * (-T(t.dt) * R2), T(k) * Theta});
+    return spiral_readout(t, p, r, cx<T>{T(1), T(0)}) * zk;
+}
+
+template<typename T>
+cx<T> spiral_jacobian_entry(const float* echo, const float* dT1, const float* dT2, const float* params, int64_t nv,
+                            const Spiral& t, const float* coils, const float* vec, int c, int r, int k) {
+    cx<T> res;
+    auto ld = [&](const float* a, int64_t i) { return cx<T>{T(a[2 * i]), T(a[2 * i + 1])}; };
+    for (int64_t v = 0; v < nv; v++) {
+        Voxel<T> p = load_voxel<T>(params, nv, v);
+        const cx<T> F = spiral_factor(t, p, r, k);
+        const T R2 = T(1) / p.T2;
+        const cx<T> dF = F * ((T(k) - T(0.5) * T(t.ns)) * T(t.dt) * R2 * R2);
+        cx<T> me = ld(echo, int64_t(r) * nv + v);
+        cx<T> d1 = ld(dT1, int64_t(r) * nv + v), d2 = ld(dT2, int64_t(r) * nv + v);
+        cx<T> prod = ld(vec, 0 * nv + v) * F * p.T1 * p.rho * d1
+                   + ld(vec, 1 * nv + v) * (F * d2 + dF * me) * p.T2 * p.rho
+                   + ld(vec, 2 * nv + v) * F * me
+                   + ld(vec, 3 * nv + v) * F * cx<T>{T(0), T(1)} * me;
+        res += prod * ld(coils, int64_t(c) * nv + v);
+    }
+    return res;
+}
+
+template<typename T>
+void spiral_jacobian_hermitian_voxel(const float* echo, const float* dT1, const float* dT2, const float* params,
+                                     int64_t nv, const Spiral& t, const float* coils, int nc, const float* vec,
+                                     int64_t v, cx<T> out[4]) {
+    auto ld = [&](const float* a, int64_t i) { return cx<T>{T(a[2 * i]), T(a[2 * i + 1])}; };
+    Voxel<T> p = load_voxel<T>(params, nv, v);
+    const T R2 = T(1) / p.T2;
+    for (int i = 0; i < 4; i++) out[i] = cx<T>();
+    for (int r = 0; r < t.nr; r++) {
+        cx<T> me = ld(echo, int64_t(r) * nv + v);
+        cx<T> a1 = ld(dT1, int64_t(r) * nv + v), a2 = ld(dT2, int64_t(r) * nv + v);
+        for (int k = 0; k < t.ns; k++) {
+            const cx<T> F = spiral_factor(t, p, r, k);
+            const cx<T> dF = F * ((T(k) - T(0.5) * T(t.ns)) * T(t.dt) * R2 * R2);
+            for (int c = 0; c < nc; c++) {
+                const cx<T> f = ld(vec, (int64_t(c) * t.nr + r) * t.ns + k) * conj(ld(coils, int64_t(c) * nv + v));
+                out[0] += conj(p.T1 * p.rho) * f * conj(a1 * F);
+                out[1] += conj(p.T2 * p.rho) * f * conj(a2 * F + me * dF);
+                out[2] += f * conj(F * me);
+            }
+        }
+    }
+    out[3] = out[2] * cx<T>{T(0), T(-1)};
+}
+
 }  // namespace oracle

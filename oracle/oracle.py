@@ -33,6 +33,9 @@ _SIGS = {
     "oracle_signal_spiral_f64": [_P, _P, _I64, _I, _I, _F, _P, _P, _P, _I, _P, _I64, _P, _I],
     "oracle_jacobian_f64": [_P, _P, _P, _P, _I64, _I, _I, _F, _F, _F, _P, _I, _P, _P, _I64, _P, _I],
     "oracle_jacobian_hermitian_f64": [_P, _P, _P, _P, _I64, _I, _I, _F, _F, _F, _P, _I, _P, _P, _I64, _P, _I],
+    "oracle_spiral_jacobian_f64": [_P, _P, _P, _P, _I64, _I, _I, _F, _P, _P, _P, _I, _P, _P, _I64, _P, _I],
+    "oracle_spiral_jacobian_hermitian_f64": [_P, _P, _P, _P, _I64, _I, _I, _F, _P, _P, _P, _I, _P, _P, _I64, _P,
+                                             _I],
     "oracle_residual_f64": [_P, _P, _I64, _P],
     "oracle_cx_eval_f32": [_I, _P, _I64, _P],
     "oracle_max_threads": [],
@@ -208,6 +211,39 @@ def jacobian_hermitian(echo, dT1, dT2, params, traj, coils, vec, vidx=None, nthr
                                         C.c_float(dk.real), C.c_float(dk.imag), co.ctypes.data, Cn,
                                         ve.ctypes.data, _iptr(idx), C.c_int64(nidx), out.ctypes.data,
                                         nthreads or nthreads_default())
+    return _as_complex(out)
+
+
+def spiral_jacobian(echo, dT1, dT2, params, traj, coils, vec, entries=None, nthreads=None):
+    """J·v on a spiral trajectory (no counterpart in the reference; derived from its spiral signal)."""
+    e, d1, d2, params, co, ve = _cf(echo), _cf(dT1), _cf(dT2), _ff(params), _cf(coils), _cf(vec)
+    ks, dk = _cf(traj["k_start"]), _cf(traj["dk"])
+    R, V = echo.shape
+    Cn = coils.shape[0]
+    ent, nent = _entries(entries)
+    shape = (nent,) if ent is not None else (Cn, traj["nr"], traj["ns"])
+    out = _out(shape, "f64")
+    lib().oracle_spiral_jacobian_f64(e.ctypes.data, d1.ctypes.data, d2.ctypes.data, params.ctypes.data, C.c_int64(V),
+                                     traj["nr"], traj["ns"], C.c_float(traj["dt"]), ks.ctypes.data, dk.ctypes.data,
+                                     co.ctypes.data, Cn, ve.ctypes.data, None if ent is None else ent.ctypes.data,
+                                     C.c_int64(nent), out.ctypes.data, nthreads or nthreads_default())
+    return _as_complex(out)
+
+
+def spiral_jacobian_hermitian(echo, dT1, dT2, params, traj, coils, vec, vidx=None, nthreads=None):
+    """Jᴴ·v on a spiral trajectory: [4][n]."""
+    e, d1, d2, params, co, ve = _cf(echo), _cf(dT1), _cf(dT2), _ff(params), _cf(coils), _cf(vec)
+    ks, dk = _cf(traj["k_start"]), _cf(traj["dk"])
+    R, V = echo.shape
+    Cn = coils.shape[0]
+    idx, nidx = _ip(vidx)
+    n = nidx if idx is not None else V
+    out = _out((4, n), "f64")
+    lib().oracle_spiral_jacobian_hermitian_f64(e.ctypes.data, d1.ctypes.data, d2.ctypes.data, params.ctypes.data,
+                                               C.c_int64(V), traj["nr"], traj["ns"], C.c_float(traj["dt"]),
+                                               ks.ctypes.data, dk.ctypes.data, co.ctypes.data, Cn, ve.ctypes.data,
+                                               _iptr(idx), C.c_int64(nidx), out.ctypes.data,
+                                               nthreads or nthreads_default())
     return _as_complex(out)
 
 

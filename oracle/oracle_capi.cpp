@@ -185,6 +185,33 @@ int oracle_jacobian_hermitian_f64(const float* echo, const float* dT1, const flo
     return 0;
 }
 
+int oracle_spiral_jacobian_f64(const float* echo, const float* dT1, const float* dT2, const float* params,
+                               int64_t nv, int nr, int ns, float dt, const float* k_start, const float* dk,
+                               const float* coils, int nc, const float* vec, const int* entries, int64_t nent,
+                               double* out, int nthreads) {
+    Spiral t {nr, ns, dt, k_start, dk};
+    for_entries<double>(nc, nr, ns, entries, nent, out, nthreads, [&](int c, int r, int k) {
+        return spiral_jacobian_entry<double>(echo, dT1, dT2, params, nv, t, coils, vec, c, r, k);
+    });
+    return 0;
+}
+
+int oracle_spiral_jacobian_hermitian_f64(const float* echo, const float* dT1, const float* dT2, const float* params,
+                                         int64_t nv, int nr, int ns, float dt, const float* k_start,
+                                         const float* dk, const float* coils, int nc, const float* vec,
+                                         const int* vidx, int64_t nidx, double* out, int nthreads) {
+    Spiral t {nr, ns, dt, k_start, dk};
+    int64_t n = vidx ? nidx : nv;
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 4)
+    for (int64_t i = 0; i < n; i++) {
+        int64_t v = vidx ? vidx[i] : i;
+        cx<double> res[4];
+        spiral_jacobian_hermitian_voxel<double>(echo, dT1, dT2, params, nv, t, coils, nc, vec, v, res);
+        for (int f = 0; f < 4; f++) store<double>(out, f * n + i, res[f]);
+    }
+    return 0;
+}
+
 // residual d = lhs - rhs, returns Σ|d|²   (src/utils/residual_kernels.cuh:73-96)
 double oracle_residual_f64(const float* lhs, const float* rhs, int64_t n, double* out) {
     double acc = 0;

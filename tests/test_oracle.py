@@ -268,6 +268,64 @@ def test_jacobian_matches_finite_difference_of_signal(oracle, workloads):
     assert oracle.rel_l2(Jv, fd) < 2e-3
 
 
+def _small_spiral_j(workloads, rng, n_side=4, nr=5, ns=7, nc=2):
+    p = workloads.tissue(rng, n_side, 20.0)
+    nv = n_side * n_side
+    traj = workloads.spiral(rng, nr, ns, 20.0, 4e-6)
+    coils = workloads.cn(rng, (nc, nv))
+    echo, d1, d2 = (workloads.cn(rng, (nr, nv)) for _ in range(3))
+    return p, traj, coils, echo, d1, d2
+
+
+def test_spiral_jacobian_adjointness(oracle, workloads):
+    # the spiral products have no counterpart in the reference; Jᴴ must be the exact adjoint of J
+    rng = np.random.default_rng(15)
+    p, traj, coils, echo, d1, d2 = _small_spiral_j(workloads, rng)
+    nv = p.shape[1]
+    v = workloads.cn(rng, (4, nv))
+    u = workloads.cn(rng, (coils.shape[0], traj["nr"], traj["ns"]))
+    Jv = oracle.spiral_jacobian(echo, d1, d2, p, traj, coils, v)
+    JHu = oracle.spiral_jacobian_hermitian(echo, d1, d2, p, traj, coils, u)
+    lhs = np.vdot(u.astype(np.complex128), Jv)
+    rhs = np.vdot(JHu, v.astype(np.complex128))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-12
+
+
+def test_spiral_jacobian_matches_finite_difference_of_spiral_signal(oracle, workloads):
+    # J·v on a spiral equals the directional derivative of the reference's spiral signal model
+    # (rewind exp((S/2)Δt R2), z^k = exp(k(-Δt R2 + iΘ))) with the T-scaled columns
+    rng = np.random.default_rng(19)
+    n_side, nr, ns, nc = 4, 5, 6, 2
+    p = workloads.tissue(rng, n_side, 20.0).astype(np.float64)
+    nv = n_side ** 2
+    traj = workloads.spiral(rng, nr, ns, 20.0, 4e-6)
+    coils = workloads.cn(rng, (nc, nv))
+    tr = np.linspace(0.01, 0.5, nr)[:, None]
+
+    def model(T1, T2):
+        m = (1 - 2 * np.exp(-tr / T1)) * np.exp(-0.004 / T2) * np.exp(1j * tr * 3)
+        d1 = (-2 * np.exp(-tr / T1) * tr / T1 ** 2) * np.exp(-0.004 / T2) * np.exp(1j * tr * 3)
+        d2 = (1 - 2 * np.exp(-tr / T1)) * np.exp(-0.004 / T2) * (0.004 / T2 ** 2) * np.exp(1j * tr * 3)
+        return m, d1, d2
+
+    m, d1, d2 = model(p[0], p[1])
+    v = rng.standard_normal((4, nv))
+    Jv = oracle.spiral_jacobian(m, d1, d2, p.astype(np.float32), traj, coils, v.astype(np.complex64))
+
+    def sig(h):
+        q = p.copy()
+        q[0] = p[0] * (1 + h * v[0])
+        q[1] = p[1] * (1 + h * v[1])
+        q[4] = p[4] + h * v[2]
+        q[5] = p[5] + h * v[3]
+        mm, _, _ = model(q[0], q[1])
+        return oracle.signal_spiral(mm, q.astype(np.float32), traj, coils)
+
+    h = 1e-3
+    fd = (sig(h) - sig(-h)) / (2 * h)
+    assert oracle.rel_l2(Jv, fd) < 2e-3
+
+
 def test_residual(oracle):
     rng = np.random.default_rng(3)
     a = (rng.standard_normal((2, 3, 4)) + 1j * rng.standard_normal((2, 3, 4))).astype(np.complex64)
