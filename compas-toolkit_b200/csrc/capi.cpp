@@ -121,6 +121,17 @@ void read_array(const compas_array* arr, void* dest, int64_t length, size_t elem
     base->copy_bytes_to(dest, size_t(length) * elem);
 }
 
+// calls fn with the Cartesian or spiral trajectory behind `obj` (the Jacobians accept both here;
+// the reference's accept Cartesian only)
+template<typename F>
+auto with_trajectory(const void* obj, F fn) {
+    if (!obj) throw compas::CompasException("null trajectory");
+    const auto* base = handle<compas::Object>(obj);
+    if (const auto* c = dynamic_cast<const compas::CartesianTrajectory*>(base)) return fn(*c);
+    if (const auto* s = dynamic_cast<const compas::SpiralTrajectory*>(base)) return fn(*s);
+    throw compas::CompasException(std::string("invalid trajectory object: ") + base->name());
+}
+
 compas::SimulateSignalMethod signal_method(int m) {
     if (m < 0 || m > 5) throw compas::CompasException("invalid SimulateSignalMethod");
     return compas::SimulateSignalMethod(m);
@@ -315,10 +326,13 @@ compas_array* compas_compute_jacobian(const compas_context* ctx, int ncoils, con
         if (co.size(0) != ncoils) throw compas::CompasException("ncoils does not match the coil array");
         auto method =
             low_precision == 0 ? compas::JacobianComputeMethod::GemmFast : compas::JacobianComputeMethod::GemmLow;
-        return new_array(compas::compute_jacobian(
-            ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"), array_of<cfloat, 2>(delta_echos_T1, "delta_echos_T1"),
-            array_of<cfloat, 2>(delta_echos_T2, "delta_echos_T2"), unwrap<compas::TissueParameters>(parameters),
-            unwrap<compas::CartesianTrajectory>(trajectory), co, array_of<cfloat, 2>(vector, "vector"), method));
+        return with_trajectory(trajectory, [&](const auto& traj) {
+            return new_array(compas::compute_jacobian(
+                ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"),
+                array_of<cfloat, 2>(delta_echos_T1, "delta_echos_T1"),
+                array_of<cfloat, 2>(delta_echos_T2, "delta_echos_T2"), unwrap<compas::TissueParameters>(parameters),
+                traj, co, array_of<cfloat, 2>(vector, "vector"), method));
+        });
     });
 }
 
@@ -332,10 +346,13 @@ compas_array* compas_compute_jacobian_hermitian(const compas_context* ctx, int n
         if (co.size(0) != ncoils) throw compas::CompasException("ncoils does not match the coil array");
         auto method =
             low_precision == 0 ? compas::JacobianComputeMethod::GemmFast : compas::JacobianComputeMethod::GemmLow;
-        return new_array(compas::compute_jacobian_hermitian(
-            ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"), array_of<cfloat, 2>(delta_echos_T1, "delta_echos_T1"),
-            array_of<cfloat, 2>(delta_echos_T2, "delta_echos_T2"), unwrap<compas::TissueParameters>(parameters),
-            unwrap<compas::CartesianTrajectory>(trajectory), co, array_of<cfloat, 3>(vector, "vector"), method));
+        return with_trajectory(trajectory, [&](const auto& traj) {
+            return new_array(compas::compute_jacobian_hermitian(
+                ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"),
+                array_of<cfloat, 2>(delta_echos_T1, "delta_echos_T1"),
+                array_of<cfloat, 2>(delta_echos_T2, "delta_echos_T2"), unwrap<compas::TissueParameters>(parameters),
+                traj, co, array_of<cfloat, 3>(vector, "vector"), method));
+        });
     });
 }
 
@@ -393,11 +410,14 @@ compas_array* compas_b200_compute_jacobian(const compas_context* ctx, const comp
                                            const compas_object* parameters, const compas_object* trajectory,
                                            const compas_array* coils, const compas_array* vector, int method) {
     return guarded([&] {
-        return new_array(compas::compute_jacobian(
-            ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"), array_of<cfloat, 2>(delta_echos_T1, "delta_echos_T1"),
-            array_of<cfloat, 2>(delta_echos_T2, "delta_echos_T2"), unwrap<compas::TissueParameters>(parameters),
-            unwrap<compas::CartesianTrajectory>(trajectory), array_of<cfloat, 2>(coils, "coils"),
-            array_of<cfloat, 2>(vector, "vector"), jacobian_method(method)));
+        return with_trajectory(trajectory, [&](const auto& traj) {
+            return new_array(compas::compute_jacobian(
+                ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"),
+                array_of<cfloat, 2>(delta_echos_T1, "delta_echos_T1"),
+                array_of<cfloat, 2>(delta_echos_T2, "delta_echos_T2"), unwrap<compas::TissueParameters>(parameters),
+                traj, array_of<cfloat, 2>(coils, "coils"), array_of<cfloat, 2>(vector, "vector"),
+                jacobian_method(method)));
+        });
     });
 }
 
@@ -408,11 +428,14 @@ compas_array* compas_b200_compute_jacobian_hermitian(const compas_context* ctx, 
                                                      const compas_object* trajectory, const compas_array* coils,
                                                      const compas_array* vector, int method) {
     return guarded([&] {
-        return new_array(compas::compute_jacobian_hermitian(
-            ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"), array_of<cfloat, 2>(delta_echos_T1, "delta_echos_T1"),
-            array_of<cfloat, 2>(delta_echos_T2, "delta_echos_T2"), unwrap<compas::TissueParameters>(parameters),
-            unwrap<compas::CartesianTrajectory>(trajectory), array_of<cfloat, 2>(coils, "coils"),
-            array_of<cfloat, 3>(vector, "vector"), jacobian_method(method)));
+        return with_trajectory(trajectory, [&](const auto& traj) {
+            return new_array(compas::compute_jacobian_hermitian(
+                ctx_of(ctx), array_of<cfloat, 2>(echos, "echos"),
+                array_of<cfloat, 2>(delta_echos_T1, "delta_echos_T1"),
+                array_of<cfloat, 2>(delta_echos_T2, "delta_echos_T2"), unwrap<compas::TissueParameters>(parameters),
+                traj, array_of<cfloat, 2>(coils, "coils"), array_of<cfloat, 3>(vector, "vector"),
+                jacobian_method(method)));
+        });
     });
 }
 

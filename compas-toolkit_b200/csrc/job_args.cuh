@@ -47,6 +47,10 @@ struct SpiralArgs {
     const float2* k_start;
     const float2* delta_k;
     float2* signal;  // [C][R][S]
+    // J·v only (the spiral kernel's JAC form): derivative echoes and the direction [4][V]
+    const float2* dT1;
+    const float2* dT2;
+    const float2* vec;
 };
 
 // per-voxel constants of the generated operand (written by tc_prep_kernel)

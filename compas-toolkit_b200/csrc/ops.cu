@@ -317,4 +317,41 @@ Array<cfloat, 2> compute_jacobian_hermitian(const CompasContext& ctx, Array<cflo
     return JHv;
 }
 
+// Spiral trajectories (no counterpart in the reference, whose Jacobians take CartesianTrajectory
+// only): derived from the spiral signal model; plain FP32 SIMT kernels for every method.
+Array<cfloat, 3> compute_jacobian(const CompasContext& ctx, Array<cfloat, 2> echos, Array<cfloat, 2> delta_echos_T1,
+                                  Array<cfloat, 2> delta_echos_T2, TissueParameters parameters,
+                                  SpiralTrajectory trajectory, Array<cfloat, 2> coil_sensitivities,
+                                  Array<cfloat, 2> vector, JacobianComputeMethod) {
+    const int ns = trajectory.samples_per_readout, nreadouts = trajectory.nreadouts;
+    const int nvoxels = parameters.nvoxels, ncoils = int(coil_sensitivities.size(0));
+    check_jacobian_shapes(nreadouts, nvoxels, echos, delta_echos_T1, delta_echos_T2, coil_sensitivities);
+    COMPAS_CHECK(vector.size(0) == 4 && vector.size(1) == nvoxels);
+    COMPAS_CHECK(trajectory.k_start.size() == nreadouts && trajectory.delta_k.size() == nreadouts);
+    Array<cfloat, 3> Jv({ncoils, nreadouts, ns}, ctx.device(), ctx.stream());
+    launch_jacobian_spiral(ctx, parameters.data.data(), parameters.data.size(1), nvoxels, echos.data(),
+                           delta_echos_T1.data(), delta_echos_T2.data(), coil_sensitivities.data(), ncoils,
+                           vector.data(), nreadouts, ns, trajectory.delta_t, trajectory.k_start.data(),
+                           trajectory.delta_k.data(), Jv.data());
+    return Jv;
+}
+
+Array<cfloat, 2> compute_jacobian_hermitian(const CompasContext& ctx, Array<cfloat, 2> echos,
+                                            Array<cfloat, 2> delta_echos_T1, Array<cfloat, 2> delta_echos_T2,
+                                            TissueParameters parameters, SpiralTrajectory trajectory,
+                                            Array<cfloat, 2> coil_sensitivities, Array<cfloat, 3> vector,
+                                            JacobianComputeMethod) {
+    const int ns = trajectory.samples_per_readout, nreadouts = trajectory.nreadouts;
+    const int nvoxels = parameters.nvoxels, ncoils = int(coil_sensitivities.size(0));
+    check_jacobian_shapes(nreadouts, nvoxels, echos, delta_echos_T1, delta_echos_T2, coil_sensitivities);
+    COMPAS_CHECK(vector.size(0) == ncoils && vector.size(1) == nreadouts && vector.size(2) == ns);
+    COMPAS_CHECK(trajectory.k_start.size() == nreadouts && trajectory.delta_k.size() == nreadouts);
+    Array<cfloat, 2> JHv({4, nvoxels}, ctx.device(), ctx.stream());
+    launch_jacobian_hermitian_spiral(ctx, parameters.data.data(), parameters.data.size(1), nvoxels, echos.data(),
+                                     delta_echos_T1.data(), delta_echos_T2.data(), coil_sensitivities.data(), ncoils,
+                                     vector.data(), nreadouts, ns, trajectory.delta_t, trajectory.k_start.data(),
+                                     trajectory.delta_k.data(), JHv.data());
+    return JHv;
+}
+
 }  // namespace compas

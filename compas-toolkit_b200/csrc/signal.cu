@@ -197,9 +197,10 @@ constexpr int SP_THREADS = 128, SP_KPT = 8, SP_VCH = 64;
 
 // One block of the spiral signal: samples bx·SP_THREADS·SP_KPT.., readout r, coils cz·CT..
 // Shared by the one-operation kernel (blockIdx) and the batched kernel: bit-identical results.
-template<int CT>
+template<int CT, bool JAC = false>
 __device__ __forceinline__ void spiral_tile(const SpiralArgs& a, const int bx, const int r, const int cz) {
     __shared__ float2 sA[SP_VCH];
+    __shared__ float2 sAQ[JAC ? SP_VCH : 1];  // J·v: the (k - S/2)-weighted source
     __shared__ double sTurns[SP_VCH];
     __shared__ float sDecay[SP_VCH];
     __shared__ float2 sStep[SP_VCH];
@@ -217,7 +218,7 @@ __device__ __forceinline__ void spiral_tile(const SpiralArgs& a, const int bx, c
     for (int v0 = 0; v0 < a.nvoxels; v0 += SP_VCH) {
         for (int i = threadIdx.x; i < SP_VCH; i += SP_THREADS) {
             const int v = v0 + i;
-            float2 A = make_float2(0.f, 0.f), step = make_float2(0.f, 0.f);
+            float2 A = make_float2(0.f, 0.f), AQ = make_float2(0.f, 0.f), step = make_float2(0.f, 0.f);
             double turns = 0.0;
             float dec = 0.0f;
             if (v < a.nvoxels) {
@@ -229,12 +230,30 @@ __device__ __forceinline__ void spiral_tile(const SpiralArgs& a, const int bx, c
                 const double half = 0.5 * double(a.S) * double(a.dt);
                 const float2 rw = cis_rad(-half * twopi * double(B0) + double(ks.x) * double(x));
                 const float mag = expf(float(half) * R2);
-                A = cmul(cmul(a.echo[int64_t(r) * a.nvoxels + v], cscale(mag, rw)), rho);
+                if constexpr (!JAC) {
+                    A = cmul(cmul(a.echo[int64_t(r) * a.nvoxels + v], cscale(mag, rw)), rho);
+                } else {
+                    // J·v source (product_kernels.cuh:56-60 with the spiral factor): P = T1ρv0·∂T1m +
+                    // T2ρv1·∂T2m + (v2 + i v3)·m and Q = ΔtR2²·T2ρv1·m, both times the readout factor
+                    const float T1 = a.params[v];
+                    const int64_t idx = int64_t(r) * a.nvoxels + v;
+                    const float2 me = a.echo[idx], d1 = a.dT1[idx], d2 = a.dT2[idx];
+                    const float2 w0 = a.vec[v], w1 = a.vec[a.nvoxels + v];
+                    const float2 w2 = a.vec[2 * int64_t(a.nvoxels) + v], w3 = a.vec[3 * int64_t(a.nvoxels) + v];
+                    const float2 c1 = cmul(w0, cscale(T1, rho)), c2 = cmul(w1, cscale(T2, rho));
+                    const float2 cm = make_float2(w2.x - w3.y, w2.y + w3.x);
+                    const float2 P = cadd(cadd(cmul(c1, d1), cmul(c2, d2)), cmul(cm, me));
+                    const float2 Q = cmul(cscale(a.dt * R2 * R2, c2), me);
+                    const float2 rd = cscale(mag, rw);
+                    A = cmul(rd, P);
+                    AQ = cmul(rd, Q);
+                }
                 turns = (double(dkr.x) * x + double(dkr.y) * y + double(a.dt) * twopi * B0) * inv_2pi;
                 dec = -a.dt * R2;
                 step = cscale(__expf(dec), cis_turns(turns));
             }
             sA[i] = A;
+            if constexpr (JAC) sAQ[i] = AQ;
             sTurns[i] = turns;
             sDecay[i] = dec;
             sStep[i] = step;
@@ -249,16 +268,30 @@ __device__ __forceinline__ void spiral_tile(const SpiralArgs& a, const int bx, c
             for (int i = 0; i < nv; i++) {
                 const float2 ph = cis_turns(double(k0) * sTurns[i]);
                 const float m0 = __expf(float(k0) * sDecay[i]);
-                float2 e = cmul(sA[i], make_float2(m0 * ph.x, m0 * ph.y));
+                const float2 z0 = make_float2(m0 * ph.x, m0 * ph.y);
+                float2 e = cmul(sA[i], z0);
                 const float2 step = sStep[i];
                 float2 coil[CT];
 #pragma unroll
                 for (int c = 0; c < CT; c++) coil[c] = sCoil[c][i];
+                if constexpr (!JAC) {
 #pragma unroll
-                for (int j = 0; j < SP_KPT; j++) {
+                    for (int j = 0; j < SP_KPT; j++) {
 #pragma unroll
-                    for (int c = 0; c < CT; c++) acc[c][j] = cfma(coil[c], e, acc[c][j]);
-                    e = cmul(e, step);
+                        for (int c = 0; c < CT; c++) acc[c][j] = cfma(coil[c], e, acc[c][j]);
+                        e = cmul(e, step);
+                    }
+                } else {
+                    float2 f = cmul(sAQ[i], z0);
+#pragma unroll
+                    for (int j = 0; j < SP_KPT; j++) {
+                        const float kk = float(k0 + j) - 0.5f * float(a.S);
+                        const float2 t = make_float2(fmaf(kk, f.x, e.x), fmaf(kk, f.y, e.y));
+#pragma unroll
+                        for (int c = 0; c < CT; c++) acc[c][j] = cfma(coil[c], t, acc[c][j]);
+                        e = cmul(e, step);
+                        f = cmul(f, step);
+                    }
                 }
             }
         }
@@ -278,6 +311,12 @@ __device__ __forceinline__ void spiral_tile(const SpiralArgs& a, const int bx, c
 template<int CT>
 __global__ void __launch_bounds__(SP_THREADS) signal_spiral_kernel(SpiralArgs a) {
     spiral_tile<CT>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// J·v on a spiral trajectory (no counterpart in the reference, whose Jacobians are Cartesian only)
+template<int CT>
+__global__ void __launch_bounds__(SP_THREADS) jacobian_spiral_kernel(SpiralArgs a) {
+    spiral_tile<CT, true>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 __device__ __forceinline__ int job_of_block(const int* __restrict__ offsets, int njobs, int b) {
@@ -436,6 +475,39 @@ void launch_signal_spiral(const CompasContext& ctx, const float* params, int64_t
 // Coils per block for `ncoils` coils: minimises (blocks per readout) × (modelled instructions
 // per staged voxel and thread), where a block of CT coils costs 4·CT·8 FMAs for the products,
 // 8 complex steps and ~50 instructions for the start factor and shared-memory loads.
+void launch_jacobian_spiral(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
+                            const cfloat* echos, const cfloat* dT1, const cfloat* dT2, const cfloat* coils, int ncoils,
+                            const cfloat* vec, int nreadouts, int ns, float dt, const cfloat* k_start,
+                            const cfloat* delta_k, cfloat* Jv) {
+    if (int64_t(ncoils) * nreadouts * ns == 0) return;
+    kernels::SpiralArgs a {};
+    a.params = params;
+    a.pstride = pstride;
+    a.nvoxels = nvoxels;
+    a.echo = reinterpret_cast<const float2*>(echos);
+    a.dT1 = reinterpret_cast<const float2*>(dT1);
+    a.dT2 = reinterpret_cast<const float2*>(dT2);
+    a.vec = reinterpret_cast<const float2*>(vec);
+    a.coils = reinterpret_cast<const float2*>(coils);
+    a.R = nreadouts;
+    a.S = ns;
+    a.C = ncoils;
+    a.dt = dt;
+    a.k_start = reinterpret_cast<const float2*>(k_start);
+    a.delta_k = reinterpret_cast<const float2*>(delta_k);
+    a.signal = reinterpret_cast<float2*>(Jv);
+    DeviceGuard guard(ctx.device());
+    const int ct = spiral_coil_group(ncoils);
+    dim3 grid(div_ceil(ns, kernels::SP_THREADS * kernels::SP_KPT), nreadouts, div_ceil(ncoils, ct));
+    switch (ct) {
+        case 1: kernels::jacobian_spiral_kernel<1><<<grid, kernels::SP_THREADS, 0, ctx.stream()>>>(a); break;
+        case 2: kernels::jacobian_spiral_kernel<2><<<grid, kernels::SP_THREADS, 0, ctx.stream()>>>(a); break;
+        case 4: kernels::jacobian_spiral_kernel<4><<<grid, kernels::SP_THREADS, 0, ctx.stream()>>>(a); break;
+        default: kernels::jacobian_spiral_kernel<8><<<grid, kernels::SP_THREADS, 0, ctx.stream()>>>(a); break;
+    }
+    check_launch("jacobian_spiral_kernel");
+}
+
 int spiral_coil_group(int ncoils) {
     int best = 1;
     double best_cost = 1e300;

@@ -444,6 +444,19 @@ Array<cfloat, 2> compute_jacobian_hermitian(const CompasContext& ctx, Array<cflo
                                             Array<cfloat, 2> coil_sensitivities, Array<cfloat, 3> vector,
                                             JacobianComputeMethod kind = JacobianComputeMethod::Direct);
 
+// J·v and Jᴴ·v on a spiral trajectory (no counterpart in the reference, whose Jacobians take a
+// CartesianTrajectory only): the derivatives of the spiral signal model with the Cartesian
+// column scaling; FP32 kernels for every method
+Array<cfloat, 3> compute_jacobian(const CompasContext& ctx, Array<cfloat, 2> echos, Array<cfloat, 2> delta_echos_T1,
+                                  Array<cfloat, 2> delta_echos_T2, TissueParameters parameters,
+                                  SpiralTrajectory trajectory, Array<cfloat, 2> coil_sensitivities,
+                                  Array<cfloat, 2> vector, JacobianComputeMethod kind = JacobianComputeMethod::Direct);
+Array<cfloat, 2> compute_jacobian_hermitian(const CompasContext& ctx, Array<cfloat, 2> echos,
+                                            Array<cfloat, 2> delta_echos_T1, Array<cfloat, 2> delta_echos_T2,
+                                            TissueParameters parameters, SpiralTrajectory trajectory,
+                                            Array<cfloat, 2> coil_sensitivities, Array<cfloat, 3> vector,
+                                            JacobianComputeMethod kind = JacobianComputeMethod::Direct);
+
 // lhs - rhs and Σ|lhs - rhs|²   (compas/utils/residual.h:20-24)
 Array<cfloat, 3> compute_residual(CompasContext ctx, Array<cfloat, 3> lhs, Array<cfloat, 3> rhs,
                                   float* objective_out = nullptr);
