@@ -205,10 +205,12 @@ class CompasArray:
 
     @property
     def __cuda_array_interface__(self) -> dict:
-        """Zero-copy view for CUDA-aware libraries (e.g. torch.as_tensor(arr, device="cuda")); the
-        consumer orders its use after the context's stream, on which the array was produced."""
-        typestr = "<c8" if self.dtype == np.complex64 else "<f4"
-        return {"shape": self.shape, "typestr": typestr, "data": (self.device_ptr(), False), "version": 3,
+        """Zero-copy float32 view for CUDA-aware libraries (e.g. torch.as_tensor(arr, device="cuda"));
+        the consumer orders its use after the context's stream, on which the array was produced."""
+        # complex values are exposed as float32 pairs (trailing axis of 2): consumers differ in
+        # their support of complex type strings
+        shape = self.shape + (2,) if self.dtype == np.complex64 else self.shape
+        return {"shape": shape, "typestr": "<f4", "data": (self.device_ptr(), False), "version": 3,
                 "strides": None, "stream": int(self.context.stream) or None}
 
     def read_into(self, out: np.ndarray) -> np.ndarray:

@@ -104,8 +104,8 @@ def gpu_to_tensor(ctx):
     def fn(arr):
         lib_stream = torch.cuda.ExternalStream(ctx.stream)
         torch.cuda.current_stream().wait_stream(lib_stream)
-        view = torch.as_tensor(arr, device="cuda")  # zero-copy view of the library's buffer
-        out = torch.view_as_real(view).clone()
+        view = torch.as_tensor(arr, device="cuda")  # zero-copy float32 view [..., 2] of the buffer
+        out = view.clone()
         # the library releases `arr` on its own stream: order that after the copy
         lib_stream.wait_stream(torch.cuda.current_stream())
         return out
