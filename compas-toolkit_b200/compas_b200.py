@@ -210,7 +210,7 @@ class CompasArray:
         # complex values are exposed as float32 pairs (trailing axis of 2): consumers differ in
         # their support of complex type strings
         shape = self.shape + (2,) if self.dtype == np.complex64 else self.shape
-        return {"shape": shape, "typestr": "<f4", "data": (self.device_ptr(), False), "version": 3,
+        return {"shape": shape, "typestr": "<f4", "data": (self.device_ptr, False), "version": 3,
                 "strides": None, "stream": int(self.context.stream) or None}
 
     def read_into(self, out: np.ndarray) -> np.ndarray:
