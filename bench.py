@@ -396,8 +396,8 @@ def batched(cb, ctx, stream, args, rank):
 
 
 def served(cb, ctx, args):
-    """Served request stream: Poisson arrivals at each rate of reconstruction requests (simulate +
-    signal + residual, and for Cartesian trajectories the FD derivatives and Jᴴ·r) drawn from 12
+    """Served request stream: Poisson arrivals at each rate of reconstruction requests (simulate,
+    FD derivative simulations, signal, residual, Jᴴ·r) drawn from 12
     distinct requests (voxels logU[4k,200k], coils U{4..16}, FISP/pSSFP, Cartesian/spiral, TRs
     U{400..1120}) whose sequences, trajectories, coils and data stay resident; HBM budget 150 GB.
     Latency = submit -> results complete on the device, measured by the engine."""
@@ -416,7 +416,7 @@ def served(cb, ctx, args):
     rng = np.random.default_rng(6)
     out = {"workload": "12 distinct requests reused: voxels logU[4k,200k], coils U{4..16}, TRs U{400..1120}, "
                        "FISP (25 states, 35 positions) / pSSFP (35 z), Cartesian (S=sqrt V) / spiral (TRs x 1000); "
-                       "request = simulate + signal + residual (+ FD derivatives + J^H r for Cartesian)",
+                       "request = simulate + FD derivative simulations + signal + residual + J^H r",
            "memory_budget_gb": 150, "max_inflight_batches": 4, "max_batch_requests": 16, "runs": []}
 
     warmed = set()

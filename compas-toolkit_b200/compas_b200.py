@@ -541,8 +541,8 @@ class GaussNewtonStep(_Object):
 class ServeEngine(_Object):
     """compas_b200_make_server: continuous-batching request loop on one GPU.
 
-    submit() queues a reconstruction request (simulate -> signal -> residual against `data`, and
-    for Cartesian trajectories the gradient Jᴴ·r) and returns a ticket; wait() blocks for it.
+    submit() queues a reconstruction request (simulate -> signal -> residual against `data` and the
+    gradient Jᴴ·r with finite-difference derivatives) and returns a ticket; wait() blocks for it.
     Requests are admitted by estimated device footprint against the memory budget, run in
     batches (persistent work-queue simulations, batched signals) on up to
     `max_inflight_batches` streams at once, and give the same bits as the one-request calls."""
@@ -580,10 +580,8 @@ class ServeEngine(_Object):
                 "batch": batch.value}
 
     def result(self, ticket: int, which: str = "residual") -> CompasArray:
-        shape, nv, cart = self._meta[int(ticket)]
+        shape, nv, _ = self._meta[int(ticket)]
         idx = {"residual": 0, "gradient": 1}[which]
-        if idx == 1 and not cart:
-            raise CompasError("spiral requests have no gradient")
         ptr = library().compas_b200_server_result(self.ptr, int(ticket), idx)
         return _result(ptr, self.context, shape if idx == 0 else (4, nv), "compas_b200_server_result")
 

@@ -573,8 +573,11 @@ compas_object* compas_b200_make_gauss_newton(const compas_context* context, cons
         if (const auto* f = dynamic_cast<const compas::FISPSequence*>(seq)) s = *f;
         else if (const auto* p = dynamic_cast<const compas::pSSFPSequence*>(seq)) s = *p;
         else throw compas::CompasException(std::string("invalid sequence object: ") + seq->name());
-        return new_obj(compas::GaussNewtonStep(ctx, unwrap<compas::TissueParameters>(parameters), s,
-                                               unwrap<compas::CartesianTrajectory>(trajectory),
+        std::variant<compas::CartesianTrajectory, compas::SpiralTrajectory> t =
+            with_trajectory(trajectory, [](const auto& traj) {
+                return std::variant<compas::CartesianTrajectory, compas::SpiralTrajectory>(traj);
+            });
+        return new_obj(compas::GaussNewtonStep(ctx, unwrap<compas::TissueParameters>(parameters), s, t,
                                                array_of<cfloat, 2>(coils, "coils"), array_of<cfloat, 3>(data, "data"),
                                                cg_iterations, delta, jacobian_method(method)));
     });

@@ -152,7 +152,7 @@ struct GaussNewtonStep::Impl {
     TissueParameters params;   // the estimate, updated in place by every iteration
     Array<float, 2> perturbed;
     std::variant<FISPSequence, pSSFPSequence> sequence;
-    CartesianTrajectory trajectory;
+    std::variant<CartesianTrajectory, SpiralTrajectory> trajectory;
     Array<cfloat, 2> coils;
     Array<cfloat, 3> data;
     int cg_iterations = 4;
@@ -198,9 +198,30 @@ void GaussNewtonStep::Impl::enqueue() const {
     const int64_t nsig = signal.numel();
     const int64_t necho = echos.numel();
     const int C = int(coils.size(0));
-    const CartesianGeom geo = cartesian_geom(trajectory);
     const float* pdata = params.data.data();
     const int64_t pstride = params.data.size(1);
+    const auto* cart = std::get_if<CartesianTrajectory>(&trajectory);
+    const auto* spiral = std::get_if<SpiralTrajectory>(&trajectory);
+    const CartesianGeom geo = cart ? cartesian_geom(*cart) : CartesianGeom {};
+    // J·d and Jᴴ·b on the request's trajectory (spiral: the FP32 spiral kernels)
+    auto jv = [&](const cfloat* vec, cfloat* out) {
+        if (cart)
+            launch_jacobian(ctx, pdata, pstride, V, echos.data(), dT1.data(), dT2.data(), coils.data(), C, vec, geo, out,
+                            prec);
+        else
+            launch_jacobian_spiral(ctx, pdata, pstride, V, echos.data(), dT1.data(), dT2.data(), coils.data(), C, vec,
+                                   spiral->nreadouts, spiral->samples_per_readout, spiral->delta_t,
+                                   spiral->k_start.data(), spiral->delta_k.data(), out);
+    };
+    auto jhv = [&](const cfloat* vec, cfloat* out) {
+        if (cart)
+            launch_jacobian_hermitian(ctx, pdata, pstride, V, echos.data(), dT1.data(), dT2.data(), coils.data(), C,
+                                      vec, geo, out, prec);
+        else
+            launch_jacobian_hermitian_spiral(ctx, pdata, pstride, V, echos.data(), dT1.data(), dT2.data(),
+                                             coils.data(), C, vec, spiral->nreadouts, spiral->samples_per_readout,
+                                             spiral->delta_t, spiral->k_start.data(), spiral->delta_k.data(), out);
+    };
     cudaStream_t st = ctx.stream();
     const int eb = int(std::min<int64_t>((necho + 255) / 256, 148 * 16));
     const int sb = int(std::min<int64_t>((nsig + 255) / 256, 148 * 16));
@@ -221,20 +242,23 @@ void GaussNewtonStep::Impl::enqueue() const {
     }
 
     // residual b = y - s and the objective ‖b‖²
-    launch_signal_cartesian(ctx, pdata, pstride, V, echos.data(), coils.data(), C, geo, signal.data(), prec);
+    if (cart)
+        launch_signal_cartesian(ctx, pdata, pstride, V, echos.data(), coils.data(), C, geo, signal.data(), prec);
+    else
+        launch_signal_spiral(ctx, pdata, pstride, V, echos.data(), coils.data(), C, spiral->nreadouts,
+                             spiral->samples_per_readout, spiral->delta_t, spiral->k_start.data(),
+                             spiral->delta_k.data(), signal.data());
     launch_residual(ctx, data.data(), signal.data(), nsig, b.data(), partials.data(), npartials,
                     scalars.data() + kObjective);
 
     // CGLS, k iterations of one J·d and one Jᴴ·b each
-    launch_jacobian_hermitian(ctx, pdata, pstride, V, echos.data(), dT1.data(), dT2.data(), coils.data(), C, b.data(),
-                              geo, g.data(), prec);
+    jhv(b.data(), g.data());
     cg_start_kernel<<<vb, 256, 0, st>>>(reinterpret_cast<const float2*>(g.data()), nv4, x.data(),
                                         reinterpret_cast<float2*>(d.data()));
     check_launch("cg_start_kernel");
     norm2(g.data(), nv4, true, kGamma, 0);
     for (int it = 0; it < cg_iterations; it++) {
-        launch_jacobian(ctx, pdata, pstride, V, echos.data(), dT1.data(), dT2.data(), coils.data(), C, d.data(), geo,
-                        q.data(), prec);
+        jv(d.data(), q.data());
         norm2(q.data(), nsig, false, kQQ, 1);
         cg_step_x_kernel<<<vb, 256, 0, st>>>(x.data(), reinterpret_cast<const float2*>(d.data()), nv4,
                                              scalars.data());
@@ -243,8 +267,7 @@ void GaussNewtonStep::Impl::enqueue() const {
         cg_step_b_kernel<<<sb, 256, 0, st>>>(reinterpret_cast<float2*>(b.data()),
                                              reinterpret_cast<const float2*>(q.data()), nsig, scalars.data());
         check_launch("cg_step_b_kernel");
-        launch_jacobian_hermitian(ctx, pdata, pstride, V, echos.data(), dT1.data(), dT2.data(), coils.data(), C,
-                                  b.data(), geo, g.data(), prec);
+        jhv(b.data(), g.data());
         norm2(g.data(), nv4, true, kGammaNew, 2);
         cg_direction_kernel<<<vb, 256, 0, st>>>(reinterpret_cast<const float2*>(g.data()),
                                                 reinterpret_cast<float2*>(d.data()), nv4, scalars.data());
@@ -255,7 +278,8 @@ void GaussNewtonStep::Impl::enqueue() const {
 }
 
 GaussNewtonStep::GaussNewtonStep(const CompasContext& ctx, TissueParameters parameters,
-                                 std::variant<FISPSequence, pSSFPSequence> sequence, CartesianTrajectory trajectory,
+                                 std::variant<FISPSequence, pSSFPSequence> sequence,
+                                 std::variant<CartesianTrajectory, SpiralTrajectory> trajectory,
                                  Array<cfloat, 2> coil_sensitivities, Array<cfloat, 3> data, int cg_iterations,
                                  float delta, JacobianComputeMethod method) :
     m_impl(std::make_shared<Impl>(ctx)) {
@@ -263,7 +287,10 @@ GaussNewtonStep::GaussNewtonStep(const CompasContext& ctx, TissueParameters para
     const int dev = ctx.device();
     const int V = parameters.nvoxels;
     const int C = int(coil_sensitivities.size(0));
-    const int R = trajectory.nreadouts, S = trajectory.samples_per_readout;
+    const Trajectory& tr = std::holds_alternative<CartesianTrajectory>(trajectory)
+                               ? static_cast<const Trajectory&>(std::get<CartesianTrajectory>(trajectory))
+                               : static_cast<const Trajectory&>(std::get<SpiralTrajectory>(trajectory));
+    const int R = tr.nreadouts, S = tr.samples_per_readout;
     int nreadouts = 0;
     if (const auto* f = std::get_if<FISPSequence>(&sequence)) nreadouts = int(f->RF_train.size()) * f->undersampling_factor;
     else nreadouts = int(std::get<pSSFPSequence>(sequence).RF_train.size());

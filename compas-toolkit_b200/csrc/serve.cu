@@ -1,7 +1,7 @@
 // serve.cu — continuous-batching request loop for reconstruction requests on one GPU.
 //
-// A request asks for simulate → signal → residual (and, for Cartesian trajectories, the
-// finite-difference derivatives and the gradient Jᴴ·r). The reference has no serving layer:
+// A request asks for simulate → signal → residual, the finite-difference derivatives and the
+// gradient Jᴴ·r (Cartesian or spiral trajectory). The reference has no serving layer:
 // its callers issue these operations one call at a time (src/simulate/fisp.cu, pssfp.cu,
 // src/simulate/derivative.cu, src/trajectories/signal.cu, src/utils/residual.cu,
 // src/jacobian/hermitian.cu). Here:
@@ -156,14 +156,14 @@ size_t ServeEngine::Impl::estimate(const ServeRequest& r) const {
     const int64_t R = t.nreadouts, S = t.samples_per_readout, C = r.coil_sensitivities.size(0);
     const bool cart = std::holds_alternative<CartesianTrajectory>(r.trajectory);
     const int64_t echo = 8 * R * V, sig = 8 * C * R * S;
-    int64_t bytes = echo * (cart ? 3 : 1) + (cart ? 2 * 36 * V : 0);  // echoes, derivative echoes, T1/T2+Δ copies
+    int64_t bytes = echo * 3 + 2 * 36 * V;                            // echoes, derivative echoes, T1/T2+Δ copies
     bytes += 2 * sig;                                                  // signal, residual
     bytes += 40 * V + 8 * C * V;                                       // per-voxel tables, coil·w
     if (cart && signal_precision(opt.method) == Precision::SplitBF16) {
         const TcPlan p = tc_plan(ctx.device(), int(V), int(R), int(S), int(C), false);
         if (p.splits > 1) bytes += int64_t(p.splits) * sig;            // split-K partials of the signal
     }
-    if (cart) bytes += 32 * V * 17;                                    // gradient and its split partials
+    bytes += 32 * V * 17;                                              // gradient and its split partials
     return size_t(bytes + bytes / 16 + (1 << 20));
 }
 
@@ -214,10 +214,9 @@ void ServeEngine::Impl::launch(Slot& slot, std::vector<uint64_t> ids) {
     DeviceGuard guard(dev);
     for (size_t i = 0; i < n; i++) {
         const ServeRequest& r = ts[i]->request;
-        const bool cart = std::holds_alternative<CartesianTrajectory>(r.trajectory);
         if (r.echo_key != 0) {
             auto e = cache.find(r.echo_key);
-            if (e != cache.end() && (!cart || e->second.dT1.size() > 0)) {
+            if (e != cache.end()) {
                 e->second.users++;
                 run->cache_reads.push_back(r.echo_key);
                 cache_lru.splice(cache_lru.begin(), cache_lru, e->second.lru);
@@ -237,7 +236,7 @@ void ServeEngine::Impl::launch(Slot& slot, std::vector<uint64_t> ids) {
         job.coil_sensitivities = r.coil_sensitivities;
         main_job[i] = int(jobs.size());
         jobs.push_back(job);
-        if (cart) {
+        {  // derivative simulations at T1 + Δ and T2 + Δ
             const int V = r.parameters.nvoxels;
             for (int field = 0; field < 2; field++) {
                 Array<float, 2> p({TissueParameterField::NUM_FIELDS, V}, dev, slot.stream);
@@ -300,11 +299,18 @@ void ServeEngine::Impl::launch(Slot& slot, std::vector<uint64_t> ids) {
         const int np = residual_partial_count(ns);
         launch_residual(sctx, r.data.data(), run->signals[i].data(), ns, run->residuals[i].data(),
                         run->partials.data() + run->partial_offset[i], np, run->objectives.data() + i);
+        run->gradients[i] = Array<cfloat, 2>({4, V}, dev, slot.stream);
         if (const auto* cart = std::get_if<CartesianTrajectory>(&r.trajectory)) {
-            run->gradients[i] = Array<cfloat, 2>({4, V}, dev, slot.stream);
             launch_jacobian_hermitian(sctx, pd, ps, V, run->echos[i].data(), run->dT1[i].data(), run->dT2[i].data(),
                                       r.coil_sensitivities.data(), C, run->residuals[i].data(), cartesian_geom(*cart),
                                       run->gradients[i].data(), prec);
+        } else {
+            const auto& sp = std::get<SpiralTrajectory>(r.trajectory);
+            launch_jacobian_hermitian_spiral(sctx, pd, ps, V, run->echos[i].data(), run->dT1[i].data(),
+                                             run->dT2[i].data(), r.coil_sensitivities.data(), C,
+                                             run->residuals[i].data(), sp.nreadouts, sp.samples_per_readout,
+                                             sp.delta_t, sp.k_start.data(), sp.delta_k.data(),
+                                             run->gradients[i].data());
         }
     }
     COMPAS_CUDA_CHECK(cudaEventCreateWithFlags(&run->done, cudaEventDisableTiming));

@@ -504,8 +504,8 @@ class SimulationBatch: public Object {
 
 // A reconstruction request: simulate the echoes of `parameters` under `sequence`, form the
 // signal on `trajectory` with `coil_sensitivities`, the residual b = data - s and its norm, and
-// (Cartesian trajectories: the reference's Jacobians accept no other) the gradient Jᴴ·b with
-// forward-difference ∂m/∂T1, ∂m/∂T2. Requests with the same nonzero `echo_key` share echoes and
+// the gradient Jᴴ·b with forward-difference ∂m/∂T1, ∂m/∂T2 (on a spiral trajectory through the
+// spiral Jacobian, which the reference does not have). Requests with the same nonzero `echo_key` share echoes and
 // derivatives: while an entry is resident, a request with its key skips the simulations (the
 // caller guarantees that equal keys mean equal parameters and sequence).
 struct ServeRequest {
@@ -519,7 +519,7 @@ struct ServeRequest {
 
 struct ServeResult {
     Array<cfloat, 3> residual;  // data - s
-    Array<cfloat, 2> gradient;  // Jᴴ·(data - s) [4][nvoxels]; empty for spiral trajectories
+    Array<cfloat, 2> gradient;  // Jᴴ·(data - s) [4][nvoxels]
     float objective = 0;        // ‖data - s‖²
     double queued_ms = 0;       // submit → admitted to a batch
     double device_ms = 0;       // admitted → results complete on the device
@@ -582,7 +582,8 @@ class ServeEngine: public Object {
 class GaussNewtonStep: public Object {
   public:
     GaussNewtonStep(const CompasContext& ctx, TissueParameters parameters,
-                    std::variant<FISPSequence, pSSFPSequence> sequence, CartesianTrajectory trajectory,
+                    std::variant<FISPSequence, pSSFPSequence> sequence,
+                    std::variant<CartesianTrajectory, SpiralTrajectory> trajectory,
                     Array<cfloat, 2> coil_sensitivities, Array<cfloat, 3> data, int cg_iterations = 4,
                     float delta = DEFAULT_FINITE_DIFFERENCE_DELTA,
                     JacobianComputeMethod method = JacobianComputeMethod::GemmFast);

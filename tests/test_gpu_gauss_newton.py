@@ -106,3 +106,25 @@ def test_iterations_lower_the_objective(setup):
         objs.append(gn.objective())
     assert objs[-1] < 0.5 * objs[0], objs
     assert all(np.isfinite(objs))
+
+
+def test_spiral_iteration_graph_matches_eager_and_lowers_the_objective(setup):
+    # the same iteration on a spiral trajectory (spiral J·v / Jᴴ·v, an addition to the reference)
+    cb, ctx, start, seq, _, coils, _ = setup
+    rng = np.random.default_rng(23)
+    truth, _, _, _, _ = _problem()
+    traj = cb.SpiralTrajectory.from_dict(ctx, W.spiral(rng, 60, 40, 22.4, 4e-6))
+    p_true = cb.TissueParameters.from_soa(ctx, truth)
+    y = cb.magnetization_to_signal(ctx, cb.simulate_magnetization(ctx, p_true, seq), p_true, traj, coils).to_numpy()
+    eager = _gn(cb, ctx, start, seq, traj, coils, y, cg_iterations=3)
+    graph = _gn(cb, ctx, start, seq, traj, coils, y, cg_iterations=3)
+    objs = []
+    for it in range(3):
+        eager.run(graph=False)
+        graph.run(graph=True)
+        ctx.synchronize()
+        for name in ("parameters", "gradient", "step", "scalars"):
+            assert np.array_equal(eager.array(name).to_numpy(), graph.array(name).to_numpy()), (it, name)
+        objs.append(graph.objective())
+    assert objs[-1] < objs[0], objs
+

@@ -1,7 +1,7 @@
 """Continuous-batching serving engine (compas_b200_make_server / _submit / _wait).
 
-A request is simulate -> signal -> residual against measured data and, for Cartesian
-trajectories, the gradient Jᴴ·r with forward-difference derivatives. The tests submit a mix of
+A request is simulate -> signal -> residual against measured data and the gradient Jᴴ·r with
+forward-difference derivatives (Cartesian or spiral). The tests submit a mix of
 FISP/pSSFP, Cartesian/spiral requests of different sizes from several threads while batches are
 running, and check that every result (objective, residual, gradient) is bit-identical to the
 same request computed alone through the one-request operations; that requests larger than the
@@ -36,10 +36,9 @@ def _alone(cb, ctx, objs, d):
     s = cb.magnetization_to_signal(ctx, echos, params, traj, coils, method="MatmulFast")
     obj, diff = cb.compute_residual(ctx, d["data"], s)
     out = {"objective": obj, "residual": diff.to_numpy()}
-    if isinstance(traj, cb.CartesianTrajectory):
-        dd = cb.simulate_magnetization_derivatives(ctx, echos, params, seq)
-        out["gradient"] = cb.compute_jacobian_hermitian(ctx, echos, dd, params, traj, coils, diff,
-                                                        method="GemmFast").to_numpy()
+    dd = cb.simulate_magnetization_derivatives(ctx, echos, params, seq)
+    out["gradient"] = cb.compute_jacobian_hermitian(ctx, echos, dd, params, traj, coils, diff,
+                                                    method="GemmFast").to_numpy()
     return out
 
 
@@ -57,12 +56,11 @@ def env():
     return cb, ctx, dicts, objs, data, alone
 
 
-def _check_same(cb, eng, ticket, ref, is_cart, key):
+def _check_same(cb, eng, ticket, ref, key):
     info = eng.wait(ticket)
     assert info["objective"] == ref["objective"], key
     assert np.array_equal(eng.result(ticket, "residual").to_numpy(), ref["residual"]), key
-    if is_cart:
-        assert np.array_equal(eng.result(ticket, "gradient").to_numpy(), ref["gradient"]), key
+    assert np.array_equal(eng.result(ticket, "gradient").to_numpy(), ref["gradient"]), key
     return info
 
 
@@ -84,7 +82,7 @@ def test_mixed_requests_from_threads_match_alone_bitwise(env):
         th.join()
     batches = set()
     for i, d in enumerate(dicts):
-        info = _check_same(cb, eng, tickets[i], alone[i], d["traj"]["kind"] == "cartesian", i)
+        info = _check_same(cb, eng, tickets[i], alone[i], i)
         batches.add(info["batch"])
         assert info["latency_ms"] >= info["device_ms"] >= 0
         eng.release(tickets[i])
@@ -100,7 +98,7 @@ def test_budget_admission_and_oversized_request(env):
     eng = cb.ServeEngine(ctx, memory_budget_gb=0.02, max_inflight_batches=4, max_batch_requests=8)
     ts = [eng.submit(*objs[i], data[i]) for i in range(4)]
     for i, t in enumerate(ts):
-        _check_same(cb, eng, t, alone[i], dicts[i]["traj"]["kind"] == "cartesian", i)
+        _check_same(cb, eng, t, alone[i], i)
         eng.release(t)
     st = eng.stats()
     assert st["peak_bytes"] <= 0.02 * 2 ** 30
@@ -116,7 +114,7 @@ def test_echo_key_reuses_resident_echoes(env):
     i = next(k for k, d in enumerate(dicts) if d["traj"]["kind"] == "cartesian")
     eng = cb.ServeEngine(ctx, memory_budget_gb=4.0, echo_cache_gb=1.0)
     t1 = eng.submit(*objs[i], data[i], echo_key=77)
-    _check_same(cb, eng, t1, alone[i], True, "first")
+    _check_same(cb, eng, t1, alone[i], "first")
     t2 = eng.submit(*objs[i], data[i], echo_key=77)
-    _check_same(cb, eng, t2, alone[i], True, "cached")
+    _check_same(cb, eng, t2, alone[i], "cached")
     assert eng.stats()["echo_cache_hits"] == 1
