@@ -12,7 +12,9 @@
 //    pSSFP CTA fits in the registers a FISP CTA leaves free on an SM);
 //  * signal: after its family's simulation, the Cartesian signals of that family run as ONE
 //    batched split-BF16 tensor-core launch (plus one batched prep and one batched split-K
-//    sum), the spiral signals as one batched launch per coil grouping. A flattened CTA index is
+//    sum), the spiral signals on the split-BF16 tensor-core kernel one launch per job (each job's
+//    readouts × sample tiles fill the GPU), or with the FP32 method as one batched launch per coil
+//    grouping. A flattened CTA index is
 //    mapped to (job, tile) by a binary search over per-job CTA offsets; jobs are ordered by
 //    decreasing work per CTA. The voxel split of each job is the one it gets alone;
 //  * all device memory (echoes, signals, argument tables, split-K partials, per-voxel tables)
@@ -100,6 +102,7 @@ struct SimulationBatch::Impl {
         TcGroup tc;
         std::vector<SpiralGroup> spirals;
         std::vector<int> simt_cartesian;  // jobs whose Cartesian signal runs on the FP32 kernels
+        std::vector<int> tc_spiral;       // spiral jobs on the split-BF16 tensor-core kernel
         std::vector<int> empty_signals;   // jobs with no voxels: their signal is zero
     };
     Family families[2];  // 0: FISP (context stream), 1: pSSFP (side stream)
@@ -218,6 +221,8 @@ void SimulationBatch::Impl::plan_signal(Family& fam, const std::vector<int>& mem
         if (std::holds_alternative<CartesianTrajectory>(job.trajectory)) {
             if (prec == Precision::SplitBF16 && tensor_cores_available(dev)) tc_jobs.push_back(j);
             else fam.simt_cartesian.push_back(j);
+        } else if (prec == Precision::SplitBF16 && tensor_cores_available(dev)) {
+            fam.tc_spiral.push_back(j);  // one tensor-core launch per job (each fills the GPU alone)
         } else {
             const int cg = spiral_coil_group(C);
             spiral_by_group[cg == 1 ? 0 : cg == 2 ? 1 : cg == 4 ? 2 : 3].push_back(j);
@@ -347,6 +352,15 @@ void SimulationBatch::Impl::enqueue(const Family& fam, cudaStream_t stream, int*
     for (const auto& g : fam.spirals)
         launch_signal_spiral_batch(stream, dev, g.coil_group, as<kernels::SpiralArgs>(g.args), as<int>(g.cta_offsets),
                                    g.njobs, g.ctas);
+    const CompasContext sctx(dev, stream);
+    for (int j : fam.tc_spiral) {
+        const auto& job = jobs[size_t(j)];
+        const auto& t = std::get<SpiralTrajectory>(job.trajectory);
+        launch_signal_spiral(sctx, job.parameters.data.data(), job.parameters.data.size(1), job.parameters.nvoxels,
+                             echos[size_t(j)].data(), job.coil_sensitivities.data(),
+                             int(job.coil_sensitivities.size(0)), t.nreadouts, t.samples_per_readout, t.delta_t,
+                             t.k_start.data(), t.delta_k.data(), signals[size_t(j)].data(), Precision::SplitBF16);
+    }
 }
 
 SimulationBatch::SimulationBatch(const CompasContext& ctx, std::vector<SimulationJob> jobs,

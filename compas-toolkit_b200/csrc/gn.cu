@@ -211,7 +211,7 @@ void GaussNewtonStep::Impl::enqueue() const {
         else
             launch_jacobian_spiral(ctx, pdata, pstride, V, echos.data(), dT1.data(), dT2.data(), coils.data(), C, vec,
                                    spiral->nreadouts, spiral->samples_per_readout, spiral->delta_t,
-                                   spiral->k_start.data(), spiral->delta_k.data(), out);
+                                   spiral->k_start.data(), spiral->delta_k.data(), out, prec);
     };
     auto jhv = [&](const cfloat* vec, cfloat* out) {
         if (cart)
@@ -247,7 +247,7 @@ void GaussNewtonStep::Impl::enqueue() const {
     else
         launch_signal_spiral(ctx, pdata, pstride, V, echos.data(), coils.data(), C, spiral->nreadouts,
                              spiral->samples_per_readout, spiral->delta_t, spiral->k_start.data(),
-                             spiral->delta_k.data(), signal.data());
+                             spiral->delta_k.data(), signal.data(), prec);
     launch_residual(ctx, data.data(), signal.data(), nsig, b.data(), partials.data(), npartials,
                     scalars.data() + kObjective);
 

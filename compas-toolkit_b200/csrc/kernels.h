@@ -65,11 +65,11 @@ void launch_signal_cartesian(const CompasContext& ctx, const float* params, int6
                              cfloat* signal, Precision prec);
 void launch_signal_spiral(const CompasContext& ctx, const float* params, int64_t param_stride, int nvoxels,
                           const cfloat* echos, const cfloat* coils, int ncoils, int nreadouts, int ns, float dt,
-                          const cfloat* k_start, const cfloat* delta_k, cfloat* signal);
+                          const cfloat* k_start, const cfloat* delta_k, cfloat* signal, Precision prec);
 void launch_jacobian_spiral(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
                             const cfloat* echos, const cfloat* dT1, const cfloat* dT2, const cfloat* coils, int ncoils,
                             const cfloat* vec, int nreadouts, int ns, float dt, const cfloat* k_start,
-                            const cfloat* delta_k, cfloat* Jv);
+                            const cfloat* delta_k, cfloat* Jv, Precision prec);
 void launch_jacobian_hermitian_spiral(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
                                       const cfloat* echos, const cfloat* dT1, const cfloat* dT2,
                                       const cfloat* coils, int ncoils, const cfloat* vec, int nreadouts, int ns,

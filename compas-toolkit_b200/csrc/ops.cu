@@ -270,7 +270,7 @@ Array<cfloat, 3> magnetization_to_signal(const CompasContext& context, Array<cfl
         COMPAS_CHECK(sp->k_start.size() == nreadouts && sp->delta_k.size() == nreadouts);
         launch_signal_spiral(context, parameters.data.data(), parameters.data.size(1), nvoxels, echos.data(),
                              coil_sensitivities.data(), ncoils, nreadouts, ns, sp->delta_t, sp->k_start.data(),
-                             sp->delta_k.data(), signal.data());
+                             sp->delta_k.data(), signal.data(), signal_precision(method));
     } else {
         COMPAS_ERROR("invalid trajectory type");
     }
@@ -318,11 +318,12 @@ Array<cfloat, 2> compute_jacobian_hermitian(const CompasContext& ctx, Array<cflo
 }
 
 // Spiral trajectories (no counterpart in the reference, whose Jacobians take CartesianTrajectory
-// only): derived from the spiral signal model; plain FP32 SIMT kernels for every method.
+// only): derived from the spiral signal model. J·v: split-BF16 tensor cores for GemmFast/GemmLow,
+// FP32 otherwise; Jᴴ·v: FP32 for every method.
 Array<cfloat, 3> compute_jacobian(const CompasContext& ctx, Array<cfloat, 2> echos, Array<cfloat, 2> delta_echos_T1,
                                   Array<cfloat, 2> delta_echos_T2, TissueParameters parameters,
                                   SpiralTrajectory trajectory, Array<cfloat, 2> coil_sensitivities,
-                                  Array<cfloat, 2> vector, JacobianComputeMethod) {
+                                  Array<cfloat, 2> vector, JacobianComputeMethod kind) {
     const int ns = trajectory.samples_per_readout, nreadouts = trajectory.nreadouts;
     const int nvoxels = parameters.nvoxels, ncoils = int(coil_sensitivities.size(0));
     check_jacobian_shapes(nreadouts, nvoxels, echos, delta_echos_T1, delta_echos_T2, coil_sensitivities);
@@ -332,7 +333,7 @@ Array<cfloat, 3> compute_jacobian(const CompasContext& ctx, Array<cfloat, 2> ech
     launch_jacobian_spiral(ctx, parameters.data.data(), parameters.data.size(1), nvoxels, echos.data(),
                            delta_echos_T1.data(), delta_echos_T2.data(), coil_sensitivities.data(), ncoils,
                            vector.data(), nreadouts, ns, trajectory.delta_t, trajectory.k_start.data(),
-                           trajectory.delta_k.data(), Jv.data());
+                           trajectory.delta_k.data(), Jv.data(), jacobian_precision(kind));
     return Jv;
 }
 

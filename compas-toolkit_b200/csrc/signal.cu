@@ -443,9 +443,9 @@ void launch_jacobian_simt(const CompasContext& ctx, const float* params, int64_t
     run_signal_gemm<kernels::GenMode::Jacobian>(ctx, a, Jv);
 }
 
-void launch_signal_spiral(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
-                          const cfloat* echos, const cfloat* coils, int ncoils, int nreadouts, int ns, float dt,
-                          const cfloat* k_start, const cfloat* delta_k, cfloat* signal) {
+void launch_signal_spiral_simt(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
+                               const cfloat* echos, const cfloat* coils, int ncoils, int nreadouts, int ns, float dt,
+                               const cfloat* k_start, const cfloat* delta_k, cfloat* signal) {
     if (int64_t(ncoils) * nreadouts * ns == 0) return;
     kernels::SpiralArgs a {};
     a.params = params;
@@ -475,10 +475,10 @@ void launch_signal_spiral(const CompasContext& ctx, const float* params, int64_t
 // Coils per block for `ncoils` coils: minimises (blocks per readout) × (modelled instructions
 // per staged voxel and thread), where a block of CT coils costs 4·CT·8 FMAs for the products,
 // 8 complex steps and ~50 instructions for the start factor and shared-memory loads.
-void launch_jacobian_spiral(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
-                            const cfloat* echos, const cfloat* dT1, const cfloat* dT2, const cfloat* coils, int ncoils,
-                            const cfloat* vec, int nreadouts, int ns, float dt, const cfloat* k_start,
-                            const cfloat* delta_k, cfloat* Jv) {
+void launch_jacobian_spiral_simt(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
+                                 const cfloat* echos, const cfloat* dT1, const cfloat* dT2, const cfloat* coils,
+                                 int ncoils, const cfloat* vec, int nreadouts, int ns, float dt,
+                                 const cfloat* k_start, const cfloat* delta_k, cfloat* Jv) {
     if (int64_t(ncoils) * nreadouts * ns == 0) return;
     kernels::SpiralArgs a {};
     a.params = params;
@@ -548,4 +548,35 @@ void launch_sum_partials_batch(cudaStream_t stream, int device, const kernels::P
     check_launch("sum_partials_batch_kernel");
 }
 
+bool launch_signal_spiral_tc(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
+                             const cfloat* echos, const cfloat* coils, int ncoils, int nreadouts, int ns, float dt,
+                             const cfloat* k_start, const cfloat* delta_k, cfloat* signal);
+bool launch_jacobian_spiral_tc(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
+                               const cfloat* echos, const cfloat* dT1, const cfloat* dT2, const cfloat* coils,
+                               int ncoils, const cfloat* vec, int nreadouts, int ns, float dt, const cfloat* k_start,
+                               const cfloat* delta_k, cfloat* Jv);
+
+void launch_signal_spiral(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
+                          const cfloat* echos, const cfloat* coils, int ncoils, int nreadouts, int ns, float dt,
+                          const cfloat* k_start, const cfloat* delta_k, cfloat* signal, Precision prec) {
+    if (prec == Precision::SplitBF16 && launch_signal_spiral_tc(ctx, params, pstride, nvoxels, echos, coils, ncoils,
+                                                                nreadouts, ns, dt, k_start, delta_k, signal))
+        return;
+    launch_signal_spiral_simt(ctx, params, pstride, nvoxels, echos, coils, ncoils, nreadouts, ns, dt, k_start, delta_k,
+                              signal);
+}
+
+void launch_jacobian_spiral(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
+                            const cfloat* echos, const cfloat* dT1, const cfloat* dT2, const cfloat* coils, int ncoils,
+                            const cfloat* vec, int nreadouts, int ns, float dt, const cfloat* k_start,
+                            const cfloat* delta_k, cfloat* Jv, Precision prec) {
+    if (prec == Precision::SplitBF16 && launch_jacobian_spiral_tc(ctx, params, pstride, nvoxels, echos, dT1, dT2,
+                                                                  coils, ncoils, vec, nreadouts, ns, dt, k_start,
+                                                                  delta_k, Jv))
+        return;
+    launch_jacobian_spiral_simt(ctx, params, pstride, nvoxels, echos, dT1, dT2, coils, ncoils, vec, nreadouts, ns, dt,
+                                k_start, delta_k, Jv);
+}
+
 }  // namespace compas
+

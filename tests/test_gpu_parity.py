@@ -195,17 +195,23 @@ def test_signal_mrstat_scale_sampled(cb, ctx, oracle, workloads, method):
     assert oracle.rel_l2(got, ref) < tol
 
 
-def test_signal_spiral(cb, ctx, oracle, workloads):
-    rng = np.random.default_rng(8)
+@pytest.mark.parametrize("nc", [1, 3, 11, 20])
+@pytest.mark.parametrize("method", [None, "MatmulFast", "Direct"])
+def test_signal_spiral(cb, ctx, oracle, workloads, method, nc):
+    # None: the reference's spiral C-ABI entry point (split-BF16 tensor cores here, like the
+    # Cartesian entry point with low_precision = 0); 300 samples = 3 ragged sample tiles; 3/11/20
+    # coils = one 8-coil group, one 16-coil group, two 16-coil groups
+    rng = np.random.default_rng(8 + nc)
     p = workloads.tissue(rng, 9, 22.4)
     traj = workloads.spiral(rng, 13, 300, 22.4, 4e-6)
-    coils = workloads.cn(rng, (3, 81))
+    coils = workloads.cn(rng, (nc, 81))
     echo = workloads.cn(rng, (13, 81))
     params = cb.TissueParameters.from_soa(ctx, p)
     t = cb.trajectory_from_dict(ctx, traj)
-    got = cb.magnetization_to_signal(ctx, echo, params, t, coils).to_numpy()
+    got = cb.magnetization_to_signal(ctx, echo, params, t, coils, method=method).to_numpy()
     ref = oracle.signal_spiral(echo, p, traj, coils)
-    assert oracle.rel_l2(got, ref) < TOL_FP32
+    tol = TOL_FP32 if method == "Direct" else TOL_BF16X3
+    assert oracle.rel_l2(got, ref) < tol
 
 
 # ------------------------------------------------------------------------------------------------

@@ -1,8 +1,8 @@
 """J·v and Jᴴ·v on spiral trajectories (an addition: the reference's Jacobians accept Cartesian
 trajectories only). The GPU kernels are checked against the oracle's derivation from the spiral
 signal model (itself pinned by adjointness and finite differences in test_oracle.py) within the FP32
-tolerance of the other tests, through the reference C-ABI entry points, which dispatch on the
-trajectory type; plus adjointness on the GPU. Sizes cross the kernels' tile boundaries: samples
+tolerance (FP32 kernels) or the split-BF16 tolerance (tensor-core J·v), through the C-ABI entry
+points, which dispatch on the trajectory type; plus adjointness on the GPU. Sizes cross the kernels' tile boundaries: samples
 past one 1024-sample block and 64-sample chunks, coil counts 1, 3, 5 and 9 (coil groups of 1, 4, 8
 and 8+1), enough readouts for the Jᴴ·v readout splits."""
 import numpy as np
@@ -13,6 +13,7 @@ import workloads as W
 pytestmark = pytest.mark.gpu
 
 TOL_FP32 = 1e-5
+TOL_BF16X3 = 1e-4
 
 
 def _case(seed, nv, nr, ns, nc):
@@ -35,17 +36,22 @@ def ctx():
     return cb.Context(0)
 
 
-@pytest.mark.parametrize("nc,ns", [(1, 1100), (3, 150), (5, 70), (9, 130)])
-def test_spiral_jacobian_matches_oracle(ctx, oracle, nc, ns):
+@pytest.mark.parametrize("method", ["Direct", "GemmFast"])
+@pytest.mark.parametrize("nc,ns", [(1, 1100), (3, 150), (5, 70), (9, 130), (18, 40)])
+def test_spiral_jacobian_matches_oracle(ctx, oracle, nc, ns, method):
+    # Direct: FP32 SIMT kernel; GemmFast: split-BF16 tensor-core kernel (the C-ABI entry point's choice)
     import compas_b200 as cb
 
     p, traj_d, coils, echo, d1, d2, v, u = _case(40 + nc, 150, 9, ns, nc)
     params = cb.TissueParameters.from_soa(ctx, p)
     traj = cb.SpiralTrajectory.from_dict(ctx, traj_d)
     d = {"T1": d1, "T2": d2}
-    got = cb.compute_jacobian(ctx, echo, d, params, traj, coils, v).to_numpy()
+    got = cb.compute_jacobian(ctx, echo, d, params, traj, coils, v, method=method).to_numpy()
     ref = oracle.spiral_jacobian(echo, d1, d2, p, traj_d, coils, v)
-    assert oracle.rel_l2(got, ref) < TOL_FP32
+    assert oracle.rel_l2(got, ref) < (TOL_FP32 if method == "Direct" else TOL_BF16X3)
+    if method == "GemmFast":
+        via_abi = cb.compute_jacobian(ctx, echo, d, params, traj, coils, v).to_numpy()
+        assert np.array_equal(via_abi, got)
 
 
 @pytest.mark.parametrize("nc,nr,ns", [(1, 33, 100), (3, 12, 130), (9, 40, 70)])
@@ -71,7 +77,7 @@ def test_spiral_adjointness_on_gpu(ctx):
     params = cb.TissueParameters.from_soa(ctx, p)
     traj = cb.SpiralTrajectory.from_dict(ctx, traj_d)
     d = {"T1": d1, "T2": d2}
-    Jv = cb.compute_jacobian(ctx, echo, d, params, traj, coils, v).to_numpy().astype(np.complex128)
+    Jv = cb.compute_jacobian(ctx, echo, d, params, traj, coils, v, method="Direct").to_numpy().astype(np.complex128)
     JHu = cb.compute_jacobian_hermitian(ctx, echo, d, params, traj, coils, u).to_numpy().astype(np.complex128)
     lhs = np.vdot(u.astype(np.complex128), Jv)
     rhs = np.vdot(JHu, v.astype(np.complex128))
