@@ -78,6 +78,10 @@ struct TcArgs {
     const VoxelGen* vgen;         // [V] per-voxel generation constants (prep kernel)
     const float2* coilw;          // [C][V] coil·w
     const float4* jcoef;          // J·v only: [V][2] {T1ρv0, T2ρv1}, {v2 + i v3, ΔtR2²·T2ρv1}
+    // A operand already split and laid out as shared-memory stage images (tc_pack_a_kernel):
+    // block (readout tile, voxel stage) = hi then lo plane, 16 KB each; nullptr: convert in-kernel
+    const unsigned char* apack;
+    int apack_stages;             // voxel stages per readout tile in apack
 };
 
 // one split-K reduction: out[i] = Σ_q partials[q·n + i], q = 0..nsplit-1 in order

@@ -46,6 +46,7 @@ constexpr int TC_A_BYTES = TC_M * TC_K * 2;  // 16 KB per hi/lo plane
 constexpr int TC_B_BYTES = TC_N * TC_K * 2;  // 32 KB per hi/lo plane
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
 constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 128 /*barriers*/;
+constexpr int TC_APACK_BLOCK = 2 * TC_A_BYTES;  // hi + lo image of one (readout tile, voxel stage)
 
 
 
@@ -91,6 +92,44 @@ __global__ void tc_prep_kernel(TcArgs a, VoxelGen* vgen, float2* coilw, float4* 
     tc_prep_voxel<JAC>(a, blockIdx.x * blockDim.x + threadIdx.x, vgen, coilw, jcoef);
 }
 
+// Pack the A operand once per call as the shared-memory images the contraction consumes: element
+// (readout r, column g) with g = 32·stage + j (signal: voxel g; J·v: voxel g/2, term g%2 = P or Q')
+// is split into hi/lo BF16 and stored at the swizzled position of row r % 128, column j in block
+// (r / 128, stage). Rows past R and columns past V are zero. Every contraction CTA of a readout
+// tile then loads each stage with one bulk copy instead of converting it again (once per pair tile).
+template<bool JAC>
+__global__ void tc_pack_a_kernel(TcArgs a, unsigned char* __restrict__ pack) {
+    constexpr int TERMS = JAC ? 2 : 1;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int rp = blockIdx.y;  // padded readout row
+    if (g >= a.apack_stages * 32) return;
+    const int stage = g >> 5, j = g & 31;
+    const int v = g / TERMS;
+    float2 e = make_float2(0.f, 0.f);
+    if (rp < a.R && v < a.nvoxels) {
+        const int64_t idx = int64_t(rp) * a.nvoxels + v;
+        if constexpr (!JAC) {
+            e = a.echo[idx];
+        } else {
+            const float4 k0 = a.jcoef[2 * int64_t(v)], k1 = a.jcoef[2 * int64_t(v) + 1];
+            const float2 me = a.echo[idx];
+            if ((g & 1) == 0) {
+                const float2 d1 = a.dT1[idx], d2 = a.dT2[idx];
+                e = cadd(cadd(cmul(make_float2(k0.x, k0.y), d1), cmul(make_float2(k0.z, k0.w), d2)),
+                         cmul(make_float2(k1.x, k1.y), me));
+            } else {
+                e = cmul(make_float2(k1.z, k1.w), me);
+            }
+        }
+    }
+    uint32_t h, l;
+    tc::split2(e.x, e.y, h, l);
+    unsigned char* blk = pack + (int64_t(rp >> 7) * a.apack_stages + stage) * TC_APACK_BLOCK;
+    const uint32_t off = tc::sw128_offset(rp & 127, j >> 2) + uint32_t(j & 3) * 4;
+    *reinterpret_cast<uint32_t*>(blk + off) = h;
+    *reinterpret_cast<uint32_t*>(blk + TC_A_BYTES + off) = l;
+}
+
 // One output tile (pair tile bx, readout tile by, voxel split bz) of one contraction. Shared by
 // the one-operation kernel (tile = blockIdx) and the batched kernel, so both give bit-identical
 // results.
@@ -105,8 +144,10 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + TC_STAGES * TC_STAGE_BYTES);
     uint64_t* empty = full + TC_STAGES;
     uint64_t* done = empty + TC_STAGES;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    uint64_t* afull = done + 1;  // packed A: the stage's bulk copy has landed
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(afull + TC_STAGES);
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+    const bool packed = a.apack != nullptr;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int n_pair0 = bx * (TC_N / 2);                  // first (c,k) pair of this tile
@@ -119,8 +160,9 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_STAGES; s++) {
-            tc::mbar_init(&full[s], 512);
+            tc::mbar_init(&full[s], packed ? 256 : 512);
             tc::mbar_init(&empty[s], 1);
+            tc::mbar_init(&afull[s], 1);
         }
         tc::mbar_init(done, 1);
         *abort_flag = 0;
@@ -132,7 +174,26 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp < 8) {
+    if (warp < 8 && packed) {
+        // ---------------- A from the packed images: one bulk copy (hi + lo, 32 KB) per stage
+        if (threadIdx.x == 0) {
+            const unsigned char* src = a.apack + (int64_t(by) * a.apack_stages + v_begin / VPS) * TC_APACK_BLOCK;
+            int issued[TC_STAGES];
+            for (int s = 0; s < TC_STAGES; s++) issued[s] = -1;
+            for (int it = 0; it < nstages; it++) {
+                const int buf = it % TC_STAGES;
+                if (!tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status)) *abort_flag = 1;
+                if (*(volatile int*)abort_flag) break;
+                tc::mbar_arrive_expect_tx(&afull[buf], TC_APACK_BLOCK);
+                tc::bulk_copy_g2s(smem + buf * TC_STAGE_BYTES, src + int64_t(it) * TC_APACK_BLOCK, TC_APACK_BLOCK,
+                                  &afull[buf]);
+                issued[buf] = it;
+            }
+            // copies still in flight land before the CTA can finish (bounded)
+            for (int s = 0; s < TC_STAGES; s++)
+                if (issued[s] >= 0) tc::mbar_wait(&afull[s], (issued[s] / TC_STAGES) & 1, a.status);
+        }
+    } else if (warp < 8) {
         // ---------------- A producer: 128 readouts × VPS voxels → BF16 hi/lo, swizzled.
         // thread → (16-byte chunk along K, readouts rsub + 32·pass); the next stage's global
         // loads are issued before the current stage is converted and stored.
@@ -303,6 +364,7 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
             for (int it = 0; it < nstages; it++) {
                 const int buf = it % TC_STAGES;
                 if (!tc::mbar_wait(&full[buf], (it / TC_STAGES) & 1, a.status)) *abort_flag = 1;
+                if (packed && !tc::mbar_wait(&afull[buf], (it / TC_STAGES) & 1, a.status)) *abort_flag = 1;
                 if (*(volatile int*)abort_flag) break;
                 tc::tc_fence_after();
                 const uint32_t base = tc::smem_u32(smem + buf * TC_STAGE_BYTES);
@@ -500,6 +562,24 @@ bool run_tc(const CompasContext& ctx, kernels::TcArgs a, bool jac, cfloat* out) 
             a, reinterpret_cast<kernels::VoxelGen*>(vgen.data()), reinterpret_cast<float2*>(coilw.data()), nullptr);
     }
     check_launch("tc_prep_kernel");
+    // pack A once when several pair tiles would each convert it (it then costs one pass over the
+    // echoes instead of `ntiles` conversions)
+    const int vps = jac ? 16 : 32;
+    const int apack_stages = div_ceil(a.nvoxels, vps);
+    const bool pack = ntiles >= 2;
+    Array<unsigned char> apack({pack ? int64_t(mtiles) * apack_stages * kernels::TC_APACK_BLOCK : 0}, ctx.device(),
+                               ctx.stream());
+    a.apack = nullptr;
+    a.apack_stages = apack_stages;
+    if (pack) {
+        dim3 pgrid(div_ceil(apack_stages * 32, 256), mtiles * kernels::TC_M);
+        if (jac)
+            kernels::tc_pack_a_kernel<true><<<pgrid, 256, 0, ctx.stream()>>>(a, apack.data());
+        else
+            kernels::tc_pack_a_kernel<false><<<pgrid, 256, 0, ctx.stream()>>>(a, apack.data());
+        check_launch("tc_pack_a_kernel");
+        a.apack = apack.data();
+    }
     auto fn = jac ? kernels::tc_contract_kernel<true> : kernels::tc_contract_kernel<false>;
     set_tc_smem_attribute(jac, false);
     dim3 grid(ntiles, mtiles, splits);
