@@ -88,9 +88,9 @@ struct SimulationBatch::Impl {
         int head = 0;
     };
     struct TcGroup {
-        Array<unsigned char> args, prep_offsets, cta_offsets, sums, sum_offsets;
-        int njobs = 0, prep_blocks = 0, ctas = 0, nsums = 0, sum_blocks = 0;
-        std::vector<Array<unsigned char>> scratch;  // per-voxel tables and partials
+        Array<unsigned char> args, prep_offsets, pack_offsets, cta_offsets, sums, sum_offsets;
+        int njobs = 0, prep_blocks = 0, pack_blocks = 0, ctas = 0, nsums = 0, sum_blocks = 0;
+        std::vector<Array<unsigned char>> scratch;  // per-voxel tables, packed A and partials
     };
     struct SpiralGroup {
         int coil_group;
@@ -245,7 +245,7 @@ void SimulationBatch::Impl::plan_signal(Family& fam, const std::vector<int>& mem
         std::stable_sort(es.begin(), es.end(), [](const Entry& a, const Entry& b) { return a.plan.vchunk > b.plan.vchunk; });
         TcGroup& g = fam.tc;
         std::vector<kernels::TcArgs> args;
-        std::vector<int64_t> prep_counts, cta_counts, sum_counts;
+        std::vector<int64_t> prep_counts, pack_counts, cta_counts, sum_counts;
         std::vector<kernels::PartialSum> sums;
         for (const auto& e : es) {
             const auto& job = jobs[size_t(e.job)];
@@ -256,11 +256,9 @@ void SimulationBatch::Impl::plan_signal(Family& fam, const std::vector<int>& mem
                                                cartesian_geom(t));
             a.vchunk = e.plan.vchunk;
             a.status = detail::device_status_word(dev);
-            Array<unsigned char> vgen({int64_t(V) * int64_t(sizeof(kernels::VoxelGen))}, dev, ctx.stream());
-            Array<unsigned char> coilw({int64_t(C) * V * int64_t(sizeof(float2))}, dev, ctx.stream());
-            a.vgen = reinterpret_cast<const kernels::VoxelGen*>(vgen.data());
-            a.coilw = reinterpret_cast<const float2*>(coilw.data());
-            a.jcoef = nullptr;
+            const TcTables tables = tc_tables(V, t.nreadouts, t.samples_per_readout, C, false);
+            Array<unsigned char> scratch({tables.bytes}, dev, ctx.stream());
+            tc_assign_tables(a, tables, scratch.data());
             const int64_t n = int64_t(C) * t.nreadouts * t.samples_per_readout;
             float2* out = reinterpret_cast<float2*>(signals[size_t(e.job)].data());
             if (e.plan.splits > 1) {
@@ -272,10 +270,10 @@ void SimulationBatch::Impl::plan_signal(Family& fam, const std::vector<int>& mem
             } else {
                 a.out = out;
             }
-            g.scratch.push_back(std::move(vgen));
-            g.scratch.push_back(std::move(coilw));
+            g.scratch.push_back(std::move(scratch));
             args.push_back(a);
             prep_counts.push_back(div_ceil(V, 128));
+            pack_counts.push_back(tc_pack_blocks(t.nreadouts, a.apack_stages));
             cta_counts.push_back(int64_t(e.plan.ntiles) * e.plan.mtiles * e.plan.splits);
         }
         int64_t total = 0;
@@ -283,6 +281,8 @@ void SimulationBatch::Impl::plan_signal(Family& fam, const std::vector<int>& mem
         g.args = upload_table(ctx, args);
         g.prep_offsets = upload_table(ctx, prefix(prep_counts, &total));
         g.prep_blocks = int(total);
+        g.pack_offsets = upload_table(ctx, prefix(pack_counts, &total));
+        g.pack_blocks = int(total);
         g.cta_offsets = upload_table(ctx, prefix(cta_counts, &total));
         g.ctas = int(total);
         g.nsums = int(sums.size());
@@ -345,7 +345,7 @@ void SimulationBatch::Impl::enqueue(const Family& fam, cudaStream_t stream, int*
     const auto& tc = fam.tc;
     if (tc.njobs > 0) {
         launch_tc_batch(stream, dev, false, as<kernels::TcArgs>(tc.args), tc.njobs, as<int>(tc.prep_offsets),
-                        tc.prep_blocks, as<int>(tc.cta_offsets), tc.ctas);
+                        tc.prep_blocks, as<int>(tc.pack_offsets), tc.pack_blocks, as<int>(tc.cta_offsets), tc.ctas);
         launch_sum_partials_batch(stream, dev, as<kernels::PartialSum>(tc.sums), as<int>(tc.sum_offsets), tc.nsums,
                                   tc.sum_blocks);
     }

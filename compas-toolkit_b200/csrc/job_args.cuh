@@ -53,14 +53,6 @@ struct SpiralArgs {
     const float2* vec;
 };
 
-// per-voxel constants of the generated operand (written by tc_prep_kernel)
-struct VoxelGen {
-    double theta;  // Θ_v = Δk_re·x + Δk_im·y + 2πΔt·B0 (rad per sample)
-    float2 step;   // e^{-Δt/T2 + iΘ_v}
-    float decay;   // -Δt/T2
-    int valid;
-};
-
 struct TcArgs {
     const float* params;
     int64_t pstride;
@@ -75,13 +67,16 @@ struct TcArgs {
     int vchunk;           // voxels per split
     float2* out;          // [splits][C][R][S]
     unsigned int* status;
-    const VoxelGen* vgen;         // [V] per-voxel generation constants (prep kernel)
-    const float2* coilw;          // [C][V] coil·w
-    const float4* jcoef;          // J·v only: [V][2] {T1ρv0, T2ρv1}, {v2 + i v3, ΔtR2²·T2ρv1}
-    // A operand already split and laid out as shared-memory stage images (tc_pack_a_kernel):
-    // block (readout tile, voxel stage) = hi then lo plane, 16 KB each; nullptr: convert in-kernel
+    // tables written by the prep kernel:
+    const float2* vstep;   // [V] e^{-Δt/T2 + iΘ_v}, the per-sample step of E_k
+    const float2* estart;  // [S / egk][V] E_k exactly (FP64-reduced phase) at k = 0, egk, 2·egk, …
+    int egk;               // restart granularity: TC_PPG when it divides S, else 1
+    const float2* coilw;   // [C][V] coil·w
+    const float4* jcoef;   // J·v only: [V][2] {T1ρv0, T2ρv1}, {v2 + i v3, ΔtR2²·T2ρv1}
+    // A operand split and laid out as shared-memory stage images (tc_pack_a): block (readout
+    // tile, voxel stage) = hi then lo plane, 16 KB each
     const unsigned char* apack;
-    int apack_stages;             // voxel stages per readout tile in apack
+    int apack_stages;      // voxel stages per readout tile in apack
 };
 
 // one split-K reduction: out[i] = Σ_q partials[q·n + i], q = 0..nsplit-1 in order

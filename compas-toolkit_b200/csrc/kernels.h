@@ -100,9 +100,20 @@ TcPlan tc_plan(int device, int nvoxels, int R, int S, int C, bool jac);
 // argument block of a Cartesian signal contraction; out / vchunk / status / tables set by the caller
 kernels::TcArgs tc_signal_args(const float* params, int64_t pstride, int nvoxels, const cfloat* echos,
                                const cfloat* coils, int ncoils, const CartesianGeom& g);
-// batched prep (prep_blocks flattened 128-thread blocks) and contraction (ctas flattened CTAs)
+// device scratch of one contraction, carved from one allocation (byte offsets, 256-aligned):
+// per-voxel E_k step and restart values, coil·w, J·v coefficients and the packed A images
+struct TcTables {
+    int64_t vstep, estart, coilw, jcoef, apack, bytes;
+    int egk, apack_stages;
+};
+TcTables tc_tables(int nvoxels, int R, int S, int C, bool jac);
+void tc_assign_tables(kernels::TcArgs& a, const TcTables& t, unsigned char* base);
+int tc_pack_blocks(int R, int apack_stages);  // 256-thread blocks of one job's A packing
+// batched prep (prep_blocks flattened 128-thread blocks), A packing (pack_blocks flattened
+// 256-thread blocks) and contraction (ctas flattened CTAs)
 void launch_tc_batch(cudaStream_t stream, int device, bool jac, const kernels::TcArgs* jobs, int njobs,
-                     const int* prep_offsets, int prep_blocks, const int* cta_offsets, int ctas);
+                     const int* prep_offsets, int prep_blocks, const int* pack_offsets, int pack_blocks,
+                     const int* cta_offsets, int ctas);
 
 // ---- batched spiral signal and split-K sums -----------------------------------------------
 int spiral_coil_group(int ncoils);  // coils per block (1, 2, 4 or 8) of the spiral kernel

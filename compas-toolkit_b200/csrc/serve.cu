@@ -162,6 +162,7 @@ size_t ServeEngine::Impl::estimate(const ServeRequest& r) const {
     if (cart && signal_precision(opt.method) == Precision::SplitBF16) {
         const TcPlan p = tc_plan(ctx.device(), int(V), int(R), int(S), int(C), false);
         if (p.splits > 1) bytes += int64_t(p.splits) * sig;            // split-K partials of the signal
+        bytes += tc_tables(int(V), int(R), int(S), int(C), false).bytes;  // E_k tables and packed A
     }
     bytes += 32 * V * 17;                                              // gradient and its split partials
     return size_t(bytes + bytes / 16 + (1 << 20));

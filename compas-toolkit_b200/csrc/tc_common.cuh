@@ -75,6 +75,11 @@ __device__ __forceinline__ int bar_red_or(int id, int count, int pred) {
     return out;
 }
 
+// named barrier over `count` threads (a multiple of 32; every participant passes the same id)
+__device__ __forceinline__ void bar_sync(int id, int count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
 // arrive on `bar` and add `bytes` to the transaction count its phase waits for
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)

@@ -13,16 +13,19 @@
 // product is accumulated in FP32 TMEM as hi·hi + hi·lo + lo·hi (three tcgen05.mma per K step);
 // the dropped lo·lo term is ≤ 2⁻¹⁶ relative, giving ~1e-5 relative L2 against FP64.
 //
-// CTA organisation (544 threads, 1 CTA/SM, 192 KB shared memory in 2 pipeline stages):
-//   warps 0-7   convert the A tile (128 readouts × 64 K) from the FP32 echoes into BF16 hi/lo,
-//               128-byte swizzled K-major (next stage's loads in flight during the stores);
-//               warps 0-3 afterwards drain the TMEM accumulator;
-//   warps 8-15  generate the B tile (256 rows × 64 K): E_k by an exact FP64-reduced start and a
-//               complex recurrence along k, times the per-voxel coil·w factor;
-//   warp 16     allocates 256 TMEM columns and one lane issues the 12 MMAs per stage.
-// Per-voxel constants (phase step, decay, coil·w, J·v coefficients) come from a small prep kernel.
-// Stages hand over through mbarriers (full: producers → MMA, empty: tcgen05.commit → producers).
-// The voxel range is split over CTAs (split-K); partial tiles are summed in a fixed order.
+// Per call, small kernels first write per-voxel tables (the E_k step, E_k itself at every
+// TC_PPG-th sample with the phase reduced in FP64, coil·w, the J·v coefficients) and pack A once
+// as the split, swizzled shared-memory images the contraction consumes.
+// CTA organisation of the contraction (576 threads, 1 CTA/SM, 192 KB shared memory in 2 stages):
+//   warps 0-15  generate the B tile (256 rows × 64 K): thread = (2 voxels, group of TC_PPG pairs);
+//               a group starts from the exact E_k table value × coil·w and steps along k with the
+//               complex recurrence. Afterwards they drain the TMEM accumulator through shared
+//               memory into coalesced rows of the output;
+//   warp 16     allocates 256 TMEM columns and one lane issues the 12 MMAs per stage;
+//   warp 17     one lane loads each stage's A image (32 KB) with one bulk copy.
+// Stages hand over through mbarriers (full: producers → MMA, afull: copy landed, empty:
+// tcgen05.commit → producers and copy). The voxel range is split over CTAs (split-K); partial
+// tiles are summed in a fixed order. Every wait is bounded.
 #include <cuda_bf16.h>
 
 #include <mutex>
@@ -39,40 +42,53 @@ void sum_partials(const CompasContext& ctx, const cfloat* partials, int nsplit, 
 
 namespace kernels {
 
-constexpr int TC_M = 128, TC_N = 256, TC_K = 64;  // real-ified tile; TC_N/2 = 128 complex pairs
-constexpr int TC_THREADS = 544;  // 8 A-producer + 8 B-producer warps + 1 MMA warp
+constexpr int TC_M = 128, TC_N = 256, TC_K = 64;  // real-ified tile
+constexpr int TC_PAIRS = TC_N / 2;                 // complex (c, k) pairs per tile
+constexpr int TC_PPG = 4;                          // consecutive pairs per producer thread
+constexpr int TC_B_THREADS = 512;                  // 16 producer warps: 16 voxel halves × 32 groups
+constexpr int TC_MMA_WARP = 16, TC_COPY_WARP = 17;
+constexpr int TC_THREADS = 576;
 constexpr int TC_STAGES = 2;
 constexpr int TC_A_BYTES = TC_M * TC_K * 2;  // 16 KB per hi/lo plane
 constexpr int TC_B_BYTES = TC_N * TC_K * 2;  // 32 KB per hi/lo plane
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
 constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 128 /*barriers*/;
 constexpr int TC_APACK_BLOCK = 2 * TC_A_BYTES;  // hi + lo image of one (readout tile, voxel stage)
+constexpr int TC_TROW = TC_PAIRS + 2;           // float2 per row of the transposed output tile
+static_assert(TC_PAIRS == (TC_B_THREADS / 16) * TC_PPG, "producer groups cover the pair tile");
+static_assert(TC_M * TC_TROW * 8 <= TC_STAGES * TC_STAGE_BYTES, "output tile fits the stage buffers");
+static_assert((TC_TROW * 8) % 16 == 0, "transposed rows stay 16-byte aligned");
 
-
-
-// one thread per voxel: generation constants, coil·w for every coil and (J·v) the four complex
-// coefficients of P and Q' — done once per call instead of once per CTA and stage
+// one thread per voxel: the E_k step, E_k at the restart points, coil·w for every coil and
+// (J·v) the four complex coefficients of P and Q' — once per call instead of per CTA and stage
 template<bool JAC>
-__device__ __forceinline__ void tc_prep_voxel(const TcArgs& a, const int v, VoxelGen* vgen, float2* coilw,
-                                              float4* jcoef) {
+__device__ __forceinline__ void tc_prep_voxel(const TcArgs& a, const int v) {
     if (v >= a.nvoxels) return;
     const double twopi = 6.283185307179586476925;
     const float T1 = a.params[v], T2 = a.params[a.pstride + v], B0 = a.params[3 * a.pstride + v];
     const float x = a.params[6 * a.pstride + v], y = a.params[7 * a.pstride + v];
     const float2 rho = make_float2(a.params[4 * a.pstride + v], a.params[5 * a.pstride + v]);
-    VoxelGen g;
-    g.theta = double(a.dk_re) * x + double(a.dk_im) * y + double(a.dt) * twopi * B0;
-    g.decay = -a.dt / T2;
-    const float2 st = cis_rad(g.theta);
-    const float sm = __expf(g.decay);
-    g.step = make_float2(sm * st.x, sm * st.y);
-    g.valid = 1;
-    vgen[v] = g;
+    // Θ_v = Δk_re·x + Δk_im·y + 2πΔt·B0 (rad per sample), decay -Δt/T2 per sample
+    const double theta = double(a.dk_re) * x + double(a.dk_im) * y + double(a.dt) * twopi * B0;
+    const float decay = -a.dt / T2;
+    const float2 st = cis_rad(theta);
+    const float sm = __expf(decay);
+    const_cast<float2*>(a.vstep)[v] = make_float2(sm * st.x, sm * st.y);
+    // E_k = e^{(k - S/2)(decay + iΘ)} at k = q·egk, the phase argument reduced modulo 2π in FP64
+    float2* estart = const_cast<float2*>(a.estart);
+    const int nq = a.S / a.egk;
+    for (int q = 0; q < nq; q++) {
+        const float ks = float(q * a.egk) - 0.5f * float(a.S);
+        const float2 ph = cis_rad(double(ks) * theta);
+        const float mg = __expf(ks * decay);
+        estart[int64_t(q) * a.nvoxels + v] = make_float2(mg * ph.x, mg * ph.y);
+    }
     float2 w = make_float2(1.f, 0.f);
     if constexpr (!JAC) {
         w = rho;
         if (a.dk_im != 0.0f) w = cmul(w, cis_rad(0.5 * double(a.S) * double(a.dk_im) * y));
     }
+    float2* coilw = const_cast<float2*>(a.coilw);
     for (int c = 0; c < a.C; c++) coilw[int64_t(c) * a.nvoxels + v] = cmul(a.coils[int64_t(c) * a.nvoxels + v], w);
     if constexpr (JAC) {
         // P = c1·∂T1m + c2·∂T2m + cm·m,  Q' = cq·m   (product_kernels.cuh:56-60, dE/dT2 folded)
@@ -82,27 +98,26 @@ __device__ __forceinline__ void tc_prep_voxel(const TcArgs& a, const int v, Voxe
         const float2 cm = make_float2(w2.x - w3.y, w2.y + w3.x);
         const float R2 = 1.0f / T2;
         const float2 cq = cscale(a.dt * R2 * R2, c2);
+        float4* jcoef = const_cast<float4*>(a.jcoef);
         jcoef[2 * int64_t(v)] = make_float4(c1.x, c1.y, c2.x, c2.y);
         jcoef[2 * int64_t(v) + 1] = make_float4(cm.x, cm.y, cq.x, cq.y);
     }
 }
 
 template<bool JAC>
-__global__ void tc_prep_kernel(TcArgs a, VoxelGen* vgen, float2* coilw, float4* jcoef) {
-    tc_prep_voxel<JAC>(a, blockIdx.x * blockDim.x + threadIdx.x, vgen, coilw, jcoef);
+__global__ void tc_prep_kernel(TcArgs a) {
+    tc_prep_voxel<JAC>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Pack the A operand once per call as the shared-memory images the contraction consumes: element
 // (readout r, column g) with g = 32·stage + j (signal: voxel g; J·v: voxel g/2, term g%2 = P or Q')
 // is split into hi/lo BF16 and stored at the swizzled position of row r % 128, column j in block
 // (r / 128, stage). Rows past R and columns past V are zero. Every contraction CTA of a readout
-// tile then loads each stage with one bulk copy instead of converting it again (once per pair tile).
+// tile then loads each stage with one bulk copy.
 template<bool JAC>
-__global__ void tc_pack_a_kernel(TcArgs a, unsigned char* __restrict__ pack) {
-    constexpr int TERMS = JAC ? 2 : 1;
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    const int rp = blockIdx.y;  // padded readout row
+__device__ __forceinline__ void tc_pack_a(const TcArgs& a, const int g, const int rp) {
     if (g >= a.apack_stages * 32) return;
+    constexpr int TERMS = JAC ? 2 : 1;
     const int stage = g >> 5, j = g & 31;
     const int v = g / TERMS;
     float2 e = make_float2(0.f, 0.f);
@@ -124,10 +139,16 @@ __global__ void tc_pack_a_kernel(TcArgs a, unsigned char* __restrict__ pack) {
     }
     uint32_t h, l;
     tc::split2(e.x, e.y, h, l);
-    unsigned char* blk = pack + (int64_t(rp >> 7) * a.apack_stages + stage) * TC_APACK_BLOCK;
+    unsigned char* blk = const_cast<unsigned char*>(a.apack) + (int64_t(rp >> 7) * a.apack_stages + stage) * TC_APACK_BLOCK;
     const uint32_t off = tc::sw128_offset(rp & 127, j >> 2) + uint32_t(j & 3) * 4;
     *reinterpret_cast<uint32_t*>(blk + off) = h;
     *reinterpret_cast<uint32_t*>(blk + TC_A_BYTES + off) = l;
+}
+
+// grid (columns / 256, padded readout rows)
+template<bool JAC>
+__global__ void tc_pack_a_kernel(TcArgs a) {
+    tc_pack_a<JAC>(a, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
 }
 
 // One output tile (pair tile bx, readout tile by, voxel split bz) of one contraction. Shared by
@@ -138,29 +159,26 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
                                         unsigned char* smem_raw) {
     constexpr int TERMS = JAC ? 2 : 1;            // complex terms per voxel along K
     constexpr int VPS = TC_K / (2 * TERMS);       // voxels per stage (32 or 16)
-    constexpr int VPC = 4 / TERMS;                // voxels per 16-byte chunk (4 or 2)
-    constexpr int VPH = VPC / 2;                  // voxels per 8-byte half chunk (2 or 1)
+    constexpr int VPH = 2 / TERMS;                // voxels per 8-byte half chunk (2 or 1)
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + TC_STAGES * TC_STAGE_BYTES);
     uint64_t* empty = full + TC_STAGES;
-    uint64_t* done = empty + TC_STAGES;
-    uint64_t* afull = done + 1;  // packed A: the stage's bulk copy has landed
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(afull + TC_STAGES);
+    uint64_t* afull = empty + TC_STAGES;  // the stage's A bulk copy has landed
+    uint64_t* done = afull + TC_STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
-    const bool packed = a.apack != nullptr;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n_pair0 = bx * (TC_N / 2);                  // first (c,k) pair of this tile
+    const int n_pair0 = bx * TC_PAIRS;  // first (c,k) pair of this tile
     const int r0 = by * TC_M;
-    const int split = bz;
-    const int v_begin = split * a.vchunk;
+    const int v_begin = bz * a.vchunk;
     const int v_end = min(a.nvoxels, v_begin + a.vchunk);
     const int nstages = max(1, (v_end - v_begin + VPS - 1) / VPS);
     const int npairs = a.C * a.S;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_STAGES; s++) {
-            tc::mbar_init(&full[s], packed ? 256 : 512);
+            tc::mbar_init(&full[s], TC_B_THREADS);
             tc::mbar_init(&empty[s], 1);
             tc::mbar_init(&afull[s], 1);
         }
@@ -168,15 +186,15 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
         *abort_flag = 0;
         tc::fence_mbarrier_init();
     }
-    if (warp == 16) tc::tmem_alloc(tmem_slot, 256);
+    if (warp == TC_MMA_WARP) tc::tmem_alloc(tmem_slot, 256);
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp < 8 && packed) {
-        // ---------------- A from the packed images: one bulk copy (hi + lo, 32 KB) per stage
-        if (threadIdx.x == 0) {
+    if (warp == TC_COPY_WARP) {
+        // ---------------- A: one bulk copy (hi + lo, 32 KB) per stage
+        if (lane == 0) {
             const unsigned char* src = a.apack + (int64_t(by) * a.apack_stages + v_begin / VPS) * TC_APACK_BLOCK;
             int issued[TC_STAGES];
             for (int s = 0; s < TC_STAGES; s++) issued[s] = -1;
@@ -193,178 +211,14 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
             for (int s = 0; s < TC_STAGES; s++)
                 if (issued[s] >= 0) tc::mbar_wait(&afull[s], (issued[s] / TC_STAGES) & 1, a.status);
         }
-    } else if (warp < 8) {
-        // ---------------- A producer: 128 readouts × VPS voxels → BF16 hi/lo, swizzled.
-        // thread → (16-byte chunk along K, readouts rsub + 32·pass); the next stage's global
-        // loads are issued before the current stage is converted and stored.
-        const int t = threadIdx.x;
-        const int chunk = t & 7, rsub = t >> 3;
-        float x[TC_M / 32][8];
-        auto load_stage = [&](int it) {
-            const int v0 = v_begin + it * VPS + VPC * chunk;
-            if constexpr (!JAC) {
-#pragma unroll
-                for (int pass = 0; pass < TC_M / 32; pass++) {
-                    const int r = r0 + rsub + 32 * pass;
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        const int v = v0 + q;
-                        float2 e = make_float2(0.f, 0.f);
-                        if (r < a.R && v < v_end) e = __ldg(a.echo + int64_t(r) * a.nvoxels + v);
-                        x[pass][2 * q] = e.x;
-                        x[pass][2 * q + 1] = e.y;
-                    }
-                }
-            } else {
-                float4 k0[2], k1[2];
-#pragma unroll
-                for (int q = 0; q < 2; q++) {
-                    const int v = v0 + q;
-                    k0[q] = k1[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (v < v_end) {
-                        k0[q] = __ldg(a.jcoef + 2 * int64_t(v));
-                        k1[q] = __ldg(a.jcoef + 2 * int64_t(v) + 1);
-                    }
-                }
-#pragma unroll
-                for (int pass = 0; pass < TC_M / 32; pass++) {
-                    const int r = r0 + rsub + 32 * pass;
-#pragma unroll
-                    for (int q = 0; q < 2; q++) {
-                        const int v = v0 + q;
-                        float2 P = make_float2(0.f, 0.f), Q = P;
-                        if (r < a.R && v < v_end) {
-                            const int64_t idx = int64_t(r) * a.nvoxels + v;
-                            const float2 me = __ldg(a.echo + idx), d1 = __ldg(a.dT1 + idx), d2 = __ldg(a.dT2 + idx);
-                            P = cadd(cadd(cmul(make_float2(k0[q].x, k0[q].y), d1), cmul(make_float2(k0[q].z, k0[q].w), d2)),
-                                     cmul(make_float2(k1[q].x, k1[q].y), me));
-                            Q = cmul(make_float2(k1[q].z, k1[q].w), me);
-                        }
-                        x[pass][4 * q] = P.x;
-                        x[pass][4 * q + 1] = P.y;
-                        x[pass][4 * q + 2] = Q.x;
-                        x[pass][4 * q + 3] = Q.y;
-                    }
-                }
-            }
-        };
-        load_stage(0);
-        for (int it = 0; it < nstages; it++) {
-            const int buf = it % TC_STAGES;
-            if (!tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status)) *abort_flag = 1;
-            if (*(volatile int*)abort_flag) break;
-            unsigned char* Ah = smem + buf * TC_STAGE_BYTES;
-            unsigned char* Al = Ah + TC_A_BYTES;
-            uint32_t h[TC_M / 32][4], l[TC_M / 32][4];
-#pragma unroll
-            for (int pass = 0; pass < TC_M / 32; pass++)
-#pragma unroll
-                for (int q = 0; q < 4; q++) tc::split2(x[pass][2 * q], x[pass][2 * q + 1], h[pass][q], l[pass][q]);
-            if (it + 1 < nstages) load_stage(it + 1);  // in flight while the stores below run
-#pragma unroll
-            for (int pass = 0; pass < TC_M / 32; pass++) {
-                const uint32_t off = tc::sw128_offset(rsub + 32 * pass, chunk);
-                *reinterpret_cast<uint4*>(Ah + off) = make_uint4(h[pass][0], h[pass][1], h[pass][2], h[pass][3]);
-                *reinterpret_cast<uint4*>(Al + off) = make_uint4(l[pass][0], l[pass][1], l[pass][2], l[pass][3]);
-            }
-            tc::fence_async_shared();
-            tc::mbar_arrive(&full[buf]);
-        }
-    } else if (warp < 16) {
-        // ---------------- B producer: 128 pairs × VPS voxels of F = coil·w·E_k.
-        // thread → (8-byte half chunk hq = VPH voxels, group pg of 8 consecutive pairs)
-        const int t = threadIdx.x - 256;
-        const int hq = t & 15, pg = t >> 4;
-        const int n_first = n_pair0 + pg * 8;
-        const int c_first = n_first / a.S, k_first = n_first - c_first * a.S;
-        VoxelGen vg[VPH], vg_next[VPH];
-        auto load_gen = [&](int it, VoxelGen (&dst)[VPH]) {
-#pragma unroll
-            for (int i = 0; i < VPH; i++) {
-                const int v = v_begin + it * VPS + VPH * hq + i;
-                if (v < v_end) {
-                    dst[i] = a.vgen[v];
-                } else {
-                    dst[i].theta = 0.0;
-                    dst[i].step = make_float2(0.f, 0.f);
-                    dst[i].decay = 0.0f;
-                    dst[i].valid = 0;
-                }
-            }
-        };
-        load_gen(0, vg);
-        for (int it = 0; it < nstages; it++) {
-            const int buf = it % TC_STAGES;
-            const int vbase = v_begin + it * VPS + VPH * hq;
-            if (it + 1 < nstages) load_gen(it + 1, vg_next);
-            if (!tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status)) *abort_flag = 1;
-            if (*(volatile int*)abort_flag) break;
-            unsigned char* Bh = smem + buf * TC_STAGE_BYTES + 2 * TC_A_BYTES;
-            unsigned char* Bl = Bh + TC_B_BYTES;
-            int c = c_first, k = k_first;
-            bool restart = true;
-            float2 G[VPH];
-#pragma unroll 2
-            for (int jj = 0; jj < 8; jj++) {
-                const int j = pg * 8 + jj;
-                const bool pok = (n_first + jj) < npairs;
-                const float ks = float(k) - 0.5f * float(a.S);
-                if (restart) {
-#pragma unroll
-                    for (int i = 0; i < VPH; i++) {
-                        G[i] = make_float2(0.f, 0.f);
-                        if (pok && vg[i].valid) {
-                            const float2 ph = cis_rad(double(ks) * vg[i].theta);
-                            const float mg = __expf(ks * vg[i].decay);
-                            G[i] = cmul(make_float2(mg * ph.x, mg * ph.y), __ldg(a.coilw + int64_t(c) * a.nvoxels + vbase + i));
-                        }
-                    }
-                }
-                uint32_t h0[2], l0[2], h1[2], l1[2];
-                if constexpr (!JAC) {
-#pragma unroll
-                    for (int i = 0; i < 2; i++) {
-                        const float2 F = pok ? G[i] : make_float2(0.f, 0.f);
-                        tc::split2(F.x, -F.y, h0[i], l0[i]);
-                        tc::split2(F.y, F.x, h1[i], l1[i]);
-                    }
-                } else {
-                    const float2 F = pok ? G[0] : make_float2(0.f, 0.f);
-                    tc::split2(F.x, -F.y, h0[0], l0[0]);
-                    tc::split2(ks * F.x, -ks * F.y, h0[1], l0[1]);
-                    tc::split2(F.y, F.x, h1[0], l1[0]);
-                    tc::split2(ks * F.y, ks * F.x, h1[1], l1[1]);
-                }
-                const uint32_t o0 = tc::sw128_offset(2 * j, hq >> 1) + (hq & 1) * 8;
-                const uint32_t o1 = tc::sw128_offset(2 * j + 1, hq >> 1) + (hq & 1) * 8;
-                *reinterpret_cast<uint2*>(Bh + o0) = make_uint2(h0[0], h0[1]);
-                *reinterpret_cast<uint2*>(Bl + o0) = make_uint2(l0[0], l0[1]);
-                *reinterpret_cast<uint2*>(Bh + o1) = make_uint2(h1[0], h1[1]);
-                *reinterpret_cast<uint2*>(Bl + o1) = make_uint2(l1[0], l1[1]);
-                // next pair: same coil → one recurrence step, new coil → exact restart
-                if (++k == a.S) {
-                    k = 0;
-                    ++c;
-                    restart = true;
-                } else {
-                    restart = false;
-#pragma unroll
-                    for (int i = 0; i < VPH; i++) G[i] = cmul(G[i], vg[i].step);
-                }
-            }
-            tc::fence_async_shared();
-            tc::mbar_arrive(&full[buf]);
-#pragma unroll
-            for (int i = 0; i < VPH; i++) vg[i] = vg_next[i];
-        }
-    } else {
-        // ---------------- MMA issuer (warp 16, lane 0)
+    } else if (warp == TC_MMA_WARP) {
+        // ---------------- MMA issuer (one lane)
         if (lane == 0) {
             constexpr uint32_t idesc = tc::idesc_bf16_f32(TC_M, TC_N);
             for (int it = 0; it < nstages; it++) {
                 const int buf = it % TC_STAGES;
                 if (!tc::mbar_wait(&full[buf], (it / TC_STAGES) & 1, a.status)) *abort_flag = 1;
-                if (packed && !tc::mbar_wait(&afull[buf], (it / TC_STAGES) & 1, a.status)) *abort_flag = 1;
+                if (!tc::mbar_wait(&afull[buf], (it / TC_STAGES) & 1, a.status)) *abort_flag = 1;
                 if (*(volatile int*)abort_flag) break;
                 tc::tc_fence_after();
                 const uint32_t base = tc::smem_u32(smem + buf * TC_STAGE_BYTES);
@@ -382,45 +236,148 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
                 tc::mma_commit(&empty[buf]);
             }
             tc::mma_commit(done);
+            tc::mbar_wait(done, 0, a.status);  // the MMAs finish before the TMEM is released
         }
         __syncwarp();
-    }
-
-    // ---------------- epilogue: warps 0-3 drain TMEM rows 32w..32w+31
-    if (warp < 4) {
-        const bool waited = tc::mbar_wait(done, 0, a.status);
-        tc::tc_fence_after();
-        // tcgen05.ld is .sync.aligned: the whole warp takes the same branch
-        const bool ok = __all_sync(0xffffffffu, waited && !*(volatile int*)abort_flag);
-        if (ok) {
-            const int r = r0 + warp * 32 + lane;
-            float2* outp = a.out + int64_t(split) * npairs * a.R;
-#pragma unroll 1
-            for (int qq = 0; qq < TC_N / 32; qq++) {
-                float v[32];
-                tc::tmem_load32(tmem + (uint32_t(warp * 32) << 16) + uint32_t(qq * 32), v);
-                if (r < a.R) {
-                    int n = n_pair0 + qq * 16;
-                    int c = n / a.S, k = n - c * a.S;
+    } else {
+        // ---------------- B producers: TC_PAIRS pairs × VPS voxels of F = coil·w·E_k per stage.
+        // thread → (8-byte half chunk hq = VPH voxels, group pg of TC_PPG consecutive pairs)
+        const int t = threadIdx.x;
+        const int hq = t & 15, pg = t >> 4;
+        const int n_first = n_pair0 + pg * TC_PPG;
+        const int c_first = n_first / a.S, k_first = n_first - c_first * a.S;
+        const bool group_ok = n_first < npairs;
+        // the group's start value E_{k_first} (k_first is a multiple of egk), step and coil·w
+        // travel one stage ahead of their use
+        const float2* e_row = a.estart + int64_t(k_first / a.egk) * a.nvoxels;
+        const float2* w_row = a.coilw + int64_t(c_first) * a.nvoxels;
+        float2 step[VPH], e0[VPH], cw[VPH], step_n[VPH], e0_n[VPH], cw_n[VPH];
+        auto load_gen = [&](int it, float2 (&st)[VPH], float2 (&ee)[VPH], float2 (&ww)[VPH]) {
 #pragma unroll
-                    for (int i = 0; i < 16; i++) {
-                        if (n + i < npairs) outp[(int64_t(c) * a.R + r) * a.S + k] = make_float2(v[2 * i], v[2 * i + 1]);
-                        if (++k == a.S) {
-                            k = 0;
-                            ++c;
-                        }
-                    }
+            for (int i = 0; i < VPH; i++) {
+                const int v = v_begin + it * VPS + VPH * hq + i;
+                st[i] = ee[i] = ww[i] = make_float2(0.f, 0.f);
+                if (group_ok && v < v_end) {
+                    st[i] = __ldg(a.vstep + v);
+                    ee[i] = __ldg(e_row + v);
+                    ww[i] = __ldg(w_row + v);
                 }
             }
+        };
+        load_gen(0, step, e0, cw);
+        for (int it = 0; it < nstages; it++) {
+            const int buf = it % TC_STAGES;
+            const int vbase = v_begin + it * VPS + VPH * hq;
+            if (it + 1 < nstages) load_gen(it + 1, step_n, e0_n, cw_n);
+            if (!tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status)) *abort_flag = 1;
+            if (*(volatile int*)abort_flag) break;
+            unsigned char* Bh = smem + buf * TC_STAGE_BYTES + 2 * TC_A_BYTES;
+            unsigned char* Bl = Bh + TC_B_BYTES;
+            float2 G[VPH];
+#pragma unroll
+            for (int i = 0; i < VPH; i++) G[i] = cmul(e0[i], cw[i]);
+            int c = c_first, k = k_first;
+#pragma unroll
+            for (int jj = 0; jj < TC_PPG; jj++) {
+                const int j = pg * TC_PPG + jj;
+                const bool pok = (n_first + jj) < npairs;
+                if (jj > 0) {
+                    if (++k == a.S) {
+                        // next coil (only when TC_PPG does not divide S): restart at k = 0
+                        k = 0;
+                        ++c;
+#pragma unroll
+                        for (int i = 0; i < VPH; i++) {
+                            const int v = vbase + i;
+                            float2 e = make_float2(0.f, 0.f), w = e;
+                            if (pok && v < v_end) {
+                                e = __ldg(a.estart + v);
+                                w = __ldg(a.coilw + int64_t(c) * a.nvoxels + v);
+                            }
+                            G[i] = cmul(e, w);
+                        }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < VPH; i++) G[i] = cmul(G[i], step[i]);
+                    }
+                }
+                const float ks = float(k) - 0.5f * float(a.S);
+                // one hi/lo split per value: BF16 rounding is sign-symmetric, so the split of
+                // (x, -y) is the split of (x, y) with the upper sign bit flipped and the split
+                // of (y, x) is the same pair with its halves swapped
+                uint32_t h0[2], l0[2], h1[2], l1[2];
+#pragma unroll
+                for (int i = 0; i < 2; i++) {
+                    float2 F = pok ? G[JAC ? 0 : i] : make_float2(0.f, 0.f);
+                    if (JAC && i == 1) F = make_float2(ks * F.x, ks * F.y);
+                    uint32_t h, l;
+                    tc::split2(F.x, F.y, h, l);
+                    h0[i] = h ^ 0x80000000u;
+                    l0[i] = l ^ 0x80000000u;
+                    h1[i] = __byte_perm(h, 0, 0x1032);
+                    l1[i] = __byte_perm(l, 0, 0x1032);
+                }
+                const uint32_t o0 = tc::sw128_offset(2 * j, hq >> 1) + (hq & 1) * 8;
+                const uint32_t o1 = tc::sw128_offset(2 * j + 1, hq >> 1) + (hq & 1) * 8;
+                *reinterpret_cast<uint2*>(Bh + o0) = make_uint2(h0[0], h0[1]);
+                *reinterpret_cast<uint2*>(Bl + o0) = make_uint2(l0[0], l0[1]);
+                *reinterpret_cast<uint2*>(Bh + o1) = make_uint2(h1[0], h1[1]);
+                *reinterpret_cast<uint2*>(Bl + o1) = make_uint2(l1[0], l1[1]);
+            }
+            tc::fence_async_shared();
+            tc::mbar_arrive(&full[buf]);
+#pragma unroll
+            for (int i = 0; i < VPH; i++) {
+                step[i] = step_n[i];
+                e0[i] = e0_n[i];
+                cw[i] = cw_n[i];
+            }
         }
-    } else if (warp == 16) {
-        // make sure the MMAs finished before the TMEM is released (bounded)
-        if (lane == 0) tc::mbar_wait(done, 0, a.status);
-        __syncwarp();
+
+        // ---------------- epilogue: TMEM → shared memory (row = readout, pairs along the row) →
+        // coalesced rows of out[c][r][k]. Warp w reads TMEM lanes 32·(w%4).. (its quarter) and
+        // column chunks w/4 and w/4 + 4; all 16 warps then write 8 rows each.
+        const bool waited = tc::mbar_wait(done, 0, a.status);
+        tc::tc_fence_after();
+        // one decision for all 512 producer threads (tcgen05.ld is .sync.aligned, the barriers
+        // below need every participant)
+        const bool ok = !tc::bar_red_or(1, TC_B_THREADS, !(waited && !*(volatile int*)abort_flag));
+        if (ok) {
+            float2* T = reinterpret_cast<float2*>(smem);  // [TC_M][TC_TROW]; the stage buffers are free
+            const int quarter = warp & 3;
+            const int row = quarter * 32 + lane;
+#pragma unroll 1
+            for (int h = 0; h < 2; h++) {
+                const int qq = (warp >> 2) + 4 * h;  // 32 columns = 16 pairs
+                float v[32];
+                tc::tmem_load32(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(qq * 32), v);
+                float4* dst = reinterpret_cast<float4*>(T + row * TC_TROW + qq * 16);
+#pragma unroll
+                for (int m = 0; m < 8; m++) dst[m] = make_float4(v[4 * m], v[4 * m + 1], v[4 * m + 2], v[4 * m + 3]);
+            }
+            tc::bar_sync(1, TC_B_THREADS);
+            float2* outp = a.out + int64_t(bz) * npairs * a.R;
+            int64_t base[TC_PAIRS / 32];
+            bool pv[TC_PAIRS / 32];
+#pragma unroll
+            for (int m = 0; m < TC_PAIRS / 32; m++) {
+                const int n = n_pair0 + lane + 32 * m;
+                const int cc = n / a.S, kk = n - cc * a.S;
+                pv[m] = n < npairs;
+                base[m] = int64_t(cc) * a.R * a.S + kk;
+            }
+#pragma unroll 1
+            for (int rr = warp; rr < TC_M && r0 + rr < a.R; rr += TC_B_THREADS / 32) {
+                const int64_t roff = int64_t(r0 + rr) * a.S;
+#pragma unroll
+                for (int m = 0; m < TC_PAIRS / 32; m++)
+                    if (pv[m]) outp[base[m] + roff] = T[rr * TC_TROW + lane + 32 * m];
+            }
+        }
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 16) {
+    if (warp == TC_MMA_WARP) {
         tc::tc_fence_after();
         tc::tmem_dealloc(tmem, 256);
     }
@@ -434,7 +391,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
 
 // tile grid of one contraction: (pair tiles, readout tiles, voxel splits)
 __device__ __forceinline__ int3 tc_grid_of(const TcArgs& a) {
-    return make_int3((a.C * a.S + TC_N / 2 - 1) / (TC_N / 2), (a.R + TC_M - 1) / TC_M,
+    return make_int3((a.C * a.S + TC_PAIRS - 1) / TC_PAIRS, (a.R + TC_M - 1) / TC_M,
                      (a.nvoxels + a.vchunk - 1) / a.vchunk);
 }
 
@@ -483,15 +440,31 @@ __global__ void tc_prep_batch_kernel(const TcArgs* __restrict__ jobs, const int*
         local = blockIdx.x - block_offsets[j];
     }
     __syncthreads();
-    tc_prep_voxel<JAC>(job, local * blockDim.x + threadIdx.x, const_cast<VoxelGen*>(job.vgen),
-                       const_cast<float2*>(job.coilw), const_cast<float4*>(job.jcoef));
+    tc_prep_voxel<JAC>(job, local * blockDim.x + threadIdx.x);
+}
+
+// batched tc_pack_a_kernel: flattened 256-thread block b → job j, local block l = b - offsets[j]
+// covering columns (l % gx)·256 + t of padded readout row l / gx, gx = ⌈32·apack_stages / 256⌉
+template<bool JAC>
+__global__ void tc_pack_batch_kernel(const TcArgs* __restrict__ jobs, const int* __restrict__ block_offsets,
+                                     int njobs) {
+    __shared__ TcArgs job;
+    __shared__ int local;
+    if (threadIdx.x == 0) {
+        const int j = job_of_block(block_offsets, njobs, blockIdx.x);
+        job = jobs[j];
+        local = blockIdx.x - block_offsets[j];
+    }
+    __syncthreads();
+    const int gx = (job.apack_stages * 32 + 255) / 256;
+    tc_pack_a<JAC>(job, (local % gx) * 256 + threadIdx.x, local / gx);
 }
 
 }  // namespace kernels
 
 TcPlan tc_plan(int device, int nvoxels, int R, int S, int C, bool jac) {
     TcPlan p;
-    p.ntiles = div_ceil(C * S, kernels::TC_N / 2);
+    p.ntiles = div_ceil(C * S, kernels::TC_PAIRS);
     p.mtiles = div_ceil(R, kernels::TC_M);
     const int tiles = p.ntiles * p.mtiles;
     const int vps = jac ? 16 : 32;
@@ -521,6 +494,36 @@ TcPlan tc_plan(int device, int nvoxels, int R, int S, int C, bool jac) {
     return p;
 }
 
+TcTables tc_tables(int nvoxels, int R, int S, int C, bool jac) {
+    TcTables t;
+    const int64_t V = std::max(nvoxels, 0);
+    const int vps = jac ? 16 : 32;
+    t.egk = (S % kernels::TC_PPG == 0) ? kernels::TC_PPG : 1;
+    t.apack_stages = div_ceil(std::max(nvoxels, 1), vps);
+    auto align = [](int64_t b) { return (b + 255) / 256 * 256; };
+    t.vstep = 0;
+    t.estart = t.vstep + align(8 * V);
+    t.coilw = t.estart + align(8 * V * (S / t.egk));
+    t.jcoef = t.coilw + align(8 * V * C);
+    t.apack = t.jcoef + align(jac ? 32 * V : 0);
+    t.bytes = t.apack + int64_t(div_ceil(R, kernels::TC_M)) * t.apack_stages * kernels::TC_APACK_BLOCK;
+    return t;
+}
+
+void tc_assign_tables(kernels::TcArgs& a, const TcTables& t, unsigned char* base) {
+    a.vstep = reinterpret_cast<const float2*>(base + t.vstep);
+    a.estart = reinterpret_cast<const float2*>(base + t.estart);
+    a.egk = t.egk;
+    a.coilw = reinterpret_cast<const float2*>(base + t.coilw);
+    a.jcoef = reinterpret_cast<const float4*>(base + t.jcoef);
+    a.apack = base + t.apack;
+    a.apack_stages = t.apack_stages;
+}
+
+int tc_pack_blocks(int R, int apack_stages) {
+    return div_ceil(apack_stages * 32, 256) * div_ceil(R, kernels::TC_M) * kernels::TC_M;
+}
+
 namespace {
 
 void set_tc_smem_attribute(bool jac, bool batch) {
@@ -539,50 +542,28 @@ bool run_tc(const CompasContext& ctx, kernels::TcArgs a, bool jac, cfloat* out) 
     DeviceGuard guard(ctx.device());
     const int npairs = a.C * a.S;
     const TcPlan plan = tc_plan(ctx.device(), a.nvoxels, a.R, a.S, a.C, jac);
-    const int ntiles = plan.ntiles, mtiles = plan.mtiles;
-    int splits = plan.splits;
+    const int splits = plan.splits;
     a.vchunk = plan.vchunk;
     const int64_t n = int64_t(npairs) * a.R;
     Array<cfloat, 2> partials({splits > 1 ? splits : 0, n}, ctx.device(), ctx.stream());
-    // per-voxel tables: 24 B generation constants, C coil·w values, J·v coefficients
-    Array<float, 2> vgen({a.nvoxels, int64_t(sizeof(kernels::VoxelGen) / sizeof(float))}, ctx.device(), ctx.stream());
-    Array<cfloat, 2> coilw({a.C, a.nvoxels}, ctx.device(), ctx.stream());
-    Array<float, 2> jcoef({jac ? a.nvoxels : 0, 8}, ctx.device(), ctx.stream());
-    a.vgen = reinterpret_cast<const kernels::VoxelGen*>(vgen.data());
-    a.coilw = reinterpret_cast<const float2*>(coilw.data());
-    a.jcoef = reinterpret_cast<const float4*>(jcoef.data());
+    const TcTables tables = tc_tables(a.nvoxels, a.R, a.S, a.C, jac);
+    Array<unsigned char> scratch({tables.bytes}, ctx.device(), ctx.stream());
+    tc_assign_tables(a, tables, scratch.data());
     a.out = reinterpret_cast<float2*>(splits > 1 ? partials.data() : out);
     a.status = detail::device_status_word(ctx.device());
+    // per-voxel tables, then A packed once (one pass over the echoes instead of one per pair tile)
+    const dim3 pgrid(div_ceil(a.apack_stages * 32, 256), plan.mtiles * kernels::TC_M);
     if (jac) {
-        kernels::tc_prep_kernel<true><<<div_ceil(a.nvoxels, 128), 128, 0, ctx.stream()>>>(
-            a, reinterpret_cast<kernels::VoxelGen*>(vgen.data()), reinterpret_cast<float2*>(coilw.data()),
-            reinterpret_cast<float4*>(jcoef.data()));
+        kernels::tc_prep_kernel<true><<<div_ceil(a.nvoxels, 128), 128, 0, ctx.stream()>>>(a);
+        kernels::tc_pack_a_kernel<true><<<pgrid, 256, 0, ctx.stream()>>>(a);
     } else {
-        kernels::tc_prep_kernel<false><<<div_ceil(a.nvoxels, 128), 128, 0, ctx.stream()>>>(
-            a, reinterpret_cast<kernels::VoxelGen*>(vgen.data()), reinterpret_cast<float2*>(coilw.data()), nullptr);
+        kernels::tc_prep_kernel<false><<<div_ceil(a.nvoxels, 128), 128, 0, ctx.stream()>>>(a);
+        kernels::tc_pack_a_kernel<false><<<pgrid, 256, 0, ctx.stream()>>>(a);
     }
-    check_launch("tc_prep_kernel");
-    // pack A once when several pair tiles would each convert it (it then costs one pass over the
-    // echoes instead of `ntiles` conversions)
-    const int vps = jac ? 16 : 32;
-    const int apack_stages = div_ceil(a.nvoxels, vps);
-    const bool pack = ntiles >= 2;
-    Array<unsigned char> apack({pack ? int64_t(mtiles) * apack_stages * kernels::TC_APACK_BLOCK : 0}, ctx.device(),
-                               ctx.stream());
-    a.apack = nullptr;
-    a.apack_stages = apack_stages;
-    if (pack) {
-        dim3 pgrid(div_ceil(apack_stages * 32, 256), mtiles * kernels::TC_M);
-        if (jac)
-            kernels::tc_pack_a_kernel<true><<<pgrid, 256, 0, ctx.stream()>>>(a, apack.data());
-        else
-            kernels::tc_pack_a_kernel<false><<<pgrid, 256, 0, ctx.stream()>>>(a, apack.data());
-        check_launch("tc_pack_a_kernel");
-        a.apack = apack.data();
-    }
+    check_launch("tc_prep_kernel / tc_pack_a_kernel");
     auto fn = jac ? kernels::tc_contract_kernel<true> : kernels::tc_contract_kernel<false>;
     set_tc_smem_attribute(jac, false);
-    dim3 grid(ntiles, mtiles, splits);
+    dim3 grid(plan.ntiles, plan.mtiles, splits);
     fn<<<grid, kernels::TC_THREADS, kernels::TC_SMEM, ctx.stream()>>>(a);
     check_launch("tc_contract_kernel");
     if (splits > 1) sum_partials(ctx, partials.data(), splits, n, out);
@@ -640,13 +621,19 @@ kernels::TcArgs tc_signal_args(const float* params, int64_t pstride, int nvoxels
 }
 
 void launch_tc_batch(cudaStream_t stream, int device, bool jac, const kernels::TcArgs* jobs, int njobs,
-                     const int* prep_offsets, int prep_blocks, const int* cta_offsets, int ctas) {
+                     const int* prep_offsets, int prep_blocks, const int* pack_offsets, int pack_blocks,
+                     const int* cta_offsets, int ctas) {
     if (njobs <= 0) return;
     DeviceGuard guard(device);
     if (prep_blocks > 0) {
         if (jac) kernels::tc_prep_batch_kernel<true><<<prep_blocks, 128, 0, stream>>>(jobs, prep_offsets, njobs);
         else kernels::tc_prep_batch_kernel<false><<<prep_blocks, 128, 0, stream>>>(jobs, prep_offsets, njobs);
         check_launch("tc_prep_batch_kernel");
+    }
+    if (pack_blocks > 0) {
+        if (jac) kernels::tc_pack_batch_kernel<true><<<pack_blocks, 256, 0, stream>>>(jobs, pack_offsets, njobs);
+        else kernels::tc_pack_batch_kernel<false><<<pack_blocks, 256, 0, stream>>>(jobs, pack_offsets, njobs);
+        check_launch("tc_pack_batch_kernel");
     }
     if (ctas <= 0) return;
     set_tc_smem_attribute(jac, true);
@@ -656,6 +643,5 @@ void launch_tc_batch(cudaStream_t stream, int device, bool jac, const kernels::T
         kernels::tc_contract_batch_kernel<false><<<ctas, kernels::TC_THREADS, kernels::TC_SMEM, stream>>>(jobs, cta_offsets, njobs);
     check_launch("tc_contract_batch_kernel");
 }
-
 
 }  // namespace compas
