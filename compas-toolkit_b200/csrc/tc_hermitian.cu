@@ -4,21 +4,26 @@
 // regrouping). For every voxel v and (readout r, coil c) pair p:
 //   Y_p(v) = Σ_k u[c][r][k]·conj(E_k(v)),   Ỹ_p(v) = Σ_k (k - S/2)·u[c][r][k]·conj(E_k(v))
 // is a GEMM with M = voxels, N = pairs, K = samples. A CTA owns 128 voxels (the 128 TMEM
-// lanes), so the follow-up contraction over readouts with the echoes
-//   mHv_c += conj(m[r])·Y,  dmHv0_c += conj(∂T1m[r])·Y,  dmHv1_c += conj(∂T2m[r])·Y + ΔtR2²·conj(m[r])·Ỹ
-// happens inside each epilogue thread; the four per-voxel results never leave registers, every
-// echo element is read once for all coils, and no [R][V] temporary is written (the reference
-// writes two FP32 [2][R][V] arrays per coil and re-reads the echoes per coil).
+// lanes), so the follow-up contraction over coils and readouts
+//   Z_r = Σ_c conj(C_c)·Y_rc,  Z̃_r = Σ_c conj(C_c)·Ỹ_rc,
+//   mHv += conj(m[r])·Z_r,  dmHv0 += conj(∂T1m[r])·Z_r,  dmHv1 += conj(∂T2m[r])·Z_r + ΔtR2²·conj(m[r])·Z̃_r
+// happens inside each epilogue thread; the per-voxel results never leave registers, every echo
+// element is read once for all coils, and no [R][V] temporary is written (the reference writes
+// two FP32 [2][R][V] arrays per coil and re-reads the echoes per coil).
 //
 // Real-ified operands (re/im interleaved along K = 2S):
-//   A'[v]            = (Re ē_k, Im ē_k) with ē = conj(E_k(v))     — generated, 128 voxels × 32 samples/stage
+//   A'[v]            = (Re ē_k, Im ē_k) with ē = conj(E_k(v))     — 128 voxels × 32 samples per stage
 //   B'[0·64 + p]     = (u_re, -u_im)     → Y_re    B'[1·64 + p] = (u_im, u_re)      → Y_im
 //   B'[2·64 + p]     = (k-S/2)(u_re, -u_im) → Ỹ_re B'[3·64 + p] = (k-S/2)(u_im, u_re) → Ỹ_im
+// A does not depend on the pair tile, so a small kernel writes it once per call as the swizzled
+// BF16 hi/lo shared-memory images of every (voxel tile, 32-sample stage): E_k exactly at every
+// 16th sample (phase reduced modulo 2π in FP64) and the complex recurrence in between. The
+// contraction then loads each stage's A with one bulk copy.
 // D[128 voxels][256] accumulates in TMEM; two accumulators (512 columns) alternate between
 // consecutive pair tiles so the epilogue of tile t overlaps the MMAs of tile t+1.
-// Warp roles: 0-7 epilogue (warps w and w+4 share TMEM lanes 32(w%4).. = voxels and split each
-// tile's pairs), 8-11 generate A, 12-15 convert u (B), 16 allocates TMEM and issues the MMAs.
-// All waits are bounded.
+// Warp roles (576 threads): 0-7 epilogue (warps w and w+4 share TMEM lanes 32(w%4).. = voxels
+// and split each tile's pairs), 8-15 convert u (B), 16 allocates TMEM and issues the MMAs,
+// 17 loads A. All waits are bounded.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -33,12 +38,15 @@ void sum_partials(const CompasContext& ctx, const cfloat* partials, int nsplit, 
 namespace kernels {
 
 constexpr int TH_M = 128, TH_N = 256, TH_K = 64, TH_PAIRS = 64;
-constexpr int TH_THREADS = 544;  // 8 epilogue + 4 A + 4 B warps + 1 MMA warp
+constexpr int TH_THREADS = 576;  // 8 epilogue + 8 B warps + MMA warp + copy warp
+constexpr int TH_MMA_WARP = 16, TH_COPY_WARP = 17;
+constexpr int TH_B_THREADS = 256;
 constexpr int TH_STAGES = 2;
 constexpr int TH_A_BYTES = TH_M * TH_K * 2;
 constexpr int TH_B_BYTES = TH_N * TH_K * 2;
 constexpr int TH_STAGE_BYTES = 2 * TH_A_BYTES + 2 * TH_B_BYTES;
 constexpr int TH_SMEM = TH_STAGES * TH_STAGE_BYTES + 1024 + 256;
+constexpr int TH_APACK_BLOCK = 2 * TH_A_BYTES;  // hi + lo image of one (voxel tile, stage)
 
 struct ThArgs {
     const float* params;
@@ -52,23 +60,66 @@ struct ThArgs {
     int R, S, C;
     float dt, dk_re, dk_im;
     int tiles_per_split;  // pair tiles handled by one CTA
+    const unsigned char* apack;  // [voxel tiles][stages] A images
     float2* out;          // [splits][4][V]
     unsigned int* status;
 };
+
+// A images: thread = (voxel row t of tile blockIdx.x, 16-sample segment blockIdx.y) writes
+// conj(E_k(v)) for k = 16·seg .. 16·seg + 15 (zero past S or past the last voxel)
+__global__ void __launch_bounds__(128) tc_hermitian_pack_kernel(ThArgs a) {
+    const int t = threadIdx.x;
+    const int v = blockIdx.x * TH_M + t;
+    const int seg = blockIdx.y;
+    const int kstages = (a.S + 31) / 32;
+    const double twopi = 6.283185307179586476925;
+    float2 e = make_float2(0.f, 0.f), step = e;
+    const bool vok = v < a.nvoxels;
+    if (vok) {
+        const float T2 = a.params[a.pstride + v], B0 = a.params[3 * a.pstride + v];
+        const float x = a.params[6 * a.pstride + v], y = a.params[7 * a.pstride + v];
+        const double theta = double(a.dk_re) * x + double(a.dk_im) * y + double(a.dt) * twopi * B0;
+        const float decay = -a.dt / T2;
+        const float2 st = cis_rad(theta);
+        const float sm = __expf(decay);
+        step = make_float2(sm * st.x, sm * st.y);
+        const int kb = seg * 16;
+        const float s0 = float(kb) - 0.5f * float(a.S);
+        const float2 ph = cis_rad(double(s0) * theta);
+        const float mg = __expf(s0 * decay);
+        e = make_float2(mg * ph.x, mg * ph.y);
+    }
+    unsigned char* blk = const_cast<unsigned char*>(a.apack) + (int64_t(blockIdx.x) * kstages + seg / 2) * TH_APACK_BLOCK;
+#pragma unroll
+    for (int cq = 0; cq < 4; cq++) {  // 4 chunks of 4 samples
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const bool kok = vok && (seg * 16 + 4 * cq + i) < a.S;
+            tc::split2(kok ? e.x : 0.0f, kok ? -e.y : 0.0f, h[i], l[i]);
+            e = cmul(e, step);
+        }
+        const uint32_t off = tc::sw128_offset(t, (seg & 1) * 4 + cq);
+        *reinterpret_cast<uint4*>(blk + off) = make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4*>(blk + TH_A_BYTES + off) = make_uint4(l[0], l[1], l[2], l[3]);
+    }
+}
 
 __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + TH_STAGES * TH_STAGE_BYTES);
     uint64_t* empty = full + TH_STAGES;
-    uint64_t* acc_full = empty + TH_STAGES;
+    uint64_t* afull = empty + TH_STAGES;
+    uint64_t* acc_full = afull + TH_STAGES;
     uint64_t* acc_empty = acc_full + 2;
     uint64_t* done = acc_empty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int v0 = blockIdx.x * TH_M;
+    const int vt = blockIdx.x;
+    const int v0 = vt * TH_M;
     const int split = blockIdx.y;
     const int npairs = a.R * a.C;
     const int ntiles_total = (npairs + TH_PAIRS - 1) / TH_PAIRS;
@@ -76,11 +127,13 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
     const int tile_end = min(ntiles_total, tile_begin + a.tiles_per_split);
     const int ntiles = max(0, tile_end - tile_begin);
     const int kstages = (a.S + 31) / 32;  // 32 samples (64 K) per stage
+    const int nstages = ntiles * kstages;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TH_STAGES; s++) {
-            tc::mbar_init(&full[s], 256);
+            tc::mbar_init(&full[s], TH_B_THREADS);
             tc::mbar_init(&empty[s], 1);
+            tc::mbar_init(&afull[s], 1);
         }
         for (int s = 0; s < 2; s++) {
             tc::mbar_init(&acc_full[s], 1);
@@ -90,198 +143,212 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
         *abort_flag = 0;
         tc::fence_mbarrier_init();
     }
-    if (warp == 16) tc::tmem_alloc(tmem_slot, 512);
+    if (warp == TH_MMA_WARP) tc::tmem_alloc(tmem_slot, 512);
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const double twopi = 6.283185307179586476925;
 
-    if (warp < 12) {
-        // per-voxel constants: warps 0-7 (epilogue) and 8-11 (A producer) own voxel v0 + (tid & 127)
+    if (warp < 8) {
+        // ---------------- epilogue: thread = voxel = TMEM lane 32·(warp%4) + lane; warps w and
+        // w+4 take alternate 8-pair chunks of every tile
         const int t = threadIdx.x & 127;
         const int v = v0 + t;
         const bool vok = v < a.nvoxels;
         const int vc = vok ? v : (a.nvoxels - 1);
-        const float T1 = a.params[vc], T2 = a.params[a.pstride + vc], B0 = a.params[3 * a.pstride + vc];
-        const float x = a.params[6 * a.pstride + vc], y = a.params[7 * a.pstride + vc];
-        const double theta = double(a.dk_re) * x + double(a.dk_im) * y + double(a.dt) * twopi * B0;
-        const float decay = -a.dt / T2;
-        if (warp >= 8) {
-            // ---------------- A producer: 32 samples of conj(E_k(v)) per stage, row t
-            const float2 st = cis_rad(theta);
-            const float sm = __expf(decay);
-            const float2 step = make_float2(sm * st.x, sm * st.y);
-            int g = 0;  // global stage counter (same order as the B producer and the MMA issuer)
-            for (int tl = 0; tl < ntiles; tl++) {
-                for (int ks = 0; ks < kstages; ks++, g++) {
-                    const int buf = g % TH_STAGES;
-                    if (!tc::mbar_wait(&empty[buf], ((g / TH_STAGES) & 1) ^ 1, a.status)) *abort_flag = 1;
-                    if (*(volatile int*)abort_flag) break;
-                    unsigned char* Ah = smem + buf * TH_STAGE_BYTES;
-                    unsigned char* Al = Ah + TH_A_BYTES;
-                    // exact restarts at k0 and k0+16 (FP64-reduced phase), recurrence between
+        const float T1 = a.params[vc], T2 = a.params[a.pstride + vc];
+        const float2 rho = make_float2(a.params[4 * a.pstride + vc], a.params[5 * a.pstride + vc]);
+        const float R2 = 1.0f / T2;
+        const float dscale = a.dt * R2 * R2;
+        const int quarter = warp & 3, parity = warp >> 2;
+        // Σ_r over conj(∂T1m)·Z, conj(∂T2m)·Z + ΔtR2²·conj(m)·Z̃, conj(m)·Z
+        float2 acc[3];
 #pragma unroll
-                    for (int half = 0; half < 2; half++) {
-                        const int kb = ks * 32 + half * 16;
-                        const float s0 = float(kb) - 0.5f * float(a.S);
-                        const float2 ph = cis_rad(double(s0) * theta);
-                        const float mg = __expf(s0 * decay);
-                        float2 e = make_float2(mg * ph.x, mg * ph.y);
-#pragma unroll
-                        for (int cq = 0; cq < 4; cq++) {  // 4 chunks of 4 samples
-                            uint32_t h[4], l[4];
-#pragma unroll
-                            for (int i = 0; i < 4; i++) {
-                                const bool kok = vok && (kb + 4 * cq + i) < a.S;
-                                tc::split2(kok ? e.x : 0.0f, kok ? -e.y : 0.0f, h[i], l[i]);
-                                e = cmul(e, step);
-                            }
-                            const uint32_t off = tc::sw128_offset(t, half * 4 + cq);
-                            *reinterpret_cast<uint4*>(Ah + off) = make_uint4(h[0], h[1], h[2], h[3]);
-                            *reinterpret_cast<uint4*>(Al + off) = make_uint4(l[0], l[1], l[2], l[3]);
-                        }
-                    }
-                    tc::fence_async_shared();
-                    tc::mbar_arrive(&full[buf]);
-                }
-                if (*(volatile int*)abort_flag) break;
+        for (int f = 0; f < 3; f++) acc[f] = make_float2(0.f, 0.f);
+        bool ok = true;
+        for (int tl = 0; tl < ntiles; tl++) {
+            const int abuf = tl & 1;
+            const bool waited = tc::mbar_wait(&acc_full[abuf], (tl >> 1) & 1, a.status);
+            tc::tc_fence_after();
+            if (!__all_sync(0xffffffffu, waited && !*(volatile int*)abort_flag)) {
+                *abort_flag = 1;
+                ok = false;
+                break;
             }
-        } else {
-            // ---------------- epilogue: thread = voxel = TMEM lane 32·(warp%4) + lane; warps w and
-            // w+4 take alternate 8-pair chunks of every tile
-            const float2 rho = make_float2(a.params[4 * a.pstride + vc], a.params[5 * a.pstride + vc]);
-            const float R2 = 1.0f / T2;
-            const float dscale = a.dt * R2 * R2;
-            const int quarter = warp & 3, parity = warp >> 2;
-            float2 acc[4];
-#pragma unroll
-            for (int f = 0; f < 4; f++) acc[f] = make_float2(0.f, 0.f);
-            bool ok = true;
-            for (int tl = 0; tl < ntiles; tl++) {
-                const int abuf = tl & 1;
-                const bool waited = tc::mbar_wait(&acc_full[abuf], (tl >> 1) & 1, a.status);
-                tc::tc_fence_after();
-                if (!__all_sync(0xffffffffu, waited && !*(volatile int*)abort_flag)) {
-                    *abort_flag = 1;
-                    ok = false;
-                    break;
-                }
-                const uint32_t tbase = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(abuf * 256);
-                const int p0 = (tile_begin + tl) * TH_PAIRS;
+            const uint32_t tbase = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(abuf * 256);
+            const int p0 = (tile_begin + tl) * TH_PAIRS;
 #pragma unroll 1
-                for (int ch = parity; ch < TH_PAIRS / 8; ch += 2) {  // 8 pairs at a time
-                    const int pb = p0 + ch * 8;
-                    // loads first (echo, ∂echo, coil of the 8 pairs), then the TMEM reads and math
-                    float2 m[8], m1[8], m2[8], cc[8];
-                    {
-                        int r = pb / a.C, c = pb - r * a.C;
-#pragma unroll
-                        for (int i = 0; i < 8; i++) {
-                            if (vok && pb + i < npairs) {
-                                const int64_t idx = int64_t(r) * a.nvoxels + v;
-                                m[i] = __ldg(a.echo + idx);
-                                m1[i] = __ldg(a.dT1 + idx);
-                                m2[i] = __ldg(a.dT2 + idx);
-                                cc[i] = __ldg(a.coils + int64_t(c) * a.nvoxels + v);
-                            } else {
-                                m[i] = m1[i] = m2[i] = cc[i] = make_float2(0.f, 0.f);
-                            }
-                            if (++c == a.C) {
-                                c = 0;
-                                ++r;
-                            }
-                        }
-                    }
-                    float yr[8], yi[8], tr[8], ti[8];
-                    tc::tmem_load8(tbase + 0 * 64 + ch * 8, yr);
-                    tc::tmem_load8(tbase + 1 * 64 + ch * 8, yi);
-                    tc::tmem_load8(tbase + 2 * 64 + ch * 8, tr);
-                    tc::tmem_load8(tbase + 3 * 64 + ch * 8, ti);
+            for (int ch = parity; ch < TH_PAIRS / 8; ch += 2) {  // 8 pairs at a time
+                const int pb = p0 + ch * 8;
+                const int rb = pb / a.C;
+                // loads first: the coil factor of each pair and the echoes of the chunk's first
+                // two readouts (more readouts only with fewer than 4 coils: loaded when needed)
+                float2 cc[8], m[2], m1[2], m2[2];
+                {
+                    int c = pb - rb * a.C;
 #pragma unroll
                     for (int i = 0; i < 8; i++) {
-                        const float2 Y = make_float2(yr[i], yi[i]), Yt = make_float2(tr[i], ti[i]);
-                        const float2 mH = cmulc(Y, m[i]);
-                        const float2 d0 = cmulc(Y, m1[i]);
-                        const float2 dd1 = cadd(cmulc(Y, m2[i]), cscale(dscale, cmulc(Yt, m[i])));
-                        const float2 rc = cmul(rho, cc[i]);
-                        acc[0] = cadd(acc[0], cmulc(d0, cscale(T1, rc)));
-                        acc[1] = cadd(acc[1], cmulc(dd1, cscale(T2, rc)));
-                        const float2 cm = cmulc(mH, cc[i]);
-                        acc[2] = cadd(acc[2], cm);
-                        acc[3] = cadd(acc[3], make_float2(cm.y, -cm.x));
+                        cc[i] = (vok && pb + i < npairs) ? __ldg(a.coils + int64_t(c) * a.nvoxels + v)
+                                                         : make_float2(0.f, 0.f);
+                        if (++c == a.C) c = 0;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 2; q++) {
+                        const int r = rb + q;
+                        m[q] = m1[q] = m2[q] = make_float2(0.f, 0.f);
+                        if (vok && r < a.R) {
+                            const int64_t idx = int64_t(r) * a.nvoxels + v;
+                            m[q] = __ldg(a.echo + idx);
+                            m1[q] = __ldg(a.dT1 + idx);
+                            m2[q] = __ldg(a.dT2 + idx);
+                        }
                     }
                 }
-                tc::tc_fence_before();
-                tc::mbar_arrive(&acc_empty[abuf]);
-            }
-            // combine the two warps of each lane quarter through shared memory (stage buffer 0,
-            // free once every tile has been consumed) and write the four results
-            float2* red = reinterpret_cast<float2*>(smem);
-            asm volatile("bar.sync 2, 256;" ::: "memory");  // epilogue warps only: all MMAs consumed
-            if (parity == 1) {
+                float yr[8], yi[8], tr[8], ti[8];
+                tc::tmem_load8(tbase + 0 * 64 + ch * 8, yr);
+                tc::tmem_load8(tbase + 1 * 64 + ch * 8, yi);
+                tc::tmem_load8(tbase + 2 * 64 + ch * 8, tr);
+                tc::tmem_load8(tbase + 3 * 64 + ch * 8, ti);
+                int r = rb, c = pb - rb * a.C;
+                float2 Z = make_float2(0.f, 0.f), Zt = Z;
 #pragma unroll
-                for (int f = 0; f < 4; f++) red[f * 128 + t] = acc[f];
+                for (int i = 0; i < 8; i++) {
+                    Z = cadd(Z, cmulc(make_float2(yr[i], yi[i]), cc[i]));
+                    Zt = cadd(Zt, cmulc(make_float2(tr[i], ti[i]), cc[i]));
+                    const bool next_r = ++c == a.C;
+                    if (next_r || i == 7) {
+                        // fold readout r's coil sum into the voxel's results
+                        float2 me, d1, d2;
+                        if (r == rb) {
+                            me = m[0], d1 = m1[0], d2 = m2[0];
+                        } else if (r == rb + 1) {
+                            me = m[1], d1 = m1[1], d2 = m2[1];
+                        } else {
+                            me = d1 = d2 = make_float2(0.f, 0.f);
+                            if (vok && r < a.R) {
+                                const int64_t idx = int64_t(r) * a.nvoxels + v;
+                                me = __ldg(a.echo + idx);
+                                d1 = __ldg(a.dT1 + idx);
+                                d2 = __ldg(a.dT2 + idx);
+                            }
+                        }
+                        acc[0] = cadd(acc[0], cmulc(Z, d1));
+                        acc[1] = cadd(acc[1], cadd(cmulc(Z, d2), cscale(dscale, cmulc(Zt, me))));
+                        acc[2] = cadd(acc[2], cmulc(Z, me));
+                        Z = Zt = make_float2(0.f, 0.f);
+                    }
+                    if (next_r) {
+                        c = 0;
+                        ++r;
+                    }
+                }
             }
-            asm volatile("bar.sync 2, 256;" ::: "memory");
-            if (parity == 0 && ok && vok && !*(volatile int*)abort_flag) {
-                float2* o = a.out + int64_t(split) * 4 * a.nvoxels;
+            tc::tc_fence_before();
+            tc::mbar_arrive(&acc_empty[abuf]);
+        }
+        // combine the two warps of each lane quarter through shared memory (stage buffer 0,
+        // free once every tile has been consumed) and write the four results
+        float2* red = reinterpret_cast<float2*>(smem);
+        tc::bar_sync(2, 256);  // epilogue warps only: all MMAs consumed
+        if (parity == 1) {
 #pragma unroll
-                for (int f = 0; f < 4; f++) o[int64_t(f) * a.nvoxels + v] = cadd(acc[f], red[f * 128 + t]);
-            }
+            for (int f = 0; f < 3; f++) red[f * 128 + t] = acc[f];
+        }
+        tc::bar_sync(2, 256);
+        if (parity == 0 && ok && vok && !*(volatile int*)abort_flag) {
+#pragma unroll
+            for (int f = 0; f < 3; f++) acc[f] = cadd(acc[f], red[f * 128 + t]);
+            // conj(T1ρ·C)·… : the ρ factors of the T1 / T2 blocks, taken out of the coil sums
+            const float2 r1 = cscale(T1, rho), r2 = cscale(T2, rho);
+            float2* o = a.out + int64_t(split) * 4 * a.nvoxels;
+            o[v] = cmulc(acc[0], r1);
+            o[a.nvoxels + v] = cmulc(acc[1], r2);
+            o[2 * int64_t(a.nvoxels) + v] = acc[2];
+            o[3 * int64_t(a.nvoxels) + v] = make_float2(acc[2].y, -acc[2].x);  // -i·mHv
         }
     } else if (warp < 16) {
-        // ---------------- B producer: u → rows (u_re,-u_im), (u_im,u_re) and their (k-S/2)-scaled copies
-        const int t = threadIdx.x - 384;
-        const int pl = t & 63, half = t >> 6;  // pair within tile, 16-sample half of the stage
-        int g = 0;
-        for (int tl = 0; tl < ntiles; tl++) {
+        // ---------------- B producer: u → rows (u_re,-u_im), (u_im,u_re) and their (k-S/2)-scaled
+        // copies; thread = (pair pl of the tile, 8-sample quarter of the stage)
+        const int t = threadIdx.x - 256;
+        const int pl = t & 63, qtr = t >> 6;
+        float2 uv[8];
+        auto load_u = [&](int g) {
+            const int tl = g / kstages, ks = g - tl * kstages;
             const int p = (tile_begin + tl) * TH_PAIRS + pl;
             const bool pok = p < npairs;
             const int r = pok ? p / a.C : 0, c = pok ? p - r * a.C : 0;
             const float2* urow = a.u + (int64_t(c) * a.R + r) * a.S;
-            for (int ks = 0; ks < kstages; ks++, g++) {
-                const int buf = g % TH_STAGES;
-                const int kb = ks * 32 + half * 16;
-                float2 uv[16];
+            const int kb = ks * 32 + qtr * 8;
 #pragma unroll
-                for (int i = 0; i < 16; i++)
-                    uv[i] = (pok && kb + i < a.S) ? __ldg(urow + kb + i) : make_float2(0.f, 0.f);
+            for (int i = 0; i < 8; i++) uv[i] = (pok && kb + i < a.S) ? __ldg(urow + kb + i) : make_float2(0.f, 0.f);
+        };
+        if (nstages > 0) load_u(0);
+        for (int g = 0; g < nstages; g++) {
+            const int buf = g % TH_STAGES;
+            const int ks = g % kstages;
+            if (!tc::mbar_wait(&empty[buf], ((g / TH_STAGES) & 1) ^ 1, a.status)) *abort_flag = 1;
+            if (*(volatile int*)abort_flag) break;
+            unsigned char* Bh = smem + buf * TH_STAGE_BYTES + 2 * TH_A_BYTES;
+            unsigned char* Bl = Bh + TH_B_BYTES;
+            const int kb = ks * 32 + qtr * 8;
+#pragma unroll
+            for (int cq = 0; cq < 2; cq++) {  // 4 samples per 16-byte chunk
+                // one hi/lo split per value: the split of (x, -y) is the split of (x, y) with the
+                // upper sign bit flipped, the split of (y, x) the same pair with halves swapped
+                uint32_t h0[4], l0[4], h1[4], l1[4], h2[4], l2[4], h3[4], l3[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const float2 w = uv[4 * cq + i];
+                    const float ksf = float(kb + 4 * cq + i) - 0.5f * float(a.S);
+                    uint32_t h, l, hs, ls;
+                    tc::split2(w.x, w.y, h, l);
+                    tc::split2(ksf * w.x, ksf * w.y, hs, ls);
+                    h0[i] = h ^ 0x80000000u;
+                    l0[i] = l ^ 0x80000000u;
+                    h1[i] = __byte_perm(h, 0, 0x1032);
+                    l1[i] = __byte_perm(l, 0, 0x1032);
+                    h2[i] = hs ^ 0x80000000u;
+                    l2[i] = ls ^ 0x80000000u;
+                    h3[i] = __byte_perm(hs, 0, 0x1032);
+                    l3[i] = __byte_perm(ls, 0, 0x1032);
+                }
+                const int chunk = qtr * 2 + cq;
+                const uint32_t o0 = tc::sw128_offset(0 * 64 + pl, chunk), o1 = tc::sw128_offset(1 * 64 + pl, chunk);
+                const uint32_t o2 = tc::sw128_offset(2 * 64 + pl, chunk), o3 = tc::sw128_offset(3 * 64 + pl, chunk);
+                *reinterpret_cast<uint4*>(Bh + o0) = make_uint4(h0[0], h0[1], h0[2], h0[3]);
+                *reinterpret_cast<uint4*>(Bl + o0) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
+                *reinterpret_cast<uint4*>(Bh + o1) = make_uint4(h1[0], h1[1], h1[2], h1[3]);
+                *reinterpret_cast<uint4*>(Bl + o1) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
+                *reinterpret_cast<uint4*>(Bh + o2) = make_uint4(h2[0], h2[1], h2[2], h2[3]);
+                *reinterpret_cast<uint4*>(Bl + o2) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
+                *reinterpret_cast<uint4*>(Bh + o3) = make_uint4(h3[0], h3[1], h3[2], h3[3]);
+                *reinterpret_cast<uint4*>(Bl + o3) = make_uint4(l3[0], l3[1], l3[2], l3[3]);
+            }
+            tc::fence_async_shared();
+            tc::mbar_arrive(&full[buf]);
+            if (g + 1 < nstages) load_u(g + 1);  // in flight while the next stage's slot frees up
+        }
+    } else if (warp == TH_COPY_WARP) {
+        // ---------------- A: one bulk copy (hi + lo, 32 KB) per stage
+        if (lane == 0) {
+            const unsigned char* src = a.apack + int64_t(vt) * kstages * TH_APACK_BLOCK;
+            int issued[TH_STAGES];
+            for (int s = 0; s < TH_STAGES; s++) issued[s] = -1;
+            for (int g = 0; g < nstages; g++) {
+                const int buf = g % TH_STAGES;
                 if (!tc::mbar_wait(&empty[buf], ((g / TH_STAGES) & 1) ^ 1, a.status)) *abort_flag = 1;
                 if (*(volatile int*)abort_flag) break;
-                unsigned char* Bh = smem + buf * TH_STAGE_BYTES + 2 * TH_A_BYTES;
-                unsigned char* Bl = Bh + TH_B_BYTES;
-#pragma unroll
-                for (int cq = 0; cq < 4; cq++) {  // 4 samples per 16-byte chunk
-                    uint32_t h0[4], l0[4], h1[4], l1[4], h2[4], l2[4], h3[4], l3[4];
-#pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        const float2 w = uv[4 * cq + i];
-                        const float ksf = float(kb + 4 * cq + i) - 0.5f * float(a.S);
-                        tc::split2(w.x, -w.y, h0[i], l0[i]);
-                        tc::split2(w.y, w.x, h1[i], l1[i]);
-                        tc::split2(ksf * w.x, -ksf * w.y, h2[i], l2[i]);
-                        tc::split2(ksf * w.y, ksf * w.x, h3[i], l3[i]);
-                    }
-                    const int chunk = half * 4 + cq;
-                    const uint32_t o0 = tc::sw128_offset(0 * 64 + pl, chunk), o1 = tc::sw128_offset(1 * 64 + pl, chunk);
-                    const uint32_t o2 = tc::sw128_offset(2 * 64 + pl, chunk), o3 = tc::sw128_offset(3 * 64 + pl, chunk);
-                    *reinterpret_cast<uint4*>(Bh + o0) = make_uint4(h0[0], h0[1], h0[2], h0[3]);
-                    *reinterpret_cast<uint4*>(Bl + o0) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
-                    *reinterpret_cast<uint4*>(Bh + o1) = make_uint4(h1[0], h1[1], h1[2], h1[3]);
-                    *reinterpret_cast<uint4*>(Bl + o1) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
-                    *reinterpret_cast<uint4*>(Bh + o2) = make_uint4(h2[0], h2[1], h2[2], h2[3]);
-                    *reinterpret_cast<uint4*>(Bl + o2) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
-                    *reinterpret_cast<uint4*>(Bh + o3) = make_uint4(h3[0], h3[1], h3[2], h3[3]);
-                    *reinterpret_cast<uint4*>(Bl + o3) = make_uint4(l3[0], l3[1], l3[2], l3[3]);
-                }
-                tc::fence_async_shared();
-                tc::mbar_arrive(&full[buf]);
+                tc::mbar_arrive_expect_tx(&afull[buf], TH_APACK_BLOCK);
+                tc::bulk_copy_g2s(smem + buf * TH_STAGE_BYTES, src + int64_t(g % kstages) * TH_APACK_BLOCK,
+                                  TH_APACK_BLOCK, &afull[buf]);
+                issued[buf] = g;
             }
-            if (*(volatile int*)abort_flag) break;
+            // copies still in flight land before the CTA can finish (bounded)
+            for (int s = 0; s < TH_STAGES; s++)
+                if (issued[s] >= 0) tc::mbar_wait(&afull[s], (issued[s] / TH_STAGES) & 1, a.status);
         }
     } else {
-        // ---------------- MMA issuer
+        // ---------------- MMA issuer (warp 16, one lane)
         if (lane == 0) {
             constexpr uint32_t idesc = tc::idesc_bf16_f32(TH_M, TH_N);
             int g = 0;
@@ -296,6 +363,7 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
                 for (int ks = 0; ks < kstages; ks++, g++) {
                     const int buf = g % TH_STAGES;
                     if (!tc::mbar_wait(&full[buf], (g / TH_STAGES) & 1, a.status)) *abort_flag = 1;
+                    if (!tc::mbar_wait(&afull[buf], (g / TH_STAGES) & 1, a.status)) *abort_flag = 1;
                     if (*(volatile int*)abort_flag) break;
                     tc::tc_fence_after();
                     const uint32_t base = tc::smem_u32(smem + buf * TH_STAGE_BYTES);
@@ -321,7 +389,7 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 16) {
+    if (warp == TH_MMA_WARP) {
         tc::tc_fence_after();
         tc::tmem_dealloc(tmem, 512);
     }
@@ -357,6 +425,7 @@ bool launch_jacobian_hermitian_tc(const CompasContext& ctx, const float* params,
     a.status = detail::device_status_word(ctx.device());
     const int vtiles = div_ceil(nvoxels, kernels::TH_M);
     const int ptiles = div_ceil(ncoils * g.nreadouts, kernels::TH_PAIRS);
+    const int kstages = div_ceil(g.ns, 32);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device());
     // split the pair tiles over CTAs (≥ 4 tiles each) to minimise the idle part of the last wave
@@ -375,6 +444,8 @@ bool launch_jacobian_hermitian_tc(const CompasContext& ctx, const float* params,
     splits = div_ceil(ptiles, a.tiles_per_split);
     const int64_t n = 4 * int64_t(nvoxels);
     Array<cfloat, 2> partials({splits > 1 ? splits : 0, n}, ctx.device(), ctx.stream());
+    Array<unsigned char> apack({int64_t(vtiles) * kstages * kernels::TH_APACK_BLOCK}, ctx.device(), ctx.stream());
+    a.apack = apack.data();
     a.out = reinterpret_cast<float2*>(splits > 1 ? partials.data() : JHv);
     static bool attr_set = false;
     if (!attr_set) {
@@ -382,6 +453,8 @@ bool launch_jacobian_hermitian_tc(const CompasContext& ctx, const float* params,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, kernels::TH_SMEM));
         attr_set = true;
     }
+    kernels::tc_hermitian_pack_kernel<<<dim3(vtiles, 2 * kstages), kernels::TH_M, 0, ctx.stream()>>>(a);
+    check_launch("tc_hermitian_pack_kernel");
     dim3 grid(vtiles, splits);
     kernels::tc_hermitian_kernel<<<grid, kernels::TH_THREADS, kernels::TH_SMEM, ctx.stream()>>>(a);
     check_launch("tc_hermitian_kernel");
