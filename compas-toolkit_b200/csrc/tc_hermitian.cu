@@ -41,10 +41,10 @@ constexpr int TH_M = 128, TH_N = 256, TH_K = 64, TH_PAIRS = 64;
 constexpr int TH_THREADS = 576;  // 8 epilogue + 8 B warps + MMA warp + copy warp
 constexpr int TH_MMA_WARP = 16, TH_COPY_WARP = 17;
 constexpr int TH_B_THREADS = 256;
-constexpr int TH_STAGES = 2;
-constexpr int TH_A_BYTES = TH_M * TH_K * 2;
-constexpr int TH_B_BYTES = TH_N * TH_K * 2;
-constexpr int TH_STAGE_BYTES = 2 * TH_A_BYTES + 2 * TH_B_BYTES;
+constexpr int TH_STAGES = 3;
+constexpr int TH_A_BYTES = TH_M * TH_K * 2;           // 16 KB per plane: this CTA's 128 voxels
+constexpr int TH_BH_BYTES = (TH_N / 2) * TH_K * 2;    // 16 KB per plane: this CTA's 128 of the 256 B rows
+constexpr int TH_STAGE_BYTES = 2 * TH_A_BYTES + 2 * TH_BH_BYTES;
 constexpr int TH_SMEM = TH_STAGES * TH_STAGE_BYTES + 1024 + 256;
 constexpr int TH_APACK_BLOCK = 2 * TH_A_BYTES;  // hi + lo image of one (voxel tile, stage)
 
@@ -105,7 +105,11 @@ __global__ void __launch_bounds__(128) tc_hermitian_pack_kernel(ThArgs a) {
     }
 }
 
-__global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
+// One CTA pair (cluster of 2) per pair of voxel tiles and pair-tile range: each CTA loads its own
+// voxel tile's A and converts half of B — rank 0 the rows of Y (u), rank 1 the rows of Ỹ
+// ((k - S/2)·u) — and the leader issues M = 256 MMAs over both. Producers of both CTAs arrive on
+// the leader's barriers; the leader's commits arrive on both CTAs' barriers.
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + TH_STAGES * TH_STAGE_BYTES);
@@ -118,7 +122,8 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int vt = blockIdx.x;
+    const uint32_t rank = tc::cluster_ctarank();
+    const int vt = blockIdx.x;  // this CTA's voxel tile
     const int v0 = vt * TH_M;
     const int split = blockIdx.y;
     const int npairs = a.R * a.C;
@@ -131,21 +136,22 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TH_STAGES; s++) {
-            tc::mbar_init(&full[s], TH_B_THREADS);
+            tc::mbar_init(&full[s], 2 * TH_B_THREADS + 1);  // B of both CTAs + the peer's A landed
             tc::mbar_init(&empty[s], 1);
             tc::mbar_init(&afull[s], 1);
         }
         for (int s = 0; s < 2; s++) {
             tc::mbar_init(&acc_full[s], 1);
-            tc::mbar_init(&acc_empty[s], 256);
+            tc::mbar_init(&acc_empty[s], 2 * 256);  // epilogue threads of both CTAs
         }
         tc::mbar_init(done, 1);
         *abort_flag = 0;
         tc::fence_mbarrier_init();
     }
-    if (warp == TH_MMA_WARP) tc::tmem_alloc(tmem_slot, 512);
+    if (warp == TH_MMA_WARP) tc::tmem_alloc_pair(tmem_slot, 512);
     tc::tc_fence_before();
     __syncthreads();
+    tc::cluster_sync();  // both CTAs' barriers exist before either arrives on the other's
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
@@ -165,6 +171,20 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
         float2 acc[3];
 #pragma unroll
         for (int f = 0; f < 3; f++) acc[f] = make_float2(0.f, 0.f);
+        // echoes of readout r: those of a chunk's first readout are requested one chunk ahead,
+        // the second readout's (4-7 coils) at the start of the chunk, further ones (fewer than 4
+        // coils) when needed
+        auto load_echo = [&](int r, float2& e0, float2& e1, float2& e2) {
+            e0 = e1 = e2 = make_float2(0.f, 0.f);
+            if (vok && r < a.R) {
+                const int64_t idx = int64_t(r) * a.nvoxels + v;
+                e0 = __ldg(a.echo + idx);
+                e1 = __ldg(a.dT1 + idx);
+                e2 = __ldg(a.dT2 + idx);
+            }
+        };
+        float2 m[2], m1[2], m2[2], mn, m1n, m2n;
+        if (ntiles > 0) load_echo((tile_begin * TH_PAIRS + parity * 8) / a.C, m[0], m1[0], m2[0]);
         bool ok = true;
         for (int tl = 0; tl < ntiles; tl++) {
             const int abuf = tl & 1;
@@ -181,9 +201,14 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
             for (int ch = parity; ch < TH_PAIRS / 8; ch += 2) {  // 8 pairs at a time
                 const int pb = p0 + ch * 8;
                 const int rb = pb / a.C;
-                // loads first: the coil factor of each pair and the echoes of the chunk's first
-                // two readouts (more readouts only with fewer than 4 coils: loaded when needed)
-                float2 cc[8], m[2], m1[2], m2[2];
+                if ((pb + 7) / a.C > rb) load_echo(rb + 1, m[1], m1[1], m2[1]);
+                {
+                    const bool more = ch + 2 < TH_PAIRS / 8;
+                    const int tln = more ? tl : tl + 1, chn = more ? ch + 2 : parity;
+                    if (tln < ntiles) load_echo(((tile_begin + tln) * TH_PAIRS + chn * 8) / a.C, mn, m1n, m2n);
+                }
+                // coil factor of each pair (a small table that stays in L1)
+                float2 cc[8];
                 {
                     int c = pb - rb * a.C;
 #pragma unroll
@@ -192,23 +217,10 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
                                                          : make_float2(0.f, 0.f);
                         if (++c == a.C) c = 0;
                     }
-#pragma unroll
-                    for (int q = 0; q < 2; q++) {
-                        const int r = rb + q;
-                        m[q] = m1[q] = m2[q] = make_float2(0.f, 0.f);
-                        if (vok && r < a.R) {
-                            const int64_t idx = int64_t(r) * a.nvoxels + v;
-                            m[q] = __ldg(a.echo + idx);
-                            m1[q] = __ldg(a.dT1 + idx);
-                            m2[q] = __ldg(a.dT2 + idx);
-                        }
-                    }
                 }
                 float yr[8], yi[8], tr[8], ti[8];
-                tc::tmem_load8(tbase + 0 * 64 + ch * 8, yr);
-                tc::tmem_load8(tbase + 1 * 64 + ch * 8, yi);
-                tc::tmem_load8(tbase + 2 * 64 + ch * 8, tr);
-                tc::tmem_load8(tbase + 3 * 64 + ch * 8, ti);
+                tc::tmem_load8x4(tbase + 0 * 64 + ch * 8, tbase + 1 * 64 + ch * 8, tbase + 2 * 64 + ch * 8,
+                                 tbase + 3 * 64 + ch * 8, yr, yi, tr, ti);
                 int r = rb, c = pb - rb * a.C;
                 float2 Z = make_float2(0.f, 0.f), Zt = Z;
 #pragma unroll
@@ -224,13 +236,7 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
                         } else if (r == rb + 1) {
                             me = m[1], d1 = m1[1], d2 = m2[1];
                         } else {
-                            me = d1 = d2 = make_float2(0.f, 0.f);
-                            if (vok && r < a.R) {
-                                const int64_t idx = int64_t(r) * a.nvoxels + v;
-                                me = __ldg(a.echo + idx);
-                                d1 = __ldg(a.dT1 + idx);
-                                d2 = __ldg(a.dT2 + idx);
-                            }
+                            load_echo(r, me, d1, d2);
                         }
                         acc[0] = cadd(acc[0], cmulc(Z, d1));
                         acc[1] = cadd(acc[1], cadd(cmulc(Z, d2), cscale(dscale, cmulc(Zt, me))));
@@ -242,9 +248,12 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
                         ++r;
                     }
                 }
+                m[0] = mn;
+                m1[0] = m1n;
+                m2[0] = m2n;
             }
             tc::tc_fence_before();
-            tc::mbar_arrive(&acc_empty[abuf]);
+            tc::mbar_arrive_cluster(&acc_empty[abuf], 0);
         }
         // combine the two warps of each lane quarter through shared memory (stage buffer 0,
         // free once every tile has been consumed) and write the four results
@@ -267,12 +276,13 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
             o[3 * int64_t(a.nvoxels) + v] = make_float2(acc[2].y, -acc[2].x);  // -i·mHv
         }
     } else if (warp < 16) {
-        // ---------------- B producer: u → rows (u_re,-u_im), (u_im,u_re) and their (k-S/2)-scaled
-        // copies; thread = (pair pl of the tile, 8-sample quarter of the stage)
+        // ---------------- B producer: this CTA's 128 of the 256 B rows — rank 0 (u_re,-u_im),
+        // (u_im,u_re), rank 1 the same of (k-S/2)·u; thread = (pair pl, 8-sample quarter)
         const int t = threadIdx.x - 256;
         const int pl = t & 63, qtr = t >> 6;
-        float2 uv[8];
-        auto load_u = [&](int g) {
+        // u is loaded two stages ahead: stage g + 2 is requested once stage g is converted
+        float2 uv[8], uv1[8];
+        auto load_u = [&](int g, float2 (&dst)[8]) {
             const int tl = g / kstages, ks = g - tl * kstages;
             const int p = (tile_begin + tl) * TH_PAIRS + pl;
             const bool pok = p < npairs;
@@ -280,56 +290,52 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
             const float2* urow = a.u + (int64_t(c) * a.R + r) * a.S;
             const int kb = ks * 32 + qtr * 8;
 #pragma unroll
-            for (int i = 0; i < 8; i++) uv[i] = (pok && kb + i < a.S) ? __ldg(urow + kb + i) : make_float2(0.f, 0.f);
+            for (int i = 0; i < 8; i++) dst[i] = (pok && kb + i < a.S) ? __ldg(urow + kb + i) : make_float2(0.f, 0.f);
         };
-        if (nstages > 0) load_u(0);
+        if (nstages > 0) load_u(0, uv);
+        if (nstages > 1) load_u(1, uv1);
         for (int g = 0; g < nstages; g++) {
             const int buf = g % TH_STAGES;
             const int ks = g % kstages;
             if (!tc::mbar_wait(&empty[buf], ((g / TH_STAGES) & 1) ^ 1, a.status)) *abort_flag = 1;
             if (*(volatile int*)abort_flag) break;
             unsigned char* Bh = smem + buf * TH_STAGE_BYTES + 2 * TH_A_BYTES;
-            unsigned char* Bl = Bh + TH_B_BYTES;
+            unsigned char* Bl = Bh + TH_BH_BYTES;
             const int kb = ks * 32 + qtr * 8;
 #pragma unroll
             for (int cq = 0; cq < 2; cq++) {  // 4 samples per 16-byte chunk
                 // one hi/lo split per value: the split of (x, -y) is the split of (x, y) with the
                 // upper sign bit flipped, the split of (y, x) the same pair with halves swapped
-                uint32_t h0[4], l0[4], h1[4], l1[4], h2[4], l2[4], h3[4], l3[4];
+                uint32_t h0[4], l0[4], h1[4], l1[4];
 #pragma unroll
                 for (int i = 0; i < 4; i++) {
-                    const float2 w = uv[4 * cq + i];
-                    const float ksf = float(kb + 4 * cq + i) - 0.5f * float(a.S);
-                    uint32_t h, l, hs, ls;
+                    float2 w = uv[4 * cq + i];
+                    if (rank) {
+                        const float ksf = float(kb + 4 * cq + i) - 0.5f * float(a.S);
+                        w = make_float2(ksf * w.x, ksf * w.y);
+                    }
+                    uint32_t h, l;
                     tc::split2(w.x, w.y, h, l);
-                    tc::split2(ksf * w.x, ksf * w.y, hs, ls);
                     h0[i] = h ^ 0x80000000u;
                     l0[i] = l ^ 0x80000000u;
                     h1[i] = __byte_perm(h, 0, 0x1032);
                     l1[i] = __byte_perm(l, 0, 0x1032);
-                    h2[i] = hs ^ 0x80000000u;
-                    l2[i] = ls ^ 0x80000000u;
-                    h3[i] = __byte_perm(hs, 0, 0x1032);
-                    l3[i] = __byte_perm(ls, 0, 0x1032);
                 }
                 const int chunk = qtr * 2 + cq;
-                const uint32_t o0 = tc::sw128_offset(0 * 64 + pl, chunk), o1 = tc::sw128_offset(1 * 64 + pl, chunk);
-                const uint32_t o2 = tc::sw128_offset(2 * 64 + pl, chunk), o3 = tc::sw128_offset(3 * 64 + pl, chunk);
+                const uint32_t o0 = tc::sw128_offset(pl, chunk), o1 = tc::sw128_offset(64 + pl, chunk);
                 *reinterpret_cast<uint4*>(Bh + o0) = make_uint4(h0[0], h0[1], h0[2], h0[3]);
                 *reinterpret_cast<uint4*>(Bl + o0) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
                 *reinterpret_cast<uint4*>(Bh + o1) = make_uint4(h1[0], h1[1], h1[2], h1[3]);
                 *reinterpret_cast<uint4*>(Bl + o1) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
-                *reinterpret_cast<uint4*>(Bh + o2) = make_uint4(h2[0], h2[1], h2[2], h2[3]);
-                *reinterpret_cast<uint4*>(Bl + o2) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
-                *reinterpret_cast<uint4*>(Bh + o3) = make_uint4(h3[0], h3[1], h3[2], h3[3]);
-                *reinterpret_cast<uint4*>(Bl + o3) = make_uint4(l3[0], l3[1], l3[2], l3[3]);
             }
             tc::fence_async_shared();
-            tc::mbar_arrive(&full[buf]);
-            if (g + 1 < nstages) load_u(g + 1);  // in flight while the next stage's slot frees up
+            tc::mbar_arrive_cluster(&full[buf], 0);
+#pragma unroll
+            for (int i = 0; i < 8; i++) uv[i] = uv1[i];
+            if (g + 2 < nstages) load_u(g + 2, uv1);
         }
     } else if (warp == TH_COPY_WARP) {
-        // ---------------- A: one bulk copy (hi + lo, 32 KB) per stage
+        // ---------------- A: one bulk copy (hi + lo, 32 KB) per stage into this CTA's buffer
         if (lane == 0) {
             const unsigned char* src = a.apack + int64_t(vt) * kstages * TH_APACK_BLOCK;
             int issued[TH_STAGES];
@@ -347,10 +353,10 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
             for (int s = 0; s < TH_STAGES; s++)
                 if (issued[s] >= 0) tc::mbar_wait(&afull[s], (issued[s] / TH_STAGES) & 1, a.status);
         }
-    } else {
-        // ---------------- MMA issuer (warp 16, one lane)
+    } else if (rank == 0) {
+        // ---------------- MMA issuer (leader, warp 16, one lane): M = 256 over both CTAs
         if (lane == 0) {
-            constexpr uint32_t idesc = tc::idesc_bf16_f32(TH_M, TH_N);
+            constexpr uint32_t idesc = tc::idesc_bf16_f32(2 * TH_M, TH_N);
             int g = 0;
             for (int tl = 0; tl < ntiles && !*(volatile int*)abort_flag; tl++) {
                 const int abuf = tl & 1;
@@ -368,30 +374,43 @@ __global__ void __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
                     tc::tc_fence_after();
                     const uint32_t base = tc::smem_u32(smem + buf * TH_STAGE_BYTES);
                     const uint32_t ah = base, al = base + TH_A_BYTES;
-                    const uint32_t bh = base + 2 * TH_A_BYTES, bl = bh + TH_B_BYTES;
+                    const uint32_t bh = base + 2 * TH_A_BYTES, bl = bh + TH_BH_BYTES;
 #pragma unroll
                     for (int k16 = 0; k16 < TH_K / 16; k16++) {
                         const uint32_t koff = k16 * 32;
                         const uint64_t dah = tc::sw128_kmajor_desc(ah + koff), dal = tc::sw128_kmajor_desc(al + koff);
                         const uint64_t dbh = tc::sw128_kmajor_desc(bh + koff), dbl = tc::sw128_kmajor_desc(bl + koff);
-                        tc::mma_bf16(d, dah, dbh, idesc, (ks > 0 || k16 > 0) ? 1u : 0u);
-                        tc::mma_bf16(d, dah, dbl, idesc, 1u);
-                        tc::mma_bf16(d, dal, dbh, idesc, 1u);
+                        tc::mma_bf16_pair(d, dah, dbh, idesc, (ks > 0 || k16 > 0) ? 1u : 0u);
+                        tc::mma_bf16_pair(d, dah, dbl, idesc, 1u);
+                        tc::mma_bf16_pair(d, dal, dbh, idesc, 1u);
                     }
-                    tc::mma_commit(&empty[buf]);
+                    tc::mma_commit_pair(&empty[buf]);
                 }
-                tc::mma_commit(&acc_full[abuf]);
+                tc::mma_commit_pair(&acc_full[abuf]);
             }
-            tc::mma_commit(done);
+            tc::mma_commit_pair(done);
             tc::mbar_wait(done, 0, a.status);  // all MMAs complete before TMEM is released
+        }
+        __syncwarp();
+    } else {
+        // ---------------- peer, warp 16: tell the leader when each stage's A has landed here
+        if (lane == 0) {
+            for (int g = 0; g < nstages; g++) {
+                const int buf = g % TH_STAGES;
+                if (!tc::mbar_wait(&afull[buf], (g / TH_STAGES) & 1, a.status)) *abort_flag = 1;
+                if (*(volatile int*)abort_flag) break;
+                tc::mbar_arrive_cluster(&full[buf], 0);
+            }
+            tc::mbar_wait(done, 0, a.status);
         }
         __syncwarp();
     }
     tc::tc_fence_before();
     __syncthreads();
+    tc::cluster_sync();  // neither CTA leaves while the other may still signal it or read TMEM
     if (warp == TH_MMA_WARP) {
         tc::tc_fence_after();
-        tc::tmem_dealloc(tmem, 512);
+        tc::tmem_dealloc_pair(tmem, 512);
     }
 }
 
@@ -423,7 +442,7 @@ bool launch_jacobian_hermitian_tc(const CompasContext& ctx, const float* params,
     a.dk_re = g.dk_re;
     a.dk_im = g.dk_im;
     a.status = detail::device_status_word(ctx.device());
-    const int vtiles = div_ceil(nvoxels, kernels::TH_M);
+    const int vtiles = 2 * div_ceil(nvoxels, 2 * kernels::TH_M);  // whole CTA pairs
     const int ptiles = div_ceil(ncoils * g.nreadouts, kernels::TH_PAIRS);
     const int kstages = div_ceil(g.ns, 32);
     int sms = 148;
