@@ -12,9 +12,9 @@
 // two FP32 [2][R][V] arrays per coil and re-reads the echoes per coil).
 //
 // Real-ified operands (re/im interleaved along K = 2S):
-//   A'[v]            = (Re ē_k, Im ē_k) with ē = conj(E_k(v))     — 128 voxels × 32 samples per stage
-//   B'[0·64 + p]     = (u_re, -u_im)     → Y_re    B'[1·64 + p] = (u_im, u_re)      → Y_im
-//   B'[2·64 + p]     = (k-S/2)(u_re, -u_im) → Ỹ_re B'[3·64 + p] = (k-S/2)(u_im, u_re) → Ỹ_im
+//   A'[v]  = (Re ē_k, Im ē_k) with ē = conj(E_k(v))     — 256 voxels (a CTA pair) × 32 samples per stage
+//   B'[n]  for n = h·128 + type·32 + q, pair p = h·32 + q of the 64-pair tile:
+//          type 0 (u_re, -u_im) → Y_re, 1 (u_im, u_re) → Y_im, 2 and 3 the same of (k-S/2)·u → Ỹ_re, Ỹ_im
 // A does not depend on the pair tile, so a small kernel writes it once per call as the swizzled
 // BF16 hi/lo shared-memory images of every (voxel tile, 32-sample stage): E_k exactly at every
 // 16th sample (phase reduced modulo 2π in FP64) and the complex recurrence in between. The
@@ -106,9 +106,9 @@ __global__ void __launch_bounds__(128) tc_hermitian_pack_kernel(ThArgs a) {
 }
 
 // One CTA pair (cluster of 2) per pair of voxel tiles and pair-tile range: each CTA loads its own
-// voxel tile's A and converts half of B — rank 0 the rows of Y (u), rank 1 the rows of Ỹ
-// ((k - S/2)·u) — and the leader issues M = 256 MMAs over both. Producers of both CTAs arrive on
-// the leader's barriers; the leader's commits arrive on both CTAs' barriers.
+// voxel tile's A and converts half of B — the four rows of 32 of the tile's 64 pairs, so it reads
+// only those pairs' u — and the leader issues M = 256 MMAs over both. Producers of both CTAs
+// arrive on the leader's barriers; the leader's commits arrive on both CTAs' barriers.
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TH_THREADS, 1) tc_hermitian_kernel(ThArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -219,8 +219,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TH_THREADS, 1) tc_he
                     }
                 }
                 float yr[8], yi[8], tr[8], ti[8];
-                tc::tmem_load8x4(tbase + 0 * 64 + ch * 8, tbase + 1 * 64 + ch * 8, tbase + 2 * 64 + ch * 8,
-                                 tbase + 3 * 64 + ch * 8, yr, yi, tr, ti);
+                // columns: [pair half][Y_re, Y_im, Ỹ_re, Ỹ_im][32 pairs]
+                const uint32_t cb = tbase + uint32_t((ch >> 2) * 128 + (ch & 3) * 8);
+                tc::tmem_load8x4(cb, cb + 32, cb + 64, cb + 96, yr, yi, tr, ti);
                 int r = rb, c = pb - rb * a.C;
                 float2 Z = make_float2(0.f, 0.f), Zt = Z;
 #pragma unroll
@@ -276,21 +277,34 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TH_THREADS, 1) tc_he
             o[3 * int64_t(a.nvoxels) + v] = make_float2(acc[2].y, -acc[2].x);  // -i·mHv
         }
     } else if (warp < 16) {
-        // ---------------- B producer: this CTA's 128 of the 256 B rows — rank 0 (u_re,-u_im),
-        // (u_im,u_re), rank 1 the same of (k-S/2)·u; thread = (pair pl, 8-sample quarter)
+        // ---------------- B producer: the CTA's 32 pairs of the tile (rank·32 ..), all four rows
+        // each: (u_re,-u_im) → Y_re, (u_im,u_re) → Y_im and the same of (k-S/2)·u → Ỹ_re, Ỹ_im.
+        // thread = (pair q, 4-sample quad sq): 8 lanes cover one pair's 32 samples, so each load
+        // instruction reads 4 contiguous 128-byte pieces of u
         const int t = threadIdx.x - 256;
-        const int pl = t & 63, qtr = t >> 6;
+        const int sq = t & 7, q = t >> 3;
+        const int pl = int(rank) * 32 + q;  // pair within the tile
         // u is loaded two stages ahead: stage g + 2 is requested once stage g is converted
-        float2 uv[8], uv1[8];
-        auto load_u = [&](int g, float2 (&dst)[8]) {
+        const bool vec16 = (a.S & 1) == 0 && (reinterpret_cast<uintptr_t>(a.u) & 15) == 0;  // 16-byte aligned rows
+        float2 uv[4], uv1[4];
+        auto load_u = [&](int g, float2 (&dst)[4]) {
             const int tl = g / kstages, ks = g - tl * kstages;
             const int p = (tile_begin + tl) * TH_PAIRS + pl;
             const bool pok = p < npairs;
             const int r = pok ? p / a.C : 0, c = pok ? p - r * a.C : 0;
             const float2* urow = a.u + (int64_t(c) * a.R + r) * a.S;
-            const int kb = ks * 32 + qtr * 8;
+            const int kb = ks * 32 + sq * 4;
+            if (pok && vec16 && kb + 4 <= a.S) {
+                const float4 x0 = __ldg(reinterpret_cast<const float4*>(urow + kb));
+                const float4 x1 = __ldg(reinterpret_cast<const float4*>(urow + kb + 2));
+                dst[0] = make_float2(x0.x, x0.y);
+                dst[1] = make_float2(x0.z, x0.w);
+                dst[2] = make_float2(x1.x, x1.y);
+                dst[3] = make_float2(x1.z, x1.w);
+            } else {
 #pragma unroll
-            for (int i = 0; i < 8; i++) dst[i] = (pok && kb + i < a.S) ? __ldg(urow + kb + i) : make_float2(0.f, 0.f);
+                for (int i = 0; i < 4; i++) dst[i] = (pok && kb + i < a.S) ? __ldg(urow + kb + i) : make_float2(0.f, 0.f);
+            }
         };
         if (nstages > 0) load_u(0, uv);
         if (nstages > 1) load_u(1, uv1);
@@ -301,37 +315,41 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TH_THREADS, 1) tc_he
             if (*(volatile int*)abort_flag) break;
             unsigned char* Bh = smem + buf * TH_STAGE_BYTES + 2 * TH_A_BYTES;
             unsigned char* Bl = Bh + TH_BH_BYTES;
-            const int kb = ks * 32 + qtr * 8;
+            const int kb = ks * 32 + sq * 4;
+            // one hi/lo split per value: the split of (x, -y) is the split of (x, y) with the upper
+            // sign bit flipped, the split of (y, x) the same pair with halves swapped
+            uint32_t h0[4], l0[4], h1[4], l1[4], h2[4], l2[4], h3[4], l3[4];
 #pragma unroll
-            for (int cq = 0; cq < 2; cq++) {  // 4 samples per 16-byte chunk
-                // one hi/lo split per value: the split of (x, -y) is the split of (x, y) with the
-                // upper sign bit flipped, the split of (y, x) the same pair with halves swapped
-                uint32_t h0[4], l0[4], h1[4], l1[4];
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    float2 w = uv[4 * cq + i];
-                    if (rank) {
-                        const float ksf = float(kb + 4 * cq + i) - 0.5f * float(a.S);
-                        w = make_float2(ksf * w.x, ksf * w.y);
-                    }
-                    uint32_t h, l;
-                    tc::split2(w.x, w.y, h, l);
-                    h0[i] = h ^ 0x80000000u;
-                    l0[i] = l ^ 0x80000000u;
-                    h1[i] = __byte_perm(h, 0, 0x1032);
-                    l1[i] = __byte_perm(l, 0, 0x1032);
-                }
-                const int chunk = qtr * 2 + cq;
-                const uint32_t o0 = tc::sw128_offset(pl, chunk), o1 = tc::sw128_offset(64 + pl, chunk);
-                *reinterpret_cast<uint4*>(Bh + o0) = make_uint4(h0[0], h0[1], h0[2], h0[3]);
-                *reinterpret_cast<uint4*>(Bl + o0) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
-                *reinterpret_cast<uint4*>(Bh + o1) = make_uint4(h1[0], h1[1], h1[2], h1[3]);
-                *reinterpret_cast<uint4*>(Bl + o1) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
+            for (int i = 0; i < 4; i++) {
+                const float2 w = uv[i];
+                const float ksf = float(kb + i) - 0.5f * float(a.S);
+                uint32_t h, l, hs, ls;
+                tc::split2(w.x, w.y, h, l);
+                tc::split2(ksf * w.x, ksf * w.y, hs, ls);
+                h0[i] = h ^ 0x80000000u;
+                l0[i] = l ^ 0x80000000u;
+                h1[i] = __byte_perm(h, 0, 0x1032);
+                l1[i] = __byte_perm(l, 0, 0x1032);
+                h2[i] = hs ^ 0x80000000u;
+                l2[i] = ls ^ 0x80000000u;
+                h3[i] = __byte_perm(hs, 0, 0x1032);
+                l3[i] = __byte_perm(ls, 0, 0x1032);
             }
+            // local row = type·32 + q (global B row rank·128 + type·32 + q), 16-byte chunk sq
+            const uint32_t o0 = tc::sw128_offset(0 * 32 + q, sq), o1 = tc::sw128_offset(1 * 32 + q, sq);
+            const uint32_t o2 = tc::sw128_offset(2 * 32 + q, sq), o3 = tc::sw128_offset(3 * 32 + q, sq);
+            *reinterpret_cast<uint4*>(Bh + o0) = make_uint4(h0[0], h0[1], h0[2], h0[3]);
+            *reinterpret_cast<uint4*>(Bl + o0) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
+            *reinterpret_cast<uint4*>(Bh + o1) = make_uint4(h1[0], h1[1], h1[2], h1[3]);
+            *reinterpret_cast<uint4*>(Bl + o1) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
+            *reinterpret_cast<uint4*>(Bh + o2) = make_uint4(h2[0], h2[1], h2[2], h2[3]);
+            *reinterpret_cast<uint4*>(Bl + o2) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
+            *reinterpret_cast<uint4*>(Bh + o3) = make_uint4(h3[0], h3[1], h3[2], h3[3]);
+            *reinterpret_cast<uint4*>(Bl + o3) = make_uint4(l3[0], l3[1], l3[2], l3[3]);
             tc::fence_async_shared();
             tc::mbar_arrive_cluster(&full[buf], 0);
 #pragma unroll
-            for (int i = 0; i < 8; i++) uv[i] = uv1[i];
+            for (int i = 0; i < 4; i++) uv[i] = uv1[i];
             if (g + 2 < nstages) load_u(g + 2, uv1);
         }
     } else if (warp == TH_COPY_WARP) {
