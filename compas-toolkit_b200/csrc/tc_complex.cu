@@ -16,16 +16,20 @@
 // Per call, small kernels first write per-voxel tables (the E_k step, E_k itself at every
 // TC_PPG-th sample with the phase reduced in FP64, coil·w, the J·v coefficients) and pack A once
 // as the split, swizzled shared-memory images the contraction consumes.
-// CTA organisation of the contraction (576 threads, 1 CTA/SM, 192 KB shared memory in 2 stages):
-//   warps 0-15  generate the B tile (256 rows × 64 K): thread = (2 voxels, group of TC_PPG pairs);
-//               a group starts from the exact E_k table value × coil·w and steps along k with the
-//               complex recurrence. Afterwards they drain the TMEM accumulator through shared
-//               memory into coalesced rows of the output;
-//   warp 16     allocates 256 TMEM columns and one lane issues the 12 MMAs per stage;
+// The contraction runs on CTA pairs (cluster of 2, tcgen05 cta_group::2): one MMA of M = 256
+// readouts (128 per CTA) × N = 256 spans both SMs' tensor cores; each CTA holds its own A half and
+// generates the B rows of half the tile's 128 pairs.
+// CTA organisation (576 threads, 1 CTA/SM, 192 KB shared memory in 3 stages of 64 KB):
+//   warps 0-15  generate this CTA's half of the B tile (128 rows × 64 K): thread = (2 voxels,
+//               group of TC_PPG pairs); a group starts from the exact E_k table value × coil·w and
+//               steps along k with the complex recurrence. Afterwards they drain the TMEM
+//               accumulator through shared memory into coalesced rows of the output;
+//   warp 16     allocates 256 TMEM columns (both CTAs); in the leader one lane issues the 12 MMAs
+//               per stage, in the peer one lane tells the leader when its A has landed;
 //   warp 17     one lane loads each stage's A image (32 KB) with one bulk copy.
-// Stages hand over through mbarriers (full: producers → MMA, afull: copy landed, empty:
-// tcgen05.commit → producers and copy). The voxel range is split over CTAs (split-K); partial
-// tiles are summed in a fixed order. Every wait is bounded.
+// Stages hand over through mbarriers (full, in the leader: producers of both CTAs → MMA; afull:
+// copy landed; empty, in both: tcgen05.commit multicast → producers and copy). The voxel range is
+// split over CTA pairs (split-K); partial tiles are summed in a fixed order. Every wait is bounded.
 #include <cuda_bf16.h>
 
 #include <mutex>
@@ -42,20 +46,20 @@ void sum_partials(const CompasContext& ctx, const cfloat* partials, int nsplit, 
 
 namespace kernels {
 
-constexpr int TC_M = 128, TC_N = 256, TC_K = 64;  // real-ified tile
+constexpr int TC_M = 128, TC_N = 256, TC_K = 64;  // real-ified tile of one CTA (M = 256 per CTA pair)
 constexpr int TC_PAIRS = TC_N / 2;                 // complex (c, k) pairs per tile
-constexpr int TC_PPG = 4;                          // consecutive pairs per producer thread
+constexpr int TC_PPG = 2;                          // consecutive pairs per producer thread
 constexpr int TC_B_THREADS = 512;                  // 16 producer warps: 16 voxel halves × 32 groups
 constexpr int TC_MMA_WARP = 16, TC_COPY_WARP = 17;
 constexpr int TC_THREADS = 576;
-constexpr int TC_STAGES = 2;
-constexpr int TC_A_BYTES = TC_M * TC_K * 2;  // 16 KB per hi/lo plane
-constexpr int TC_B_BYTES = TC_N * TC_K * 2;  // 32 KB per hi/lo plane
-constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
+constexpr int TC_STAGES = 3;
+constexpr int TC_A_BYTES = TC_M * TC_K * 2;         // 16 KB per hi/lo plane: this CTA's 128 readouts
+constexpr int TC_BH_BYTES = (TC_N / 2) * TC_K * 2;  // 16 KB per hi/lo plane: this CTA's 128 of the 256 B rows
+constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_BH_BYTES;
 constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 128 /*barriers*/;
 constexpr int TC_APACK_BLOCK = 2 * TC_A_BYTES;  // hi + lo image of one (readout tile, voxel stage)
 constexpr int TC_TROW = TC_PAIRS + 2;           // float2 per row of the transposed output tile
-static_assert(TC_PAIRS == (TC_B_THREADS / 16) * TC_PPG, "producer groups cover the pair tile");
+static_assert(TC_PAIRS / 2 == (TC_B_THREADS / 16) * TC_PPG, "a CTA's producer groups cover half the pair tile");
 static_assert(TC_M * TC_TROW * 8 <= TC_STAGES * TC_STAGE_BYTES, "output tile fits the stage buffers");
 static_assert((TC_TROW * 8) % 16 == 0, "transposed rows stay 16-byte aligned");
 
@@ -151,9 +155,12 @@ __global__ void tc_pack_a_kernel(TcArgs a) {
     tc_pack_a<JAC>(a, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
 }
 
-// One output tile (pair tile bx, readout tile by, voxel split bz) of one contraction. Shared by
-// the one-operation kernel (tile = blockIdx) and the batched kernel, so both give bit-identical
-// results.
+// One output tile (pair tile bx, readout tile by, voxel split bz) of one contraction, computed by
+// a CTA pair (cluster of 2, readout tiles by = 2·i and 2·i + 1, rank = by & 1): each CTA loads its
+// readout tile's A and generates the B rows of half the tile's pairs (rank·64 ..), the leader
+// issues M = 256 MMAs over both, producers of both CTAs arrive on the leader's barriers and the
+// leader's commits arrive on both. Shared by the one-operation kernel and the batched kernel, so
+// both give bit-identical results.
 template<bool JAC>
 __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int by, const int bz,
                                         unsigned char* smem_raw) {
@@ -169,6 +176,7 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = tc::cluster_ctarank();
     const int n_pair0 = bx * TC_PAIRS;  // first (c,k) pair of this tile
     const int r0 = by * TC_M;
     const int v_begin = bz * a.vchunk;
@@ -178,7 +186,7 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < TC_STAGES; s++) {
-            tc::mbar_init(&full[s], TC_B_THREADS);
+            tc::mbar_init(&full[s], 2 * TC_B_THREADS + 1);  // B of both CTAs + the peer's A landed
             tc::mbar_init(&empty[s], 1);
             tc::mbar_init(&afull[s], 1);
         }
@@ -186,9 +194,10 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
         *abort_flag = 0;
         tc::fence_mbarrier_init();
     }
-    if (warp == TC_MMA_WARP) tc::tmem_alloc(tmem_slot, 256);
+    if (warp == TC_MMA_WARP) tc::tmem_alloc_pair(tmem_slot, 256);
     tc::tc_fence_before();
     __syncthreads();
+    tc::cluster_sync();  // both CTAs' barriers exist before either arrives on the other's
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
@@ -211,10 +220,10 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
             for (int s = 0; s < TC_STAGES; s++)
                 if (issued[s] >= 0) tc::mbar_wait(&afull[s], (issued[s] / TC_STAGES) & 1, a.status);
         }
-    } else if (warp == TC_MMA_WARP) {
-        // ---------------- MMA issuer (one lane)
+    } else if (warp == TC_MMA_WARP && rank == 0) {
+        // ---------------- MMA issuer (leader, one lane): M = 256 over both CTAs
         if (lane == 0) {
-            constexpr uint32_t idesc = tc::idesc_bf16_f32(TC_M, TC_N);
+            constexpr uint32_t idesc = tc::idesc_bf16_f32(2 * TC_M, TC_N);
             for (int it = 0; it < nstages; it++) {
                 const int buf = it % TC_STAGES;
                 if (!tc::mbar_wait(&full[buf], (it / TC_STAGES) & 1, a.status)) *abort_flag = 1;
@@ -223,28 +232,41 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
                 tc::tc_fence_after();
                 const uint32_t base = tc::smem_u32(smem + buf * TC_STAGE_BYTES);
                 const uint32_t ah = base, al = base + TC_A_BYTES;
-                const uint32_t bh = base + 2 * TC_A_BYTES, bl = bh + TC_B_BYTES;
+                const uint32_t bh = base + 2 * TC_A_BYTES, bl = bh + TC_BH_BYTES;
 #pragma unroll
                 for (int ks = 0; ks < TC_K / 16; ks++) {
                     const uint32_t koff = ks * 32;  // 16 bf16 = 32 bytes along K inside the swizzle atom
                     const uint64_t dah = tc::sw128_kmajor_desc(ah + koff), dal = tc::sw128_kmajor_desc(al + koff);
                     const uint64_t dbh = tc::sw128_kmajor_desc(bh + koff), dbl = tc::sw128_kmajor_desc(bl + koff);
-                    tc::mma_bf16(tmem, dah, dbh, idesc, (it > 0 || ks > 0) ? 1u : 0u);
-                    tc::mma_bf16(tmem, dah, dbl, idesc, 1u);
-                    tc::mma_bf16(tmem, dal, dbh, idesc, 1u);
+                    tc::mma_bf16_pair(tmem, dah, dbh, idesc, (it > 0 || ks > 0) ? 1u : 0u);
+                    tc::mma_bf16_pair(tmem, dah, dbl, idesc, 1u);
+                    tc::mma_bf16_pair(tmem, dal, dbh, idesc, 1u);
                 }
-                tc::mma_commit(&empty[buf]);
+                tc::mma_commit_pair(&empty[buf]);
             }
-            tc::mma_commit(done);
+            tc::mma_commit_pair(done);
             tc::mbar_wait(done, 0, a.status);  // the MMAs finish before the TMEM is released
         }
         __syncwarp();
+    } else if (warp == TC_MMA_WARP) {
+        // ---------------- peer, warp 16: tell the leader when each stage's A has landed here
+        if (lane == 0) {
+            for (int it = 0; it < nstages; it++) {
+                const int buf = it % TC_STAGES;
+                if (!tc::mbar_wait(&afull[buf], (it / TC_STAGES) & 1, a.status)) *abort_flag = 1;
+                if (*(volatile int*)abort_flag) break;
+                tc::mbar_arrive_cluster(&full[buf], 0);
+            }
+            tc::mbar_wait(done, 0, a.status);
+        }
+        __syncwarp();
     } else {
-        // ---------------- B producers: TC_PAIRS pairs × VPS voxels of F = coil·w·E_k per stage.
+        // ---------------- B producers: this CTA's TC_PAIRS / 2 pairs (rank·64 ..) × VPS voxels of
+        // F = coil·w·E_k per stage; local B rows 2j, 2j+1 for local pair j.
         // thread → (8-byte half chunk hq = VPH voxels, group pg of TC_PPG consecutive pairs)
         const int t = threadIdx.x;
         const int hq = t & 15, pg = t >> 4;
-        const int n_first = n_pair0 + pg * TC_PPG;
+        const int n_first = n_pair0 + int(rank) * (TC_PAIRS / 2) + pg * TC_PPG;
         const int c_first = n_first / a.S, k_first = n_first - c_first * a.S;
         const bool group_ok = n_first < npairs;
         // the group's start value E_{k_first} (k_first is a multiple of egk), step and coil·w
@@ -272,7 +294,7 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
             if (!tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status)) *abort_flag = 1;
             if (*(volatile int*)abort_flag) break;
             unsigned char* Bh = smem + buf * TC_STAGE_BYTES + 2 * TC_A_BYTES;
-            unsigned char* Bl = Bh + TC_B_BYTES;
+            unsigned char* Bl = Bh + TC_BH_BYTES;
             float2 G[VPH];
 #pragma unroll
             for (int i = 0; i < VPH; i++) G[i] = cmul(e0[i], cw[i]);
@@ -325,7 +347,7 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
                 *reinterpret_cast<uint2*>(Bl + o1) = make_uint2(l1[0], l1[1]);
             }
             tc::fence_async_shared();
-            tc::mbar_arrive(&full[buf]);
+            tc::mbar_arrive_cluster(&full[buf], 0);
 #pragma unroll
             for (int i = 0; i < VPH; i++) {
                 step[i] = step_n[i];
@@ -377,21 +399,23 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
     }
     tc::tc_fence_before();
     __syncthreads();
+    tc::cluster_sync();  // neither CTA leaves while the other may still signal it or read TMEM
     if (warp == TC_MMA_WARP) {
         tc::tc_fence_after();
-        tc::tmem_dealloc(tmem, 256);
+        tc::tmem_dealloc_pair(tmem, 256);
     }
 }
 
+// grid (readout tiles, pair tiles, voxel splits); readout tiles 2i, 2i+1 form a cluster
 template<bool JAC>
-__global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    tc_tile<JAC>(a, blockIdx.x, blockIdx.y, blockIdx.z, smem_raw);
+    tc_tile<JAC>(a, blockIdx.y, blockIdx.x, blockIdx.z, smem_raw);
 }
 
-// tile grid of one contraction: (pair tiles, readout tiles, voxel splits)
+// tile grid of one contraction: (pair tiles, readout-tile pairs, voxel splits)
 __device__ __forceinline__ int3 tc_grid_of(const TcArgs& a) {
-    return make_int3((a.C * a.S + TC_PAIRS - 1) / TC_PAIRS, (a.R + TC_M - 1) / TC_M,
+    return make_int3((a.C * a.S + TC_PAIRS - 1) / TC_PAIRS, (a.R + 2 * TC_M - 1) / (2 * TC_M),
                      (a.nvoxels + a.vchunk - 1) / a.vchunk);
 }
 
@@ -407,13 +431,13 @@ __device__ __forceinline__ int job_of_block(const int* __restrict__ offsets, int
 }
 
 // Batched contraction: one launch for many jobs. Flattened CTA b belongs to job j
-// (cta_offsets[j] ≤ b < cta_offsets[j+1]) and takes the tile the one-operation grid of that job
-// would give blockIdx = (l % nx, (l / nx) % ny, l / (nx·ny)), l = b - cta_offsets[j]. Jobs are
+// (cta_offsets[j] ≤ b < cta_offsets[j+1], all offsets even) and, with l = b - cta_offsets[j] and
+// (nx, ny) the job's pair tiles and readout-tile pairs, takes pair tile (l/2) % nx, readout tile
+// 2·((l/2 / nx) % ny) + (l & 1) and split (l/2) / (nx·ny); CTAs 2i, 2i+1 form a cluster. Jobs are
 // ordered by decreasing work per CTA, so the block scheduler runs the longest tiles first.
 template<bool JAC>
-__global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_batch_kernel(const TcArgs* __restrict__ jobs,
-                                                                         const int* __restrict__ cta_offsets,
-                                                                         int njobs) {
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
+    tc_contract_batch_kernel(const TcArgs* __restrict__ jobs, const int* __restrict__ cta_offsets, int njobs) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ TcArgs job;
     __shared__ int3 tile;
@@ -421,8 +445,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_batch_kernel(const 
         const int j = job_of_block(cta_offsets, njobs, blockIdx.x);
         job = jobs[j];
         const int3 g = tc_grid_of(job);
-        const int l = blockIdx.x - cta_offsets[j];
-        tile = make_int3(l % g.x, (l / g.x) % g.y, l / (g.x * g.y));
+        const int l = blockIdx.x - cta_offsets[j], l2 = l >> 1;
+        tile = make_int3(l2 % g.x, 2 * ((l2 / g.x) % g.y) + (l & 1), l2 / (g.x * g.y));
     }
     __syncthreads();
     tc_tile<JAC>(job, tile.x, tile.y, tile.z, smem_raw);
@@ -465,7 +489,7 @@ __global__ void tc_pack_batch_kernel(const TcArgs* __restrict__ jobs, const int*
 TcPlan tc_plan(int device, int nvoxels, int R, int S, int C, bool jac) {
     TcPlan p;
     p.ntiles = div_ceil(C * S, kernels::TC_PAIRS);
-    p.mtiles = div_ceil(R, kernels::TC_M);
+    p.mtiles = 2 * div_ceil(R, 2 * kernels::TC_M);  // readout tiles, whole CTA pairs
     const int tiles = p.ntiles * p.mtiles;
     const int vps = jac ? 16 : 32;
     // split the voxel range over CTAs: pick the split count (≥ 16 stages per split) whose grid
@@ -506,7 +530,7 @@ TcTables tc_tables(int nvoxels, int R, int S, int C, bool jac) {
     t.coilw = t.estart + align(8 * V * (S / t.egk));
     t.jcoef = t.coilw + align(8 * V * C);
     t.apack = t.jcoef + align(jac ? 32 * V : 0);
-    t.bytes = t.apack + int64_t(div_ceil(R, kernels::TC_M)) * t.apack_stages * kernels::TC_APACK_BLOCK;
+    t.bytes = t.apack + int64_t(2 * div_ceil(R, 2 * kernels::TC_M)) * t.apack_stages * kernels::TC_APACK_BLOCK;
     return t;
 }
 
@@ -521,7 +545,7 @@ void tc_assign_tables(kernels::TcArgs& a, const TcTables& t, unsigned char* base
 }
 
 int tc_pack_blocks(int R, int apack_stages) {
-    return div_ceil(apack_stages * 32, 256) * div_ceil(R, kernels::TC_M) * kernels::TC_M;
+    return div_ceil(apack_stages * 32, 256) * 2 * div_ceil(R, 2 * kernels::TC_M) * kernels::TC_M;
 }
 
 namespace {
@@ -563,7 +587,7 @@ bool run_tc(const CompasContext& ctx, kernels::TcArgs a, bool jac, cfloat* out) 
     check_launch("tc_prep_kernel / tc_pack_a_kernel");
     auto fn = jac ? kernels::tc_contract_kernel<true> : kernels::tc_contract_kernel<false>;
     set_tc_smem_attribute(jac, false);
-    dim3 grid(plan.ntiles, plan.mtiles, splits);
+    dim3 grid(plan.mtiles, plan.ntiles, splits);
     fn<<<grid, kernels::TC_THREADS, kernels::TC_SMEM, ctx.stream()>>>(a);
     check_launch("tc_contract_kernel");
     if (splits > 1) sum_partials(ctx, partials.data(), splits, n, out);
