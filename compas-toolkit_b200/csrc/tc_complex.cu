@@ -118,40 +118,50 @@ __global__ void tc_prep_kernel(TcArgs a) {
 // is split into hi/lo BF16 and stored at the swizzled position of row r % 128, column j in block
 // (r / 128, stage). Rows past R and columns past V are zero. Every contraction CTA of a readout
 // tile then loads each stage with one bulk copy.
+// Thread = one 16-byte chunk (4 columns) of one row: 4 voxels (signal) or 2 voxels × 2 terms
+// (J·v); a warp reads contiguous echo rows and writes whole 128-byte rows of 4 blocks.
 template<bool JAC>
-__device__ __forceinline__ void tc_pack_a(const TcArgs& a, const int g, const int rp) {
-    if (g >= a.apack_stages * 32) return;
-    constexpr int TERMS = JAC ? 2 : 1;
-    const int stage = g >> 5, j = g & 31;
-    const int v = g / TERMS;
-    float2 e = make_float2(0.f, 0.f);
-    if (rp < a.R && v < a.nvoxels) {
-        const int64_t idx = int64_t(rp) * a.nvoxels + v;
+__device__ __forceinline__ void tc_pack_a(const TcArgs& a, const int cg, const int rp) {
+    if (cg >= a.apack_stages * 8) return;
+    const int stage = cg >> 3, chunk = cg & 7;
+    float2 e[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) e[i] = make_float2(0.f, 0.f);
+    if (rp < a.R) {
+        const int64_t row = int64_t(rp) * a.nvoxels;
         if constexpr (!JAC) {
-            e = a.echo[idx];
+            const int v0 = stage * 32 + chunk * 4;
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                if (v0 + i < a.nvoxels) e[i] = __ldg(a.echo + row + v0 + i);
         } else {
-            const float4 k0 = a.jcoef[2 * int64_t(v)], k1 = a.jcoef[2 * int64_t(v) + 1];
-            const float2 me = a.echo[idx];
-            if ((g & 1) == 0) {
-                const float2 d1 = a.dT1[idx], d2 = a.dT2[idx];
-                e = cadd(cadd(cmul(make_float2(k0.x, k0.y), d1), cmul(make_float2(k0.z, k0.w), d2)),
-                         cmul(make_float2(k1.x, k1.y), me));
-            } else {
-                e = cmul(make_float2(k1.z, k1.w), me);
+            const int v0 = stage * 16 + chunk * 2;
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                const int v = v0 + i;
+                if (v < a.nvoxels) {
+                    // P = c1·∂T1m + c2·∂T2m + cm·m,  Q' = cq·m
+                    const float4 k0 = __ldg(a.jcoef + 2 * int64_t(v)), k1 = __ldg(a.jcoef + 2 * int64_t(v) + 1);
+                    const float2 me = __ldg(a.echo + row + v), d1 = __ldg(a.dT1 + row + v), d2 = __ldg(a.dT2 + row + v);
+                    e[2 * i] = cadd(cadd(cmul(make_float2(k0.x, k0.y), d1), cmul(make_float2(k0.z, k0.w), d2)),
+                                    cmul(make_float2(k1.x, k1.y), me));
+                    e[2 * i + 1] = cmul(make_float2(k1.z, k1.w), me);
+                }
             }
         }
     }
-    uint32_t h, l;
-    tc::split2(e.x, e.y, h, l);
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) tc::split2(e[i].x, e[i].y, h[i], l[i]);
     unsigned char* blk = const_cast<unsigned char*>(a.apack) + (int64_t(rp >> 7) * a.apack_stages + stage) * TC_APACK_BLOCK;
-    const uint32_t off = tc::sw128_offset(rp & 127, j >> 2) + uint32_t(j & 3) * 4;
-    *reinterpret_cast<uint32_t*>(blk + off) = h;
-    *reinterpret_cast<uint32_t*>(blk + TC_A_BYTES + off) = l;
+    const uint32_t off = tc::sw128_offset(rp & 127, chunk);
+    *reinterpret_cast<uint4*>(blk + off) = make_uint4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<uint4*>(blk + TC_A_BYTES + off) = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
-// grid (columns / 256, padded readout rows)
+// grid (chunks / 256, padded readout rows)
 template<bool JAC>
-__global__ void tc_pack_a_kernel(TcArgs a) {
+__global__ void __launch_bounds__(256) tc_pack_a_kernel(TcArgs a) {
     tc_pack_a<JAC>(a, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
 }
 
@@ -468,7 +478,7 @@ __global__ void tc_prep_batch_kernel(const TcArgs* __restrict__ jobs, const int*
 }
 
 // batched tc_pack_a_kernel: flattened 256-thread block b → job j, local block l = b - offsets[j]
-// covering columns (l % gx)·256 + t of padded readout row l / gx, gx = ⌈32·apack_stages / 256⌉
+// covering chunks (l % gx)·256 + t of padded readout row l / gx, gx = ⌈8·apack_stages / 256⌉
 template<bool JAC>
 __global__ void tc_pack_batch_kernel(const TcArgs* __restrict__ jobs, const int* __restrict__ block_offsets,
                                      int njobs) {
@@ -480,7 +490,7 @@ __global__ void tc_pack_batch_kernel(const TcArgs* __restrict__ jobs, const int*
         local = blockIdx.x - block_offsets[j];
     }
     __syncthreads();
-    const int gx = (job.apack_stages * 32 + 255) / 256;
+    const int gx = (job.apack_stages * 8 + 255) / 256;
     tc_pack_a<JAC>(job, (local % gx) * 256 + threadIdx.x, local / gx);
 }
 
@@ -545,7 +555,7 @@ void tc_assign_tables(kernels::TcArgs& a, const TcTables& t, unsigned char* base
 }
 
 int tc_pack_blocks(int R, int apack_stages) {
-    return div_ceil(apack_stages * 32, 256) * 2 * div_ceil(R, 2 * kernels::TC_M) * kernels::TC_M;
+    return div_ceil(apack_stages * 8, 256) * 2 * div_ceil(R, 2 * kernels::TC_M) * kernels::TC_M;
 }
 
 namespace {
@@ -576,7 +586,7 @@ bool run_tc(const CompasContext& ctx, kernels::TcArgs a, bool jac, cfloat* out) 
     a.out = reinterpret_cast<float2*>(splits > 1 ? partials.data() : out);
     a.status = detail::device_status_word(ctx.device());
     // per-voxel tables, then A packed once (one pass over the echoes instead of one per pair tile)
-    const dim3 pgrid(div_ceil(a.apack_stages * 32, 256), plan.mtiles * kernels::TC_M);
+    const dim3 pgrid(div_ceil(a.apack_stages * 8, 256), plan.mtiles * kernels::TC_M);
     if (jac) {
         kernels::tc_prep_kernel<true><<<div_ceil(a.nvoxels, 128), 128, 0, ctx.stream()>>>(a);
         kernels::tc_pack_a_kernel<true><<<pgrid, 256, 0, ctx.stream()>>>(a);
