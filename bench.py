@@ -306,7 +306,7 @@ def main():
     sig_tf = sig_flops / (sig_ms / 1e3) / 1e12
     roofline_signal = {"bound": "tensor", "kernel": "signal (split-BF16 tcgen05)", "achieved": sig_tf,
                        "peak": peaks["bf16_tflops_sustained"], "unit": "TFLOP/s",
-                       "frac": sig_tf / peaks["bf16_tflops_sustained"], "traffic": profile_traffic("signal_tc_mrstat"),
+                       "frac": sig_tf / peaks["bf16_tflops_sustained"], "traffic": profile_traffic("cartesian_contraction_pairs_mrstat160"),
                        "note": f"algorithmic 8·C·R·S·V flops; split-BF16 issues 3 BF16 MMAs per product, so the "
                                f"attainable algorithmic rate is 1/3 of the BF16 peak ({peak_kind})"}
 
