@@ -220,7 +220,7 @@ void GaussNewtonStep::Impl::enqueue() const {
         else
             launch_jacobian_hermitian_spiral(ctx, pdata, pstride, V, echos.data(), dT1.data(), dT2.data(),
                                              coils.data(), C, vec, spiral->nreadouts, spiral->samples_per_readout,
-                                             spiral->delta_t, spiral->k_start.data(), spiral->delta_k.data(), out);
+                                             spiral->delta_t, spiral->k_start.data(), spiral->delta_k.data(), out, prec);
     };
     cudaStream_t st = ctx.stream();
     const int eb = int(std::min<int64_t>((necho + 255) / 256, 148 * 16));

@@ -73,7 +73,13 @@ void launch_jacobian_spiral(const CompasContext& ctx, const float* params, int64
 void launch_jacobian_hermitian_spiral(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
                                       const cfloat* echos, const cfloat* dT1, const cfloat* dT2,
                                       const cfloat* coils, int ncoils, const cfloat* vec, int nreadouts, int ns,
-                                      float dt, const cfloat* k_start, const cfloat* delta_k, cfloat* JHv);
+                                      float dt, const cfloat* k_start, const cfloat* delta_k, cfloat* JHv,
+                                      Precision prec);
+// split-BF16 tensor-core form; false when it does not apply (no tensor cores, readouts > 1024 samples)
+bool launch_jacobian_hermitian_spiral_tc(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
+                                         const cfloat* echos, const cfloat* dT1, const cfloat* dT2,
+                                         const cfloat* coils, int ncoils, const cfloat* vec, int nreadouts, int ns,
+                                         float dt, const cfloat* k_start, const cfloat* delta_k, cfloat* JHv);
 void launch_jacobian(const CompasContext& ctx, const float* params, int64_t param_stride, int nvoxels,
                      const cfloat* echos, const cfloat* dT1, const cfloat* dT2, const cfloat* coils, int ncoils,
                      const cfloat* vec, const CartesianGeom& g, cfloat* Jv, Precision prec);

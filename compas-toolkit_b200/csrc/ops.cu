@@ -318,8 +318,8 @@ Array<cfloat, 2> compute_jacobian_hermitian(const CompasContext& ctx, Array<cflo
 }
 
 // Spiral trajectories (no counterpart in the reference, whose Jacobians take CartesianTrajectory
-// only): derived from the spiral signal model. J·v: split-BF16 tensor cores for GemmFast/GemmLow,
-// FP32 otherwise; Jᴴ·v: FP32 for every method.
+// only): derived from the spiral signal model. J·v and Jᴴ·v: split-BF16 tensor cores for
+// GemmFast/GemmLow, FP32 otherwise.
 Array<cfloat, 3> compute_jacobian(const CompasContext& ctx, Array<cfloat, 2> echos, Array<cfloat, 2> delta_echos_T1,
                                   Array<cfloat, 2> delta_echos_T2, TissueParameters parameters,
                                   SpiralTrajectory trajectory, Array<cfloat, 2> coil_sensitivities,
@@ -341,7 +341,7 @@ Array<cfloat, 2> compute_jacobian_hermitian(const CompasContext& ctx, Array<cflo
                                             Array<cfloat, 2> delta_echos_T1, Array<cfloat, 2> delta_echos_T2,
                                             TissueParameters parameters, SpiralTrajectory trajectory,
                                             Array<cfloat, 2> coil_sensitivities, Array<cfloat, 3> vector,
-                                            JacobianComputeMethod) {
+                                            JacobianComputeMethod kind) {
     const int ns = trajectory.samples_per_readout, nreadouts = trajectory.nreadouts;
     const int nvoxels = parameters.nvoxels, ncoils = int(coil_sensitivities.size(0));
     check_jacobian_shapes(nreadouts, nvoxels, echos, delta_echos_T1, delta_echos_T2, coil_sensitivities);
@@ -351,7 +351,7 @@ Array<cfloat, 2> compute_jacobian_hermitian(const CompasContext& ctx, Array<cflo
     launch_jacobian_hermitian_spiral(ctx, parameters.data.data(), parameters.data.size(1), nvoxels, echos.data(),
                                      delta_echos_T1.data(), delta_echos_T2.data(), coil_sensitivities.data(), ncoils,
                                      vector.data(), nreadouts, ns, trajectory.delta_t, trajectory.k_start.data(),
-                                     trajectory.delta_k.data(), JHv.data());
+                                     trajectory.delta_k.data(), JHv.data(), jacobian_precision(kind));
     return JHv;
 }
 

@@ -311,7 +311,7 @@ void ServeEngine::Impl::launch(Slot& slot, std::vector<uint64_t> ids) {
                                              run->dT2[i].data(), r.coil_sensitivities.data(), C,
                                              run->residuals[i].data(), sp.nreadouts, sp.samples_per_readout,
                                              sp.delta_t, sp.k_start.data(), sp.delta_k.data(),
-                                             run->gradients[i].data());
+                                             run->gradients[i].data(), prec);
         }
     }
     COMPAS_CUDA_CHECK(cudaEventCreateWithFlags(&run->done, cudaEventDisableTiming));

@@ -126,8 +126,13 @@ __global__ void __launch_bounds__(SH_THREADS) spiral_hermitian_kernel(SpiralHerm
 void launch_jacobian_hermitian_spiral(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
                                       const cfloat* echos, const cfloat* dT1, const cfloat* dT2,
                                       const cfloat* coils, int ncoils, const cfloat* vec, int nreadouts, int ns,
-                                      float dt, const cfloat* k_start, const cfloat* delta_k, cfloat* JHv) {
+                                      float dt, const cfloat* k_start, const cfloat* delta_k, cfloat* JHv,
+                                      Precision prec) {
     if (nvoxels == 0) return;
+    if (prec == Precision::SplitBF16 &&
+        launch_jacobian_hermitian_spiral_tc(ctx, params, pstride, nvoxels, echos, dT1, dT2, coils, ncoils, vec,
+                                            nreadouts, ns, dt, k_start, delta_k, JHv))
+        return;
     DeviceGuard guard(ctx.device());
     if (int64_t(ncoils) * nreadouts * ns == 0) {
         COMPAS_CUDA_CHECK(cudaMemsetAsync(JHv, 0, sizeof(cfloat) * 4 * size_t(nvoxels), ctx.stream()));

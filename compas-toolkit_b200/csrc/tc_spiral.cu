@@ -25,6 +25,7 @@
 // Every wait is bounded.
 #include <cuda_bf16.h>
 
+#include <cstdlib>
 #include <mutex>
 
 #include "common.cuh"
@@ -379,9 +380,12 @@ bool launch_tc_spiral(const CompasContext& ctx, kernels::TsArgs a, bool jac) {
     Array<cfloat, 2> partials({splits > 1 ? splits : 0, n}, ctx.device(), ctx.stream());
     if (splits > 1) a.out = reinterpret_cast<float2*>(partials.data());
     // readouts in chunks whose base table ([readouts][TERMS][T][V] complex) stays near 1 GB
+    // (COMPAS_B200_SPIRAL_TABLE_BYTES overrides the budget; results do not depend on it)
     const int terms = jac ? 2 : 1;
     const int64_t per_readout = int64_t(terms) * T * a.nvoxels * int64_t(sizeof(float2));
-    const int chunk = int(std::max<int64_t>(1, std::min<int64_t>(a.R, (int64_t(1) << 30) / per_readout)));
+    int64_t budget = int64_t(1) << 30;
+    if (const char* e = std::getenv("COMPAS_B200_SPIRAL_TABLE_BYTES")) budget = std::max<int64_t>(1, std::atoll(e));
+    const int chunk = int(std::max<int64_t>(1, std::min<int64_t>(a.R, budget / per_readout)));
     Array<cfloat, 2> base({std::min(chunk, a.R), int64_t(terms) * T * a.nvoxels}, ctx.device(), ctx.stream());
     a.base = reinterpret_cast<const float2*>(base.data());
     if (jac) set_smem_attribute<true>();

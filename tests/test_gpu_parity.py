@@ -195,6 +195,36 @@ def test_signal_mrstat_scale_sampled(cb, ctx, oracle, workloads, method):
     assert oracle.rel_l2(got, ref) < tol
 
 
+@pytest.mark.parametrize("method", ["MatmulFast", "Direct"])
+def test_signal_spiral_long_readouts(cb, ctx, oracle, workloads, method):
+    # 1100 samples = 9 sample tiles of the tensor-core kernel (one W warp covers tiles 0 and 8)
+    rng = np.random.default_rng(31)
+    p = workloads.tissue(rng, 7, 22.4)
+    traj = workloads.spiral(rng, 5, 1100, 22.4, 4e-6)
+    coils = workloads.cn(rng, (3, 49))
+    echo = workloads.cn(rng, (5, 49))
+    got = cb.magnetization_to_signal(ctx, echo, cb.TissueParameters.from_soa(ctx, p), cb.trajectory_from_dict(ctx, traj),
+                                     coils, method=method).to_numpy()
+    ref = oracle.signal_spiral(echo, p, traj, coils)
+    assert oracle.rel_l2(got, ref) < (TOL_FP32 if method == "Direct" else TOL_BF16X3)
+
+
+def test_signal_spiral_readout_chunks_bitwise(cb, ctx, oracle, workloads, monkeypatch):
+    # the tensor-core kernel runs the readouts in chunks bounded by the size of its per-voxel table;
+    # a tiny budget (one readout per chunk) gives the same bits as one chunk
+    rng = np.random.default_rng(32)
+    p = workloads.tissue(rng, 9, 22.4)
+    traj = workloads.spiral(rng, 6, 300, 22.4, 4e-6)
+    coils = workloads.cn(rng, (4, 81))
+    echo = workloads.cn(rng, (6, 81))
+    args = (echo, cb.TissueParameters.from_soa(ctx, p), cb.trajectory_from_dict(ctx, traj), coils)
+    whole = cb.magnetization_to_signal(ctx, *args, method="MatmulFast").to_numpy()
+    monkeypatch.setenv("COMPAS_B200_SPIRAL_TABLE_BYTES", "1")
+    chunked = cb.magnetization_to_signal(ctx, *args, method="MatmulFast").to_numpy()
+    assert np.array_equal(whole, chunked)
+    assert oracle.rel_l2(chunked, oracle.signal_spiral(echo, p, traj, coils)) < TOL_BF16X3
+
+
 @pytest.mark.parametrize("nc", [1, 3, 11, 20])
 @pytest.mark.parametrize("method", [None, "MatmulFast", "Direct"])
 def test_signal_spiral(cb, ctx, oracle, workloads, method, nc):

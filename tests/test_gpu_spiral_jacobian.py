@@ -1,7 +1,7 @@
 """J·v and Jᴴ·v on spiral trajectories (an addition: the reference's Jacobians accept Cartesian
 trajectories only). The GPU kernels are checked against the oracle's derivation from the spiral
 signal model (itself pinned by adjointness and finite differences in test_oracle.py) within the FP32
-tolerance (FP32 kernels) or the split-BF16 tolerance (tensor-core J·v), through the C-ABI entry
+tolerance (FP32 kernels) or the split-BF16 tolerance (tensor-core J·v and Jᴴ·v), through the C-ABI entry
 points, which dispatch on the trajectory type; plus adjointness on the GPU. Sizes cross the kernels' tile boundaries: samples
 past one 1024-sample block and 64-sample chunks, coil counts 1, 3, 5 and 9 (coil groups of 1, 4, 8
 and 8+1), enough readouts for the Jᴴ·v readout splits."""
@@ -54,20 +54,41 @@ def test_spiral_jacobian_matches_oracle(ctx, oracle, nc, ns, method):
         assert np.array_equal(via_abi, got)
 
 
-@pytest.mark.parametrize("nc,nr,ns", [(1, 33, 100), (3, 12, 130), (9, 40, 70)])
-def test_spiral_jacobian_hermitian_matches_oracle(ctx, oracle, nc, nr, ns):
+@pytest.mark.parametrize("method", ["Direct", "GemmFast"])
+@pytest.mark.parametrize("nc,nr,ns", [(1, 33, 100), (3, 12, 130), (9, 40, 70), (2, 5, 1100)])
+def test_spiral_jacobian_hermitian_matches_oracle(ctx, oracle, nc, nr, ns, method):
+    # Direct: FP32 kernel; GemmFast: split-BF16 tensor-core kernel (readouts of at most 1024 samples,
+    # coil groups of at most 8: 9 coils = 5 + 4; 1100 samples take the FP32 kernel)
     import compas_b200 as cb
 
     p, traj_d, coils, echo, d1, d2, v, u = _case(60 + nc, 290, nr, ns, nc)
     params = cb.TissueParameters.from_soa(ctx, p)
     traj = cb.SpiralTrajectory.from_dict(ctx, traj_d)
     d = {"T1": d1, "T2": d2}
-    got = cb.compute_jacobian_hermitian(ctx, echo, d, params, traj, coils, u).to_numpy()
+    got = cb.compute_jacobian_hermitian(ctx, echo, d, params, traj, coils, u, method=method).to_numpy()
     ref = oracle.spiral_jacobian_hermitian(echo, d1, d2, p, traj_d, coils, u)
-    assert oracle.rel_l2(got, ref) < TOL_FP32
-    # the explicit-method entry point gives the same bits (one kernel for every method)
-    got2 = cb.compute_jacobian_hermitian(ctx, echo, d, params, traj, coils, u, method="Direct").to_numpy()
-    assert np.array_equal(got, got2)
+    assert oracle.rel_l2(got, ref) < (TOL_FP32 if method == "Direct" else TOL_BF16X3)
+    if method == "GemmFast":
+        # the reference's entry point (low_precision = 0) takes the same split-BF16 kernel
+        via_abi = cb.compute_jacobian_hermitian(ctx, echo, d, params, traj, coils, u).to_numpy()
+        assert np.array_equal(via_abi, got)
+
+
+def test_spiral_jacobian_hermitian_readout_chunks_bitwise(ctx, oracle, monkeypatch):
+    # the tensor-core Jᴴ·v runs the readouts in chunks bounded by its per-voxel table; one readout
+    # per chunk changes only the order in which readouts are summed (FP32 rounding)
+    import compas_b200 as cb
+
+    p, traj_d, coils, echo, d1, d2, v, u = _case(71, 300, 7, 200, 3)
+    params = cb.TissueParameters.from_soa(ctx, p)
+    traj = cb.SpiralTrajectory.from_dict(ctx, traj_d)
+    d = {"T1": d1, "T2": d2}
+    whole = cb.compute_jacobian_hermitian(ctx, echo, d, params, traj, coils, u, method="GemmFast").to_numpy()
+    monkeypatch.setenv("COMPAS_B200_SPIRAL_TABLE_BYTES", "1")
+    chunked = cb.compute_jacobian_hermitian(ctx, echo, d, params, traj, coils, u, method="GemmFast").to_numpy()
+    assert oracle.rel_l2(chunked, whole) < 1e-6
+    ref = oracle.spiral_jacobian_hermitian(echo, d1, d2, p, traj_d, coils, u)
+    assert oracle.rel_l2(chunked, ref) < TOL_BF16X3
 
 
 def test_spiral_adjointness_on_gpu(ctx):
@@ -77,8 +98,10 @@ def test_spiral_adjointness_on_gpu(ctx):
     params = cb.TissueParameters.from_soa(ctx, p)
     traj = cb.SpiralTrajectory.from_dict(ctx, traj_d)
     d = {"T1": d1, "T2": d2}
-    Jv = cb.compute_jacobian(ctx, echo, d, params, traj, coils, v, method="Direct").to_numpy().astype(np.complex128)
-    JHu = cb.compute_jacobian_hermitian(ctx, echo, d, params, traj, coils, u).to_numpy().astype(np.complex128)
-    lhs = np.vdot(u.astype(np.complex128), Jv)
-    rhs = np.vdot(JHu, v.astype(np.complex128))
-    assert abs(lhs - rhs) / abs(lhs) < 1e-5
+    for method, tol in (("Direct", 1e-5), ("GemmFast", 1e-4)):
+        Jv = cb.compute_jacobian(ctx, echo, d, params, traj, coils, v, method=method).to_numpy().astype(np.complex128)
+        JHu = cb.compute_jacobian_hermitian(ctx, echo, d, params, traj, coils, u, method=method)
+        JHu = JHu.to_numpy().astype(np.complex128)
+        lhs = np.vdot(u.astype(np.complex128), Jv)
+        rhs = np.vdot(JHu, v.astype(np.complex128))
+        assert abs(lhs - rhs) / abs(lhs) < tol
