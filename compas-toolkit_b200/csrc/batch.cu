@@ -274,7 +274,7 @@ void SimulationBatch::Impl::plan_signal(Family& fam, const std::vector<int>& mem
             args.push_back(a);
             prep_counts.push_back(div_ceil(V, 128));
             pack_counts.push_back(tc_pack_blocks(t.nreadouts, a.apack_stages));
-            cta_counts.push_back(int64_t(e.plan.ntiles) * e.plan.mtiles * e.plan.splits);
+            cta_counts.push_back(e.plan.ctas);
         }
         int64_t total = 0;
         g.njobs = int(args.size());

@@ -77,6 +77,7 @@ struct TcArgs {
     // tile, voxel stage) = hi then lo plane, 16 KB each
     const unsigned char* apack;
     int apack_stages;      // voxel stages per readout tile in apack
+    int nr;                // readouts per tile (a multiple of 16, ≤ 256; each CTA of a pair holds nr/2)
 };
 
 // one split-K reduction: out[i] = Σ_q partials[q·n + i], q = 0..nsplit-1 in order

@@ -100,8 +100,12 @@ bool tensor_cores_available(int device);
 // tile grid and voxel split of one split-BF16 contraction (a function of its shape only, so a
 // job gives the same partial sums alone and inside a batch)
 struct TcPlan {
-    int ntiles, mtiles, splits, vchunk;
+    int ntiles, mtiles, splits, vchunk;  // pair tiles, readout tiles, voxel splits, voxels per split
+    int nr;                              // readouts per tile
+    int64_t ctas;                        // CTAs of the contraction (CTA pairs × 2)
 };
+// readouts per tile of the Cartesian contraction: the multiple of 16 up to 256 that pads R least
+int tc_readout_tile(int R);
 TcPlan tc_plan(int device, int nvoxels, int R, int S, int C, bool jac);
 // argument block of a Cartesian signal contraction; out / vchunk / status / tables set by the caller
 kernels::TcArgs tc_signal_args(const float* params, int64_t pstride, int nvoxels, const cfloat* echos,
@@ -110,11 +114,11 @@ kernels::TcArgs tc_signal_args(const float* params, int64_t pstride, int nvoxels
 // per-voxel E_k step and restart values, coil·w, J·v coefficients and the packed A images
 struct TcTables {
     int64_t vstep, estart, coilw, jcoef, apack, bytes;
-    int egk, apack_stages;
+    int egk, apack_stages, nr;
 };
 TcTables tc_tables(int nvoxels, int R, int S, int C, bool jac);
 void tc_assign_tables(kernels::TcArgs& a, const TcTables& t, unsigned char* base);
-int tc_pack_blocks(int R, int apack_stages);  // 256-thread blocks of one job's A packing
+int tc_pack_blocks(int R, int apack_stages);  // 256-thread blocks of one job's echo packing
 // batched prep (prep_blocks flattened 128-thread blocks), A packing (pack_blocks flattened
 // 256-thread blocks) and contraction (ctas flattened CTAs)
 void launch_tc_batch(cudaStream_t stream, int device, bool jac, const kernels::TcArgs* jobs, int njobs,

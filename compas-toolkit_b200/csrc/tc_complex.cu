@@ -5,28 +5,29 @@
 // src/jacobian/product_kernels.cuh:7-67):
 //   signal: out[c][r][k] = Σ_v echo[r][v] · F_{c,k}(v),        F = coil·ρ·E_k·e^{i(S/2)Δk_im y}
 //   J·v:    out[c][r][k] = Σ_v P[r][v]·F_{c,k}(v) + Q'[r][v]·(k-S/2)·F_{c,k}(v),  F = coil·E_k
-// The complex contraction is real-ified by interleaving re/im along K: A'[r] = (A_re, A_im) per
-// complex term, B'[2j] = (F_re, -F_im), B'[2j+1] = (F_im, F_re) per output pair j = (c, k), so
-// one real GEMM D[128 readouts][256 = 128 pairs × re/im] = A'·B'ᵀ yields the complex tile.
+// The complex contraction is real-ified by interleaving re/im along K: the streamed row
+// (A_re, A_im) per complex term, the generated rows (F_re, -F_im) and (F_im, F_re) per output pair
+// j = (c, k), so one real GEMM D[2j + re/im][readout] yields the complex tile.
 //
 // Precision: every operand x is split as x = hi + lo (two BF16s, |x - hi - lo| ≤ 2⁻¹⁸|x|) and the
 // product is accumulated in FP32 TMEM as hi·hi + hi·lo + lo·hi (three tcgen05.mma per K step);
 // the dropped lo·lo term is ≤ 2⁻¹⁶ relative, giving ~1e-5 relative L2 against FP64.
 //
 // Per call, small kernels first write per-voxel tables (the E_k step, E_k itself at every
-// TC_PPG-th sample with the phase reduced in FP64, coil·w, the J·v coefficients) and pack A once
-// as the split, swizzled shared-memory images the contraction consumes.
-// The contraction runs on CTA pairs (cluster of 2, tcgen05 cta_group::2): one MMA of M = 256
-// readouts (128 per CTA) × N = 256 spans both SMs' tensor cores; each CTA holds its own A half and
-// generates the B rows of half the tile's 128 pairs.
+// TC_PPG-th sample with the phase reduced in FP64, coil·w, the J·v coefficients) and pack the
+// streamed operand once as the split, swizzled shared-memory images the contraction consumes.
+// The contraction runs on CTA pairs (cluster of 2, tcgen05 cta_group::2): one MMA spans both SMs'
+// tensor cores with M = 256 generated rows (128 (coil, sample) pairs × re/im; each CTA generates
+// its 128) and N = nr readouts (each CTA holds nr/2; nr is the multiple of 16 up to 256 that pads R
+// least, e.g. 224 for 1120 readouts).
 // CTA organisation (576 threads, 1 CTA/SM, 192 KB shared memory in 3 stages of 64 KB):
-//   warps 0-15  generate this CTA's half of the B tile (128 rows × 64 K): thread = (2 voxels,
+//   warps 0-15  generate this CTA's 128 rows (64 pairs × 64 K per stage): thread = (2 voxels,
 //               group of TC_PPG pairs); a group starts from the exact E_k table value × coil·w and
 //               steps along k with the complex recurrence. Afterwards they drain the TMEM
 //               accumulator through shared memory into coalesced rows of the output;
 //   warp 16     allocates 256 TMEM columns (both CTAs); in the leader one lane issues the 12 MMAs
-//               per stage, in the peer one lane tells the leader when its A has landed;
-//   warp 17     one lane loads each stage's A image (32 KB) with one bulk copy.
+//               per stage, in the peer one lane tells the leader when its streamed half has landed;
+//   warp 17     one lane loads each stage's half readout tile (hi and lo planes) by bulk copies.
 // Stages hand over through mbarriers (full, in the leader: producers of both CTAs → MMA; afull:
 // copy landed; empty, in both: tcgen05.commit multicast → producers and copy). The voxel range is
 // split over CTA pairs (split-K); partial tiles are summed in a fixed order. Every wait is bounded.
@@ -53,15 +54,12 @@ constexpr int TC_B_THREADS = 512;                  // 16 producer warps: 16 voxe
 constexpr int TC_MMA_WARP = 16, TC_COPY_WARP = 17;
 constexpr int TC_THREADS = 576;
 constexpr int TC_STAGES = 3;
-constexpr int TC_A_BYTES = TC_M * TC_K * 2;         // 16 KB per hi/lo plane: this CTA's 128 readouts
-constexpr int TC_BH_BYTES = (TC_N / 2) * TC_K * 2;  // 16 KB per hi/lo plane: this CTA's 128 of the 256 B rows
+constexpr int TC_A_BYTES = TC_M * TC_K * 2;         // 16 KB slot per hi/lo plane: this CTA's ≤ 128 readouts
+constexpr int TC_BH_BYTES = (TC_N / 2) * TC_K * 2;  // 16 KB per hi/lo plane: this CTA's 128 generated rows
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_BH_BYTES;
 constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 128 /*barriers*/;
-constexpr int TC_APACK_BLOCK = 2 * TC_A_BYTES;  // hi + lo image of one (readout tile, voxel stage)
-constexpr int TC_TROW = TC_PAIRS + 2;           // float2 per row of the transposed output tile
 static_assert(TC_PAIRS / 2 == (TC_B_THREADS / 16) * TC_PPG, "a CTA's producer groups cover half the pair tile");
-static_assert(TC_M * TC_TROW * 8 <= TC_STAGES * TC_STAGE_BYTES, "output tile fits the stage buffers");
-static_assert((TC_TROW * 8) % 16 == 0, "transposed rows stay 16-byte aligned");
+static_assert((TC_PAIRS / 2) * (2 * 256 + 2) * 4 <= TC_STAGES * TC_STAGE_BYTES, "output tile fits the stage buffers");
 
 // one thread per voxel: the E_k step, E_k at the restart points, coil·w for every coil and
 // (J·v) the four complex coefficients of P and Q' — once per call instead of per CTA and stage
@@ -113,11 +111,12 @@ __global__ void tc_prep_kernel(TcArgs a) {
     tc_prep_voxel<JAC>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-// Pack the A operand once per call as the shared-memory images the contraction consumes: element
-// (readout r, column g) with g = 32·stage + j (signal: voxel g; J·v: voxel g/2, term g%2 = P or Q')
-// is split into hi/lo BF16 and stored at the swizzled position of row r % 128, column j in block
-// (r / 128, stage). Rows past R and columns past V are zero. Every contraction CTA of a readout
-// tile then loads each stage with one bulk copy.
+// Pack the streamed operand (echoes, or the J·v sources) once per call as the shared-memory images
+// the contraction consumes: element (readout r, column g) with g = 32·stage + j (signal: voxel g;
+// J·v: voxel g/2, term g%2 = P or Q') is split into hi/lo BF16 and stored at the swizzled position
+// of row r % (nr/2), column j in block (readout tile r / nr, half (r % nr) / (nr/2), stage). Rows
+// past R and columns past V are zero. Each CTA of a pair then loads its half of a stage with two
+// bulk copies (hi, lo).
 // Thread = one 16-byte chunk (4 columns) of one row: 4 voxels (signal) or 2 voxels × 2 terms
 // (J·v); a warp reads contiguous echo rows and writes whole 128-byte rows of 4 blocks.
 template<bool JAC>
@@ -153,10 +152,15 @@ __device__ __forceinline__ void tc_pack_a(const TcArgs& a, const int cg, const i
     uint32_t h[4], l[4];
 #pragma unroll
     for (int i = 0; i < 4; i++) tc::split2(e[i].x, e[i].y, h[i], l[i]);
-    unsigned char* blk = const_cast<unsigned char*>(a.apack) + (int64_t(rp >> 7) * a.apack_stages + stage) * TC_APACK_BLOCK;
-    const uint32_t off = tc::sw128_offset(rp & 127, chunk);
+    // block (readout tile, half for CTA rank, stage): hi plane of nr/2 rows, then the lo plane
+    const int half_rows = a.nr / 2;
+    const int tile = rp / a.nr, within = rp - tile * a.nr;
+    const int half = within / half_rows, hrow = within - half * half_rows;
+    unsigned char* blk = const_cast<unsigned char*>(a.apack) +
+                         ((int64_t(tile) * 2 + half) * a.apack_stages + stage) * int64_t(half_rows) * 256;
+    const uint32_t off = tc::sw128_offset(hrow, chunk);
     *reinterpret_cast<uint4*>(blk + off) = make_uint4(h[0], h[1], h[2], h[3]);
-    *reinterpret_cast<uint4*>(blk + TC_A_BYTES + off) = make_uint4(l[0], l[1], l[2], l[3]);
+    *reinterpret_cast<uint4*>(blk + half_rows * 128 + off) = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
 // grid (chunks / 256, padded readout rows)
@@ -166,11 +170,13 @@ __global__ void __launch_bounds__(256) tc_pack_a_kernel(TcArgs a) {
 }
 
 // One output tile (pair tile bx, readout tile by, voxel split bz) of one contraction, computed by
-// a CTA pair (cluster of 2, readout tiles by = 2·i and 2·i + 1, rank = by & 1): each CTA loads its
-// readout tile's A and generates the B rows of half the tile's pairs (rank·64 ..), the leader
-// issues M = 256 MMAs over both, producers of both CTAs arrive on the leader's barriers and the
-// leader's commits arrive on both. Shared by the one-operation kernel and the batched kernel, so
-// both give bit-identical results.
+// a CTA pair (cluster of 2, rank 0 / 1): each CTA generates the rows of half the tile's 128 pairs
+// (rank·64 .., the MMA's A: M = 256 over the pair) and loads half of the readout tile's streamed
+// operand (the MMA's B: N = nr readouts over the pair, any multiple of 16 up to 256, so R needs
+// little padding); the leader issues the MMAs, producers of both CTAs arrive on the leader's
+// barriers and the leader's commits arrive on both. D per CTA: 128 rows (64 pairs × re/im) × nr
+// readout columns. Shared by the one-operation kernel and the batched kernel, so both give
+// bit-identical results.
 template<bool JAC>
 __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int by, const int bz,
                                         unsigned char* smem_raw) {
@@ -188,7 +194,7 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = tc::cluster_ctarank();
     const int n_pair0 = bx * TC_PAIRS;  // first (c,k) pair of this tile
-    const int r0 = by * TC_M;
+    const int r0 = by * a.nr;
     const int v_begin = bz * a.vchunk;
     const int v_end = min(a.nvoxels, v_begin + a.vchunk);
     const int nstages = max(1, (v_end - v_begin + VPS - 1) / VPS);
@@ -212,18 +218,22 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
     const uint32_t tmem = *tmem_slot;
 
     if (warp == TC_COPY_WARP) {
-        // ---------------- A: one bulk copy (hi + lo, 32 KB) per stage
+        // ---------------- streamed operand: this CTA's half of the readout tile, two bulk copies
+        // (hi and lo planes of nr/2 rows) per stage
         if (lane == 0) {
-            const unsigned char* src = a.apack + (int64_t(by) * a.apack_stages + v_begin / VPS) * TC_APACK_BLOCK;
+            const uint32_t plane = uint32_t(a.nr / 2) * 128;
+            const unsigned char* src =
+                a.apack + ((int64_t(by) * 2 + rank) * a.apack_stages + v_begin / VPS) * int64_t(2 * plane);
             int issued[TC_STAGES];
             for (int s = 0; s < TC_STAGES; s++) issued[s] = -1;
             for (int it = 0; it < nstages; it++) {
                 const int buf = it % TC_STAGES;
                 if (!tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status)) *abort_flag = 1;
                 if (*(volatile int*)abort_flag) break;
-                tc::mbar_arrive_expect_tx(&afull[buf], TC_APACK_BLOCK);
-                tc::bulk_copy_g2s(smem + buf * TC_STAGE_BYTES, src + int64_t(it) * TC_APACK_BLOCK, TC_APACK_BLOCK,
-                                  &afull[buf]);
+                tc::mbar_arrive_expect_tx(&afull[buf], 2 * plane);
+                const unsigned char* blk = src + int64_t(it) * 2 * plane;
+                tc::bulk_copy_g2s(smem + buf * TC_STAGE_BYTES, blk, plane, &afull[buf]);
+                tc::bulk_copy_g2s(smem + buf * TC_STAGE_BYTES + TC_A_BYTES, blk + plane, plane, &afull[buf]);
                 issued[buf] = it;
             }
             // copies still in flight land before the CTA can finish (bounded)
@@ -233,16 +243,17 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
     } else if (warp == TC_MMA_WARP && rank == 0) {
         // ---------------- MMA issuer (leader, one lane): M = 256 over both CTAs
         if (lane == 0) {
-            constexpr uint32_t idesc = tc::idesc_bf16_f32(2 * TC_M, TC_N);
+            const uint32_t idesc = tc::idesc_bf16_f32(2 * TC_M, a.nr);
             for (int it = 0; it < nstages; it++) {
                 const int buf = it % TC_STAGES;
                 if (!tc::mbar_wait(&full[buf], (it / TC_STAGES) & 1, a.status)) *abort_flag = 1;
                 if (!tc::mbar_wait(&afull[buf], (it / TC_STAGES) & 1, a.status)) *abort_flag = 1;
                 if (*(volatile int*)abort_flag) break;
                 tc::tc_fence_after();
+                // A (M): the generated rows; B (N): the streamed readouts
                 const uint32_t base = tc::smem_u32(smem + buf * TC_STAGE_BYTES);
-                const uint32_t ah = base, al = base + TC_A_BYTES;
-                const uint32_t bh = base + 2 * TC_A_BYTES, bl = bh + TC_BH_BYTES;
+                const uint32_t bh = base, bl = base + TC_A_BYTES;
+                const uint32_t ah = base + 2 * TC_A_BYTES, al = ah + TC_BH_BYTES;
 #pragma unroll
                 for (int ks = 0; ks < TC_K / 16; ks++) {
                     const uint32_t koff = ks * 32;  // 16 bf16 = 32 bytes along K inside the swizzle atom
@@ -366,44 +377,47 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
             }
         }
 
-        // ---------------- epilogue: TMEM → shared memory (row = readout, pairs along the row) →
-        // coalesced rows of out[c][r][k]. Warp w reads TMEM lanes 32·(w%4).. (its quarter) and
-        // column chunks w/4 and w/4 + 4; all 16 warps then write 8 rows each.
+        // ---------------- epilogue: D[row = 2j + re/im of local pair j][col = readout] → shared memory
+        // T[j][col] (float2) → rows of out[c][r][k] along k. Warp w reads TMEM lanes 32·(w%4).. (its
+        // quarter) and 32-column chunks w/4, w/4 + 4; all 16 warps then write readout rows.
         const bool waited = tc::mbar_wait(done, 0, a.status);
         tc::tc_fence_after();
         // one decision for all 512 producer threads (tcgen05.ld is .sync.aligned, the barriers
         // below need every participant)
         const bool ok = !tc::bar_red_or(1, TC_B_THREADS, !(waited && !*(volatile int*)abort_flag));
         if (ok) {
-            float2* T = reinterpret_cast<float2*>(smem);  // [TC_M][TC_TROW]; the stage buffers are free
+            float* T = reinterpret_cast<float*>(smem);  // [64][TP]; the stage buffers are free
+            const int TP = 2 * a.nr + 2;                // row pitch (floats): conflict-free columns
             const int quarter = warp & 3;
-            const int row = quarter * 32 + lane;
+            const int row = quarter * 32 + lane, jr = row >> 1, ri = row & 1;
 #pragma unroll 1
-            for (int h = 0; h < 2; h++) {
-                const int qq = (warp >> 2) + 4 * h;  // 32 columns = 16 pairs
+            for (int ch = warp >> 2; ch * 32 < a.nr; ch += 4) {
                 float v[32];
-                tc::tmem_load32(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(qq * 32), v);
-                float4* dst = reinterpret_cast<float4*>(T + row * TC_TROW + qq * 16);
+                tc::tmem_load32(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(ch * 32), v);
 #pragma unroll
-                for (int m = 0; m < 8; m++) dst[m] = make_float4(v[4 * m], v[4 * m + 1], v[4 * m + 2], v[4 * m + 3]);
+                for (int i = 0; i < 32; i++)
+                    if (ch * 32 + i < a.nr) T[jr * TP + 2 * (ch * 32 + i) + ri] = v[i];
             }
             tc::bar_sync(1, TC_B_THREADS);
             float2* outp = a.out + int64_t(bz) * npairs * a.R;
-            int64_t base[TC_PAIRS / 32];
-            bool pv[TC_PAIRS / 32];
+            int64_t base[2];
+            bool pv[2];
 #pragma unroll
-            for (int m = 0; m < TC_PAIRS / 32; m++) {
-                const int n = n_pair0 + lane + 32 * m;
+            for (int m = 0; m < 2; m++) {
+                const int n = n_pair0 + int(rank) * (TC_PAIRS / 2) + lane + 32 * m;
                 const int cc = n / a.S, kk = n - cc * a.S;
                 pv[m] = n < npairs;
                 base[m] = int64_t(cc) * a.R * a.S + kk;
             }
 #pragma unroll 1
-            for (int rr = warp; rr < TC_M && r0 + rr < a.R; rr += TC_B_THREADS / 32) {
-                const int64_t roff = int64_t(r0 + rr) * a.S;
+            for (int col = warp; col < a.nr && r0 + col < a.R; col += TC_B_THREADS / 32) {
+                const int64_t roff = int64_t(r0 + col) * a.S;
 #pragma unroll
-                for (int m = 0; m < TC_PAIRS / 32; m++)
-                    if (pv[m]) outp[base[m] + roff] = T[rr * TC_TROW + lane + 32 * m];
+                for (int m = 0; m < 2; m++)
+                    if (pv[m]) {
+                        const float* t = T + (lane + 32 * m) * TP + 2 * col;
+                        outp[base[m] + roff] = make_float2(t[0], t[1]);
+                    }
             }
         }
     }
@@ -416,16 +430,16 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
     }
 }
 
-// grid (readout tiles, pair tiles, voxel splits); readout tiles 2i, 2i+1 form a cluster
+// grid (2 × pair tiles, readout tiles, voxel splits); CTAs 2i, 2i + 1 form a cluster
 template<bool JAC>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    tc_tile<JAC>(a, blockIdx.y, blockIdx.x, blockIdx.z, smem_raw);
+    tc_tile<JAC>(a, blockIdx.x >> 1, blockIdx.y, blockIdx.z, smem_raw);
 }
 
-// tile grid of one contraction: (pair tiles, readout-tile pairs, voxel splits)
+// tile grid of one contraction: (pair tiles, readout tiles, voxel splits), 2 CTAs per tile
 __device__ __forceinline__ int3 tc_grid_of(const TcArgs& a) {
-    return make_int3((a.C * a.S + TC_PAIRS - 1) / TC_PAIRS, (a.R + 2 * TC_M - 1) / (2 * TC_M),
+    return make_int3((a.C * a.S + TC_PAIRS - 1) / TC_PAIRS, (a.R + a.nr - 1) / a.nr,
                      (a.nvoxels + a.vchunk - 1) / a.vchunk);
 }
 
@@ -442,8 +456,8 @@ __device__ __forceinline__ int job_of_block(const int* __restrict__ offsets, int
 
 // Batched contraction: one launch for many jobs. Flattened CTA b belongs to job j
 // (cta_offsets[j] ≤ b < cta_offsets[j+1], all offsets even) and, with l = b - cta_offsets[j] and
-// (nx, ny) the job's pair tiles and readout-tile pairs, takes pair tile (l/2) % nx, readout tile
-// 2·((l/2 / nx) % ny) + (l & 1) and split (l/2) / (nx·ny); CTAs 2i, 2i+1 form a cluster. Jobs are
+// (nx, ny) the job's pair tiles and readout tiles, takes pair tile (l/2) % nx, readout tile
+// (l/2 / nx) % ny and split (l/2) / (nx·ny) as rank l & 1; CTAs 2i, 2i+1 form a cluster. Jobs are
 // ordered by decreasing work per CTA, so the block scheduler runs the longest tiles first.
 template<bool JAC>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
@@ -456,7 +470,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TC_THREADS, 1)
         job = jobs[j];
         const int3 g = tc_grid_of(job);
         const int l = blockIdx.x - cta_offsets[j], l2 = l >> 1;
-        tile = make_int3(l2 % g.x, 2 * ((l2 / g.x) % g.y) + (l & 1), l2 / (g.x * g.y));
+        tile = make_int3(l2 % g.x, (l2 / g.x) % g.y, l2 / (g.x * g.y));
     }
     __syncthreads();
     tc_tile<JAC>(job, tile.x, tile.y, tile.z, smem_raw);
@@ -496,11 +510,25 @@ __global__ void tc_pack_batch_kernel(const TcArgs* __restrict__ jobs, const int*
 
 }  // namespace kernels
 
+int tc_readout_tile(int R) {
+    int best = 256;
+    int64_t padded = int64_t(div_ceil(std::max(R, 1), 256)) * 256;
+    for (int nr = 240; nr >= 16; nr -= 16) {
+        const int64_t p = int64_t(div_ceil(std::max(R, 1), nr)) * nr;
+        if (p < padded) {
+            padded = p;
+            best = nr;
+        }
+    }
+    return best;
+}
+
 TcPlan tc_plan(int device, int nvoxels, int R, int S, int C, bool jac) {
     TcPlan p;
     p.ntiles = div_ceil(C * S, kernels::TC_PAIRS);
-    p.mtiles = 2 * div_ceil(R, 2 * kernels::TC_M);  // readout tiles, whole CTA pairs
-    const int tiles = p.ntiles * p.mtiles;
+    p.nr = tc_readout_tile(R);
+    p.mtiles = div_ceil(std::max(R, 1), p.nr);
+    const int tiles = 2 * p.ntiles * p.mtiles;  // CTAs per voxel split
     const int vps = jac ? 16 : 32;
     // split the voxel range over CTAs: pick the split count (≥ 16 stages per split) whose grid
     // leaves the least idle SM time in the last wave of one CTA per SM
@@ -525,6 +553,7 @@ TcPlan tc_plan(int device, int nvoxels, int R, int S, int C, bool jac) {
     splits = std::max(splits, div_ceil(std::max(nvoxels, 1), max_voxels));
     p.vchunk = std::max(vps, div_ceil(div_ceil(std::max(nvoxels, 1), splits), vps) * vps);
     p.splits = std::max(1, div_ceil(nvoxels, p.vchunk));
+    p.ctas = int64_t(tiles) * p.splits;
     return p;
 }
 
@@ -534,13 +563,14 @@ TcTables tc_tables(int nvoxels, int R, int S, int C, bool jac) {
     const int vps = jac ? 16 : 32;
     t.egk = (S % kernels::TC_PPG == 0) ? kernels::TC_PPG : 1;
     t.apack_stages = div_ceil(std::max(nvoxels, 1), vps);
+    t.nr = tc_readout_tile(R);
     auto align = [](int64_t b) { return (b + 255) / 256 * 256; };
     t.vstep = 0;
     t.estart = t.vstep + align(8 * V);
     t.coilw = t.estart + align(8 * V * (S / t.egk));
     t.jcoef = t.coilw + align(8 * V * C);
     t.apack = t.jcoef + align(jac ? 32 * V : 0);
-    t.bytes = t.apack + int64_t(2 * div_ceil(R, 2 * kernels::TC_M)) * t.apack_stages * kernels::TC_APACK_BLOCK;
+    t.bytes = t.apack + int64_t(div_ceil(std::max(R, 1), t.nr)) * t.nr * t.apack_stages * 256;
     return t;
 }
 
@@ -552,10 +582,12 @@ void tc_assign_tables(kernels::TcArgs& a, const TcTables& t, unsigned char* base
     a.jcoef = reinterpret_cast<const float4*>(base + t.jcoef);
     a.apack = base + t.apack;
     a.apack_stages = t.apack_stages;
+    a.nr = t.nr;
 }
 
 int tc_pack_blocks(int R, int apack_stages) {
-    return div_ceil(apack_stages * 8, 256) * 2 * div_ceil(R, 2 * kernels::TC_M) * kernels::TC_M;
+    const int nr = tc_readout_tile(R);
+    return div_ceil(apack_stages * 8, 256) * div_ceil(std::max(R, 1), nr) * nr;
 }
 
 namespace {
@@ -586,7 +618,7 @@ bool run_tc(const CompasContext& ctx, kernels::TcArgs a, bool jac, cfloat* out) 
     a.out = reinterpret_cast<float2*>(splits > 1 ? partials.data() : out);
     a.status = detail::device_status_word(ctx.device());
     // per-voxel tables, then A packed once (one pass over the echoes instead of one per pair tile)
-    const dim3 pgrid(div_ceil(a.apack_stages * 8, 256), plan.mtiles * kernels::TC_M);
+    const dim3 pgrid(div_ceil(a.apack_stages * 8, 256), plan.mtiles * plan.nr);
     if (jac) {
         kernels::tc_prep_kernel<true><<<div_ceil(a.nvoxels, 128), 128, 0, ctx.stream()>>>(a);
         kernels::tc_pack_a_kernel<true><<<pgrid, 256, 0, ctx.stream()>>>(a);
@@ -597,7 +629,7 @@ bool run_tc(const CompasContext& ctx, kernels::TcArgs a, bool jac, cfloat* out) 
     check_launch("tc_prep_kernel / tc_pack_a_kernel");
     auto fn = jac ? kernels::tc_contract_kernel<true> : kernels::tc_contract_kernel<false>;
     set_tc_smem_attribute(jac, false);
-    dim3 grid(plan.mtiles, plan.ntiles, splits);
+    dim3 grid(2 * plan.ntiles, plan.mtiles, splits);
     fn<<<grid, kernels::TC_THREADS, kernels::TC_SMEM, ctx.stream()>>>(a);
     check_launch("tc_contract_kernel");
     if (splits > 1) sum_partials(ctx, partials.data(), splits, n, out);
