@@ -13,8 +13,10 @@
 // precession sin/cos is evaluated once per z instead of twice per TR). The rotation uses
 // the unnormalised-axis Rodrigues form
 //     m' = cos θ·m + (sin θ/θ)·(a×m) + ((1-cos θ)/θ²)·(a·m)·a,   θ² = a·a,
-// whose three coefficients are Taylor polynomials in θ² (coefficients 1/n!) for θ ≤ 0.5 rad,
-// accurate to < 3e-10, so the hot loop runs on the FMA pipe; larger angles use sqrt/sincos.
+// whose coefficients sin θ/θ and (1-cos θ)/θ² are Taylor polynomials in θ² (coefficients 1/n!)
+// for θ ≤ 0.5 rad, accurate to < 3e-10, and cos θ = 1 - θ²·(1-cos θ)/θ², so the hot loop runs on
+// the FMA pipe; larger angles use sqrt/sincos. The relaxation after each RF sample is folded into
+// the rotation (E2 scales its coefficients, E1 enters as E1/E2 on the longitudinal result).
 #include "common.cuh"
 #include "compas/compas.h"
 #include "job_args.cuh"
@@ -38,23 +40,49 @@ struct Iso {
     float x, y, z;
 };
 
-// rotation about the unnormalised axis (ax, ay, az) by |a|   (isochromat.cuh:14-73)
-__device__ __forceinline__ void rodrigues(Iso& m, float ax, float ay, float az, float axy2) {
+// Per-voxel constants of rotate_relax: the Taylor coefficients of sin θ/θ and (1-cos θ)/θ² (1/n!)
+// times E2, E2 itself, E1/E2 and 1 - E1.
+struct RotRelax {
+    float s0, s1, s2, s3, s4, h0, h1, h2, h3, h4, E2, r, oneE1;
+};
+
+__device__ __forceinline__ RotRelax make_rot_relax(float E1, float E2) {
+    RotRelax k;
+    k.s0 = E2;
+    k.s1 = E2 * (-1.0f / 6.0f);
+    k.s2 = E2 * (1.0f / 120.0f);
+    k.s3 = E2 * (-1.0f / 5040.0f);
+    k.s4 = E2 * (1.0f / 362880.0f);
+    k.h0 = E2 * 0.5f;
+    k.h1 = E2 * (-1.0f / 24.0f);
+    k.h2 = E2 * (1.0f / 720.0f);
+    k.h3 = E2 * (-1.0f / 40320.0f);
+    k.h4 = E2 * (1.0f / 3628800.0f);
+    k.E2 = E2;
+    k.r = E1 / E2;
+    k.oneE1 = 1.0f - E1;
+    return k;
+}
+
+// rotation about the unnormalised axis (ax, ay, az) by |a|   (isochromat.cuh:14-73), followed by
+// relaxation: transverse components times E2, longitudinal z·E1 + 1 - E1. E2 is folded into the
+// rotation coefficients and E1 enters as E1/E2 on the E2-scaled longitudinal result.
+__device__ __forceinline__ void rotate_relax(Iso& m, float ax, float ay, float az, float axy2, const RotRelax& k) {
     const float t2 = fmaf(az, az, axy2);
-    float c, s, h;
+    float c, s, h;  // E2·cos θ, E2·sin θ/θ, E2·(1-cos θ)/θ²
     if (t2 <= 0.25f) {
-        // cos θ, sin θ/θ, (1-cos θ)/θ² as Taylor series in x = θ² through x⁴
+        // Taylor series in x = θ² through x⁴, cos θ = 1 - x·(1-cos θ)/θ²
         const float x = t2;
-        c = fmaf(x, fmaf(x, fmaf(x, fmaf(x, 1.0f / 40320.0f, -1.0f / 720.0f), 1.0f / 24.0f), -0.5f), 1.0f);
-        s = fmaf(x, fmaf(x, fmaf(x, fmaf(x, 1.0f / 362880.0f, -1.0f / 5040.0f), 1.0f / 120.0f), -1.0f / 6.0f), 1.0f);
-        h = fmaf(x, fmaf(x, fmaf(x, fmaf(x, 1.0f / 3628800.0f, -1.0f / 40320.0f), 1.0f / 720.0f), -1.0f / 24.0f), 0.5f);
+        s = fmaf(x, fmaf(x, fmaf(x, fmaf(x, k.s4, k.s3), k.s2), k.s1), k.s0);
+        h = fmaf(x, fmaf(x, fmaf(x, fmaf(x, k.h4, k.h3), k.h2), k.h1), k.h0);
+        c = fmaf(-x, h, k.E2);
     } else {
         const float th = sqrtf(t2);
         float sn, cs;
         sincosf(th, &sn, &cs);
-        c = cs;
-        s = sn / th;
-        h = (1.0f - cs) / t2;
+        c = k.E2 * cs;
+        s = k.E2 * (sn / th);
+        h = k.E2 * ((1.0f - cs) / t2);
     }
     const float cx = ay * m.z - az * m.y;
     const float cy = az * m.x - ax * m.z;
@@ -62,7 +90,7 @@ __device__ __forceinline__ void rodrigues(Iso& m, float ax, float ay, float az, 
     const float hd = h * fmaf(ax, m.x, fmaf(ay, m.y, az * m.z));
     m.x = fmaf(c, m.x, fmaf(s, cx, hd * ax));
     m.y = fmaf(c, m.y, fmaf(s, cy, hd * ay));
-    m.z = fmaf(c, m.z, fmaf(s, cz, hd * az));
+    m.z = fmaf(k.r, fmaf(c, m.z, fmaf(s, cz, hd * az)), k.oneE1);
 }
 
 // One tile (128/GZ voxels) of a pSSFP simulation. Shared by the one-simulation kernel
@@ -101,6 +129,7 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
         (void)E2_inv;
     }
 
+    const RotRelax rr = make_rot_relax(E1_ex, E2_ex);
     auto excite = [&](int row) {
         const float2* zr = a.zap + int64_t(row) * a.nRF;
         for (int i = 0; i < a.nRF; i++) {
@@ -108,12 +137,7 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
             const float ax = zp.x * B1, ay = -zp.y * B1;
             const float axy2 = fmaf(ax, ax, ay * ay);
 #pragma unroll
-            for (int k = 0; k < ZT; k++) {
-                rodrigues(m[k], ax, ay, az[k], axy2);
-                m[k].x *= E2_ex;
-                m[k].y *= E2_ex;
-                m[k].z = fmaf(m[k].z, E1_ex, 1.0f - E1_ex);
-            }
+            for (int k = 0; k < ZT; k++) rotate_relax(m[k], ax, ay, az[k], axy2, rr);
         }
     };
     auto precess = [&]() {
