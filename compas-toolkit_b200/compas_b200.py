@@ -79,6 +79,10 @@ _SIGS = {
     "compas_b200_pssfp_config_info": ([_I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
     "compas_b200_fisp_launch_choice": ([_I, _I64, _I, C.POINTER(C.c_int), C.POINTER(C.c_int)], None),
     "compas_b200_pssfp_launch_choice": ([_I, _I64], _I),
+    "compas_b200_simulate_magnetization_tangents": ([_P, _P, _P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)], _I),
+    "compas_b200_set_fisp_tangent_launch": ([_I], None),
+    "compas_b200_fisp_tangent_config_count": ([], _I),
+    "compas_b200_fisp_tangent_config_info": ([_I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
     "compas_b200_make_batch": ([_P, _I, _P, _P, _P, _P, _I], _P),
     "compas_b200_batch_run": ([_P], _I),
     "compas_b200_batch_echos": ([_P, _I], _P),
@@ -374,6 +378,22 @@ def simulate_magnetization_derivatives(context, echos, parameters, sequence, del
             "T2": simulate_magnetization_derivative(context, 1, echos, parameters, sequence, delta)}
 
 
+def simulate_magnetization_tangents(context: Context, parameters: TissueParameters, sequence) -> dict:
+    """Echoes and their exact derivatives ∂/∂T1, ∂/∂T2 in one pass (forward-mode tangents):
+    {"echos", "T1", "T2"}, each [nreadouts][nvoxels]. "echos" is simulate_magnetization's
+    recurrence (equal to FP32 rounding); "T1"/"T2" are the Δ → 0 limit of
+    simulate_magnetization_derivative."""
+    if not isinstance(sequence, (FispSequence, pSSFPSequence)):
+        raise CompasError("unknown sequence type")
+    out = [_P(), _P(), _P()]
+    rc = library().compas_b200_simulate_magnetization_tangents(context.ptr, parameters.ptr, sequence.ptr,
+                                                               C.byref(out[0]), C.byref(out[1]), C.byref(out[2]))
+    if rc != 0:
+        _check(None, "simulate_magnetization_tangents!")
+    shape = (sequence.nreadouts, parameters.nvoxels)
+    return {k: CompasArray(context, p.value, np.complex64, shape) for k, p in zip(("echos", "T1", "T2"), out)}
+
+
 def magnetization_to_signal(context: Context, echos, parameters: TissueParameters, trajectory, coils,
                             method: Optional[str] = None, low_precision: bool = False) -> CompasArray:
     """method=None uses the reference's C ABI entry point (MatmulFast, or MatmulLow when
@@ -497,9 +517,10 @@ class SimulationBatch(_Object):
 
 
 class GaussNewtonStep(_Object):
-    """compas_b200_make_gauss_newton: one Gauss-Newton iteration on the device (simulate, FD
-    derivatives, signal, residual against `data`, `cg_iterations` CGLS steps of J·v / Jᴴ·v,
-    parameter update), captured as a CUDA graph on the first graph run."""
+    """compas_b200_make_gauss_newton: one Gauss-Newton iteration on the device (simulate,
+    derivatives — forward differences with step `delta`, or exact tangents for delta=0 — signal,
+    residual against `data`, `cg_iterations` CGLS steps of J·v / Jᴴ·v, parameter update),
+    captured as a CUDA graph on the first graph run."""
 
     ARRAYS = {"parameters": 0, "echos": 1, "dT1": 2, "dT2": 3, "signal": 4, "gradient": 5, "step": 6,
               "scalars": 7}
@@ -613,6 +634,21 @@ def launch_count() -> int:
 def set_fisp_launch(config: int = -1, warps: int = -1):
     library().compas_b200_set_fisp_launch(int(config), int(warps))
     _check()
+
+
+def set_fisp_tangent_launch(config: int = -1):
+    library().compas_b200_set_fisp_tangent_launch(int(config))
+    _check()
+
+
+def fisp_tangent_configs() -> list:
+    lib = library()
+    out = []
+    for i in range(lib.compas_b200_fisp_tangent_config_count()):
+        k, g = C.c_int(), C.c_int()
+        lib.compas_b200_fisp_tangent_config_info(i, C.byref(k), C.byref(g))
+        out.append((k.value, g.value))
+    return out
 
 
 def set_pssfp_launch(config: int = -1):

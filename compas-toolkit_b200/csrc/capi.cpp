@@ -150,6 +150,7 @@ void residual_noalloc(int device, const cfloat* lhs, const cfloat* rhs, cfloat* 
 unsigned long long launch_count();
 void set_fisp_override(int config, int warps);
 void set_pssfp_override(int config);
+void set_fisp_tangent_override(int config);
 }  // namespace compas
 
 extern "C" {
@@ -394,6 +395,27 @@ compas_array* compas_simulate_magnetization_derivative_fisp(const compas_context
     });
 }
 
+int compas_b200_simulate_magnetization_tangents(const compas_context* ctx, const compas_object* parameters,
+                                                const compas_object* sequence, compas_array** echos,
+                                                compas_array** delta_echos_T1, compas_array** delta_echos_T2) {
+    t_has_error = false;
+    guarded([&] {
+        if (!echos || !delta_echos_T1 || !delta_echos_T2) throw compas::CompasException("null output pointer");
+        if (!sequence) throw compas::CompasException("null object handle");
+        const auto& params = unwrap<compas::TissueParameters>(parameters);
+        const auto* seq = handle<compas::Object>(sequence);
+        compas::MagnetizationTangents t;
+        if (const auto* fisp = dynamic_cast<const compas::FISPSequence*>(seq))
+            t = compas::simulate_magnetization_tangents(ctx_of(ctx), params, *fisp);
+        else
+            t = compas::simulate_magnetization_tangents(ctx_of(ctx), params, unwrap<compas::pSSFPSequence>(sequence));
+        *echos = new_array(std::move(t.echos));
+        *delta_echos_T1 = new_array(std::move(t.dT1));
+        *delta_echos_T2 = new_array(std::move(t.dT2));
+    });
+    return t_has_error ? -1 : 0;
+}
+
 compas_array* compas_b200_magnetization_to_signal(const compas_context* ctx, const compas_array* echos,
                                                   const compas_object* parameters, const compas_object* trajectory,
                                                   const compas_array* coils, int method) {
@@ -470,6 +492,18 @@ int64_t compas_b200_array_extent(const compas_array* array, int axis) {
 
 void compas_b200_set_fisp_launch(int config, int warps) {
     guarded([&] { compas::set_fisp_override(config, warps); });
+}
+
+void compas_b200_set_fisp_tangent_launch(int config) {
+    guarded([&] { compas::set_fisp_tangent_override(config); });
+}
+
+int compas_b200_fisp_tangent_config_count(void) {
+    return compas::fisp_tangent_config_count();
+}
+
+int compas_b200_fisp_tangent_config_info(int index, int* states_per_lane, int* lanes) {
+    return compas::fisp_tangent_config_info(index, states_per_lane, lanes) ? 1 : 0;
 }
 
 void compas_b200_set_pssfp_launch(int config) {

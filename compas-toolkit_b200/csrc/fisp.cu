@@ -19,6 +19,7 @@
 // * The per-(position, TR) RF angle and phase table is built once per sequence and kept
 //   resident with it.
 #include <cfloat>
+#include <type_traits>
 
 #include "common.cuh"
 #include "compas/compas.h"
@@ -209,10 +210,105 @@ struct EPG {
     }
 };
 
+// Forward-mode tangents ∂/∂T1 and ∂/∂T2 carried with the state.
+//
+// The reference differentiates by forward differences, one more simulation per field at
+// p + Δ·e_field (src/simulate/derivative.cu:11-62, derivative_kernels.cuh:6-35). Every step of
+// the recurrence is affine in the state, x' = M(θ)·x + b(θ), so its tangent is
+// x'_θ = M·x_θ + M_θ·x + b_θ. With the relaxation folded into the excitation (file header) the
+// extra terms are the same excitation applied to a shifted input:
+//  * T1 enters through E1 = e^{-t/T1} on Z and the regrowth (1 - E1) on Z0, and
+//    ∂E1/∂T1 = s1·E1 with s1 = t/T1², so M_θ·x + b_θ = M·(0, 0, s1·(z - δ_{n0})): the T1 tangent
+//    is the excitation of (u₁, g₁, z₁ + s1·(z - δ_{n0}));
+//  * T2 enters through c = E2·e^{2πi·B0·t} on F+ and conj(F-), ∂c/∂T2 = s2·c with s2 = t/T2²:
+//    the T2 tangent is the excitation of (u₂ + s2·u, g₂ + s2·g, z₂).
+// Per state and TR that is 26 + 28 + 30 FP32 operations, about what the value and two
+// forward-difference simulations cost, without the differences' cancellation error.
+template<int K, int G>
+struct EPGTangent {
+    EPG<K, G> x, d1, d2;  // value, ∂/∂T1, ∂/∂T2
+
+    __device__ __forceinline__ void init(int sub) {
+        x.init(sub);
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            d1.u[i] = d1.g[i] = d1.z[i] = make_float2(0.f, 0.f);
+            d2.u[i] = d2.g[i] = d2.z[i] = make_float2(0.f, 0.f);
+        }
+    }
+
+    template<bool ONEHOT>
+    __device__ __forceinline__ void shift(int sub, int N) {
+        x.template shift<ONEHOT>(sub, N);
+        d1.template shift<ONEHOT>(sub, N);
+        d2.template shift<ONEHOT>(sub, N);
+    }
+
+    // z - δ_{n0}: the regrowth's share of ∂Z/∂E1 (state 0 lives in slot 0 of lane 0)
+    __device__ __forceinline__ float2 zshift(int i, int sub) const {
+        return make_float2(i == 0 && sub == 0 ? x.z[0].x - 1.0f : x.z[i].x, x.z[i].y);
+    }
+
+    // excitation k, which holds the relaxation over t before it; s1 = t/T1², s2 = t/T2²
+    __device__ __forceinline__ void excite(const ExciteCoefs& k, float s1, float s2, int sub) {
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            const float2 zs = zshift(i, sub);
+            float2 z1 = make_float2(fmaf(s1, zs.x, d1.z[i].x), fmaf(s1, zs.y, d1.z[i].y));
+            float2 u2 = make_float2(fmaf(s2, x.u[i].x, d2.u[i].x), fmaf(s2, x.u[i].y, d2.u[i].y));
+            float2 g2 = make_float2(fmaf(s2, x.g[i].x, d2.g[i].x), fmaf(s2, x.g[i].y, d2.g[i].y));
+            excite_state(d1.u[i], d1.g[i], z1, k);
+            d1.z[i] = z1;
+            excite_state(u2, g2, d2.z[i], k);
+            d2.u[i] = u2;
+            d2.g[i] = g2;
+        }
+        x.excite(k, sub);
+    }
+
+    // relaxation over t: F·c, Z·E1, Z0 += 1 - E1
+    __device__ __forceinline__ void relax(float2 c, float E1, float s1, float s2, int sub) {
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            const float2 zs = zshift(i, sub);
+            d1.u[i] = cmul(d1.u[i], c);
+            d1.g[i] = cmul(d1.g[i], c);
+            d1.z[i] = cscale(E1, make_float2(fmaf(s1, zs.x, d1.z[i].x), fmaf(s1, zs.y, d1.z[i].y)));
+            d2.u[i] = cmul(make_float2(fmaf(s2, x.u[i].x, d2.u[i].x), fmaf(s2, x.u[i].y, d2.u[i].y)), c);
+            d2.g[i] = cmul(make_float2(fmaf(s2, x.g[i].x, d2.g[i].x), fmaf(s2, x.g[i].y, d2.g[i].y)), c);
+            d2.z[i] = cscale(E1, d2.z[i]);
+        }
+        x.relax(c, E1, sub);
+    }
+
+    // inversion, spoiling, then longitudinal relaxation over TI (s1 = TI/T1²)
+    __device__ __forceinline__ void invert_decay(float E1, float s1, int sub) {
+        x.invert_spoil();
+        d1.invert_spoil();
+        d2.invert_spoil();
+#pragma unroll
+        for (int i = 0; i < K; i++) {
+            const float2 zs = zshift(i, sub);
+            d1.z[i] = cscale(E1, make_float2(fmaf(s1, zs.x, d1.z[i].x), fmaf(s1, zs.y, d1.z[i].y)));
+            d2.z[i] = cscale(E1, d2.z[i]);
+            x.z[i] = cscale(E1, x.z[i]);
+        }
+        if (sub == 0) x.z[0].x += 1.0f - E1;
+    }
+
+    __device__ __forceinline__ void spoil() {
+        x.spoil();
+        d1.spoil();
+        d2.spoil();
+    }
+};
+
 // One voxel tile (VB = 32/G voxels, all slice positions) of a FISP simulation; the CTA's W
 // warps sweep the positions. Shared by the one-simulation kernel (tile = blockIdx.x) and the
 // batched work-queue kernel (tile taken from the queue), so both give bit-identical echoes.
-template<int K, int G, bool ONEHOT>
+// TAN: also propagate ∂/∂T1 and ∂/∂T2 (EPGTangent) and write them to a.dT1, a.dT2; the
+// value goes through the same operations either way.
+template<int K, int G, bool ONEHOT, bool TAN = false>
 __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, float2* samples) {
     constexpr int VB = 32 / G;
     const int W = blockDim.x >> 5;
@@ -242,21 +338,30 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
     const float E1_W = expf(-a.TW * R1);
     const float2 c_W = cscale(expf(-a.TW * R2), rot(a.TW));
     const float beta = 1.0f - E1_TR;
+    // tangent factors t/T1², t/T2² of each relaxation interval
+    const float s1_TR = a.TR * R1 * R1, s2_TR = a.TR * R2 * R2, s2_TE = a.TE * R2 * R2;
+    const float s1_TI = a.TI * R1 * R1, s1_W = a.TW * R1 * R1, s2_W = a.TW * R2 * R2;
+    const int plane = W * 32 * VB;  // sample planes: value, ∂/∂T1, ∂/∂T2
+    constexpr int NQ = TAN ? 3 : 1;
 
     const int nrounds = (a.P + W - 1) / W;
     for (int round = 0; round < nrounds; round++) {
         const int p = round * W + warp;
         const bool pok = p < a.P;  // warp-uniform
         const float4* tab = a.table + int64_t(pok ? p : 0) * a.nTR;
-        EPG<K, G> st;
+        std::conditional_t<TAN, EPGTangent<K, G>, EPG<K, G>> st;
         st.init(sub);
         for (int rep = a.reps; rep >= 1; rep--) {
             const bool sampled = (rep == 1);
             if (a.inversion) {  // invert, spoil, decay(TI), regrowth (fisp_kernels.cuh:146-152)
-                st.invert_spoil();
+                if constexpr (TAN) {
+                    st.invert_decay(E1_TI, s1_TI, sub);
+                } else {
+                    st.invert_spoil();
 #pragma unroll
-                for (int i = 0; i < K; i++) st.z[i] = cscale(E1_TI, st.z[i]);
-                if (sub == 0) st.z[0].x += 1.0f - E1_TI;
+                    for (int i = 0; i < K; i++) st.z[i] = cscale(E1_TI, st.z[i]);
+                    if (sub == 0) st.z[0].x += 1.0f - E1_TI;
+                }
             }
             for (int t0 = 0; t0 < a.nTR; t0 += 32) {
                 const int nt = min(32, a.nTR - t0);
@@ -264,29 +369,47 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
                     for (int j = 0; j < nt; j++) {
                         const int t = t0 + j;
                         const float4 tv = __ldg(tab + t);
-                        if (t == 0) {
-                            st.excite(make_coefs(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), sub);
+                        if constexpr (TAN) {
+                            if (t == 0) {
+                                st.excite(make_coefs(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), 0.0f, 0.0f, sub);
+                            } else {
+                                st.template shift<ONEHOT>(sub, a.N);
+                                st.excite(make_coefs(tv, B1, c_TR, E1_TR, beta), s1_TR, s2_TR, sub);
+                            }
+                            if (sampled && sub == 0) {
+                                float2* q = samples + (warp * 32 + j) * VB + grp;
+                                q[0] = cmul(c_TE, st.x.u[0]);
+                                q[plane] = cmul(c_TE, st.d1.u[0]);
+                                q[2 * plane] = cmul(c_TE, make_float2(fmaf(s2_TE, st.x.u[0].x, st.d2.u[0].x),
+                                                                      fmaf(s2_TE, st.x.u[0].y, st.d2.u[0].y)));
+                            }
                         } else {
-                            st.template shift<ONEHOT>(sub, a.N);
-                            st.excite(make_coefs(tv, B1, c_TR, E1_TR, beta), sub);
+                            if (t == 0) {
+                                st.excite(make_coefs(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), sub);
+                            } else {
+                                st.template shift<ONEHOT>(sub, a.N);
+                                st.excite(make_coefs(tv, B1, c_TR, E1_TR, beta), sub);
+                            }
+                            if (sampled && sub == 0) samples[(warp * 32 + j) * VB + grp] = cmul(c_TE, st.u[0]);
                         }
-                        if (sampled && sub == 0) samples[(warp * 32 + j) * VB + grp] = cmul(c_TE, st.u[0]);
                     }
                 } else if (sampled && sub == 0) {
-                    for (int j = 0; j < nt; j++) samples[(warp * 32 + j) * VB + grp] = make_float2(0.f, 0.f);
+                    for (int j = 0; j < nt; j++)
+                        for (int q = 0; q < NQ; q++) samples[q * plane + (warp * 32 + j) * VB + grp] = make_float2(0.f, 0.f);
                 }
                 if (sampled) {
                     __syncthreads();
                     // Σ over the warps' positions in fixed order, then write / accumulate the
                     // undersampling-expanded rows (fisp_kernels.cuh:246-259)
-                    for (int e = threadIdx.x; e < nt * VB; e += blockDim.x) {
-                        const int j = e / VB, gv = e % VB;
+                    for (int e = threadIdx.x; e < NQ * nt * VB; e += blockDim.x) {
+                        const int qn = e / (nt * VB), j = (e / VB) % nt, gv = e % VB;
                         const int v = tile * VB + gv;
                         float2 acc = make_float2(0.f, 0.f);
-                        for (int w = 0; w < W; w++) acc = cadd(acc, samples[(w * 32 + j) * VB + gv]);
+                        for (int w = 0; w < W; w++) acc = cadd(acc, samples[qn * plane + (w * 32 + j) * VB + gv]);
                         if (v < a.nvoxels) {
+                            float2* out = qn == 0 ? a.echo : qn == 1 ? a.dT1 : a.dT2;
                             for (int q = 0; q < a.uf; q++) {
-                                float2* dst = a.echo + (int64_t(t0 + j) * a.uf + q) * a.echo_stride + a.voxel_begin + v;
+                                float2* dst = out + (int64_t(t0 + j) * a.uf + q) * a.echo_stride + a.voxel_begin + v;
                                 *dst = round == 0 ? acc : cadd(*dst, acc);
                             }
                         }
@@ -296,10 +419,17 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
             }
             if (rep > 1) {  // close the repetition: relax to TR, dephase, spoil, wait (fisp_kernels.cuh:195-200)
                 if (pok) {
-                    st.relax(c_TR, E1_TR, sub);
-                    st.template shift<ONEHOT>(sub, a.N);
-                    if (a.wait_spoil) st.spoil();
-                    st.relax(c_W, E1_W, sub);
+                    if constexpr (TAN) {
+                        st.relax(c_TR, E1_TR, s1_TR, s2_TR, sub);
+                        st.template shift<ONEHOT>(sub, a.N);
+                        if (a.wait_spoil) st.spoil();
+                        st.relax(c_W, E1_W, s1_W, s2_W, sub);
+                    } else {
+                        st.relax(c_TR, E1_TR, sub);
+                        st.template shift<ONEHOT>(sub, a.N);
+                        if (a.wait_spoil) st.spoil();
+                        st.relax(c_W, E1_W, sub);
+                    }
                 }
             }
         }
@@ -341,6 +471,13 @@ __global__ void __launch_bounds__(256, 1) fisp_queue_kernel(const FispArgs* __re
     }
 }
 
+// One FISP simulation with its T1 and T2 tangents: value, ∂/∂T1, ∂/∂T2 into a.echo, a.dT1, a.dT2.
+template<int K, int G>
+__global__ void __launch_bounds__(256, 1) fisp_tangent_kernel(FispArgs a) {
+    extern __shared__ float2 samples[];  // [3][W][32][VB]
+    fisp_tile<K, G, kOneHotZeroing<K, G>, true>(a, blockIdx.x, samples);
+}
+
 }  // namespace kernels
 
 // ------------------------------------------------------------------------------------------
@@ -380,6 +517,22 @@ const FispConfig kFispConfigs[] = {
     {8, 16, kernels::fisp_epg_kernel<8, 16>, kernels::fisp_queue_kernel<8, 16>},
     {4, 32, kernels::fisp_epg_kernel<4, 32>, kernels::fisp_queue_kernel<4, 32>},
 };
+
+// Tangent layouts: three state vectors per (voxel, position), so at most 8 states per lane
+// (8 × 18 floats); the 25-state MR-STAT case splits over 4 lanes of 7 states.
+struct FispTangentConfig {
+    int K, G;
+    FispKernel fn;
+};
+const FispTangentConfig kFispTangentConfigs[] = {
+    {1, 1, kernels::fisp_tangent_kernel<1, 1>}, {2, 1, kernels::fisp_tangent_kernel<2, 1>},
+    {4, 1, kernels::fisp_tangent_kernel<4, 1>}, {8, 1, kernels::fisp_tangent_kernel<8, 1>},
+    {2, 4, kernels::fisp_tangent_kernel<2, 4>}, {4, 4, kernels::fisp_tangent_kernel<4, 4>},
+    {7, 4, kernels::fisp_tangent_kernel<7, 4>}, {8, 4, kernels::fisp_tangent_kernel<8, 4>},
+    {4, 8, kernels::fisp_tangent_kernel<4, 8>}, {8, 8, kernels::fisp_tangent_kernel<8, 8>},
+    {8, 16, kernels::fisp_tangent_kernel<8, 16>},
+};
+constexpr int kFispTangentConfigCount = int(sizeof(kFispTangentConfigs) / sizeof(kFispTangentConfigs[0]));
 
 }  // namespace
 
@@ -483,6 +636,7 @@ kernels::FispArgs fisp_args(const CompasContext& ctx, const TissueParameters& pa
     a.TI = seq.TI;
     a.echo = reinterpret_cast<float2*>(echo);
     a.echo_stride = echo_stride;
+    a.dT1 = a.dT2 = nullptr;
     return a;
 }
 
@@ -533,6 +687,62 @@ void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int v
     check_launch("fisp_epg_kernel");
 }
 
+int fisp_tangent_config_count() {
+    return kFispTangentConfigCount;
+}
+
+bool fisp_tangent_config_info(int index, int* K, int* G) {
+    if (index < 0 || index >= kFispTangentConfigCount) return false;
+    *K = kFispTangentConfigs[index].K;
+    *G = kFispTangentConfigs[index].G;
+    return true;
+}
+
+// Tangent layout for N states: with many (voxel, position) pairs and N ≤ 8 all states in one
+// lane; otherwise the covering layout with the least padding, fewer lanes on ties. The warps
+// per CTA are the value kernel's (tuned_fisp_launch): 8 for the MR-STAT slice, where 7 and 5
+// measured 9 % and 54 % slower (one CTA of 255-register threads per SM).
+FispLaunch fisp_tangent_default_launch(int N, int64_t nvoxels, int P) {
+    const bool wide = nvoxels * P >= 148LL * 32 * 8;
+    int best = -1;
+    for (int i = 0; i < kFispTangentConfigCount; i++) {
+        const auto& c = kFispTangentConfigs[i];
+        if (c.K * c.G < N || (c.G == 1) != (wide && N <= 8)) continue;
+        const auto& b = kFispTangentConfigs[best < 0 ? 0 : best];
+        if (best < 0 || c.K * c.G < b.K * b.G) best = i;
+    }
+    if (best < 0)
+        for (int i = 0; i < kFispTangentConfigCount; i++)
+            if (kFispTangentConfigs[i].K * kFispTangentConfigs[i].G >= N) {
+                best = i;
+                break;
+            }
+    return FispLaunch {best, tuned_fisp_launch(N, nvoxels, P).warps};
+}
+
+void launch_fisp_tangent(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
+                         const FISPSequence& seq, cfloat* echo, cfloat* dT1, cfloat* dT2, int64_t echo_stride,
+                         FispLaunch L) {
+    const int nTR = int(seq.RF_train.size());
+    const int P = int(seq.sliceprofiles.size(0));
+    const int N = seq.max_state;
+    kernels::FispArgs a = fisp_args(ctx, params, voxel_begin, nvoxels, seq, echo, echo_stride);  // validates
+    if (nvoxels <= 0 || nTR <= 0) return;
+    if (L.config < 0) L = fisp_tangent_default_launch(N, nvoxels, P);
+    COMPAS_CHECK(L.config >= 0 && L.config < kFispTangentConfigCount);
+    const auto& cfg = kFispTangentConfigs[L.config];
+    COMPAS_CHECK(cfg.K * cfg.G >= N);
+    a.dT1 = reinterpret_cast<float2*>(dT1);
+    a.dT2 = reinterpret_cast<float2*>(dT2);
+    const int VB = 32 / cfg.G;
+    const int W = std::max(1, std::min(L.warps, 8));
+    const size_t smem = 3 * size_t(W) * 32 * VB * sizeof(float2);  // ≤ 192 KB
+    DeviceGuard guard(ctx.device());
+    allow_smem(reinterpret_cast<const void*>(cfg.fn), smem);
+    cfg.fn<<<div_ceil(nvoxels, VB), 32 * W, smem, ctx.stream()>>>(a);
+    check_launch("fisp_tangent_kernel");
+}
+
 void launch_fisp_queue(cudaStream_t stream, int device, FispLaunch L, int max_state, const kernels::FispArgs* jobs,
                        const int2* items, int nitems, int* head) {
     if (nitems <= 0) return;
@@ -558,6 +768,20 @@ Array<cfloat, 2> simulate_magnetization(const CompasContext& context, TissuePara
     Array<cfloat, 2> echos({nreadouts, nvoxels}, context.device(), context.stream());
     launch_fisp(context, parameters, 0, nvoxels, sequence, echos.data(), nvoxels, tuned_fisp_launch(sequence.max_state, nvoxels, int(sequence.sliceprofiles.size(0))));
     return echos;
+}
+
+MagnetizationTangents simulate_magnetization_tangents(const CompasContext& context, TissueParameters parameters,
+                                                      FISPSequence sequence) {
+    COMPAS_CHECK(sequence.undersampling_factor >= 1);
+    const int nreadouts = int(sequence.RF_train.size()) * sequence.undersampling_factor;
+    const int nvoxels = parameters.nvoxels;
+    MagnetizationTangents out {{{nreadouts, nvoxels}, context.device(), context.stream()},
+                               {{nreadouts, nvoxels}, context.device(), context.stream()},
+                               {{nreadouts, nvoxels}, context.device(), context.stream()}};
+    launch_fisp_tangent(context, parameters, 0, nvoxels, sequence, out.echos.data(), out.dT1.data(), out.dT2.data(),
+                        nvoxels, tuned_fisp_tangent_launch(sequence.max_state, nvoxels,
+                                                           int(sequence.sliceprofiles.size(0))));
+    return out;
 }
 
 }  // namespace compas

@@ -9,7 +9,8 @@
 // on the context's stream with every buffer allocated once, and is captured into a CUDA graph
 // on first use, so one replay issues the ~20 kernels of an iteration with one launch:
 //
-//   m = simulate(p);  ∂m/∂T1, ∂m/∂T2 by forward differences (absolute step Δ, as the reference);
+//   m = simulate(p);  ∂m/∂T1, ∂m/∂T2 by forward differences (absolute step Δ, as the reference),
+//   or, with Δ = 0, m and its exact derivatives in one forward-mode tangent pass;
 //   s = signal(m);  b = y - s;  objective = ‖b‖²;
 //   CGLS on the linearised problem  min_δ ‖J δ - b‖²  over real δ in the scaled coordinates
 //   of the Jacobian (δT1/T1, δT2/T2, δRe ρ, δIm ρ), starting from δ = 0:
@@ -227,11 +228,22 @@ void GaussNewtonStep::Impl::enqueue() const {
     const int sb = int(std::min<int64_t>((nsig + 255) / 256, 148 * 16));
     const int vb = int(std::min<int64_t>((nv4 + 255) / 256, 148 * 16));
 
-    // model and finite-difference derivatives
-    simulate(params, echos.data());
+    // model and derivatives: exact tangents in one pass (delta = 0), or forward differences
+    if (delta == 0.0f) {
+        if (const auto* f = std::get_if<FISPSequence>(&sequence)) {
+            launch_fisp_tangent(ctx, params, 0, V, *f, echos.data(), dT1.data(), dT2.data(), V,
+                                tuned_fisp_tangent_launch(f->max_state, V, int(f->sliceprofiles.size(0))));
+        } else {
+            const auto& s = std::get<pSSFPSequence>(sequence);
+            launch_pssfp_tangent(ctx, params, 0, V, s, echos.data(), dT1.data(), dT2.data(), V,
+                                 tuned_pssfp_launch(int(s.z.size()), V));
+        }
+    } else {
+        simulate(params, echos.data());
+    }
     const TissueParameters shifted(perturbed, params.has_z, params.has_b0, params.has_b1);
     const Array<cfloat, 2>* dst[2] = {&dT1, &dT2};
-    for (int field = 0; field < 2; field++) {
+    for (int field = 0; field < 2 && delta != 0.0f; field++) {
         add_difference_kernel<<<div_ceil(V, 256), 256, 0, st>>>(pdata, perturbed.data(), V, field, delta);
         check_launch("add_difference_kernel");
         simulate(shifted, dst[field]->data());
@@ -298,7 +310,7 @@ GaussNewtonStep::GaussNewtonStep(const CompasContext& ctx, TissueParameters para
     COMPAS_CHECK(coil_sensitivities.size(1) == V);
     COMPAS_CHECK(data.size(0) == C && data.size(1) == R && data.size(2) == S);
     if (cg_iterations < 1) COMPAS_ERROR("at least one conjugate-gradient iteration is needed");
-    if (delta == 0.0f) COMPAS_ERROR("finite-difference step must be nonzero");
+    if (!std::isfinite(delta)) COMPAS_ERROR("finite-difference step must be finite (0 selects exact derivatives)");
     COMPAS_CHECK(V > 0);
 
     // the estimate is a private copy of the parameters (updated in place by every iteration)

@@ -22,6 +22,8 @@ struct FispArgs {
     float TR, TE, TW, TI;
     float2* echo;          // [nTR*uf][echo_stride], column = voxel_begin + local voxel
     int64_t echo_stride;
+    float2* dT1;           // ∂echo/∂T1, ∂echo/∂T2 (same layout); used by the tangent kernels only
+    float2* dT2;
 };
 
 struct PssfpArgs {
@@ -34,6 +36,8 @@ struct PssfpArgs {
     float dt_ex, dt_inv, dt_pr, gz_ex, gz_pr;
     float2* echo;  // [nTR][echo_stride]
     int64_t echo_stride;
+    float2* dT1;   // ∂echo/∂T1, ∂echo/∂T2 (same layout); used by the tangent kernels only
+    float2* dT2;
 };
 
 struct SpiralArgs {

@@ -32,6 +32,15 @@ int fisp_tile_voxels(FispLaunch L);  // voxels per work item (tile) of layout L
 void launch_fisp_queue(cudaStream_t stream, int device, FispLaunch L, int max_state, const kernels::FispArgs* jobs,
                        const int2* items, int nitems, int* head);
 
+// value and T1/T2 tangents (forward mode) in one launch; L.config indexes the tangent layouts
+int fisp_tangent_config_count();
+bool fisp_tangent_config_info(int index, int* K, int* G);
+FispLaunch fisp_tangent_default_launch(int N, int64_t nvoxels, int P);
+FispLaunch tuned_fisp_tangent_launch(int N, int64_t nvoxels, int P);  // honours the test override
+void launch_fisp_tangent(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
+                         const FISPSequence& seq, cfloat* echo, cfloat* dT1, cfloat* dT2, int64_t echo_stride,
+                         FispLaunch L);
+
 // ---- pSSFP ------------------------------------------------------------------------------
 struct PssfpLaunch {
     int config;  // index into the instantiated (ZT, GZ) layouts, -1 = default
@@ -45,6 +54,10 @@ void launch_pssfp(const CompasContext& ctx, const TissueParameters& params, int 
 kernels::PssfpArgs pssfp_args(const CompasContext& ctx, const TissueParameters& params, int voxel_begin,
                               int nvoxels, const pSSFPSequence& seq, cfloat* echo, int64_t echo_stride);
 int pssfp_tile_voxels(PssfpLaunch L);
+// value and T1/T2 tangents (forward mode) in one launch of layout L
+void launch_pssfp_tangent(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
+                          const pSSFPSequence& seq, cfloat* echo, cfloat* dT1, cfloat* dT2, int64_t echo_stride,
+                          PssfpLaunch L);
 void launch_pssfp_queue(cudaStream_t stream, int device, PssfpLaunch L, int nz, const kernels::PssfpArgs* jobs,
                         const int2* items, int nitems, int* head);
 

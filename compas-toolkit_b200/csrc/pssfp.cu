@@ -62,39 +62,66 @@ __device__ __forceinline__ RotRelax make_rot_relax(float E1, float E2) {
     return k;
 }
 
-// rotation about the unnormalised axis (ax, ay, az) by |a|   (isochromat.cuh:14-73), followed by
-// relaxation: transverse components times E2, longitudinal z·E1 + 1 - E1. E2 is folded into the
-// rotation coefficients and E1 enters as E1/E2 on the E2-scaled longitudinal result.
-__device__ __forceinline__ void rotate_relax(Iso& m, float ax, float ay, float az, float axy2, const RotRelax& k) {
-    const float t2 = fmaf(az, az, axy2);
-    float c, s, h;  // E2·cos θ, E2·sin θ/θ, E2·(1-cos θ)/θ²
+// E2-scaled rotation coefficients for θ² = t2: E2·cos θ, E2·sin θ/θ, E2·(1-cos θ)/θ²
+struct RotCoefs {
+    float c, s, h;
+};
+
+__device__ __forceinline__ RotCoefs rot_coefs(float t2, const RotRelax& k) {
+    RotCoefs q;
     if (t2 <= 0.25f) {
         // Taylor series in x = θ² through x³ (the next terms, x⁴/9! and x⁴/10!, are below 1.1e-8
         // relative for x ≤ 0.25, under FP32 resolution), cos θ = 1 - x·(1-cos θ)/θ²
         const float x = t2;
-        s = fmaf(x, fmaf(x, fmaf(x, k.s3, k.s2), k.s1), k.s0);
-        h = fmaf(x, fmaf(x, fmaf(x, k.h3, k.h2), k.h1), k.h0);
-        c = fmaf(-x, h, k.E2);
+        q.s = fmaf(x, fmaf(x, fmaf(x, k.s3, k.s2), k.s1), k.s0);
+        q.h = fmaf(x, fmaf(x, fmaf(x, k.h3, k.h2), k.h1), k.h0);
+        q.c = fmaf(-x, q.h, k.E2);
     } else {
         const float th = sqrtf(t2);
         float sn, cs;
         sincosf(th, &sn, &cs);
-        c = k.E2 * cs;
-        s = k.E2 * (sn / th);
-        h = k.E2 * ((1.0f - cs) / t2);
+        q.c = k.E2 * cs;
+        q.s = k.E2 * (sn / th);
+        q.h = k.E2 * ((1.0f - cs) / t2);
     }
+    return q;
+}
+
+// rotation about the unnormalised axis (ax, ay, az) by |a|   (isochromat.cuh:14-73), followed by
+// relaxation: transverse components times E2, longitudinal z·E1 + 1 - E1. E2 is folded into the
+// rotation coefficients and E1 enters as E1/E2 on the E2-scaled longitudinal result.
+__device__ __forceinline__ void rotate_relax(Iso& m, float ax, float ay, float az, const RotCoefs& q,
+                                             const RotRelax& k) {
     const float cx = ay * m.z - az * m.y;
     const float cy = az * m.x - ax * m.z;
     const float cz = ax * m.y - ay * m.x;
-    const float hd = h * fmaf(ax, m.x, fmaf(ay, m.y, az * m.z));
-    m.x = fmaf(c, m.x, fmaf(s, cx, hd * ax));
-    m.y = fmaf(c, m.y, fmaf(s, cy, hd * ay));
-    m.z = fmaf(k.r, fmaf(c, m.z, fmaf(s, cz, hd * az)), k.oneE1);
+    const float hd = q.h * fmaf(ax, m.x, fmaf(ay, m.y, az * m.z));
+    m.x = fmaf(q.c, m.x, fmaf(q.s, cx, hd * ax));
+    m.y = fmaf(q.c, m.y, fmaf(q.s, cy, hd * ay));
+    m.z = fmaf(k.r, fmaf(q.c, m.z, fmaf(q.s, cz, hd * az)), k.oneE1);
+}
+
+// Tangent of rotate_relax: the same linear map applied to d (without the regrowth 1 - E1) plus
+// the explicit derivative (px, py, pz) of the step at the current state.
+__device__ __forceinline__ void rotate_relax_tangent(Iso& d, float ax, float ay, float az, const RotCoefs& q,
+                                                     const RotRelax& k, float px, float py, float pz) {
+    const float cx = ay * d.z - az * d.y;
+    const float cy = az * d.x - ax * d.z;
+    const float cz = ax * d.y - ay * d.x;
+    const float hd = q.h * fmaf(ax, d.x, fmaf(ay, d.y, az * d.z));
+    d.x = fmaf(q.c, d.x, fmaf(q.s, cx, fmaf(hd, ax, px)));
+    d.y = fmaf(q.c, d.y, fmaf(q.s, cy, fmaf(hd, ay, py)));
+    d.z = fmaf(k.r, fmaf(q.c, d.z, fmaf(q.s, cz, hd * az)), pz);
 }
 
 // One tile (128/GZ voxels) of a pSSFP simulation. Shared by the one-simulation kernel
 // (tile = blockIdx.x) and the batched work-queue kernel, so both give bit-identical echoes.
-template<int ZT, int GZ>
+// TAN: also propagate ∂m/∂T1 and ∂m/∂T2 (forward mode) and write their sums to a.dT1, a.dT2.
+// Every step is affine in m: m' = D(θ)·R·m + (0, 0, 1 - E1) with D = diag(E2, E2, E1), so the
+// tangent is d' = D·R·d + D_θ·R·m - (0, 0, E1_θ), and with ∂E/∂T = E·t/T² the explicit term is
+// (0, 0, t/T1²·(m'_z - 1)) for T1 and (t/T2²·m'_x, t/T2²·m'_y, 0) for T2, in terms of the new
+// state m'. The value goes through the same operations either way.
+template<int ZT, int GZ, bool TAN = false>
 __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
     const int lane = threadIdx.x & 31;
     const int sub = lane % GZ;
@@ -110,8 +137,13 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
     const float E1_pr = expf(-a.dt_pr * R1), E2_pr = expf(-a.dt_pr * R2);
     const float E1_inv = expf(-a.dt_inv * R1), E2_inv = expf(-a.dt_inv * R2);
     const float twopi = 6.28318530717958647692f;
+    // tangent factors t/T1², t/T2² of each relaxation interval
+    const float s1_ex = a.dt_ex * R1 * R1, s2_ex = a.dt_ex * R2 * R2;
+    const float s1_pr = a.dt_pr * R1 * R1, s2_pr = a.dt_pr * R2 * R2;
+    const float s1_inv = a.dt_inv * R1 * R1;
 
     Iso m[ZT];
+    Iso d1[TAN ? ZT : 1], d2[TAN ? ZT : 1];  // ∂m/∂T1, ∂m/∂T2
     float az[ZT], cpr[ZT], spr[ZT];
     bool valid[ZT];
     const float cinv = cospif(B1);  // invert(p): z·cos(πB1)   (isochromat.cuh:100-112)
@@ -126,6 +158,10 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
         m[k].y = 0.0f;
         m[k].z = cinv * E1_inv + (1.0f - E1_inv);
         (void)E2_inv;
+        if constexpr (TAN) {
+            d1[k] = Iso {0.0f, 0.0f, s1_inv * (m[k].z - 1.0f)};
+            d2[k] = Iso {0.0f, 0.0f, 0.0f};
+        }
     }
 
     const RotRelax rr = make_rot_relax(E1_ex, E2_ex);
@@ -136,17 +172,35 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
             const float ax = zp.x * B1, ay = -zp.y * B1;
             const float axy2 = fmaf(ax, ax, ay * ay);
 #pragma unroll
-            for (int k = 0; k < ZT; k++) rotate_relax(m[k], ax, ay, az[k], axy2, rr);
+            for (int k = 0; k < ZT; k++) {
+                const RotCoefs q = rot_coefs(fmaf(az[k], az[k], axy2), rr);
+                rotate_relax(m[k], ax, ay, az[k], q, rr);
+                if constexpr (TAN) {
+                    rotate_relax_tangent(d1[k], ax, ay, az[k], q, rr, 0.0f, 0.0f, s1_ex * (m[k].z - 1.0f));
+                    rotate_relax_tangent(d2[k], ax, ay, az[k], q, rr, s2_ex * m[k].x, s2_ex * m[k].y, 0.0f);
+                }
+            }
+        }
+    };
+    // free precession by the angle (c, s) and relaxation over dt_pr
+    auto precess_by = [&](int k, float c, float s) {
+        const float x = m[k].x, y = m[k].y;
+        m[k].x = E2_pr * (c * x - s * y);
+        m[k].y = E2_pr * (c * y + s * x);
+        m[k].z = fmaf(m[k].z, E1_pr, 1.0f - E1_pr);
+        if constexpr (TAN) {
+            const float x1 = d1[k].x, y1 = d1[k].y, x2 = d2[k].x, y2 = d2[k].y;
+            d1[k].x = E2_pr * (c * x1 - s * y1);
+            d1[k].y = E2_pr * (c * y1 + s * x1);
+            d1[k].z = fmaf(d1[k].z, E1_pr, s1_pr * (m[k].z - 1.0f));
+            d2[k].x = fmaf(s2_pr, m[k].x, E2_pr * (c * x2 - s * y2));
+            d2[k].y = fmaf(s2_pr, m[k].y, E2_pr * (c * y2 + s * x2));
+            d2[k].z = d2[k].z * E1_pr;
         }
     };
     auto precess = [&]() {
 #pragma unroll
-        for (int k = 0; k < ZT; k++) {
-            const float x = m[k].x, y = m[k].y;
-            m[k].x = E2_pr * (cpr[k] * x - spr[k] * y);
-            m[k].y = E2_pr * (cpr[k] * y + spr[k] * x);
-            m[k].z = fmaf(m[k].z, E1_pr, 1.0f - E1_pr);
-        }
+        for (int k = 0; k < ZT; k++) precess_by(k, cpr[k], spr[k]);
     };
 
     // α/2 pulse, then re- and prephaser with twice the prephasing gradient (pssfp_kernels.cuh:73-80)
@@ -157,10 +211,7 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
         const float z = valid[k] ? a.z[zi] : 0.0f;
         float s2, c2;
         sincosf(-(2.0f * a.gz_pr * z) - a.dt_pr * twopi * B0, &s2, &c2);
-        const float x = m[k].x, y = m[k].y;
-        m[k].x = E2_pr * (c2 * x - s2 * y);
-        m[k].y = E2_pr * (c2 * y + s2 * x);
-        m[k].z = fmaf(m[k].z, E1_pr, 1.0f - E1_pr);
+        precess_by(k, c2, s2);
     }
 
     for (int t = 0; t < a.nTR; t++) {  // pssfp_kernels.cuh:83-107
@@ -179,7 +230,31 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
             sx += __shfl_xor_sync(0xffffffffu, sx, d, GZ);
             sy += __shfl_xor_sync(0xffffffffu, sy, d, GZ);
         }
-        if (sub == 0 && vok) a.echo[int64_t(t) * a.echo_stride + a.voxel_begin + vloc] = make_float2(sx, sy);
+        const int64_t at = int64_t(t) * a.echo_stride + a.voxel_begin + vloc;
+        if (sub == 0 && vok) a.echo[at] = make_float2(sx, sy);
+        if constexpr (TAN) {
+            float t1x = 0.0f, t1y = 0.0f, t2x = 0.0f, t2y = 0.0f;
+#pragma unroll
+            for (int k = 0; k < ZT; k++) {
+                if (valid[k]) {
+                    t1x += d1[k].x;
+                    t1y += d1[k].y;
+                    t2x += d2[k].x;
+                    t2y += d2[k].y;
+                }
+            }
+#pragma unroll
+            for (int d = GZ / 2; d > 0; d /= 2) {
+                t1x += __shfl_xor_sync(0xffffffffu, t1x, d, GZ);
+                t1y += __shfl_xor_sync(0xffffffffu, t1y, d, GZ);
+                t2x += __shfl_xor_sync(0xffffffffu, t2x, d, GZ);
+                t2y += __shfl_xor_sync(0xffffffffu, t2y, d, GZ);
+            }
+            if (sub == 0 && vok) {
+                a.dT1[at] = make_float2(t1x, t1y);
+                a.dT2[at] = make_float2(t2x, t2y);
+            }
+        }
         precess();
     }
 }
@@ -187,6 +262,12 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
 template<int ZT, int GZ>
 __global__ void __launch_bounds__(128) pssfp_kernel(PssfpArgs a) {
     pssfp_tile<ZT, GZ>(a, blockIdx.x);
+}
+
+// One pSSFP simulation with its T1 and T2 tangents into a.echo, a.dT1, a.dT2.
+template<int ZT, int GZ>
+__global__ void __launch_bounds__(128) pssfp_tangent_kernel(PssfpArgs a) {
+    pssfp_tile<ZT, GZ, true>(a, blockIdx.x);
 }
 
 // Persistent work-queue kernel for a batch of pSSFP simulations sharing one (ZT, GZ) layout:
@@ -219,22 +300,37 @@ struct PssfpConfig {
     int ZT, GZ;
     PssfpKernel fn;
     PssfpQueueKernel queue;
+    PssfpKernel tangent;
 };
 const PssfpConfig kPssfpConfigs[] = {
-    {1, 1, kernels::pssfp_kernel<1, 1>, kernels::pssfp_queue_kernel<1, 1>},
-    {2, 1, kernels::pssfp_kernel<2, 1>, kernels::pssfp_queue_kernel<2, 1>},
-    {4, 1, kernels::pssfp_kernel<4, 1>, kernels::pssfp_queue_kernel<4, 1>},
-    {8, 1, kernels::pssfp_kernel<8, 1>, kernels::pssfp_queue_kernel<8, 1>},
-    {9, 4, kernels::pssfp_kernel<9, 4>, kernels::pssfp_queue_kernel<9, 4>},
-    {5, 8, kernels::pssfp_kernel<5, 8>, kernels::pssfp_queue_kernel<5, 8>},
-    {3, 16, kernels::pssfp_kernel<3, 16>, kernels::pssfp_queue_kernel<3, 16>},
-    {2, 32, kernels::pssfp_kernel<2, 32>, kernels::pssfp_queue_kernel<2, 32>},
-    {1, 32, kernels::pssfp_kernel<1, 32>, kernels::pssfp_queue_kernel<1, 32>},
-    {18, 2, kernels::pssfp_kernel<18, 2>, kernels::pssfp_queue_kernel<18, 2>},
-    {4, 4, kernels::pssfp_kernel<4, 4>, kernels::pssfp_queue_kernel<4, 4>},
-    {8, 4, kernels::pssfp_kernel<8, 4>, kernels::pssfp_queue_kernel<8, 4>},
-    {4, 8, kernels::pssfp_kernel<4, 8>, kernels::pssfp_queue_kernel<4, 8>},
-    {12, 4, kernels::pssfp_kernel<12, 4>, kernels::pssfp_queue_kernel<12, 4>},
+    {1, 1, kernels::pssfp_kernel<1, 1>, kernels::pssfp_queue_kernel<1, 1>,
+     kernels::pssfp_tangent_kernel<1, 1>},
+    {2, 1, kernels::pssfp_kernel<2, 1>, kernels::pssfp_queue_kernel<2, 1>,
+     kernels::pssfp_tangent_kernel<2, 1>},
+    {4, 1, kernels::pssfp_kernel<4, 1>, kernels::pssfp_queue_kernel<4, 1>,
+     kernels::pssfp_tangent_kernel<4, 1>},
+    {8, 1, kernels::pssfp_kernel<8, 1>, kernels::pssfp_queue_kernel<8, 1>,
+     kernels::pssfp_tangent_kernel<8, 1>},
+    {9, 4, kernels::pssfp_kernel<9, 4>, kernels::pssfp_queue_kernel<9, 4>,
+     kernels::pssfp_tangent_kernel<9, 4>},
+    {5, 8, kernels::pssfp_kernel<5, 8>, kernels::pssfp_queue_kernel<5, 8>,
+     kernels::pssfp_tangent_kernel<5, 8>},
+    {3, 16, kernels::pssfp_kernel<3, 16>, kernels::pssfp_queue_kernel<3, 16>,
+     kernels::pssfp_tangent_kernel<3, 16>},
+    {2, 32, kernels::pssfp_kernel<2, 32>, kernels::pssfp_queue_kernel<2, 32>,
+     kernels::pssfp_tangent_kernel<2, 32>},
+    {1, 32, kernels::pssfp_kernel<1, 32>, kernels::pssfp_queue_kernel<1, 32>,
+     kernels::pssfp_tangent_kernel<1, 32>},
+    {18, 2, kernels::pssfp_kernel<18, 2>, kernels::pssfp_queue_kernel<18, 2>,
+     kernels::pssfp_tangent_kernel<18, 2>},
+    {4, 4, kernels::pssfp_kernel<4, 4>, kernels::pssfp_queue_kernel<4, 4>,
+     kernels::pssfp_tangent_kernel<4, 4>},
+    {8, 4, kernels::pssfp_kernel<8, 4>, kernels::pssfp_queue_kernel<8, 4>,
+     kernels::pssfp_tangent_kernel<8, 4>},
+    {4, 8, kernels::pssfp_kernel<4, 8>, kernels::pssfp_queue_kernel<4, 8>,
+     kernels::pssfp_tangent_kernel<4, 8>},
+    {12, 4, kernels::pssfp_kernel<12, 4>, kernels::pssfp_queue_kernel<12, 4>,
+     kernels::pssfp_tangent_kernel<12, 4>},
 };
 }  // namespace
 
@@ -318,6 +414,7 @@ kernels::PssfpArgs pssfp_args(const CompasContext& ctx, const TissueParameters& 
     a.gz_pr = seq.gamma_dt_GRz.pr;
     a.echo = reinterpret_cast<float2*>(echo);
     a.echo_stride = echo_stride;
+    a.dT1 = a.dT2 = nullptr;
     return a;
 }
 
@@ -360,6 +457,35 @@ void launch_pssfp_queue(cudaStream_t stream, int device, PssfpLaunch L, int nz, 
     const int grid = std::max(1, std::min(nitems, std::max(1, per_sm) * sms));
     cfg.queue<<<grid, kPssfpThreads, 0, stream>>>(jobs, items, nitems, head);
     check_launch("pssfp_queue_kernel");
+}
+
+// Value and T1/T2 tangents in one launch, with the value kernel's layout L.
+void launch_pssfp_tangent(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
+                          const pSSFPSequence& seq, cfloat* echo, cfloat* dT1, cfloat* dT2, int64_t echo_stride,
+                          PssfpLaunch L) {
+    const int nz = int(seq.z.size());
+    kernels::PssfpArgs a = pssfp_args(ctx, params, voxel_begin, nvoxels, seq, echo, echo_stride);
+    if (nvoxels <= 0) return;
+    if (L.config < 0) L = pssfp_default_launch(nz, nvoxels);
+    const auto& cfg = checked_config(L, nz);
+    a.dT1 = reinterpret_cast<float2*>(dT1);
+    a.dT2 = reinterpret_cast<float2*>(dT2);
+    const int64_t total = int64_t(nvoxels) * cfg.GZ;
+    DeviceGuard guard(ctx.device());
+    cfg.tangent<<<unsigned((total + kPssfpThreads - 1) / kPssfpThreads), kPssfpThreads, 0, ctx.stream()>>>(a);
+    check_launch("pssfp_tangent_kernel");
+}
+
+MagnetizationTangents simulate_magnetization_tangents(const CompasContext& context, TissueParameters parameters,
+                                                      pSSFPSequence sequence) {
+    const int nTR = int(sequence.RF_train.size());
+    const int nvoxels = parameters.nvoxels;
+    MagnetizationTangents out {{{nTR, nvoxels}, context.device(), context.stream()},
+                               {{nTR, nvoxels}, context.device(), context.stream()},
+                               {{nTR, nvoxels}, context.device(), context.stream()}};
+    launch_pssfp_tangent(context, parameters, 0, nvoxels, sequence, out.echos.data(), out.dT1.data(), out.dT2.data(),
+                         nvoxels, tuned_pssfp_launch(int(sequence.z.size()), nvoxels));
+    return out;
 }
 
 Array<cfloat, 2> simulate_magnetization(const CompasContext& context, TissueParameters parameters,

@@ -23,7 +23,7 @@
 namespace compas {
 
 namespace {
-std::atomic<int> g_fisp_cfg {-1}, g_fisp_warps {-1}, g_pssfp_cfg {-1};
+std::atomic<int> g_fisp_cfg {-1}, g_fisp_warps {-1}, g_pssfp_cfg {-1}, g_fisp_tangent_cfg {-1};
 
 struct Table {
     std::map<std::tuple<int, int, int>, std::pair<int, int>> fisp;  // (N, vbucket, pbucket) -> (cfg, warps)
@@ -68,6 +68,21 @@ void set_fisp_override(int config, int warps) {
     if (config >= fisp_config_count()) COMPAS_ERROR("FISP layout index out of range");
     g_fisp_cfg = config;
     g_fisp_warps = warps;
+}
+
+void set_fisp_tangent_override(int config) {
+    if (config >= fisp_tangent_config_count()) COMPAS_ERROR("FISP tangent layout index out of range");
+    g_fisp_tangent_cfg = config;
+}
+
+// Tangent layout: the override when it covers N states, else the default; the warps per CTA are
+// always the value kernel's, so the value sums the positions in the same order.
+FispLaunch tuned_fisp_tangent_launch(int N, int64_t nvoxels, int P) {
+    FispLaunch d = fisp_tangent_default_launch(N, nvoxels, P);
+    const int cfg = g_fisp_tangent_cfg.load();
+    int K = 0, G = 0;
+    if (cfg >= 0 && fisp_tangent_config_info(cfg, &K, &G) && K * G >= N) d.config = cfg;
+    return d;
 }
 
 void set_pssfp_override(int config) {

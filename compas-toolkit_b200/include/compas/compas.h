@@ -412,6 +412,18 @@ Array<cfloat, 2> simulate_magnetization_derivative(const CompasContext& context,
                                                    TissueParameters parameters, FISPSequence sequence,
                                                    float delta = DEFAULT_FINITE_DIFFERENCE_DELTA);
 
+// m, ∂m/∂T1 and ∂m/∂T2 in one pass: forward-mode tangents propagated with the state, the
+// Δ → 0 limit of simulate_magnetization_derivative for the fields T1 and T2 without the
+// difference's cancellation error. echos is the value recurrence of simulate_magnetization (equal
+// to FP32 rounding: the compiler may contract a different multiply-add in the two kernels).
+struct MagnetizationTangents {
+    Array<cfloat, 2> echos, dT1, dT2;  // [nreadouts][nvoxels] each
+};
+MagnetizationTangents simulate_magnetization_tangents(const CompasContext& context, TissueParameters parameters,
+                                                      FISPSequence sequence);
+MagnetizationTangents simulate_magnetization_tangents(const CompasContext& context, TissueParameters parameters,
+                                                      pSSFPSequence sequence);
+
 // echo[r][v] · exp(i y_v Im k_start[r])   (compas/trajectories/phase_encoding.h:19-23)
 Array<cfloat, 2> phase_encoding(const CompasContext& ctx, const Array<cfloat, 2>& echos,
                                 const TissueParameters& parameters, const CartesianTrajectory& trajectory);
@@ -574,7 +586,8 @@ class ServeEngine: public Object {
 
 // One Gauss–Newton iteration of MR-STAT parameter fitting, on the device and captured as a CUDA
 // graph on first use (no counterpart in the reference, whose callers chain the operations):
-// simulate m(p), finite-difference ∂m/∂T1 and ∂m/∂T2, s = signal(m), b = y - s, then
+// simulate m(p), ∂m/∂T1 and ∂m/∂T2 (forward differences with step `delta`; delta = 0 takes the
+// exact forward-mode tangents of simulate_magnetization_tangents), s = signal(m), b = y - s, then
 // `cg_iterations` CGLS iterations (one J·d and one Jᴴ·b each) on min ‖J δ - b‖² over real δ in
 // the Jacobian's scaled coordinates (δT1/T1, δT2/T2, δRe ρ, δIm ρ), and the update
 // T1·c(δ0), T2·c(δ1), ρ + δ2 + iδ3 with c(x) = clamp(1 + x, ½, 2). The estimate is a private

@@ -130,6 +130,16 @@ COMPAS_API compas_array* compas_simulate_magnetization_derivative_fisp(const com
  * reference's jl_errorf path is not available. */
 COMPAS_API const char* compas_last_error(void);
 
+/* m, ∂m/∂T1 and ∂m/∂T2 of a FISP or pSSFP sequence in one pass (forward-mode tangents carried
+ * with the state). Replaces the pair compas_simulate_magnetization_derivative_{fisp,pssfp}
+ * (bindings.cpp:376-411; compas/simulate/derivative.h:7-47) for the fields T1 and T2 by their
+ * Δ → 0 limit, and compas_simulate_magnetization_{fisp,pssfp} (bindings.cpp:230-254) for the
+ * value (the same recurrence, equal to FP32 rounding). Writes three new [nreadouts][nvoxels] arrays; returns 0, or -1
+ * with compas_last_error() set. */
+COMPAS_API int compas_b200_simulate_magnetization_tangents(const compas_context* ctx, const compas_object* parameters,
+                                                const compas_object* sequence, compas_array** echos,
+                                                compas_array** delta_echos_T1, compas_array** delta_echos_T2);
+
 /* Explicit-method variants of the signal and Jacobian entry points: `method` takes the
  * reference's enum values SimulateSignalMethod {Naive=0, Direct, MatmulPedantic, Matmul,
  * MatmulFast, MatmulLow} (compas/trajectories/signal.h:14-44) and JacobianComputeMethod
@@ -178,6 +188,11 @@ COMPAS_API int compas_b200_fisp_config_count(void);
 COMPAS_API int compas_b200_fisp_config_info(int index, int* states_per_lane, int* lanes);
 COMPAS_API int compas_b200_pssfp_config_count(void);
 COMPAS_API int compas_b200_pssfp_config_info(int index, int* iso_per_lane, int* lanes);
+/* Layouts of the FISP tangent kernel (compas_b200_simulate_magnetization_tangents); the
+ * override (-1 = built-in choice) applies when it covers the state count. */
+COMPAS_API void compas_b200_set_fisp_tangent_launch(int config);
+COMPAS_API int compas_b200_fisp_tangent_config_count(void);
+COMPAS_API int compas_b200_fisp_tangent_config_info(int index, int* states_per_lane, int* lanes);
 /* The layout a simulation of this shape gets (override, tuning table, or built-in choice). */
 COMPAS_API void compas_b200_fisp_launch_choice(int max_state, int64_t nvoxels, int npositions, int* config,
                                                int* warps);
@@ -203,7 +218,8 @@ COMPAS_API compas_array* compas_b200_batch_echos(const compas_object* batch, int
 COMPAS_API compas_array* compas_b200_batch_signal(const compas_object* batch, int job);
 
 /* One Gauss-Newton iteration of parameter fitting on the device (no counterpart in the
- * reference): simulate, finite-difference dm/dT1 and dm/dT2, signal, residual against `data`
+ * reference): simulate, dm/dT1 and dm/dT2 (forward differences with step `delta`, or, for
+ * delta = 0, exact forward-mode tangents in the simulation pass), signal, residual against `data`
  * ([ncoils][nreadouts][ns] complex), `cg_iterations` CGLS steps of J.v / J^H.v, parameter update.
  * Captured as a CUDA graph on the first graph run. `method` is a JacobianComputeMethod value.
  * The estimate starts as a copy of `parameters`. Released with compas_destroy_object. */

@@ -266,6 +266,24 @@ def cx_eval_f32(op: int, packed: np.ndarray) -> np.ndarray:
     return out
 
 
+def derivative_central(simulate, params, seq, field: int, rel_step: float = 1e-4, vidx=None, **kw):
+    """∂echo/∂params[field] by an FP64 central difference of an oracle simulation (`fisp` or
+    `pssfp`) with a step of rel_step·|p| per voxel (voxels are independent, so all are stepped at
+    once). The reference's derivative is the forward difference with an absolute step
+    (src/simulate/derivative.cu:11-62, derivative_kernels.cuh:6-35); this is its Δ → 0 limit to
+    O(step²), the quantity the tangent kernels compute. The stepped parameters are float32 (the
+    oracle's input type), so the exact float32 difference of the two points divides."""
+    p = _ff(params)
+    step = np.maximum(np.abs(p[field]) * np.float32(rel_step), np.float32(1e-12)).astype(np.float32)
+    hi, lo = p.copy(), p.copy()
+    hi[field] = p[field] + step
+    lo[field] = p[field] - step
+    den = hi[field].astype(np.float64) - lo[field].astype(np.float64)
+    if vidx is not None:
+        den = den[np.asarray(vidx)]
+    return (simulate(hi, seq, vidx=vidx, **kw) - simulate(lo, seq, vidx=vidx, **kw)) / den[None, :]
+
+
 def rel_l2(x, ref) -> float:
     x = np.asarray(x, np.complex128)
     ref = np.asarray(ref, np.complex128)

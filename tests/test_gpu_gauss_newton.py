@@ -1,11 +1,12 @@
 """Gauss-Newton iteration on the device (compas_b200_make_gauss_newton / _run).
 
-One iteration simulates m(p), the forward-difference derivatives dm/dT1 and dm/dT2, the signal
-s(p), the residual b = y - s, runs CGLS steps of J·d / Jᴴ·b on min ‖J δ - b‖² and updates the
-parameters. The tests check that (1) the CUDA-graph replay gives the same bits as the eager
-kernel sequence over two iterations, (2) with one CGLS step the step equals α·Re(Jᴴ b) with
-α = ‖g‖²/‖J g‖², recomputed here from the public operations, within the FP32 tolerance of the
-other tests, and (3) fitting data simulated from known parameters lowers the objective.
+One iteration simulates m(p), the derivatives dm/dT1 and dm/dT2 (forward differences, or exact
+tangents for delta = 0), the signal s(p), the residual b = y - s, runs CGLS steps of J·d / Jᴴ·b
+on min ‖J δ - b‖² and updates the parameters. The tests check that (1) the CUDA-graph replay
+gives the same bits as the eager kernel sequence over two iterations, (2) with one CGLS step the
+step equals α·Re(Jᴴ b) with α = ‖g‖²/‖J g‖², recomputed here from the public operations, within
+the FP32 tolerance of the other tests, (3) fitting data simulated from known parameters lowers the
+objective, and (4) the same with exact derivatives, which equal simulate_magnetization_tangents.
 """
 import numpy as np
 import pytest
@@ -128,3 +129,31 @@ def test_spiral_iteration_graph_matches_eager_and_lowers_the_objective(setup):
         objs.append(graph.objective())
     assert objs[-1] < objs[0], objs
 
+
+
+@pytest.mark.parametrize("kind", ["fisp", "pssfp"])
+def test_exact_derivative_iteration(setup, kind):
+    # delta = 0: the iteration takes m, ∂m/∂T1, ∂m/∂T2 from one tangent pass
+    cb, ctx, start, seq, traj, coils, y = setup
+    if kind == "pssfp":
+        rng = np.random.default_rng(24)
+        seq = cb.pSSFPSequence.from_dict(ctx, W.pssfp_sequence(rng, 60, nrf=5, nz=6))
+        truth, _, _, _, _ = _problem()
+        p_true = cb.TissueParameters.from_soa(ctx, truth)
+        y = cb.magnetization_to_signal(ctx, cb.simulate_magnetization(ctx, p_true, seq), p_true, traj, coils,
+                                       method="MatmulFast").to_numpy()
+    eager = _gn(cb, ctx, start, seq, traj, coils, y, cg_iterations=3, delta=0.0)
+    graph = _gn(cb, ctx, start, seq, traj, coils, y, cg_iterations=3, delta=0.0)
+    tangents = cb.simulate_magnetization_tangents(ctx, cb.TissueParameters.from_soa(ctx, start), seq)
+    objs = []
+    for it in range(3):
+        eager.run(graph=False)
+        graph.run(graph=True)
+        ctx.synchronize()
+        if it == 0:
+            for name, key in (("echos", "echos"), ("dT1", "T1"), ("dT2", "T2")):
+                assert np.array_equal(graph.array(name).to_numpy(), tangents[key].to_numpy()), name
+        for name in ("parameters", "echos", "dT1", "dT2", "signal", "gradient", "step", "scalars"):
+            assert np.array_equal(eager.array(name).to_numpy(), graph.array(name).to_numpy()), (it, name)
+        objs.append(graph.objective())
+    assert objs[-1] < 0.5 * objs[0], objs

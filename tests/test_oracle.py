@@ -75,6 +75,39 @@ def test_fisp_relaxation_after_inversion(oracle, workloads):
     assert abs(e - want) < 1e-9
 
 
+def test_derivative_central_known_answer(oracle, workloads):
+    # the readout above, e = -i sinα (1 - 2 e^{-TI/T1}) e^{-TE/T2}, differentiated in closed form:
+    # ∂e/∂T1 = -i sinα (-2 e^{-TI/T1} TI/T1²) e^{-TE/T2},  ∂e/∂T2 = e·TE/T2²
+    T1, T2, TI, TE, a = 1.1, 0.09, 0.4, 3e-3, 1e-3
+    seq = workloads.fisp_sequence(np.array([a]), np.ones((1, 1)), 8e-3, TE, TI, 3)
+    p = _one_voxel(T1=T1, T2=T2)
+    f = lambda q: float(np.float32(q))
+    sa, E2 = np.sin(np.deg2rad(f(a))), np.exp(-f(TE) / f(T2))
+    e = -1j * sa * (1 - 2 * np.exp(-f(TI) / f(T1))) * E2
+    d1 = -1j * sa * (-2 * np.exp(-f(TI) / f(T1)) * f(TI) / f(T1) ** 2) * E2
+    d2 = e * f(TE) / f(T2) ** 2
+    got1 = oracle.derivative_central(oracle.fisp, p, seq, 0)[0, 0]
+    got2 = oracle.derivative_central(oracle.fisp, p, seq, 1)[0, 0]
+    # O(step²) truncation at a relative step of 1e-4
+    assert abs(got1 - d1) < 1e-7 * abs(d1) and abs(got2 - d2) < 1e-7 * abs(d2)
+
+
+@pytest.mark.parametrize("kind", ["fisp", "pssfp"])
+def test_derivative_central_converges(oracle, workloads, kind):
+    # central differences at two steps agree to O(step²): the FP64 derivative oracle has converged
+    rng = np.random.default_rng(9)
+    if kind == "fisp":
+        w = workloads.tiny(n_side=3, ntr=31, P=2, max_state=6)
+        p, seqd, sim = w["params"], w["seq"], oracle.fisp
+    else:
+        seqd = workloads.pssfp_sequence(rng, 19, nrf=5, nz=6)
+        p, sim = workloads.tissue(rng, 3, 20.0), oracle.pssfp
+    for field in (0, 1):
+        coarse = oracle.derivative_central(sim, p, seqd, field, rel_step=1e-3)
+        fine = oracle.derivative_central(sim, p, seqd, field, rel_step=1e-4)
+        assert oracle.rel_l2(coarse, fine) < 1e-5, field
+
+
 def test_fisp_b0_conjugate_symmetry(oracle, workloads):
     # real RF: the EPG evolution under -B0 is D·conj(evolution under +B0) with D = diag(-1,-1,1)
     w = workloads.tiny()
