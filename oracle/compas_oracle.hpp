@@ -10,13 +10,15 @@
 // twin" that follows the reference's formulas and operation order in FP32.
 //
 // Each function cites the reference file:line it restates. Parity status: the
-// reference ships no golden vectors and cannot be built here (its `kmm` runtime
-// submodule is absent, there is no GPU and no Julia). The oracle is pinned by
-// (a) golden vectors produced by the reference's own host-compilable
-// `compas/core/complex_type.h` (see oracle/ref_golden.cpp), (b) analytic
-// known-answer tests and (c) structural identities (adjointness of J and Jᴴ,
-// finite differences, undersampling replication). Everything beyond that is
-// "parity unpinned" against the reference's own outputs.
+// reference ships no golden vectors and cannot be built as shipped (its `kmm`
+// runtime submodule is absent, there is no Julia). The oracle is pinned by
+// (a) golden vectors from the reference's own code built for the host: the
+// complex primitives of `compas/core/complex_type.h` (oracle/ref_golden.cpp)
+// and the FISP / pSSFP simulation kernels run one thread at a time
+// (oracle/ref_sim.cpp), which the FP64 simulation matches to FP32 rounding;
+// (b) analytic known-answer tests and (c) structural identities (adjointness
+// of J and Jᴴ, finite differences, undersampling replication). The signal and
+// Jacobian formulas are pinned by (b) and (c) only.
 #pragma once
 
 #include <cmath>

@@ -1,0 +1,83 @@
+// Host stand-in for the kmm view types that compas-toolkit's include/compas/core/view.h aliases.
+// TEST INFRASTRUCTURE ONLY: enough for oracle/ref_sim.cpp to compile the reference's simulation
+// kernels for the host (element access, row access, size, drop_axis). Not the kmm library.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <type_traits>
+
+#include "kmm/utils/geometry.hpp"
+
+namespace kmm {
+
+// rank-N view over strided host memory (strides in elements)
+template<typename T, size_t N = 1>
+struct View {
+    T* ptr = nullptr;
+    int64_t ext[N] = {};
+    int64_t str[N] = {};
+
+    T* data() const { return ptr; }
+
+    int64_t size(size_t axis) const { return ext[axis]; }
+    int64_t size() const {
+        int64_t n = 1;
+        for (size_t i = 0; i < N; i++) n *= ext[i];
+        return n;
+    }
+
+    // view without axis A at index i
+    template<size_t A = 0, size_t M = N, std::enable_if_t<(M >= 2), int> = 0>
+    View<T, N - 1> drop_axis(int64_t i) const {
+        View<T, N - 1> v;
+        v.ptr = ptr + i * str[A];
+        for (size_t a = 0, b = 0; a < N; a++) {
+            if (a == A) continue;
+            v.ext[b] = ext[a];
+            v.str[b] = str[a];
+            b++;
+        }
+        return v;
+    }
+
+    decltype(auto) operator[](int64_t i) const {
+        if constexpr (N == 1) {
+            return static_cast<T&>(ptr[i * str[0]]);
+        } else {
+            return drop_axis<0>(i);
+        }
+    }
+};
+
+template<typename T, size_t N = 1> using ViewMut = View<T, N>;
+template<typename T, size_t N = 1> using ViewStrided = View<T, N>;
+template<typename T, size_t N = 1> using ViewStridedMut = View<T, N>;
+template<typename T, size_t N = 1> using Subview = View<T, N>;
+template<typename T, size_t N = 1> using SubviewMut = View<T, N>;
+template<typename T, size_t N = 1> using SubviewStrided = View<T, N>;
+template<typename T, size_t N = 1> using SubviewStridedMut = View<T, N>;
+template<typename T, size_t N = 1> using GPUView = View<T, N>;
+template<typename T, size_t N = 1> using GPUViewMut = View<T, N>;
+template<typename T, size_t N = 1> using GPUViewStrided = View<T, N>;
+template<typename T, size_t N = 1> using GPUViewStridedMut = View<T, N>;
+template<typename T, size_t N = 1> using GPUSubview = View<T, N>;
+template<typename T, size_t N = 1> using GPUSubviewMut = View<T, N>;
+template<typename T, size_t N = 1> using GPUSubviewStrided = View<T, N>;
+template<typename T, size_t N = 1> using GPUSubviewStridedMut = View<T, N>;
+
+// contiguous row-major view of a host buffer
+template<typename T, typename... I>
+View<T, sizeof...(I)> host_view(T* data, I... extents) {
+    View<T, sizeof...(I)> v;
+    v.ptr = data;
+    const int64_t e[] = {int64_t(extents)...};
+    int64_t s = 1;
+    for (size_t a = sizeof...(I); a-- > 0;) {
+        v.ext[a] = e[a];
+        v.str[a] = s;
+        s *= e[a];
+    }
+    return v;
+}
+
+}  // namespace kmm

@@ -44,3 +44,38 @@ def workloads():
     import workloads as w
 
     return w
+
+
+@pytest.fixture(scope="session")
+def ref_simulations():
+    """Seeded FISP and pSSFP cases with echoes computed by the reference's own simulation kernels
+    on the CPU (tests/golden/ref_simulations.json, made by tests/golden/make_golden.py). Each case
+    is (params float32 [9][nv], sequence dict in the oracle's / workloads' format, echoes complex128
+    [nreadouts][nv])."""
+    import json
+
+    import numpy as np
+
+    data = json.loads((ROOT / "tests" / "golden" / "ref_simulations.json").read_text())
+
+    def cx(a):
+        a = np.asarray(a, np.float64)
+        return a[0::2] + 1j * a[1::2]
+
+    out = {"fisp": [], "pssfp": []}
+    for c in data["fisp"]:
+        nv, ntr, P = c["nv"], c["nTR"], c["P"]
+        seq = {"rf": cx(c["rf"]).astype(np.complex64),
+               "slices": cx(c["slices"]).reshape(P, ntr).astype(np.complex64),
+               "TR": c["TR"], "TE": c["TE"], "TI": c["TI"], "TW": c["TW"], "max_state": c["max_state"],
+               "uf": c["uf"], "reps": c["reps"], "inversion": c["inversion"], "wait_spoil": c["wait_spoil"]}
+        out["fisp"].append((np.array(c["params"], np.float32).reshape(9, nv), seq,
+                            cx(c["echos"]).reshape(ntr * c["uf"], nv)))
+    for c in data["pssfp"]:
+        nv, ntr = c["nv"], c["nTR"]
+        seq = {"rf": cx(c["rf"]).astype(np.complex64), "TR": c["TR"],
+               "gdtrf": cx(c["gamma_dt_RF"]).astype(np.complex64), "dt": tuple(c["dt"]),
+               "gz": tuple(c["gamma_dt_GRz"]), "z": np.array(c["z"], np.float32)}
+        out["pssfp"].append((np.array(c["params"], np.float32).reshape(9, nv), seq,
+                             cx(c["echos"]).reshape(ntr, nv)))
+    return out

@@ -1,8 +1,11 @@
-"""Regenerate tests/golden/ref_complex_ops.json from the reference's own code.
+"""Regenerate the golden fixtures from the reference's own code.
 
-Builds oracle/_ref/ref_golden (oracle/Makefile target `ref`, which compiles
-oracle/ref_golden.cpp against the reference's include tree, by default
-/root/reference/include) and stores its JSON output next to this script.
+Builds oracle/_ref/ref_golden and oracle/_ref/ref_sim (oracle/Makefile target `ref`, which
+compiles oracle/ref_golden.cpp and oracle/ref_sim.cpp against the reference's include and src
+trees, by default under /root/reference) and stores their JSON output next to this script:
+  * ref_complex_ops.json  — complex_type.h primitives (FP32);
+  * ref_simulations.json  — inputs and echoes of seeded FISP and pSSFP cases from the reference's
+                            simulation kernels run one thread at a time on the CPU.
 Run from the repository root:  python tests/golden/make_golden.py
 """
 import json
@@ -21,6 +24,15 @@ def main() -> int:
                        "fma :174-178, operator* :220-223), FP32, host build by oracle/Makefile `ref`")
     (Path(__file__).parent / "ref_complex_ops.json").write_text(json.dumps(data, indent=0))
     print("wrote", {k: len(v) for k, v in data.items() if isinstance(v, list)})
+
+    out = subprocess.run([str(ROOT / "oracle" / "_ref" / "ref_sim")], check=True, capture_output=True, text=True)
+    sims = json.loads(out.stdout)
+    sims["_source"] = ("compas-toolkit src/simulate/fisp_kernels.cuh (simulate_fisp, expand_undersampled_echos), "
+                       "src/simulate/pssfp_kernels.cuh (simulate_pssfp) with src/operators/epg.cuh and "
+                       "isochromat.cuh, FP32, run per voxel with a warp size of 1 on the host (oracle/ref_sim.cpp); "
+                       "fast-math intrinsics replaced by libm")
+    (Path(__file__).parent / "ref_simulations.json").write_text(json.dumps(sims))
+    print("wrote", {k: len(v) for k, v in sims.items() if isinstance(v, list)})
     return 0
 
 

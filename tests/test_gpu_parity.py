@@ -120,6 +120,26 @@ def test_fisp_rejects_bad_state_count(cb, ctx, workloads):
 
 
 # ------------------------------------------------------------------------------------------------
+# against the reference's own kernels
+# ------------------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("kind", ["fisp", "pssfp"])
+def test_simulation_matches_reference_kernels(cb, ctx, ref_simulations, oracle, kind):
+    # golden echoes of the reference's FISP / pSSFP kernels (run on the CPU in FP32); both FP32
+    # results lie within 1e-5 of the FP64 oracle, so they agree to 2e-5. The C ABI's FISP sequence
+    # always has the inversion prepulse and wait spoiling, so cases without them are skipped here.
+    tried = 0
+    for i, (p, seq, echos) in enumerate(ref_simulations[kind]):
+        if kind == "fisp" and not (seq["inversion"] and seq["wait_spoil"]):
+            continue
+        s = (cb.FispSequence if kind == "fisp" else cb.pSSFPSequence).from_dict(ctx, seq)
+        got = cb.simulate_magnetization(ctx, cb.TissueParameters.from_soa(ctx, p), s).to_numpy()
+        assert oracle.rel_l2(got, echos) < 2e-5, (kind, i)
+        tried += 1
+    assert tried >= 3
+
+
+# ------------------------------------------------------------------------------------------------
 # pSSFP
 # ------------------------------------------------------------------------------------------------
 

@@ -43,6 +43,16 @@ def _one_voxel(T1=0.8, T2=0.06, B1=1.0, B0=0.0, rho=1.0, x=0.0, y=0.0, z=0.0):
     return p
 
 
+@pytest.mark.parametrize("kind", ["fisp", "pssfp"])
+def test_oracle_matches_reference_kernels(oracle, ref_simulations, kind):
+    # echoes of the reference's own FISP / pSSFP kernels (run on the CPU, FP32): the FP64 oracle
+    # agrees to FP32 rounding, the FP32 twin (the reference's arithmetic order) to ~1e-7
+    sim = oracle.fisp if kind == "fisp" else oracle.pssfp
+    for i, (p, seq, echos) in enumerate(ref_simulations[kind]):
+        assert oracle.rel_l2(sim(p, seq), echos) < 1e-5, (kind, i)
+        assert oracle.rel_l2(sim(p, seq, dtype="f32"), echos) < 1e-6, (kind, i)
+
+
 def test_fisp_zero_rf_gives_zero_echo(oracle, workloads):
     seq = workloads.fisp_sequence(np.zeros(20), np.ones((2, 20)), 8e-3, 4e-3, 20e-3, 6)
     e = oracle.fisp(_one_voxel(), seq)
