@@ -14,11 +14,11 @@
 // runtime submodule is absent, there is no Julia). The oracle is pinned by
 // (a) golden vectors from the reference's own code built for the host: the
 // complex primitives of `compas/core/complex_type.h` (oracle/ref_golden.cpp)
-// and the FISP / pSSFP simulation kernels run one thread at a time
-// (oracle/ref_sim.cpp), which the FP64 simulation matches to FP32 rounding;
-// (b) analytic known-answer tests and (c) structural identities (adjointness
-// of J and Jᴴ, finite differences, undersampling replication). The signal and
-// Jacobian formulas are pinned by (b) and (c) only.
+// and its FISP / pSSFP simulation, phase-encoding, signal (Cartesian naive,
+// spiral), Jacobian (naive J·v, Jᴴ·v) and residual kernels run one thread at a
+// time (oracle/ref_sim.cpp), which the FP64 functions here match to FP32
+// rounding; (b) analytic known-answer tests and (c) structural identities
+// (adjointness of J and Jᴴ, finite differences, undersampling replication).
 #pragma once
 
 #include <cmath>

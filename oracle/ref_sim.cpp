@@ -11,17 +11,29 @@
 //    position (the batch-of-1 path of src/simulate/pssfp.cu:16-41).
 // The EPG operators (src/operators/epg.cuh) and the isochromat operators
 // (src/operators/isochromat.cuh) are the reference's; the fast-math intrinsics are exact libm
-// calls (oracle/refshim/cuda_host_shim.h). Prints the inputs and echoes of seeded cases as JSON;
-// tests/golden/make_golden.py stores them as tests/golden/ref_simulations.json.
+// calls (oracle/refshim/cuda_host_shim.h). The signal, Jacobian, phase-encoding and residual
+// kernels run the same way (one thread per output element or voxel) on seeded Cartesian and spiral
+// cases. Prints inputs and outputs as JSON; tests/golden/make_golden.py stores them as
+// tests/golden/ref_simulations.json.
 #include <cstdio>
 #include <random>
 #include <vector>
 
+#include "jacobian/product_kernels.cuh"
 #include "simulate/fisp_kernels.cuh"
 #include "simulate/pssfp_kernels.cuh"
+#include "trajectories/phase_encoding_kernels.cuh"
+#include "trajectories/signal_kernels.cuh"
+#include "utils/residual_kernels.cuh"
 
 using compas::cfloat;
 using kmm::host_view;
+
+// ref_sim_hermitian.cpp (its own translation unit, as in the reference: hermitian_kernels.cuh and
+// product_kernels.cuh both define kernels::compute_sample_decay)
+void run_jacobian_hermitian_naive(int nv, int R, int S, int C, cfloat* jhv, cfloat* echos, cfloat* d1, cfloat* d2,
+                                  float* params, const compas::CartesianTrajectoryView& traj, cfloat* coils,
+                                  cfloat* u);
 
 namespace {
 
@@ -188,6 +200,142 @@ void pssfp_case(const PssfpCase& c, bool last) {
     std::printf("}%s\n", last ? "" : ",");
 }
 
+std::vector<cfloat> random_complex(size_t n) {
+    std::vector<cfloat> a(n);
+    for (auto& x : a) x = cfloat(uniform(-1.0f, 1.0f), uniform(-1.0f, 1.0f));
+    return a;
+}
+
+// one thread per launch over the grid (gx, gy, gz), as blockIdx with blockDim 1
+template<typename F>
+void launch_grid(int gx, int gy, int gz, F&& kernel) {
+    for (int k = 0; k < gz; k++)
+        for (int j = 0; j < gy; j++)
+            for (int i = 0; i < gx; i++) {
+                blockDim = {1, 1, 1};
+                gridDim = {unsigned(gx), unsigned(gy), unsigned(gz)};
+                blockIdx = {unsigned(i), unsigned(j), unsigned(k)};
+                threadIdx = {0, 0, 0};
+                kernel();
+            }
+}
+
+// Cartesian trajectory: phase encoding (phase_encoding_kernels.cuh:10-25), the naive signal
+// (signal_kernels.cuh:137-167), J·v (product_kernels.cuh:7-66) and Jᴴ·v
+// (hermitian_kernels.cuh:30-92), the residual (residual_kernels.cuh, one-thread blocks)
+void cartesian_case(int nv, int R, int S, int C) {
+    std::vector<float> p = tissue(nv);
+    const float fov = 0.2f, dk = 2.0f * float(M_PI) / fov, dt = 1e-5f;
+    std::vector<cfloat> k_start(R);
+    for (int r = 0; r < R; r++) k_start[r] = cfloat(-0.5f * S * dk, float(r % R - R / 2) * dk);
+    auto echos = random_complex(size_t(R) * nv), d1 = random_complex(size_t(R) * nv),
+         d2 = random_complex(size_t(R) * nv), coils = random_complex(size_t(C) * nv),
+         v = random_complex(size_t(4) * nv), u = random_complex(size_t(C) * R * S),
+         rhs = random_complex(size_t(C) * R * S);
+
+    compas::CartesianTrajectoryView traj;
+    traj.nreadouts = R;
+    traj.samples_per_readout = S;
+    traj.delta_t = dt;
+    traj.k_start = host_view(k_start.data(), R);
+    traj.delta_k = cfloat(dk, 0.0f);  // the C ABI takes a real Δk (julia-bindings/src/bindings.cpp:198-212)
+    const auto pv = params_view(p, nv);
+    auto ev = host_view(echos.data(), R, nv), d1v = host_view(d1.data(), R, nv), d2v = host_view(d2.data(), R, nv);
+    auto cv = host_view(coils.data(), C, nv);
+
+    std::vector<cfloat> ph(size_t(R) * nv), signal(size_t(C) * R * S), jv(size_t(C) * R * S), jhv(size_t(4) * nv);
+    launch_grid(nv, R, 1, [&] {
+        compas::kernels::phase_encoding(kmm::Bounds<2, int> {{0, nv}, {0, R}, {}}, host_view(ph.data(), R, nv), ev,
+                                        pv, traj);
+    });
+    launch_grid(S, R, C, [&] {
+        compas::kernels::sum_signal_cartesian_naive(kmm::Range<int> {0, nv}, host_view(signal.data(), C, R, S), ev,
+                                                    pv, traj, cv);
+    });
+    for (int c = 0; c < C; c++)
+        launch_grid(S, R, 1, [&] {
+            compas::kernels::jacobian_product_naive(kmm::Range<int> {0, nv}, c, R, S, host_view(jv.data(), C, R, S),
+                                                    ev, d1v, d2v, pv, traj, cv, host_view(v.data(), 4, nv));
+        });
+    run_jacobian_hermitian_naive(nv, R, S, C, jhv.data(), echos.data(), d1.data(), d2.data(), p.data(), traj,
+                                 coils.data(), u.data());
+    const int n = C * R * S;
+    std::vector<cfloat> diff(n);
+    std::vector<float> partial(1), objective(1);
+    launch_grid(1, 1, 1, [&] {
+        compas::kernels::calculate_elementwise_difference<1>(kmm::Range<int> {0, n}, signal.data(), rhs.data(),
+                                                             diff.data(), host_view(partial.data(), 1));
+    });
+    launch_grid(1, 1, 1, [&] {
+        compas::kernels::accumulate_partial_sums<1>(host_view(partial.data(), 1), host_view(objective.data(), 1));
+    });
+
+    std::printf("{\"nv\": %d, \"R\": %d, \"S\": %d, \"C\": %d, \"dt\": %.9g, \"dk\": %.9g,\n", nv, R, S, C, dt,
+                dk);
+    print_floats("params", p);
+    print_complex("k_start", k_start);
+    print_complex("echos", echos);
+    print_complex("dT1", d1);
+    print_complex("dT2", d2);
+    print_complex("coils", coils);
+    print_complex("v", v);
+    print_complex("u", u);
+    print_complex("rhs", rhs);
+    print_complex("phase_encoded", ph);
+    print_complex("signal", signal);
+    print_complex("jv", jv);
+    print_complex("jhv", jhv);
+    print_complex("residual", diff);
+    std::printf("\"objective\": %.9g}\n", objective[0]);
+}
+
+// spiral trajectory: prepare_readout_echos, prepare_sample_decay_spiral and sum_signal_spiral
+// (signal_kernels.cuh:12-30, 93-105, 274-345) in the host code's order (signal.cu:197-236),
+// with one-thread cooperative groups
+void spiral_case(int nv, int R, int S, int C) {
+    std::vector<float> p = tissue(nv);
+    const float fov = 0.2f, dt = 4e-6f;
+    std::vector<cfloat> k_start(R), delta_k(R);
+    for (int r = 0; r < R; r++) {
+        const float a = 2.0f * float(M_PI) * r / R;
+        k_start[r] = cfloat(std::cos(a), std::sin(a)) * (2.0f * float(M_PI) / fov);
+        delta_k[r] = cfloat(-std::sin(a), std::cos(a)) * (0.5f * float(M_PI) / fov);
+    }
+    auto echos = random_complex(size_t(R) * nv), coils = random_complex(size_t(C) * nv);
+    compas::SpiralTrajectoryView traj;
+    traj.nreadouts = R;
+    traj.samples_per_readout = S;
+    traj.delta_t = dt;
+    traj.k_start = host_view(k_start.data(), R);
+    traj.delta_k = host_view(delta_k.data(), R);
+    const auto pv = params_view(p, nv);
+
+    std::vector<cfloat> readout_echos(size_t(R) * nv), decay(size_t(R) * nv), signal(size_t(C) * R * S);
+    launch_grid(nv, R, 1, [&] {
+        compas::kernels::prepare_readout_echos(kmm::Range<int> {0, nv}, kmm::Range<int> {0, R},
+                                               host_view(readout_echos.data(), R, nv),
+                                               host_view(echos.data(), R, nv), pv, traj);
+    });
+    launch_grid(nv, R, 1, [&] {
+        compas::kernels::prepare_sample_decay_spiral(host_view(decay.data(), R, nv), pv, traj);
+    });
+    launch_grid(S, R, C, [&] {
+        compas::kernels::sum_signal_spiral<1, 1, 1, 1>(host_view(signal.data(), C, R, S),
+                                                      host_view(decay.data(), R, nv),
+                                                      host_view(readout_echos.data(), R, nv),
+                                                      host_view(coils.data(), C, nv));
+    });
+
+    std::printf("{\"nv\": %d, \"R\": %d, \"S\": %d, \"C\": %d, \"dt\": %.9g,\n", nv, R, S, C, dt);
+    print_floats("params", p);
+    print_complex("k_start", k_start);
+    print_complex("delta_k", delta_k);
+    print_complex("echos", echos);
+    print_complex("coils", coils);
+    print_complex("signal", signal, true);
+    std::printf("}\n");
+}
+
 }  // namespace
 
 int main() {
@@ -200,6 +348,10 @@ int main() {
     pssfp_case({6, 30, 5, 7, 10.0f, 60.0f}, false);
     pssfp_case({5, 25, 15, 35, 10.0f, 60.0f}, false);
     pssfp_case({4, 20, 3, 9, 120.0f, 180.0f}, true);
-    std::printf("]}\n");
+    std::printf("],\n\"cartesian\": ");
+    cartesian_case(12, 10, 8, 3);
+    std::printf(",\n\"spiral\": ");
+    spiral_case(10, 6, 12, 2);
+    std::printf("}\n");
     return 0;
 }

@@ -7,21 +7,31 @@
 #include <cmath>
 #include <sys/types.h>
 
+#include "kernel_float.h"
+
 struct compas_ref_dim3 {
     unsigned x = 0, y = 0, z = 0;
 };
 inline compas_ref_dim3 threadIdx, blockIdx, blockDim {1, 1, 1}, gridDim {1, 1, 1};
 
 #define __global__
+#define __device__
 #define __shared__ static
 #define __launch_bounds__(...)
 #define KMM_ASSUME(expr) ((void)0)
+#define __builtin_assume(expr) ((void)0)
+
+// CUDA's global min / max
+#include <algorithm>
+using std::max;
+using std::min;
 
 struct float2 {
     float x, y;
 };
 
 inline void __syncwarp() {}
+inline void __syncthreads() {}
 
 // Warp shuffles for a warp size of 1 (the only one these host launches use): the source lane
 // is always outside the one-lane segment, so a shuffle returns the caller's own value. The

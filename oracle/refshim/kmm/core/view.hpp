@@ -2,6 +2,7 @@
 // TEST INFRASTRUCTURE ONLY: enough for oracle/ref_sim.cpp to compile the reference's simulation
 // kernels for the host (element access, row access, size, drop_axis). Not the kmm library.
 #pragma once
+#include <array>
 #include <cstddef>
 #include <cstdint>
 #include <type_traits>
@@ -38,6 +39,20 @@ struct View {
             b++;
         }
         return v;
+    }
+
+    template<typename... I>
+    bool in_bounds(I... index) const {
+        static_assert(sizeof...(I) == N);
+        const int64_t i[] = {int64_t(index)...};
+        for (size_t a = 0; a < N; a++)
+            if (i[a] < 0 || i[a] >= ext[a]) return false;
+        return true;
+    }
+    bool in_bounds(const std::array<int64_t, N>& i) const {
+        for (size_t a = 0; a < N; a++)
+            if (i[a] < 0 || i[a] >= ext[a]) return false;
+        return true;
     }
 
     decltype(auto) operator[](int64_t i) const {

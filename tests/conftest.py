@@ -48,10 +48,11 @@ def workloads():
 
 @pytest.fixture(scope="session")
 def ref_simulations():
-    """Seeded FISP and pSSFP cases with echoes computed by the reference's own simulation kernels
-    on the CPU (tests/golden/ref_simulations.json, made by tests/golden/make_golden.py). Each case
-    is (params float32 [9][nv], sequence dict in the oracle's / workloads' format, echoes complex128
-    [nreadouts][nv])."""
+    """Seeded cases computed by the reference's own kernels on the CPU
+    (tests/golden/ref_simulations.json, made by tests/golden/make_golden.py). "fisp" / "pssfp":
+    lists of (params float32 [9][nv], sequence dict in the oracle's / workloads' format, echoes
+    complex128 [nreadouts][nv]); "cartesian" / "spiral": one dict each with the inputs (complex64,
+    the library's layouts) and the reference's outputs (complex128)."""
     import json
 
     import numpy as np
@@ -62,7 +63,7 @@ def ref_simulations():
         a = np.asarray(a, np.float64)
         return a[0::2] + 1j * a[1::2]
 
-    out = {"fisp": [], "pssfp": []}
+    out = {"fisp": [], "pssfp": [], "cartesian": None, "spiral": None}
     for c in data["fisp"]:
         nv, ntr, P = c["nv"], c["nTR"], c["P"]
         seq = {"rf": cx(c["rf"]).astype(np.complex64),
@@ -78,4 +79,24 @@ def ref_simulations():
                "gz": tuple(c["gamma_dt_GRz"]), "z": np.array(c["z"], np.float32)}
         out["pssfp"].append((np.array(c["params"], np.float32).reshape(9, nv), seq,
                              cx(c["echos"]).reshape(ntr, nv)))
+    # Cartesian and spiral operator cases: inputs in the library's / oracle's layouts, complex64
+    c = data["cartesian"]
+    nv, R, S, C = c["nv"], c["R"], c["S"], c["C"]
+    f32 = lambda key, *shape: cx(c[key]).reshape(shape).astype(np.complex64)  # noqa: E731
+    out["cartesian"] = {
+        "params": np.array(c["params"], np.float32).reshape(9, nv),
+        "traj": {"kind": "cartesian", "nr": R, "ns": S, "dt": c["dt"], "k_start": f32("k_start", R),
+                 "dk": c["dk"]},
+        "echos": f32("echos", R, nv), "dT1": f32("dT1", R, nv), "dT2": f32("dT2", R, nv),
+        "coils": f32("coils", C, nv), "v": f32("v", 4, nv), "u": f32("u", C, R, S), "rhs": f32("rhs", C, R, S),
+        "phase_encoded": cx(c["phase_encoded"]).reshape(R, nv), "signal": cx(c["signal"]).reshape(C, R, S),
+        "jv": cx(c["jv"]).reshape(C, R, S), "jhv": cx(c["jhv"]).reshape(4, nv),
+        "residual": cx(c["residual"]).reshape(C, R, S), "objective": float(c["objective"])}
+    c = data["spiral"]
+    nv, R, S, C = c["nv"], c["R"], c["S"], c["C"]
+    out["spiral"] = {
+        "params": np.array(c["params"], np.float32).reshape(9, nv),
+        "traj": {"kind": "spiral", "nr": R, "ns": S, "dt": c["dt"], "k_start": f32("k_start", R),
+                 "dk": f32("delta_k", R)},
+        "echos": f32("echos", R, nv), "coils": f32("coils", C, nv), "signal": cx(c["signal"]).reshape(C, R, S)}
     return out

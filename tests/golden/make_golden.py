@@ -4,8 +4,9 @@ Builds oracle/_ref/ref_golden and oracle/_ref/ref_sim (oracle/Makefile target `r
 compiles oracle/ref_golden.cpp and oracle/ref_sim.cpp against the reference's include and src
 trees, by default under /root/reference) and stores their JSON output next to this script:
   * ref_complex_ops.json  — complex_type.h primitives (FP32);
-  * ref_simulations.json  — inputs and echoes of seeded FISP and pSSFP cases from the reference's
-                            simulation kernels run one thread at a time on the CPU.
+  * ref_simulations.json  — inputs and outputs of seeded FISP, pSSFP, Cartesian (phase encoding,
+                            signal, J·v, Jᴴ·v, residual) and spiral (signal) cases from the
+                            reference's kernels run one thread at a time on the CPU.
 Run from the repository root:  python tests/golden/make_golden.py
 """
 import json
@@ -29,10 +30,14 @@ def main() -> int:
     sims = json.loads(out.stdout)
     sims["_source"] = ("compas-toolkit src/simulate/fisp_kernels.cuh (simulate_fisp, expand_undersampled_echos), "
                        "src/simulate/pssfp_kernels.cuh (simulate_pssfp) with src/operators/epg.cuh and "
-                       "isochromat.cuh, FP32, run per voxel with a warp size of 1 on the host (oracle/ref_sim.cpp); "
+                       "isochromat.cuh; src/trajectories/phase_encoding_kernels.cuh, signal_kernels.cuh "
+                       "(sum_signal_cartesian_naive; prepare_readout_echos, prepare_sample_decay_spiral, "
+                       "sum_signal_spiral), src/jacobian/product_kernels.cuh (jacobian_product_naive), "
+                       "hermitian_kernels.cuh (jacobian_hermitian_product_naive), src/utils/residual_kernels.cuh; "
+                       "FP32, one-thread launches on the host (oracle/ref_sim.cpp, ref_sim_hermitian.cpp); "
                        "fast-math intrinsics replaced by libm")
     (Path(__file__).parent / "ref_simulations.json").write_text(json.dumps(sims))
-    print("wrote", {k: len(v) for k, v in sims.items() if isinstance(v, list)})
+    print("wrote", sorted(k for k in sims if not k.startswith("_")))
     return 0
 
 

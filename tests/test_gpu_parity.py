@@ -139,6 +139,36 @@ def test_simulation_matches_reference_kernels(cb, ctx, ref_simulations, oracle, 
     assert tried >= 3
 
 
+def test_operators_match_reference_kernels(cb, ctx, ref_simulations, oracle):
+    # phase encoding, every signal method, every Jacobian method, the residual and the spiral signal
+    # against the outputs of the reference's own naive kernels (FP32 on the CPU, within 3e-7 of the
+    # FP64 oracle): the plain FP32 methods to 1e-5 and the split-BF16 ones to 1e-4, plus that 3e-7
+    c = ref_simulations["cartesian"]
+    params = cb.TissueParameters.from_soa(ctx, c["params"])
+    traj = cb.trajectory_from_dict(ctx, c["traj"])
+    got = cb.phase_encoding(ctx, c["echos"], params, traj).to_numpy()
+    assert oracle.rel_l2(got, c["phase_encoded"]) < TOL_FP32
+    for m in PLAIN_SIGNAL + TC_SIGNAL:
+        got = cb.magnetization_to_signal(ctx, c["echos"], params, traj, c["coils"], method=m).to_numpy()
+        assert oracle.rel_l2(got, c["signal"]) < (TOL_FP32 if m in PLAIN_SIGNAL else TOL_BF16X3), m
+    d = {"T1": c["dT1"], "T2": c["dT2"]}
+    for m in PLAIN_JAC + TC_JAC:
+        tol = TOL_FP32 if m in PLAIN_JAC else TOL_BF16X3
+        jv = cb.compute_jacobian(ctx, c["echos"], d, params, traj, c["coils"], c["v"], method=m).to_numpy()
+        assert oracle.rel_l2(jv, c["jv"]) < tol, ("J·v", m)
+        jhv = cb.compute_jacobian_hermitian(ctx, c["echos"], d, params, traj, c["coils"], c["u"], method=m).to_numpy()
+        assert oracle.rel_l2(jhv, c["jhv"]) < tol, ("Jᴴ·v", m)
+    obj, diff = cb.compute_residual(ctx, c["signal"].astype(np.complex64), c["rhs"])
+    assert oracle.rel_l2(diff.to_numpy(), c["residual"]) < TOL_FP32
+    assert abs(obj - c["objective"]) < TOL_FP32 * c["objective"]
+    s = ref_simulations["spiral"]
+    params = cb.TissueParameters.from_soa(ctx, s["params"])
+    traj = cb.trajectory_from_dict(ctx, s["traj"])
+    for m in ("Direct", "MatmulFast"):
+        got = cb.magnetization_to_signal(ctx, s["echos"], params, traj, s["coils"], method=m).to_numpy()
+        assert oracle.rel_l2(got, s["signal"]) < (TOL_FP32 if m == "Direct" else TOL_BF16X3), ("spiral", m)
+
+
 # ------------------------------------------------------------------------------------------------
 # pSSFP
 # ------------------------------------------------------------------------------------------------

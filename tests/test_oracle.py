@@ -53,6 +53,24 @@ def test_oracle_matches_reference_kernels(oracle, ref_simulations, kind):
         assert oracle.rel_l2(sim(p, seq, dtype="f32"), echos) < 1e-6, (kind, i)
 
 
+def test_oracle_operators_match_reference_kernels(oracle, ref_simulations):
+    # phase encoding, the naive Cartesian signal, J·v, Jᴴ·v, the residual and the spiral signal of
+    # the reference's kernels (FP32 on the CPU) against the FP64 oracle: FP32 rounding only
+    c = ref_simulations["cartesian"]
+    p, t = c["params"], c["traj"]
+    assert oracle.rel_l2(oracle.phase_encoding(c["echos"], p, t["k_start"]), c["phase_encoded"]) < 1e-6
+    assert oracle.rel_l2(oracle.signal_cartesian(c["echos"], p, t, c["coils"]), c["signal"]) < 1e-6
+    assert oracle.rel_l2(oracle.signal_cartesian(c["echos"], p, t, c["coils"], dtype="f32"), c["signal"]) < 1e-7
+    jv = oracle.jacobian(c["echos"], c["dT1"], c["dT2"], p, t, c["coils"], c["v"])
+    assert oracle.rel_l2(jv, c["jv"]) < 1e-6
+    jhv = oracle.jacobian_hermitian(c["echos"], c["dT1"], c["dT2"], p, t, c["coils"], c["u"])
+    assert oracle.rel_l2(jhv, c["jhv"]) < 1e-6
+    obj, diff = oracle.residual(c["signal"].astype(np.complex64), c["rhs"])
+    assert oracle.rel_l2(diff, c["residual"]) < 1e-6 and abs(obj - c["objective"]) < 1e-6 * obj
+    s = ref_simulations["spiral"]
+    assert oracle.rel_l2(oracle.signal_spiral(s["echos"], s["params"], s["traj"], s["coils"]), s["signal"]) < 1e-6
+
+
 def test_fisp_zero_rf_gives_zero_echo(oracle, workloads):
     seq = workloads.fisp_sequence(np.zeros(20), np.ones((2, 20)), 8e-3, 4e-3, 20e-3, 6)
     e = oracle.fisp(_one_voxel(), seq)
