@@ -266,6 +266,59 @@ def cx_eval_f32(op: int, packed: np.ndarray) -> np.ndarray:
     return out
 
 
+_REF = None
+_REF_PATH = _HERE / "_ref" / "libref_kernels.so"
+
+
+def ref_kernels():
+    """The reference's own FISP and Cartesian-signal kernels built for the host
+    (oracle/_ref/libref_kernels.so, oracle/Makefile target `ref`), or None where they were not
+    built (no reference tree at build time)."""
+    global _REF
+    if _REF is None and _REF_PATH.exists():
+        L = C.CDLL(str(_REF_PATH))
+        L.ref_fisp.argtypes = [_P, _I64, _P, _I64, _P, _P, _I, _I, _F, _F, _F, _F, _I, _I, _I, _I, _I, _P, _I]
+        L.ref_fisp.restype = C.c_int
+        L.ref_signal_cartesian_entries.argtypes = [_P, _P, _I64, _I, _I, _F, _P, _F, _P, _I, _P, _I64, _P, _I]
+        L.ref_signal_cartesian_entries.restype = None
+        _REF = L
+    return _REF
+
+
+def ref_fisp(params, seq, vidx=None, nthreads=None):
+    """Echoes [nTR*uf][n] from the reference's simulate_fisp kernel run on the host cores."""
+    L = ref_kernels()
+    params = _ff(params)
+    nv = params.shape[1]
+    idx, nidx = _ip(vidx)
+    n = nidx if idx is not None else nv
+    rf, slices = _cf(seq["rf"]), _cf(seq["slices"])
+    nTR, P = len(seq["rf"]), seq["slices"].shape[0]
+    out = np.zeros((nTR * int(seq.get("uf", 1)), n, 2), np.float32)
+    rc = L.ref_fisp(params.ctypes.data, C.c_int64(nv), _iptr(idx), C.c_int64(n), rf.ctypes.data, slices.ctypes.data,
+                    nTR, P, C.c_float(seq["TR"]), C.c_float(seq["TE"]), C.c_float(seq.get("TW", 0.0)),
+                    C.c_float(seq["TI"]), int(seq["max_state"]), int(seq.get("uf", 1)), int(seq.get("reps", 1)),
+                    int(seq.get("inversion", 1)), int(seq.get("wait_spoil", 1)), out.ctypes.data,
+                    nthreads or nthreads_default())
+    if rc != 0:
+        raise ValueError("ref_fisp rejected its arguments")
+    return _as_complex(out)
+
+
+def ref_signal_cartesian(echo, params, traj, coils, entries, nthreads=None):
+    """Signal entries (coil, readout, sample) from the reference's naive Cartesian kernel on the host."""
+    L = ref_kernels()
+    e, params, ks, co = _cf(echo), _ff(params), _cf(traj["k_start"]), _cf(coils)
+    R, V = echo.shape
+    ent = np.ascontiguousarray(entries, dtype=np.int32)
+    out = np.zeros((len(ent), 2), np.float32)
+    L.ref_signal_cartesian_entries(e.ctypes.data, params.ctypes.data, C.c_int64(V), traj["nr"], traj["ns"],
+                                   C.c_float(traj["dt"]), ks.ctypes.data, C.c_float(complex(traj["dk"]).real),
+                                   co.ctypes.data, coils.shape[0], ent.ctypes.data, C.c_int64(len(ent)),
+                                   out.ctypes.data, nthreads or nthreads_default())
+    return _as_complex(out)
+
+
 def derivative_central(simulate, params, seq, field: int, rel_step: float = 1e-4, vidx=None, **kw):
     """∂echo/∂params[field] by an FP64 central difference of an oracle simulation (`fisp` or
     `pssfp`) with a step of rel_step·|p| per voxel (voxels are independent, so all are stepped at

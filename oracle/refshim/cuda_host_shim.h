@@ -9,14 +9,16 @@
 
 #include "kernel_float.h"
 
+// Launch coordinates per host thread: each thread runs its own one-thread launches. Shared
+// memory becomes a per-thread static, which is what one thread per block sees.
 struct compas_ref_dim3 {
     unsigned x = 0, y = 0, z = 0;
 };
-inline compas_ref_dim3 threadIdx, blockIdx, blockDim {1, 1, 1}, gridDim {1, 1, 1};
+inline thread_local compas_ref_dim3 threadIdx, blockIdx, blockDim {1, 1, 1}, gridDim {1, 1, 1};
 
 #define __global__
 #define __device__
-#define __shared__ static
+#define __shared__ static thread_local
 #define __launch_bounds__(...)
 #define KMM_ASSUME(expr) ((void)0)
 #define __builtin_assume(expr) ((void)0)

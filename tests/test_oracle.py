@@ -71,6 +71,24 @@ def test_oracle_operators_match_reference_kernels(oracle, ref_simulations):
     assert oracle.rel_l2(oracle.signal_spiral(s["echos"], s["params"], s["traj"], s["coils"]), s["signal"]) < 1e-6
 
 
+def test_reference_kernel_library_matches_oracle(oracle, workloads):
+    # oracle/_ref/libref_kernels.so (the reference's simulate_fisp and naive Cartesian signal built
+    # for the host; the CPU baseline of bench.py) against the FP64 oracle on a threaded run
+    if oracle.ref_kernels() is None:
+        pytest.skip("oracle/_ref/libref_kernels.so not built (no reference tree at build time)")
+    w = workloads.tiny(n_side=6, ntr=29, P=3, max_state=25, seed=5)
+    w["seq"]["reps"], w["seq"]["uf"], w["seq"]["TW"] = 2, 2, 0.02
+    idx = np.array([0, 5, 17, 35])
+    ref = oracle.fisp(w["params"], w["seq"], vidx=idx)
+    assert oracle.rel_l2(oracle.ref_fisp(w["params"], w["seq"], vidx=idx, nthreads=3), ref) < 1e-5
+    assert oracle.rel_l2(oracle.ref_fisp(w["params"], w["seq"], nthreads=4)[:, idx], ref) < 1e-5
+    echo = workloads.cn(np.random.default_rng(6), (29, 36))
+    ent = np.array([[0, 0, 0], [2, 13, 6], [1, 28, 3]])
+    got = oracle.ref_signal_cartesian(echo, w["params"], w["traj"], w["coils"], ent, nthreads=2)
+    want = oracle.signal_cartesian(echo, w["params"], w["traj"], w["coils"], entries=ent)
+    assert oracle.rel_l2(got, want) < 1e-5
+
+
 def test_fisp_zero_rf_gives_zero_echo(oracle, workloads):
     seq = workloads.fisp_sequence(np.zeros(20), np.ones((2, 20)), 8e-3, 4e-3, 20e-3, 6)
     e = oracle.fisp(_one_voxel(), seq)
