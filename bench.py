@@ -213,6 +213,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-jacobian", action="store_true", help="skip the J·v / Jᴴ·v measurements")
+    ap.add_argument("--no-reference-kernels", action="store_true",
+                    help="skip timing the reference's own kernels built for the GPU")
     ap.add_argument("--no-gn", action="store_true", help="skip the Gauss-Newton iteration timings")
     ap.add_argument("--serve-rates", default="2,4,8",
                     help="Poisson arrival rates (requests/s) of the served stream, empty to skip")
@@ -338,6 +340,8 @@ def main():
            "stage_ms": {"simulate_fisp": sim_ms, "signal_cartesian": sig_ms},
            "signal_tflops": sig_tf, "peaks": peak_kind}
 
+    if world == 1 and not args.no_reference_kernels:
+        out["reference_kernels_gpu"] = reference_kernels_gpu(cb, ctx, stream, w, sim_ms, args)
     if not args.no_jacobian:
         out["jacobian"] = jacobian_products(cb, ctx, stream, args, peaks, rank)
     if args.batch_jobs > 0:
@@ -484,6 +488,68 @@ def served(cb, ctx, args):
     out["runs"].append(stream_run(rates[len(rates) // 2], "Direct", args.serve_requests, False))
     out["runs"].append(stream_run(rates[-1], "MatmulFast", args.serve_requests, True))
     return out
+
+
+def reference_kernels_gpu(cb, ctx, stream, w, sim_ms, args):
+    """The reference's own FISP and pSSFP kernels on the same B200 ("reference kernels, re-hosted":
+    oracle/_ref/libref_gpu.so, its unmodified src/simulate/*_kernels.cuh with its CUDA flags and
+    launch shapes), timed with CUDA events on the same workloads as this library: the MR-STAT FISP
+    slice of the main measurement and a pSSFP slice (35 z, 15 RF samples, 320 TRs). rel_l2 compares
+    the two implementations' echoes over the whole array."""
+    import torch
+    import workloads
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    if oracle.ref_gpu() is None:
+        return {"unavailable": "oracle/_ref/libref_gpu.so not built (the reference tree was absent at build time)"}
+
+    def timed(fn, s, reps=2):
+        with torch.cuda.stream(s):
+            r = fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            for _ in range(reps):
+                r = fn()
+            e1.record(s)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, r
+
+    def rel(a, b):
+        a, b = torch.as_tensor(a, device="cuda"), torch.as_tensor(b, device="cuda")
+        a, b = torch.view_as_real(a) if a.is_complex() else a, torch.view_as_real(b) if b.is_complex() else b
+        return float(torch.linalg.vector_norm((a - b).double()) / torch.linalg.vector_norm(b.double()))
+
+    ts = torch.cuda.Stream()
+    res = {"what": "the reference's simulate_fisp / simulate_pssfp kernels (fisp_kernels.cuh, pssfp_kernels.cuh), "
+                   "unmodified, compiled with nvcc --use_fast_math for sm_100 against stand-ins for the absent "
+                   "kmm views; launch code restated from src/simulate/fisp.cu and pssfp.cu"}
+    V = w["params"].shape[1]
+    nTR = len(w["seq"]["rf"])
+    ref_ms, ref_e = timed(lambda: oracle.ref_gpu_fisp(w["params"], w["seq"]), ts)
+    p = cb.TissueParameters.from_soa(ctx, w["params"])
+    mine = cb.simulate_magnetization(ctx, p, cb.FispSequence.from_dict(ctx, w["seq"]))
+    ctx.synchronize()
+    res["fisp_mrstat"] = {"voxels": V, "readouts": nTR, "reference_ms": ref_ms, "this_ms": sim_ms,
+                          "reference_voxel_tr_per_s": V * nTR / (ref_ms / 1e3),
+                          "this_voxel_tr_per_s": V * nTR / (sim_ms / 1e3), "speedup": ref_ms / sim_ms,
+                          "rel_l2": rel(torch.view_as_real(ref_e), mine)}
+    del ref_e, mine
+    rng = np.random.default_rng(7)
+    pd = workloads.pssfp_sequence(rng, 320, nrf=15, nz=35)
+    pp = workloads.tissue(rng, args.n_side, 22.4)
+    ref_ms, ref_e = timed(lambda: oracle.ref_gpu_pssfp(pp, pd), ts)
+    p = cb.TissueParameters.from_soa(ctx, pp)
+    seq = cb.pSSFPSequence.from_dict(ctx, pd)
+    this_ms, mine = timed(lambda: cb.simulate_magnetization(ctx, p, seq), stream)
+    res["pssfp_320tr"] = {"voxels": pp.shape[1], "readouts": 320, "reference_ms": ref_ms, "this_ms": this_ms,
+                          "reference_voxel_tr_per_s": pp.shape[1] * 320 / (ref_ms / 1e3),
+                          "this_voxel_tr_per_s": pp.shape[1] * 320 / (this_ms / 1e3), "speedup": ref_ms / this_ms,
+                          "rel_l2": rel(torch.view_as_real(ref_e), mine)}
+    res["out_of_bounds_flag"] = oracle.ref_gpu().ref_gpu_out_of_bounds()
+    return res
 
 
 def derivatives(cb, ctx, stream, args, rank):

@@ -285,6 +285,74 @@ def ref_kernels():
     return _REF
 
 
+_REF_GPU = None
+_REF_GPU_PATH = _HERE / "_ref" / "libref_gpu.so"
+
+
+def ref_gpu():
+    """The reference's FISP and pSSFP kernels built for the B200 with its own CUDA flags
+    (oracle/_ref/libref_gpu.so, "reference kernels, re-hosted"), or None where they were not built.
+    Entry points take device pointers (ints) and a cudaStream_t."""
+    global _REF_GPU
+    if _REF_GPU is None and _REF_GPU_PATH.exists():
+        L = C.CDLL(str(_REF_GPU_PATH))
+        L.ref_gpu_fisp.argtypes = [_P, _I, _P, _P, _I, _I, _F, _F, _F, _F, _I, _I, _I, _P, _P, _P]
+        L.ref_gpu_fisp.restype = C.c_int
+        L.ref_gpu_pssfp.argtypes = [_P, _I, _P, _I, _F, _P, _I, _P, _P, _P, _I, _P, _P]
+        L.ref_gpu_pssfp.restype = C.c_int
+        L.ref_gpu_out_of_bounds.argtypes = []
+        L.ref_gpu_out_of_bounds.restype = C.c_int
+        _REF_GPU = L
+    return _REF_GPU
+
+
+def ref_gpu_fisp(params, seq):
+    """FISP echoes [nTR*uf][nv] (torch complex64) from the re-hosted reference kernels, launched on
+    torch's current CUDA stream (the inputs' temporaries are freed in that stream's order);
+    `params` [9][nv] float32, `seq` a workloads-style dict."""
+    import torch
+
+    L = ref_gpu()
+    dev = torch.device("cuda")
+    p = torch.as_tensor(_ff(params), device=dev)
+    nv = p.shape[1]
+    rf = torch.as_tensor(np.ascontiguousarray(seq["rf"], np.complex64), device=dev)
+    sl = torch.as_tensor(np.ascontiguousarray(seq["slices"], np.complex64), device=dev)
+    nTR, P, uf = rf.shape[0], sl.shape[0], int(seq.get("uf", 1))
+    tr = torch.empty((nv, nTR), dtype=torch.complex64, device=dev)
+    out = torch.empty((nTR * uf, nv), dtype=torch.complex64, device=dev)
+    st = torch.cuda.current_stream()
+    rc = L.ref_gpu_fisp(p.data_ptr(), nv, rf.data_ptr(), sl.data_ptr(), nTR, P, seq["TR"], seq["TE"],
+                        seq.get("TW", 0.0), seq["TI"], int(seq["max_state"]), uf, int(seq.get("reps", 1)),
+                        tr.data_ptr(), out.data_ptr(), C.c_void_p(st.cuda_stream))
+    if rc != 0:
+        raise ValueError("ref_gpu_fisp rejected its arguments")
+    return out
+
+
+def ref_gpu_pssfp(params, seq):
+    """pSSFP echoes [nTR][nv] (torch complex64) from the re-hosted reference kernels, on torch's
+    current CUDA stream."""
+    import torch
+
+    L = ref_gpu()
+    dev = torch.device("cuda")
+    p = torch.as_tensor(_ff(params), device=dev)
+    nv = p.shape[1]
+    rf = torch.as_tensor(np.ascontiguousarray(seq["rf"], np.complex64), device=dev)
+    g = torch.as_tensor(np.ascontiguousarray(seq["gdtrf"], np.complex64), device=dev)
+    z = torch.as_tensor(_ff(seq["z"]), device=dev)
+    dt = (C.c_float * 3)(*seq["dt"])
+    gz = (C.c_float * 3)(*seq["gz"])
+    out = torch.empty((rf.shape[0], nv), dtype=torch.complex64, device=dev)
+    st = torch.cuda.current_stream()
+    rc = L.ref_gpu_pssfp(p.data_ptr(), nv, rf.data_ptr(), rf.shape[0], seq["TR"], g.data_ptr(), g.shape[0], dt, gz,
+                         z.data_ptr(), z.shape[0], out.data_ptr(), C.c_void_p(st.cuda_stream))
+    if rc != 0:
+        raise ValueError("ref_gpu_pssfp rejected its arguments")
+    return out
+
+
 def ref_fisp(params, seq, vidx=None, nthreads=None):
     """Echoes [nTR*uf][n] from the reference's simulate_fisp kernel run on the host cores."""
     L = ref_kernels()
