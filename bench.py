@@ -552,6 +552,56 @@ def reference_kernels_gpu(cb, ctx, stream, w, sim_ms, args):
     return res
 
 
+def reference_products_gpu(w, stream, reps, this_ms, lib):
+    """The reference's default product paths on the same B200 and inputs: MatmulFast signal and
+    GemmFast J·v / Jᴴ·v (its kernels plus TF32 cuBLAS, re-hosted: oracle/_ref/libref_gpu.so). rel_l2
+    compares their results with this library's split-BF16 ones."""
+    import torch
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    if oracle.ref_gpu() is None:
+        return {"unavailable": "oracle/_ref/libref_gpu.so not built (the reference tree was absent at build time)"}
+    cb, ctx, params, traj, arr, d = lib
+    ins = {k: torch.as_tensor(np.ascontiguousarray(w[k]), device="cuda")
+           for k in ("echo", "dT1", "dT2", "v", "r", "coils")}
+    ts = torch.cuda.Stream()
+    runs = {"signal": lambda: oracle.ref_gpu_signal_cartesian(w["params"], ins["echo"], w["traj"], ins["coils"]),
+            "jv": lambda: oracle.ref_gpu_jacobian(w["params"], ins["echo"], ins["dT1"], ins["dT2"], w["traj"],
+                                                  ins["coils"], ins["v"]),
+            "jhv": lambda: oracle.ref_gpu_jacobian(w["params"], ins["echo"], ins["dT1"], ins["dT2"], w["traj"],
+                                                   ins["coils"], ins["r"], hermitian=True)}
+    mine = {"signal": lambda: cb.magnetization_to_signal(ctx, arr["echo"], params, traj, arr["coils"],
+                                                         method="MatmulFast"),
+            "jv": lambda: cb.compute_jacobian(ctx, arr["echo"], d, params, traj, arr["coils"], arr["v"],
+                                              method="GemmFast"),
+            "jhv": lambda: cb.compute_jacobian_hermitian(ctx, arr["echo"], d, params, traj, arr["coils"], arr["r"],
+                                                         method="GemmFast")}
+    res = {"what": "the reference's MatmulFast signal and GemmFast J·v / Jᴴ·v (the C ABI's defaults): its unmodified "
+                   "kernels and its four-GEMM complex products on TF32 cuBLAS, launch code restated from "
+                   "src/trajectories/signal.cu, src/jacobian/product.cu, hermitian.cu"}
+    for name, fn in runs.items():
+        with torch.cuda.stream(ts):
+            out = fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ts)
+            for _ in range(reps):
+                out = fn()
+            e1.record(ts)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        ours = torch.as_tensor(mine[name](), device="cuda")
+        ctx.synchronize()
+        a = torch.view_as_real(out).double()
+        rel = float(torch.linalg.vector_norm(a - ours.double()) / torch.linalg.vector_norm(ours.double()))
+        res[name] = {"reference_ms": ms, "this_ms": this_ms[name], "speedup": ms / this_ms[name], "rel_l2": rel}
+        del out, ours
+    res["out_of_bounds_flag"] = oracle.ref_gpu_out_of_bounds()
+    return res
+
+
 def derivatives(cb, ctx, stream, args, rank):
     """∂m/∂T1 and ∂m/∂T2 two ways: the reference's forward differences (value simulation plus one
     simulation per field at p + Δ, Δ = 1e-4) and the forward-mode tangents (value and both
@@ -689,8 +739,11 @@ def jacobian_products(cb, ctx, stream, args, peaks, rank):
     f_jh = 16.0 * C_ * R * S * V + 24.0 * C_ * R * V
     peak = peaks["bf16_tflops_sustained"]
     tf = lambda f, ms: f / (ms / 1e3) / 1e12
+    reference = reference_products_gpu(w, stream, reps, {"signal": sig, "jv": jv, "jhv": jhv},
+                                       (cb, ctx, params, traj, arr, d))
     return {"workload": f"{args.n_side}x{args.n_side}={V} voxels, Cartesian {R}x{S}, {C_} coils, random echoes / "
                         "∂echoes, v and residual CN(0,1)",
+            "reference_default_paths_gpu": reference,
             "jv_ms": jv, "jv_tflops": tf(f_j, jv), "jhv_ms": jhv, "jhv_tflops": tf(f_jh, jhv),
             "signal_ms": sig, "signal_tflops": tf(f_sig, sig),
             "signal_plus_jhv_tflops": tf(f_sig + f_jh, sig + jhv),

@@ -300,10 +300,65 @@ def ref_gpu():
         L.ref_gpu_fisp.restype = C.c_int
         L.ref_gpu_pssfp.argtypes = [_P, _I, _P, _I, _F, _P, _I, _P, _P, _P, _I, _P, _P]
         L.ref_gpu_pssfp.restype = C.c_int
-        L.ref_gpu_out_of_bounds.argtypes = []
-        L.ref_gpu_out_of_bounds.restype = C.c_int
+        L.ref_gpu_signal_cartesian.argtypes = [_P, _I, _P, _P, _I, _I, _I, _F, _P, _F, _P, _P]
+        L.ref_gpu_signal_cartesian.restype = None
+        L.ref_gpu_jacobian.argtypes = [_P, _I, _P, _P, _P, _P, _I, _I, _I, _F, _P, _F, _P, _P, _P]
+        L.ref_gpu_jacobian.restype = None
+        L.ref_gpu_jacobian_hermitian.argtypes = [_P, _I, _P, _P, _P, _P, _I, _I, _I, _F, _P, _F, _P, _P, _P]
+        L.ref_gpu_jacobian_hermitian.restype = None
+        for name in ("ref_gpu_out_of_bounds", "ref_gpu_products_out_of_bounds", "ref_gpu_hermitian_out_of_bounds"):
+            getattr(L, name).argtypes = []
+            getattr(L, name).restype = C.c_int
         _REF_GPU = L
     return _REF_GPU
+
+
+def ref_gpu_out_of_bounds() -> int:
+    """1 when any view index of the re-hosted reference kernels was out of range (and clamped)."""
+    L = ref_gpu()
+    flags = [L.ref_gpu_out_of_bounds(), L.ref_gpu_products_out_of_bounds(), L.ref_gpu_hermitian_out_of_bounds()]
+    return -1 if min(flags) < 0 else max(flags)
+
+
+def _dev(a, dtype):
+    import torch
+
+    if isinstance(a, torch.Tensor):
+        return a.to(device="cuda", dtype=dtype).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(a), device="cuda").to(dtype).contiguous()
+
+
+def ref_gpu_signal_cartesian(params, echos, traj, coils):
+    """Signal [C][R][S] (torch complex64) of the reference's default Cartesian path (MatmulFast: its
+    kernels plus TF32 cuBLAS) on torch's current stream."""
+    import torch
+
+    p, e, c = _dev(_ff(params), torch.float32), _dev(echos, torch.complex64), _dev(coils, torch.complex64)
+    ks = _dev(traj["k_start"], torch.complex64)
+    V, C_, R, S = p.shape[1], c.shape[0], traj["nr"], traj["ns"]
+    out = torch.empty((C_, R, S), dtype=torch.complex64, device="cuda")
+    ref_gpu().ref_gpu_signal_cartesian(p.data_ptr(), V, e.data_ptr(), c.data_ptr(), C_, R, S, traj["dt"],
+                                       ks.data_ptr(), float(complex(traj["dk"]).real), out.data_ptr(),
+                                       C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    return out
+
+
+def ref_gpu_jacobian(params, echos, dT1, dT2, traj, coils, vector, hermitian=False):
+    """J·v [C][R][S] (vector [4][V]) or, with hermitian, Jᴴ·v [4][V] (vector [C][R][S]) of the
+    reference's default GemmFast paths (its kernels plus TF32 cuBLAS), torch complex64."""
+    import torch
+
+    p = _dev(_ff(params), torch.float32)
+    e, d1, d2 = (_dev(x, torch.complex64) for x in (echos, dT1, dT2))
+    c, v = _dev(coils, torch.complex64), _dev(vector, torch.complex64)
+    ks = _dev(traj["k_start"], torch.complex64)
+    V, C_, R, S = p.shape[1], c.shape[0], traj["nr"], traj["ns"]
+    shape = (4, V) if hermitian else (C_, R, S)
+    out = torch.empty(shape, dtype=torch.complex64, device="cuda")
+    fn = ref_gpu().ref_gpu_jacobian_hermitian if hermitian else ref_gpu().ref_gpu_jacobian
+    fn(p.data_ptr(), V, e.data_ptr(), d1.data_ptr(), d2.data_ptr(), c.data_ptr(), C_, R, S, traj["dt"], ks.data_ptr(),
+       float(complex(traj["dk"]).real), v.data_ptr(), out.data_ptr(), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    return out
 
 
 def ref_gpu_fisp(params, seq):
