@@ -494,8 +494,9 @@ def reference_kernels_gpu(cb, ctx, stream, w, sim_ms, args):
     """The reference's own FISP and pSSFP kernels on the same B200 ("reference kernels, re-hosted":
     oracle/_ref/libref_gpu.so, its unmodified src/simulate/*_kernels.cuh with its CUDA flags and
     launch shapes), timed with CUDA events on the same workloads as this library: the MR-STAT FISP
-    slice of the main measurement and a pSSFP slice (35 z, 15 RF samples, 320 TRs). rel_l2 compares
-    the two implementations' echoes over the whole array."""
+    slice of the main measurement, a pSSFP slice (35 z, 15 RF samples, 320 TRs) and a 16-coil spiral
+    signal (its only spiral method). rel_l2 compares the two implementations' results over the
+    whole array."""
     import torch
     import workloads
 
@@ -548,7 +549,25 @@ def reference_kernels_gpu(cb, ctx, stream, w, sim_ms, args):
                           "reference_voxel_tr_per_s": pp.shape[1] * 320 / (ref_ms / 1e3),
                           "this_voxel_tr_per_s": pp.shape[1] * 320 / (this_ms / 1e3), "speedup": ref_ms / this_ms,
                           "rel_l2": rel(torch.view_as_real(ref_e), mine)}
-    res["out_of_bounds_flag"] = oracle.ref_gpu().ref_gpu_out_of_bounds()
+    del ref_e, mine
+    # spiral signal: 30000 voxels, 760 interleaves x 1000 samples, 16 coils (the reference's only
+    # spiral method; here split-BF16 tensor cores)
+    rng = np.random.default_rng(8)
+    sp = workloads.tissue_voxels(rng, 30000, 22.4)
+    st = workloads.spiral(rng, 760, 1000, 22.4, 4e-6)
+    coils = workloads.cn(rng, (16, 30000))
+    echo = workloads.cn(rng, (760, 30000)) * 0.1
+    ref_ms, ref_s = timed(lambda: oracle.ref_gpu_signal_spiral(sp, echo, st, coils), ts)
+    p = cb.TissueParameters.from_soa(ctx, sp)
+    traj = cb.trajectory_from_dict(ctx, st)
+    e_arr, c_arr = cb.CompasArray.from_numpy(ctx, echo), cb.CompasArray.from_numpy(ctx, coils)
+    this_ms, mine = timed(lambda: cb.magnetization_to_signal(ctx, e_arr, p, traj, c_arr, method="MatmulFast"), stream)
+    flops = 8.0 * 16 * 760 * 1000 * 30000
+    res["spiral_signal_16coils"] = {"voxels": 30000, "readouts": 760, "samples": 1000, "reference_ms": ref_ms,
+                                    "this_ms": this_ms, "reference_tflops": flops / ref_ms / 1e9,
+                                    "this_tflops": flops / this_ms / 1e9, "speedup": ref_ms / this_ms,
+                                    "rel_l2": rel(torch.view_as_real(ref_s), mine)}
+    res["out_of_bounds_flag"] = oracle.ref_gpu_out_of_bounds()
     return res
 
 

@@ -302,6 +302,8 @@ def ref_gpu():
         L.ref_gpu_pssfp.restype = C.c_int
         L.ref_gpu_signal_cartesian.argtypes = [_P, _I, _P, _P, _I, _I, _I, _F, _P, _F, _P, _P]
         L.ref_gpu_signal_cartesian.restype = None
+        L.ref_gpu_signal_spiral.argtypes = [_P, _I, _P, _P, _I, _I, _I, _F, _P, _P, _P, _P]
+        L.ref_gpu_signal_spiral.restype = None
         L.ref_gpu_jacobian.argtypes = [_P, _I, _P, _P, _P, _P, _I, _I, _I, _F, _P, _F, _P, _P, _P]
         L.ref_gpu_jacobian.restype = None
         L.ref_gpu_jacobian_hermitian.argtypes = [_P, _I, _P, _P, _P, _P, _I, _I, _I, _F, _P, _F, _P, _P, _P]
@@ -340,6 +342,20 @@ def ref_gpu_signal_cartesian(params, echos, traj, coils):
     ref_gpu().ref_gpu_signal_cartesian(p.data_ptr(), V, e.data_ptr(), c.data_ptr(), C_, R, S, traj["dt"],
                                        ks.data_ptr(), float(complex(traj["dk"]).real), out.data_ptr(),
                                        C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    return out
+
+
+def ref_gpu_signal_spiral(params, echos, traj, coils):
+    """Spiral signal [C][R][S] (torch complex64) of the reference's spiral kernels on torch's
+    current stream."""
+    import torch
+
+    p, e, c = _dev(_ff(params), torch.float32), _dev(echos, torch.complex64), _dev(coils, torch.complex64)
+    ks, dk = _dev(traj["k_start"], torch.complex64), _dev(traj["dk"], torch.complex64)
+    V, C_, R, S = p.shape[1], c.shape[0], traj["nr"], traj["ns"]
+    out = torch.empty((C_, R, S), dtype=torch.complex64, device="cuda")
+    ref_gpu().ref_gpu_signal_spiral(p.data_ptr(), V, e.data_ptr(), c.data_ptr(), C_, R, S, traj["dt"], ks.data_ptr(),
+                                    dk.data_ptr(), out.data_ptr(), C.c_void_p(torch.cuda.current_stream().cuda_stream))
     return out
 
 

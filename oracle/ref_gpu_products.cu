@@ -7,7 +7,8 @@
 // cuBLAS calls of src/utils/gemm.cu (ref_gpu_gemm.cuh), in TF32 as the C ABI's defaults select
 // (julia-bindings/src/bindings.cpp:264, 307: low_precision = 0 → MatmulFast / GemmFast):
 //  * signal: src/trajectories/signal.cu:103-156 (magnetization_to_signal_cartesian_gemm<float>);
-//  * J·v: src/jacobian/product.cu:201-285 (compute_jacobian_gemm<float>), one voxel chunk.
+//  * J·v: src/jacobian/product.cu:201-285 (compute_jacobian_gemm<float>), one voxel chunk;
+//  * spiral signal: src/trajectories/signal.cu:170-240 (its only spiral method, no cuBLAS).
 #include <cuda_runtime.h>
 
 #include "kernel_float.h"  // the stand-in; some reference kernel headers use it without including it
@@ -91,6 +92,35 @@ void ref_gpu_jacobian(float* params, int V, float* echos, float* dT1, float* dT2
         compas::kernels::convert_planar_to_complex<float><<<dim3(div_up(S, 32), div_up(R, 4)), dim3(32, 4), 0, stream>>>(
             R, S, host_view(out + int64_t(c) * R * S, R, S), host_view(jv_coil, 2, R, S));
     }
+}
+
+// spiral signal [C][R][S] from echos [R][V], coils [C][V], per-readout k_start and Δk [R] (complex):
+// src/trajectories/signal.cu:170-240 (magnetization_to_signal_spiral) with its launch shapes
+void ref_gpu_signal_spiral(float* params, int V, float* echos, float* coils, int C, int R, int S, float dt,
+                           float* k_start, float* delta_k, float* signal, void* stream_ptr) {
+    auto stream = static_cast<cudaStream_t>(stream_ptr);
+    const compas::TissueParametersView pv(host_view(params, 9, V));
+    compas::SpiralTrajectoryView traj;
+    traj.nreadouts = R;
+    traj.samples_per_readout = S;
+    traj.delta_t = dt;
+    traj.k_start = host_view(reinterpret_cast<cfloat*>(k_start), R);
+    traj.delta_k = host_view(reinterpret_cast<cfloat*>(delta_k), R);
+    auto* readout_echos = reinterpret_cast<cfloat*>(ref_gpu::scratch("spiral.readout_echos", size_t(2) * R * V));
+    auto* decay = reinterpret_cast<cfloat*>(ref_gpu::scratch("spiral.sample_decay", size_t(2) * R * V));
+    const dim3 block(32, 4), grid(div_up(V, 32), div_up(R, 4));
+    compas::kernels::prepare_readout_echos<<<grid, block, 0, stream>>>(
+        kmm::Range<int> {0, V}, kmm::Range<int> {0, R}, host_view(readout_echos, R, V),
+        host_view(reinterpret_cast<cfloat*>(echos), R, V), pv, traj);
+    compas::kernels::prepare_sample_decay_spiral<<<grid, block, 0, stream>>>(host_view(decay, R, V), pv, traj);
+    constexpr unsigned threads_per_block = 64, threads_cooperative = 32, samples_per_thread = 8,
+                       coils_per_thread = 1;
+    const dim3 sgrid(div_up(int64_t(div_up(S, samples_per_thread)) * threads_cooperative, threads_per_block),
+                     unsigned(R), div_up(C, coils_per_thread));
+    compas::kernels::sum_signal_spiral<threads_per_block, threads_cooperative, samples_per_thread, coils_per_thread>
+        <<<sgrid, threads_per_block, 0, stream>>>(host_view(reinterpret_cast<cfloat*>(signal), C, R, S),
+                                                  host_view(decay, R, V), host_view(readout_echos, R, V),
+                                                  host_view(reinterpret_cast<cfloat*>(coils), C, V));
 }
 
 int ref_gpu_products_out_of_bounds(void) {

@@ -86,3 +86,23 @@ def test_reference_products_on_gpu(ref, ref_simulations, workloads):
         traj = cb.trajectory_from_dict(ctx, t)
         mine = cb.magnetization_to_signal(ctx, case["echos"], params, traj, case["coils"], method="MatmulFast")
         assert ref.rel_l2(mine.to_numpy(), sig) < 2e-3
+
+
+def test_reference_spiral_signal_on_gpu(ref, ref_simulations, workloads):
+    import compas_b200 as cb
+
+    ctx = cb.Context(0)
+    rng = np.random.default_rng(8)
+    s = ref_simulations["spiral"]
+    p = workloads.tissue(rng, 9, 22.4)
+    big = {"params": p, "traj": workloads.spiral(rng, 13, 300, 22.4, 4e-6), "coils": workloads.cn(rng, (3, 81)),
+           "echos": workloads.cn(rng, (13, 81))}
+    for case in (s, big):
+        got = ref.ref_gpu_signal_spiral(case["params"], case["echos"], case["traj"], case["coils"]).cpu().numpy()
+        assert ref.ref_gpu_out_of_bounds() == 0
+        want = ref.signal_spiral(case["echos"], case["params"], case["traj"], case["coils"])
+        assert ref.rel_l2(got, want) < 1e-4
+        params = cb.TissueParameters.from_soa(ctx, case["params"])
+        mine = cb.magnetization_to_signal(ctx, case["echos"], params, cb.trajectory_from_dict(ctx, case["traj"]),
+                                          case["coils"], method="MatmulFast").to_numpy()
+        assert ref.rel_l2(mine, got) < 2e-4
