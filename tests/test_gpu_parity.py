@@ -409,3 +409,35 @@ def test_shape_mismatch_raises(cb, ctx, workloads):
     params, _, traj = _upload(cb, ctx, w)
     with pytest.raises(cb.CompasError):
         cb.magnetization_to_signal(ctx, np.zeros((3, 3), np.complex64), params, traj, w["coils"])
+
+
+def test_empty_voxel_set(cb, ctx, workloads):
+    # zero voxels: every operation returns correctly shaped empty or all-zero results (the
+    # products are sums over voxels) without launching a kernel over an empty grid
+    w = workloads.tiny(n_side=4, ntr=11, ns=6, nc=2, P=2, max_state=5)
+    empty = np.zeros((9, 0), np.float32)
+    params = cb.TissueParameters.from_soa(ctx, empty)
+    seq = cb.FispSequence.from_dict(ctx, w["seq"])
+    traj = cb.trajectory_from_dict(ctx, w["traj"])
+    coils = np.zeros((2, 0), np.complex64)
+    e = cb.simulate_magnetization(ctx, params, seq)
+    assert e.to_numpy().shape == (11, 0)
+    rng = np.random.default_rng(2)
+    ps = cb.pSSFPSequence.from_dict(ctx, workloads.pssfp_sequence(rng, 9, nrf=3, nz=5))
+    assert cb.simulate_magnetization(ctx, params, ps).to_numpy().shape == (9, 0)
+    for seqx, nr in ((seq, 11), (ps, 9)):
+        t = cb.simulate_magnetization_tangents(ctx, params, seqx)
+        assert all(t[k].to_numpy().shape == (nr, 0) for k in ("echos", "T1", "T2"))
+    d = {"T1": e, "T2": e}
+    for m in PLAIN_SIGNAL + TC_SIGNAL:
+        s = cb.magnetization_to_signal(ctx, e, params, traj, coils, method=m).to_numpy()
+        assert s.shape == (2, 11, 6) and not s.any(), m
+    for m in PLAIN_JAC + TC_JAC:
+        jv = cb.compute_jacobian(ctx, e, d, params, traj, coils, np.zeros((4, 0), np.complex64), method=m)
+        assert jv.to_numpy().shape == (2, 11, 6) and not jv.to_numpy().any(), m
+        u = workloads.cn(rng, (2, 11, 6))
+        jh = cb.compute_jacobian_hermitian(ctx, e, d, params, traj, coils, u, method=m)
+        assert jh.to_numpy().shape == (4, 0), m
+    st = workloads.spiral(rng, 11, 20, 22.4, 4e-6)
+    s = cb.magnetization_to_signal(ctx, e, params, cb.trajectory_from_dict(ctx, st), coils).to_numpy()
+    assert s.shape == (2, 11, 20) and not s.any()
