@@ -42,12 +42,13 @@ void fisp_voxels(float* params, int64_t nv, const int* vidx, int64_t nidx, cfloa
             const int v = vidx ? vidx[q] : int(q);
             std::fill(row.begin(), row.end(), cfloat(0));
             // the voxel's transposed echo row [nTR]; the kernel addresses it as row `voxel` of a
-            // [nv][nTR] view, so give it a view whose row v is this buffer
+            // [nv][nTR] view, so give it a view with a zero voxel stride, every row of which is
+            // this buffer
             kmm::View<cfloat, 2> tview;
-            tview.ptr = row.data() - int64_t(v) * nTR;
+            tview.ptr = row.data();
             tview.ext[0] = nv;
             tview.ext[1] = nTR;
-            tview.str[0] = nTR;
+            tview.str[0] = 0;
             tview.str[1] = 1;
             for (int i = 0; i < P; i++) {
                 blockDim = {1, 1, 1};
@@ -109,15 +110,12 @@ void ref_signal_cartesian_entries(float* echos, float* params, int64_t nv, int R
 #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
     for (int64_t e = 0; e < nent; e++) {
         cfloat value;
-        kmm::View<cfloat, 3> sview;  // a one-element signal at (c, r, s)
+        kmm::View<cfloat, 3> sview;  // every (c, r, s) of this [C][R][S] view is `value` (zero strides)
         const int c = entries[3 * e], r = entries[3 * e + 1], s = entries[3 * e + 2];
-        sview.ptr = &value - (int64_t(c) * R * S + int64_t(r) * S + s);
+        sview.ptr = &value;
         sview.ext[0] = C;
         sview.ext[1] = R;
         sview.ext[2] = S;
-        sview.str[0] = int64_t(R) * S;
-        sview.str[1] = S;
-        sview.str[2] = 1;
         blockDim = {1, 1, 1};
         blockIdx = {unsigned(s), unsigned(r), unsigned(c)};
         threadIdx = {0, 0, 0};
