@@ -320,6 +320,11 @@ def main():
                 "note": f"FP32 SIMT peak 148 SM x 128 lanes x 2 x {f_mhz:.0f} MHz (median SM clock under load); "
                         "algorithmic flops = 86·N·P per voxel·TR (reference formulation); HBM is not binding "
                         "(8 B written per voxel·TR)"}
+    # the HBM fraction beside it: algorithmic bytes = echoes written (8 B per voxel·readout) + the
+    # nine parameter rows read (36 B per voxel)
+    epg_bytes = 8.0 * V * nTR + 36.0 * V
+    roofline["hbm"] = {"achieved_gbs": epg_bytes / (sim_ms / 1e3) / 1e9, "peak_gbs": peaks["hbm_gbs"],
+                       "frac": epg_bytes / (sim_ms / 1e3) / 1e9 / peaks["hbm_gbs"]}
     sig_flops = 8.0 * C_ * R * S * V
     sig_tf = sig_flops / (sig_ms / 1e3) / 1e12
     roofline_signal = {"bound": "tensor", "kernel": "signal (split-BF16 tcgen05)", "achieved": sig_tf,
@@ -327,6 +332,11 @@ def main():
                        "frac": sig_tf / peaks["bf16_tflops_sustained"], "traffic": profile_traffic("cartesian_contraction_pairs_mrstat160"),
                        "note": f"algorithmic 8·C·R·S·V flops; split-BF16 issues 3 BF16 MMAs per product, so the "
                                f"attainable algorithmic rate is 1/3 of the BF16 peak ({peak_kind})"}
+    # algorithmic bytes: echoes read (8·R·V), coils and parameters (8·C·V + 36·V), signal written (8·C·R·S)
+    sig_bytes = 8.0 * R * V + 8.0 * C_ * V + 36.0 * V + 8.0 * C_ * R * S
+    roofline_signal["frac_of_split_bf16_ceiling"] = sig_tf / (peaks["bf16_tflops_sustained"] / 3)
+    roofline_signal["hbm"] = {"achieved_gbs": sig_bytes / (sig_ms / 1e3) / 1e9, "peak_gbs": peaks["hbm_gbs"],
+                              "frac": sig_bytes / (sig_ms / 1e3) / 1e9 / peaks["hbm_gbs"]}
 
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
