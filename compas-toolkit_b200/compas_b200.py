@@ -84,6 +84,8 @@ _SIGS = {
     "compas_b200_fisp_tangent_config_count": ([], _I),
     "compas_b200_fisp_tangent_config_info": ([_I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
     "compas_b200_make_batch": ([_P, _I, _P, _P, _P, _P, _I], _P),
+    "compas_b200_make_batch_tangents": ([_P, _I, _P, _P, _P, _P, _I, _P], _P),
+    "compas_b200_batch_derivative": ([_P, _I, _I], _P),
     "compas_b200_batch_run": ([_P], _I),
     "compas_b200_batch_echos": ([_P, _I], _P),
     "compas_b200_batch_signal": ([_P, _I], _P),
@@ -476,9 +478,10 @@ class SimulationBatch(_Object):
     (persistent work-queue simulation kernels, batched signal kernels).
 
     jobs: sequence of (parameters, sequence, trajectory or None, coils or None). Each job's
-    echoes and signal equal those of simulate_magnetization + magnetization_to_signal(method)."""
+    echoes and signal equal those of simulate_magnetization + magnetization_to_signal(method).
+    tangents: per-job flags; a flagged job also gets its exact ∂/∂T1, ∂/∂T2 (derivative())."""
 
-    def __init__(self, context: Context, jobs, method: str = "MatmulFast"):
+    def __init__(self, context: Context, jobs, method: str = "MatmulFast", tangents=None):
         lib = library()
         n = len(jobs)
         arr_t = C.c_void_p * max(n, 1)
@@ -487,8 +490,10 @@ class SimulationBatch(_Object):
         seqs = arr_t(*[j[1].ptr for j in jobs])
         trajs = arr_t(*[None if j[2] is None else j[2].ptr for j in jobs])
         coils = arr_t(*[None if c is None else c.ptr for c in coil_arrays])
-        ptr = lib.compas_b200_make_batch(context.ptr, n, C.cast(params, _P), C.cast(seqs, _P), C.cast(trajs, _P),
-                                         C.cast(coils, _P), SIGNAL_METHODS[method])
+        flags = None if tangents is None else (C.c_int32 * max(n, 1))(*[int(bool(t)) for t in tangents])
+        ptr = lib.compas_b200_make_batch_tangents(context.ptr, n, C.cast(params, _P), C.cast(seqs, _P),
+                                                  C.cast(trajs, _P), C.cast(coils, _P), SIGNAL_METHODS[method],
+                                                  None if flags is None else C.cast(flags, _P))
         super().__init__(ptr, (list(jobs), coil_arrays))
         self.context = context
         self.jobs = list(jobs)
@@ -501,6 +506,13 @@ class SimulationBatch(_Object):
         """Enqueue every job on the context's stream (returns without waiting)."""
         if library().compas_b200_batch_run(self.ptr) != 0:
             _check(None, "compas_b200_batch_run!")
+
+    def derivative(self, job: int, field) -> CompasArray:
+        """∂echos/∂T1 ("T1" / 0) or ∂echos/∂T2 ("T2" / 1) of a job made with tangents."""
+        f = {"T1": 0, "T2": 1}.get(field, field)
+        ptr = library().compas_b200_batch_derivative(self.ptr, int(job), int(f))
+        _check(ptr, "compas_b200_batch_derivative!")
+        return CompasArray(self.context, ptr, np.complex64, (self.jobs[job][1].nreadouts, self.jobs[job][0].nvoxels))
 
     def echos(self, job: int) -> CompasArray:
         params, seq = self.jobs[job][0], self.jobs[job][1]

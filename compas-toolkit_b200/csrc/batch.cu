@@ -5,7 +5,8 @@
 // idle and pays one launch chain per job. Here a batch is planned once:
 //
 //  * simulation: jobs are grouped by kernel layout — the layout each job would get alone, so
-//    the per-job bits do not depend on the batch. Every group is ONE persistent work-queue
+//    the per-job bits do not depend on the batch (jobs with tangents in groups of their own, on
+//    the tangent kernels). Every group is ONE persistent work-queue
 //    launch: CTAs (as many as fit on the GPU) take (job, voxel tile) items through an atomic
 //    counter; items are ordered longest job first so the last wave is short. FISP groups run on
 //    the context's stream, pSSFP groups on a second stream, so the two families overlap (a
@@ -74,6 +75,7 @@ struct SimulationBatch::Impl {
     std::vector<SimulationJob> jobs;
     Precision prec = Precision::SplitBF16;
     std::vector<Array<cfloat, 2>> echos;
+    std::vector<Array<cfloat, 2>> dT1, dT2;  // tangent jobs only (empty otherwise)
     std::vector<Array<cfloat, 3>> signals;
     Array<int> heads;  // one work-queue counter per simulation group
     cudaStream_t side = nullptr;
@@ -81,6 +83,7 @@ struct SimulationBatch::Impl {
 
     struct SimGroup {
         bool fisp;
+        bool tangent;              // value and T1/T2 tangents (tangent layouts for FISP)
         int config, warps, cover;  // layout, warps (FISP), max_state / nz
         Array<unsigned char> args;
         Array<unsigned char> items;
@@ -121,27 +124,34 @@ struct SimulationBatch::Impl {
 void SimulationBatch::Impl::plan_simulation(Family& fam, bool fisp, const std::vector<int>& members) {
     // group by the launch the job would get alone
     struct Key {
-        int config, warps, cover;
+        int tangent, config, warps, cover;
         bool operator<(const Key& o) const {
-            return std::tie(config, warps, cover) < std::tie(o.config, o.warps, o.cover);
+            return std::tie(tangent, config, warps, cover) < std::tie(o.tangent, o.config, o.warps, o.cover);
         }
     };
     std::vector<std::pair<Key, int>> keyed;
     for (int j : members) {
         const auto& job = jobs[size_t(j)];
         if (job.parameters.nvoxels == 0) continue;
+        const int tan = job.tangents ? 1 : 0;
         if (fisp) {
             const auto& seq = std::get<FISPSequence>(job.sequence);
             const int P = int(seq.sliceprofiles.size(0));
-            const FispLaunch L = tuned_fisp_launch(seq.max_state, job.parameters.nvoxels, P);
-            const FispLaunch D = L.config < 0 ? fisp_default_launch(seq.max_state, job.parameters.nvoxels, P) : L;
-            keyed.push_back({Key {D.config, std::max(1, std::min(D.warps, 8)), seq.max_state}, j});
+            const int V = job.parameters.nvoxels;
+            FispLaunch D;
+            if (tan) {
+                D = tuned_fisp_tangent_launch(seq.max_state, V, P);
+            } else {
+                const FispLaunch L = tuned_fisp_launch(seq.max_state, V, P);
+                D = L.config < 0 ? fisp_default_launch(seq.max_state, V, P) : L;
+            }
+            keyed.push_back({Key {tan, D.config, std::max(1, std::min(D.warps, 8)), seq.max_state}, j});
         } else {
             const auto& seq = std::get<pSSFPSequence>(job.sequence);
             const int nz = int(seq.z.size());
             const PssfpLaunch L = tuned_pssfp_launch(nz, job.parameters.nvoxels);
             const PssfpLaunch D = L.config < 0 ? pssfp_default_launch(nz, job.parameters.nvoxels) : L;
-            keyed.push_back({Key {D.config, 0, nz}, j});
+            keyed.push_back({Key {tan, D.config, 0, nz}, j});
         }
     }
     std::stable_sort(keyed.begin(), keyed.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
@@ -164,18 +174,24 @@ void SimulationBatch::Impl::plan_simulation(Family& fam, bool fisp, const std::v
         std::stable_sort(js.begin(), js.end(), [&](int a, int b) { return cost(a) > cost(b); });
         SimGroup g;
         g.fisp = fisp;
+        g.tangent = key.tangent != 0;
         g.config = key.config;
         g.warps = key.warps;
         g.cover = key.cover;
         std::vector<int> items;
         if (fisp) {
             std::vector<kernels::FispArgs> args;
-            const int vb = fisp_tile_voxels(FispLaunch {key.config, key.warps});
+            const FispLaunch L {key.config, key.warps};
+            const int vb = g.tangent ? fisp_tangent_tile_voxels(L) : fisp_tile_voxels(L);
             for (size_t q = 0; q < js.size(); q++) {
                 const auto& job = jobs[size_t(js[q])];
                 const auto& seq = std::get<FISPSequence>(job.sequence);
                 const int V = job.parameters.nvoxels;
                 args.push_back(fisp_args(ctx, job.parameters, 0, V, seq, echos[size_t(js[q])].data(), V));
+                if (g.tangent) {
+                    args.back().dT1 = reinterpret_cast<float2*>(dT1[size_t(js[q])].data());
+                    args.back().dT2 = reinterpret_cast<float2*>(dT2[size_t(js[q])].data());
+                }
                 for (int t = 0; t < div_ceil(V, vb); t++) {
                     items.push_back(int(q));
                     items.push_back(t);
@@ -190,6 +206,10 @@ void SimulationBatch::Impl::plan_simulation(Family& fam, bool fisp, const std::v
                 const auto& seq = std::get<pSSFPSequence>(job.sequence);
                 const int V = job.parameters.nvoxels;
                 args.push_back(pssfp_args(ctx, job.parameters, 0, V, seq, echos[size_t(js[q])].data(), V));
+                if (g.tangent) {
+                    args.back().dT1 = reinterpret_cast<float2*>(dT1[size_t(js[q])].data());
+                    args.back().dT2 = reinterpret_cast<float2*>(dT2[size_t(js[q])].data());
+                }
                 for (int t = 0; t < div_ceil(V, vb); t++) {
                     items.push_back(int(q));
                     items.push_back(t);
@@ -333,9 +353,15 @@ void SimulationBatch::Impl::plan_signal(Family& fam, const std::vector<int>& mem
 void SimulationBatch::Impl::enqueue(const Family& fam, cudaStream_t stream, int* head_base) const {
     const int dev = ctx.device();
     for (const auto& g : fam.sims) {
-        if (g.fisp)
+        if (g.fisp && g.tangent)
+            launch_fisp_tangent_queue(stream, dev, FispLaunch {g.config, g.warps}, g.cover,
+                                      as<kernels::FispArgs>(g.args), as<int2>(g.items), g.nitems, head_base + g.head);
+        else if (g.fisp)
             launch_fisp_queue(stream, dev, FispLaunch {g.config, g.warps}, g.cover, as<kernels::FispArgs>(g.args),
                               as<int2>(g.items), g.nitems, head_base + g.head);
+        else if (g.tangent)
+            launch_pssfp_tangent_queue(stream, dev, PssfpLaunch {g.config}, g.cover, as<kernels::PssfpArgs>(g.args),
+                                       as<int2>(g.items), g.nitems, head_base + g.head);
         else
             launch_pssfp_queue(stream, dev, PssfpLaunch {g.config}, g.cover, as<kernels::PssfpArgs>(g.args),
                                as<int2>(g.items), g.nitems, head_base + g.head);
@@ -385,6 +411,13 @@ SimulationBatch::SimulationBatch(const CompasContext& ctx, std::vector<Simulatio
             nreadouts = int(std::get<pSSFPSequence>(job.sequence).RF_train.size());
         }
         im.echos.emplace_back(std::array<int64_t, 2> {nreadouts, V}, dev, ctx.stream());
+        if (job.tangents) {
+            im.dT1.emplace_back(std::array<int64_t, 2> {nreadouts, V}, dev, ctx.stream());
+            im.dT2.emplace_back(std::array<int64_t, 2> {nreadouts, V}, dev, ctx.stream());
+        } else {
+            im.dT1.emplace_back();
+            im.dT2.emplace_back();
+        }
         if (std::holds_alternative<std::monostate>(job.trajectory)) {
             im.signals.emplace_back();
         } else {
@@ -451,6 +484,13 @@ const Array<cfloat, 2>& SimulationBatch::echos(int job) const {
 const Array<cfloat, 3>& SimulationBatch::signal(int job) const {
     if (job < 0 || job >= size()) COMPAS_ERROR("job index out of range");
     return m_impl->signals[size_t(job)];
+}
+
+const Array<cfloat, 2>& SimulationBatch::derivative(int job, int field) const {
+    if (job < 0 || job >= size()) COMPAS_ERROR("job index out of range");
+    if (!m_impl->jobs[size_t(job)].tangents) COMPAS_ERROR("the job was not planned with tangents");
+    if (field != 0 && field != 1) COMPAS_ERROR("derivatives are kept for T1 (0) and T2 (1)");
+    return field == 0 ? m_impl->dT1[size_t(job)] : m_impl->dT2[size_t(job)];
 }
 
 }  // namespace compas

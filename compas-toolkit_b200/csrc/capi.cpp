@@ -556,6 +556,15 @@ int compas_b200_pssfp_launch_choice(int nz, int64_t nvoxels) {
 compas_object* compas_b200_make_batch(const compas_context* context, int njobs, const compas_object* const* parameters,
                                       const compas_object* const* sequences, const compas_object* const* trajectories,
                                       const compas_array* const* coils, int method) {
+    return compas_b200_make_batch_tangents(context, njobs, parameters, sequences, trajectories, coils, method, nullptr);
+}
+
+compas_object* compas_b200_make_batch_tangents(const compas_context* context, int njobs,
+                                               const compas_object* const* parameters,
+                                               const compas_object* const* sequences,
+                                               const compas_object* const* trajectories,
+                                               const compas_array* const* coils, int method,
+                                               const int32_t* tangents) {
     return guarded([&] {
         const auto& ctx = ctx_of(context);
         if (njobs < 0) throw compas::CompasException("negative job count");
@@ -579,6 +588,7 @@ compas_object* compas_b200_make_batch(const compas_context* context, int njobs, 
                 if (!coils) throw compas::CompasException("null coils array");
                 job.coil_sensitivities = array_of<cfloat, 2>(coils[i], "coils");
             }
+            job.tangents = tangents && tangents[i] != 0;
             jobs.push_back(std::move(job));
         }
         return new_obj(compas::SimulationBatch(ctx, std::move(jobs), signal_method(method)));
@@ -745,6 +755,11 @@ int compas_b200_gauss_newton_graph_kernels(const compas_object* gn) {
     t_has_error = false;
     const int n = guarded([&] { return unwrap<compas::GaussNewtonStep>(gn).kernels_per_iteration(); });
     return t_has_error ? -1 : n;
+}
+
+compas_array* compas_b200_batch_derivative(const compas_object* batch, int job, int field) {
+    return guarded(
+        [&] { return new_array(compas::Array<cfloat, 2>(unwrap<compas::SimulationBatch>(batch).derivative(job, field))); });
 }
 
 compas_array* compas_b200_batch_signal(const compas_object* batch, int job) {

@@ -483,6 +483,30 @@ __global__ void __launch_bounds__(256, 1) fisp_tangent_kernel(FispArgs a) {
     fisp_tile<K, G, kOneHotZeroing<K, G>, true>(a, blockIdx.x, samples);
 }
 
+// Work-queue form of fisp_tangent_kernel for batches (same items and order as fisp_queue_kernel).
+// Every tangent layout zeroes with the one-hot test, as the one-simulation tangent kernel does, so
+// both give the same bits.
+template<int K, int G>
+__global__ void __launch_bounds__(256, 1) fisp_tangent_queue_kernel(const FispArgs* __restrict__ jobs,
+                                                                    const int2* __restrict__ items, int nitems,
+                                                                    int* __restrict__ head) {
+    static_assert(kOneHotZeroing<K, G>, "tangent layouts use one-hot zeroing");
+    extern __shared__ float2 samples[];
+    __shared__ FispArgs job;
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(head, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= nitems) break;
+        const int2 w = items[it];
+        if (threadIdx.x == 0) job = jobs[w.x];
+        __syncthreads();
+        fisp_tile<K, G, true, true>(job, w.y, samples);
+        __syncthreads();
+    }
+}
+
 }  // namespace kernels
 
 // ------------------------------------------------------------------------------------------
@@ -528,15 +552,15 @@ const FispConfig kFispConfigs[] = {
 struct FispTangentConfig {
     int K, G;
     FispKernel fn;
+    FispQueueKernel queue;
 };
+#define COMPAS_FISP_TANGENT(K, G) {K, G, kernels::fisp_tangent_kernel<K, G>, kernels::fisp_tangent_queue_kernel<K, G>}
 const FispTangentConfig kFispTangentConfigs[] = {
-    {1, 1, kernels::fisp_tangent_kernel<1, 1>}, {2, 1, kernels::fisp_tangent_kernel<2, 1>},
-    {4, 1, kernels::fisp_tangent_kernel<4, 1>}, {8, 1, kernels::fisp_tangent_kernel<8, 1>},
-    {2, 4, kernels::fisp_tangent_kernel<2, 4>}, {4, 4, kernels::fisp_tangent_kernel<4, 4>},
-    {7, 4, kernels::fisp_tangent_kernel<7, 4>}, {8, 4, kernels::fisp_tangent_kernel<8, 4>},
-    {4, 8, kernels::fisp_tangent_kernel<4, 8>}, {8, 8, kernels::fisp_tangent_kernel<8, 8>},
-    {8, 16, kernels::fisp_tangent_kernel<8, 16>},
+    COMPAS_FISP_TANGENT(1, 1), COMPAS_FISP_TANGENT(2, 1), COMPAS_FISP_TANGENT(4, 1), COMPAS_FISP_TANGENT(8, 1),
+    COMPAS_FISP_TANGENT(2, 4), COMPAS_FISP_TANGENT(4, 4), COMPAS_FISP_TANGENT(7, 4), COMPAS_FISP_TANGENT(8, 4),
+    COMPAS_FISP_TANGENT(4, 8), COMPAS_FISP_TANGENT(8, 8), COMPAS_FISP_TANGENT(8, 16),
 };
+#undef COMPAS_FISP_TANGENT
 constexpr int kFispTangentConfigCount = int(sizeof(kFispTangentConfigs) / sizeof(kFispTangentConfigs[0]));
 
 }  // namespace
@@ -746,6 +770,29 @@ void launch_fisp_tangent(const CompasContext& ctx, const TissueParameters& param
     allow_smem(reinterpret_cast<const void*>(cfg.fn), smem);
     cfg.fn<<<div_ceil(nvoxels, VB), 32 * W, smem, ctx.stream()>>>(a);
     check_launch("fisp_tangent_kernel");
+}
+
+int fisp_tangent_tile_voxels(FispLaunch L) {
+    COMPAS_CHECK(L.config >= 0 && L.config < kFispTangentConfigCount);
+    return 32 / kFispTangentConfigs[L.config].G;
+}
+
+void launch_fisp_tangent_queue(cudaStream_t stream, int device, FispLaunch L, int max_state,
+                               const kernels::FispArgs* jobs, const int2* items, int nitems, int* head) {
+    if (nitems <= 0) return;
+    COMPAS_CHECK(L.config >= 0 && L.config < kFispTangentConfigCount);
+    const auto& cfg = kFispTangentConfigs[L.config];
+    COMPAS_CHECK(cfg.K * cfg.G >= max_state);
+    const int W = std::max(1, std::min(L.warps, 8));
+    const size_t smem = 3 * size_t(W) * 32 * (32 / cfg.G) * sizeof(float2);
+    DeviceGuard guard(device);
+    allow_smem(reinterpret_cast<const void*>(cfg.queue), smem);
+    int per_sm = 1, sms = 148;
+    COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.queue, 32 * W, smem));
+    COMPAS_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int grid = std::max(1, std::min(nitems, std::max(1, per_sm) * sms));
+    cfg.queue<<<grid, 32 * W, smem, stream>>>(jobs, items, nitems, head);
+    check_launch("fisp_tangent_queue_kernel");
 }
 
 void launch_fisp_queue(cudaStream_t stream, int device, FispLaunch L, int max_state, const kernels::FispArgs* jobs,

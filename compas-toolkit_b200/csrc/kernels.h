@@ -40,6 +40,10 @@ FispLaunch tuned_fisp_tangent_launch(int N, int64_t nvoxels, int P);  // honours
 void launch_fisp_tangent(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
                          const FISPSequence& seq, cfloat* echo, cfloat* dT1, cfloat* dT2, int64_t echo_stride,
                          FispLaunch L);
+int fisp_tangent_tile_voxels(FispLaunch L);  // voxels per work item of tangent layout L
+// work-queue launch over (job, tile) items of FISP tangent jobs (args with dT1 / dT2 set)
+void launch_fisp_tangent_queue(cudaStream_t stream, int device, FispLaunch L, int max_state,
+                               const kernels::FispArgs* jobs, const int2* items, int nitems, int* head);
 
 // ---- pSSFP ------------------------------------------------------------------------------
 struct PssfpLaunch {
@@ -58,6 +62,8 @@ int pssfp_tile_voxels(PssfpLaunch L);
 void launch_pssfp_tangent(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
                           const pSSFPSequence& seq, cfloat* echo, cfloat* dT1, cfloat* dT2, int64_t echo_stride,
                           PssfpLaunch L);
+void launch_pssfp_tangent_queue(cudaStream_t stream, int device, PssfpLaunch L, int nz,
+                                const kernels::PssfpArgs* jobs, const int2* items, int nitems, int* head);
 void launch_pssfp_queue(cudaStream_t stream, int device, PssfpLaunch L, int nz, const kernels::PssfpArgs* jobs,
                         const int2* items, int nitems, int* head);
 

@@ -272,7 +272,8 @@ __global__ void __launch_bounds__(128) pssfp_tangent_kernel(PssfpArgs a) {
 
 // Persistent work-queue kernel for a batch of pSSFP simulations sharing one (ZT, GZ) layout:
 // CTAs of 128 threads take (job, tile) items, longest job first, through an atomic counter.
-template<int ZT, int GZ>
+// TAN: the value and T1/T2 tangents (pssfp_tangent_kernel's work).
+template<int ZT, int GZ, bool TAN = false>
 __global__ void __launch_bounds__(128) pssfp_queue_kernel(const PssfpArgs* __restrict__ jobs,
                                                           const int2* __restrict__ items, int nitems,
                                                           int* __restrict__ head) {
@@ -286,7 +287,7 @@ __global__ void __launch_bounds__(128) pssfp_queue_kernel(const PssfpArgs* __res
         const int2 w = items[it];
         if (threadIdx.x == 0) job = jobs[w.x];
         __syncthreads();
-        pssfp_tile<ZT, GZ>(job, w.y);
+        pssfp_tile<ZT, GZ, TAN>(job, w.y);
         __syncthreads();
     }
 }
@@ -301,36 +302,37 @@ struct PssfpConfig {
     PssfpKernel fn;
     PssfpQueueKernel queue;
     PssfpKernel tangent;
+    PssfpQueueKernel tangent_queue;
 };
 const PssfpConfig kPssfpConfigs[] = {
     {1, 1, kernels::pssfp_kernel<1, 1>, kernels::pssfp_queue_kernel<1, 1>,
-     kernels::pssfp_tangent_kernel<1, 1>},
+     kernels::pssfp_tangent_kernel<1, 1>, kernels::pssfp_queue_kernel<1, 1, true>},
     {2, 1, kernels::pssfp_kernel<2, 1>, kernels::pssfp_queue_kernel<2, 1>,
-     kernels::pssfp_tangent_kernel<2, 1>},
+     kernels::pssfp_tangent_kernel<2, 1>, kernels::pssfp_queue_kernel<2, 1, true>},
     {4, 1, kernels::pssfp_kernel<4, 1>, kernels::pssfp_queue_kernel<4, 1>,
-     kernels::pssfp_tangent_kernel<4, 1>},
+     kernels::pssfp_tangent_kernel<4, 1>, kernels::pssfp_queue_kernel<4, 1, true>},
     {8, 1, kernels::pssfp_kernel<8, 1>, kernels::pssfp_queue_kernel<8, 1>,
-     kernels::pssfp_tangent_kernel<8, 1>},
+     kernels::pssfp_tangent_kernel<8, 1>, kernels::pssfp_queue_kernel<8, 1, true>},
     {9, 4, kernels::pssfp_kernel<9, 4>, kernels::pssfp_queue_kernel<9, 4>,
-     kernels::pssfp_tangent_kernel<9, 4>},
+     kernels::pssfp_tangent_kernel<9, 4>, kernels::pssfp_queue_kernel<9, 4, true>},
     {5, 8, kernels::pssfp_kernel<5, 8>, kernels::pssfp_queue_kernel<5, 8>,
-     kernels::pssfp_tangent_kernel<5, 8>},
+     kernels::pssfp_tangent_kernel<5, 8>, kernels::pssfp_queue_kernel<5, 8, true>},
     {3, 16, kernels::pssfp_kernel<3, 16>, kernels::pssfp_queue_kernel<3, 16>,
-     kernels::pssfp_tangent_kernel<3, 16>},
+     kernels::pssfp_tangent_kernel<3, 16>, kernels::pssfp_queue_kernel<3, 16, true>},
     {2, 32, kernels::pssfp_kernel<2, 32>, kernels::pssfp_queue_kernel<2, 32>,
-     kernels::pssfp_tangent_kernel<2, 32>},
+     kernels::pssfp_tangent_kernel<2, 32>, kernels::pssfp_queue_kernel<2, 32, true>},
     {1, 32, kernels::pssfp_kernel<1, 32>, kernels::pssfp_queue_kernel<1, 32>,
-     kernels::pssfp_tangent_kernel<1, 32>},
+     kernels::pssfp_tangent_kernel<1, 32>, kernels::pssfp_queue_kernel<1, 32, true>},
     {18, 2, kernels::pssfp_kernel<18, 2>, kernels::pssfp_queue_kernel<18, 2>,
-     kernels::pssfp_tangent_kernel<18, 2>},
+     kernels::pssfp_tangent_kernel<18, 2>, kernels::pssfp_queue_kernel<18, 2, true>},
     {4, 4, kernels::pssfp_kernel<4, 4>, kernels::pssfp_queue_kernel<4, 4>,
-     kernels::pssfp_tangent_kernel<4, 4>},
+     kernels::pssfp_tangent_kernel<4, 4>, kernels::pssfp_queue_kernel<4, 4, true>},
     {8, 4, kernels::pssfp_kernel<8, 4>, kernels::pssfp_queue_kernel<8, 4>,
-     kernels::pssfp_tangent_kernel<8, 4>},
+     kernels::pssfp_tangent_kernel<8, 4>, kernels::pssfp_queue_kernel<8, 4, true>},
     {4, 8, kernels::pssfp_kernel<4, 8>, kernels::pssfp_queue_kernel<4, 8>,
-     kernels::pssfp_tangent_kernel<4, 8>},
+     kernels::pssfp_tangent_kernel<4, 8>, kernels::pssfp_queue_kernel<4, 8, true>},
     {12, 4, kernels::pssfp_kernel<12, 4>, kernels::pssfp_queue_kernel<12, 4>,
-     kernels::pssfp_tangent_kernel<12, 4>},
+     kernels::pssfp_tangent_kernel<12, 4>, kernels::pssfp_queue_kernel<12, 4, true>},
 };
 }  // namespace
 
@@ -457,6 +459,19 @@ void launch_pssfp_queue(cudaStream_t stream, int device, PssfpLaunch L, int nz, 
     const int grid = std::max(1, std::min(nitems, std::max(1, per_sm) * sms));
     cfg.queue<<<grid, kPssfpThreads, 0, stream>>>(jobs, items, nitems, head);
     check_launch("pssfp_queue_kernel");
+}
+
+void launch_pssfp_tangent_queue(cudaStream_t stream, int device, PssfpLaunch L, int nz,
+                                const kernels::PssfpArgs* jobs, const int2* items, int nitems, int* head) {
+    if (nitems <= 0) return;
+    const auto& cfg = checked_config(L, nz);
+    DeviceGuard guard(device);
+    int per_sm = 1, sms = 148;
+    COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.tangent_queue, kPssfpThreads, 0));
+    COMPAS_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int grid = std::max(1, std::min(nitems, std::max(1, per_sm) * sms));
+    cfg.tangent_queue<<<grid, kPssfpThreads, 0, stream>>>(jobs, items, nitems, head);
+    check_launch("pssfp_tangent_queue_kernel");
 }
 
 // Value and T1/T2 tangents in one launch, with the value kernel's layout L.

@@ -14,8 +14,9 @@
 //    as one exists, so requests that arrive while others run start at once and their kernels
 //    overlap with the running batches on the device;
 //  * a batch runs every simulation of its requests (the echoes, and the T1+Δ / T2+Δ copies for
-//    the derivatives) as one SimulationBatch — persistent work-queue kernels and batched
-//    signal kernels — then per request the derivative differences, the residual and Jᴴ·r;
+//    the derivatives; with Δ = 0 one tangent pass per request gives exact derivatives instead) as
+//    one SimulationBatch — persistent work-queue kernels and batched signal kernels — then per
+//    request the derivative differences, the residual and Jᴴ·r;
 //  * residency: sequences (with their device tables), trajectories and coil maps are device
 //    objects the client keeps and reuses across requests; echoes and derivatives are kept in
 //    an LRU cache by the request's echo_key, within its own byte budget;
@@ -156,7 +157,7 @@ size_t ServeEngine::Impl::estimate(const ServeRequest& r) const {
     const int64_t R = t.nreadouts, S = t.samples_per_readout, C = r.coil_sensitivities.size(0);
     const bool cart = std::holds_alternative<CartesianTrajectory>(r.trajectory);
     const int64_t echo = 8 * R * V, sig = 8 * C * R * S;
-    int64_t bytes = echo * 3 + 2 * 36 * V;                            // echoes, derivative echoes, T1/T2+Δ copies
+    int64_t bytes = echo * 3 + (opt.delta != 0.0f ? 2 * 36 * V : 0);  // echoes, derivative echoes, T1/T2+Δ copies
     bytes += 2 * sig;                                                  // signal, residual
     bytes += 40 * V + 8 * C * V;                                       // per-voxel tables, coil·w
     if (cart && signal_precision(opt.method) == Precision::SplitBF16) {
@@ -235,9 +236,10 @@ void ServeEngine::Impl::launch(Slot& slot, std::vector<uint64_t> ids) {
         if (const auto* c = std::get_if<CartesianTrajectory>(&r.trajectory)) job.trajectory = *c;
         else job.trajectory = std::get<SpiralTrajectory>(r.trajectory);
         job.coil_sensitivities = r.coil_sensitivities;
+        job.tangents = opt.delta == 0.0f;  // exact derivatives from the simulation pass itself
         main_job[i] = int(jobs.size());
         jobs.push_back(job);
-        {  // derivative simulations at T1 + Δ and T2 + Δ
+        if (!job.tangents) {  // derivative simulations at T1 + Δ and T2 + Δ
             const int V = r.parameters.nvoxels;
             for (int field = 0; field < 2; field++) {
                 Array<float, 2> p({TissueParameterField::NUM_FIELDS, V}, dev, slot.stream);
@@ -278,7 +280,10 @@ void ServeEngine::Impl::launch(Slot& slot, std::vector<uint64_t> ids) {
         if (main_job[i] >= 0) {
             run->echos[i] = run->batch->echos(main_job[i]);
             run->signals[i] = run->batch->signal(main_job[i]);
-            if (d1_job[i] >= 0) {
+            if (opt.delta == 0.0f) {
+                run->dT1[i] = run->batch->derivative(main_job[i], 0);
+                run->dT2[i] = run->batch->derivative(main_job[i], 1);
+            } else if (d1_job[i] >= 0) {
                 run->dT1[i] = run->batch->echos(d1_job[i]);
                 run->dT2[i] = run->batch->echos(d2_job[i]);
                 for (Array<cfloat, 2>* d : {&run->dT1[i], &run->dT2[i]}) {

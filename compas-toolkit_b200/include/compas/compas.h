@@ -484,6 +484,7 @@ struct SimulationJob {
     std::variant<FISPSequence, pSSFPSequence> sequence;
     std::variant<std::monostate, CartesianTrajectory, SpiralTrajectory> trajectory;
     Array<cfloat, 2> coil_sensitivities;  // [ncoils][nvoxels]
+    bool tangents = false;  // also ∂echos/∂T1 and ∂echos/∂T2 (forward-mode tangents): derivative()
 };
 
 // Many jobs of uneven size in a handful of launches: every FISP job of one launch layout runs
@@ -502,6 +503,9 @@ class SimulationBatch: public Object {
     int size() const;
     const Array<cfloat, 2>& echos(int job) const;   // [nreadouts][nvoxels]
     const Array<cfloat, 3>& signal(int job) const;  // [ncoils][nreadouts][ns]; empty without trajectory
+    // ∂echos/∂T1 (field 0) or ∂echos/∂T2 (field 1) of a job with `tangents` set (the same bits as
+    // simulate_magnetization_tangents for it alone)
+    const Array<cfloat, 2>& derivative(int job, int field) const;
     const char* name() const override { return "compas::SimulationBatch"; }
 
     struct Impl;
@@ -546,7 +550,7 @@ struct ServeOptions {
     int max_batch_requests = 16;                      // requests admitted into one batch
     size_t echo_cache_bytes = size_t(16) << 30;      // resident echoes/derivatives (within the budget)
     SimulateSignalMethod method = SimulateSignalMethod::MatmulFast;
-    float delta = DEFAULT_FINITE_DIFFERENCE_DELTA;
+    float delta = DEFAULT_FINITE_DIFFERENCE_DELTA;  // forward-difference step; 0: exact tangents
 };
 
 struct ServeStats {

@@ -214,6 +214,17 @@ COMPAS_API compas_object* compas_b200_make_batch(const compas_context* ctx, int 
 COMPAS_API int compas_b200_batch_run(const compas_object* batch);
 /* New array handles sharing the batch's result storage (valid while the batch exists or
  * until released with compas_destroy_array; the next run overwrites them). */
+/* As compas_b200_make_batch; tangents[i] != 0 (or tangents == NULL for none) also computes job
+ * i's exact derivatives ∂echos/∂T1, ∂echos/∂T2 in the same pass (forward-mode tangents, the bits of
+ * compas_b200_simulate_magnetization_tangents for it alone), read with compas_b200_batch_derivative. */
+COMPAS_API compas_object* compas_b200_make_batch_tangents(const compas_context* ctx, int njobs,
+                                                          const compas_object* const* parameters,
+                                                          const compas_object* const* sequences,
+                                                          const compas_object* const* trajectories,
+                                                          const compas_array* const* coils, int method,
+                                                          const int32_t* tangents);
+/* field 0: ∂echos/∂T1, 1: ∂echos/∂T2 of a job made with tangents ([nreadouts][nvoxels]) */
+COMPAS_API compas_array* compas_b200_batch_derivative(const compas_object* batch, int job, int field);
 COMPAS_API compas_array* compas_b200_batch_echos(const compas_object* batch, int job);
 COMPAS_API compas_array* compas_b200_batch_signal(const compas_object* batch, int job);
 
@@ -244,8 +255,9 @@ COMPAS_API int compas_b200_gauss_newton_graph_kernels(const compas_object* gn);
  * `memory_budget_gb`, grouped into batches (at most `max_batch_requests` each, at most
  * `max_inflight_batches` on the device at once) and give residual, objective and (Cartesian)
  * gradient J^H.r. A nonzero echo_key lets requests with equal parameters and sequence share
- * resident echoes (`echo_cache_gb`). `method` is a SimulateSignalMethod value. Released with
- * compas_destroy_object, which finishes queued requests first. */
+ * resident echoes (`echo_cache_gb`). `method` is a SimulateSignalMethod value. `delta` is the
+ * forward-difference step of the derivatives; 0 takes exact forward-mode tangents from the
+ * simulation pass. Released with compas_destroy_object, which finishes queued requests first. */
 COMPAS_API compas_object* compas_b200_make_server(const compas_context* ctx, double memory_budget_gb,
                                                   int max_inflight_batches, int max_batch_requests,
                                                   double echo_cache_gb, int method, float delta);

@@ -81,3 +81,31 @@ def test_batch_rejects_mismatched_trajectory(ctx):
     wrong = cb.CartesianTrajectory.from_dict(ctx, W.cartesian(d["ntr"] + 1, 8, 22.4, 5e-6, 8))
     with pytest.raises(cb.CompasError, match="readouts"):
         cb.SimulationBatch(ctx, [(params, seq, wrong, coils)])
+
+
+def test_batch_tangent_jobs_match_one_job_calls_bitwise(ctx):
+    # jobs flagged for tangents run on the tangent work-queue kernels in groups of their own; their
+    # echoes and derivatives are the bits of simulate_magnetization_tangents for each alone, the
+    # other jobs keep the bits of simulate_magnetization
+    import compas_b200 as cb
+
+    dicts = _mixed_jobs()
+    jobs = [cb.job_from_dict(ctx, d) for d in dicts]
+    flags = [j % 2 == 0 for j in range(len(jobs))]
+    batch = cb.SimulationBatch(ctx, jobs, method="MatmulFast", tangents=flags)
+    batch.run()
+    ctx.synchronize()
+    for j, (params, seq, traj, coils) in enumerate(jobs):
+        if flags[j]:
+            t = cb.simulate_magnetization_tangents(ctx, params, seq)
+            echos = t["echos"]
+            for f in ("T1", "T2"):
+                assert np.array_equal(batch.derivative(j, f).to_numpy(), t[f].to_numpy()), (j, f)
+        else:
+            echos = cb.simulate_magnetization(ctx, params, seq)
+            with pytest.raises(cb.CompasError):
+                batch.derivative(j, "T1")
+        assert np.array_equal(batch.echos(j).to_numpy(), echos.to_numpy()), (j, "echos")
+        if traj is not None:
+            s_ref = cb.magnetization_to_signal(ctx, echos, params, traj, coils, method="MatmulFast").to_numpy()
+            assert np.array_equal(batch.signal(j).to_numpy(), s_ref), (j, "signal")

@@ -118,3 +118,23 @@ def test_echo_key_reuses_resident_echoes(env):
     t2 = eng.submit(*objs[i], data[i], echo_key=77)
     _check_same(cb, eng, t2, alone[i], "cached")
     assert eng.stats()["echo_cache_hits"] == 1
+
+
+def test_exact_derivative_requests_match_alone_bitwise(env):
+    # delta = 0: each request's simulation is one tangent pass (the exact ∂/∂T1, ∂/∂T2); the
+    # residual and gradient equal the one-request operations with simulate_magnetization_tangents
+    cb, ctx, dicts, objs, data, _ = env
+    ref = []
+    for (params, seq, traj, coils), d in zip(objs, dicts):
+        t = cb.simulate_magnetization_tangents(ctx, params, seq)
+        s = cb.magnetization_to_signal(ctx, t["echos"], params, traj, coils, method="MatmulFast")
+        obj, diff = cb.compute_residual(ctx, d["data"], s)
+        g = cb.compute_jacobian_hermitian(ctx, t["echos"], {"T1": t["T1"], "T2": t["T2"]}, params, traj, coils,
+                                          diff, method="GemmFast").to_numpy()
+        ref.append({"objective": obj, "residual": diff.to_numpy(), "gradient": g})
+    eng = cb.ServeEngine(ctx, memory_budget_gb=8.0, max_inflight_batches=2, max_batch_requests=4, delta=0.0)
+    tickets = [eng.submit(*objs[i], data[i]) for i in range(len(dicts))]
+    for i, t in enumerate(tickets):
+        _check_same(cb, eng, t, ref[i], i)
+        eng.release(t)
+    assert eng.stats()["failed"] == 0
