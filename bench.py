@@ -428,7 +428,8 @@ def batched(cb, ctx, stream, args, rank):
 
 def served(cb, ctx, args):
     """Served request stream: Poisson arrivals at each rate of reconstruction requests (simulate,
-    FD derivative simulations, signal, residual, Jᴴ·r) drawn from 12
+    FD derivative simulations — or one exact tangent pass in the delta = 0 run — signal, residual,
+    Jᴴ·r) drawn from 12
     distinct requests (voxels logU[4k,200k], coils U{4..16}, FISP/pSSFP, Cartesian/spiral, TRs
     U{400..1120}) whose sequences, trajectories, coils and data stay resident; HBM budget 150 GB.
     Latency = submit -> results complete on the device, measured by the engine."""
@@ -452,15 +453,15 @@ def served(cb, ctx, args):
 
     warmed = set()
 
-    def stream_run(rate, method, nreq, echo_keys):
+    def stream_run(rate, method, nreq, echo_keys, delta=1e-4):
         eng = cb.ServeEngine(ctx, memory_budget_gb=150.0, max_inflight_batches=4, max_batch_requests=16,
-                             method=method)
-        if method not in warmed:  # first use of each kernel family and of every sequence table
+                             method=method, delta=delta)
+        if (method, delta) not in warmed:  # first use of each kernel family and of every sequence table
             for t in [eng.submit(*o) for o in objs]:
                 eng.wait(t)
                 eng.release(t)
             eng.reset_stats()
-            warmed.add(method)
+            warmed.add((method, delta))
         picks = rng.integers(0, len(objs), nreq)
         gaps = rng.exponential(1.0 / rate, nreq)
         tickets = [None] * nreq
@@ -487,6 +488,7 @@ def served(cb, ctx, args):
         st = eng.stats()
         done_vtr = float(sum(vtr[int(i)] for i in picks))
         return {"rate_per_s": rate, "method": method, "requests": nreq, "echo_reuse": echo_keys,
+                "derivatives": "exact tangents" if delta == 0 else f"forward differences, step {delta}",
                 "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
                 "voxel_tr_per_s": done_vtr / wall, "requests_per_s": nreq / wall, "batches": st["batches"],
                 "max_concurrent_batches": st["max_concurrent_batches"], "peak_gb": st["peak_bytes"] / 2 ** 30,
@@ -497,6 +499,7 @@ def served(cb, ctx, args):
         out["runs"].append(stream_run(r, "MatmulFast", args.serve_requests, False))
     out["runs"].append(stream_run(rates[len(rates) // 2], "Direct", args.serve_requests, False))
     out["runs"].append(stream_run(rates[-1], "MatmulFast", args.serve_requests, True))
+    out["runs"].append(stream_run(rates[len(rates) // 2], "MatmulFast", args.serve_requests, False, delta=0.0))
     return out
 
 
