@@ -682,8 +682,11 @@ size_t fisp_smem_bytes(const FispConfig& cfg, int W) {
     return size_t(W) * 32 * (32 / cfg.G) * sizeof(float2);  // ≤ 64 KB (W ≤ 8)
 }
 
+// Opt in to `smem` bytes of dynamic shared memory. Without the attribute a launch may use at most
+// 48 KB minus the kernel's static shared memory (the work-queue kernels keep their job's argument
+// block there), so the attribute is set from 40 KB on.
 void allow_smem(const void* fn, size_t smem) {
-    if (smem > 48 * 1024)
+    if (smem > 40 * 1024)
         COMPAS_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
 }
 

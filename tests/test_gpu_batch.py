@@ -90,8 +90,13 @@ def test_batch_tangent_jobs_match_one_job_calls_bitwise(ctx):
     import compas_b200 as cb
 
     dicts = _mixed_jobs()
+    # the MR-STAT sequence (25 states, 35 positions: 8 warps, 48 KB of dynamic shared memory in the
+    # tangent queue kernel beside its static argument block) on a few voxels
+    m = W.mrstat(n_side=20, ntr=64)
+    dicts.append({"kind": "fisp", "params": m["params"], "seq": m["seq"], "traj": m["traj"], "coils": m["coils"]})
     jobs = [cb.job_from_dict(ctx, d) for d in dicts]
     flags = [j % 2 == 0 for j in range(len(jobs))]
+    flags[-1] = True
     batch = cb.SimulationBatch(ctx, jobs, method="MatmulFast", tangents=flags)
     batch.run()
     ctx.synchronize()
