@@ -79,7 +79,17 @@ class ClockSampler:
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
-        time.sleep(0.3)
+        # start timing only once nvidia-smi is polling: its start-up (NVML initialisation) takes
+        # the driver for up to a second and must not fall inside the timed region
+        deadline = time.perf_counter() + 5.0
+        while self.proc is not None and time.perf_counter() < deadline:
+            try:
+                if Path(self.path).read_text().count("\n") >= 1:
+                    break
+            except OSError:
+                pass
+            time.sleep(0.05)
+        time.sleep(0.1)
         return self
 
     def __exit__(self, *exc):
