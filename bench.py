@@ -366,6 +366,7 @@ def main():
         out["jacobian"] = jacobian_products(cb, ctx, stream, args, peaks, rank)
     if args.batch_jobs > 0:
         out["batched"] = batched(cb, ctx, stream, args, rank)
+    out["elementwise"] = elementwise(cb, ctx, stream, w, params, seq, traj, peaks)
     if not args.no_gn:
         out["derivatives"] = derivatives(cb, ctx, stream, args, rank)
         out["gauss_newton"] = gauss_newton(cb, ctx, stream, args, rank)
@@ -511,6 +512,53 @@ def served(cb, ctx, args):
     out["runs"].append(stream_run(rates[-1], "MatmulFast", args.serve_requests, True))
     out["runs"].append(stream_run(rates[len(rates) // 2], "MatmulFast", args.serve_requests, False, delta=0.0))
     return out
+
+
+def elementwise(cb, ctx, stream, w, params, seq, traj, peaks):
+    """The HBM-bound operations of the path, against the measured HBM copy bandwidth:
+    phase_encoding of the MR-STAT echoes [1120][50176] (read + write 8 B per element, through the
+    public API) and the residual diff = lhs - rhs, Σ|diff|² over 2^24 complex values (read 16 B,
+    write 8 B per element; the allocation-free entry point on caller-owned buffers, since the
+    public one returns the objective to the host). Calls are enqueued behind a 20 ms spin kernel,
+    so the timed span holds the kernels only, not the host's per-call overhead."""
+    import torch
+
+    echos = cb.simulate_magnetization(ctx, params, seq)
+    ctx.synchronize()
+    R, V = echos.shape
+    reps = 5
+
+    def gpu_ms(fn):
+        fn()
+        ctx.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            torch.cuda._sleep(40_000_000)
+            e0.record(stream)
+            keep = [fn() for _ in range(reps)]
+            e1.record(stream)
+        ctx.synchronize()
+        del keep
+        return e0.elapsed_time(e1) / reps
+
+    n_pe = R * V
+    pe_ms = gpu_ms(lambda: cb.phase_encoding(ctx, echos, params, traj))
+    n = 1 << 24
+    g = torch.Generator(device="cuda").manual_seed(9)
+    a = torch.randn(2 * n, device="cuda", generator=g)
+    b = torch.randn(2 * n, device="cuda", generator=g)
+    diff = torch.empty_like(a)
+    obj = torch.empty(1, device="cuda")
+    fn = cb.library().compas_b200_compute_residual_noalloc
+    res_ms = gpu_ms(lambda: fn(ctx.device, a.data_ptr(), b.data_ptr(), diff.data_ptr(), obj.data_ptr(), n,
+                               ctx.stream or None))
+    hbm = peaks["hbm_gbs"]
+    pe_gbs = 16.0 * n_pe / (pe_ms / 1e3) / 1e9
+    res_gbs = 24.0 * n / (res_ms / 1e3) / 1e9
+    return {"phase_encoding": {"elements": n_pe, "ms": pe_ms, "algorithmic_bytes": 16.0 * n_pe, "gbs": pe_gbs,
+                               "frac_of_hbm": pe_gbs / hbm},
+            "residual": {"elements": n, "ms": res_ms, "algorithmic_bytes": 24.0 * n, "gbs": res_gbs,
+                         "frac_of_hbm": res_gbs / hbm}}
 
 
 def reference_kernels_gpu(cb, ctx, stream, w, sim_ms, args):

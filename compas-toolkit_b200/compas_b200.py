@@ -70,6 +70,7 @@ _SIGS = {
     "compas_b200_array_device_ptr": ([_P], _P),
     "compas_b200_array_rank": ([_P], _I),
     "compas_b200_array_extent": ([_P, _I], _I64),
+    "compas_b200_compute_residual_noalloc": ([_I, _P, _P, _P, _P, _I64, _P], _I),
     "compas_b200_launch_count": ([], C.c_uint64),
     "compas_b200_set_fisp_launch": ([_I, _I], None),
     "compas_b200_set_pssfp_launch": ([_I], None),

@@ -10,8 +10,9 @@
 //
 // Limits and sharing:
 //  * the scratch holds 65536 partial sums (256 KB, resident on every GPU that loads the library
-//    until the process exits); one partial per block of 256 elements bounds n at 16,777,216
-//    complex values — larger n is rejected with an error;
+//    until the process exits); the kernels run the allocating entry point's grid-stride launch of
+//    at most 1024 blocks, and n is bounded at 16,777,216 complex values (larger n is rejected with
+//    an error, the limit callers were given);
 //  * every call on a device uses the same scratch and leaves its partial sums in it; calls whose
 //    work overlaps on the GPU (different streams, or threads without ordering) race on it and must
 //    be serialised by the caller;
@@ -22,6 +23,7 @@
 #include <sstream>
 
 #include "common.cuh"
+#include "kernels.h"
 
 namespace compas {
 namespace kernels {
@@ -80,7 +82,9 @@ void residual_noalloc(int device, const cfloat* lhs, const cfloat* rhs, cfloat* 
         COMPAS_CUDA_CHECK(cudaMemsetAsync(objective, 0, sizeof(float), stream));
         return;
     }
-    const int blocks = int((n + kBlock - 1) / kBlock);  // ≤ kScratchPartials by the check above
+    // the allocating entry point's grid (grid-stride, at most 1024 blocks): the same kernels in the
+    // same order, so diff and objective are the same bits, and the scratch holds every partial
+    const int blocks = residual_partial_count(n);
     kernels::residual_kernel<<<blocks, kBlock, 0, stream>>>(reinterpret_cast<const float2*>(lhs),
                                                             reinterpret_cast<const float2*>(rhs), n,
                                                             reinterpret_cast<float2*>(diff), partials);

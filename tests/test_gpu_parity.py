@@ -357,6 +357,11 @@ def test_phase_encoding(cb, ctx, oracle, workloads):
     echo = workloads.cn(np.random.default_rng(3), (400, 4096))
     got = cb.phase_encoding(ctx, echo, params, traj).to_numpy()
     assert oracle.rel_l2(got, oracle.phase_encoding(echo, w["params"], w["traj"]["k_start"])) < TOL_FP32
+    # an odd voxel count: the elements are the same bits as in the full array
+    odd = 4095
+    p_odd = cb.TissueParameters.from_soa(ctx, np.ascontiguousarray(w["params"][:, :odd]))
+    got_odd = cb.phase_encoding(ctx, np.ascontiguousarray(echo[:, :odd]), p_odd, traj).to_numpy()
+    assert np.array_equal(got_odd, got[:, :odd])
 
 
 def test_residual(cb, ctx, oracle):

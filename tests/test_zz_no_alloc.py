@@ -56,6 +56,7 @@ def test_noalloc_residual_matches_allocating_entry_point_twice(lib_and_ctx):
         assert np.array_equal(diff, diff_ref)
         obj = float(dobj.item())
         assert abs(obj - obj_ref) <= TOL_FP32 * obj_ref, (call, obj, obj_ref)
+        assert obj == obj_ref  # the same launch as the allocating entry point: the same bits
 
 
 def test_noalloc_residual_rejects_sizes_beyond_its_scratch(lib_and_ctx):
