@@ -38,16 +38,19 @@ __global__ void fill_kernel(float* p, int64_t n, float value) {
 }
 
 // echo[r][v]·exp(i y_v Im k_start[r])   (src/trajectories/phase_encoding_kernels.cuh:225-240)
+// One voxel per thread; the CTA rows stride over the readouts, so y is read once per voxel and a
+// few thousand CTAs cover the array.
 __global__ void phase_encoding_kernel(const float2* __restrict__ echo, const float* __restrict__ params,
                                       int64_t pstride, int nvoxels, int nreadouts, const float2* __restrict__ k_start,
                                       float2* __restrict__ out) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    const int r = blockIdx.y * blockDim.y + threadIdx.y;
-    if (v >= nvoxels || r >= nreadouts) return;
-    const float y = params[7 * pstride + v];
-    const float2 f = cis_rad(double(y) * double(k_start[r].y));
-    const int64_t i = int64_t(r) * nvoxels + v;
-    out[i] = cmul(echo[i], f);
+    if (v >= nvoxels) return;
+    const double y = double(params[7 * pstride + v]);
+    for (int r = blockIdx.y; r < nreadouts; r += gridDim.y) {
+        const float2 f = cis_rad(y * double(k_start[r].y));
+        const int64_t i = int64_t(r) * nvoxels + v;
+        out[i] = cmul(echo[i], f);
+    }
 }
 
 // d = lhs - rhs, per-block Σ|d|² (fixed-order tree)   (src/utils/residual_kernels.cuh:73-96)
@@ -111,7 +114,9 @@ void launch_phase_encoding(const CompasContext& ctx, const cfloat* echos, const 
                            int nvoxels, int nreadouts, const cfloat* k_start, cfloat* out) {
     if (int64_t(nvoxels) * nreadouts == 0) return;
     DeviceGuard guard(ctx.device());
-    dim3 block(64, 4), grid(div_ceil(nvoxels, 64), div_ceil(nreadouts, 4));
+    const int cols = div_ceil(nvoxels, 256);
+    const int rows = std::max(1, std::min(nreadouts, div_ceil(148 * 16, cols)));  // ~16 CTAs per SM
+    dim3 block(256), grid(cols, rows);
     kernels::phase_encoding_kernel<<<grid, block, 0, ctx.stream()>>>(
         reinterpret_cast<const float2*>(echos), params, pstride, nvoxels, nreadouts,
         reinterpret_cast<const float2*>(k_start), reinterpret_cast<float2*>(out));
