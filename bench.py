@@ -79,8 +79,8 @@ class ClockSampler:
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
-        # start timing only once nvidia-smi is polling: its start-up (NVML initialisation) takes
-        # the driver for up to a second and must not fall inside the timed region
+        # start timing only once nvidia-smi is polling: its start-up (NVML initialisation) occupies
+        # the NVIDIA kernel driver for up to a second and must not fall inside the timed region
         deadline = time.perf_counter() + 5.0
         while self.proc is not None and time.perf_counter() < deadline:
             try:
