@@ -147,10 +147,23 @@ struct EPG {
             u[0] = g[0];
         } else {
             const unsigned mask = 0xffffffffu;
-            float gx = __shfl_down_sync(mask, g[0].x, 1, G);
-            float gy = __shfl_down_sync(mask, g[0].y, 1, G);
-            float ux = __shfl_up_sync(mask, u[K - 1].x, 1, G);
-            float uy = __shfl_up_sync(mask, u[K - 1].y, 1, G);
+            float gx, gy, ux, uy;
+            if constexpr ((G & (G - 1)) == 0) {
+                gx = __shfl_down_sync(mask, g[0].x, 1, G);
+                gy = __shfl_down_sync(mask, g[0].y, 1, G);
+                ux = __shfl_up_sync(mask, u[K - 1].x, 1, G);
+                uy = __shfl_up_sync(mask, u[K - 1].y, 1, G);
+            } else {
+                // groups that do not divide the warp (32 / G groups, the last 32 % G lanes idle):
+                // explicit neighbour lanes; the values that cross a group boundary are replaced
+                // below, as in the power-of-two case
+                const int lane = threadIdx.x & 31;
+                const int next = min(lane + 1, 31), prev = max(lane - 1, 0);
+                gx = __shfl_sync(mask, g[0].x, next);
+                gy = __shfl_sync(mask, g[0].y, next);
+                ux = __shfl_sync(mask, u[K - 1].x, prev);
+                uy = __shfl_sync(mask, u[K - 1].y, prev);
+            }
 #pragma unroll
             for (int i = 0; i < K - 1; i++) g[i] = g[i + 1];
             g[K - 1] = (sub == G - 1) ? make_float2(0.f, 0.f) : make_float2(gx, gy);
@@ -314,7 +327,11 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
     const int W = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grp = lane / G, sub = lane % G;
-    const int vloc = tile * VB + grp;
+    // a group size that does not divide 32 leaves the last 32 % G lanes without a voxel: they run
+    // alongside (on a clamped voxel) and write nothing
+    constexpr bool kSpareLanes = (32 % G) != 0;
+    const bool writer = sub == 0 && (!kSpareLanes || grp < VB);
+    const int vloc = tile * VB + (kSpareLanes ? min(grp, VB - 1) : grp);
     const bool vok = vloc < a.nvoxels;
     const int64_t vcol = a.voxel_begin + (vok ? vloc : a.nvoxels - 1);
 
@@ -381,7 +398,7 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
                                 st.template shift<ONEHOT>(sub, a.N);
                                 st.excite(make_coefs(tv, B1, c_TR, E1_TR, beta), s1_TR, s2_TR, sub);
                             }
-                            if (sampled && sub == 0) {
+                            if (sampled && writer) {
                                 float2* q = samples + (warp * 32 + j) * VB + grp;
                                 q[0] = cmul(c_TE, st.x.u[0]);
                                 q[plane] = cmul(c_TE, st.d1.u[0]);
@@ -395,10 +412,10 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
                                 st.template shift<ONEHOT>(sub, a.N);
                                 st.excite(make_coefs(tv, B1, c_TR, E1_TR, beta), sub);
                             }
-                            if (sampled && sub == 0) samples[(warp * 32 + j) * VB + grp] = cmul(c_TE, st.u[0]);
+                            if (sampled && writer) samples[(warp * 32 + j) * VB + grp] = cmul(c_TE, st.u[0]);
                         }
                     }
-                } else if (sampled && sub == 0) {
+                } else if (sampled && writer) {
                     for (int j = 0; j < nt; j++)
                         for (int q = 0; q < NQ; q++) samples[q * plane + (warp * 32 + j) * VB + grp] = make_float2(0.f, 0.f);
                 }
@@ -548,7 +565,8 @@ const FispConfig kFispConfigs[] = {
 };
 
 // Tangent layouts: three state vectors per (voxel, position), so at most 8 states per lane
-// (8 × 18 floats); the 25-state MR-STAT case splits over 4 lanes of 7 states.
+// (8 × 18 floats); the 25-state MR-STAT case splits over 5 lanes of 5 states (6 groups per warp,
+// 2 lanes idle) or 4 lanes of 7.
 struct FispTangentConfig {
     int K, G;
     FispKernel fn;
@@ -557,7 +575,8 @@ struct FispTangentConfig {
 #define COMPAS_FISP_TANGENT(K, G) {K, G, kernels::fisp_tangent_kernel<K, G>, kernels::fisp_tangent_queue_kernel<K, G>}
 const FispTangentConfig kFispTangentConfigs[] = {
     COMPAS_FISP_TANGENT(1, 1), COMPAS_FISP_TANGENT(2, 1), COMPAS_FISP_TANGENT(4, 1), COMPAS_FISP_TANGENT(8, 1),
-    COMPAS_FISP_TANGENT(2, 4), COMPAS_FISP_TANGENT(4, 4), COMPAS_FISP_TANGENT(7, 4), COMPAS_FISP_TANGENT(8, 4),
+    COMPAS_FISP_TANGENT(2, 4), COMPAS_FISP_TANGENT(4, 4), COMPAS_FISP_TANGENT(5, 5), COMPAS_FISP_TANGENT(7, 4),
+    COMPAS_FISP_TANGENT(8, 4),
     COMPAS_FISP_TANGENT(4, 8), COMPAS_FISP_TANGENT(8, 8), COMPAS_FISP_TANGENT(8, 16),
 };
 #undef COMPAS_FISP_TANGENT
