@@ -76,3 +76,20 @@ def test_null_handles_are_rejected(cb):
     assert b"null" in lib.compas_last_error()
     assert lib.compas_make_fisp_sequence(None, None, 0.0, 0.0, 0.0, 4, 0.0, 1, 1) is None
     assert lib.compas_last_error() is not None
+
+
+def test_null_handles_are_rejected_by_the_tangent_entry_points(cb):
+    import ctypes as C
+
+    lib = cb.library()
+    outs = [C.c_void_p(), C.c_void_p(), C.c_void_p()]
+    rc = lib.compas_b200_simulate_magnetization_tangents(None, None, None, C.byref(outs[0]), C.byref(outs[1]),
+                                                        C.byref(outs[2]))
+    assert rc == -1 and lib.compas_last_error() is not None
+    assert not any(o.value for o in outs)
+    assert lib.compas_b200_simulate_magnetization_tangents(None, None, None, None, None, None) == -1
+    assert b"null" in lib.compas_last_error()
+    assert lib.compas_b200_batch_derivative(None, 0, 0) is None
+    assert b"null" in lib.compas_last_error()
+    assert lib.compas_b200_make_batch_tangents(None, 0, None, None, None, None, 4, None) is None
+    assert lib.compas_last_error() is not None
