@@ -319,6 +319,14 @@ struct EPGTangent {
 // One voxel tile (VB = 32/G voxels, all slice positions) of a FISP simulation; the CTA's W
 // warps sweep the positions. Shared by the one-simulation kernel (tile = blockIdx.x) and the
 // batched work-queue kernel (tile taken from the queue), so both give bit-identical echoes.
+// TRs per sample chunk: the CTA's warps meet at a barrier once per chunk to sum their positions'
+// samples in shared memory ([W][chunk][VB] per sample plane). The split-lane tangent layouts use
+// 64 TRs, halving their barriers (271 -> 266 ms on the 224² MR-STAT slice); the value kernel keeps
+// 32 (64 measured 0.5 % slower), and so do the one-lane tangent layouts (three planes of 32 voxels
+// per warp would not fit in 227 KB at 64).
+template<int G, bool TAN>
+constexpr int kFispChunk = (TAN && G > 1) ? 64 : 32;
+
 // TAN: also propagate ∂/∂T1 and ∂/∂T2 (EPGTangent) and write them to a.dT1, a.dT2; the
 // value goes through the same operations either way.
 template<int K, int G, bool ONEHOT, bool TAN = false>
@@ -358,7 +366,8 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
     // tangent factors t/T1², t/T2² of each relaxation interval
     const float s1_TR = a.TR * R1 * R1, s2_TR = a.TR * R2 * R2, s2_TE = a.TE * R2 * R2;
     const float s1_TI = a.TI * R1 * R1, s1_W = a.TW * R1 * R1, s2_W = a.TW * R2 * R2;
-    const int plane = W * 32 * VB;  // sample planes: value, ∂/∂T1, ∂/∂T2
+    constexpr int CH = kFispChunk<G, TAN>;
+    const int plane = W * CH * VB;  // sample planes: value, ∂/∂T1, ∂/∂T2
     constexpr int NQ = TAN ? 3 : 1;
 
     const int nrounds = (a.P + W - 1) / W;
@@ -380,8 +389,8 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
                     if (sub == 0) st.z[0].x += 1.0f - E1_TI;
                 }
             }
-            for (int t0 = 0; t0 < a.nTR; t0 += 32) {
-                const int nt = min(32, a.nTR - t0);
+            for (int t0 = 0; t0 < a.nTR; t0 += CH) {
+                const int nt = min(CH, a.nTR - t0);
                 if (pok) {
                     // two TRs per iteration, so the compiler can absorb one of the two dephasing
                     // shifts in register renaming (value kernel 63.6 -> 59.6 ms, tangent kernel
@@ -399,7 +408,7 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
                                 st.excite(make_coefs(tv, B1, c_TR, E1_TR, beta), s1_TR, s2_TR, sub);
                             }
                             if (sampled && writer) {
-                                float2* q = samples + (warp * 32 + j) * VB + grp;
+                                float2* q = samples + (warp * CH + j) * VB + grp;
                                 q[0] = cmul(c_TE, st.x.u[0]);
                                 q[plane] = cmul(c_TE, st.d1.u[0]);
                                 q[2 * plane] = cmul(c_TE, make_float2(fmaf(s2_TE, st.x.u[0].x, st.d2.u[0].x),
@@ -412,12 +421,12 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
                                 st.template shift<ONEHOT>(sub, a.N);
                                 st.excite(make_coefs(tv, B1, c_TR, E1_TR, beta), sub);
                             }
-                            if (sampled && writer) samples[(warp * 32 + j) * VB + grp] = cmul(c_TE, st.u[0]);
+                            if (sampled && writer) samples[(warp * CH + j) * VB + grp] = cmul(c_TE, st.u[0]);
                         }
                     }
                 } else if (sampled && writer) {
                     for (int j = 0; j < nt; j++)
-                        for (int q = 0; q < NQ; q++) samples[q * plane + (warp * 32 + j) * VB + grp] = make_float2(0.f, 0.f);
+                        for (int q = 0; q < NQ; q++) samples[q * plane + (warp * CH + j) * VB + grp] = make_float2(0.f, 0.f);
                 }
                 if (sampled) {
                     __syncthreads();
@@ -427,7 +436,7 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
                         const int qn = e / (nt * VB), j = (e / VB) % nt, gv = e % VB;
                         const int v = tile * VB + gv;
                         float2 acc = make_float2(0.f, 0.f);
-                        for (int w = 0; w < W; w++) acc = cadd(acc, samples[qn * plane + (w * 32 + j) * VB + gv]);
+                        for (int w = 0; w < W; w++) acc = cadd(acc, samples[qn * plane + (w * CH + j) * VB + gv]);
                         if (v < a.nvoxels) {
                             float2* out = qn == 0 ? a.echo : qn == 1 ? a.dT1 : a.dT2;
                             for (int q = 0; q < a.uf; q++) {
@@ -697,8 +706,13 @@ const FispConfig& checked_config(FispLaunch L, int N) {
     return cfg;
 }
 
+// samples of one chunk: [W][chunk][32 / G] complex per plane (kernels::kFispChunk)
 size_t fisp_smem_bytes(const FispConfig& cfg, int W) {
     return size_t(W) * 32 * (32 / cfg.G) * sizeof(float2);  // ≤ 64 KB (W ≤ 8)
+}
+
+size_t fisp_tangent_smem_bytes(int G, int W) {
+    return 3 * size_t(W) * (G == 1 ? 32 : 64) * (32 / G) * sizeof(float2);  // ≤ 192 KB
 }
 
 // Opt in to `smem` bytes of dynamic shared memory. Without the attribute a launch may use at most
@@ -787,7 +801,7 @@ void launch_fisp_tangent(const CompasContext& ctx, const TissueParameters& param
     a.dT2 = reinterpret_cast<float2*>(dT2);
     const int VB = 32 / cfg.G;
     const int W = std::max(1, std::min(L.warps, 8));
-    const size_t smem = 3 * size_t(W) * 32 * VB * sizeof(float2);  // ≤ 192 KB
+    const size_t smem = fisp_tangent_smem_bytes(cfg.G, W);
     DeviceGuard guard(ctx.device());
     allow_smem(reinterpret_cast<const void*>(cfg.fn), smem);
     cfg.fn<<<div_ceil(nvoxels, VB), 32 * W, smem, ctx.stream()>>>(a);
@@ -806,7 +820,7 @@ void launch_fisp_tangent_queue(cudaStream_t stream, int device, FispLaunch L, in
     const auto& cfg = kFispTangentConfigs[L.config];
     COMPAS_CHECK(cfg.K * cfg.G >= max_state);
     const int W = std::max(1, std::min(L.warps, 8));
-    const size_t smem = 3 * size_t(W) * 32 * (32 / cfg.G) * sizeof(float2);
+    const size_t smem = fisp_tangent_smem_bytes(cfg.G, W);
     DeviceGuard guard(device);
     allow_smem(reinterpret_cast<const void*>(cfg.queue), smem);
     int per_sm = 1, sms = 148;
