@@ -458,6 +458,54 @@ def ref_signal_cartesian(echo, params, traj, coils, entries, nthreads=None):
     return _as_complex(out)
 
 
+def cartesian_model_entries(echo_rows, T2, B0, x, y, rho, coils, traj, entries):
+    """FP64 numpy form of the Cartesian forward model that compute_jacobian differentiates,
+    s[c][r][k] = Σ_v C[c][v]·ρ_v·m[r][v]·E_k(v), E_k = exp((k − S/2)(−Δt/T2 + iΘ)),
+    Θ = Re Δk·x + Im Δk·y + 2πΔt·B0 (src/jacobian/product_kernels.cuh:42-63 with
+    include/compas/trajectories/cartesian_view.cuh:65-80; for a real Δk it equals the signal of
+    src/trajectories/signal_kernels.cuh's naive kernel). Every input is float64 / complex128, so a
+    finite difference at a relative step of 1e-4 keeps about 12 digits: echo_rows maps each readout
+    r that occurs in `entries` to its complex128 row m[r][:]; T2, B0, x, y float64 [V]; rho
+    complex128 [V]; coils complex [C][V]. Returns complex128 [len(entries)]."""
+    # Δt and Δk cross the C ABI as float32; round them as the library and the oracle see them
+    S, dt = traj["ns"], float(np.float32(traj["dt"]))
+    dk = complex(traj["dk"])
+    dk = complex(float(np.float32(dk.real)), float(np.float32(dk.imag)))
+    theta = dk.real * x + dk.imag * y + 2 * np.pi * dt * B0
+    arg = -dt / T2 + 1j * theta
+    co = np.asarray(coils, np.complex128)
+    out = np.empty(len(entries), np.complex128)
+    for i, (c, r, k) in enumerate(np.asarray(entries)):
+        E = np.exp((float(k) - 0.5 * S) * arg)
+        out[i] = np.sum(co[c] * rho * echo_rows[int(r)] * E)
+    return out
+
+
+def jacobian_fd_entries(echo, dT1, dT2, params, traj, coils, vec, entries, h=1e-4):
+    """J·v at `entries` by an FP64 central difference of cartesian_model_entries along the direction
+    that the Jacobian's columns are scaled for (product_kernels.cuh:56-60): T1 → T1·(1 + h·w0),
+    T2 → T2·(1 + h·w1), ρ → ρ + h·(w2 + i·w3), with the echoes linearised,
+    m → m + h·(w0·T1·∂m/∂T1 + w1·T2·∂m/∂T2). A complex v splits by linearity into
+    J(Re v) + i·J(Im v), each a real direction. The truncation error is O(h²) ≈ 1e-8 relative."""
+    p = np.asarray(params, np.float64)
+    T1, T2, B0, x, y = p[0], p[1], p[3], p[6], p[7]
+    rho = p[4] + 1j * p[5]
+    rows = sorted({int(r) for r in np.asarray(entries)[:, 1]})
+    m = {r: np.asarray(echo[r], np.complex128) for r in rows}
+    m1 = {r: np.asarray(dT1[r], np.complex128) * T1 for r in rows}
+    m2 = {r: np.asarray(dT2[r], np.complex128) * T2 for r in rows}
+    vec = np.asarray(vec, np.complex128)
+
+    def along(w):
+        def at(s):
+            mm = {r: m[r] + s * h * (w[0] * m1[r] + w[1] * m2[r]) for r in rows}
+            return cartesian_model_entries(mm, T2 * (1 + s * h * w[1]), B0, x, y, rho + s * h * (w[2] + 1j * w[3]),
+                                           coils, traj, entries)
+        return (at(1.0) - at(-1.0)) / (2 * h)
+
+    return along(vec.real) + 1j * along(vec.imag)
+
+
 def derivative_central(simulate, params, seq, field: int, rel_step: float = 1e-4, vidx=None, **kw):
     """∂echo/∂params[field] by an FP64 central difference of an oracle simulation (`fisp` or
     `pssfp`) with a step of rel_step·|p| per voxel (voxels are independent, so all are stepped at

@@ -347,6 +347,23 @@ def test_jacobian_matches_finite_difference_of_signal(oracle, workloads):
     assert oracle.rel_l2(Jv, fd) < 2e-3
 
 
+def test_cartesian_model_matches_signal_and_jacobian(oracle, workloads):
+    # the FP64 model used for the finite-difference checks at full size: for a real Δk it is the
+    # reference's naive Cartesian signal, and its central difference along v is the oracle's J·v
+    rng = np.random.default_rng(19)
+    p, traj, coils, echo, d1, d2 = _small_j(workloads, rng)
+    nc, nr, ns = coils.shape[0], traj["nr"], traj["ns"]
+    ent = np.array([(c, r, k) for c in range(nc) for r in range(nr) for k in range(ns)])
+    q = p.astype(np.float64)
+    rows = {r: echo[r].astype(np.complex128) for r in range(nr)}
+    model = oracle.cartesian_model_entries(rows, q[1], q[3], q[6], q[7], q[4] + 1j * q[5], coils, traj, ent)
+    sig = oracle.signal_cartesian(echo, p, traj, coils, entries=ent)
+    assert oracle.rel_l2(model, sig) < 1e-12
+    v = workloads.cn(rng, (4, p.shape[1]))
+    fd = oracle.jacobian_fd_entries(echo, d1, d2, p, traj, coils, v, ent)
+    assert oracle.rel_l2(fd, oracle.jacobian(echo, d1, d2, p, traj, coils, v, entries=ent)) < 1e-7
+
+
 def _small_spiral_j(workloads, rng, n_side=4, nr=5, ns=7, nc=2):
     p = workloads.tissue(rng, n_side, 20.0)
     nv = n_side * n_side
