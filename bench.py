@@ -9,9 +9,13 @@ Jᴴ·v product are reported beside it in TFLOP/s.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-Under torchrun each rank simulates its own independent slice (weak scaling, no
-collective on the data path); timing is device-side (CUDA events on the library's
-stream), max over ranks.
+Under torchrun (N > 1) the one slice is sharded over the ranks (strong scaling): each rank
+takes its voxel range (compas_b200_voxel_shard), simulates it and contracts it into a partial
+signal, and the library's NCCL communicator sums the partials, so every rank ends the step with
+the full signal (compas_b200_magnetization_to_signal_sharded; the all-reduce is inside the timed
+region). Timing is device-side (CUDA events on the library's stream), max over ranks. The
+secondary blocks (Jacobian products, batches, Gauss-Newton, serving, CPU baseline) run on the
+single-GPU run only.
 """
 from __future__ import annotations
 
@@ -31,6 +35,10 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "compas-toolkit_b200"))
 
 METRIC = "EPG voxel·TR/s"
+# FMA-pipe lane operations the FISP kernel executes per (voxel, slice position, TR) at 25 states in
+# the packed 26-slot layout: 26 per state slot for the excitation update plus the per-TR
+# coefficients, dephasing moves and sample (ncu, profiles/fisp_epg_mrstat.txt)
+FISP_LANE_OPS_PER_ITEM = 732
 UNIT = "voxel·TR/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "sm_max_mhz": 1965.0}
@@ -130,10 +138,11 @@ def dist_env():
     return rank, world, local
 
 
-def cpu_forward_rate(w, seconds_budget=20.0):
-    """One forward step (FISP simulation + Cartesian signal) on the host cores, timed on a voxel
-    sample of the simulation and an entry sample of the signal (each entry a sum over all voxels)
-    and scaled to the full step. Runs the reference's own kernels compiled for the host
+def cpu_forward_rate(w, nv_sample=2048, ne_sample=64):
+    """One forward step (FISP simulation + Cartesian signal) on the host cores, timed on a fixed
+    sample — `nv_sample` voxels evenly spaced over the slice for the simulation and `ne_sample`
+    signal entries (each a sum over all voxels) — and extrapolated to the full step; both arms of
+    the bench use the same sample. Runs the reference's own kernels compiled for the host
     (oracle/_ref/libref_kernels.so: simulate_fisp, sum_signal_cartesian_naive) where they were
     built, else the oracle's FP32 restatement of the reference arithmetic."""
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -152,22 +161,14 @@ def cpu_forward_rate(w, seconds_budget=20.0):
     V = w["params"].shape[1]
     nTR = len(w["seq"]["rf"])
     C_, R, S = w["coils"].shape[0], w["traj"]["nr"], w["traj"]["ns"]
-    nv = 2 * threads
+    nv = min(V, nv_sample)
     idx = np.arange(nv) * (V // nv)
     t0 = time.perf_counter()
     sim(idx)
     t_sim = time.perf_counter() - t0
     per_voxel = t_sim / nv
-    if per_voxel * nv < seconds_budget / 4:  # grow the sample to ~a quarter of the budget
-        nv2 = int(min(V, max(nv, (seconds_budget / 4) / per_voxel)))
-        idx = np.arange(nv2) * (V // nv2)
-        t0 = time.perf_counter()
-        sim(idx)
-        t_sim = time.perf_counter() - t0
-        nv = nv2
-        per_voxel = t_sim / nv
     # signal: a few entries, each a full sum over all voxels
-    ne = 2 * threads
+    ne = ne_sample
     rng = np.random.default_rng(0)
     ent = np.stack([rng.integers(0, C_, ne), rng.integers(0, R, ne), rng.integers(0, S, ne)], 1)
     echo_full = np.zeros((R, V), np.complex64)
@@ -180,8 +181,9 @@ def cpu_forward_rate(w, seconds_budget=20.0):
     what = ("the reference's simulate_fisp and sum_signal_cartesian_naive kernels built for the host "
             "(oracle/_ref/libref_kernels.so)" if ref else "oracle FP32 twin")
     return {"value": V * nTR / full, "unit": UNIT, "cores": threads, "kind": "reference" if ref else "port",
-            "sample": f"{what}: FISP on {nv} voxels ({t_sim:.1f} s) + signal on {ne} entries summed over "
-                      f"all {V} voxels ({t_sig:.1f} s), scaled to one full forward step ({full:.0f} s)"}
+            "sample": f"{what}: FISP on a fixed sample of {nv} of {V} voxels ({100.0 * nv / V:.1f} %, {t_sim:.1f} s) "
+                      f"+ signal on {ne} of {C_ * R * S} entries, each summed over all {V} voxels ({t_sig:.1f} s); "
+                      f"extrapolated to one full forward step ({full:.0f} s)"}
 
 
 def run_reference(args):
@@ -194,7 +196,7 @@ def run_reference(args):
     per_step = []
     base = None
     for i in range(args.warmup + args.steps):
-        r = cpu_forward_rate(w, seconds_budget=8.0)
+        r = cpu_forward_rate(w)
         if i >= args.warmup:
             per_step.append(r["value"])
             base = r
@@ -254,23 +256,37 @@ def main():
         import torch.distributed as dist
 
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import compas_b200 as cb
     import workloads
 
     peaks, peak_kind = load_peaks()
-    w = workloads.mrstat(seed=2 + rank, n_side=args.n_side)
+    w = workloads.mrstat(seed=2, n_side=args.n_side)
     V = w["params"].shape[1]
     nTR = len(w["seq"]["rf"])
     P, N = w["seq"]["slices"].shape[0], w["seq"]["max_state"]
     C_, R, S = w["coils"].shape[0], w["traj"]["nr"], w["traj"]["ns"]
+    # this rank's voxels of the slice (all of them on one GPU)
+    vb, ve = cb.voxel_shard(V, rank, world)
+    p_local = np.ascontiguousarray(w["params"][:, vb:ve])
+    c_local = np.ascontiguousarray(w["coils"][:, vb:ve])
 
     ctx = cb.Context(local)
-    params = cb.TissueParameters.from_soa(ctx, w["params"])
+    params = cb.TissueParameters.from_soa(ctx, p_local)
     seq = cb.FispSequence.from_dict(ctx, w["seq"])
     traj = cb.CartesianTrajectory.from_dict(ctx, w["traj"])
-    coils = cb.CompasArray.from_numpy(ctx, w["coils"])
+    coils = cb.CompasArray.from_numpy(ctx, c_local)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    comm = None
+    if world > 1:
+        from sharding import library_communicator
+
+        comm = library_communicator(cb, ctx, rank, world)
+
+    def signal_of(e, p, c):
+        if comm is None:
+            return cb.magnetization_to_signal(ctx, e, p, traj, c)
+        return cb.magnetization_to_signal_sharded(ctx, comm, e, p, traj, c)  # partials summed by NCCL
 
     def step(events=None):
         if events:
@@ -278,7 +294,7 @@ def main():
         e = cb.simulate_magnetization(ctx, params, seq)
         if events:
             events[1].record(stream)
-        s = cb.magnetization_to_signal(ctx, e, params, traj, coils)
+        s = signal_of(e, params, coils)
         if events:
             events[2].record(stream)
         return e, s
@@ -307,6 +323,7 @@ def main():
         t_end.record(stream)
         barrier()
         launches = cb.launch_count() - launches0
+    last_signal = keep[-1][1] if keep else None
     keep.clear()
     total_ms = t_start.elapsed_time(t_end)
     sim_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
@@ -316,26 +333,36 @@ def main():
         t = torch.tensor([ms_step], device=f"cuda:{local}")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms_step = float(t.item())
-    value = world * V * nTR / (ms_step / 1e3)
+    value = V * nTR / (ms_step / 1e3)  # the whole slice per step, over all ranks
     clocks = clk.summary()
 
     # roofline of the dominant kernel (FISP EPG): FP32-SIMT bound, 86·N·P flops per voxel·TR
     f_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
     fp32_peak_tf = 148 * 128 * 2 * f_mhz * 1e6 / 1e12
-    epg_flops = 86.0 * N * P * V * nTR
+    Vl = ve - vb  # voxels this rank simulates
+    epg_flops = 86.0 * N * P * Vl * nTR
     epg_tf = epg_flops / (sim_ms / 1e3) / 1e12
+    # the FP32 work the kernel executes: FMA-pipe lane operations per (voxel, slice position, TR),
+    # measured by ncu on the packed 26-slot layout (profiles/fisp_epg_mrstat.txt: FMA pipe busy
+    # cycles x 32 lanes / (voxels x positions x TRs)); against 148 SM x 128 lanes per cycle
+    lane_ops = FISP_LANE_OPS_PER_ITEM * P * Vl * nTR
+    exec_frac = lane_ops / (sim_ms / 1e3) / (148 * 128 * f_mhz * 1e6)
     roofline = {"bound": "fp32", "kernel": "fisp_epg_kernel", "achieved": epg_tf, "peak": fp32_peak_tf,
                 "unit": "TFLOP/s", "frac": epg_tf / fp32_peak_tf,
                 "traffic": profile_traffic("fisp_epg_mrstat"),
-                "note": f"FP32 SIMT peak 148 SM x 128 lanes x 2 x {f_mhz:.0f} MHz (median SM clock under load); "
-                        "algorithmic flops = 86·N·P per voxel·TR (reference formulation); HBM is not binding "
-                        "(8 B written per voxel·TR)"}
+                "executed": {"fp32_lane_ops_per_voxel_position_tr": FISP_LANE_OPS_PER_ITEM,
+                             "fp32_lane_ops": lane_ops, "frac_of_fp32_peak": exec_frac},
+                "note": f"FP32 SIMT peak 148 SM x 128 lanes x 2 x {f_mhz:.0f} MHz (median SM clock under load). "
+                        "achieved/frac count the reference formulation's 86·N·P flops per voxel·TR; the kernel "
+                        "executes 26 FP32 operations per EPG state and TR where that formulation has 48, so frac "
+                        "can pass 1. executed.frac_of_fp32_peak is the FP32 work actually issued (FMA-pipe lane "
+                        "operations, two per FFMA2) over the FP32 peak. HBM is not binding (8 B written per voxel·TR)"}
     # the HBM fraction beside it: algorithmic bytes = echoes written (8 B per voxel·readout) + the
     # nine parameter rows read (36 B per voxel)
-    epg_bytes = 8.0 * V * nTR + 36.0 * V
+    epg_bytes = 8.0 * Vl * nTR + 36.0 * Vl
     roofline["hbm"] = {"achieved_gbs": epg_bytes / (sim_ms / 1e3) / 1e9, "peak_gbs": peaks["hbm_gbs"],
                        "frac": epg_bytes / (sim_ms / 1e3) / 1e9 / peaks["hbm_gbs"]}
-    sig_flops = 8.0 * C_ * R * S * V
+    sig_flops = 8.0 * C_ * R * S * Vl
     sig_tf = sig_flops / (sig_ms / 1e3) / 1e12
     roofline_signal = {"bound": "tensor", "kernel": "signal (split-BF16 tcgen05)", "achieved": sig_tf,
                        "peak": peaks["bf16_tflops_sustained"], "unit": "TFLOP/s",
@@ -343,41 +370,61 @@ def main():
                        "note": f"algorithmic 8·C·R·S·V flops; split-BF16 issues 3 BF16 MMAs per product, so the "
                                f"attainable algorithmic rate is 1/3 of the BF16 peak ({peak_kind})"}
     # algorithmic bytes: echoes read (8·R·V), coils and parameters (8·C·V + 36·V), signal written (8·C·R·S)
-    sig_bytes = 8.0 * R * V + 8.0 * C_ * V + 36.0 * V + 8.0 * C_ * R * S
+    sig_bytes = 8.0 * R * Vl + 8.0 * C_ * Vl + 36.0 * Vl + 8.0 * C_ * R * S
     roofline_signal["frac_of_split_bf16_ceiling"] = sig_tf / (peaks["bf16_tflops_sustained"] / 3)
     roofline_signal["hbm"] = {"achieved_gbs": sig_bytes / (sig_ms / 1e3) / 1e9, "peak_gbs": peaks["hbm_gbs"],
                               "frac": sig_bytes / (sig_ms / 1e3) / 1e9 / peaks["hbm_gbs"]}
 
+    # FP64 error of the step's split-BF16 signal against the oracle on 256 entries, each summed over
+    # this rank's voxels with the GPU's own echoes (outside the timed region; one GPU only)
+    signal_err = None
+    if world == 1 and last_signal is not None:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle
+
+        e_host = cb.simulate_magnetization(ctx, params, seq).to_numpy()
+        rng = np.random.default_rng(5)
+        ent = np.stack([rng.integers(0, C_, 256), rng.integers(0, R, 256), rng.integers(0, S, 256)], 1)
+        ref = oracle.signal_cartesian(e_host, p_local, w["traj"], c_local, entries=ent)
+        got = last_signal.to_numpy()[ent[:, 0], ent[:, 1], ent[:, 2]]
+        signal_err = oracle.rel_l2(got, ref)
+        del e_host
+    roofline_signal["rel_err_fp64"] = signal_err
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+           "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
            "vs_baseline": None, "dtype": "fp32 (EPG), bf16x3->fp32 (signal)", "data": "synthetic",
            "config": {"workload": f"mrstat: {args.n_side}x{args.n_side}={V} voxels, FISP 1120 TR, 25 EPG states, "
-                                  f"35 slice positions, 4 coils, Cartesian 1120x{args.n_side} readouts; one "
-                                  "independent slice per GPU",
-                      "parallelism": f"voxel-independent, {world} rank(s), no collective",
+                                  f"35 slice positions, 4 coils, Cartesian 1120x{args.n_side} readouts; the one "
+                                  "slice sharded over the GPUs",
+                      "parallelism": (f"voxel shards over {world} ranks ({ve - vb} voxels on rank {rank}), NCCL "
+                                      "all-reduce of the partial signal inside the step" if world > 1 else
+                                      "one GPU"),
                       "l2": "working set > L2 (echo array 450 MB per step)", "seed": 2},
            "gpu_launches": launches, "clocks": clocks, "roofline": roofline, "roofline_signal": roofline_signal,
            "stage_ms": {"simulate_fisp": sim_ms, "signal_cartesian": sig_ms},
            "signal_tflops": sig_tf, "peaks": peak_kind}
 
-    if world == 1 and not args.no_reference_kernels:
+    single = world == 1
+    if single and not args.no_reference_kernels:
         out["reference_kernels_gpu"] = reference_kernels_gpu(cb, ctx, stream, w, sim_ms, args)
-    if not args.no_jacobian:
+    if single and not args.no_jacobian:
         out["jacobian"] = jacobian_products(cb, ctx, stream, args, peaks, rank)
-    if args.batch_jobs > 0:
+    if single and args.batch_jobs > 0:
         out["batched"] = batched(cb, ctx, stream, args, rank)
-    out["elementwise"] = elementwise(cb, ctx, stream, w, params, seq, traj, peaks)
-    if not args.no_gn:
+    if single:
+        out["elementwise"] = elementwise(cb, ctx, stream, w, params, seq, traj, peaks)
+    if single and not args.no_gn:
         out["derivatives"] = derivatives(cb, ctx, stream, args, rank)
         out["gauss_newton"] = gauss_newton(cb, ctx, stream, args, rank)
-    if args.serve_rates and rank == 0:
+    if single and args.serve_rates:
         out["served"] = served(cb, ctx, args)
     if not args.no_e2e:
-        out["e2e"] = e2e(cb, ctx, w, args, local)
+        out["e2e"] = e2e(cb, ctx, w, args, local, (vb, ve), signal_of, world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_forward_rate(w)
     if world > 1:
         torch.distributed.barrier()
+        del comm
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(out))
@@ -529,8 +576,12 @@ def elementwise(cb, ctx, stream, w, params, seq, traj, peaks):
     reps = 5
 
     def gpu_ms(fn):
-        fn()
+        # warm-up with as many results alive as the timed loop keeps, so that the memory pool has
+        # grown to its size before timing (growing it maps memory on the host, which would show up
+        # inside the timed span)
+        warm = [fn() for _ in range(reps)]
         ctx.synchronize()
+        del warm
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
             torch.cuda._sleep(40_000_000)
@@ -559,6 +610,23 @@ def elementwise(cb, ctx, stream, w, params, seq, traj, peaks):
                                "frac_of_hbm": pe_gbs / hbm},
             "residual": {"elements": n, "ms": res_ms, "algorithmic_bytes": 24.0 * n, "gbs": res_gbs,
                          "frac_of_hbm": res_gbs / hbm}}
+
+
+def ref_gpu_timed(oracle, timed, fn, stream):
+    """One re-hosted reference call, timed: the index-checked build runs first and gives the result;
+    where its out-of-bounds flag stays clear, the build without index checks (which kmm's own views
+    do not make either) is timed on the same launches, else the checked build. Returns
+    (ms, result, which build was timed)."""
+    import torch
+
+    with torch.cuda.stream(stream):
+        out = fn(unchecked=False)
+    torch.cuda.synchronize()
+    if oracle.ref_gpu_out_of_bounds() == 0 and oracle.ref_gpu(unchecked=True) is not None:
+        ms, _ = timed(lambda: fn(unchecked=True), stream)
+        return ms, out, "unchecked views"
+    ms, _ = timed(lambda: fn(unchecked=False), stream)
+    return ms, out, "index-checked views"
 
 
 def reference_kernels_gpu(cb, ctx, stream, w, sim_ms, args):
@@ -600,7 +668,9 @@ def reference_kernels_gpu(cb, ctx, stream, w, sim_ms, args):
                    "kmm views; launch code restated from src/simulate/fisp.cu and pssfp.cu"}
     V = w["params"].shape[1]
     nTR = len(w["seq"]["rf"])
-    ref_ms, ref_e = timed(lambda: oracle.ref_gpu_fisp(w["params"], w["seq"]), ts)
+    ref_ms, ref_e, build = ref_gpu_timed(oracle, timed, lambda **kw: oracle.ref_gpu_fisp(w["params"], w["seq"], **kw),
+                                         ts)
+    res["timed_build"] = build
     p = cb.TissueParameters.from_soa(ctx, w["params"])
     mine = cb.simulate_magnetization(ctx, p, cb.FispSequence.from_dict(ctx, w["seq"]))
     ctx.synchronize()
@@ -612,7 +682,7 @@ def reference_kernels_gpu(cb, ctx, stream, w, sim_ms, args):
     rng = np.random.default_rng(7)
     pd = workloads.pssfp_sequence(rng, 320, nrf=15, nz=35)
     pp = workloads.tissue(rng, args.n_side, 22.4)
-    ref_ms, ref_e = timed(lambda: oracle.ref_gpu_pssfp(pp, pd), ts)
+    ref_ms, ref_e, _ = ref_gpu_timed(oracle, timed, lambda **kw: oracle.ref_gpu_pssfp(pp, pd, **kw), ts)
     p = cb.TissueParameters.from_soa(ctx, pp)
     seq = cb.pSSFPSequence.from_dict(ctx, pd)
     this_ms, mine = timed(lambda: cb.simulate_magnetization(ctx, p, seq), stream)
@@ -628,7 +698,8 @@ def reference_kernels_gpu(cb, ctx, stream, w, sim_ms, args):
     st = workloads.spiral(rng, 760, 1000, 22.4, 4e-6)
     coils = workloads.cn(rng, (16, 30000))
     echo = workloads.cn(rng, (760, 30000)) * 0.1
-    ref_ms, ref_s = timed(lambda: oracle.ref_gpu_signal_spiral(sp, echo, st, coils), ts)
+    ref_ms, ref_s, _ = ref_gpu_timed(oracle, timed, lambda **kw: oracle.ref_gpu_signal_spiral(sp, echo, st, coils, **kw),
+                                     ts)
     p = cb.TissueParameters.from_soa(ctx, sp)
     traj = cb.trajectory_from_dict(ctx, st)
     e_arr, c_arr = cb.CompasArray.from_numpy(ctx, echo), cb.CompasArray.from_numpy(ctx, coils)
@@ -657,11 +728,12 @@ def reference_products_gpu(w, stream, reps, this_ms, lib):
     ins = {k: torch.as_tensor(np.ascontiguousarray(w[k]), device="cuda")
            for k in ("echo", "dT1", "dT2", "v", "r", "coils")}
     ts = torch.cuda.Stream()
-    runs = {"signal": lambda: oracle.ref_gpu_signal_cartesian(w["params"], ins["echo"], w["traj"], ins["coils"]),
-            "jv": lambda: oracle.ref_gpu_jacobian(w["params"], ins["echo"], ins["dT1"], ins["dT2"], w["traj"],
-                                                  ins["coils"], ins["v"]),
-            "jhv": lambda: oracle.ref_gpu_jacobian(w["params"], ins["echo"], ins["dT1"], ins["dT2"], w["traj"],
-                                                   ins["coils"], ins["r"], hermitian=True)}
+    runs = {"signal": lambda **kw: oracle.ref_gpu_signal_cartesian(w["params"], ins["echo"], w["traj"], ins["coils"],
+                                                                   **kw),
+            "jv": lambda **kw: oracle.ref_gpu_jacobian(w["params"], ins["echo"], ins["dT1"], ins["dT2"], w["traj"],
+                                                       ins["coils"], ins["v"], **kw),
+            "jhv": lambda **kw: oracle.ref_gpu_jacobian(w["params"], ins["echo"], ins["dT1"], ins["dT2"], w["traj"],
+                                                        ins["coils"], ins["r"], hermitian=True, **kw)}
     mine = {"signal": lambda: cb.magnetization_to_signal(ctx, arr["echo"], params, traj, arr["coils"],
                                                          method="MatmulFast"),
             "jv": lambda: cb.compute_jacobian(ctx, arr["echo"], d, params, traj, arr["coils"], arr["v"],
@@ -671,17 +743,21 @@ def reference_products_gpu(w, stream, reps, this_ms, lib):
     res = {"what": "the reference's MatmulFast signal and GemmFast J·v / Jᴴ·v (the C ABI's defaults): its unmodified "
                    "kernels and its four-GEMM complex products on TF32 cuBLAS, launch code restated from "
                    "src/trajectories/signal.cu, src/jacobian/product.cu, hermitian.cu"}
-    for name, fn in runs.items():
-        with torch.cuda.stream(ts):
-            out = fn()
+    def timed(fn, s):
+        with torch.cuda.stream(s):
+            fn()
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(ts)
+            e0.record(s)
             for _ in range(reps):
-                out = fn()
-            e1.record(ts)
+                r = fn()
+            e1.record(s)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / reps
+        return e0.elapsed_time(e1) / reps, r
+
+    for name, fn in runs.items():
+        ms, out, build = ref_gpu_timed(oracle, timed, fn, ts)
+        res["timed_build"] = build
         ours = torch.as_tensor(mine[name](), device="cuda")
         ctx.synchronize()
         a = torch.view_as_real(out).double()
@@ -824,6 +900,7 @@ def jacobian_products(cb, ctx, stream, args, peaks, rank):
                                                          method="Direct"), 1)
     jhv_plain = timed(lambda: cb.compute_jacobian_hermitian(ctx, arr["echo"], d, params, traj, arr["coils"],
                                                             arr["r"], method="Direct"), 1)
+    err = products_error_fp64(cb, ctx, w, params, traj, arr, d)
     f_sig = 8.0 * C_ * R * S * V
     f_j = 16.0 * C_ * R * S * V
     f_jh = 16.0 * C_ * R * S * V + 24.0 * C_ * R * V
@@ -840,22 +917,59 @@ def jacobian_products(cb, ctx, stream, args, peaks, rank):
             "signal_plus_jhv_frac_of_bf16": tf(f_sig + f_jh, sig + jhv) / peak,
             "plain_fp32_signal_ms": sig_plain, "plain_fp32_jhv_ms": jhv_plain,
             "tensor_vs_plain_signal_plus_jhv": (sig_plain + jhv_plain) / (sig + jhv),
+            "rel_err_fp64": err,
             "note": "algorithmic flops 8·C·R·S·V (signal), 16·C·R·S·V (J·v), 16·C·R·S·V + 24·C·R·V (Jᴴ·v); "
                     "split-BF16 issues 3 MMAs per product; fraction of the sustained BF16 peak (measured)"}
 
 
-def e2e(cb, ctx, w, args, local):
+def products_error_fp64(cb, ctx, w, params, traj, arr, d, nent=256, nvox=128):
+    """Relative L2 error against the FP64 oracle of the signal, J·v and Jᴴ·v on the Jacobian
+    workload, split-BF16 (MatmulFast / GemmFast) and plain FP32 (Direct): 256 random
+    (coil, readout, sample) entries, each summed over all voxels, and Jᴴ·v on 128 random voxels
+    (outside any timed region)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    V = w["params"].shape[1]
+    C_, R, S = w["coils"].shape[0], w["traj"]["nr"], w["traj"]["ns"]
+    rng = np.random.default_rng(17)
+    ent = np.stack([rng.integers(0, C_, nent), rng.integers(0, R, nent), rng.integers(0, S, nent)], 1)
+    idx = np.sort(rng.choice(V, nvox, replace=False))
+    at = lambda a: a[ent[:, 0], ent[:, 1], ent[:, 2]]  # noqa: E731
+    ref = {"signal": oracle.signal_cartesian(w["echo"], w["params"], w["traj"], w["coils"], entries=ent),
+           "jv": oracle.jacobian(w["echo"], w["dT1"], w["dT2"], w["params"], w["traj"], w["coils"], w["v"],
+                                 entries=ent),
+           "jhv": oracle.jacobian_hermitian(w["echo"], w["dT1"], w["dT2"], w["params"], w["traj"], w["coils"],
+                                            w["r"], vidx=idx)}
+    out = {"sample": f"{nent} entries summed over all {V} voxels (signal, J·v), {nvox} voxels (Jᴴ·v)"}
+    for tc, plain in (("MatmulFast", "Direct"),):
+        for m in (tc, plain):
+            s = cb.magnetization_to_signal(ctx, arr["echo"], params, traj, arr["coils"], method=m).to_numpy()
+            out[f"signal_{m}"] = oracle.rel_l2(at(s), ref["signal"])
+    for m in ("GemmFast", "Direct"):
+        jv = cb.compute_jacobian(ctx, arr["echo"], d, params, traj, arr["coils"], arr["v"], method=m).to_numpy()
+        out[f"jv_{m}"] = oracle.rel_l2(at(jv), ref["jv"])
+        jh = cb.compute_jacobian_hermitian(ctx, arr["echo"], d, params, traj, arr["coils"], arr["r"],
+                                           method=m).to_numpy()
+        out[f"jhv_{m}"] = oracle.rel_l2(jh[:, idx], ref["jhv"])
+    return out
+
+
+def e2e(cb, ctx, w, args, local, voxels, signal_of, world):
     """Same step through the public API from pinned host buffers: every step uploads the
-    tissue parameters, sequence, trajectory and coils and reads the signal back."""
+    tissue parameters, sequence, trajectory and coils (this rank's voxels) and reads the signal
+    back; over several ranks the signal call is the sharded one (NCCL sum of the partials) and the
+    time is the slowest rank's."""
     import torch
 
     def pinned(a):
         t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
         return t.numpy()
 
-    p_h = pinned(w["params"])
+    vb, ve = voxels
+    p_h = pinned(w["params"][:, vb:ve])
     rf_h, sl_h = pinned(w["seq"]["rf"]), pinned(w["seq"]["slices"])
-    ks_h, co_h = pinned(w["traj"]["k_start"]), pinned(w["coils"])
+    ks_h, co_h = pinned(w["traj"]["k_start"]), pinned(w["coils"][:, vb:ve])
     C_, R, S = co_h.shape[0], w["traj"]["nr"], w["traj"]["ns"]
     out_h = pinned(np.zeros((C_, R, S), np.complex64))
     s = w["seq"]
@@ -867,19 +981,25 @@ def e2e(cb, ctx, w, args, local):
         traj = cb.CartesianTrajectory(ctx, t["nr"], t["ns"], t["dt"], ks_h, t["dk"])
         coils = cb.CompasArray.from_numpy(ctx, co_h)
         e = cb.simulate_magnetization(ctx, params, seq)
-        sig = cb.magnetization_to_signal(ctx, e, params, traj, coils)
+        sig = signal_of(e, params, coils)
         sig.read_into(out_h)
 
     for _ in range(max(1, args.warmup)):
         step()
     steps = max(1, min(args.steps, 3))
     ctx.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
     t0 = time.perf_counter()
     for _ in range(steps):
         step()
     ctx.synchronize()
     dt = (time.perf_counter() - t0) / steps
-    V, nTR = p_h.shape[1], len(rf_h)
+    if world > 1:
+        t = torch.tensor([dt], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        dt = float(t.item())
+    V, nTR = w["params"].shape[1], len(rf_h)
     h2d = p_h.nbytes + rf_h.nbytes + sl_h.nbytes + ks_h.nbytes + co_h.nbytes
     return {"value": V * nTR / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(out_h.nbytes), "ms_per_step": dt * 1e3,

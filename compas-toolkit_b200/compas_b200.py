@@ -76,6 +76,7 @@ _SIGS = {
     "compas_b200_set_pssfp_launch": ([_I], None),
     "compas_b200_fisp_config_count": ([], _I),
     "compas_b200_fisp_config_info": ([_I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
+    "compas_b200_fisp_config_packed": ([_I], _I),
     "compas_b200_pssfp_config_count": ([], _I),
     "compas_b200_pssfp_config_info": ([_I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
     "compas_b200_fisp_launch_choice": ([_I, _I64, _I, C.POINTER(C.c_int), C.POINTER(C.c_int)], None),
@@ -96,6 +97,15 @@ _SIGS = {
     "compas_b200_gauss_newton_graph_kernels": ([_P], _I),
     "compas_b200_make_server": ([_P, C.c_double, _I, _I, C.c_double, _I, _F], _P),
     "compas_b200_server_submit": ([_P, _P, _P, _P, _P, _P, C.c_uint64], _I64),
+    "compas_b200_server_submit_flags": ([_P, _P, _P, _P, _P, _P, C.c_uint64, _I], _I64),
+    "compas_b200_wait_probe": ([_P, _I64], _I),
+    "compas_b200_gauss_newton_set_line_search": ([_P, _I], _I),
+    "compas_b200_voxel_shard": ([_I64, _I, _I, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], _I),
+    "compas_b200_comm_unique_id": ([C.c_char_p, _I], _I),
+    "compas_b200_make_communicator": ([_P, _I, _I, C.c_char_p], _P),
+    "compas_b200_allreduce_sum": ([_P, _P, _P], _I),
+    "compas_b200_magnetization_to_signal_sharded": ([_P, _P, _P, _P, _P, _P, _I], _P),
+    "compas_b200_compute_jacobian_sharded": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _I], _P),
     "compas_b200_server_wait": ([_P, _I64, C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int)], _I),
     "compas_b200_server_result": ([_P, _I64, _I], _P),
     "compas_b200_server_release": ([_P, _I64], _I),
@@ -299,8 +309,9 @@ class FispSequence(_Object):
 
 
 class pSSFPSequence(_Object):
-    """compas_make_pssfp_sequence. `z` is passed as float32 (the reference's Julia wrapper
-    converted it to ComplexF32, which disagrees with the C++ side)."""
+    """compas_make_pssfp_sequence. `z` is passed as float32, which is what the C++ side reads
+    (compas/sequences/pssfp.h: Array<float>); the reference's Julia wrapper converts it to
+    ComplexF32 (CompasToolkit.jl), which does not match."""
 
     def __init__(self, context: Context, RF_train, TR: float, gamma_dt_RF, dt: Sequence[float],
                  gamma_dt_GRz: Sequence[float], z):
@@ -533,13 +544,14 @@ class GaussNewtonStep(_Object):
     """compas_b200_make_gauss_newton: one Gauss-Newton iteration on the device (simulate,
     derivatives — forward differences with step `delta`, or exact tangents for delta=0 — signal,
     residual against `data`, `cg_iterations` CGLS steps of J·v / Jᴴ·v, parameter update),
-    captured as a CUDA graph on the first graph run."""
+    captured as a CUDA graph on the first graph run. line_search (default): the update takes the
+    first of the steps t = 1, ½ that does not raise the objective, else none."""
 
     ARRAYS = {"parameters": 0, "echos": 1, "dT1": 2, "dT2": 3, "signal": 4, "gradient": 5, "step": 6,
               "scalars": 7}
 
     def __init__(self, context: Context, parameters: TissueParameters, sequence, trajectory, coils, data,
-                 cg_iterations: int = 4, delta: float = 1e-4, method: str = "GemmFast"):
+                 cg_iterations: int = 4, delta: float = 1e-4, method: str = "GemmFast", line_search: bool = True):
         c = _arr(context, coils, np.complex64)
         d = _arr(context, data, np.complex64)
         ptr = library().compas_b200_make_gauss_newton(context.ptr, parameters.ptr, sequence.ptr, trajectory.ptr,
@@ -552,6 +564,16 @@ class GaussNewtonStep(_Object):
                        "dT1": (sequence.nreadouts, self.nvoxels), "dT2": (sequence.nreadouts, self.nvoxels),
                        "signal": tuple(d.shape), "gradient": (4, self.nvoxels), "step": (4, self.nvoxels),
                        "scalars": (8,)}
+        if not line_search:
+            self.set_line_search(False)
+
+    def set_line_search(self, on: bool):
+        if library().compas_b200_gauss_newton_set_line_search(self.ptr, int(bool(on))) != 0:
+            _check(None, "compas_b200_gauss_newton_set_line_search!")
+
+    def step_length(self) -> float:
+        """Step length the line search took in the last iteration: 1, 0.5 or 0 (blocks)."""
+        return float(self.array("scalars").to_numpy()[7])
 
     def run(self, graph: bool = True):
         """Enqueue one iteration on the context's stream."""
@@ -594,11 +616,14 @@ class ServeEngine(_Object):
         self.context = context
         self._meta = {}
 
-    def submit(self, parameters: TissueParameters, sequence, trajectory, coils, data, echo_key: int = 0) -> int:
+    def submit(self, parameters: TissueParameters, sequence, trajectory, coils, data, echo_key: int = 0,
+               inject_wait_timeout: bool = False) -> int:
+        """Queue a request. inject_wait_timeout (a test hook of the failure path) makes the batch
+        that runs it also run a kernel whose bounded wait gives up, so that batch's requests fail."""
         c = _arr(self.context, coils, np.complex64)
         d = _arr(self.context, data, np.complex64)
-        t = library().compas_b200_server_submit(self.ptr, parameters.ptr, sequence.ptr, trajectory.ptr, c.ptr, d.ptr,
-                                                int(echo_key))
+        t = library().compas_b200_server_submit_flags(self.ptr, parameters.ptr, sequence.ptr, trajectory.ptr, c.ptr,
+                                                      d.ptr, int(echo_key), 1 if inject_wait_timeout else 0)
         if t < 0:
             _check(None, "compas_b200_server_submit!")
         self._meta[t] = (tuple(d.shape), parameters.nvoxels, isinstance(trajectory, CartesianTrajectory))
@@ -639,6 +664,73 @@ class ServeEngine(_Object):
         library().compas_b200_server_reset_stats(self.ptr)
 
 
+def voxel_shard(nvoxels: int, rank: int, world: int) -> tuple:
+    """Voxels [begin, end) of `rank` among `world` ranks (the library's partition: contiguous,
+    sizes differ by at most one). Host-only: needs no GPU."""
+    b, e = C.c_int64(), C.c_int64()
+    if library().compas_b200_voxel_shard(int(nvoxels), int(rank), int(world), C.byref(b), C.byref(e)) != 0:
+        _check(None, "compas_b200_voxel_shard")
+    return b.value, e.value
+
+
+def comm_unique_id() -> bytes:
+    """A new NCCL unique id (128 bytes): one rank makes it, every rank passes it to Communicator."""
+    buf = C.create_string_buffer(128)
+    if library().compas_b200_comm_unique_id(buf, 128) != 128:
+        _check(None, "compas_b200_comm_unique_id")
+    return buf.raw
+
+
+class Communicator(_Object):
+    """compas_b200_make_communicator: the library's NCCL communicator over `world` processes, one
+    GPU each (blocks until every rank has joined with the same unique id)."""
+
+    def __init__(self, context: Context, rank: int, world: int, unique_id: bytes):
+        if len(unique_id) != 128:
+            raise CompasError("an NCCL unique id has 128 bytes")
+        ptr = library().compas_b200_make_communicator(context.ptr, int(rank), int(world), bytes(unique_id))
+        super().__init__(ptr)
+        _check(ptr, "compas_b200_make_communicator!")
+        self.context, self.rank, self.world = context, int(rank), int(world)
+
+    def allreduce_sum(self, array: CompasArray) -> CompasArray:
+        """In-place sum of a library array over the ranks (ordered on the context's stream)."""
+        if library().compas_b200_allreduce_sum(self.context.ptr, self.ptr, array.ptr) != 0:
+            _check(None, "compas_b200_allreduce_sum!")
+        return array
+
+
+def magnetization_to_signal_sharded(context: Context, comm: Communicator, echos, parameters: TissueParameters,
+                                    trajectory, coils, method: str = "MatmulFast") -> CompasArray:
+    """Full signal of a slice whose voxels are sharded over the communicator's ranks: this rank's
+    echoes [R][V_rank], parameters and coils; the ranks' partials are summed by NCCL."""
+    e = _arr(context, echos, np.complex64)
+    c = _arr(context, coils, np.complex64)
+    ptr = library().compas_b200_magnetization_to_signal_sharded(context.ptr, comm.ptr, e.ptr, parameters.ptr,
+                                                                trajectory.ptr, c.ptr, SIGNAL_METHODS[method])
+    return _result(ptr, context, (c.shape[0], trajectory.nreadouts, trajectory.samples_per_readout),
+                   "magnetization_to_signal_sharded")
+
+
+def compute_jacobian_sharded(context: Context, comm: Communicator, echos, dechos: dict, parameters: TissueParameters,
+                             trajectory, coils, v, method: str = "GemmFast") -> CompasArray:
+    """J·v of a slice whose voxels are sharded over the ranks (this rank's voxels in, full sum out)."""
+    e, d1, d2 = (_arr(context, a, np.complex64) for a in (echos, dechos["T1"], dechos["T2"]))
+    c = _arr(context, coils, np.complex64)
+    vv = _arr(context, v, np.complex64)
+    ptr = library().compas_b200_compute_jacobian_sharded(context.ptr, comm.ptr, e.ptr, d1.ptr, d2.ptr, parameters.ptr,
+                                                         trajectory.ptr, c.ptr, vv.ptr, JACOBIAN_METHODS[method])
+    return _result(ptr, context, (c.shape[0], trajectory.nreadouts, trajectory.samples_per_readout),
+                   "compute_jacobian_sharded")
+
+
+def wait_probe(context: Context, limit_cycles: int = 2_000_000):
+    """Enqueue the failure-channel self-test: a kernel whose bounded wait on a barrier nobody
+    completes gives up after `limit_cycles` SM cycles; the next synchronize raises CompasError."""
+    if library().compas_b200_wait_probe(context.ptr, int(limit_cycles)) != 0:
+        _check(None, "compas_b200_wait_probe")
+
+
 def launch_count() -> int:
     """Kernels launched by libcompas_b200.so so far in this process."""
     return int(library().compas_b200_launch_count())
@@ -677,6 +769,11 @@ def fisp_configs() -> list:
         lib.compas_b200_fisp_config_info(i, C.byref(k), C.byref(g))
         out.append((k.value, g.value))
     return out
+
+
+def fisp_config_packed(index: int) -> bool:
+    """Whether FISP layout `index` is packed (two states per two-wide FP32 instruction)."""
+    return bool(library().compas_b200_fisp_config_packed(int(index)))
 
 
 def fisp_launch_choice(max_state: int, nvoxels: int, npositions: int) -> tuple:

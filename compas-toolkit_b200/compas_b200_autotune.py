@@ -1,8 +1,9 @@
 """Autotuner for the simulation kernels' launch layouts.
 
 The FISP EPG kernel is instantiated for several register layouts — K states per lane × G lanes
-per (voxel, slice position) — and runs with W warps per CTA (W slice positions in flight per
-voxel tile); the pSSFP kernel for ZT isochromats per lane × GZ lanes per voxel. Which layout is
+per (voxel, slice position), and packed one-lane layouts that hold K states as K/2 pairs of
+two-wide FP32 registers — and runs with W warps per CTA (W slice positions in flight per voxel
+tile); the pSSFP kernel for ZT isochromats per lane × GZ lanes per voxel. Which layout is
 fastest depends on the number of states / z positions, the voxel count and the slice positions.
 This script times every covering layout on the current GPU for a set of shape classes and writes
 the winners to a tuning table that the library reads from the file named by COMPAS_B200_TUNING:
@@ -10,8 +11,8 @@ the winners to a tuning table that the library reads from the file named by COMP
     fisp  <N> <log2 voxels> <log2 positions> <layout> <warps>
     pssfp <nz> <log2 voxels> <layout>
 
-Layouts change only the work distribution (FISP warps also change the order in which slice
-positions are summed), so every candidate stays within the library's FP32 tolerance.
+Layouts change only the work distribution; the FISP echoes are the same bits for every layout and
+warp count (slice positions are summed one at a time in increasing order).
 
     python compas-toolkit_b200/compas_b200_autotune.py --out tuning.txt [--quick]
 """
@@ -43,6 +44,11 @@ def _time(ctx, fn, reps):
     e1.record(stream)
     ctx.synchronize()
     return e0.elapsed_time(e1) / reps
+
+
+def _fisp_name(cfg):
+    K, G = cb.fisp_configs()[cfg]
+    return f"({K}, {G}{', packed' if cb.fisp_config_packed(cfg) else ''})"
 
 
 def tune_fisp(ctx, N, nv, P, ntr, reps, warps=(4, 5, 6, 7, 8)):
@@ -101,9 +107,8 @@ def main(argv=None):
             res, default, dms = tune_fisp(ctx, N, nv, P, args.ntr, reps=2 if args.quick else 3)
             ms, cfg, w = res[0]
             lines.append(f"fisp {N} {int(math.log2(nv))} {int(math.log2(P))} {cfg} {w}")
-            report.append(f"# fisp N={N} P={P} V={nv}: best {tuple(cb.fisp_configs()[cfg])} W={w} {ms:.3f} ms; "
-                          f"built-in {tuple(cb.fisp_configs()[default[0]])} W={default[1]} {dms:.3f} ms "
-                          f"({len(res)} candidates)")
+            report.append(f"# fisp N={N} P={P} V={nv}: best {_fisp_name(cfg)} W={w} {ms:.3f} ms; "
+                          f"built-in {_fisp_name(default[0])} W={default[1]} {dms:.3f} ms ({len(res)} candidates)")
     for nz in ([35] if args.quick else [9, 35]):
         for nv in voxel_classes:
             res, default, dms = tune_pssfp(ctx, nz, nv, args.ntr, reps=2 if args.quick else 3)

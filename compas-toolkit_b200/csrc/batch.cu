@@ -275,7 +275,7 @@ void SimulationBatch::Impl::plan_signal(Family& fam, const std::vector<int>& mem
                                                echos[size_t(e.job)].data(), job.coil_sensitivities.data(), C,
                                                cartesian_geom(t));
             a.vchunk = e.plan.vchunk;
-            a.status = detail::device_status_word(dev);
+            a.status = ctx.status_word();
             const TcTables tables = tc_tables(V, t.nreadouts, t.samples_per_readout, C, false);
             Array<unsigned char> scratch({tables.bytes}, dev, ctx.stream());
             tc_assign_tables(a, tables, scratch.data());
@@ -378,7 +378,7 @@ void SimulationBatch::Impl::enqueue(const Family& fam, cudaStream_t stream, int*
     for (const auto& g : fam.spirals)
         launch_signal_spiral_batch(stream, dev, g.coil_group, as<kernels::SpiralArgs>(g.args), as<int>(g.cta_offsets),
                                    g.njobs, g.ctas);
-    const CompasContext sctx(dev, stream);
+    const CompasContext sctx(dev, stream, ctx.status_word());
     for (int j : fam.tc_spiral) {
         const auto& job = jobs[size_t(j)];
         const auto& t = std::get<SpiralTrajectory>(job.trajectory);

@@ -443,6 +443,80 @@ compas_array* compas_b200_compute_jacobian(const compas_context* ctx, const comp
     });
 }
 
+int compas_b200_voxel_shard(int64_t nvoxels, int rank, int world, int64_t* begin, int64_t* end) {
+    t_has_error = false;
+    guarded([&] {
+        if (!begin || !end) throw compas::CompasException("null output pointer");
+        const compas::VoxelRange r = compas::voxel_shard(nvoxels, rank, world);
+        *begin = r.begin;
+        *end = r.end;
+    });
+    return t_has_error ? -1 : 0;
+}
+
+int compas_b200_comm_unique_id(char* out, int nbytes) {
+    t_has_error = false;
+    const int n = guarded([&] {
+        const std::vector<char> id = compas::Communicator::unique_id();
+        if (!out || nbytes < int(id.size())) throw compas::CompasException("the unique id needs 128 bytes");
+        std::memcpy(out, id.data(), id.size());
+        return int(id.size());
+    });
+    return t_has_error ? -1 : n;
+}
+
+compas_object* compas_b200_make_communicator(const compas_context* ctx, int rank, int world, const char* unique_id) {
+    return guarded([&]() -> compas_object* {
+        if (!unique_id) throw compas::CompasException("null unique id");
+        return new_obj(compas::Communicator(ctx_of(ctx), rank, world, std::vector<char>(unique_id, unique_id + 128)));
+    });
+}
+
+int compas_b200_allreduce_sum(const compas_context* ctx, const compas_object* comm, compas_array* array) {
+    t_has_error = false;
+    guarded([&] {
+        if (!array) throw compas::CompasException("null array");
+        const auto* base = dynamic_cast<const compas::ArrayBase*>(handle<compas::Object>(array));
+        if (!base) throw compas::CompasException("handle is not an array");
+        if (base->element_size() != sizeof(float) && base->element_size() != 2 * sizeof(float))
+            throw compas::CompasException("all-reduce of a float or complex array only");
+        unwrap<compas::Communicator>(comm).allreduce_sum(ctx_of(ctx), static_cast<float*>(base->raw_data()),
+                                                         int64_t(base->nbytes() / sizeof(float)));
+    });
+    return t_has_error ? -1 : 0;
+}
+
+compas_array* compas_b200_magnetization_to_signal_sharded(const compas_context* ctx, const compas_object* comm,
+                                                          const compas_array* echos, const compas_object* parameters,
+                                                          const compas_object* trajectory, const compas_array* coils,
+                                                          int method) {
+    return guarded([&] {
+        return with_trajectory(trajectory, [&](const auto& traj) {
+            return new_array(compas::magnetization_to_signal_sharded(
+                ctx_of(ctx), unwrap<compas::Communicator>(comm), array_of<cfloat, 2>(echos, "echos"),
+                unwrap<compas::TissueParameters>(parameters), traj, array_of<cfloat, 2>(coils, "coils"),
+                signal_method(method)));
+        });
+    });
+}
+
+compas_array* compas_b200_compute_jacobian_sharded(const compas_context* ctx, const compas_object* comm,
+                                                   const compas_array* echos, const compas_array* delta_echos_T1,
+                                                   const compas_array* delta_echos_T2, const compas_object* parameters,
+                                                   const compas_object* trajectory, const compas_array* coils,
+                                                   const compas_array* vector, int method) {
+    return guarded([&] {
+        return with_trajectory(trajectory, [&](const auto& traj) {
+            return new_array(compas::compute_jacobian_sharded(
+                ctx_of(ctx), unwrap<compas::Communicator>(comm), array_of<cfloat, 2>(echos, "echos"),
+                array_of<cfloat, 2>(delta_echos_T1, "delta_echos_T1"),
+                array_of<cfloat, 2>(delta_echos_T2, "delta_echos_T2"), unwrap<compas::TissueParameters>(parameters),
+                traj, array_of<cfloat, 2>(coils, "coils"), array_of<cfloat, 2>(vector, "vector"),
+                jacobian_method(method)));
+        });
+    });
+}
+
 compas_array* compas_b200_compute_jacobian_hermitian(const compas_context* ctx, const compas_array* echos,
                                                      const compas_array* delta_echos_T1,
                                                      const compas_array* delta_echos_T2,
@@ -521,6 +595,12 @@ int compas_b200_compute_residual_noalloc(int device, const compas_cfloat* lhs, c
     return rc;
 }
 
+int compas_b200_wait_probe(const compas_context* ctx, int64_t limit_cycles) {
+    t_has_error = false;
+    guarded([&] { compas::launch_wait_probe(ctx_of(ctx), (long long)limit_cycles); });
+    return t_has_error ? -1 : 0;
+}
+
 uint64_t compas_b200_launch_count(void) {
     return compas::launch_count();
 }
@@ -531,6 +611,10 @@ int compas_b200_fisp_config_count(void) {
 
 int compas_b200_fisp_config_info(int index, int* states_per_lane, int* lanes) {
     return compas::fisp_config_info(index, states_per_lane, lanes) ? 1 : 0;
+}
+
+int compas_b200_fisp_config_packed(int index) {
+    return compas::fisp_config_packed(index) ? 1 : 0;
 }
 
 int compas_b200_pssfp_config_count(void) {
@@ -633,6 +717,12 @@ int compas_b200_gauss_newton_run(const compas_object* gn, int use_graph) {
     return t_has_error ? -1 : 0;
 }
 
+int compas_b200_gauss_newton_set_line_search(const compas_object* gn, int on) {
+    t_has_error = false;
+    guarded([&] { const_cast<compas::GaussNewtonStep&>(unwrap<compas::GaussNewtonStep>(gn)).set_line_search(on != 0); });
+    return t_has_error ? -1 : 0;
+}
+
 compas_array* compas_b200_gauss_newton_array(const compas_object* gn, int which) {
     return guarded([&]() -> compas_array* {
         const auto& g = unwrap<compas::GaussNewtonStep>(gn);
@@ -675,6 +765,13 @@ compas_object* compas_b200_make_server(const compas_context* context, double mem
 int64_t compas_b200_server_submit(const compas_object* server, const compas_object* parameters,
                                   const compas_object* sequence, const compas_object* trajectory,
                                   const compas_array* coils, const compas_array* data, uint64_t echo_key) {
+    return compas_b200_server_submit_flags(server, parameters, sequence, trajectory, coils, data, echo_key, 0);
+}
+
+int64_t compas_b200_server_submit_flags(const compas_object* server, const compas_object* parameters,
+                                        const compas_object* sequence, const compas_object* trajectory,
+                                        const compas_array* coils, const compas_array* data, uint64_t echo_key,
+                                        int flags) {
     t_has_error = false;
     const int64_t id = guarded([&]() -> int64_t {
         compas::ServeRequest r;
@@ -692,6 +789,7 @@ int64_t compas_b200_server_submit(const compas_object* server, const compas_obje
         r.coil_sensitivities = array_of<cfloat, 2>(coils, "coils");
         r.data = array_of<cfloat, 3>(data, "data");
         r.echo_key = echo_key;
+        r.inject_wait_timeout = (flags & COMPAS_B200_REQUEST_INJECT_WAIT_TIMEOUT) != 0;
         return int64_t(server_of(server).submit(std::move(r)));
     });
     return t_has_error ? -1 : id;

@@ -76,6 +76,30 @@ __device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {  // c + a
     return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, c.y)));
 }
 
+// ------------------------------------------------------------------------------------------
+// two-wide FP32 arithmetic of sm_100 (FADD2 / FMUL2 / FFMA2): one instruction performs the
+// same round-to-nearest operation on .x and on .y, so two independent operands travel through
+// one issue slot. Results equal the scalar operations bit for bit.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+    return __fadd2_rn(a, b);
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d)
+        : "l"(*reinterpret_cast<const unsigned long long*>(&a)), "l"(*reinterpret_cast<const unsigned long long*>(&b)));
+    return *reinterpret_cast<const float2*>(&d);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+    return __fmul2_rn(a, b);
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {  // a*b + c, one rounding
+    return __ffma2_rn(a, b, c);
+}
+__device__ __forceinline__ float2 bcast2(float s) {
+    return make_float2(s, s);
+}
+
 // e^{i·2π·turns}: accurate for any magnitude of `turns` (sincospi reduces exactly)
 __device__ __forceinline__ float2 cis_turns(double turns) {
     double frac = turns - rint(turns);  // exact in FP64 for |turns| < 2^52

@@ -1,7 +1,7 @@
 // fisp.cu — FISP extended-phase-graph simulation on sm_100a.
 //
 // Restates the reference's FISP EPG recurrence (src/operators/epg.cuh:13-322,
-// src/simulate/fisp_kernels.cuh:99-223, src/simulate/fisp.cu:269-402) with a layout
+// src/simulate/fisp_kernels.cuh:99-223, src/simulate/fisp.cu:7-140) with a layout
 // chosen for B200:
 //
 // * Work unit: one (voxel, slice position) pair per group of G lanes; each lane keeps
@@ -118,29 +118,19 @@ struct EPG {
 
     // dephasing gradient (epg.cuh:229-298): F- one state down with zero at ≥ N-1,
     // F+ one state up, F+0 = conj(F-0).
-    // ONEHOT selects how F-[N-1] is zeroed when the layout holds more than N states. With the
-    // argument block in a kernel parameter, the compare against N-1 per slot compiles to
-    // predicated moves. With the block in shared memory (work-queue kernel) the compiler folds
-    // that compare chain into one store at a run-time index, which moves the whole state to
-    // local memory; a one-hot bit test per slot keeps it in registers there. Both zero the
-    // same element, so the results are identical.
-    template<bool ONEHOT>
+    // When the layout holds more than N states, F-[N-1] is zeroed by a one-hot bit test per slot.
+    // Written as a compare of each slot index against N-1, the compiler may fold the unrolled
+    // chain into one store at a run-time index, which moves the whole state to local memory.
     __device__ __forceinline__ void shift(int sub, int N) {
         if constexpr (G == 1) {
 #pragma unroll
             for (int i = 0; i < K - 1; i++) g[i] = g[i + 1];
             g[K - 1] = make_float2(0.f, 0.f);
             if (N < K) {
-                if constexpr (ONEHOT) {
-                    const unsigned cut = 1u << (N - 1);
+                const unsigned cut = 1u << (N - 1);
 #pragma unroll
-                    for (int i = 0; i < K - 1; i++)
-                        if (cut & (1u << i)) g[i] = make_float2(0.f, 0.f);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < K; i++)
-                        if (i == N - 1) g[i] = make_float2(0.f, 0.f);
-                }
+                for (int i = 0; i < K - 1; i++)
+                    if (cut & (1u << i)) g[i] = make_float2(0.f, 0.f);
             }
 #pragma unroll
             for (int i = K - 1; i > 0; i--) u[i] = u[i - 1];
@@ -169,16 +159,10 @@ struct EPG {
             g[K - 1] = (sub == G - 1) ? make_float2(0.f, 0.f) : make_float2(gx, gy);
             const int lane_n = (N - 1) / K, slot_n = (N - 1) % K;
             if (sub == lane_n) {
-                if constexpr (ONEHOT) {
-                    const unsigned cut = 1u << slot_n;
+                const unsigned cut = 1u << slot_n;
 #pragma unroll
-                    for (int i = 0; i < K; i++)
-                        if (cut & (1u << i)) g[i] = make_float2(0.f, 0.f);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < K; i++)
-                        if (i == slot_n) g[i] = make_float2(0.f, 0.f);
-                }
+                for (int i = 0; i < K; i++)
+                    if (cut & (1u << i)) g[i] = make_float2(0.f, 0.f);
             }
 #pragma unroll
             for (int i = K - 1; i > 0; i--) u[i] = u[i - 1];
@@ -221,6 +205,167 @@ struct EPG {
 #pragma unroll
         for (int i = 0; i < K; i++) u[i] = g[i] = make_float2(0.f, 0.f);
     }
+
+    // inversion, spoiling, then longitudinal relaxation and regrowth over TI
+    __device__ __forceinline__ void invert_decay(float E1, int sub) {
+        invert_spoil();
+#pragma unroll
+        for (int i = 0; i < K; i++) z[i] = cscale(E1, z[i]);
+        if (sub == 0) z[0].x += 1.0f - E1;
+    }
+
+    __device__ __forceinline__ float2 f0() const { return u[0]; }  // F+ of state 0 (lane sub == 0)
+};
+
+// The excitation coefficients of make_coefs broadcast to both halves of a pair. The packed state
+// keeps -Im Z and forms -Im Q, which turns every negated coefficient of excite_state into a
+// positive one except -e_im (the two-wide FMA has no operand negation, so each negated copy would
+// cost a register pair).
+struct ExciteCoefs2 {
+    float2 A1, A2, A3, A4, dre, dim, ere, neim, f;
+    float bre, bim, bz;
+};
+
+__device__ __forceinline__ ExciteCoefs2 make_coefs2(float4 tab, float B1, float2 c, float E1, float beta) {
+    const ExciteCoefs k = make_coefs(tab, B1, c, E1, beta);
+    ExciteCoefs2 q;
+    q.A1 = bcast2(k.A1);
+    q.A2 = bcast2(k.A2);
+    q.A3 = bcast2(k.A3);
+    q.A4 = bcast2(k.A4);
+    q.dre = bcast2(k.dre);
+    q.dim = bcast2(k.dim);
+    q.ere = bcast2(k.ere);
+    q.neim = bcast2(-k.eim);
+    q.f = bcast2(k.f);
+    q.bre = k.bre;
+    q.bim = k.bim;
+    q.bz = k.bz;
+    return q;
+}
+
+// Packed-pair EPG state (one lane per voxel/position, 2·KP state slots): pair j holds state j in
+// .x and state j + KP in .y, one register pair per real component (Re/Im of F+, of conj(F-), and
+// Re Z and -Im Z). All states of a TR share the excitation coefficients, so every operation of
+// excite_state becomes one two-wide instruction (add2/mul2/fma2) on a pair: 26 issue slots per
+// two states instead of 52, with the same roundings as the scalar update (negating an operand or
+// a result is exact). Only the two states that cross the pair boundary in the dephasing shift
+// (KP-1 → KP for F+, KP → KP-1 for conj(F-)) move between halves.
+template<int KP>
+struct EPGPacked {
+    static_assert(KP >= 2, "at least two pairs");
+    static constexpr int K = 2 * KP;
+    float2 ur[KP], ui[KP], gr[KP], gi[KP], zr[KP], zn[KP];  // zn = -Im Z
+
+    __device__ __forceinline__ void init(int) {
+#pragma unroll
+        for (int j = 0; j < KP; j++) ur[j] = ui[j] = gr[j] = gi[j] = zr[j] = zn[j] = make_float2(0.f, 0.f);
+        zr[0].x = 1.0f;
+    }
+
+    // dephasing (epg.cuh:229-298): conj(F-) one state down (state s ← s+1, zero at ≥ N-1), F+ one
+    // state up (s ← s-1), F+0 = conj(F-0). The zeroing of state N-1 uses a one-hot bit test per
+    // slot, which keeps the state in registers.
+    __device__ __forceinline__ void shift(int, int N) {
+        const float cr = gr[0].y, ci = gi[0].y;  // conj(F-) of state KP → state KP-1
+#pragma unroll
+        for (int j = 0; j < KP - 1; j++) {
+            gr[j] = gr[j + 1];
+            gi[j] = gi[j + 1];
+        }
+        gr[KP - 1] = make_float2(cr, 0.f);
+        gi[KP - 1] = make_float2(ci, 0.f);
+        if (N == K - 1) {  // one padding slot (25 states in 26): state K-2 is pair KP-2, high half
+            gr[KP - 2].y = gi[KP - 2].y = 0.f;
+        } else if (N < K - 1) {
+            const unsigned cut = 1u << (N - 1);
+#pragma unroll
+            for (int j = 0; j < KP; j++) {
+                if (cut & (1u << j)) gr[j].x = gi[j].x = 0.f;
+                if (cut & (1u << (j + KP))) gr[j].y = gi[j].y = 0.f;
+            }
+        }
+        const float ar = ur[KP - 1].x, ai = ui[KP - 1].x;  // F+ of state KP-1 → state KP
+#pragma unroll
+        for (int j = KP - 1; j > 0; j--) {
+            ur[j] = ur[j - 1];
+            ui[j] = ui[j - 1];
+        }
+        ur[0] = make_float2(gr[0].x, ar);
+        ui[0] = make_float2(gi[0].x, ai);
+    }
+
+    // excite_state on a pair with Qn = -Im Q, zn = -Im Z and nQhi = -Im Qh:
+    //   Qh_r = A4·Qr + A3·Qn + d_im·zn,   -Qh_i = A2·Qr + A1·Qn + d_re·zn,
+    //   Z_r' = e_re·Pr - e_im·Pi + f·Z_r,   -Z_i' = e_re·Qn - e_im·Qr + f·zn
+    __device__ __forceinline__ void excite(const ExciteCoefs2& k, int) {
+#pragma unroll
+        for (int j = 0; j < KP; j++) {
+            const float2 Pr = add2(ur[j], gr[j]), Pi = add2(ui[j], gi[j]);
+            const float2 Qr = sub2(ur[j], gr[j]), Qn = sub2(gi[j], ui[j]);
+            const float2 Phr = fma2(k.A1, Pr, fma2(k.A2, Pi, mul2(k.dre, zr[j])));
+            const float2 Phi = fma2(k.A3, Pr, fma2(k.A4, Pi, mul2(k.dim, zr[j])));
+            const float2 Qhr = fma2(k.A4, Qr, fma2(k.A3, Qn, mul2(k.dim, zn[j])));
+            const float2 nQhi = fma2(k.A2, Qr, fma2(k.A1, Qn, mul2(k.dre, zn[j])));
+            const float2 nzr = fma2(k.ere, Pr, fma2(k.neim, Pi, mul2(k.f, zr[j])));
+            const float2 nzn = fma2(k.ere, Qn, fma2(k.neim, Qr, mul2(k.f, zn[j])));
+            ur[j] = add2(Phr, Qhr);
+            ui[j] = sub2(Phi, nQhi);
+            gr[j] = sub2(Phr, Qhr);
+            gi[j] = add2(Phi, nQhi);
+            zr[j] = nzr;
+            zn[j] = nzn;
+        }
+        ur[0].x += k.bre;
+        ui[0].x += k.bim;
+        gr[0].x += k.bre;
+        gi[0].x += k.bim;
+        zr[0].x += k.bz;
+    }
+
+    // F *= c (F+ by c, conj(F-) by c), Z *= E1, Z0 += 1 - E1
+    __device__ __forceinline__ void relax(float2 c, float E1, int) {
+        const float2 cx = bcast2(c.x), cy = bcast2(c.y), ncy = bcast2(-c.y), e1 = bcast2(E1);
+#pragma unroll
+        for (int j = 0; j < KP; j++) {
+            const float2 a = fma2(ur[j], cx, mul2(ui[j], ncy)), b = fma2(ur[j], cy, mul2(ui[j], cx));
+            const float2 d = fma2(gr[j], cx, mul2(gi[j], ncy)), e = fma2(gr[j], cy, mul2(gi[j], cx));
+            ur[j] = a;
+            ui[j] = b;
+            gr[j] = d;
+            gi[j] = e;
+            zr[j] = mul2(e1, zr[j]);
+            zn[j] = mul2(e1, zn[j]);
+        }
+        zr[0].x += 1.0f - E1;
+    }
+
+    __device__ __forceinline__ void invert_spoil() {
+#pragma unroll
+        for (int j = 0; j < KP; j++) {
+            ur[j] = ui[j] = gr[j] = gi[j] = make_float2(0.f, 0.f);
+            zr[j] = make_float2(-zr[j].x, -zr[j].y);
+            zn[j] = make_float2(-zn[j].x, -zn[j].y);
+        }
+    }
+
+    __device__ __forceinline__ void spoil() {
+#pragma unroll
+        for (int j = 0; j < KP; j++) ur[j] = ui[j] = gr[j] = gi[j] = make_float2(0.f, 0.f);
+    }
+
+    __device__ __forceinline__ void invert_decay(float E1, int) {
+        invert_spoil();
+        const float2 e1 = bcast2(E1);
+#pragma unroll
+        for (int j = 0; j < KP; j++) {
+            zr[j] = mul2(e1, zr[j]);
+            zn[j] = mul2(e1, zn[j]);
+        }
+        zr[0].x += 1.0f - E1;
+    }
+
+    __device__ __forceinline__ float2 f0() const { return make_float2(ur[0].x, ui[0].x); }
 };
 
 // Forward-mode tangents ∂/∂T1 and ∂/∂T2 carried with the state.
@@ -250,11 +395,10 @@ struct EPGTangent {
         }
     }
 
-    template<bool ONEHOT>
     __device__ __forceinline__ void shift(int sub, int N) {
-        x.template shift<ONEHOT>(sub, N);
-        d1.template shift<ONEHOT>(sub, N);
-        d2.template shift<ONEHOT>(sub, N);
+        x.shift(sub, N);
+        d1.shift(sub, N);
+        d2.shift(sub, N);
     }
 
     // z - δ_{n0}: the regrowth's share of ∂Z/∂E1 (state 0 lives in slot 0 of lane 0)
@@ -316,9 +460,18 @@ struct EPGTangent {
     }
 };
 
-// One voxel tile (VB = 32/G voxels, all slice positions) of a FISP simulation; the CTA's W
-// warps sweep the positions. Shared by the one-simulation kernel (tile = blockIdx.x) and the
-// batched work-queue kernel (tile taken from the queue), so both give bit-identical echoes.
+// The work of a FISP simulation is a list of items (voxel tile, slice position), tile-major:
+// item = tile·P + p, a tile being VB = 32/G voxels. A CTA runs a contiguous range of items in
+// rounds of W: in each round warp w runs item base + w (its whole TR sequence), so a round may
+// hold the last positions of one tile and the first of the next and no warp idles at a tile's
+// end (35 positions on 8 warps no longer leave a round of 3). The one-simulation kernel gives each
+// CTA a contiguous range of whole tiles; the batched work-queue kernel runs one tile per queue
+// item. Both call this function.
+// Summation: the echo of a voxel is the sum over positions in increasing p, accumulated one
+// position at a time, ((s_0 + s_1) + s_2) + … . A round adds its positions of a tile to the
+// partial sum the previous round wrote to the echo array, so the result does not depend on how
+// the items fall into rounds: the work-queue kernel gives the same bits as the one-simulation
+// kernel.
 // TRs per sample chunk: the CTA's warps meet at a barrier once per chunk to sum their positions'
 // samples in shared memory ([W][chunk][VB] per sample plane). The split-lane tangent layouts use
 // 64 TRs, halving their barriers (271 -> 266 ms on the 224² MR-STAT slice); the value kernel keeps
@@ -327,68 +480,81 @@ struct EPGTangent {
 template<int G, bool TAN>
 constexpr int kFispChunk = (TAN && G > 1) ? 64 : 32;
 
+// state type of a layout: PACKED (G = 1, K even) → EPGPacked<K/2>; TAN → EPGTangent; else EPG
+template<int K, int G, bool TAN, bool PACKED>
+using FispState = std::conditional_t<TAN, EPGTangent<K, G>, std::conditional_t<PACKED, EPGPacked<K / 2>, EPG<K, G>>>;
+
 // TAN: also propagate ∂/∂T1 and ∂/∂T2 (EPGTangent) and write them to a.dT1, a.dT2; the
 // value goes through the same operations either way.
-template<int K, int G, bool ONEHOT, bool TAN = false>
-__device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, float2* samples) {
+template<int K, int G, bool TAN = false, bool PACKED = false>
+__device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_begin, const int item_end,
+                                           float2* samples) {
+    static_assert(!PACKED || (G == 1 && K % 2 == 0 && !TAN), "packed layouts hold one voxel per lane");
     constexpr int VB = 32 / G;
     const int W = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grp = lane / G, sub = lane % G;
+    const int P = a.P;
     // a group size that does not divide 32 leaves the last 32 % G lanes without a voxel: they run
     // alongside (on a clamped voxel) and write nothing
     constexpr bool kSpareLanes = (32 % G) != 0;
     const bool writer = sub == 0 && (!kSpareLanes || grp < VB);
-    const int vloc = tile * VB + (kSpareLanes ? min(grp, VB - 1) : grp);
-    const bool vok = vloc < a.nvoxels;
-    const int64_t vcol = a.voxel_begin + (vok ? vloc : a.nvoxels - 1);
-
-    const float T1 = a.params[0 * a.param_stride + vcol];
-    const float T2 = a.params[1 * a.param_stride + vcol];
-    const float B1 = a.params[2 * a.param_stride + vcol];
-    const float B0 = a.params[3 * a.param_stride + vcol];
-
-    // per-voxel relaxation factors (fisp_kernels.cuh:110-144)
-    const float R1 = 1.0f / T1, R2 = 1.0f / T2;
-    auto rot = [&](float dt) -> float2 {
-        if (B0 == 0.0f) return make_float2(1.f, 0.f);
-        float s, c;
-        sincospif(2.0f * dt * B0, &s, &c);
-        return make_float2(c, s);
-    };
-    const float E1_TR = expf(-a.TR * R1), E2_TR = expf(-a.TR * R2);
-    const float2 c_TR = cscale(E2_TR, rot(a.TR));
-    const float2 c_TE = cscale(expf(-a.TE * R2), rot(a.TE));
-    const float E1_TI = expf(-a.TI * R1);
-    const float E1_W = expf(-a.TW * R1);
-    const float2 c_W = cscale(expf(-a.TW * R2), rot(a.TW));
-    const float beta = 1.0f - E1_TR;
-    // tangent factors t/T1², t/T2² of each relaxation interval
-    const float s1_TR = a.TR * R1 * R1, s2_TR = a.TR * R2 * R2, s2_TE = a.TE * R2 * R2;
-    const float s1_TI = a.TI * R1 * R1, s1_W = a.TW * R1 * R1, s2_W = a.TW * R2 * R2;
     constexpr int CH = kFispChunk<G, TAN>;
     const int plane = W * CH * VB;  // sample planes: value, ∂/∂T1, ∂/∂T2
     constexpr int NQ = TAN ? 3 : 1;
 
-    const int nrounds = (a.P + W - 1) / W;
-    for (int round = 0; round < nrounds; round++) {
-        const int p = round * W + warp;
-        const bool pok = p < a.P;  // warp-uniform
-        const float4* tab = a.table + int64_t(pok ? p : 0) * a.nTR;
-        std::conditional_t<TAN, EPGTangent<K, G>, EPG<K, G>> st;
+    for (int base = item_begin; base < item_end; base += W) {
+        const int nact = min(W, item_end - base);  // warps with an item this round
+        const int item = base + min(warp, nact - 1);
+        const bool pok = warp < nact;  // warp-uniform
+        const int tile = item / P, p = item % P;
+        const int vloc = tile * VB + (kSpareLanes ? min(grp, VB - 1) : grp);
+        const bool vok = vloc < a.nvoxels;
+        const int64_t vcol = a.voxel_begin + (vok ? vloc : a.nvoxels - 1);
+
+        const float T1 = a.params[0 * a.param_stride + vcol];
+        const float T2 = a.params[1 * a.param_stride + vcol];
+        const float B1 = a.params[2 * a.param_stride + vcol];
+        const float B0 = a.params[3 * a.param_stride + vcol];
+
+        // per-voxel relaxation factors (fisp_kernels.cuh:110-144)
+        const float R1 = 1.0f / T1, R2 = 1.0f / T2;
+        auto rot = [&](float dt) -> float2 {
+            if (B0 == 0.0f) return make_float2(1.f, 0.f);
+            float s, c;
+            sincospif(2.0f * dt * B0, &s, &c);
+            return make_float2(c, s);
+        };
+        const float E1_TR = expf(-a.TR * R1), E2_TR = expf(-a.TR * R2);
+        const float2 c_TR = cscale(E2_TR, rot(a.TR));
+        const float2 c_TE = cscale(expf(-a.TE * R2), rot(a.TE));
+        const float E1_TI = expf(-a.TI * R1);
+        const float E1_W = expf(-a.TW * R1);
+        const float2 c_W = cscale(expf(-a.TW * R2), rot(a.TW));
+        const float beta = 1.0f - E1_TR;
+        // tangent factors t/T1², t/T2² of each relaxation interval
+        const float s1_TR = a.TR * R1 * R1, s2_TR = a.TR * R2 * R2, s2_TE = a.TE * R2 * R2;
+        const float s1_TI = a.TI * R1 * R1, s1_W = a.TW * R1 * R1, s2_W = a.TW * R2 * R2;
+
+        // segments of this round: runs of consecutive warps on the same tile (bit w set where
+        // warp w starts one); every thread derives the same mask
+        unsigned starts = 0;
+        for (int w = 0; w < nact; w++)
+            if (w == 0 || (base + w) / P != (base + w - 1) / P) starts |= 1u << w;
+        const int nseg = __popc(starts);
+
+        const float4* tab = a.table + int64_t(p) * a.nTR;
+        FispState<K, G, TAN, PACKED> st;
         st.init(sub);
         for (int rep = a.reps; rep >= 1; rep--) {
             const bool sampled = (rep == 1);
             if (a.inversion) {  // invert, spoil, decay(TI), regrowth (fisp_kernels.cuh:146-152)
-                if constexpr (TAN) {
-                    st.invert_decay(E1_TI, s1_TI, sub);
-                } else {
-                    st.invert_spoil();
-#pragma unroll
-                    for (int i = 0; i < K; i++) st.z[i] = cscale(E1_TI, st.z[i]);
-                    if (sub == 0) st.z[0].x += 1.0f - E1_TI;
-                }
+                if constexpr (TAN) st.invert_decay(E1_TI, s1_TI, sub);
+                else st.invert_decay(E1_TI, sub);
             }
+            // the RF table entry of the next TR is loaded one TR ahead, so its latency hides behind
+            // a whole TR of state updates (the last load repeats entry nTR-1: in bounds)
+            float4 tv_next = __ldg(tab);
             for (int t0 = 0; t0 < a.nTR; t0 += CH) {
                 const int nt = min(CH, a.nTR - t0);
                 if (pok) {
@@ -399,12 +565,13 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
 #pragma unroll 2
                     for (int j = 0; j < nt; j++) {
                         const int t = t0 + j;
-                        const float4 tv = __ldg(tab + t);
+                        const float4 tv = tv_next;
+                        tv_next = __ldg(tab + min(t + 1, a.nTR - 1));
                         if constexpr (TAN) {
                             if (t == 0) {
                                 st.excite(make_coefs(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), 0.0f, 0.0f, sub);
                             } else {
-                                st.template shift<ONEHOT>(sub, a.N);
+                                st.shift(sub, a.N);
                                 st.excite(make_coefs(tv, B1, c_TR, E1_TR, beta), s1_TR, s2_TR, sub);
                             }
                             if (sampled && writer) {
@@ -415,35 +582,53 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
                                                                       fmaf(s2_TE, st.x.u[0].y, st.d2.u[0].y)));
                             }
                         } else {
-                            if (t == 0) {
-                                st.excite(make_coefs(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), sub);
+                            if constexpr (PACKED) {
+                                if (t == 0) {
+                                    st.excite(make_coefs2(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), sub);
+                                } else {
+                                    st.shift(sub, a.N);
+                                    st.excite(make_coefs2(tv, B1, c_TR, E1_TR, beta), sub);
+                                }
                             } else {
-                                st.template shift<ONEHOT>(sub, a.N);
-                                st.excite(make_coefs(tv, B1, c_TR, E1_TR, beta), sub);
+                                if (t == 0) {
+                                    st.excite(make_coefs(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), sub);
+                                } else {
+                                    st.shift(sub, a.N);
+                                    st.excite(make_coefs(tv, B1, c_TR, E1_TR, beta), sub);
+                                }
                             }
-                            if (sampled && writer) samples[(warp * CH + j) * VB + grp] = cmul(c_TE, st.u[0]);
+                            if (sampled && writer) samples[(warp * CH + j) * VB + grp] = cmul(c_TE, st.f0());
                         }
                     }
-                } else if (sampled && writer) {
-                    for (int j = 0; j < nt; j++)
-                        for (int q = 0; q < NQ; q++) samples[q * plane + (warp * CH + j) * VB + grp] = make_float2(0.f, 0.f);
                 }
                 if (sampled) {
                     __syncthreads();
-                    // Σ over the warps' positions in fixed order, then write / accumulate the
-                    // undersampling-expanded rows (fisp_kernels.cuh:246-259)
-                    for (int e = threadIdx.x; e < NQ * nt * VB; e += blockDim.x) {
-                        const int qn = e / (nt * VB), j = (e / VB) % nt, gv = e % VB;
-                        const int v = tile * VB + gv;
-                        float2 acc = make_float2(0.f, 0.f);
-                        for (int w = 0; w < W; w++) acc = cadd(acc, samples[qn * plane + (w * CH + j) * VB + gv]);
-                        if (v < a.nvoxels) {
-                            float2* out = qn == 0 ? a.echo : qn == 1 ? a.dT1 : a.dT2;
-                            for (int q = 0; q < a.uf; q++) {
-                                float2* dst = out + (int64_t(t0 + j) * a.uf + q) * a.echo_stride + a.voxel_begin + v;
-                                *dst = round == 0 ? acc : cadd(*dst, acc);
+                    // per segment, add its positions in increasing order to the tile's partial
+                    // sum (the echo rows, unless the segment starts at position 0), then write
+                    // the undersampling-expanded rows (fisp_kernels.cuh:246-259)
+                    const int span = nt * VB;
+                    for (int e = threadIdx.x; e < NQ * nseg * span; e += blockDim.x) {
+                        const int qn = e / (nseg * span), rest = e % (nseg * span);
+                        const int sgi = rest / span, j = (rest % span) / VB, gv = rest % VB;
+                        int w0 = 0;  // first warp of segment sgi: the (sgi+1)-th set bit of `starts`
+                        for (int w = 0, c = 0; w < nact; w++) {
+                            if (starts & (1u << w)) {
+                                if (c == sgi) {
+                                    w0 = w;
+                                    break;
+                                }
+                                c++;
                             }
                         }
+                        const int seg_tile = (base + w0) / P;
+                        const int v = seg_tile * VB + gv;
+                        if (v >= a.nvoxels) continue;
+                        float2* out = qn == 0 ? a.echo : qn == 1 ? a.dT1 : a.dT2;
+                        const float2* col = samples + qn * plane + j * VB + gv;
+                        float2* row0 = out + int64_t(t0 + j) * a.uf * a.echo_stride + a.voxel_begin + v;
+                        float2 acc = (base + w0) % P == 0 ? col[w0 * CH * VB] : cadd(*row0, col[w0 * CH * VB]);
+                        for (int w = w0 + 1; w < nact && !(starts & (1u << w)); w++) acc = cadd(acc, col[w * CH * VB]);
+                        for (int q = 0; q < a.uf; q++) row0[int64_t(q) * a.echo_stride] = acc;
                     }
                     __syncthreads();
                 }
@@ -452,12 +637,12 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
                 if (pok) {
                     if constexpr (TAN) {
                         st.relax(c_TR, E1_TR, s1_TR, s2_TR, sub);
-                        st.template shift<ONEHOT>(sub, a.N);
+                        st.shift(sub, a.N);
                         if (a.wait_spoil) st.spoil();
                         st.relax(c_W, E1_W, s1_W, s2_W, sub);
                     } else {
                         st.relax(c_TR, E1_TR, sub);
-                        st.template shift<ONEHOT>(sub, a.N);
+                        st.shift(sub, a.N);
                         if (a.wait_spoil) st.spoil();
                         st.relax(c_W, E1_W, sub);
                     }
@@ -467,22 +652,25 @@ __device__ __forceinline__ void fisp_tile(const FispArgs& a, const int tile, flo
     }
 }
 
-// Zeroing form of the one-simulation kernel: the compare chain only for 25 states in one lane,
-// where it measured 6 % faster on B200 (69.7 vs 73.8 ms on the 224² MR-STAT slice); the
-// one-hot test elsewhere, where the compare chain puts the state in local memory (K = 16, 20).
-template<int K, int G>
-constexpr bool kOneHotZeroing = !(K == 25 && G == 1);
-
-template<int K, int G>
-__global__ void __launch_bounds__(256, 1) fisp_epg_kernel(FispArgs a) {
+// Range of whole tiles of CTA `cta` when `ntiles` tiles are split over `nctas` CTAs (sizes differ
+// by at most one tile).
+__device__ __forceinline__ int2 cta_tile_range(int ntiles, int cta, int nctas) {
+    return make_int2(int(int64_t(ntiles) * cta / nctas), int(int64_t(ntiles) * (cta + 1) / nctas));
+}
+// One FISP simulation: a persistent grid of CTAs, each running a contiguous range of whole voxel
+// tiles (cta_tile_range). PACKED: the two-wide layout EPGPacked<K/2> (one lane per voxel).
+template<int K, int G, bool PACKED = false>
+__global__ void __launch_bounds__(256, 1) fisp_epg_kernel(FispArgs a, int ntiles) {
     extern __shared__ float2 samples[];  // [W][32][VB]
-    fisp_tile<K, G, kOneHotZeroing<K, G>>(a, blockIdx.x, samples);
+    if (a.skip != nullptr && *a.skip != 0) return;  // uniform over the grid
+    const int2 r = cta_tile_range(ntiles, blockIdx.x, gridDim.x);
+    fisp_items<K, G, false, PACKED>(a, r.x * a.P, r.y * a.P, samples);
 }
 
-// Persistent work-queue kernel for a batch of FISP simulations sharing one (K, G, W) layout:
+// Persistent work-queue kernel for a batch of FISP simulations sharing one layout and W:
 // each CTA takes (job, tile) items from `items` in order through an atomic counter until the
 // queue is empty. Items are ordered longest job first, so the last wave is short.
-template<int K, int G>
+template<int K, int G, bool PACKED = false>
 __global__ void __launch_bounds__(256, 1) fisp_queue_kernel(const FispArgs* __restrict__ jobs,
                                                             const int2* __restrict__ items, int nitems,
                                                             int* __restrict__ head) {
@@ -497,26 +685,24 @@ __global__ void __launch_bounds__(256, 1) fisp_queue_kernel(const FispArgs* __re
         const int2 w = items[it];
         if (threadIdx.x == 0) job = jobs[w.x];
         __syncthreads();
-        fisp_tile<K, G, true>(job, w.y, samples);
+        fisp_items<K, G, false, PACKED>(job, w.y * job.P, (w.y + 1) * job.P, samples);
         __syncthreads();  // job and s_item are rewritten by the next item
     }
 }
 
 // One FISP simulation with its T1 and T2 tangents: value, ∂/∂T1, ∂/∂T2 into a.echo, a.dT1, a.dT2.
 template<int K, int G>
-__global__ void __launch_bounds__(256, 1) fisp_tangent_kernel(FispArgs a) {
-    extern __shared__ float2 samples[];  // [3][W][32][VB]
-    fisp_tile<K, G, kOneHotZeroing<K, G>, true>(a, blockIdx.x, samples);
+__global__ void __launch_bounds__(256, 1) fisp_tangent_kernel(FispArgs a, int ntiles) {
+    extern __shared__ float2 samples[];  // [3][W][chunk][VB]
+    const int2 r = cta_tile_range(ntiles, blockIdx.x, gridDim.x);
+    fisp_items<K, G, true>(a, r.x * a.P, r.y * a.P, samples);
 }
 
 // Work-queue form of fisp_tangent_kernel for batches (same items and order as fisp_queue_kernel).
-// Every tangent layout zeroes with the one-hot test, as the one-simulation tangent kernel does, so
-// both give the same bits.
 template<int K, int G>
 __global__ void __launch_bounds__(256, 1) fisp_tangent_queue_kernel(const FispArgs* __restrict__ jobs,
                                                                     const int2* __restrict__ items, int nitems,
                                                                     int* __restrict__ head) {
-    static_assert(kOneHotZeroing<K, G>, "tangent layouts use one-hot zeroing");
     extern __shared__ float2 samples[];
     __shared__ FispArgs job;
     __shared__ int s_item;
@@ -528,7 +714,7 @@ __global__ void __launch_bounds__(256, 1) fisp_tangent_queue_kernel(const FispAr
         const int2 w = items[it];
         if (threadIdx.x == 0) job = jobs[w.x];
         __syncthreads();
-        fisp_tile<K, G, true, true>(job, w.y, samples);
+        fisp_items<K, G, true>(job, w.y * job.P, (w.y + 1) * job.P, samples);
         __syncthreads();
     }
 }
@@ -541,37 +727,31 @@ __global__ void __launch_bounds__(256, 1) fisp_tangent_queue_kernel(const FispAr
 
 namespace {
 
-using FispKernel = void (*)(kernels::FispArgs);
+using FispKernel = void (*)(kernels::FispArgs, int);
 using FispQueueKernel = void (*)(const kernels::FispArgs*, const int2*, int, int*);
 
 struct FispConfig {
     int K, G;
+    bool packed;  // EPGPacked<K/2>: two states per two-wide instruction
     FispKernel fn;
     FispQueueKernel queue;
 };
 
 // Instantiated layouts: (states per lane K, lanes per voxel/position G). Coverage K·G ≥ N.
+// The packed one-lane layouts come last, so the indices of the others (which a tuning table
+// names) keep their meaning.
+#define COMPAS_FISP(K, G) {K, G, false, kernels::fisp_epg_kernel<K, G>, kernels::fisp_queue_kernel<K, G>}
+#define COMPAS_FISP_PACKED(K) {K, 1, true, kernels::fisp_epg_kernel<K, 1, true>, kernels::fisp_queue_kernel<K, 1, true>}
 const FispConfig kFispConfigs[] = {
-    {1, 1, kernels::fisp_epg_kernel<1, 1>, kernels::fisp_queue_kernel<1, 1>},
-    {2, 1, kernels::fisp_epg_kernel<2, 1>, kernels::fisp_queue_kernel<2, 1>},
-    {4, 1, kernels::fisp_epg_kernel<4, 1>, kernels::fisp_queue_kernel<4, 1>},
-    {6, 1, kernels::fisp_epg_kernel<6, 1>, kernels::fisp_queue_kernel<6, 1>},
-    {8, 1, kernels::fisp_epg_kernel<8, 1>, kernels::fisp_queue_kernel<8, 1>},
-    {12, 1, kernels::fisp_epg_kernel<12, 1>, kernels::fisp_queue_kernel<12, 1>},
-    {16, 1, kernels::fisp_epg_kernel<16, 1>, kernels::fisp_queue_kernel<16, 1>},
-    {20, 1, kernels::fisp_epg_kernel<20, 1>, kernels::fisp_queue_kernel<20, 1>},
-    {25, 1, kernels::fisp_epg_kernel<25, 1>, kernels::fisp_queue_kernel<25, 1>},
-    {2, 4, kernels::fisp_epg_kernel<2, 4>, kernels::fisp_queue_kernel<2, 4>},
-    {4, 2, kernels::fisp_epg_kernel<4, 2>, kernels::fisp_queue_kernel<4, 2>},
-    {4, 4, kernels::fisp_epg_kernel<4, 4>, kernels::fisp_queue_kernel<4, 4>},
-    {4, 8, kernels::fisp_epg_kernel<4, 8>, kernels::fisp_queue_kernel<4, 8>},
-    {7, 4, kernels::fisp_epg_kernel<7, 4>, kernels::fisp_queue_kernel<7, 4>},
-    {13, 2, kernels::fisp_epg_kernel<13, 2>, kernels::fisp_queue_kernel<13, 2>},
-    {8, 4, kernels::fisp_epg_kernel<8, 4>, kernels::fisp_queue_kernel<8, 4>},
-    {8, 8, kernels::fisp_epg_kernel<8, 8>, kernels::fisp_queue_kernel<8, 8>},
-    {8, 16, kernels::fisp_epg_kernel<8, 16>, kernels::fisp_queue_kernel<8, 16>},
-    {4, 32, kernels::fisp_epg_kernel<4, 32>, kernels::fisp_queue_kernel<4, 32>},
+    COMPAS_FISP(1, 1), COMPAS_FISP(2, 1), COMPAS_FISP(4, 1), COMPAS_FISP(6, 1), COMPAS_FISP(8, 1),
+    COMPAS_FISP(12, 1), COMPAS_FISP(16, 1), COMPAS_FISP(20, 1), COMPAS_FISP(25, 1),
+    COMPAS_FISP(2, 4), COMPAS_FISP(4, 2), COMPAS_FISP(4, 4), COMPAS_FISP(4, 8), COMPAS_FISP(7, 4),
+    COMPAS_FISP(13, 2), COMPAS_FISP(8, 4), COMPAS_FISP(8, 8), COMPAS_FISP(8, 16), COMPAS_FISP(4, 32),
+    COMPAS_FISP_PACKED(4), COMPAS_FISP_PACKED(8), COMPAS_FISP_PACKED(12), COMPAS_FISP_PACKED(16),
+    COMPAS_FISP_PACKED(20), COMPAS_FISP_PACKED(26),
 };
+#undef COMPAS_FISP
+#undef COMPAS_FISP_PACKED
 
 // Tangent layouts: three state vectors per (voxel, position), so at most 8 states per lane
 // (8 × 18 floats); the 25-state MR-STAT case splits over 5 lanes of 5 states (6 groups per warp,
@@ -604,6 +784,10 @@ bool fisp_config_info(int index, int* K, int* G) {
     return true;
 }
 
+bool fisp_config_packed(int index) {
+    return index >= 0 && index < fisp_config_count() && kFispConfigs[index].packed;
+}
+
 // Default layout choice for `N` states (from layout and autotuner timings on B200):
 //  * many (voxel, position) pairs: all states of a voxel in one lane (G = 1, K ≥ N) — no shuffles;
 //    25 states × 35 positions at 25600 voxels: 38.6 ms vs 51 ms for the best split layout;
@@ -616,15 +800,24 @@ FispLaunch fisp_default_launch(int N, int64_t nvoxels, int P) {
     const bool wide = pairs >= 148LL * 32 * 8;
     int best = -1;
     auto waste = [&](int i) { return kFispConfigs[i].K * kFispConfigs[i].G - N; };
+    // issue slots of the state update per lane and TR, in units of one state's 26 operations
+    auto cost = [&](int i) { return kFispConfigs[i].packed ? kFispConfigs[i].K / 2 : kFispConfigs[i].K; };
     for (int i = 0; i < fisp_config_count(); i++) {
         const auto& c = kFispConfigs[i];
         if (c.K * c.G < N) continue;
         bool preferred;
-        if (N <= 25 && wide) preferred = (c.G == 1);
+        if (N <= 26 && wide) preferred = (c.G == 1);
         else if (N <= 32 && !wide) preferred = (c.G == 4);
         else preferred = true;
         if (!preferred) continue;
-        if (best < 0 || waste(i) < waste(best) || (waste(i) == waste(best) && c.G < kFispConfigs[best].G)) best = i;
+        if (best < 0) {
+            best = i;
+        } else if (c.G == 1 && kFispConfigs[best].G == 1) {
+            // one lane per voxel: the fewest issue slots, then the least padding (scalar on ties)
+            if (cost(i) < cost(best) || (cost(i) == cost(best) && waste(i) < waste(best))) best = i;
+        } else if (waste(i) < waste(best) || (waste(i) == waste(best) && c.G < kFispConfigs[best].G)) {
+            best = i;
+        }
     }
     if (best < 0) {  // nothing matched the preference: the covering layout with the least waste
         for (int i = 0; i < fisp_config_count(); i++)
@@ -694,6 +887,7 @@ kernels::FispArgs fisp_args(const CompasContext& ctx, const TissueParameters& pa
     a.echo = reinterpret_cast<float2*>(echo);
     a.echo_stride = echo_stride;
     a.dT1 = a.dT2 = nullptr;
+    a.skip = nullptr;
     return a;
 }
 
@@ -715,6 +909,15 @@ size_t fisp_tangent_smem_bytes(int G, int W) {
     return 3 * size_t(W) * (G == 1 ? 32 : 64) * (32 / G) * sizeof(float2);  // ≤ 192 KB
 }
 
+// CTAs of `fn` resident on the device at once with this block size and dynamic shared memory:
+// the grid of the persistent one-simulation kernels
+int resident_ctas(const void* fn, int threads, size_t smem, int device) {
+    int per_sm = 1, sms = 148;
+    COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+    COMPAS_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    return std::max(1, per_sm) * sms;
+}
+
 // Opt in to `smem` bytes of dynamic shared memory. Without the attribute a launch may use at most
 // 48 KB minus the kernel's static shared memory (the work-queue kernels keep their job's argument
 // block there), so the attribute is set from 40 KB on.
@@ -731,7 +934,7 @@ int fisp_tile_voxels(FispLaunch L) {
 }
 
 void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
-                 const FISPSequence& seq, cfloat* echo, int64_t echo_stride, FispLaunch L) {
+                 const FISPSequence& seq, cfloat* echo, int64_t echo_stride, FispLaunch L, const int* skip) {
     const int nTR = int(seq.RF_train.size());
     const int P = int(seq.sliceprofiles.size(0));
     const int N = seq.max_state;
@@ -740,15 +943,17 @@ void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int v
         return;
     }
     if (L.config < 0) L = fisp_default_launch(N, nvoxels, P);
-    const kernels::FispArgs a = fisp_args(ctx, params, voxel_begin, nvoxels, seq, echo, echo_stride);
+    kernels::FispArgs a = fisp_args(ctx, params, voxel_begin, nvoxels, seq, echo, echo_stride);
+    a.skip = skip;
     const auto& cfg = checked_config(L, N);
     const int VB = 32 / cfg.G;
     const int W = std::max(1, std::min(L.warps, 8));
-    dim3 grid(div_ceil(nvoxels, VB)), block(32 * W);
+    const int ntiles = div_ceil(nvoxels, VB);
     const size_t smem = fisp_smem_bytes(cfg, W);
     DeviceGuard guard(ctx.device());
     allow_smem(reinterpret_cast<const void*>(cfg.fn), smem);
-    cfg.fn<<<grid, block, smem, ctx.stream()>>>(a);
+    const int grid = std::min(ntiles, resident_ctas(reinterpret_cast<const void*>(cfg.fn), 32 * W, smem, ctx.device()));
+    cfg.fn<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles);
     check_launch("fisp_epg_kernel");
 }
 
@@ -801,10 +1006,12 @@ void launch_fisp_tangent(const CompasContext& ctx, const TissueParameters& param
     a.dT2 = reinterpret_cast<float2*>(dT2);
     const int VB = 32 / cfg.G;
     const int W = std::max(1, std::min(L.warps, 8));
+    const int ntiles = div_ceil(nvoxels, VB);
     const size_t smem = fisp_tangent_smem_bytes(cfg.G, W);
     DeviceGuard guard(ctx.device());
     allow_smem(reinterpret_cast<const void*>(cfg.fn), smem);
-    cfg.fn<<<div_ceil(nvoxels, VB), 32 * W, smem, ctx.stream()>>>(a);
+    const int grid = std::min(ntiles, resident_ctas(reinterpret_cast<const void*>(cfg.fn), 32 * W, smem, ctx.device()));
+    cfg.fn<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles);
     check_launch("fisp_tangent_kernel");
 }
 

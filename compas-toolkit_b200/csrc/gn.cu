@@ -18,6 +18,13 @@
 //       q = J d;  α = γ/‖q‖²;  δ += α d;  b -= α q;  g = Re(Jᴴ b);  γ' = ‖g‖²;  d = g + (γ'/γ) d
 //   p ← (T1·c(δ0), T2·c(δ1), Re ρ + δ2, Im ρ + δ3) with c(x) = min(max(1 + x, ½), 2), which
 //   keeps T1, T2 positive for large steps.
+// With the line search (the default), the step is tried on the objective first: the trial
+// p(t) (δ scaled by t) is simulated, its signal and ‖y - s(p(t))‖² computed, and the first of
+// t = 1, ½ whose objective is not above ‖y - s(p)‖² is taken; if neither is, p stays, so the
+// objective never rises from one iteration to the next (the reference's objective:
+// src/utils/residual.cu:8-46). A graph cannot branch, so the kernels of the t = ½ trial read a
+// device flag and return at once when t = 1 was taken; and an accepted trial's echoes are m of
+// the next iteration's estimate, so that iteration copies them instead of simulating again.
 //
 // Scalars (γ, α, β, norms) stay on the device; every reduction uses a fixed grid and a fixed
 // summation order, so a replayed graph reproduces the eager iteration bit for bit.
@@ -45,7 +52,14 @@ constexpr int kRedBlocks = 296;  // fixed grid of every reduction: 2 CTAs per SM
 constexpr int kRedThreads = 256;
 
 // scalar slots in the device scalar array
-enum Scalar { kObjective = 0, kGamma = 1, kGammaNew = 2, kQQ = 3, kAlpha = 4, kBeta = 5, kNumScalars = 8 };
+enum Scalar {
+    kObjective = 0, kGamma = 1, kGammaNew = 2, kQQ = 3, kAlpha = 4, kBeta = 5,
+    kTrial = 6,       // ‖y - s(p(t))‖² of the last trial of the line search
+    kStepLength = 7,  // t taken by the line search: 1, ½, or 0 (no step)
+    kNumScalars = 8
+};
+// device flags of the line search
+enum Flag { kAccepted = 0, kHaveEchoes = 1, kNumFlags = 2 };
 
 __device__ __forceinline__ float block_sum(float v, float* red) {
     red[threadIdx.x] = v;
@@ -137,6 +151,59 @@ __global__ void gn_update_kernel(float* __restrict__ params, int64_t pstride, in
     params[5 * pstride + v] += x[3 * int64_t(nvoxels) + v];
 }
 
+// trial parameters p(t): T1·c(t·δ0), T2·c(t·δ1), ρ + t·(δ2 + iδ3), the other fields as in p (the
+// trial array holds them from construction). The first trial resets the accepted flag and the
+// step length; a later trial returns at once when an earlier one was taken.
+__global__ void gn_trial_kernel(const float* __restrict__ params, float* __restrict__ trial, int64_t pstride,
+                                int nvoxels, const float* __restrict__ x, float t, bool first, int* __restrict__ flags,
+                                float* __restrict__ scalars) {
+    if (first) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            flags[kAccepted] = 0;
+            scalars[kStepLength] = 0.0f;
+        }
+    } else if (flags[kAccepted] != 0) {
+        return;
+    }
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nvoxels) return;
+    const float c1 = fminf(fmaxf(fmaf(t, x[v], 1.0f), 0.5f), 2.0f);
+    const float c2 = fminf(fmaxf(fmaf(t, x[nvoxels + v], 1.0f), 0.5f), 2.0f);
+    trial[0 * pstride + v] = params[0 * pstride + v] * c1;
+    trial[1 * pstride + v] = params[1 * pstride + v] * c2;
+    trial[4 * pstride + v] = fmaf(t, x[2 * int64_t(nvoxels) + v], params[4 * pstride + v]);
+    trial[5 * pstride + v] = fmaf(t, x[3 * int64_t(nvoxels) + v], params[5 * pstride + v]);
+}
+
+// take step length t when no earlier trial was taken and this trial's objective is not above the
+// estimate's (a NaN objective is never taken)
+__global__ void gn_decide_kernel(float* __restrict__ scalars, int* __restrict__ flags, float t) {
+    if (flags[kAccepted] != 0) return;
+    if (scalars[kTrial] <= scalars[kObjective]) {
+        flags[kAccepted] = 1;
+        scalars[kStepLength] = t;
+    }
+}
+
+// p ← the taken trial (fields T1, T2, ρ); records whether the trial's echoes are m(p) now
+__global__ void gn_commit_kernel(float* __restrict__ params, const float* __restrict__ trial, int64_t pstride,
+                                 int nvoxels, int* __restrict__ flags) {
+    const bool taken = flags[kAccepted] != 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) flags[kHaveEchoes] = taken ? 1 : 0;
+    if (!taken) return;
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nvoxels) return;
+    for (int f : {0, 1, 4, 5}) params[f * pstride + v] = trial[f * pstride + v];
+}
+
+// echos ← the last taken trial's echoes, when they belong to the current estimate
+__global__ void gn_take_echoes_kernel(float2* __restrict__ echos, const float2* __restrict__ trial_echos, int64_t n,
+                                      const int* __restrict__ flags) {
+    if (flags[kHaveEchoes] == 0) return;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        echos[i] = trial_echos[i];
+}
+
 }  // namespace
 }  // namespace kernels
 
@@ -159,6 +226,11 @@ struct GaussNewtonStep::Impl {
     int cg_iterations = 4;
     float delta = DEFAULT_FINITE_DIFFERENCE_DELTA;
     Precision prec = Precision::SplitBF16;
+    bool line_search = true;
+    Array<float, 2> trial;          // trial parameters of the line search
+    Array<cfloat, 2> trial_echos;   // m(trial)
+    Array<cfloat, 3> trial_signal;  // s(trial)
+    Array<int> flags;               // kernels::Flag
 
     Array<cfloat, 2> echos, dT1, dT2;
     Array<cfloat, 3> signal, b, q;
@@ -169,14 +241,15 @@ struct GaussNewtonStep::Impl {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 
-    void simulate(const TissueParameters& p, cfloat* out) const {
+    // m(p) into `out`; with `skip`, nothing when *skip != 0 at run time
+    void simulate(const TissueParameters& p, cfloat* out, const int* skip = nullptr) const {
         const int V = p.nvoxels;
         if (const auto* f = std::get_if<FISPSequence>(&sequence)) {
-            launch_fisp(ctx, p, 0, V, *f, out, V,
-                        tuned_fisp_launch(f->max_state, V, int(f->sliceprofiles.size(0))));
+            launch_fisp(ctx, p, 0, V, *f, out, V, tuned_fisp_launch(f->max_state, V, int(f->sliceprofiles.size(0))),
+                        skip);
         } else {
             const auto& s = std::get<pSSFPSequence>(sequence);
-            launch_pssfp(ctx, p, 0, V, s, out, V, tuned_pssfp_launch(int(s.z.size()), V));
+            launch_pssfp(ctx, p, 0, V, s, out, V, tuned_pssfp_launch(int(s.z.size()), V), skip);
         }
     }
 
@@ -238,6 +311,13 @@ void GaussNewtonStep::Impl::enqueue() const {
             launch_pssfp_tangent(ctx, params, 0, V, s, echos.data(), dT1.data(), dT2.data(), V,
                                  tuned_pssfp_launch(int(s.z.size()), V));
         }
+    } else if (line_search) {
+        // the previous iteration's taken trial already simulated the estimate: copy its echoes
+        gn_take_echoes_kernel<<<eb, 256, 0, st>>>(reinterpret_cast<float2*>(echos.data()),
+                                                  reinterpret_cast<const float2*>(trial_echos.data()), necho,
+                                                  flags.data());
+        check_launch("gn_take_echoes_kernel");
+        simulate(params, echos.data(), flags.data() + kHaveEchoes);
     } else {
         simulate(params, echos.data());
     }
@@ -285,8 +365,34 @@ void GaussNewtonStep::Impl::enqueue() const {
                                                 reinterpret_cast<float2*>(d.data()), nv4, scalars.data());
         check_launch("cg_direction_kernel");
     }
-    gn_update_kernel<<<div_ceil(V, 256), 256, 0, st>>>(params.data.data(), pstride, V, x.data());
-    check_launch("gn_update_kernel");
+    if (!line_search) {
+        gn_update_kernel<<<div_ceil(V, 256), 256, 0, st>>>(params.data.data(), pstride, V, x.data());
+        check_launch("gn_update_kernel");
+        return;
+    }
+
+    // line search on the objective: t = 1, then t = ½ (whose kernels return at once if 1 was taken)
+    const TissueParameters tp(trial, params.has_z, params.has_b0, params.has_b1);
+    const float steps[2] = {1.0f, 0.5f};
+    for (int k = 0; k < 2; k++) {
+        gn_trial_kernel<<<div_ceil(V, 256), 256, 0, st>>>(pdata, trial.data(), pstride, V, x.data(), steps[k], k == 0,
+                                                          flags.data(), scalars.data());
+        check_launch("gn_trial_kernel");
+        simulate(tp, trial_echos.data(), k == 0 ? nullptr : flags.data() + kAccepted);
+        if (cart)
+            launch_signal_cartesian(ctx, trial.data(), pstride, V, trial_echos.data(), coils.data(), C, geo,
+                                    trial_signal.data(), prec);
+        else
+            launch_signal_spiral(ctx, trial.data(), pstride, V, trial_echos.data(), coils.data(), C, spiral->nreadouts,
+                                 spiral->samples_per_readout, spiral->delta_t, spiral->k_start.data(),
+                                 spiral->delta_k.data(), trial_signal.data(), prec);
+        launch_residual(ctx, data.data(), trial_signal.data(), nsig, q.data(), partials.data(), npartials,
+                        scalars.data() + kTrial);
+        gn_decide_kernel<<<1, 1, 0, st>>>(scalars.data(), flags.data(), steps[k]);
+        check_launch("gn_decide_kernel");
+    }
+    gn_commit_kernel<<<div_ceil(V, 256), 256, 0, st>>>(params.data.data(), trial.data(), pstride, V, flags.data());
+    check_launch("gn_commit_kernel");
 }
 
 GaussNewtonStep::GaussNewtonStep(const CompasContext& ctx, TissueParameters parameters,
@@ -340,6 +446,13 @@ GaussNewtonStep::GaussNewtonStep(const CompasContext& ctx, TissueParameters para
     im.d = Array<cfloat, 2>({4, V}, dev, ctx.stream());
     im.x = Array<float, 2>({4, V}, dev, ctx.stream());
     im.scalars = Array<float>({kernels::kNumScalars}, dev, ctx.stream());
+    im.trial = Array<float, 2>({TissueParameterField::NUM_FIELDS, V}, dev, ctx.stream());
+    COMPAS_CUDA_CHECK(cudaMemcpyAsync(im.trial.data(), own.data(), own.nbytes(), cudaMemcpyDeviceToDevice,
+                                      ctx.stream()));
+    im.trial_echos = Array<cfloat, 2>({R, V}, dev, ctx.stream());
+    im.trial_signal = Array<cfloat, 3>({C, R, S}, dev, ctx.stream());
+    im.flags = Array<int>({kernels::kNumFlags}, dev, ctx.stream());
+    COMPAS_CUDA_CHECK(cudaMemsetAsync(im.flags.data(), 0, im.flags.nbytes(), ctx.stream()));
     im.npartials = residual_partial_count(im.signal.numel());
     im.partials = Array<float>({std::max(im.npartials, kernels::kRedBlocks)}, dev, ctx.stream());
     COMPAS_CUDA_CHECK(cudaMemsetAsync(im.scalars.data(), 0, im.scalars.nbytes(), ctx.stream()));
@@ -371,6 +484,24 @@ void GaussNewtonStep::run(bool use_graph) {
         COMPAS_CUDA_CHECK(cudaGraphInstantiate(&im.exec, im.graph, 0));
     }
     COMPAS_CUDA_CHECK(cudaGraphLaunch(im.exec, im.ctx.stream()));
+}
+
+void GaussNewtonStep::set_line_search(bool on) {
+    Impl& im = *m_impl;
+    if (im.line_search == on) return;
+    im.ctx.synchronize();
+    if (im.exec) cudaGraphExecDestroy(im.exec);
+    if (im.graph) cudaGraphDestroy(im.graph);
+    im.exec = nullptr;
+    im.graph = nullptr;
+    im.line_search = on;
+    // the estimate's echoes are simulated again on the next run
+    DeviceGuard guard(im.ctx.device());
+    COMPAS_CUDA_CHECK(cudaMemsetAsync(im.flags.data(), 0, im.flags.nbytes(), im.ctx.stream()));
+}
+
+bool GaussNewtonStep::line_search() const {
+    return m_impl->line_search;
 }
 
 int GaussNewtonStep::kernels_per_iteration() const {

@@ -24,6 +24,7 @@ struct FispArgs {
     int64_t echo_stride;
     float2* dT1;           // ∂echo/∂T1, ∂echo/∂T2 (same layout); used by the tangent kernels only
     float2* dT2;
+    const int* skip;       // one-simulation kernel: returns at once when *skip != 0 (null: never)
 };
 
 struct PssfpArgs {
@@ -38,6 +39,7 @@ struct PssfpArgs {
     int64_t echo_stride;
     float2* dT1;   // ∂echo/∂T1, ∂echo/∂T2 (same layout); used by the tangent kernels only
     float2* dT2;
+    const int* skip;  // one-simulation kernel: returns at once when *skip != 0 (null: never)
 };
 
 struct SpiralArgs {

@@ -16,13 +16,17 @@ struct FispLaunch {
 };
 int fisp_config_count();
 bool fisp_config_info(int index, int* K, int* G);
+bool fisp_config_packed(int index);  // EPGPacked layout (two states per FFMA2)
 FispLaunch fisp_default_launch(int N, int64_t nvoxels, int P);
 FispLaunch tuned_fisp_launch(int N, int64_t nvoxels, int P);
 const Array<float, 3>& fisp_excite_table(const CompasContext& ctx, const FISPSequence& seq);
 // simulates voxels [voxel_begin, voxel_begin + nvoxels) of `params` into echo columns
 // voxel_begin.. of a [nTR*uf][echo_stride] complex array
+// `skip` (device int, may be null): when it holds a nonzero value at run time the kernel returns
+// without writing (a step of a captured graph that is not needed this time)
 void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
-                 const FISPSequence& seq, cfloat* echo, int64_t echo_stride, FispLaunch L);
+                 const FISPSequence& seq, cfloat* echo, int64_t echo_stride, FispLaunch L,
+                 const int* skip = nullptr);
 // argument block of one FISP simulation (validates the sequence, builds its table on first use)
 kernels::FispArgs fisp_args(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
                             const FISPSequence& seq, cfloat* echo, int64_t echo_stride);
@@ -54,7 +58,8 @@ bool pssfp_config_info(int index, int* ZT, int* GZ);
 PssfpLaunch pssfp_default_launch(int nz, int64_t nvoxels);
 PssfpLaunch tuned_pssfp_launch(int nz, int64_t nvoxels);
 void launch_pssfp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
-                  const pSSFPSequence& seq, cfloat* echo, int64_t echo_stride, PssfpLaunch L);
+                  const pSSFPSequence& seq, cfloat* echo, int64_t echo_stride, PssfpLaunch L,
+                  const int* skip = nullptr);
 kernels::PssfpArgs pssfp_args(const CompasContext& ctx, const TissueParameters& params, int voxel_begin,
                               int nvoxels, const pSSFPSequence& seq, cfloat* echo, int64_t echo_stride);
 int pssfp_tile_voxels(PssfpLaunch L);
@@ -151,5 +156,9 @@ void launch_signal_spiral_batch(cudaStream_t stream, int device, int coil_group,
                                 const int* cta_offsets, int njobs, int ctas);
 void launch_sum_partials_batch(cudaStream_t stream, int device, const kernels::PartialSum* jobs,
                                const int* block_offsets, int njobs, int blocks);
+
+// a one-thread kernel whose bounded wait on a barrier nobody completes gives up after
+// `limit_cycles` SM cycles and records STATUS_WAIT_TIMEOUT in ctx's status word (diag.cu)
+void launch_wait_probe(const CompasContext& ctx, long long limit_cycles);
 
 }  // namespace compas

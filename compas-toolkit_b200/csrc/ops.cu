@@ -37,7 +37,7 @@ __global__ void fill_kernel(float* p, int64_t n, float value) {
         p[i] = value;
 }
 
-// echo[r][v]·exp(i y_v Im k_start[r])   (src/trajectories/phase_encoding_kernels.cuh:225-240)
+// echo[r][v]·exp(i y_v Im k_start[r])   (src/trajectories/phase_encoding_kernels.cuh:10-25)
 // One voxel per thread; the CTA rows stride over the readouts, so y is read once per voxel and a
 // few thousand CTAs cover the array.
 __global__ void phase_encoding_kernel(const float2* __restrict__ echo, const float* __restrict__ params,
@@ -53,7 +53,7 @@ __global__ void phase_encoding_kernel(const float2* __restrict__ echo, const flo
     }
 }
 
-// d = lhs - rhs, per-block Σ|d|² (fixed-order tree)   (src/utils/residual_kernels.cuh:73-96)
+// d = lhs - rhs, per-block Σ|d|² (fixed-order tree)   (src/utils/residual_kernels.cuh:26-64)
 __global__ void residual_kernel(const float2* __restrict__ lhs, const float2* __restrict__ rhs, int64_t n,
                                 float2* __restrict__ out, float* __restrict__ partials) {
     __shared__ float red[256];

@@ -261,6 +261,7 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
 
 template<int ZT, int GZ>
 __global__ void __launch_bounds__(128) pssfp_kernel(PssfpArgs a) {
+    if (a.skip != nullptr && *a.skip != 0) return;  // uniform over the grid
     pssfp_tile<ZT, GZ>(a, blockIdx.x);
 }
 
@@ -417,6 +418,7 @@ kernels::PssfpArgs pssfp_args(const CompasContext& ctx, const TissueParameters& 
     a.echo = reinterpret_cast<float2*>(echo);
     a.echo_stride = echo_stride;
     a.dT1 = a.dT2 = nullptr;
+    a.skip = nullptr;
     return a;
 }
 
@@ -436,9 +438,10 @@ int pssfp_tile_voxels(PssfpLaunch L) {
 }
 
 void launch_pssfp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
-                  const pSSFPSequence& seq, cfloat* echo, int64_t echo_stride, PssfpLaunch L) {
+                  const pSSFPSequence& seq, cfloat* echo, int64_t echo_stride, PssfpLaunch L, const int* skip) {
     const int nz = int(seq.z.size());
-    const kernels::PssfpArgs a = pssfp_args(ctx, params, voxel_begin, nvoxels, seq, echo, echo_stride);
+    kernels::PssfpArgs a = pssfp_args(ctx, params, voxel_begin, nvoxels, seq, echo, echo_stride);
+    a.skip = skip;
     if (nvoxels <= 0) return;
     if (L.config < 0) L = pssfp_default_launch(nz, nvoxels);
     const auto& cfg = checked_config(L, nz);

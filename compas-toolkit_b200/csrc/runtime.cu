@@ -2,7 +2,7 @@
 // stream-ordered allocations from the device memory pool, blocking transfers, and a
 // per-device status word that kernels use to report errors instead of trapping.
 //
-// Replaces the reference's kmm runtime for this path (compas/core/context.h:158-264):
+// Replaces the reference's kmm runtime for this path (compas/core/context.h:19-125):
 // no chunking across devices, no task graph — operations are issued in order on the
 // device's stream, so every result is ready for any later operation on that stream.
 #include <atomic>
@@ -140,9 +140,13 @@ void CompasContext::synchronize() const {
     check_device_status();
 }
 
+unsigned int* CompasContext::status_word() const {
+    return m_status ? m_status : detail::device_status_word(m_device);
+}
+
 void CompasContext::check_device_status() const {
     DeviceGuard guard(m_device);
-    unsigned int* word = detail::device_status_word(m_device);
+    unsigned int* word = status_word();
     unsigned int value = 0;
     COMPAS_CUDA_CHECK(cudaMemcpyAsync(&value, word, sizeof(value), cudaMemcpyDeviceToHost, m_stream));
     COMPAS_CUDA_CHECK(cudaStreamSynchronize(m_stream));

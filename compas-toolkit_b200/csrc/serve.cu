@@ -97,6 +97,7 @@ struct ServeEngine::Impl {
     };
     struct Slot {
         cudaStream_t stream = nullptr;
+        unsigned int* status = nullptr;  // this slot's device status word: its kernels' errors only
         std::unique_ptr<Running> running;
     };
 
@@ -136,6 +137,7 @@ struct ServeEngine::Impl {
                 cudaStreamSynchronize(s.stream);
                 cudaStreamDestroy(s.stream);
             }
+            if (s.status) cudaFree(s.status);
         }
     }
 
@@ -187,7 +189,7 @@ void ServeEngine::Impl::evict_for(size_t need) {
 
 void ServeEngine::Impl::launch(Slot& slot, std::vector<uint64_t> ids) {
     const int dev = ctx.device();
-    const CompasContext sctx(dev, slot.stream);
+    const CompasContext sctx(dev, slot.stream, slot.status);
     auto run = std::make_unique<Running>();
     run->ids = ids;
     run->id = batches++;
@@ -261,6 +263,11 @@ void ServeEngine::Impl::launch(Slot& slot, std::vector<uint64_t> ids) {
         run->batch = std::make_unique<SimulationBatch>(sctx, jobs, opt.method);
         run->batch->run();
     }
+    for (const auto& t : ts)
+        if (t->request.inject_wait_timeout) {
+            launch_wait_probe(sctx, 2000000);  // ~1 ms, then STATUS_WAIT_TIMEOUT in this slot's word
+            break;
+        }
 
     // per request: derivative differences, signal of resident echoes, residual, gradient
     run->objectives = Array<float>({int64_t(std::max<size_t>(n, 1))}, dev, slot.stream);
@@ -329,10 +336,11 @@ void ServeEngine::Impl::finalize(Slot& slot, bool ok, const std::string& error) 
     Running& run = *slot.running;
     const auto now = Clock::now();
     std::vector<float> obj(run.ids.size(), 0.0f);
+    std::string message = error;
     if (ok && !run.ids.empty()) {
         // the batch is complete and nothing follows it on the slot stream: these copies return at once
         unsigned int status = 0;
-        unsigned int* word = detail::device_status_word(ctx.device());
+        unsigned int* word = slot.status;  // errors of this batch's kernels, and of no other batch
         cudaError_t e = cudaMemcpyAsync(obj.data(), run.objectives.data(), obj.size() * sizeof(float),
                                         cudaMemcpyDeviceToHost, slot.stream);
         if (e == cudaSuccess)
@@ -343,6 +351,7 @@ void ServeEngine::Impl::finalize(Slot& slot, bool ok, const std::string& error) 
             (void)cudaGetLastError();
         } else if (status != 0) {
             ok = false;
+            message = std::string("a kernel of the request's batch reported an error: ") + status_message(status);
             cudaMemsetAsync(word, 0, sizeof(unsigned int), slot.stream);
         }
     }
@@ -353,7 +362,7 @@ void ServeEngine::Impl::finalize(Slot& slot, bool ok, const std::string& error) 
         used -= t.footprint;
         if (!ok) {
             t.failed = true;
-            t.error = error.empty() ? "a kernel of the request's batch reported an error" : error;
+            t.error = message.empty() ? "a kernel of the request's batch reported an error" : message;
             st.failed++;
             continue;
         }
@@ -499,7 +508,11 @@ ServeEngine::ServeEngine(const CompasContext& ctx, ServeOptions options) :
         COMPAS_ERROR("serving needs at least one batch slot and one request per batch");
     DeviceGuard guard(ctx.device());
     im.slots.resize(size_t(options.max_inflight_batches));
-    for (auto& s : im.slots) COMPAS_CUDA_CHECK(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+    for (auto& s : im.slots) {
+        COMPAS_CUDA_CHECK(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+        COMPAS_CUDA_CHECK(cudaMalloc(&s.status, sizeof(unsigned int)));
+        COMPAS_CUDA_CHECK(cudaMemset(s.status, 0, sizeof(unsigned int)));
+    }
     im.worker = std::thread([&im] { im.loop(); });
 }
 

@@ -1,7 +1,7 @@
 // signal.cu — magnetization_to_signal (Cartesian, spiral) and J·v, plain FP32 path.
 //
 // Cartesian signal (reference: src/trajectories/signal_kernels.cuh:137-167,
-// compas/trajectories/cartesian_view.cuh:273-308) and J·v (src/jacobian/product_kernels.cuh:
+// compas/trajectories/cartesian_view.cuh:28-63) and J·v (src/jacobian/product_kernels.cuh:
 // 7-67) are both contractions over voxels of a streamed operand A[r][v] with a generated
 // operand B[(c,k)][v] = coil[c][v]·E_k(v):
 //   E_k(v) = exp((k - S/2)·(-Δt/T2 + iΘ_v)),  Θ_v = Δk_re·x + Δk_im·y + 2πΔt·B0.
@@ -226,7 +226,7 @@ __device__ __forceinline__ void spiral_tile(const SpiralArgs& a, const int bx, c
                 const float x = a.params[6 * a.pstride + v], y = a.params[7 * a.pstride + v];
                 const float2 rho = make_float2(a.params[4 * a.pstride + v], a.params[5 * a.pstride + v]);
                 const float R2 = 1.0f / T2;
-                // rewind by (S/2)Δt and prephase with Re k0·x   (spiral_view.cuh:352-398)
+                // rewind by (S/2)Δt and prephase with Re k0·x   (spiral_view.cuh:13-59)
                 const double half = 0.5 * double(a.S) * double(a.dt);
                 const float2 rw = cis_rad(-half * twopi * double(B0) + double(ks.x) * double(x));
                 const float mag = expf(float(half) * R2);

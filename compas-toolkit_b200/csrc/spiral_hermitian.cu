@@ -2,7 +2,7 @@
 //
 // The reference's Jᴴ·v accepts only Cartesian trajectories (compas/jacobian/hermitian.h:30,
 // src/jacobian/hermitian_kernels.cuh:30-92). On a spiral, readout r of voxel v carries its own
-// factor F_rvk = readout_rv · z_rv^k (the spiral signal model: spiral_view.cuh:352-412), with
+// factor F_rvk = readout_rv · z_rv^k (the spiral signal model: spiral_view.cuh:13-73), with
 // dF/dT2 = (k - S/2)·Δt·R2²·F like the Cartesian dE/dT2. With U_rv(k) = Σ_c conj(C_cv)·u[c][r][k]:
 //
 //   Y_rv  = Σ_k conj(F_rvk)·U_rv(k),   Ỹ_rv = Σ_k (k - S/2)·conj(F_rvk)·U_rv(k)

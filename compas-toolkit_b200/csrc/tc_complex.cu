@@ -616,7 +616,7 @@ bool run_tc(const CompasContext& ctx, kernels::TcArgs a, bool jac, cfloat* out) 
     Array<unsigned char> scratch({tables.bytes}, ctx.device(), ctx.stream());
     tc_assign_tables(a, tables, scratch.data());
     a.out = reinterpret_cast<float2*>(splits > 1 ? partials.data() : out);
-    a.status = detail::device_status_word(ctx.device());
+    a.status = ctx.status_word();
     // per-voxel tables, then A packed once (one pass over the echoes instead of one per pair tile)
     const dim3 pgrid(div_ceil(a.apack_stages * 8, 256), plan.mtiles * plan.nr);
     if (jac) {

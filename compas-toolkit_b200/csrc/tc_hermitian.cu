@@ -459,7 +459,7 @@ bool launch_jacobian_hermitian_tc(const CompasContext& ctx, const float* params,
     a.dt = g.dt;
     a.dk_re = g.dk_re;
     a.dk_im = g.dk_im;
-    a.status = detail::device_status_word(ctx.device());
+    a.status = ctx.status_word();
     const int vtiles = 2 * div_ceil(nvoxels, 2 * kernels::TH_M);  // whole CTA pairs
     const int ptiles = div_ceil(ncoils * g.nreadouts, kernels::TH_PAIRS);
     const int kstages = div_ceil(g.ns, 32);

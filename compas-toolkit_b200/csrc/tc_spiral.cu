@@ -1,6 +1,6 @@
 // tc_spiral.cu — split-BF16 tcgen05 kernels for the spiral signal and the spiral J·v.
 //
-// Spiral signal (reference: src/trajectories/signal_kernels.cuh:274-345, spiral_view.cuh:352-412):
+// Spiral signal (reference: src/trajectories/signal_kernels.cuh:274-345, spiral_view.cuh:13-73):
 //   s[c][r][k] = Σ_v C[c][v]·A_rv·z_rv^k,  A_rv = ρ_v·m[r][v]·rewind_rv,  z_rv = e^{-Δt R2 + iΘ_rv}.
 // Writing the sample as k = 128·t + j gives z^k = z^{128t}·z^j, so for one readout
 //   s[c][r][128t + j] = Σ_v P[j][v]·W[v][(t, c)],   P[j][v] = z_rv^j,   W[v][(t, c)] = z_rv^{128t}·A_rv·C[c][v]
@@ -93,7 +93,7 @@ __global__ void tc_spiral_base_kernel(TsArgs a, float2* __restrict__ base) {
     const float R2 = 1.0f / T2;
     const float dec = -a.dt * R2;
     const double turns = (double(dkr.x) * x + double(dkr.y) * y + double(a.dt) * twopi * B0) * inv_2pi;
-    // rewind by (S/2)Δt and prephase with Re k0·x   (spiral_view.cuh:352-398)
+    // rewind by (S/2)Δt and prephase with Re k0·x   (spiral_view.cuh:13-59)
     const float2 rw = cis_rad(-hdt * twopi * double(B0) + double(ks.x) * double(x));
     const float2 rd = cscale(expf(float(hdt) * R2), rw);
     float2 s0, s1 = make_float2(0.f, 0.f);
@@ -358,7 +358,7 @@ bool launch_tc_spiral(const CompasContext& ctx, kernels::TsArgs a, bool jac) {
         COMPAS_CUDA_CHECK(cudaMemsetAsync(a.out, 0, sizeof(float2) * size_t(a.C) * a.R * a.S, ctx.stream()));
         return true;
     }
-    a.status = detail::device_status_word(ctx.device());
+    a.status = ctx.status_word();
     a.T = T;
     // coils per CTA: as many as fit 2·T·CT ≤ 256 real columns, spread evenly over the coil groups
     const int ct_max = std::max(1, kernels::TS_NMAX / (2 * T));

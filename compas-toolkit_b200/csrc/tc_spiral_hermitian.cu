@@ -1,6 +1,6 @@
 // tc_spiral_hermitian.cu — Jᴴ·u on a spiral trajectory on tcgen05 tensor cores, split-BF16.
 //
-// Jᴴu (the FP32 form is spiral_hermitian.cu; signal model: spiral_view.cuh:352-412) needs, per
+// Jᴴu (the FP32 form is spiral_hermitian.cu; signal model: spiral_view.cuh:13-73) needs, per
 // readout r and voxel v,
 //   Y_rv = Σ_k conj(F_rvk)·U_rv(k),  Ỹ_rv = Σ_k (k - S/2)·conj(F_rvk)·U_rv(k),
 //   F_rvk = rd_rv·z_rv^k,  U_rv(k) = Σ_c conj(C_cv)·u[c][r][k].
@@ -84,7 +84,7 @@ __global__ void tc_spiral_hermitian_prep_kernel(TxArgs a, float2* __restrict__ c
     const float x = a.params[6 * a.pstride + v], y = a.params[7 * a.pstride + v];
     const float R2 = 1.0f / T2;
     const float dec = -a.dt * R2;
-    // readout factor: rewind by (S/2)Δt, prephase with Re k0·x   (spiral_view.cuh:352-398)
+    // readout factor: rewind by (S/2)Δt, prephase with Re k0·x   (spiral_view.cuh:13-59)
     const float2 rd = cscale(expf(float(half) * R2), cis_rad(-half * twopi * double(B0) + double(ks.x) * double(x)));
     const double turns = (double(dkr.x) * x + double(dkr.y) * y + double(a.dt) * twopi * B0) * inv_2pi;
     for (int t = 0; t < a.T; t++) {
@@ -416,7 +416,7 @@ bool launch_jacobian_hermitian_spiral_tc(const CompasContext& ctx, const float* 
     a.k_start = reinterpret_cast<const float2*>(k_start);
     a.delta_k = reinterpret_cast<const float2*>(delta_k);
     a.T = T;
-    a.status = detail::device_status_word(ctx.device());
+    a.status = ctx.status_word();
     const int groups = div_ceil(ncoils, kernels::TX_CTMAX);
     a.CT = div_ceil(ncoils, groups);
     const int vtiles = div_ceil(nvoxels, kernels::TX_M);

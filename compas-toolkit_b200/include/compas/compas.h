@@ -19,6 +19,8 @@
 #include <variant>
 #include <vector>
 
+#include "compas/vector.h"
+
 namespace compas {
 
 using index_t = int;
@@ -60,7 +62,7 @@ class CompasException: public std::runtime_error {
     } while (0)
 
 // ------------------------------------------------------------------------------------------
-// objects and arrays   (compas/core/object.h; kmm::Array used via compas/core/context.h:155-156)
+// objects and arrays   (compas/core/object.h; kmm::Array used via compas/core/context.h:16-17)
 // ------------------------------------------------------------------------------------------
 class Object {
   public:
@@ -175,7 +177,7 @@ class Array: public ArrayBase {
 };
 
 // ------------------------------------------------------------------------------------------
-// context   (compas/core/context.h:158-264)
+// context   (compas/core/context.h:19-125)
 // ------------------------------------------------------------------------------------------
 class CompasContext {
   public:
@@ -183,9 +185,17 @@ class CompasContext {
     // a view of the device's context that issues work, and allocates, on `stream` (which the
     // caller keeps alive while work or arrays made through this view exist)
     CompasContext(int device, cudaStream_t stream) : m_device(device), m_stream(stream) {}
+    // the same with its own device status word (a device `unsigned int` the caller allocates,
+    // zeroes and keeps alive): kernels launched through this view record their errors there, and
+    // check_device_status() reads and clears only that word. Concurrent users of one device (the
+    // serving engine's slots) keep each other's errors apart this way.
+    CompasContext(int device, cudaStream_t stream, unsigned int* status_word) :
+        m_device(device), m_stream(stream), m_status(status_word) {}
     CompasContext with_device(int index) const;
     int device() const { return m_device; }
     cudaStream_t stream() const { return m_stream; }
+    // the device word this view's kernels report errors in (its own, else the device's)
+    unsigned int* status_word() const;
 
     template<typename T, size_t N>
     Array<std::decay_t<T>, N> allocate(View<T, N> content) const {
@@ -211,6 +221,7 @@ class CompasContext {
     void upload(void* dst, const void* src, size_t bytes) const;
     int m_device;
     cudaStream_t m_stream;
+    unsigned int* m_status = nullptr;
 };
 
 inline CompasContext make_context(int device = 0) {
@@ -218,7 +229,7 @@ inline CompasContext make_context(int device = 0) {
 }
 
 // ------------------------------------------------------------------------------------------
-// tissue parameters   (compas/parameters/tissue.h:16-67, tissue_view.cuh:88-101)
+// tissue parameters   (compas/parameters/tissue.h:16-67, tissue_view.cuh:42-72)
 // ------------------------------------------------------------------------------------------
 namespace TissueParameterField {
 enum { T1 = 0, T2 = 1, B1 = 2, B0 = 3, RHO_X = 4, RHO_Y = 5, X = 6, Y = 7, Z = 8, NUM_FIELDS = 9 };
@@ -258,7 +269,7 @@ TissueParameters make_tissue_parameters(
     View<float> z = {});
 
 // ------------------------------------------------------------------------------------------
-// sequences   (compas/sequences/fisp.h:10-60, pssfp.h:9-72, pssfp_view.h:7-11)
+// sequences   (compas/sequences/fisp.h:10-60, sequences/pssfp.h:9-72, pssfp_view.h:7-11)
 // ------------------------------------------------------------------------------------------
 struct FISPSequence: public Object {
     Array<cfloat> RF_train;             // [nTR] flip angle (deg) and phase
@@ -531,6 +542,10 @@ struct ServeRequest {
     Array<cfloat, 2> coil_sensitivities;  // [ncoils][nvoxels]
     Array<cfloat, 3> data;                // measured signal [ncoils][nreadouts][ns]
     uint64_t echo_key = 0;
+    // failure-path test hook: the batch holding this request also runs a kernel whose bounded wait
+    // on a barrier that nothing completes gives up, so that batch (and only it) reports
+    // STATUS_WAIT_TIMEOUT and its requests fail
+    bool inject_wait_timeout = false;
 };
 
 struct ServeResult {
@@ -613,8 +628,13 @@ class GaussNewtonStep: public Object {
     const Array<cfloat, 3>& signal() const;           // s(p)
     const Array<cfloat, 2>& gradient() const;         // Jᴴ·b of the last CG iteration [4][V]
     const Array<float, 2>& step() const;              // δ [4][V]
-    // device scalars: [0] ‖y - s(p)‖² before the update, [1] γ, [2] γ', [3] ‖q‖², [4] α, [5] β
+    // device scalars: [0] ‖y - s(p)‖² before the update, [1] γ, [2] γ', [3] ‖q‖², [4] α, [5] β,
+    // [6] objective of the last line-search trial, [7] step length taken (1, ½ or 0)
     const Array<float>& scalars() const;
+    // line search on the objective before the update (on by default): the first of the steps
+    // t = 1, ½ that does not raise ‖y - s(p)‖² is taken, else none. Changing it drops the graph.
+    void set_line_search(bool on);
+    bool line_search() const;
     int kernels_per_iteration() const;  // kernel nodes of the captured graph (-1 before capture)
     const char* name() const override { return "compas::GaussNewtonStep"; }
 
@@ -623,5 +643,53 @@ class GaussNewtonStep: public Object {
   private:
     std::shared_ptr<Impl> m_impl;
 };
+
+// ------------------------------------------------------------------------------------------
+// one slice sharded over processes, one GPU each (no counterpart in the reference's API: its kmm
+// runtime chunks voxels over the devices of one process, include/compas/core/context.h:51-68,
+// and sums the chunks' signals, src/trajectories/signal.cu:289-300)
+// ------------------------------------------------------------------------------------------
+struct VoxelRange {
+    int64_t begin = 0, end = 0;
+    int64_t size() const { return end - begin; }
+};
+// voxels [begin, end) of `rank` among `world` ranks: contiguous, sizes differ by at most one
+VoxelRange voxel_shard(int64_t nvoxels, int rank, int world);
+
+// An NCCL communicator over `world` processes, one GPU each (the context's device). Every rank
+// passes the same 128-byte unique id, made once by one rank with unique_id() and sent to the
+// others by the caller; construction blocks until all ranks have joined. NCCL (libnccl.so.2) is
+// loaded on first use.
+class Communicator: public Object {
+  public:
+    static std::vector<char> unique_id();
+    Communicator(const CompasContext& ctx, int rank, int world, const std::vector<char>& unique_id);
+    int rank() const;
+    int world() const;
+    // in-place sum of `count` floats over the ranks, stream-ordered on ctx's stream
+    void allreduce_sum(const CompasContext& ctx, float* data, int64_t count) const;
+    const char* name() const override { return "compas::Communicator"; }
+
+  private:
+    struct Impl;
+    std::shared_ptr<Impl> m_impl;
+};
+
+// The signal / J·v of a slice whose voxels are sharded over the communicator's ranks: every rank
+// passes its own voxels (echoes [R][V_rank], their parameters and coil sensitivities, for J·v their
+// derivative echoes and the [4][V_rank] direction) and receives the full [C][R][S] result, the sum
+// of the ranks' partials. Jᴴ·v needs no such variant: each rank computes its voxels' gradient from
+// the full residual with compute_jacobian_hermitian.
+Array<cfloat, 3> magnetization_to_signal_sharded(const CompasContext& ctx, const Communicator& comm,
+                                                 const Array<cfloat, 2>& echos, const TissueParameters& parameters,
+                                                 const Trajectory& trajectory, const Array<cfloat, 2>& coils,
+                                                 SimulateSignalMethod method = SimulateSignalMethod::MatmulFast);
+template<typename Traj>
+Array<cfloat, 3> compute_jacobian_sharded(const CompasContext& ctx, const Communicator& comm,
+                                          const Array<cfloat, 2>& echos, const Array<cfloat, 2>& dT1,
+                                          const Array<cfloat, 2>& dT2, const TissueParameters& parameters,
+                                          const Traj& trajectory, const Array<cfloat, 2>& coils,
+                                          const Array<cfloat, 2>& vector,
+                                          JacobianComputeMethod method = JacobianComputeMethod::GemmFast);
 
 }  // namespace compas

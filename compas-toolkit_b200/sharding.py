@@ -9,9 +9,12 @@ sum over voxels (signal, J·v). So a slice is split into contiguous voxel ranges
   produces its own voxels of [4][V]; `gather_voxels` assembles the full vector when needed.
 
 This mirrors the reference's chunking of voxels across devices with a summing reduction of the
-signal (src/trajectories/signal.cu:289-300, compas/core/context.h:51-68). The functions below
-take the per-rank compute as callables, so the partition and reduction logic is the same whether
-the ranks run the GPU library (NCCL) or a CPU restatement (gloo).
+signal (src/trajectories/signal.cu:289-300, compas/core/context.h:51-68). The partition is the
+library's (compas_b200_voxel_shard, host code); on GPUs the library's own NCCL communicator sums
+the partials (compas_b200_magnetization_to_signal_sharded / _compute_jacobian_sharded, see
+`library_communicator`). The functions below also take the per-rank compute as callables with
+torch.distributed for the sum, so the same partition and reduction run on CPU ranks (gloo) with a
+CPU restatement as the compute.
 """
 from __future__ import annotations
 
@@ -30,13 +33,11 @@ class VoxelShard:
 
     @property
     def begin(self) -> int:
-        q, r = divmod(self.nvoxels, self.world)
-        return self.rank * q + min(self.rank, r)
+        return _library_range(self.nvoxels, self.rank, self.world)[0]
 
     @property
     def end(self) -> int:
-        q, r = divmod(self.nvoxels, self.world)
-        return self.begin + q + (1 if self.rank < r else 0)
+        return _library_range(self.nvoxels, self.rank, self.world)[1]
 
     @property
     def size(self) -> int:
@@ -49,6 +50,28 @@ class VoxelShard:
 
     def counts(self) -> list:
         return [VoxelShard(self.nvoxels, r, self.world).size for r in range(self.world)]
+
+
+def _library_range(nvoxels: int, rank: int, world: int) -> tuple:
+    import compas_b200
+
+    return compas_b200.voxel_shard(nvoxels, rank, world)
+
+
+def library_communicator(cb, ctx, rank: int, world: int, group=None):
+    """The library's NCCL communicator for this rank: rank 0 makes the unique id and
+    torch.distributed broadcasts it (any backend), then every rank joins."""
+    import torch
+    import torch.distributed as dist
+
+    uid = torch.zeros(128, dtype=torch.uint8)
+    if rank == 0:
+        uid = torch.frombuffer(bytearray(cb.comm_unique_id()), dtype=torch.uint8).clone()
+    if world > 1:
+        if dist.get_backend(group) == "nccl":
+            uid = uid.cuda()
+        dist.broadcast(uid, src=0, group=group)
+    return cb.Communicator(ctx, rank, world, bytes(uid.cpu().numpy().tobytes()))
 
 
 def allreduce_sum(tensor, group=None):

@@ -177,6 +177,13 @@ COMPAS_API int64_t compas_b200_array_extent(const compas_array* array, int axis)
 COMPAS_API int compas_b200_compute_residual_noalloc(int device, const compas_cfloat* lhs, const compas_cfloat* rhs,
                                                     compas_cfloat* diff, float* objective, int64_t n, void* stream);
 
+/* Failure-channel self-test: enqueue on the context's stream a one-thread kernel whose bounded wait
+ * on a barrier that nothing completes gives up after `limit_cycles` SM cycles and records
+ * STATUS_WAIT_TIMEOUT; the next compas_synchronize / read of the context then reports "a bounded
+ * device-side wait gave up" through compas_last_error() (the device status word is cleared by
+ * that report). Returns 0, or -1 on a launch error. */
+COMPAS_API int compas_b200_wait_probe(const compas_context* ctx, int64_t limit_cycles);
+
 /* Number of kernels this library has launched in this process (all devices). */
 COMPAS_API uint64_t compas_b200_launch_count(void);
 
@@ -186,6 +193,9 @@ COMPAS_API void compas_b200_set_fisp_launch(int config, int warps);
 COMPAS_API void compas_b200_set_pssfp_launch(int config);
 COMPAS_API int compas_b200_fisp_config_count(void);
 COMPAS_API int compas_b200_fisp_config_info(int index, int* states_per_lane, int* lanes);
+/* 1 when FISP layout `index` is a packed one-lane layout (two states per two-wide FP32
+ * instruction, states_per_lane = 2 x pairs), else 0. */
+COMPAS_API int compas_b200_fisp_config_packed(int index);
 COMPAS_API int compas_b200_pssfp_config_count(void);
 COMPAS_API int compas_b200_pssfp_config_info(int index, int* iso_per_lane, int* lanes);
 /* Layouts of the FISP tangent kernel (compas_b200_simulate_magnetization_tangents); the
@@ -231,7 +241,9 @@ COMPAS_API compas_array* compas_b200_batch_signal(const compas_object* batch, in
 /* One Gauss-Newton iteration of parameter fitting on the device (no counterpart in the
  * reference): simulate, dm/dT1 and dm/dT2 (forward differences with step `delta`, or, for
  * delta = 0, exact forward-mode tangents in the simulation pass), signal, residual against `data`
- * ([ncoils][nreadouts][ns] complex), `cg_iterations` CGLS steps of J.v / J^H.v, parameter update.
+ * ([ncoils][nreadouts][ns] complex), `cg_iterations` CGLS steps of J.v / J^H.v, then a line search
+ * on the objective |y - s(p)|^2 (src/utils/residual.cu:8-46): the first of the steps t = 1, 1/2
+ * that does not raise it is taken, else none, so the objective never rises between iterations.
  * Captured as a CUDA graph on the first graph run. `method` is a JacobianComputeMethod value.
  * The estimate starts as a copy of `parameters`. Released with compas_destroy_object. */
 COMPAS_API compas_object* compas_b200_make_gauss_newton(const compas_context* ctx, const compas_object* parameters,
@@ -244,17 +256,60 @@ COMPAS_API int compas_b200_gauss_newton_run(const compas_object* gn, int use_gra
 /* New array handle sharing the iteration's device storage: 0 parameters [9][nvoxels] float,
  * 1 echoes, 2 dm/dT1, 3 dm/dT2 ([nreadouts][nvoxels] complex), 4 signal [ncoils][nreadouts][ns],
  * 5 J^H.b [4][nvoxels] complex, 6 step [4][nvoxels] float, 7 scalars [8] float
- * (objective before the update, gamma, gamma', |q|^2, alpha, beta). */
+ * (objective before the update, gamma, gamma', |q|^2, alpha, beta, objective of the last
+ * line-search trial, step length taken: 1, 0.5 or 0). */
 COMPAS_API compas_array* compas_b200_gauss_newton_array(const compas_object* gn, int which);
+/* Line search on (1, the default) or off (0: the full CGLS step is always applied). Changing it
+ * drops the captured graph. 0 on success, -1 on error. */
+COMPAS_API int compas_b200_gauss_newton_set_line_search(const compas_object* gn, int on);
 /* Kernel nodes of the captured graph, -1 before the first graph run. */
 COMPAS_API int compas_b200_gauss_newton_graph_kernels(const compas_object* gn);
+
+/* One slice sharded over processes, one GPU each (no counterpart in the reference's C ABI; its
+ * kmm runtime chunks voxels over the devices of one process, include/compas/core/context.h:51-68,
+ * and sums the chunks' signals, src/trajectories/signal.cu:289-300).
+ * compas_b200_voxel_shard: voxels [begin, end) of `rank` among `world` ranks, contiguous, sizes
+ * differing by at most one (host-only; needs no device). 0, or -1 on invalid arguments. */
+COMPAS_API int compas_b200_voxel_shard(int64_t nvoxels, int rank, int world, int64_t* begin, int64_t* end);
+/* A new NCCL unique id (128 bytes) into `out` (nbytes >= 128): one rank makes it and the caller
+ * sends it to the others. Returns the bytes written, or -1. */
+COMPAS_API int compas_b200_comm_unique_id(char* out, int nbytes);
+/* NCCL communicator over `world` processes on the context's device; every rank passes the same
+ * unique id and the call blocks until all have joined. NCCL (libnccl.so.2) is loaded at run time.
+ * Released with compas_destroy_object. */
+COMPAS_API compas_object* compas_b200_make_communicator(const compas_context* ctx, int rank, int world,
+                                                        const char* unique_id);
+/* In-place sum over the ranks of a float or complex array, ordered on the context's stream.
+ * 0, or -1 on error. */
+COMPAS_API int compas_b200_allreduce_sum(const compas_context* ctx, const compas_object* comm, compas_array* array);
+/* Signal / J.v of a slice whose voxels are sharded over the communicator's ranks: each rank passes
+ * its own voxels (echoes [nreadouts][nvoxels_rank], parameters, coils [ncoils][nvoxels_rank], for
+ * J.v also the derivative echoes and the direction [4][nvoxels_rank]) and every rank receives the
+ * full [ncoils][nreadouts][ns] sum. `method` as in compas_b200_magnetization_to_signal /
+ * compas_b200_compute_jacobian. J^H.v needs no such variant: each rank computes its own voxels'
+ * gradient from the full residual with compas_b200_compute_jacobian_hermitian. */
+COMPAS_API compas_array* compas_b200_magnetization_to_signal_sharded(const compas_context* ctx,
+                                                                     const compas_object* comm,
+                                                                     const compas_array* echos,
+                                                                     const compas_object* parameters,
+                                                                     const compas_object* trajectory,
+                                                                     const compas_array* coils, int method);
+COMPAS_API compas_array* compas_b200_compute_jacobian_sharded(const compas_context* ctx, const compas_object* comm,
+                                                              const compas_array* echos,
+                                                              const compas_array* delta_echos_T1,
+                                                              const compas_array* delta_echos_T2,
+                                                              const compas_object* parameters,
+                                                              const compas_object* trajectory,
+                                                              const compas_array* coils, const compas_array* vector,
+                                                              int method);
 
 /* Continuous-batching serving engine (no counterpart in the reference). Requests (parameters,
  * FISP or pSSFP sequence, Cartesian or spiral trajectory, coils [ncoils][nvoxels], measured data
  * [ncoils][nreadouts][ns]) are admitted by estimated device footprint against
  * `memory_budget_gb`, grouped into batches (at most `max_batch_requests` each, at most
- * `max_inflight_batches` on the device at once) and give residual, objective and (Cartesian)
- * gradient J^H.r. A nonzero echo_key lets requests with equal parameters and sequence share
+ * `max_inflight_batches` on the device at once) and give residual, objective and gradient J^H.r.
+ * Each batch slot reports kernel errors in a status word of its own, so a failing batch fails only
+ * its own requests. A nonzero echo_key lets requests with equal parameters and sequence share
  * resident echoes (`echo_cache_gb`). `method` is a SimulateSignalMethod value. `delta` is the
  * forward-difference step of the derivatives; 0 takes exact forward-mode tangents from the
  * simulation pass. Released with compas_destroy_object, which finishes queued requests first. */
@@ -266,12 +321,21 @@ COMPAS_API int64_t compas_b200_server_submit(const compas_object* server, const 
                                              const compas_object* sequence, const compas_object* trajectory,
                                              const compas_array* coils, const compas_array* data,
                                              uint64_t echo_key);
+/* compas_b200_server_submit with request flags. COMPAS_B200_REQUEST_INJECT_WAIT_TIMEOUT (a test hook
+ * of the failure path): the batch that runs the request also runs a kernel whose bounded wait
+ * gives up, so that batch's requests fail with "a bounded device-side wait gave up" while other
+ * batches, on other slots, complete. */
+#define COMPAS_B200_REQUEST_INJECT_WAIT_TIMEOUT 1
+COMPAS_API int64_t compas_b200_server_submit_flags(const compas_object* server, const compas_object* parameters,
+                                                   const compas_object* sequence, const compas_object* trajectory,
+                                                   const compas_array* coils, const compas_array* data,
+                                                   uint64_t echo_key, int flags);
 /* Block until the request completed: objective, times[3] = queued, device, latency (ms), batch
  * id; 0 on success, -1 if it failed (message in compas_last_error). */
 COMPAS_API int compas_b200_server_wait(const compas_object* server, int64_t ticket, float* objective,
                                        double* times, int* batch);
-/* Result arrays of a completed request: 0 residual [ncoils][nreadouts][ns], 1 gradient [4][nvoxels]
- * (empty for spiral trajectories). New handles, valid after release. */
+/* Result arrays of a completed request: 0 residual [ncoils][nreadouts][ns], 1 gradient J^H.r
+ * [4][nvoxels] (Cartesian and spiral trajectories). New handles, valid after release. */
 COMPAS_API compas_array* compas_b200_server_result(const compas_object* server, int64_t ticket, int which);
 COMPAS_API int compas_b200_server_release(const compas_object* server, int64_t ticket);
 COMPAS_API int compas_b200_server_drain(const compas_object* server);

@@ -70,7 +70,7 @@ template<typename T> inline cx<T> cpow(cx<T> a, T b) {
 template<typename T> inline T two_pi() { return T(2.0 * M_PI); }
 
 // Tissue parameters: SoA float[9][nv] in the device order T1,T2,B1,B0,rho_x,rho_y,x,y,z
-// (compas/parameters/tissue_view.cuh:88-101).
+// (compas/parameters/tissue_view.cuh:53-71).
 enum { F_T1 = 0, F_T2, F_B1, F_B0, F_RHOX, F_RHOY, F_X, F_Y, F_Z, F_NUM };
 
 template<typename T>
@@ -95,7 +95,7 @@ inline Voxel<T> load_voxel(const float* params, int64_t nv, int64_t v) {
 
 // --------------------------------------------------------------------------------------------
 // FISP / EPG   (src/operators/epg.cuh:13-322, src/simulate/fisp_kernels.cuh:99-223,
-//               src/simulate/fisp.cu:269-305,386-399)
+//               src/simulate/fisp.cu:7-43,386-399)
 // --------------------------------------------------------------------------------------------
 
 template<typename T>
@@ -323,7 +323,7 @@ struct Cartesian {
 };
 
 // Cartesian readout factor: rewind to readout start + x-prephaser
-// (compas/trajectories/cartesian_view.cuh:273-289)
+// (compas/trajectories/cartesian_view.cuh:28-44)
 template<typename T>
 cx<T> cart_readout_factor(const Cartesian& t, const Voxel<T>& p) {
     T R2 = T(1) / p.T2;
@@ -334,7 +334,7 @@ cx<T> cart_readout_factor(const Cartesian& t, const Voxel<T>& p) {
     return cexp(res);
 }
 
-// sample phase/decay from readout start   (cartesian_view.cuh:297-308)
+// sample phase/decay from readout start   (cartesian_view.cuh:52-63)
 template<typename T>
 cx<T> cart_sample(const Cartesian& t, const Voxel<T>& p, int k) {
     T R2 = T(1) / p.T2;
@@ -342,7 +342,7 @@ cx<T> cart_sample(const Cartesian& t, const Voxel<T>& p, int k) {
     return cexp(cx<T>{T(k) * (-T(t.dt) * R2), T(k) * Theta});
 }
 
-// echo-centred sample decay and its T2 derivative   (cartesian_view.cuh:310-337)
+// echo-centred sample decay and its T2 derivative   (cartesian_view.cuh:65-92)
 template<typename T>
 void cart_sample_abs(const Cartesian& t, const Voxel<T>& p, int k, cx<T>& E, cx<T>& dE) {
     T R2 = T(1) / p.T2;
@@ -352,7 +352,7 @@ void cart_sample_abs(const Cartesian& t, const Voxel<T>& p, int k, cx<T>& E, cx<
     dE = (s * T(t.dt) * R2 * R2) * E;
 }
 
-// phase_encoding: echo * exp(i y Im k_start[r])   (phase_encoding_kernels.cuh:225-240)
+// phase_encoding: echo * exp(i y Im k_start[r])   (phase_encoding_kernels.cuh:10-25)
 template<typename T>
 cx<T> phase_encode(cx<T> m, const Voxel<T>& p, cx<T> kstart) {
     return m * cexp(cx<T>{T(0), p.y * kstart.im});
@@ -381,7 +381,7 @@ struct Spiral {
     const float* dk;       // complex [nr]
 };
 
-// spiral readout factor: rewind + prephaser with Re k0 · x only   (spiral_view.cuh:352-398)
+// spiral readout factor: rewind + prephaser with Re k0 · x only   (spiral_view.cuh:13-59)
 template<typename T>
 cx<T> spiral_readout(const Spiral& t, const Voxel<T>& p, int r, cx<T> m) {
     T R2 = T(1) / p.T2;
@@ -391,7 +391,7 @@ cx<T> spiral_readout(const Spiral& t, const Voxel<T>& p, int r, cx<T> m) {
     return m * cexp(cx<T>{T(0), k0re * p.x});
 }
 
-// spiral per-sample step z = exp(-Δt R2 + iΘ_r)   (spiral_view.cuh:400-412)
+// spiral per-sample step z = exp(-Δt R2 + iΘ_r)   (spiral_view.cuh:61-73)
 template<typename T>
 cx<T> spiral_step(const Spiral& t, const Voxel<T>& p, int r) {
     T R2 = T(1) / p.T2;
@@ -472,7 +472,7 @@ void jacobian_hermitian_voxel(const float* echo, const float* dT1, const float* 
 // ---- spiral J·v and Jᴴ·v ----------------------------------------------------------------
 // The reference's Jacobians accept only CartesianTrajectory (compas/jacobian/product.h:30,
 // hermitian.h:30). These differentiate the spiral signal model of signal_spiral_entry
-// (spiral_view.cuh:352-412, signal_kernels.cuh:274-345) with the column scaling of the Cartesian
+// (spiral_view.cuh:13-73, signal_kernels.cuh:274-345) with the column scaling of the Cartesian
 // products (product_kernels.cuh:44-63): the per-readout factor F_rvk = readout_rv · z_rv^k depends
 // on T2 through R2 = 1/T2 in the rewind exp((S/2)Δt R2) and in z^k = exp(k(-Δt R2 + iΘ)), so
 // dF/dT2 = (k - S/2)·Δt·R2²·F, the same form as the Cartesian dE/dT2.

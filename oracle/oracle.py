@@ -285,17 +285,18 @@ def ref_kernels():
     return _REF
 
 
-_REF_GPU = None
-_REF_GPU_PATH = _HERE / "_ref" / "libref_gpu.so"
+_REF_GPU = {}
+_REF_GPU_PATH = {False: _HERE / "_ref" / "libref_gpu.so", True: _HERE / "_ref" / "libref_gpu_unchecked.so"}
 
 
-def ref_gpu():
+def ref_gpu(unchecked=False):
     """The reference's FISP and pSSFP kernels built for the B200 with its own CUDA flags
     (oracle/_ref/libref_gpu.so, "reference kernels, re-hosted"), or None where they were not built.
-    Entry points take device pointers (ints) and a cudaStream_t."""
-    global _REF_GPU
-    if _REF_GPU is None and _REF_GPU_PATH.exists():
-        L = C.CDLL(str(_REF_GPU_PATH))
+    Entry points take device pointers (ints) and a cudaStream_t. unchecked: the build without the
+    stand-in views' index checks (libref_gpu_unchecked.so), for timing launches that the checked
+    build has run without a flagged index."""
+    if unchecked not in _REF_GPU and _REF_GPU_PATH[unchecked].exists():
+        L = C.CDLL(str(_REF_GPU_PATH[unchecked]))
         L.ref_gpu_fisp.argtypes = [_P, _I, _P, _P, _I, _I, _F, _F, _F, _F, _I, _I, _I, _P, _P, _P]
         L.ref_gpu_fisp.restype = C.c_int
         L.ref_gpu_pssfp.argtypes = [_P, _I, _P, _I, _F, _P, _I, _P, _P, _P, _I, _P, _P]
@@ -311,8 +312,8 @@ def ref_gpu():
         for name in ("ref_gpu_out_of_bounds", "ref_gpu_products_out_of_bounds", "ref_gpu_hermitian_out_of_bounds"):
             getattr(L, name).argtypes = []
             getattr(L, name).restype = C.c_int
-        _REF_GPU = L
-    return _REF_GPU
+        _REF_GPU[unchecked] = L
+    return _REF_GPU.get(unchecked)
 
 
 def ref_gpu_out_of_bounds() -> int:
@@ -330,7 +331,7 @@ def _dev(a, dtype):
     return torch.as_tensor(np.ascontiguousarray(a), device="cuda").to(dtype).contiguous()
 
 
-def ref_gpu_signal_cartesian(params, echos, traj, coils):
+def ref_gpu_signal_cartesian(params, echos, traj, coils, unchecked=False):
     """Signal [C][R][S] (torch complex64) of the reference's default Cartesian path (MatmulFast: its
     kernels plus TF32 cuBLAS) on torch's current stream."""
     import torch
@@ -339,13 +340,13 @@ def ref_gpu_signal_cartesian(params, echos, traj, coils):
     ks = _dev(traj["k_start"], torch.complex64)
     V, C_, R, S = p.shape[1], c.shape[0], traj["nr"], traj["ns"]
     out = torch.empty((C_, R, S), dtype=torch.complex64, device="cuda")
-    ref_gpu().ref_gpu_signal_cartesian(p.data_ptr(), V, e.data_ptr(), c.data_ptr(), C_, R, S, traj["dt"],
+    ref_gpu(unchecked).ref_gpu_signal_cartesian(p.data_ptr(), V, e.data_ptr(), c.data_ptr(), C_, R, S, traj["dt"],
                                        ks.data_ptr(), float(complex(traj["dk"]).real), out.data_ptr(),
                                        C.c_void_p(torch.cuda.current_stream().cuda_stream))
     return out
 
 
-def ref_gpu_signal_spiral(params, echos, traj, coils):
+def ref_gpu_signal_spiral(params, echos, traj, coils, unchecked=False):
     """Spiral signal [C][R][S] (torch complex64) of the reference's spiral kernels on torch's
     current stream."""
     import torch
@@ -354,12 +355,12 @@ def ref_gpu_signal_spiral(params, echos, traj, coils):
     ks, dk = _dev(traj["k_start"], torch.complex64), _dev(traj["dk"], torch.complex64)
     V, C_, R, S = p.shape[1], c.shape[0], traj["nr"], traj["ns"]
     out = torch.empty((C_, R, S), dtype=torch.complex64, device="cuda")
-    ref_gpu().ref_gpu_signal_spiral(p.data_ptr(), V, e.data_ptr(), c.data_ptr(), C_, R, S, traj["dt"], ks.data_ptr(),
+    ref_gpu(unchecked).ref_gpu_signal_spiral(p.data_ptr(), V, e.data_ptr(), c.data_ptr(), C_, R, S, traj["dt"], ks.data_ptr(),
                                     dk.data_ptr(), out.data_ptr(), C.c_void_p(torch.cuda.current_stream().cuda_stream))
     return out
 
 
-def ref_gpu_jacobian(params, echos, dT1, dT2, traj, coils, vector, hermitian=False):
+def ref_gpu_jacobian(params, echos, dT1, dT2, traj, coils, vector, hermitian=False, unchecked=False):
     """J·v [C][R][S] (vector [4][V]) or, with hermitian, Jᴴ·v [4][V] (vector [C][R][S]) of the
     reference's default GemmFast paths (its kernels plus TF32 cuBLAS), torch complex64."""
     import torch
@@ -371,19 +372,19 @@ def ref_gpu_jacobian(params, echos, dT1, dT2, traj, coils, vector, hermitian=Fal
     V, C_, R, S = p.shape[1], c.shape[0], traj["nr"], traj["ns"]
     shape = (4, V) if hermitian else (C_, R, S)
     out = torch.empty(shape, dtype=torch.complex64, device="cuda")
-    fn = ref_gpu().ref_gpu_jacobian_hermitian if hermitian else ref_gpu().ref_gpu_jacobian
+    fn = ref_gpu(unchecked).ref_gpu_jacobian_hermitian if hermitian else ref_gpu(unchecked).ref_gpu_jacobian
     fn(p.data_ptr(), V, e.data_ptr(), d1.data_ptr(), d2.data_ptr(), c.data_ptr(), C_, R, S, traj["dt"], ks.data_ptr(),
        float(complex(traj["dk"]).real), v.data_ptr(), out.data_ptr(), C.c_void_p(torch.cuda.current_stream().cuda_stream))
     return out
 
 
-def ref_gpu_fisp(params, seq):
+def ref_gpu_fisp(params, seq, unchecked=False):
     """FISP echoes [nTR*uf][nv] (torch complex64) from the re-hosted reference kernels, launched on
     torch's current CUDA stream (the inputs' temporaries are freed in that stream's order);
     `params` [9][nv] float32, `seq` a workloads-style dict."""
     import torch
 
-    L = ref_gpu()
+    L = ref_gpu(unchecked)
     dev = torch.device("cuda")
     p = torch.as_tensor(_ff(params), device=dev)
     nv = p.shape[1]
@@ -401,12 +402,12 @@ def ref_gpu_fisp(params, seq):
     return out
 
 
-def ref_gpu_pssfp(params, seq):
+def ref_gpu_pssfp(params, seq, unchecked=False):
     """pSSFP echoes [nTR][nv] (torch complex64) from the re-hosted reference kernels, on torch's
     current CUDA stream."""
     import torch
 
-    L = ref_gpu()
+    L = ref_gpu(unchecked)
     dev = torch.device("cuda")
     p = torch.as_tensor(_ff(params), device=dev)
     nv = p.shape[1]

@@ -212,7 +212,7 @@ int oracle_spiral_jacobian_hermitian_f64(const float* echo, const float* dT1, co
     return 0;
 }
 
-// residual d = lhs - rhs, returns Σ|d|²   (src/utils/residual_kernels.cuh:73-96)
+// residual d = lhs - rhs, returns Σ|d|²   (src/utils/residual_kernels.cuh:26-64)
 double oracle_residual_f64(const float* lhs, const float* rhs, int64_t n, double* out) {
     double acc = 0;
     for (int64_t i = 0; i < n; i++) {

@@ -3,7 +3,9 @@
 // (oracle/ref_sim.cpp, oracle/ref_kernels.cpp) and, with nvcc, for the GPU (oracle/ref_gpu.cu):
 // element access, row access, size, drop_axis, in_bounds. Not the kmm library. In device code
 // every element or row index is checked against the view's extent; an index outside it sets
-// kmm_ref_out_of_bounds and is replaced by 0, so no access leaves the buffer.
+// kmm_ref_out_of_bounds and is replaced by 0, so no access leaves the buffer. Built with
+// KMM_REF_UNCHECKED the check is left out (kmm's own views do not check either), for timing the
+// reference's kernels only on launches that the checked build ran without a flagged index.
 #pragma once
 #include <array>
 #include <cstddef>
@@ -30,12 +32,13 @@ static __device__ unsigned int kmm_ref_out_of_bounds = 0;
 namespace kmm {
 
 KMM_REF_HD inline int64_t checked_index(int64_t i, int64_t extent) {
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDA_ARCH__) && !defined(KMM_REF_UNCHECKED)
     if (i < 0 || i >= extent) {
         kmm_ref_out_of_bounds = 1;
         return 0;
     }
 #endif
+    (void)extent;
     return i;
 }
 

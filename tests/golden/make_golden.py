@@ -2,7 +2,8 @@
 
 Builds oracle/_ref/ref_golden and oracle/_ref/ref_sim (oracle/Makefile target `ref`, which
 compiles oracle/ref_golden.cpp and oracle/ref_sim.cpp against the reference's include and src
-trees, by default under /root/reference) and stores their JSON output next to this script:
+trees: the directory named by COMPAS_REFERENCE, by default /root/reference) and stores their JSON
+output next to this script:
   * ref_complex_ops.json  — complex_type.h primitives (FP32);
   * ref_simulations.json  — inputs and outputs of seeded FISP, pSSFP, Cartesian (phase encoding,
                             signal, J·v, Jᴴ·v, residual) and spiral (signal) cases from the

@@ -54,7 +54,7 @@ def test_version_and_layout_tables(cb):
     assert cb.version().startswith("compas-b200")
     fisp = cb.fisp_configs()
     assert fisp and all(k * g >= 1 for k, g in fisp)
-    assert any(k * g >= 128 for k, g in fisp)  # max_state up to 128 is covered (fisp.cu:355-364)
+    assert any(k * g >= 128 for k, g in fisp)  # max_state up to 128 is covered (src/simulate/fisp.cu:93-102)
     assert any(k * g >= 35 for k, g in cb.pssfp_configs())
 
 
@@ -93,3 +93,63 @@ def test_null_handles_are_rejected_by_the_tangent_entry_points(cb):
     assert b"null" in lib.compas_last_error()
     assert lib.compas_b200_make_batch_tangents(None, 0, None, None, None, None, 4, None) is None
     assert lib.compas_last_error() is not None
+
+
+def test_voxel_shard_partition_through_the_c_abi():
+    # the library's partition of a slice over ranks (host code: runs without a GPU)
+    import ctypes as C
+
+    import compas_b200 as cb
+
+    lib = cb.library()
+    b, e = C.c_int64(), C.c_int64()
+    for nv in (0, 1, 5, 49, 50176, 200003):
+        for world in (1, 2, 3, 7, 8):
+            prev = 0
+            for rank in range(world):
+                assert lib.compas_b200_voxel_shard(nv, rank, world, C.byref(b), C.byref(e)) == 0
+                assert b.value == prev and e.value >= b.value
+                assert e.value - b.value in (nv // world, nv // world + 1)
+                prev = e.value
+            assert prev == nv
+    for bad in ((10, 2, 2), (10, -1, 2), (10, 0, 0), (-1, 0, 1)):
+        assert lib.compas_b200_voxel_shard(*bad, C.byref(b), C.byref(e)) == -1
+        assert lib.compas_last_error()
+
+
+def test_vector_value_type_on_the_host(tmp_path):
+    # compas/vector.h (vector<T, N>, vfloat3, …) compiled by the host compiler: construction,
+    # element names, layout, dot / norm / cross, elementwise arithmetic, map, comparisons
+    import shutil
+    import subprocess
+
+    cxx = shutil.which("g++") or shutil.which("c++")
+    if cxx is None:
+        pytest.skip("no host C++ compiler")
+    src = tmp_path / "v.cpp"
+    src.write_text(r"""
+#include "compas/vector.h"
+#include <cmath>
+#include <cstdio>
+using namespace compas;
+int main() {
+    vfloat3 a(1.f, 2.f, 2.f), b(0.f, 1.f, 0.f);
+    vfloat3 c = cross(a, b);
+    vdouble4 d(2.0);
+    d += vdouble4(1.0, 2.0, 3.0, 4.0);
+    d = 0.5 * (d * 2.0) - 1.0;
+    ndint<5> n(7);
+    auto m = a.map([](float x) { return int(x * 10); });
+    vfloat2 big(3e30f, 4e30f);
+    int ok = norm(a) == 3.f && dot(a, b) == 2.f && c.x == -2.f && c.y == 0.f && c.z == 1.f
+        && sizeof(vfloat3) == 12 && alignof(vfloat2) == 8 && sizeof(vfloat4) == 16 && alignof(vfloat4) == 16
+        && d[0] == 2.0 && d.w == 5.0 && n.size() == 5 && n[4] == 7 && m[1] == 20
+        && a == vfloat3(1.f, 2.f, 2.f) && a != b && !(vfloat2(1.f) == vfloat3(1.f))
+        && std::fabs(norm(big) - 5e30f) < 1e24f && std::isnan(norm(vfloat2(NAN, 1.f)));
+    std::printf("%d\n", ok);
+    return ok ? 0 : 1;
+}
+""")
+    exe = tmp_path / "v"
+    subprocess.run([cxx, "-std=c++17", "-I", str(ROOT / "compas-toolkit_b200" / "include"), str(src), "-o", str(exe)], check=True)
+    assert subprocess.run([str(exe)], capture_output=True, text=True).stdout.strip() == "1"

@@ -2,11 +2,14 @@
 
 One iteration simulates m(p), the derivatives dm/dT1 and dm/dT2 (forward differences, or exact
 tangents for delta = 0), the signal s(p), the residual b = y - s, runs CGLS steps of J·d / Jᴴ·b
-on min ‖J δ - b‖² and updates the parameters. The tests check that (1) the CUDA-graph replay
-gives the same bits as the eager kernel sequence over two iterations, (2) with one CGLS step the
-step equals α·Re(Jᴴ b) with α = ‖g‖²/‖J g‖², recomputed here from the public operations, within
-the FP32 tolerance of the other tests, (3) fitting data simulated from known parameters lowers the
-objective, and (4) the same with exact derivatives, which equal simulate_magnetization_tangents.
+on min ‖J δ - b‖² and updates the parameters after a line search on the objective (the first of
+t = 1, ½ that does not raise ‖y - s‖², else no step). The tests check that (1) the CUDA-graph
+replay gives the same bits as the eager kernel sequence over two iterations, (2) with one CGLS
+step the step equals α·Re(Jᴴ b) with α = ‖g‖²/‖J g‖², recomputed here from the public
+operations, within the FP32 tolerance of the other tests, (3) fitting data simulated from known
+parameters lowers the objective, (4) the same with exact derivatives, which equal
+simulate_magnetization_tangents, and (5) with the line search the objective never rises and the
+update is the step length it reports.
 """
 import numpy as np
 import pytest
@@ -68,8 +71,9 @@ def test_graph_replay_matches_eager_bitwise(setup):
 
 
 def test_single_cg_step_is_the_exact_line_minimiser(setup):
+    # without the line search the full CGLS step is applied
     cb, ctx, start, seq, traj, coils, y = setup
-    gn = _gn(cb, ctx, start, seq, traj, coils, y, cg_iterations=1)
+    gn = _gn(cb, ctx, start, seq, traj, coils, y, cg_iterations=1, line_search=False)
     params0 = cb.TissueParameters.from_soa(ctx, start)
     gn.run(graph=False)
     ctx.synchronize()
@@ -157,3 +161,43 @@ def test_exact_derivative_iteration(setup, kind):
             assert np.array_equal(eager.array(name).to_numpy(), graph.array(name).to_numpy()), (it, name)
         objs.append(graph.objective())
     assert objs[-1] < 0.5 * objs[0], objs
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_line_search_never_raises_the_objective(graph):
+    # the 64x64 FISP workload (400 TRs, 8 states, one coil), T1 and T2 started up to a factor 1.6
+    # off: every iteration's objective is at most the previous one, and the estimate moves by the
+    # step length the iteration reports (1, ½ or 0)
+    import compas_b200 as cb
+
+    ctx = cb.Context(0)
+    w = W.fisp_small()
+    rng = np.random.default_rng(31)
+    truth = w["params"]
+    start = truth.copy()
+    start[0] *= rng.uniform(0.6, 1.6, truth.shape[1])
+    start[1] *= rng.uniform(0.6, 1.6, truth.shape[1])
+    start = start.astype(np.float32)
+    seq = cb.FispSequence.from_dict(ctx, w["seq"])
+    traj = cb.CartesianTrajectory.from_dict(ctx, w["traj"])
+    p_true = cb.TissueParameters.from_soa(ctx, truth)
+    y = cb.magnetization_to_signal(ctx, cb.simulate_magnetization(ctx, p_true, seq), p_true, traj, w["coils"]).to_numpy()
+    gn = _gn(cb, ctx, start, seq, traj, w["coils"], y, cg_iterations=3)
+    objs, lengths = [], []
+    for _ in range(6):
+        p0 = gn.array("parameters").to_numpy()
+        gn.run(graph=graph)
+        objs.append(gn.objective())
+        t = gn.step_length()
+        lengths.append(t)
+        assert t in (0.0, 0.5, 1.0)
+        step = gn.array("step").to_numpy().astype(np.float64)
+        p1 = gn.array("parameters").to_numpy()
+        c = np.clip(1.0 + t * step[:2], 0.5, 2.0)
+        np.testing.assert_allclose(p1[0], p0[0] * c[0], rtol=1e-6)
+        np.testing.assert_allclose(p1[1], p0[1] * c[1], rtol=1e-6)
+        np.testing.assert_allclose(p1[4], p0[4] + t * step[2], rtol=1e-6, atol=1e-7)
+        if t > 0:  # the taken trial's objective is the next iteration's starting objective
+            assert float(gn.array("scalars").to_numpy()[6]) <= objs[-1]
+    assert all(b <= a for a, b in zip(objs, objs[1:])), objs
+    assert objs[-1] < objs[0], (objs, lengths)

@@ -18,7 +18,8 @@ sys.path.insert(0, {pkg!r})
 import compas_b200 as cb
 out = {{"fisp": [cb.fisp_launch_choice(*s) for s in [(25, 50176, 35), (25, 4096, 1), (8, 4096, 1)]],
        "pssfp": [cb.pssfp_launch_choice(*s) for s in [(35, 16384), (5, 4096)]],
-       "fisp_configs": cb.fisp_configs(), "pssfp_configs": cb.pssfp_configs()}}
+       "fisp_configs": cb.fisp_configs(), "pssfp_configs": cb.pssfp_configs(),
+       "fisp_packed": [cb.fisp_config_packed(i) for i in range(len(cb.fisp_configs()))]}}
 cb.set_fisp_launch(0, 2)
 out["override_uncovered"] = cb.fisp_launch_choice(25, 50176, 35)
 ok = [i for i, (k, g) in enumerate(cb.fisp_configs()) if k * g >= 25][-1]
@@ -44,7 +45,10 @@ def test_builtin_choice_covers_the_states():
     for (cfg, warps), n in zip(out["fisp"], (25, 25, 8)):
         k, g = fc[cfg]
         assert k * g >= n and 1 <= warps <= 8
-    assert tuple(fc[out["fisp"][0][0]]) == (25, 1) and out["fisp"][0][1] == 8  # 35 positions: 8 warps
+    # 25 states x 35 positions at 50176 voxels: one lane per voxel in the packed layout (13 pairs of
+    # states, two states per two-wide instruction), 8 warps
+    assert tuple(fc[out["fisp"][0][0]]) == (26, 1) and out["fisp_packed"][out["fisp"][0][0]]
+    assert out["fisp"][0][1] == 8
     assert fc[out["fisp"][2][0]][1] == 4  # few voxel/position pairs: states split over 4 lanes
     for cfg, nz in zip(out["pssfp"], (35, 5)):
         zt, gz = pc[cfg]
