@@ -37,6 +37,12 @@ namespace {
 
 constexpr int kScratchPartials = 1 << 16;
 constexpr int kBlock = 256;
+// The residual's grid-stride launch uses at most 1024 blocks (residual_partial_count), one partial
+// sum each, so the kernels never need more than 1024 of the scratch's entries. The element limit
+// below is therefore a contract with callers, fixed when this entry point was published, not a
+// capacity of the kernels.
+constexpr int kMaxResidualBlocks = 1024;
+static_assert(kScratchPartials >= kMaxResidualBlocks, "the scratch must hold one partial sum per block");
 constexpr int64_t kMaxElements = int64_t(kScratchPartials) * kBlock;
 
 static __device__ __align__(256) float g_residual_partials[kScratchPartials];
@@ -85,6 +91,7 @@ void residual_noalloc(int device, const cfloat* lhs, const cfloat* rhs, cfloat* 
     // the allocating entry point's grid (grid-stride, at most 1024 blocks): the same kernels in the
     // same order, so diff and objective are the same bits, and the scratch holds every partial
     const int blocks = residual_partial_count(n);
+    if (blocks > kMaxResidualBlocks) COMPAS_ERROR("residual grid larger than the scratch");
     kernels::residual_kernel<<<blocks, kBlock, 0, stream>>>(reinterpret_cast<const float2*>(lhs),
                                                             reinterpret_cast<const float2*>(rhs), n,
                                                             reinterpret_cast<float2*>(diff), partials);

@@ -5,8 +5,11 @@ owns a fixed device-memory budget and passes the library pre-allocated buffers. 
 caller-owned device buffers, calls it through the C ABI twice in a row with different inputs
 (its scratch is shared between calls), and checks each result against the allocating entry point
 compas_compute_residual on the same inputs: the difference array exactly, the objective within the
-FP32 tolerance of the other GPU tests. It also checks that sizes beyond the stated limit are
-rejected with an error instead of running.
+FP32 tolerance of the other GPU tests. Around those calls it reads the device's memory figures —
+the default memory pool's used and reserved bytes, PyTorch's allocated bytes and the device's free
+memory — and checks that none changes: the entry point allocates nothing. It also checks that an
+empty input writes an objective of 0 and that sizes beyond the stated limit are rejected with an
+error instead of running.
 """
 import ctypes as C
 
@@ -29,6 +32,26 @@ def lib_and_ctx():
     return cb, fn, cb.Context(0)
 
 
+def _memory(torch):
+    """(default pool used, default pool reserved, torch allocated, device free) bytes of device 0."""
+    from cuda.bindings import driver as drv
+
+    torch.cuda.synchronize(0)
+    err, dev = drv.cuDeviceGet(0)
+    assert err == drv.CUresult.CUDA_SUCCESS
+    err, pool = drv.cuDeviceGetDefaultMemPool(dev)
+    assert err == drv.CUresult.CUDA_SUCCESS
+    out = []
+    for attr in (drv.CUmemPool_attribute.CU_MEMPOOL_ATTR_USED_MEM_CURRENT,
+                 drv.CUmemPool_attribute.CU_MEMPOOL_ATTR_RESERVED_MEM_CURRENT):
+        err, v = drv.cuMemPoolGetAttribute(pool, attr)
+        assert err == drv.CUresult.CUDA_SUCCESS
+        out.append(int(v))
+    err, free, _ = drv.cuMemGetInfo()
+    assert err == drv.CUresult.CUDA_SUCCESS
+    return out[0], out[1], torch.cuda.memory_allocated(0), int(free)
+
+
 def _complex(rng, shape):
     return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
 
@@ -49,14 +72,32 @@ def test_noalloc_residual_matches_allocating_entry_point_twice(lib_and_ctx):
         db = torch.from_numpy(b.view(np.float32).reshape(-1)).to("cuda:0")
         ddiff = torch.full_like(da, float("nan"))
         dobj = torch.full((1,), float("nan"), device="cuda:0")
+        if call == 0:
+            # the first call on a device resolves the scratch (and loads the kernels' module, which
+            # places the static scratch): measure the memory figures around the later calls
+            rc = fn(0, da.data_ptr(), db.data_ptr(), ddiff.data_ptr(), dobj.data_ptr(), a.size, stream.cuda_stream)
+            assert rc == 0, cb.library().compas_last_error()
+        before = _memory(torch)
         rc = fn(0, da.data_ptr(), db.data_ptr(), ddiff.data_ptr(), dobj.data_ptr(), a.size, stream.cuda_stream)
         assert rc == 0, cb.library().compas_last_error()
         stream.synchronize()
+        assert _memory(torch) == before, "the allocation-free residual changed the device's memory use"
         diff = ddiff.cpu().numpy().view(np.complex64).reshape(shape)
         assert np.array_equal(diff, diff_ref)
         obj = float(dobj.item())
         assert abs(obj - obj_ref) <= TOL_FP32 * obj_ref, (call, obj, obj_ref)
         assert obj == obj_ref  # the same launch as the allocating entry point: the same bits
+
+
+def test_noalloc_residual_of_nothing_is_zero(lib_and_ctx):
+    import torch
+
+    cb, fn, _ = lib_and_ctx
+    dobj = torch.full((1,), float("nan"), device="cuda:0")
+    stream = torch.cuda.current_stream(0)
+    assert fn(0, None, None, None, dobj.data_ptr(), 0, stream.cuda_stream) == 0, cb.library().compas_last_error()
+    stream.synchronize()
+    assert float(dobj.item()) == 0.0
 
 
 def test_noalloc_residual_rejects_sizes_beyond_its_scratch(lib_and_ctx):
