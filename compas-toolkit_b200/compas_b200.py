@@ -101,6 +101,12 @@ _SIGS = {
     "compas_b200_wait_probe": ([_P, _I64], _I),
     "compas_b200_gauss_newton_set_line_search": ([_P, _I], _I),
     "compas_b200_voxel_shard": ([_I64, _I, _I, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], _I),
+    "compas_b200_compute_gemm": ([_P, _P, _P, _P, C.c_float, C.c_float, _I], _I),
+    "compas_b200_compute_complex_gemm": ([_P, _P, _P, _P, C.c_float, C.c_float, _I], _I),
+    "compas_b200_convert_complex_to_planar": ([_P, _P, _P], _I),
+    "compas_b200_convert_planar_to_complex": ([_P, _P, _P], _I),
+    "compas_b200_make_array_bfloat16": ([_P, _P, _I, C.POINTER(C.c_int64)], _P),
+    "compas_b200_read_array_bfloat16": ([_P, _P, _P, _I64], None),
     "compas_b200_comm_unique_id": ([C.c_char_p, _I], _I),
     "compas_b200_make_communicator": ([_P, _I, _I, C.c_char_p], _P),
     "compas_b200_allreduce_sum": ([_P, _P, _P], _I),
@@ -190,6 +196,18 @@ class CompasArray:
         self.shape = tuple(int(s) for s in shape)
 
     @staticmethod
+    def from_bfloat16(context: Context, arr) -> "CompasArray":
+        """A bfloat16 device array from float values (rounded to the nearest bfloat16); its numpy
+        side is the raw 16-bit patterns (dtype uint16, see bfloat16_bits / bfloat16_values)."""
+        bits = bfloat16_bits(arr)
+        if bits.ndim < 1 or bits.ndim > 3:
+            raise CompasError("cannot support rank > 3")
+        sizes = (C.c_int64 * bits.ndim)(*bits.shape)
+        ptr = library().compas_b200_make_array_bfloat16(context.ptr, bits.ctypes.data, bits.ndim, sizes)
+        _check(ptr, "compas_b200_make_array_bfloat16!")
+        return CompasArray(context, ptr, np.uint16, bits.shape)
+
+    @staticmethod
     def from_numpy(context: Context, arr) -> "CompasArray":
         arr = np.asarray(arr)
         if np.iscomplexobj(arr):
@@ -215,6 +233,10 @@ class CompasArray:
 
     def to_numpy(self) -> np.ndarray:
         out = np.empty(self.shape, self.dtype)
+        if self.dtype == np.uint16:
+            library().compas_b200_read_array_bfloat16(self.context.ptr, self.ptr, out.ctypes.data, out.size)
+            _check()
+            return out
         fn = library().compas_read_array_complex if self.dtype == np.complex64 else library().compas_read_array_float
         fn(self.context.ptr, self.ptr, out.ctypes.data, out.size)
         _check()
@@ -662,6 +684,59 @@ class ServeEngine(_Object):
 
     def reset_stats(self):
         library().compas_b200_server_reset_stats(self.ptr)
+
+
+def bfloat16_bits(x) -> np.ndarray:
+    """float values -> bfloat16 bit patterns (uint16), rounded to nearest even."""
+    b = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    return ((b + 0x7FFF + ((b >> 16) & 1)) >> 16).astype(np.uint16)
+
+
+def bfloat16_values(bits) -> np.ndarray:
+    """bfloat16 bit patterns (uint16) -> float32 values."""
+    return (np.asarray(bits, np.uint16).astype(np.uint32) << 16).view(np.float32)
+
+
+GEMM_METHODS = {"Pedantic": 0, "Regular": 1, "Fast": 2}
+
+
+def compute_gemm(context: Context, result: CompasArray, lhs: CompasArray, rhs: CompasArray, alpha: float = 1.0,
+                 beta: float = 0.0, method: str = "Regular") -> CompasArray:
+    """result = alpha·lhs·rhsᵀ + beta·result in place (compas/utils/gemm.h): float [m][n] result,
+    float or bfloat16 [m][k] / [n][k] operands."""
+    if library().compas_b200_compute_gemm(context.ptr, result.ptr, lhs.ptr, rhs.ptr, float(alpha), float(beta),
+                                          GEMM_METHODS[method]) != 0:
+        _check(None, "compas_b200_compute_gemm!")
+    return result
+
+
+def compute_complex_gemm(context: Context, result: CompasArray, lhs: CompasArray, rhs: CompasArray,
+                         alpha: float = 1.0, beta: float = 0.0, method: str = "Regular") -> CompasArray:
+    """The complex form on planar [2][rows][cols] arrays (plane 0 real, plane 1 imaginary)."""
+    if library().compas_b200_compute_complex_gemm(context.ptr, result.ptr, lhs.ptr, rhs.ptr, float(alpha),
+                                                  float(beta), GEMM_METHODS[method]) != 0:
+        _check(None, "compas_b200_compute_complex_gemm!")
+    return result
+
+
+def convert_complex_to_planar(context: Context, x, bfloat16: bool = False) -> CompasArray:
+    """complex [n][m] -> planar [2][n][m] (float32, or bfloat16 when `bfloat16`)."""
+    src = _arr(context, x, np.complex64)
+    shape = (2,) + src.shape
+    out = (CompasArray.from_bfloat16(context, np.zeros(shape, np.float32)) if bfloat16
+           else CompasArray.from_numpy(context, np.zeros(shape, np.float32)))
+    if library().compas_b200_convert_complex_to_planar(context.ptr, out.ptr, src.ptr) != 0:
+        _check(None, "compas_b200_convert_complex_to_planar!")
+    return out
+
+
+def convert_planar_to_complex(context: Context, x) -> CompasArray:
+    """planar float [2][n][m] -> complex [n][m]."""
+    src = _arr(context, x, np.float32)
+    out = CompasArray.from_numpy(context, np.zeros(src.shape[1:], np.complex64))
+    if library().compas_b200_convert_planar_to_complex(context.ptr, out.ptr, src.ptr) != 0:
+        _check(None, "compas_b200_convert_planar_to_complex!")
+    return out
 
 
 def voxel_shard(nvoxels: int, rank: int, world: int) -> tuple:

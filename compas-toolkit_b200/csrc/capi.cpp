@@ -142,6 +142,23 @@ compas::JacobianComputeMethod jacobian_method(int m) {
     return compas::JacobianComputeMethod(m);
 }
 
+compas::GemmComputeMethod gemm_method(int m) {
+    if (m < 0 || m > 2) throw compas::CompasException("invalid GemmComputeMethod");
+    return compas::GemmComputeMethod(m);
+}
+
+template<typename T, size_t N>
+compas::Array<T, N>* mutable_array_of(compas_array* arr, const char* what) {
+    if (!arr) throw compas::CompasException(std::string("null array: ") + what);
+    if (auto* p = dynamic_cast<compas::Array<T, N>*>(handle<compas::Object>(arr))) return p;
+    throw compas::CompasException(std::string("array `") + what + "` has the wrong element type or rank");
+}
+
+template<typename T, size_t N>
+const compas::Array<T, N>* maybe_array(const compas_array* arr) {
+    return arr ? dynamic_cast<const compas::Array<T, N>*>(handle<compas::Object>(arr)) : nullptr;
+}
+
 }  // namespace
 
 namespace compas {
@@ -441,6 +458,71 @@ compas_array* compas_b200_compute_jacobian(const compas_context* ctx, const comp
                 jacobian_method(method)));
         });
     });
+}
+
+int compas_b200_compute_gemm(const compas_context* ctx, compas_array* result, const compas_array* lhs,
+                             const compas_array* rhs, float alpha, float beta, int method) {
+    t_has_error = false;
+    guarded([&] {
+        auto& out = *mutable_array_of<float, 2>(result, "result");
+        if (const auto* l = maybe_array<compas::bfloat16, 2>(lhs)) {
+            compas::compute_gemm(ctx_of(ctx), out, *l, array_of<compas::bfloat16, 2>(rhs, "rhs"), alpha, beta,
+                                 gemm_method(method));
+        } else {
+            compas::compute_gemm(ctx_of(ctx), out, array_of<float, 2>(lhs, "lhs"), array_of<float, 2>(rhs, "rhs"),
+                                 alpha, beta, gemm_method(method));
+        }
+    });
+    return t_has_error ? -1 : 0;
+}
+
+int compas_b200_compute_complex_gemm(const compas_context* ctx, compas_array* result, const compas_array* lhs,
+                                     const compas_array* rhs, float alpha, float beta, int method) {
+    t_has_error = false;
+    guarded([&] {
+        auto& out = *mutable_array_of<float, 3>(result, "result");
+        if (const auto* l = maybe_array<compas::bfloat16, 3>(lhs)) {
+            compas::compute_complex_gemm(ctx_of(ctx), out, *l, array_of<compas::bfloat16, 3>(rhs, "rhs"), alpha, beta,
+                                         gemm_method(method));
+        } else {
+            compas::compute_complex_gemm(ctx_of(ctx), out, array_of<float, 3>(lhs, "lhs"),
+                                         array_of<float, 3>(rhs, "rhs"), alpha, beta, gemm_method(method));
+        }
+    });
+    return t_has_error ? -1 : 0;
+}
+
+int compas_b200_convert_complex_to_planar(const compas_context* ctx, compas_array* output, const compas_array* input) {
+    t_has_error = false;
+    guarded([&] {
+        const auto& in = array_of<cfloat, 2>(input, "input");
+        if (auto* o = output ? dynamic_cast<compas::Array<compas::bfloat16, 3>*>(handle<compas::Object>(output))
+                             : nullptr) {
+            compas::convert_complex_to_planar(ctx_of(ctx), *o, in);
+        } else {
+            compas::convert_complex_to_planar(ctx_of(ctx), *mutable_array_of<float, 3>(output, "output"), in);
+        }
+    });
+    return t_has_error ? -1 : 0;
+}
+
+int compas_b200_convert_planar_to_complex(const compas_context* ctx, compas_array* output, const compas_array* input) {
+    t_has_error = false;
+    guarded([&] {
+        compas::convert_planar_to_complex(ctx_of(ctx), *mutable_array_of<cfloat, 2>(output, "output"),
+                                          array_of<float, 3>(input, "input"));
+    });
+    return t_has_error ? -1 : 0;
+}
+
+const compas_array* compas_b200_make_array_bfloat16(const compas_context* context, const uint16_t* data, int rank,
+                                                    int64_t* sizes) {
+    return guarded([&] { return make_array(context, reinterpret_cast<const compas::bfloat16*>(data), rank, sizes); });
+}
+
+void compas_b200_read_array_bfloat16(const compas_context*, const compas_array* array, uint16_t* dest,
+                                     int64_t length) {
+    guarded([&] { read_array(array, dest, length, sizeof(uint16_t)); });
 }
 
 int compas_b200_voxel_shard(int64_t nvoxels, int rank, int world, int64_t* begin, int64_t* end) {

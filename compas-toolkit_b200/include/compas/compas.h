@@ -7,6 +7,7 @@
 // CPU fallback: every operation runs on the GPU and throws `CompasException` on error.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <array>
@@ -643,6 +644,38 @@ class GaussNewtonStep: public Object {
   private:
     std::shared_ptr<Impl> m_impl;
 };
+
+// ------------------------------------------------------------------------------------------
+// GEMM utilities   (compas/utils/gemm.h:7-70)
+// ------------------------------------------------------------------------------------------
+using bfloat16 = __nv_bfloat16;
+
+enum struct GemmComputeMethod {
+    Pedantic,  // highest precision: FP32 on the CUDA cores
+    Regular,   // FP32 on the CUDA cores
+    Fast       // split-BF16 on the tensor cores, ~1e-5 relative (the reference: TF32, ~1e-3)
+};
+
+// result = alpha·lhs·rhsᵀ + beta·result, lhs [m][k], rhs [n][k], result [m][n] (result is not read
+// when beta == 0). BF16 inputs run on the tensor cores with FP32 accumulation for every method.
+void compute_gemm(const CompasContext& ctx, Array<float, 2>& result, const Array<float, 2>& lhs,
+                  const Array<float, 2>& rhs, float alpha, float beta,
+                  GemmComputeMethod kind = GemmComputeMethod::Regular);
+void compute_gemm(const CompasContext& ctx, Array<float, 2>& result, const Array<bfloat16, 2>& lhs,
+                  const Array<bfloat16, 2>& rhs, float alpha, float beta,
+                  GemmComputeMethod kind = GemmComputeMethod::Regular);
+// the same for complex matrices in planar form: [2][rows][cols], plane 0 real, plane 1 imaginary
+// (no conjugation: result = alpha·lhs·rhsᵀ + beta·result)
+void compute_complex_gemm(const CompasContext& ctx, Array<float, 3>& result, const Array<float, 3>& lhs,
+                          const Array<float, 3>& rhs, float alpha, float beta,
+                          GemmComputeMethod kind = GemmComputeMethod::Regular);
+void compute_complex_gemm(const CompasContext& ctx, Array<float, 3>& result, const Array<bfloat16, 3>& lhs,
+                          const Array<bfloat16, 3>& rhs, float alpha, float beta,
+                          GemmComputeMethod kind = GemmComputeMethod::Regular);
+// interleaved complex [n][m] <-> planar [2][n][m]
+void convert_complex_to_planar(const CompasContext& ctx, Array<float, 3>& output, const Array<cfloat, 2>& input);
+void convert_complex_to_planar(const CompasContext& ctx, Array<bfloat16, 3>& output, const Array<cfloat, 2>& input);
+void convert_planar_to_complex(const CompasContext& ctx, Array<cfloat, 2>& output, const Array<float, 3>& input);
 
 // ------------------------------------------------------------------------------------------
 // one slice sharded over processes, one GPU each (no counterpart in the reference's API: its kmm

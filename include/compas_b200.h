@@ -265,6 +265,29 @@ COMPAS_API int compas_b200_gauss_newton_set_line_search(const compas_object* gn,
 /* Kernel nodes of the captured graph, -1 before the first graph run. */
 COMPAS_API int compas_b200_gauss_newton_graph_kernels(const compas_object* gn);
 
+/* GEMM utilities (compas/utils/gemm.h:7-70; the reference's C ABI does not export them).
+ * result = alpha * lhs * rhs^T + beta * result with lhs [m][k], rhs [n][k], result [m][n] float
+ * arrays (result is not read when beta == 0); the complex form takes planar [2][rows][cols] arrays
+ * (plane 0 real, plane 1 imaginary). `method` is a GemmComputeMethod value: 0 Pedantic and
+ * 1 Regular compute in FP32 on the CUDA cores, 2 Fast in split-BF16 on the tensor cores (~1e-5
+ * relative). BF16 arrays (compas_b200_make_array_bfloat16) run on the tensor cores for every method.
+ * 0, or -1 on error. */
+COMPAS_API int compas_b200_compute_gemm(const compas_context* ctx, compas_array* result, const compas_array* lhs,
+                                        const compas_array* rhs, float alpha, float beta, int method);
+COMPAS_API int compas_b200_compute_complex_gemm(const compas_context* ctx, compas_array* result,
+                                                const compas_array* lhs, const compas_array* rhs, float alpha,
+                                                float beta, int method);
+/* interleaved complex [n][m] -> planar [2][n][m] (float, or bfloat16 rounded to nearest) and back */
+COMPAS_API int compas_b200_convert_complex_to_planar(const compas_context* ctx, compas_array* output,
+                                                     const compas_array* input);
+COMPAS_API int compas_b200_convert_planar_to_complex(const compas_context* ctx, compas_array* output,
+                                                     const compas_array* input);
+/* bfloat16 arrays (raw 16-bit patterns), as compas_make_array_float / compas_read_array_float */
+COMPAS_API const compas_array* compas_b200_make_array_bfloat16(const compas_context* ctx, const uint16_t* data,
+                                                               int rank, int64_t* sizes);
+COMPAS_API void compas_b200_read_array_bfloat16(const compas_context* ctx, const compas_array* array, uint16_t* dest,
+                                                int64_t length);
+
 /* One slice sharded over processes, one GPU each (no counterpart in the reference's C ABI; its
  * kmm runtime chunks voxels over the devices of one process, include/compas/core/context.h:51-68,
  * and sums the chunks' signals, src/trajectories/signal.cu:289-300).
