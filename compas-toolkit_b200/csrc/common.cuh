@@ -100,6 +100,18 @@ __device__ __forceinline__ float2 bcast2(float s) {
     return make_float2(s, s);
 }
 
+// L2 eviction policy "keep": lines written with it are evicted after other lines (PTX createpolicy)
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ void st_l2_hint(float2* ptr, float2 v, uint64_t policy) {
+    asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(ptr), "f"(v.x), "f"(v.y), "l"(policy)
+                 : "memory");
+}
+
 // e^{i·2π·turns}: accurate for any magnitude of `turns` (sincospi reduces exactly)
 __device__ __forceinline__ float2 cis_turns(double turns) {
     double frac = turns - rint(turns);  // exact in FP64 for |turns| < 2^52

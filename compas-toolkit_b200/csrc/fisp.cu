@@ -541,7 +541,6 @@ __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_beg
         unsigned starts = 0;
         for (int w = 0; w < nact; w++)
             if (w == 0 || (base + w) / P != (base + w - 1) / P) starts |= 1u << w;
-        const int nseg = __popc(starts);
 
         const float4* tab = a.table + int64_t(p) * a.nTR;
         FispState<K, G, TAN, PACKED> st;
@@ -606,29 +605,35 @@ __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_beg
                     // per segment, add its positions in increasing order to the tile's partial
                     // sum (the echo rows, unless the segment starts at position 0), then write
                     // the undersampling-expanded rows (fisp_kernels.cuh:246-259)
-                    const int span = nt * VB;
-                    for (int e = threadIdx.x; e < NQ * nseg * span; e += blockDim.x) {
-                        const int qn = e / (nseg * span), rest = e % (nseg * span);
-                        const int sgi = rest / span, j = (rest % span) / VB, gv = rest % VB;
-                        int w0 = 0;  // first warp of segment sgi: the (sgi+1)-th set bit of `starts`
-                        for (int w = 0, c = 0; w < nact; w++) {
-                            if (starts & (1u << w)) {
-                                if (c == sgi) {
-                                    w0 = w;
-                                    break;
+                    const uint64_t l2_keep = l2_policy_evict_last();
+                    // segment bounds, the same for every thread: warps [w0, w1) on one tile
+                    for (int w0 = 0; w0 < nact;) {
+                        int w1 = w0 + 1;
+                        while (w1 < nact && !(starts & (1u << w1))) w1++;
+                        const int seg_tile = (base + w0) / P;
+                        const bool first = (base + w0) % P == 0;
+                        // a partial sum is read again by a later round: keep it in L2; the
+                        // tile's final sum streams out
+                        const bool last = (base + w1 - 1) % P == P - 1;
+#pragma unroll
+                        for (int qn = 0; qn < NQ; qn++) {
+                            float2* out = qn == 0 ? a.echo : qn == 1 ? a.dT1 : a.dT2;
+                            for (int e = threadIdx.x; e < nt * VB; e += blockDim.x) {
+                                const int j = e / VB, gv = e % VB;  // VB is a compile-time power of two or 6
+                                const int v = seg_tile * VB + gv;
+                                if (v >= a.nvoxels) continue;
+                                const float2* col = samples + qn * plane + j * VB + gv;
+                                float2* row0 = out + int64_t(t0 + j) * a.uf * a.echo_stride + a.voxel_begin + v;
+                                float2 acc = first ? col[w0 * CH * VB] : cadd(*row0, col[w0 * CH * VB]);
+                                for (int w = w0 + 1; w < w1; w++) acc = cadd(acc, col[w * CH * VB]);
+                                for (int q = 0; q < a.uf; q++) {
+                                    float2* dst = row0 + int64_t(q) * a.echo_stride;
+                                    if (last) __stcs(dst, acc);
+                                    else st_l2_hint(dst, acc, l2_keep);
                                 }
-                                c++;
                             }
                         }
-                        const int seg_tile = (base + w0) / P;
-                        const int v = seg_tile * VB + gv;
-                        if (v >= a.nvoxels) continue;
-                        float2* out = qn == 0 ? a.echo : qn == 1 ? a.dT1 : a.dT2;
-                        const float2* col = samples + qn * plane + j * VB + gv;
-                        float2* row0 = out + int64_t(t0 + j) * a.uf * a.echo_stride + a.voxel_begin + v;
-                        float2 acc = (base + w0) % P == 0 ? col[w0 * CH * VB] : cadd(*row0, col[w0 * CH * VB]);
-                        for (int w = w0 + 1; w < nact && !(starts & (1u << w)); w++) acc = cadd(acc, col[w * CH * VB]);
-                        for (int q = 0; q < a.uf; q++) row0[int64_t(q) * a.echo_stride] = acc;
+                        w0 = w1;
                     }
                     __syncthreads();
                 }
