@@ -81,6 +81,8 @@ _SIGS = {
     "compas_b200_pssfp_config_info": ([_I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
     "compas_b200_fisp_launch_choice": ([_I, _I64, _I, C.POINTER(C.c_int), C.POINTER(C.c_int)], None),
     "compas_b200_pssfp_launch_choice": ([_I, _I64], _I),
+    "compas_b200_set_tc_launch": ([_I, _I, _I], None),
+    "compas_b200_tc_launch_choice": ([_I, _I, _I, _I, _I, _I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
     "compas_b200_simulate_magnetization_tangents": ([_P, _P, _P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)], _I),
     "compas_b200_set_fisp_tangent_launch": ([_I], None),
     "compas_b200_fisp_tangent_config_count": ([], _I),
@@ -860,6 +862,35 @@ def fisp_launch_choice(max_state: int, nvoxels: int, npositions: int) -> tuple:
 
 def pssfp_launch_choice(nz: int, nvoxels: int) -> int:
     return int(library().compas_b200_pssfp_launch_choice(int(nz), int(nvoxels)))
+
+
+# tensor-core contraction kinds (COMPAS_B200_TC_* in compas_b200.h)
+TC_KINDS = {"cartesian_signal": 0, "cartesian_jacobian": 1, "cartesian_hermitian": 2,
+            "spiral_signal": 3, "spiral_jacobian": 4, "spiral_hermitian": 5}
+
+
+def _tc_kind(kind) -> int:
+    return TC_KINDS[kind] if isinstance(kind, str) else int(kind)
+
+
+def set_tc_launch(kind, tile: int = 0, splits: int = 0):
+    """Override the readout tile (Cartesian signal / J·v; a multiple of 16 in [16, 256]) and the
+    split count of one tensor-core contraction kind; 0 keeps the tuning table's or built-in choice."""
+    library().compas_b200_set_tc_launch(_tc_kind(kind), int(tile), int(splits))
+    _check()
+
+
+def tc_launch_choice(kind, nvoxels: int, nreadouts: int, samples_per_readout: int, ncoils: int,
+                     device: int = 0) -> tuple:
+    """(tile, splits) a tensor-core contraction of this shape runs with (tile 0 where the kind has none)."""
+    tile, splits = C.c_int(), C.c_int()
+    rc = library().compas_b200_tc_launch_choice(_tc_kind(kind), int(device), int(nvoxels), int(nreadouts),
+                                                int(samples_per_readout), int(ncoils), C.byref(tile),
+                                                C.byref(splits))
+    if rc != 0:
+        _check()
+        raise CompasError("compas_b200_tc_launch_choice failed")
+    return tile.value, splits.value
 
 
 def pssfp_configs() -> list:

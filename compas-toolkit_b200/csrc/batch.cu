@@ -293,7 +293,7 @@ void SimulationBatch::Impl::plan_signal(Family& fam, const std::vector<int>& mem
             g.scratch.push_back(std::move(scratch));
             args.push_back(a);
             prep_counts.push_back(div_ceil(V, 128));
-            pack_counts.push_back(tc_pack_blocks(t.nreadouts, a.apack_stages));
+            pack_counts.push_back(tc_pack_blocks(a.nr, t.nreadouts, a.apack_stages));
             cta_counts.push_back(e.plan.ctas);
         }
         int64_t total = 0;

@@ -168,6 +168,7 @@ unsigned long long launch_count();
 void set_fisp_override(int config, int warps);
 void set_pssfp_override(int config);
 void set_fisp_tangent_override(int config);
+void set_tc_override(int kind, int tile, int splits);
 }  // namespace compas
 
 extern "C" {
@@ -717,6 +718,25 @@ void compas_b200_fisp_launch_choice(int max_state, int64_t nvoxels, int npositio
 int compas_b200_pssfp_launch_choice(int nz, int64_t nvoxels) {
     compas::PssfpLaunch L = compas::tuned_pssfp_launch(nz, nvoxels);
     return L.config < 0 ? compas::pssfp_default_launch(nz, nvoxels).config : L.config;
+}
+
+void compas_b200_set_tc_launch(int kind, int tile, int splits) {
+    guarded([&] { compas::set_tc_override(kind, tile, splits); });
+}
+
+int compas_b200_tc_launch_choice(int kind, int device, int nvoxels, int nreadouts, int samples_per_readout,
+                                 int ncoils, int* tile, int* splits) {
+    int rc = -1;
+    guarded([&] {
+        if (kind < 0 || kind >= int(compas::TcKind::Count)) COMPAS_ERROR("tensor-core contraction kind out of range");
+        if (nvoxels < 0 || nreadouts < 0 || samples_per_readout < 0 || ncoils < 0) COMPAS_ERROR("negative size");
+        const compas::TcTuning t = compas::tc_launch_choice(device, compas::TcKind(kind), nvoxels, nreadouts,
+                                                            samples_per_readout, ncoils);
+        if (tile) *tile = t.tile;
+        if (splits) *splits = t.splits;
+        rc = 0;
+    });
+    return rc;
 }
 
 compas_object* compas_b200_make_batch(const compas_context* context, int njobs, const compas_object* const* parameters,

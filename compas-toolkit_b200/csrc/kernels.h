@@ -130,6 +130,38 @@ struct TcPlan {
 };
 // readouts per tile of the Cartesian contraction: the multiple of 16 up to 256 that pads R least
 int tc_readout_tile(int R);
+
+// ---- tensor-core launch knobs searched by the autotuner -----------------------------------
+// Per contraction kind: the readout tile of the Cartesian signal / J·v kernel (a multiple of 16 in
+// [16, 256]) and the split count of every kind (voxel splits of the signal and J·v kernels, pair-tile
+// splits of the Cartesian Jᴴ·v kernel, readout splits of the spiral Jᴴ·v kernel); 0 = the built-in
+// choice. The accuracy bound of the signal and J·v kernels (≤ 512 K16 steps per split) still applies
+// to a tuned split count. Chosen, in order, from an explicit override (compas_b200_set_tc_launch),
+// the tuning table's "tc" lines, and the built-in heuristics.
+enum class TcKind : int {
+    CartesianSignal = 0,
+    CartesianJacobian = 1,
+    CartesianHermitian = 2,
+    SpiralSignal = 3,
+    SpiralJacobian = 4,
+    SpiralHermitian = 5,
+    Count = 6,
+};
+struct TcTuning {
+    int tile = 0, splits = 0;
+};
+// shape class: the kind and the log2 classes of the readout count R, the voxel count and C·S (coils ×
+// samples per readout)
+TcTuning tuned_tc(TcKind kind, int R, int64_t nvoxels, int64_t coil_samples);
+void set_tc_override(int kind, int tile, int splits);
+// the launch a call of this shape gets: tile (Cartesian signal / J·v, else 0) and split count
+TcTuning tc_launch_choice(int device, TcKind kind, int nvoxels, int R, int S, int C);
+// split counts the launches run (tuned or built-in), per kind
+int tc_hermitian_splits(int device, int nvoxels, int R, int S, int C);
+int tc_spiral_splits(int device, int nvoxels, int R, int S, int C, bool jac);
+int tc_spiral_hermitian_splits(int device, int nvoxels, int R, int S, int C);
+// readouts per chunk of a spiral contraction whose per-readout table takes `per_readout_bytes`
+int spiral_table_chunk(int64_t per_readout_bytes, int R);
 TcPlan tc_plan(int device, int nvoxels, int R, int S, int C, bool jac);
 // argument block of a Cartesian signal contraction; out / vchunk / status / tables set by the caller
 kernels::TcArgs tc_signal_args(const float* params, int64_t pstride, int nvoxels, const cfloat* echos,
@@ -142,7 +174,7 @@ struct TcTables {
 };
 TcTables tc_tables(int nvoxels, int R, int S, int C, bool jac);
 void tc_assign_tables(kernels::TcArgs& a, const TcTables& t, unsigned char* base);
-int tc_pack_blocks(int R, int apack_stages);  // 256-thread blocks of one job's echo packing
+int tc_pack_blocks(int nr, int R, int apack_stages);  // 256-thread blocks of one job's echo packing
 // batched prep (prep_blocks flattened 128-thread blocks), A packing (pack_blocks flattened
 // 256-thread blocks) and contraction (ctas flattened CTAs)
 void launch_tc_batch(cudaStream_t stream, int device, bool jac, const kernels::TcArgs* jobs, int njobs,

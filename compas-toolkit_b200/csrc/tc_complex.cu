@@ -33,6 +33,7 @@
 // split over CTA pairs (split-K); partial tiles are summed in a fixed order. Every wait is bounded.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "common.cuh"
@@ -523,27 +524,47 @@ int tc_readout_tile(int R) {
     return best;
 }
 
+namespace {
+TcTuning cartesian_tuning(int nvoxels, int R, int S, int C, bool jac) {
+    return tuned_tc(jac ? TcKind::CartesianJacobian : TcKind::CartesianSignal, R, nvoxels, int64_t(C) * S);
+}
+// the tuned readout tile when it pads R to at most 1/16 more rows than the built-in tile does (a
+// tuning table entry covers a class of readout counts), else the built-in tile
+int cartesian_tile(int nvoxels, int R, int S, int C, bool jac) {
+    const int tile = cartesian_tuning(nvoxels, R, S, C, jac).tile;
+    const int builtin = tc_readout_tile(R);
+    auto padded = [R](int nr) { return int64_t(div_ceil(std::max(R, 1), nr)) * nr; };
+    return tile > 0 && 16 * padded(tile) <= 17 * padded(builtin) ? tile : builtin;
+}
+}  // namespace
+
 TcPlan tc_plan(int device, int nvoxels, int R, int S, int C, bool jac) {
     TcPlan p;
+    const TcTuning tuning = cartesian_tuning(nvoxels, R, S, C, jac);
     p.ntiles = div_ceil(C * S, kernels::TC_PAIRS);
-    p.nr = tc_readout_tile(R);
+    p.nr = cartesian_tile(nvoxels, R, S, C, jac);
     p.mtiles = div_ceil(std::max(R, 1), p.nr);
     const int tiles = 2 * p.ntiles * p.mtiles;  // CTAs per voxel split
     const int vps = jac ? 16 : 32;
-    // split the voxel range over CTAs: pick the split count (≥ 16 stages per split) whose grid
-    // leaves the least idle SM time in the last wave of one CTA per SM
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    const int max_splits = std::max(1, std::min(64, nvoxels / (16 * vps)));
     int splits = 1;
-    double best = -1.0;
-    for (int sp = 1; sp <= max_splits; sp++) {
-        const int64_t ctas = int64_t(tiles) * sp;
-        const int64_t waves = (ctas + sms - 1) / sms;
-        const double eff = double(ctas) / double(waves * sms) - 0.002 * sp;  // mild preference for fewer partials
-        if (eff > best + 1e-9) {
-            best = eff;
-            splits = sp;
+    if (tuning.splits > 0) {
+        // tuned: at most 64 splits and at least one voxel stage each
+        splits = std::min({tuning.splits, 64, std::max(1, div_ceil(std::max(nvoxels, 1), vps))});
+    } else {
+        // split the voxel range over CTAs: pick the split count (≥ 16 stages per split) whose grid
+        // leaves the least idle SM time in the last wave of one CTA per SM
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        const int max_splits = std::max(1, std::min(64, nvoxels / (16 * vps)));
+        double best = -1.0;
+        for (int sp = 1; sp <= max_splits; sp++) {
+            const int64_t ctas = int64_t(tiles) * sp;
+            const int64_t waves = (ctas + sms - 1) / sms;
+            const double eff = double(ctas) / double(waves * sms) - 0.002 * sp;  // mild preference for fewer partials
+            if (eff > best + 1e-9) {
+                best = eff;
+                splits = sp;
+            }
         }
     }
     // The tensor core's FP32 accumulation loses a little precision per MMA (relative error grows
@@ -563,7 +584,7 @@ TcTables tc_tables(int nvoxels, int R, int S, int C, bool jac) {
     const int vps = jac ? 16 : 32;
     t.egk = (S % kernels::TC_PPG == 0) ? kernels::TC_PPG : 1;
     t.apack_stages = div_ceil(std::max(nvoxels, 1), vps);
-    t.nr = tc_readout_tile(R);
+    t.nr = cartesian_tile(nvoxels, R, S, C, jac);
     auto align = [](int64_t b) { return (b + 255) / 256 * 256; };
     t.vstep = 0;
     t.estart = t.vstep + align(8 * V);
@@ -585,8 +606,7 @@ void tc_assign_tables(kernels::TcArgs& a, const TcTables& t, unsigned char* base
     a.nr = t.nr;
 }
 
-int tc_pack_blocks(int R, int apack_stages) {
-    const int nr = tc_readout_tile(R);
+int tc_pack_blocks(int nr, int R, int apack_stages) {
     return div_ceil(apack_stages * 8, 256) * div_ceil(std::max(R, 1), nr) * nr;
 }
 

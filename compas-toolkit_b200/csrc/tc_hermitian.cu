@@ -434,6 +434,34 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TH_THREADS, 1) tc_he
 
 }  // namespace kernels
 
+// pair-tile splits of the Cartesian Jᴴ·v contraction: the tuned count (at most one split per pair
+// tile), else the count (≥ 4 tiles per split, ≤ 16 splits) that leaves the least idle part of the
+// last wave of one CTA per SM. Each pair tile's accumulation is drained separately, so the count
+// changes only the partial sums.
+int tc_hermitian_splits(int device, int nvoxels, int R, int S, int C) {
+    const int vtiles = 2 * div_ceil(nvoxels, 2 * kernels::TH_M);
+    const int ptiles = div_ceil(C * R, kernels::TH_PAIRS);
+    const TcTuning tuning = tuned_tc(TcKind::CartesianHermitian, R, nvoxels, int64_t(C) * S);
+    int splits = 1;
+    if (tuning.splits > 0) {
+        splits = std::max(1, std::min(tuning.splits, ptiles));
+    } else {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        double best = -1.0;
+        for (int sp = 1; sp <= std::max(1, std::min(16, ptiles / 4)); sp++) {
+            const int64_t ctas = int64_t(vtiles) * sp;
+            const int64_t waves = (ctas + sms - 1) / sms;
+            const double eff = double(ctas) / double(waves * sms) - 0.002 * sp;
+            if (eff > best + 1e-9) {
+                best = eff;
+                splits = sp;
+            }
+        }
+    }
+    return div_ceil(ptiles, div_ceil(ptiles, splits));  // the count the launch runs (none empty)
+}
+
 bool launch_jacobian_hermitian_tc(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
                                   const cfloat* echos, const cfloat* dT1, const cfloat* dT2, const cfloat* coils,
                                   int ncoils, const cfloat* vec, const CartesianGeom& g, cfloat* JHv) {
@@ -463,20 +491,7 @@ bool launch_jacobian_hermitian_tc(const CompasContext& ctx, const float* params,
     const int vtiles = 2 * div_ceil(nvoxels, 2 * kernels::TH_M);  // whole CTA pairs
     const int ptiles = div_ceil(ncoils * g.nreadouts, kernels::TH_PAIRS);
     const int kstages = div_ceil(g.ns, 32);
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device());
-    // split the pair tiles over CTAs (≥ 4 tiles each) to minimise the idle part of the last wave
-    int splits = 1;
-    double best = -1.0;
-    for (int sp = 1; sp <= std::max(1, std::min(16, ptiles / 4)); sp++) {
-        const int64_t ctas = int64_t(vtiles) * sp;
-        const int64_t waves = (ctas + sms - 1) / sms;
-        const double eff = double(ctas) / double(waves * sms) - 0.002 * sp;
-        if (eff > best + 1e-9) {
-            best = eff;
-            splits = sp;
-        }
-    }
+    int splits = tc_hermitian_splits(ctx.device(), nvoxels, g.nreadouts, g.ns, ncoils);
     a.tiles_per_split = div_ceil(ptiles, splits);
     splits = div_ceil(ptiles, a.tiles_per_split);
     const int64_t n = 4 * int64_t(nvoxels);

@@ -26,6 +26,7 @@
 #include <cuda_bf16.h>
 
 #include <cstdlib>
+#include <algorithm>
 #include <mutex>
 
 #include "common.cuh"
@@ -337,6 +338,39 @@ __global__ void __launch_bounds__(TS_THREADS, 1) tc_spiral_kernel(TsArgs a) {
 
 }  // namespace kernels
 
+// readouts per chunk of a spiral contraction whose per-readout table takes `per_readout_bytes`: the
+// tables of one chunk stay near 1 GB (COMPAS_B200_SPIRAL_TABLE_BYTES overrides the budget)
+int spiral_table_chunk(int64_t per_readout_bytes, int R) {
+    int64_t budget = int64_t(1) << 30;
+    if (const char* e = std::getenv("COMPAS_B200_SPIRAL_TABLE_BYTES")) budget = std::max<int64_t>(1, std::atoll(e));
+    return int(std::max<int64_t>(1, std::min<int64_t>(R, budget / std::max<int64_t>(1, per_readout_bytes))));
+}
+
+// voxel splits of the spiral signal / J·v contraction: at least enough for ≤ 512 K16 steps each
+// (4096 voxels of the signal, 2048 of J·v); then the tuned count (≤ 64, ≥ one voxel stage each), or
+// else enough CTAs to fill the GPU twice (≥ 8 stages each); returned as the count the launch runs
+int tc_spiral_splits(int device, int nvoxels, int R, int S, int C, bool jac) {
+    const int T = div_ceil(std::max(S, 1), kernels::TS_M);
+    const int ct_max = std::max(1, kernels::TS_NMAX / (2 * T));
+    const int groups = div_ceil(C, ct_max);
+    const int vps = jac ? 16 : 32;
+    const int min_splits = div_ceil(std::max(nvoxels, 1), jac ? 2048 : 4096);
+    const TcTuning tuning = tuned_tc(jac ? TcKind::SpiralJacobian : TcKind::SpiralSignal, R, nvoxels, int64_t(C) * S);
+    int splits = min_splits;
+    if (tuning.splits > 0) {
+        splits = std::max(min_splits, std::min({tuning.splits, 64, div_ceil(std::max(nvoxels, 1), vps)}));
+    } else {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        const int64_t ctas = int64_t(R) * groups;
+        if (ctas * splits < 2 * sms)
+            splits = std::max(splits, int(std::min<int64_t>(div_ceil(2 * sms, int(ctas)), div_ceil(nvoxels, 8 * vps))));
+    }
+    // the count the launch runs: voxels per split rounded up to whole stages, every split non-empty
+    const int vchunk = div_ceil(div_ceil(std::max(nvoxels, 1), splits), vps) * vps;
+    return div_ceil(std::max(nvoxels, 1), vchunk);
+}
+
 namespace {
 
 template<bool JAC>
@@ -364,15 +398,8 @@ bool launch_tc_spiral(const CompasContext& ctx, kernels::TsArgs a, bool jac) {
     const int ct_max = std::max(1, kernels::TS_NMAX / (2 * T));
     const int groups = div_ceil(a.C, ct_max);
     a.CT = div_ceil(a.C, groups);
-    // voxel splits: ≤ 512 K16 steps each (4096 voxels of the signal, 2048 of J·v) and enough CTAs to
-    // fill the GPU
     const int vps = jac ? 16 : 32;
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device());
-    int splits = div_ceil(a.nvoxels, jac ? 2048 : 4096);
-    const int64_t ctas = int64_t(a.R) * groups;
-    if (ctas * splits < 2 * sms)
-        splits = std::max(splits, int(std::min<int64_t>(div_ceil(2 * sms, int(ctas)), div_ceil(a.nvoxels, 8 * vps))));
+    int splits = tc_spiral_splits(ctx.device(), a.nvoxels, a.R, a.S, a.C, jac);
     a.vchunk = div_ceil(div_ceil(a.nvoxels, splits), vps) * vps;
     splits = div_ceil(a.nvoxels, a.vchunk);
     const int64_t n = int64_t(a.C) * a.R * a.S;
@@ -382,10 +409,7 @@ bool launch_tc_spiral(const CompasContext& ctx, kernels::TsArgs a, bool jac) {
     // readouts in chunks whose base table ([readouts][TERMS][T][V] complex) stays near 1 GB
     // (COMPAS_B200_SPIRAL_TABLE_BYTES overrides the budget; results do not depend on it)
     const int terms = jac ? 2 : 1;
-    const int64_t per_readout = int64_t(terms) * T * a.nvoxels * int64_t(sizeof(float2));
-    int64_t budget = int64_t(1) << 30;
-    if (const char* e = std::getenv("COMPAS_B200_SPIRAL_TABLE_BYTES")) budget = std::max<int64_t>(1, std::atoll(e));
-    const int chunk = int(std::max<int64_t>(1, std::min<int64_t>(a.R, budget / per_readout)));
+    const int chunk = spiral_table_chunk(int64_t(terms) * T * a.nvoxels * int64_t(sizeof(float2)), a.R);
     Array<cfloat, 2> base({std::min(chunk, a.R), int64_t(terms) * T * a.nvoxels}, ctx.device(), ctx.stream());
     a.base = reinterpret_cast<const float2*>(base.data());
     if (jac) set_smem_attribute<true>();

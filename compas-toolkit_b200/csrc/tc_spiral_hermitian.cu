@@ -386,6 +386,28 @@ __global__ void __launch_bounds__(TX_THREADS, 1) tc_spiral_hermitian_kernel(TxAr
 
 }  // namespace kernels
 
+// readout splits within one readout chunk of the spiral Jᴴ·v contraction: the tuned count (at most
+// one readout each), else enough CTAs to fill the GPU twice (≥ 4 readouts each); returned as the
+// count the launch runs (every split non-empty). Each readout's accumulation is drained separately,
+// so the count changes only the partial sums.
+int tc_spiral_hermitian_splits(int device, int nvoxels, int R, int S, int C) {
+    const int T = div_ceil(std::max(S, 1), kernels::TX_M);
+    const int chunk = spiral_table_chunk(int64_t(T) * nvoxels * int64_t(sizeof(float2)), R);
+    const TcTuning tuning = tuned_tc(TcKind::SpiralHermitian, R, nvoxels, int64_t(C) * S);
+    int splits;
+    if (tuning.splits > 0) {
+        splits = std::max(1, std::min(tuning.splits, chunk));
+    } else {
+        const int groups = div_ceil(C, kernels::TX_CTMAX);
+        const int vtiles = div_ceil(nvoxels, kernels::TX_M);
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        const int want = div_ceil(2 * sms, vtiles * groups);
+        splits = std::max(1, std::min(want, div_ceil(chunk, 4)));
+    }
+    return div_ceil(chunk, div_ceil(chunk, splits));
+}
+
 bool launch_jacobian_hermitian_spiral_tc(const CompasContext& ctx, const float* params, int64_t pstride, int nvoxels,
                                          const cfloat* echos, const cfloat* dT1, const cfloat* dT2,
                                          const cfloat* coils, int ncoils, const cfloat* vec, int nreadouts, int ns,
@@ -423,16 +445,9 @@ bool launch_jacobian_hermitian_spiral_tc(const CompasContext& ctx, const float* 
     // readouts in chunks whose ct table ([readouts][T][V] complex) stays near 1 GB
     // (COMPAS_B200_SPIRAL_TABLE_BYTES overrides the budget; it changes only the order in which the
     // readouts' contributions are summed)
-    const int64_t per_readout = int64_t(T) * nvoxels * int64_t(sizeof(float2));
-    int64_t budget = int64_t(1) << 30;
-    if (const char* e = std::getenv("COMPAS_B200_SPIRAL_TABLE_BYTES")) budget = std::max<int64_t>(1, std::atoll(e));
-    const int chunk = int(std::max<int64_t>(1, std::min<int64_t>(nreadouts, budget / per_readout)));
+    const int chunk = spiral_table_chunk(int64_t(T) * nvoxels * int64_t(sizeof(float2)), nreadouts);
     const int nchunks = div_ceil(nreadouts, chunk);
-    // readout splits within a chunk so that the CTAs fill the GPU (≥ 4 readouts each)
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device());
-    const int want = div_ceil(2 * sms, vtiles * groups);
-    const int splits = std::max(1, std::min(want, div_ceil(chunk, 4)));
+    const int splits = tc_spiral_hermitian_splits(ctx.device(), nvoxels, nreadouts, ns, ncoils);
     a.readouts_per_split = div_ceil(chunk, splits);
     a.nsplit_launch = div_ceil(chunk, a.readouts_per_split);
     const int partials_per_chunk = groups * a.nsplit_launch;

@@ -1,12 +1,16 @@
 // tuning.cu — launch-layout selection for the simulation kernels.
 //
 // The FISP and pSSFP kernels are instantiated for several register layouts (states or
-// isochromats per lane × lanes per voxel). The choice is made, in order, from
+// isochromats per lane × lanes per voxel); the tensor-core contractions take a readout tile
+// (Cartesian signal / J·v) and a split count. The choice is made, in order, from
 //   1. an explicit override (compas_b200_set_*_launch, used by the autotuner while timing),
 //   2. the autotuner's table (COMPAS_B200_TUNING file, one line per shape class:
-//      "fisp <N> <voxel-bucket> <P-bucket> <config> <warps>" or
-//      "pssfp <nz> <voxel-bucket> <config>"), written by compas_b200_autotune.py,
-//   3. the built-in heuristic (fisp_default_launch / pssfp_default_launch).
+//      "fisp <N> <voxel-bucket> <P-bucket> <config> <warps>",
+//      "pssfp <nz> <voxel-bucket> <config>" or
+//      "tc <kind> <readout-bucket> <voxel-bucket> <coil·sample-bucket> <tile> <splits>"), written by
+//      compas_b200_autotune.py,
+//   3. the built-in heuristic (fisp_default_launch / pssfp_default_launch / the plan functions of
+//      the tensor-core launchers).
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -24,11 +28,18 @@ namespace compas {
 
 namespace {
 std::atomic<int> g_fisp_cfg {-1}, g_fisp_warps {-1}, g_pssfp_cfg {-1}, g_fisp_tangent_cfg {-1};
+constexpr int kTcKinds = int(TcKind::Count);
+std::atomic<int> g_tc_tile[kTcKinds], g_tc_splits[kTcKinds];  // 0 = no override (static: zero-initialised)
 
 struct Table {
     std::map<std::tuple<int, int, int>, std::pair<int, int>> fisp;  // (N, vbucket, pbucket) -> (cfg, warps)
     std::map<std::tuple<int, int>, int> pssfp;                        // (nz, vbucket) -> cfg
+    std::map<std::tuple<int, int, int, int>, std::pair<int, int>> tc;  // (kind, rbucket, vbucket, csbucket) -> (tile, splits)
 };
+
+bool valid_tc_tile(int tile) {
+    return tile == 0 || (tile >= 16 && tile <= 256 && tile % 16 == 0);
+}
 
 int bucket(int64_t n) {  // log2 bucket
     int b = 0;
@@ -57,6 +68,11 @@ const Table& table() {
             } else if (kind == "pssfp") {
                 int nz, vb, cfg;
                 if (s >> nz >> vb >> cfg) t.pssfp[{nz, vb}] = cfg;
+            } else if (kind == "tc") {
+                int k, rb, vb, cb, tile, splits;
+                if (s >> k >> rb >> vb >> cb >> tile >> splits && k >= 0 && k < kTcKinds && valid_tc_tile(tile) &&
+                    splits >= 0)
+                    t.tc[{k, rb, vb, cb}] = {tile, splits};
             }
         }
     });
@@ -124,6 +140,50 @@ PssfpLaunch tuned_pssfp_launch(int nz, int64_t nvoxels) {
         if (pssfp_config_info(it->second, &ZT, &GZ) && ZT * GZ >= nz) return PssfpLaunch {it->second};
     }
     return pssfp_default_launch(nz, nvoxels);
+}
+
+void set_tc_override(int kind, int tile, int splits) {
+    if (kind < 0 || kind >= kTcKinds) COMPAS_ERROR("tensor-core contraction kind out of range");
+    if (!valid_tc_tile(tile)) COMPAS_ERROR("tensor-core readout tile must be 0 or a multiple of 16 in [16, 256]");
+    if (splits < 0) COMPAS_ERROR("tensor-core split count must be 0 (built-in) or positive");
+    g_tc_tile[kind] = tile;
+    g_tc_splits[kind] = splits;
+}
+
+TcTuning tuned_tc(TcKind kind, int R, int64_t nvoxels, int64_t coil_samples) {
+    const int k = int(kind);
+    TcTuning t;
+    t.tile = g_tc_tile[k].load();
+    t.splits = g_tc_splits[k].load();
+    if (t.tile > 0 || t.splits > 0) return t;
+    const auto& tab = table();
+    auto it = tab.tc.find({k, bucket(R), bucket(nvoxels), bucket(coil_samples)});
+    if (it != tab.tc.end()) {
+        t.tile = it->second.first;
+        t.splits = it->second.second;
+    }
+    return t;
+}
+
+TcTuning tc_launch_choice(int device, TcKind kind, int nvoxels, int R, int S, int C) {
+    TcTuning t;
+    switch (kind) {
+    case TcKind::CartesianSignal:
+    case TcKind::CartesianJacobian: {
+        const TcPlan p = tc_plan(device, nvoxels, R, S, C, kind == TcKind::CartesianJacobian);
+        t.tile = p.nr;
+        t.splits = p.splits;
+        break;
+    }
+    case TcKind::CartesianHermitian: t.splits = tc_hermitian_splits(device, nvoxels, R, S, C); break;
+    case TcKind::SpiralSignal:
+    case TcKind::SpiralJacobian:
+        t.splits = tc_spiral_splits(device, nvoxels, R, S, C, kind == TcKind::SpiralJacobian);
+        break;
+    case TcKind::SpiralHermitian: t.splits = tc_spiral_hermitian_splits(device, nvoxels, R, S, C); break;
+    default: COMPAS_ERROR("tensor-core contraction kind out of range");
+    }
+    return t;
 }
 
 }  // namespace compas

@@ -208,6 +208,26 @@ COMPAS_API void compas_b200_fisp_launch_choice(int max_state, int64_t nvoxels, i
                                                int* warps);
 COMPAS_API int compas_b200_pssfp_launch_choice(int nz, int64_t nvoxels);
 
+/* Tensor-core contraction launches (split-BF16 methods): per kind, the readout tile of the
+ * Cartesian signal / J·v kernel (a multiple of 16 in [16, 256]) and the split count (voxel splits
+ * of the signal and J·v kernels, pair-tile splits of the Cartesian Jᴴ·v kernel, readout splits of
+ * the spiral Jᴴ·v kernel). 0 keeps the tuning table's or the built-in choice. A tile that pads the
+ * readout count to more than 17/16 of the rows the built-in tile pads it to is not used (the
+ * built-in tile is the multiple of 16 up to 256 that pads least), and the signal and J·v kernels still
+ * split so that one split accumulates at most 512 K16 steps. Overrides are process-wide and used by
+ * the autotuner while it times candidates. */
+#define COMPAS_B200_TC_CARTESIAN_SIGNAL 0
+#define COMPAS_B200_TC_CARTESIAN_JACOBIAN 1
+#define COMPAS_B200_TC_CARTESIAN_HERMITIAN 2
+#define COMPAS_B200_TC_SPIRAL_SIGNAL 3
+#define COMPAS_B200_TC_SPIRAL_JACOBIAN 4
+#define COMPAS_B200_TC_SPIRAL_HERMITIAN 5
+COMPAS_API void compas_b200_set_tc_launch(int kind, int tile, int splits);
+/* The tile (0 where the kind has none) and split count a call of this shape runs with on `device`
+ * (override, tuning table, or built-in choice). Returns 0, or -1 on a bad kind. */
+COMPAS_API int compas_b200_tc_launch_choice(int kind, int device, int nvoxels, int nreadouts,
+                                            int samples_per_readout, int ncoils, int* tile, int* splits);
+
 /* Batched jobs (no counterpart in the reference): njobs independent simulate -> signal jobs,
  * job i = (parameters[i], sequences[i] (FISP or pSSFP), trajectories[i] (Cartesian, spiral, or
  * NULL for simulate only), coils[i] ([ncoils][nvoxels] complex; NULL without trajectory)),

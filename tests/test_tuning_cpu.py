@@ -72,3 +72,73 @@ def test_tuning_table_is_used(tmp_path):
     assert out["fisp"][1] == base["fisp"][1]
     assert out["pssfp"][0] == pssfp_cfg
     assert out["pssfp"][1] == base["pssfp"][1]
+
+
+TC_PROBE = """
+import json, sys
+sys.path.insert(0, {pkg!r})
+import compas_b200 as cb
+shape = (50176, 1120, 224, 4)  # voxels, readouts, samples per readout, coils
+out = {{k: cb.tc_launch_choice(k, *shape) for k in cb.TC_KINDS}}
+out["ragged"] = cb.tc_launch_choice("cartesian_signal", 50176, 1000, 224, 4)
+cb.set_tc_launch("cartesian_signal", 112, 1)
+out["override_min_splits"] = cb.tc_launch_choice("cartesian_signal", *shape)
+cb.set_tc_launch("cartesian_hermitian", 0, 1000)
+out["override_hermitian"] = cb.tc_launch_choice("cartesian_hermitian", *shape)
+cb.set_tc_launch("spiral_jacobian", 0, 7)
+out["override_spiral"] = cb.tc_launch_choice("spiral_jacobian", 50176, 760, 1000, 8)
+errors = []
+for bad in [("cartesian_signal", 17, 0), ("cartesian_signal", 272, 0), ("cartesian_signal", 0, -1), (6, 0, 0)]:
+    try:
+        cb.set_tc_launch(*bad)
+    except cb.CompasError as e:
+        errors.append(str(e))
+out["errors"] = errors
+print(json.dumps(out))
+"""
+
+
+def _tc_probe(env_extra=None):
+    env = dict(os.environ)
+    env.pop("COMPAS_B200_TUNING", None)
+    env.update(env_extra or {})
+    r = subprocess.run([sys.executable, "-c", TC_PROBE.format(pkg=str(PKG))], capture_output=True, text=True,
+                       env=env, timeout=120)
+    assert r.returncode == 0, r.stderr
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def test_tensor_core_builtin_choice_and_overrides():
+    out = _tc_probe()
+    # Cartesian: the readout tile that pads R least (224 divides 1120); at least ceil(V / 4096)
+    # voxel splits for the signal and ceil(V / 2048) for J·v (≤ 512 K16 steps per split)
+    tile, splits = out["cartesian_signal"]
+    assert tile == 224 and splits >= 13
+    tile, splits = out["cartesian_jacobian"]
+    assert tile == 224 and splits >= 25
+    assert out["ragged"][0] == 144  # 1000 readouts: 7 tiles of 144 (1008 rows) pad least
+    assert out["cartesian_hermitian"][0] == 0 and out["cartesian_hermitian"][1] >= 1
+    assert out["spiral_signal"][1] >= 13 and out["spiral_jacobian"][1] >= 25
+    # a split override below the accuracy bound is raised to it; Jᴴ·v splits are capped at one
+    # split per 64-pair tile (4 coils x 1120 readouts = 70 tiles)
+    assert out["override_min_splits"] == [112, 13]
+    assert out["override_hermitian"] == [0, 70]
+    assert out["override_spiral"] == [0, 25]
+    assert len(out["errors"]) == 4
+
+
+def test_tensor_core_tuning_table_is_used(tmp_path):
+    base = _tc_probe()
+    table = tmp_path / "tuning.txt"
+    # kind 0 (Cartesian signal), log2 1120 = 10, log2 50176 = 15, log2 (4 x 224) = 9
+    table.write_text("tc 0 10 15 9 160 20\n"
+                     "tc 1 10 15 9 240 30\n"    # 240 pads 1120 readouts to 1200 > 17/16 x 1120: built-in tile
+                     "tc 2 10 15 9 0 5\n"
+                     "tc 0 10 15 9 17 4\n"      # invalid tile: the line is ignored (the first stays)
+                     "tc 9 10 15 9 0 4\n")      # unknown kind: ignored
+    out = _tc_probe({"COMPAS_B200_TUNING": str(table)})
+    assert out["cartesian_signal"] == [160, 20]
+    assert out["cartesian_jacobian"] == [224, 30]
+    assert out["cartesian_hermitian"] == [0, 5]
+    assert out["spiral_signal"] == base["spiral_signal"]
+    assert out["ragged"] == base["ragged"]  # 1000 readouts: log2 class 9, no line
