@@ -225,8 +225,11 @@ def main(argv=None):
             for nv in tc_voxels:
                 res, default, dms = tune_tc(ctx, kind, nv, R, S, C, reps=reps)
                 ms, tile, sp = res[0]
-                lines["tc"].append(f"tc {cb.TC_KINDS[kind]} {int(math.log2(R))} {int(math.log2(nv))} "
-                                   f"{int(math.log2(C * S))} {tile} {sp}")
+                # a line only where the search beats the built-in choice by more than 2 %: a table
+                # line applies to a whole class of shapes, the built-in plan to the exact one
+                if dms > 1.02 * ms:
+                    lines["tc"].append(f"tc {cb.TC_KINDS[kind]} {int(math.log2(R))} {int(math.log2(nv))} "
+                                       f"{int(math.log2(C * S))} {tile} {sp}")
                 report["tc"].append(f"# tc {kind} R={R} S={S} C={C} V={nv}: best (tile {tile}, splits {sp}) "
                                     f"{ms:.3f} ms; built-in (tile {default[0]}, splits {default[1]}) {dms:.3f} ms "
                                     f"({len(res)} candidates)")

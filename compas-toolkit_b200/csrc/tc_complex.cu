@@ -25,12 +25,15 @@
 //               group of TC_PPG pairs); a group starts from the exact E_k table value × coil·w and
 //               steps along k with the complex recurrence. Afterwards they drain the TMEM
 //               accumulator through shared memory into coalesced rows of the output;
-//   warp 16     allocates 256 TMEM columns (both CTAs); in the leader one lane issues the 12 MMAs
+//   warp 16     allocates 512 TMEM columns (both CTAs); in the leader one lane issues the 12 MMAs
 //               per stage, in the peer one lane tells the leader when its streamed half has landed;
 //   warp 17     one lane loads each stage's half readout tile (hi and lo planes) by bulk copies.
 // Stages hand over through mbarriers (full, in the leader: producers of both CTAs → MMA; afull:
-// copy landed; empty, in both: tcgen05.commit multicast → producers and copy). The voxel range is
-// split over CTA pairs (split-K); partial tiles are summed in a fixed order. Every wait is bounded.
+// copy landed; empty, in both: tcgen05.commit multicast → producers and copy). Every 512 K16 steps
+// (128 stages) the producers fold the TMEM accumulator into an FP32 running sum held in the other
+// half of the CTA's 512 TMEM columns, which bounds the tensor core's accumulation error for any
+// voxel count. The voxel range is split over CTA pairs (split-K) only to fill the GPU; partial
+// tiles are summed in a fixed order. Every wait is bounded.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -59,6 +62,10 @@ constexpr int TC_A_BYTES = TC_M * TC_K * 2;         // 16 KB slot per hi/lo plan
 constexpr int TC_BH_BYTES = (TC_N / 2) * TC_K * 2;  // 16 KB per hi/lo plane: this CTA's 128 generated rows
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_BH_BYTES;
 constexpr int TC_SMEM = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 128 /*barriers*/;
+// TMEM of a CTA: the MMA accumulator (columns 0 .. nr-1) and the running FP32 sum of the finished
+// accumulation chunks (columns TC_SUM_COL ..); a chunk is TC_CHUNK_STAGES stages = 512 K16 steps
+constexpr int TC_TMEM_COLS = 512, TC_SUM_COL = 256;
+constexpr int TC_CHUNK_STAGES = 128;
 static_assert(TC_PAIRS / 2 == (TC_B_THREADS / 16) * TC_PPG, "a CTA's producer groups cover half the pair tile");
 static_assert((TC_PAIRS / 2) * (2 * 256 + 2) * 4 <= TC_STAGES * TC_STAGE_BYTES, "output tile fits the stage buffers");
 
@@ -189,7 +196,9 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
     uint64_t* empty = full + TC_STAGES;
     uint64_t* afull = empty + TC_STAGES;  // the stage's A bulk copy has landed
     uint64_t* done = afull + TC_STAGES;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    uint64_t* cdone = done + 1;    // an accumulation chunk's MMAs have completed (both CTAs)
+    uint64_t* drained = cdone + 1;  // (leader) both CTAs folded the accumulator into the running sum
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -208,10 +217,12 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
             tc::mbar_init(&afull[s], 1);
         }
         tc::mbar_init(done, 1);
+        tc::mbar_init(cdone, 1);
+        tc::mbar_init(drained, 2 * TC_B_THREADS);
         *abort_flag = 0;
         tc::fence_mbarrier_init();
     }
-    if (warp == TC_MMA_WARP) tc::tmem_alloc_pair(tmem_slot, 256);
+    if (warp == TC_MMA_WARP) tc::tmem_alloc_pair(tmem_slot, TC_TMEM_COLS);
     tc::tc_fence_before();
     __syncthreads();
     tc::cluster_sync();  // both CTAs' barriers exist before either arrives on the other's
@@ -247,6 +258,14 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
             const uint32_t idesc = tc::idesc_bf16_f32(2 * TC_M, a.nr);
             for (int it = 0; it < nstages; it++) {
                 const int buf = it % TC_STAGES;
+                if (it > 0 && it % TC_CHUNK_STAGES == 0) {
+                    // end of an accumulation chunk: once its MMAs complete, the producers of both
+                    // CTAs add the accumulator into the running sum; the next chunk starts from 0
+                    tc::mma_commit_pair(cdone);
+                    if (!tc::mbar_wait(drained, ((it / TC_CHUNK_STAGES) - 1) & 1, a.status)) *abort_flag = 1;
+                    if (*(volatile int*)abort_flag) break;
+                    tc::tc_fence_after();
+                }
                 if (!tc::mbar_wait(&full[buf], (it / TC_STAGES) & 1, a.status)) *abort_flag = 1;
                 if (!tc::mbar_wait(&afull[buf], (it / TC_STAGES) & 1, a.status)) *abort_flag = 1;
                 if (*(volatile int*)abort_flag) break;
@@ -260,7 +279,7 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
                     const uint32_t koff = ks * 32;  // 16 bf16 = 32 bytes along K inside the swizzle atom
                     const uint64_t dah = tc::sw128_kmajor_desc(ah + koff), dal = tc::sw128_kmajor_desc(al + koff);
                     const uint64_t dbh = tc::sw128_kmajor_desc(bh + koff), dbl = tc::sw128_kmajor_desc(bl + koff);
-                    tc::mma_bf16_pair(tmem, dah, dbh, idesc, (it > 0 || ks > 0) ? 1u : 0u);
+                    tc::mma_bf16_pair(tmem, dah, dbh, idesc, (it % TC_CHUNK_STAGES > 0 || ks > 0) ? 1u : 0u);
                     tc::mma_bf16_pair(tmem, dah, dbl, idesc, 1u);
                     tc::mma_bf16_pair(tmem, dal, dbh, idesc, 1u);
                 }
@@ -308,13 +327,47 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
                 }
             }
         };
+        // TMEM lanes of this warp's quarter; warp w handles the 32-column chunks w/4, w/4 + 4, ...
+        const uint32_t tmem_rows = tmem + (uint32_t((warp & 3) * 32) << 16);
         load_gen(0, step, e0, cw);
         for (int it = 0; it < nstages; it++) {
             const int buf = it % TC_STAGES;
             const int vbase = v_begin + it * VPS + VPH * hq;
+            if (it > 0 && it % TC_CHUNK_STAGES == 0) {
+                // fold the finished chunk into the running sum (FP32, round to nearest): the
+                // accumulation error of the tensor core grows with the accumulated K, so no chunk
+                // accumulates more than 512 K16 steps
+                const int chunk = it / TC_CHUNK_STAGES;
+                const bool waited = tc::mbar_wait(cdone, (chunk - 1) & 1, a.status);
+                // one decision per warp (tcgen05.ld / st are warp-collective); the warp's lanes stay
+                // together because every exit from this loop is decided per warp
+                if (__any_sync(0xffffffffu, !waited || *(volatile int*)abort_flag)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                tc::tc_fence_after();
+#pragma unroll 1
+                for (int col = (warp >> 2) * 32; col < a.nr; col += (col & 16) ? 112 : 16) {
+                    // 16-column halves of the warp's 32-column chunks (w/4, w/4 + 4, ...)
+                    float acc[16];
+                    tc::tmem_load16(tmem_rows + uint32_t(col), acc);
+                    if (chunk > 1) {
+                        float sum[16];
+                        tc::tmem_load16(tmem_rows + uint32_t(TC_SUM_COL + col), sum);
+#pragma unroll
+                        for (int i = 0; i < 16; i++) acc[i] += sum[i];
+                    }
+                    tc::tmem_store16(tmem_rows + uint32_t(TC_SUM_COL + col), acc);
+                }
+                tc::tc_fence_before();
+                tc::mbar_arrive_cluster(drained, 0);
+            }
             if (it + 1 < nstages) load_gen(it + 1, step_n, e0_n, cw_n);
-            if (!tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status)) *abort_flag = 1;
-            if (*(volatile int*)abort_flag) break;
+            const bool freed = tc::mbar_wait(&empty[buf], ((it / TC_STAGES) & 1) ^ 1, a.status);
+            if (__any_sync(0xffffffffu, !freed || *(volatile int*)abort_flag)) {
+                *abort_flag = 1;
+                break;
+            }
             unsigned char* Bh = smem + buf * TC_STAGE_BYTES + 2 * TC_A_BYTES;
             unsigned char* Bl = Bh + TC_BH_BYTES;
             float2 G[VPH];
@@ -391,10 +444,20 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
             const int TP = 2 * a.nr + 2;                // row pitch (floats): conflict-free columns
             const int quarter = warp & 3;
             const int row = quarter * 32 + lane, jr = row >> 1, ri = row & 1;
+            const bool chunked = nstages > TC_CHUNK_STAGES;  // earlier chunks are in the running sum
 #pragma unroll 1
             for (int ch = warp >> 2; ch * 32 < a.nr; ch += 4) {
                 float v[32];
-                tc::tmem_load32(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(ch * 32), v);
+                tc::tmem_load32(tmem_rows + uint32_t(ch * 32), v);
+                if (chunked) {
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        float sum[16];
+                        tc::tmem_load16(tmem_rows + uint32_t(TC_SUM_COL + ch * 32 + 16 * h), sum);
+#pragma unroll
+                        for (int i = 0; i < 16; i++) v[16 * h + i] += sum[i];
+                    }
+                }
 #pragma unroll
                 for (int i = 0; i < 32; i++)
                     if (ch * 32 + i < a.nr) T[jr * TP + 2 * (ch * 32 + i) + ri] = v[i];
@@ -427,7 +490,7 @@ __device__ __forceinline__ void tc_tile(const TcArgs& a, const int bx, const int
     tc::cluster_sync();  // neither CTA leaves while the other may still signal it or read TMEM
     if (warp == TC_MMA_WARP) {
         tc::tc_fence_after();
-        tc::tmem_dealloc_pair(tmem, 256);
+        tc::tmem_dealloc_pair(tmem, TC_TMEM_COLS);
     }
 }
 
@@ -551,8 +614,12 @@ TcPlan tc_plan(int device, int nvoxels, int R, int S, int C, bool jac) {
         // tuned: at most 64 splits and at least one voxel stage each
         splits = std::min({tuning.splits, 64, std::max(1, div_ceil(std::max(nvoxels, 1), vps))});
     } else {
-        // split the voxel range over CTAs: pick the split count (≥ 16 stages per split) whose grid
-        // leaves the least idle SM time in the last wave of one CTA per SM
+        // split the voxel range over CTAs only to fill the GPU: pick the split count (≥ 16 stages
+        // per split) whose grid leaves the least idle SM time in the last wave of one CTA per SM,
+        // less 0.5 % per split for the partial tiles written and summed. (Accuracy needs no split:
+        // the tensor core's FP32 accumulation error grows with the accumulated K, ~2e-4 relative
+        // after 3750 K16 steps, measured, so each CTA folds its accumulator into an FP32 running sum
+        // every 512 K16 steps.)
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         const int max_splits = std::max(1, std::min(64, nvoxels / (16 * vps)));
@@ -560,18 +627,13 @@ TcPlan tc_plan(int device, int nvoxels, int R, int S, int C, bool jac) {
         for (int sp = 1; sp <= max_splits; sp++) {
             const int64_t ctas = int64_t(tiles) * sp;
             const int64_t waves = (ctas + sms - 1) / sms;
-            const double eff = double(ctas) / double(waves * sms) - 0.002 * sp;  // mild preference for fewer partials
+            const double eff = double(ctas) / double(waves * sms) - 0.005 * sp;
             if (eff > best + 1e-9) {
                 best = eff;
                 splits = sp;
             }
         }
     }
-    // The tensor core's FP32 accumulation loses a little precision per MMA (relative error grows
-    // with the accumulated K: ~2e-4 after 3750 K16 steps, measured), so one split accumulates at
-    // most 512 K16 steps (4096 voxels of the signal, 2048 of J·v); splits add in FP32 afterwards.
-    const int max_voxels = jac ? 2048 : 4096;
-    splits = std::max(splits, div_ceil(std::max(nvoxels, 1), max_voxels));
     p.vchunk = std::max(vps, div_ceil(div_ceil(std::max(nvoxels, 1), splits), vps) * vps);
     p.splits = std::max(1, div_ceil(nvoxels, p.vchunk));
     p.ctas = int64_t(tiles) * p.splits;

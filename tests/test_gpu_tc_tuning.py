@@ -3,9 +3,11 @@
 The readout tile of the Cartesian signal / J·v kernel and the split count of every contraction
 change only how the work is distributed over CTAs and the FP32 order in which split partial sums
 are added. Every accepted (tile, splits) must therefore meet the split-BF16 tolerance (relative L2
-1e-4) against the FP64 oracle. Cases: 9000 voxels (at least 3 voxel splits for the signal and 5 for
-J·v, from the 512-K16-step accumulation bound), Cartesian 480 readouts x 45 samples (readout tiles
-48, 96, 160 and 240 all cover 480 rows exactly), spiral 70 interleaves x 150 samples, 3 coils.
+1e-4) against the FP64 oracle. Cases: 9000 voxels, Cartesian 480 readouts x 45 samples (readout
+tiles 48, 96, 160 and 240 all cover 480 rows exactly; one split accumulates 282 stages of the signal
+or 563 of J·v, i.e. folds its TMEM accumulator into the running sum 2 or 4 times), spiral 70
+interleaves x 150 samples (at least 3 voxel splits for the signal and 5 for J·v, from the
+512-K16-step accumulation bound of that kernel), 3 coils.
 """
 import numpy as np
 import pytest
@@ -99,12 +101,12 @@ def _pick(case, kind, got):
     return got[ent[:, 0], ent[:, 1], ent[:, 2]]
 
 
-# (kind, [(tile, splits), ...]): splits at the accuracy minimum, in between and near the cap of 64
+# (kind, [(tile, splits), ...]): one split or the accuracy minimum, in between, and near the cap of 64
 # (57 and 63 are the counts that 64 requested splits round to at 9000 voxels: whole voxel stages of
 # 32 (signal) or 16 (J·v) voxels per split, every split non-empty)
 LAUNCHES = [
-    ("cartesian_signal", [(48, 3), (96, 7), (160, 57), (240, 5)]),
-    ("cartesian_jacobian", [(48, 5), (160, 11), (240, 63)]),
+    ("cartesian_signal", [(48, 1), (96, 7), (160, 57), (240, 2)]),
+    ("cartesian_jacobian", [(48, 1), (160, 11), (240, 63), (96, 3)]),
     ("cartesian_hermitian", [(0, 1), (0, 5), (0, 23)]),  # 3 coils x 480 readouts = 23 tiles of 64 pairs
     ("spiral_signal", [(0, 3), (0, 10), (0, 57)]),
     ("spiral_jacobian", [(0, 5), (0, 13), (0, 63)]),
