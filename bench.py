@@ -402,6 +402,8 @@ def main():
                       "l2": "working set > L2 (echo array 450 MB per step)", "seed": 2},
            "gpu_launches": launches, "clocks": clocks, "roofline": roofline, "roofline_signal": roofline_signal,
            "stage_ms": {"simulate_fisp": sim_ms, "signal_cartesian": sig_ms},
+           "stage_ms_per_step": {"simulate_fisp": [round(e[0].elapsed_time(e[1]), 3) for e in evs],
+                                 "signal_cartesian": [round(e[1].elapsed_time(e[2]), 3) for e in evs]},
            "signal_tflops": sig_tf, "peaks": peak_kind}
 
     single = world == 1

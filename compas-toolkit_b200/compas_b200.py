@@ -79,6 +79,7 @@ _SIGS = {
     "compas_b200_fisp_config_packed": ([_I], _I),
     "compas_b200_pssfp_config_count": ([], _I),
     "compas_b200_pssfp_config_info": ([_I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
+    "compas_b200_pssfp_config_packed": ([_I], _I),
     "compas_b200_fisp_launch_choice": ([_I, _I64, _I, C.POINTER(C.c_int), C.POINTER(C.c_int)], None),
     "compas_b200_pssfp_launch_choice": ([_I, _I64], _I),
     "compas_b200_set_tc_launch": ([_I, _I, _I], None),
@@ -851,6 +852,11 @@ def fisp_configs() -> list:
 def fisp_config_packed(index: int) -> bool:
     """Whether FISP layout `index` is packed (two states per two-wide FP32 instruction)."""
     return bool(library().compas_b200_fisp_config_packed(int(index)))
+
+
+def pssfp_config_packed(index: int) -> bool:
+    """Whether pSSFP layout `index` is packed (two isochromats per two-wide FP32 instruction)."""
+    return bool(library().compas_b200_pssfp_config_packed(int(index)))
 
 
 def fisp_launch_choice(max_state: int, nvoxels: int, npositions: int) -> tuple:

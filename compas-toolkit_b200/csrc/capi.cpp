@@ -708,6 +708,10 @@ int compas_b200_pssfp_config_info(int index, int* iso_per_lane, int* lanes) {
     return compas::pssfp_config_info(index, iso_per_lane, lanes) ? 1 : 0;
 }
 
+int compas_b200_pssfp_config_packed(int index) {
+    return compas::pssfp_config_packed(index) ? 1 : 0;
+}
+
 void compas_b200_fisp_launch_choice(int max_state, int64_t nvoxels, int npositions, int* config, int* warps) {
     compas::FispLaunch L = compas::tuned_fisp_launch(max_state, nvoxels, npositions);
     if (L.config < 0) L = compas::fisp_default_launch(max_state, nvoxels, npositions);

@@ -55,6 +55,7 @@ struct PssfpLaunch {
 };
 int pssfp_config_count();
 bool pssfp_config_info(int index, int* ZT, int* GZ);
+bool pssfp_config_packed(int index);  // two-wide layout: ZT/2 pairs of isochromats per lane
 PssfpLaunch pssfp_default_launch(int nz, int64_t nvoxels);
 PssfpLaunch tuned_pssfp_launch(int nz, int64_t nvoxels);
 void launch_pssfp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,

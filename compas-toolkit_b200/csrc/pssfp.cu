@@ -17,6 +17,9 @@
 // 1/n!) for θ ≤ 0.5 rad, accurate to 1.1e-8 relative, and cos θ = 1 - θ²·(1-cos θ)/θ², so the hot loop runs on
 // the FMA pipe; larger angles use sqrt/sincos. The relaxation after each RF sample is folded into
 // the rotation (E2 scales its coefficients, E1 enters as E1/E2 on the longitudinal result).
+// The two-wide layouts (pssfp_tile_packed) hold the isochromats of a lane in pairs and run every
+// operation as one sm_100 two-wide FP32 instruction per pair, which halves the issue slots of the
+// (issue-bound) scalar update; they are the default for 3 or more z positions.
 #include "common.cuh"
 #include "compas/compas.h"
 #include "job_args.cuh"
@@ -40,8 +43,9 @@ struct Iso {
     float x, y, z;
 };
 
-// Per-voxel constants of rotate_relax: the Taylor coefficients of sin θ/θ and (1-cos θ)/θ² (1/n!)
-// times E2, E2 itself, E1/E2 and 1 - E1.
+// Per-voxel constants of rotate_relax: the Taylor coefficients of sin θ/θ and (1-cos θ)/θ² times
+// E2 (magnitudes E2/(2n+1)! and E2/(2n+2)!; the series alternate in θ² and are evaluated in
+// y = -θ², where every term is positive), E2 itself, E1/E2 and 1 - E1.
 struct RotRelax {
     float s0, s1, s2, s3, h0, h1, h2, h3, E2, r, oneE1;
 };
@@ -49,52 +53,69 @@ struct RotRelax {
 __device__ __forceinline__ RotRelax make_rot_relax(float E1, float E2) {
     RotRelax k;
     k.s0 = E2;
-    k.s1 = E2 * (-1.0f / 6.0f);
+    k.s1 = E2 * (1.0f / 6.0f);
     k.s2 = E2 * (1.0f / 120.0f);
-    k.s3 = E2 * (-1.0f / 5040.0f);
+    k.s3 = E2 * (1.0f / 5040.0f);
     k.h0 = E2 * 0.5f;
-    k.h1 = E2 * (-1.0f / 24.0f);
+    k.h1 = E2 * (1.0f / 24.0f);
     k.h2 = E2 * (1.0f / 720.0f);
-    k.h3 = E2 * (-1.0f / 40320.0f);
+    k.h3 = E2 * (1.0f / 40320.0f);
     k.E2 = E2;
     k.r = E1 / E2;
     k.oneE1 = 1.0f - E1;
     return k;
 }
 
-// E2-scaled rotation coefficients for θ² = t2: E2·cos θ, E2·sin θ/θ, E2·(1-cos θ)/θ²
+// E2-scaled rotation coefficients for θ² = -y: E2·cos θ, E2·sin θ/θ, E2·(1-cos θ)/θ²
 struct RotCoefs {
     float c, s, h;
 };
 
-__device__ __forceinline__ RotCoefs rot_coefs(float t2, const RotRelax& k) {
+constexpr float kTaylorMax = 0.25f;  // largest θ² of the Taylor branch
+
+// Taylor series in θ² through the cubic term (the next terms, θ⁸/9! and θ⁸/10!, are below 1.1e-8
+// relative for θ² ≤ 0.25, under FP32 resolution) by Horner in y = -θ², and cos θ = 1 + y·h.
+__device__ __forceinline__ RotCoefs rot_coefs_taylor(float y, const RotRelax& k) {
     RotCoefs q;
-    if (t2 <= 0.25f) {
-        // Taylor series in x = θ² through x³ (the next terms, x⁴/9! and x⁴/10!, are below 1.1e-8
-        // relative for x ≤ 0.25, under FP32 resolution), cos θ = 1 - x·(1-cos θ)/θ²
-        const float x = t2;
-        q.s = fmaf(x, fmaf(x, fmaf(x, k.s3, k.s2), k.s1), k.s0);
-        q.h = fmaf(x, fmaf(x, fmaf(x, k.h3, k.h2), k.h1), k.h0);
-        q.c = fmaf(-x, q.h, k.E2);
-    } else {
-        const float th = sqrtf(t2);
-        float sn, cs;
-        sincosf(th, &sn, &cs);
-        q.c = k.E2 * cs;
-        q.s = k.E2 * (sn / th);
-        q.h = k.E2 * ((1.0f - cs) / t2);
-    }
+    q.s = fmaf(y, fmaf(y, fmaf(y, k.s3, k.s2), k.s1), k.s0);
+    q.h = fmaf(y, fmaf(y, fmaf(y, k.h3, k.h2), k.h1), k.h0);
+    q.c = fmaf(y, q.h, k.E2);
     return q;
+}
+
+__device__ __forceinline__ RotCoefs rot_coefs(float y, const RotRelax& k) {
+    if (y >= -kTaylorMax) return rot_coefs_taylor(y, k);
+    RotCoefs q;
+    const float t2 = -y;
+    const float th = sqrtf(t2);
+    float sn, cs;
+    sincosf(th, &sn, &cs);
+    q.c = k.E2 * cs;
+    q.s = k.E2 * (sn / th);
+    q.h = k.E2 * ((1.0f - cs) / t2);
+    return q;
+}
+
+// z component of the excitation axis of the isochromat at z (slice gradient and off-resonance
+// during an RF sample), and the precession angle over the prephasing interval with `g` times the
+// prephasing gradient
+__device__ __forceinline__ float excite_az(const PssfpArgs& a, float z, float B0) {
+    return -(a.gz_ex * z) - a.dt_ex * 6.28318530717958647692f * B0;
+}
+__device__ __forceinline__ float precess_angle(const PssfpArgs& a, float g, float z, float B0) {
+    return -(g * a.gz_pr * z) - a.dt_pr * 6.28318530717958647692f * B0;
 }
 
 // rotation about the unnormalised axis (ax, ay, az) by |a|   (isochromat.cuh:14-73), followed by
 // relaxation: transverse components times E2, longitudinal z·E1 + 1 - E1. E2 is folded into the
-// rotation coefficients and E1 enters as E1/E2 on the E2-scaled longitudinal result.
+// rotation coefficients and E1 enters as E1/E2 on the E2-scaled longitudinal result. Every
+// operation is written out (no contraction left to the compiler), in the form the packed update
+// repeats on pairs of isochromats, so both give the same bits.
 __device__ __forceinline__ void rotate_relax(Iso& m, float ax, float ay, float az, const RotCoefs& q,
                                              const RotRelax& k) {
-    const float cx = ay * m.z - az * m.y;
-    const float cy = az * m.x - ax * m.z;
-    const float cz = ax * m.y - ay * m.x;
+    const float cx = fmaf(ay, m.z, (-az) * m.y);
+    const float cy = fmaf(az, m.x, (-ax) * m.z);
+    const float cz = fmaf(ax, m.y, (-ay) * m.x);
     const float hd = q.h * fmaf(ax, m.x, fmaf(ay, m.y, az * m.z));
     m.x = fmaf(q.c, m.x, fmaf(q.s, cx, hd * ax));
     m.y = fmaf(q.c, m.y, fmaf(q.s, cy, hd * ay));
@@ -105,9 +126,9 @@ __device__ __forceinline__ void rotate_relax(Iso& m, float ax, float ay, float a
 // the explicit derivative (px, py, pz) of the step at the current state.
 __device__ __forceinline__ void rotate_relax_tangent(Iso& d, float ax, float ay, float az, const RotCoefs& q,
                                                      const RotRelax& k, float px, float py, float pz) {
-    const float cx = ay * d.z - az * d.y;
-    const float cy = az * d.x - ax * d.z;
-    const float cz = ax * d.y - ay * d.x;
+    const float cx = fmaf(ay, d.z, (-az) * d.y);
+    const float cy = fmaf(az, d.x, (-ax) * d.z);
+    const float cz = fmaf(ax, d.y, (-ay) * d.x);
     const float hd = q.h * fmaf(ax, d.x, fmaf(ay, d.y, az * d.z));
     d.x = fmaf(q.c, d.x, fmaf(q.s, cx, fmaf(hd, ax, px)));
     d.y = fmaf(q.c, d.y, fmaf(q.s, cy, fmaf(hd, ay, py)));
@@ -136,7 +157,6 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
     const float E1_ex = expf(-a.dt_ex * R1), E2_ex = expf(-a.dt_ex * R2);
     const float E1_pr = expf(-a.dt_pr * R1), E2_pr = expf(-a.dt_pr * R2);
     const float E1_inv = expf(-a.dt_inv * R1), E2_inv = expf(-a.dt_inv * R2);
-    const float twopi = 6.28318530717958647692f;
     // tangent factors t/T1², t/T2² of each relaxation interval
     const float s1_ex = a.dt_ex * R1 * R1, s2_ex = a.dt_ex * R2 * R2;
     const float s1_pr = a.dt_pr * R1 * R1, s2_pr = a.dt_pr * R2 * R2;
@@ -152,11 +172,11 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
         const int zi = sub * ZT + k;
         valid[k] = zi < a.nz;
         const float z = valid[k] ? a.z[zi] : 0.0f;
-        az[k] = -(a.gz_ex * z) - a.dt_ex * twopi * B0;
-        sincosf(-(a.gz_pr * z) - a.dt_pr * twopi * B0, &spr[k], &cpr[k]);
+        az[k] = excite_az(a, z, B0);
+        sincosf(precess_angle(a, 1.0f, z, B0), &spr[k], &cpr[k]);
         m[k].x = 0.0f;
         m[k].y = 0.0f;
-        m[k].z = cinv * E1_inv + (1.0f - E1_inv);
+        m[k].z = fmaf(cinv, E1_inv, 1.0f - E1_inv);
         (void)E2_inv;
         if constexpr (TAN) {
             d1[k] = Iso {0.0f, 0.0f, s1_inv * (m[k].z - 1.0f)};
@@ -170,10 +190,10 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
         for (int i = 0; i < a.nRF; i++) {
             const float2 zp = __ldg(zr + i);
             const float ax = zp.x * B1, ay = -zp.y * B1;
-            const float axy2 = fmaf(ax, ax, ay * ay);
+            const float naxy2 = -fmaf(ax, ax, ay * ay);
 #pragma unroll
             for (int k = 0; k < ZT; k++) {
-                const RotCoefs q = rot_coefs(fmaf(az[k], az[k], axy2), rr);
+                const RotCoefs q = rot_coefs(fmaf(-az[k], az[k], naxy2), rr);
                 rotate_relax(m[k], ax, ay, az[k], q, rr);
                 if constexpr (TAN) {
                     rotate_relax_tangent(d1[k], ax, ay, az[k], q, rr, 0.0f, 0.0f, s1_ex * (m[k].z - 1.0f));
@@ -185,8 +205,8 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
     // free precession by the angle (c, s) and relaxation over dt_pr
     auto precess_by = [&](int k, float c, float s) {
         const float x = m[k].x, y = m[k].y;
-        m[k].x = E2_pr * (c * x - s * y);
-        m[k].y = E2_pr * (c * y + s * x);
+        m[k].x = E2_pr * fmaf(c, x, (-s) * y);
+        m[k].y = E2_pr * fmaf(c, y, s * x);
         m[k].z = fmaf(m[k].z, E1_pr, 1.0f - E1_pr);
         if constexpr (TAN) {
             const float x1 = d1[k].x, y1 = d1[k].y, x2 = d2[k].x, y2 = d2[k].y;
@@ -210,7 +230,7 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
         const int zi = sub * ZT + k;
         const float z = valid[k] ? a.z[zi] : 0.0f;
         float s2, c2;
-        sincosf(-(2.0f * a.gz_pr * z) - a.dt_pr * twopi * B0, &s2, &c2);
+        sincosf(precess_angle(a, 2.0f, z, B0), &s2, &c2);
         precess_by(k, c2, s2);
     }
 
@@ -259,10 +279,143 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
     }
 }
 
-template<int ZT, int GZ>
+
+// Two-wide form of pssfp_tile (value only): a lane holds 2·ZP isochromats as ZP pairs, slot p in the
+// low and slot p + ZP in the high half of one register pair per component, and every operation of
+// the rotation, relaxation and precession is one sm_100 two-wide FP32 instruction on a pair, with
+// the RF sample's axis (ax, ay) and the per-voxel coefficients broadcast to both halves. The
+// operations are those of the scalar update in the same order, and the z sum runs over the slots in
+// the scalar order, so layout (ZP pairs, GZ lanes) gives the same bits as the scalar (2·ZP, GZ).
+template<int ZP, int GZ>
+__device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int tile) {
+    constexpr int ZT = 2 * ZP;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane % GZ;
+    const int vloc = (tile * blockDim.x + threadIdx.x) / GZ;
+    const bool vok = vloc < a.nvoxels;
+    const int64_t vcol = a.voxel_begin + (vok ? vloc : a.nvoxels - 1);
+    const float T1 = a.params[0 * a.param_stride + vcol];
+    const float T2 = a.params[1 * a.param_stride + vcol];
+    const float B1 = a.params[2 * a.param_stride + vcol];
+    const float B0 = a.params[3 * a.param_stride + vcol];
+    const float R1 = 1.0f / T1, R2 = 1.0f / T2;
+    const float E1_ex = expf(-a.dt_ex * R1), E2_ex = expf(-a.dt_ex * R2);
+    const float E1_pr = expf(-a.dt_pr * R1), E2_pr = expf(-a.dt_pr * R2);
+    const float E1_inv = expf(-a.dt_inv * R1);
+
+    float2 mx[ZP], my[ZP], mz[ZP];      // the isochromats' magnetisation
+    float2 az[ZP], naz[ZP];             // excitation axis z component and its negation
+    float2 cpr[ZP], spr[ZP], nspr[ZP];  // precession over the prephasing interval
+    bool valid[ZT];
+    const float cinv = cospif(B1);
+    const float mz0 = fmaf(cinv, E1_inv, 1.0f - E1_inv);
+#pragma unroll
+    for (int p = 0; p < ZP; p++) {
+        float zaz[2], zc[2], zs[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int k = p + h * ZP, zi = sub * ZT + k;
+            valid[k] = zi < a.nz;
+            const float z = valid[k] ? a.z[zi] : 0.0f;
+            zaz[h] = excite_az(a, z, B0);
+            sincosf(precess_angle(a, 1.0f, z, B0), &zs[h], &zc[h]);
+        }
+        az[p] = make_float2(zaz[0], zaz[1]);
+        naz[p] = make_float2(-zaz[0], -zaz[1]);
+        cpr[p] = make_float2(zc[0], zc[1]);
+        spr[p] = make_float2(zs[0], zs[1]);
+        nspr[p] = make_float2(-zs[0], -zs[1]);
+        mx[p] = my[p] = bcast2(0.0f);
+        mz[p] = bcast2(mz0);
+    }
+
+    const RotRelax rr = make_rot_relax(E1_ex, E2_ex);
+    const float2 S0 = bcast2(rr.s0), S1 = bcast2(rr.s1), S2 = bcast2(rr.s2), S3 = bcast2(rr.s3);
+    const float2 H0 = bcast2(rr.h0), H1 = bcast2(rr.h1), H2 = bcast2(rr.h2), H3 = bcast2(rr.h3);
+    const float2 E2X = bcast2(rr.E2), RX = bcast2(rr.r), ONE_E1X = bcast2(rr.oneE1);
+    auto excite = [&](int row) {
+        const float2* zr = a.zap + int64_t(row) * a.nRF;
+        for (int i = 0; i < a.nRF; i++) {
+            const float2 zp = __ldg(zr + i);
+            const float ax = zp.x * B1, ay = -zp.y * B1;
+            const float naxy2 = -fmaf(ax, ax, ay * ay);
+            const float2 AX = bcast2(ax), AY = bcast2(ay), NAX = bcast2(-ax), NAY = bcast2(-ay);
+            const float2 NAXY2 = bcast2(naxy2);
+#pragma unroll
+            for (int p = 0; p < ZP; p++) {
+                const float2 y = fma2(naz[p], az[p], NAXY2);  // -θ² of both isochromats
+                float2 c, sn, h;
+                if (y.x >= -kTaylorMax && y.y >= -kTaylorMax) {
+                    sn = fma2(y, fma2(y, fma2(y, S3, S2), S1), S0);
+                    h = fma2(y, fma2(y, fma2(y, H3, H2), H1), H0);
+                    c = fma2(y, h, E2X);
+                } else {
+                    const RotCoefs q0 = rot_coefs(y.x, rr), q1 = rot_coefs(y.y, rr);
+                    c = make_float2(q0.c, q1.c);
+                    sn = make_float2(q0.s, q1.s);
+                    h = make_float2(q0.h, q1.h);
+                }
+                const float2 cx = fma2(AY, mz[p], mul2(naz[p], my[p]));
+                const float2 cy = fma2(az[p], mx[p], mul2(NAX, mz[p]));
+                const float2 cz = fma2(AX, my[p], mul2(NAY, mx[p]));
+                const float2 hd = mul2(h, fma2(AX, mx[p], fma2(AY, my[p], mul2(az[p], mz[p]))));
+                mx[p] = fma2(c, mx[p], fma2(sn, cx, mul2(hd, AX)));
+                my[p] = fma2(c, my[p], fma2(sn, cy, mul2(hd, AY)));
+                mz[p] = fma2(RX, fma2(c, mz[p], fma2(sn, cz, mul2(hd, az[p]))), ONE_E1X);
+            }
+        }
+    };
+    const float2 E2P = bcast2(E2_pr), E1P = bcast2(E1_pr), ONE_E1P = bcast2(1.0f - E1_pr);
+    auto precess_by = [&](int p, float2 c, float2 sn, float2 nsn) {
+        const float2 x = mx[p], y = my[p];
+        mx[p] = mul2(E2P, fma2(c, x, mul2(nsn, y)));
+        my[p] = mul2(E2P, fma2(c, y, mul2(sn, x)));
+        mz[p] = fma2(mz[p], E1P, ONE_E1P);
+    };
+
+    // α/2 pulse, then re- and prephaser with twice the prephasing gradient (pssfp_kernels.cuh:73-80)
+    excite(0);
+#pragma unroll
+    for (int p = 0; p < ZP; p++) {
+        float c2[2], s2[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int zi = sub * ZT + p + h * ZP;
+            const float z = valid[p + h * ZP] ? a.z[zi] : 0.0f;
+            sincosf(precess_angle(a, 2.0f, z, B0), &s2[h], &c2[h]);
+        }
+        precess_by(p, make_float2(c2[0], c2[1]), make_float2(s2[0], s2[1]), make_float2(-s2[0], -s2[1]));
+    }
+
+    for (int t = 0; t < a.nTR; t++) {  // pssfp_kernels.cuh:83-107
+        excite(t + 1);
+#pragma unroll
+        for (int p = 0; p < ZP; p++) precess_by(p, cpr[p], spr[p], nspr[p]);
+        float sx = 0.0f, sy = 0.0f;
+#pragma unroll
+        for (int k = 0; k < ZT; k++) {
+            if (valid[k]) {
+                sx += k < ZP ? mx[k].x : mx[k - ZP].y;
+                sy += k < ZP ? my[k].x : my[k - ZP].y;
+            }
+        }
+#pragma unroll
+        for (int d = GZ / 2; d > 0; d /= 2) {
+            sx += __shfl_xor_sync(0xffffffffu, sx, d, GZ);
+            sy += __shfl_xor_sync(0xffffffffu, sy, d, GZ);
+        }
+        if (sub == 0 && vok) a.echo[int64_t(t) * a.echo_stride + a.voxel_begin + vloc] = make_float2(sx, sy);
+#pragma unroll
+        for (int p = 0; p < ZP; p++) precess_by(p, cpr[p], spr[p], nspr[p]);
+    }
+}
+
+// PACKED: ZT/2 pairs of isochromats per lane in the two-wide layout (pssfp_tile_packed)
+template<int ZT, int GZ, bool PACKED = false>
 __global__ void __launch_bounds__(128) pssfp_kernel(PssfpArgs a) {
     if (a.skip != nullptr && *a.skip != 0) return;  // uniform over the grid
-    pssfp_tile<ZT, GZ>(a, blockIdx.x);
+    if constexpr (PACKED) pssfp_tile_packed<ZT / 2, GZ>(a, blockIdx.x);
+    else pssfp_tile<ZT, GZ>(a, blockIdx.x);
 }
 
 // One pSSFP simulation with its T1 and T2 tangents into a.echo, a.dT1, a.dT2.
@@ -274,7 +427,7 @@ __global__ void __launch_bounds__(128) pssfp_tangent_kernel(PssfpArgs a) {
 // Persistent work-queue kernel for a batch of pSSFP simulations sharing one (ZT, GZ) layout:
 // CTAs of 128 threads take (job, tile) items, longest job first, through an atomic counter.
 // TAN: the value and T1/T2 tangents (pssfp_tangent_kernel's work).
-template<int ZT, int GZ, bool TAN = false>
+template<int ZT, int GZ, bool TAN = false, bool PACKED = false>
 __global__ void __launch_bounds__(128) pssfp_queue_kernel(const PssfpArgs* __restrict__ jobs,
                                                           const int2* __restrict__ items, int nitems,
                                                           int* __restrict__ head) {
@@ -288,7 +441,8 @@ __global__ void __launch_bounds__(128) pssfp_queue_kernel(const PssfpArgs* __res
         const int2 w = items[it];
         if (threadIdx.x == 0) job = jobs[w.x];
         __syncthreads();
-        pssfp_tile<ZT, GZ, TAN>(job, w.y);
+        if constexpr (PACKED) pssfp_tile_packed<ZT / 2, GZ>(job, w.y);
+        else pssfp_tile<ZT, GZ, TAN>(job, w.y);
         __syncthreads();
     }
 }
@@ -304,36 +458,22 @@ struct PssfpConfig {
     PssfpQueueKernel queue;
     PssfpKernel tangent;
     PssfpQueueKernel tangent_queue;
+    bool packed;  // value kernels in the two-wide layout (ZT/2 pairs per lane); tangents scalar
 };
+#define COMPAS_PSSFP(ZT, GZ)                                                                        \
+    {ZT, GZ, kernels::pssfp_kernel<ZT, GZ>, kernels::pssfp_queue_kernel<ZT, GZ>,                 \
+     kernels::pssfp_tangent_kernel<ZT, GZ>, kernels::pssfp_queue_kernel<ZT, GZ, true>, false}
+#define COMPAS_PSSFP_PACKED(ZT, GZ)                                                                 \
+    {ZT, GZ, kernels::pssfp_kernel<ZT, GZ, true>, kernels::pssfp_queue_kernel<ZT, GZ, false, true>, \
+     kernels::pssfp_tangent_kernel<ZT, GZ>, kernels::pssfp_queue_kernel<ZT, GZ, true>, true}
 const PssfpConfig kPssfpConfigs[] = {
-    {1, 1, kernels::pssfp_kernel<1, 1>, kernels::pssfp_queue_kernel<1, 1>,
-     kernels::pssfp_tangent_kernel<1, 1>, kernels::pssfp_queue_kernel<1, 1, true>},
-    {2, 1, kernels::pssfp_kernel<2, 1>, kernels::pssfp_queue_kernel<2, 1>,
-     kernels::pssfp_tangent_kernel<2, 1>, kernels::pssfp_queue_kernel<2, 1, true>},
-    {4, 1, kernels::pssfp_kernel<4, 1>, kernels::pssfp_queue_kernel<4, 1>,
-     kernels::pssfp_tangent_kernel<4, 1>, kernels::pssfp_queue_kernel<4, 1, true>},
-    {8, 1, kernels::pssfp_kernel<8, 1>, kernels::pssfp_queue_kernel<8, 1>,
-     kernels::pssfp_tangent_kernel<8, 1>, kernels::pssfp_queue_kernel<8, 1, true>},
-    {9, 4, kernels::pssfp_kernel<9, 4>, kernels::pssfp_queue_kernel<9, 4>,
-     kernels::pssfp_tangent_kernel<9, 4>, kernels::pssfp_queue_kernel<9, 4, true>},
-    {5, 8, kernels::pssfp_kernel<5, 8>, kernels::pssfp_queue_kernel<5, 8>,
-     kernels::pssfp_tangent_kernel<5, 8>, kernels::pssfp_queue_kernel<5, 8, true>},
-    {3, 16, kernels::pssfp_kernel<3, 16>, kernels::pssfp_queue_kernel<3, 16>,
-     kernels::pssfp_tangent_kernel<3, 16>, kernels::pssfp_queue_kernel<3, 16, true>},
-    {2, 32, kernels::pssfp_kernel<2, 32>, kernels::pssfp_queue_kernel<2, 32>,
-     kernels::pssfp_tangent_kernel<2, 32>, kernels::pssfp_queue_kernel<2, 32, true>},
-    {1, 32, kernels::pssfp_kernel<1, 32>, kernels::pssfp_queue_kernel<1, 32>,
-     kernels::pssfp_tangent_kernel<1, 32>, kernels::pssfp_queue_kernel<1, 32, true>},
-    {18, 2, kernels::pssfp_kernel<18, 2>, kernels::pssfp_queue_kernel<18, 2>,
-     kernels::pssfp_tangent_kernel<18, 2>, kernels::pssfp_queue_kernel<18, 2, true>},
-    {4, 4, kernels::pssfp_kernel<4, 4>, kernels::pssfp_queue_kernel<4, 4>,
-     kernels::pssfp_tangent_kernel<4, 4>, kernels::pssfp_queue_kernel<4, 4, true>},
-    {8, 4, kernels::pssfp_kernel<8, 4>, kernels::pssfp_queue_kernel<8, 4>,
-     kernels::pssfp_tangent_kernel<8, 4>, kernels::pssfp_queue_kernel<8, 4, true>},
-    {4, 8, kernels::pssfp_kernel<4, 8>, kernels::pssfp_queue_kernel<4, 8>,
-     kernels::pssfp_tangent_kernel<4, 8>, kernels::pssfp_queue_kernel<4, 8, true>},
-    {12, 4, kernels::pssfp_kernel<12, 4>, kernels::pssfp_queue_kernel<12, 4>,
-     kernels::pssfp_tangent_kernel<12, 4>, kernels::pssfp_queue_kernel<12, 4, true>},
+    COMPAS_PSSFP(1, 1),  COMPAS_PSSFP(2, 1), COMPAS_PSSFP(4, 1),  COMPAS_PSSFP(8, 1),  COMPAS_PSSFP(9, 4),
+    COMPAS_PSSFP(5, 8),  COMPAS_PSSFP(3, 16), COMPAS_PSSFP(2, 32), COMPAS_PSSFP(1, 32), COMPAS_PSSFP(18, 2),
+    COMPAS_PSSFP(4, 4),  COMPAS_PSSFP(8, 4), COMPAS_PSSFP(4, 8),  COMPAS_PSSFP(12, 4),
+    // the packed layouts come last, so the indices of the others (which a tuning table names) stay
+    COMPAS_PSSFP_PACKED(2, 1), COMPAS_PSSFP_PACKED(4, 1), COMPAS_PSSFP_PACKED(10, 1), COMPAS_PSSFP_PACKED(2, 4),
+    COMPAS_PSSFP_PACKED(4, 4), COMPAS_PSSFP_PACKED(6, 4), COMPAS_PSSFP_PACKED(10, 4), COMPAS_PSSFP_PACKED(6, 2),
+    COMPAS_PSSFP_PACKED(18, 2), COMPAS_PSSFP_PACKED(8, 8),
 };
 }  // namespace
 
@@ -348,24 +488,31 @@ bool pssfp_config_info(int index, int* ZT, int* GZ) {
     return true;
 }
 
-// Default pSSFP layout (from the autotuner's timings on B200): 4 lanes per voxel with the
-// fewest isochromats per lane that cover nz (9 z: ZT4·GZ4 2.3 ms vs 3.9 ms for ZT4·GZ8 at 16384
-// voxels; 35 z: ZT9·GZ4 13.8 ms vs 14.0 ms for ZT5·GZ8 at 50176 voxels); 8 lanes when that
-// needs more than 12 per lane, one lane for nz ≤ 2.
+bool pssfp_config_packed(int index) {
+    return index >= 0 && index < pssfp_config_count() && kPssfpConfigs[index].packed;
+}
+
+// Default pSSFP layout (from timings on B200, 320 TRs of 15 RF samples): for 3 or more z positions
+// the two-wide layout with the fewest slots (isochromats per lane × lanes) that cover nz, at most
+// 5 pairs per lane, fewer lanes first on a tie (35 z: ZT10·GZ4 packed 9.9 ms vs 11.7 ms for the best
+// scalar layout ZT9·GZ4 at 50176 voxels; 9 z: ZT10·GZ1 packed 1.64 ms vs 2.04 ms for ZT4·GZ4 at
+// 16384 voxels); for 1 or 2 the scalar one-lane layout (a pair would hold one idle isochromat).
 PssfpLaunch pssfp_default_launch(int nz, int64_t nvoxels) {
     (void)nvoxels;
-    const int want_gz = nz <= 2 ? 1 : (div_ceil(nz, 4) <= 12 ? 4 : 8);
     int best = -1;
+    auto slots = [](const PssfpConfig& c) { return c.ZT * c.GZ; };
     for (int i = 0; i < pssfp_config_count(); i++) {
         const auto& c = kPssfpConfigs[i];
-        if (c.GZ != want_gz || c.ZT * c.GZ < nz) continue;
-        if (best < 0 || c.ZT < kPssfpConfigs[best].ZT) best = i;
+        const bool eligible = nz <= 2 ? (!c.packed && c.GZ == 1) : (c.packed && c.ZT / 2 <= 5);
+        if (!eligible || slots(c) < nz) continue;
+        if (best < 0 || slots(c) < slots(kPssfpConfigs[best]) ||
+            (slots(c) == slots(kPssfpConfigs[best]) && c.GZ < kPssfpConfigs[best].GZ))
+            best = i;
     }
     if (best < 0) {  // smallest covering layout of any shape
         for (int i = 0; i < pssfp_config_count(); i++) {
             const auto& c = kPssfpConfigs[i];
-            if (c.ZT * c.GZ >= nz && (best < 0 || c.ZT * c.GZ < kPssfpConfigs[best].ZT * kPssfpConfigs[best].GZ))
-                best = i;
+            if (slots(c) >= nz && (best < 0 || slots(c) < slots(kPssfpConfigs[best]))) best = i;
         }
     }
     if (best < 0) best = 7;  // 2 x 32 lanes covers nz ≤ 64

@@ -198,6 +198,10 @@ COMPAS_API int compas_b200_fisp_config_info(int index, int* states_per_lane, int
 COMPAS_API int compas_b200_fisp_config_packed(int index);
 COMPAS_API int compas_b200_pssfp_config_count(void);
 COMPAS_API int compas_b200_pssfp_config_info(int index, int* iso_per_lane, int* lanes);
+/* 1 when pSSFP layout `index` is a two-wide layout (iso_per_lane / 2 pairs of isochromats per
+ * lane, one two-wide FP32 instruction per pair; the same bits as the scalar layout of that size),
+ * else 0. */
+COMPAS_API int compas_b200_pssfp_config_packed(int index);
 /* Layouts of the FISP tangent kernel (compas_b200_simulate_magnetization_tangents); the
  * override (-1 = built-in choice) applies when it covers the state count. */
 COMPAS_API void compas_b200_set_fisp_tangent_launch(int config);

@@ -19,7 +19,8 @@ import compas_b200 as cb
 out = {{"fisp": [cb.fisp_launch_choice(*s) for s in [(25, 50176, 35), (25, 4096, 1), (8, 4096, 1)]],
        "pssfp": [cb.pssfp_launch_choice(*s) for s in [(35, 16384), (5, 4096)]],
        "fisp_configs": cb.fisp_configs(), "pssfp_configs": cb.pssfp_configs(),
-       "fisp_packed": [cb.fisp_config_packed(i) for i in range(len(cb.fisp_configs()))]}}
+       "fisp_packed": [cb.fisp_config_packed(i) for i in range(len(cb.fisp_configs()))],
+       "pssfp_packed": [cb.pssfp_config_packed(i) for i in range(len(cb.pssfp_configs()))]}}
 cb.set_fisp_launch(0, 2)
 out["override_uncovered"] = cb.fisp_launch_choice(25, 50176, 35)
 ok = [i for i, (k, g) in enumerate(cb.fisp_configs()) if k * g >= 25][-1]
@@ -53,7 +54,9 @@ def test_builtin_choice_covers_the_states():
     for cfg, nz in zip(out["pssfp"], (35, 5)):
         zt, gz = pc[cfg]
         assert zt * gz >= nz
-    assert tuple(pc[out["pssfp"][0]]) == (9, 4)
+    # 35 z: the two-wide layout of 5 pairs on 4 lanes (40 slots); 5 z: 1 pair on 4 lanes (8 slots)
+    assert tuple(pc[out["pssfp"][0]]) == (10, 4) and out["pssfp_packed"][out["pssfp"][0]]
+    assert tuple(pc[out["pssfp"][1]]) == (2, 4) and out["pssfp_packed"][out["pssfp"][1]]
     # an override that does not cover the states is ignored; a covering one wins
     assert out["override_uncovered"] == out["fisp"][0]
     assert out["override"][1] == 3
