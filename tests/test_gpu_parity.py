@@ -206,6 +206,33 @@ def test_pssfp_large_rotations(cb, ctx, oracle, workloads):
     assert oracle.rel_l2(got.to_numpy(), oracle.pssfp(p, seq)) < TOL_FP32
 
 
+@pytest.mark.parametrize("scale", [1, 3])
+def test_pssfp_packed_layouts_match_scalar_bits(cb, ctx, workloads, scale):
+    # a two-wide layout runs the scalar update's operations on pairs of isochromats and sums them in
+    # the scalar order: the same bits as the scalar layout with as many isochromats per lane; at 3x
+    # the flip angles (and 20x the off-resonance) some pairs take the sincos branch
+    rng = np.random.default_rng(12 + scale)
+    seq = workloads.pssfp_sequence(rng, 19, nrf=5, nz=3)
+    seq["rf"] = (seq["rf"] * scale).astype(np.complex64)
+    p = workloads.tissue(rng, 5, 20.0)
+    p[3] *= 1 if scale == 1 else 20
+    params = cb.TissueParameters.from_soa(ctx, p)
+    s = cb.pSSFPSequence.from_dict(ctx, seq)
+    configs = cb.pssfp_configs()
+    pairs = [(i, j) for i, c in enumerate(configs) if cb.pssfp_config_packed(i) and c[0] * c[1] >= 3
+             for j, d in enumerate(configs) if not cb.pssfp_config_packed(j) and tuple(d) == tuple(c)]
+    assert len(pairs) >= 3
+    try:
+        for i, j in pairs:
+            cb.set_pssfp_launch(i)
+            packed = cb.simulate_magnetization(ctx, params, s).to_numpy()
+            cb.set_pssfp_launch(j)
+            scalar = cb.simulate_magnetization(ctx, params, s).to_numpy()
+            assert np.array_equal(packed, scalar), configs[i]
+    finally:
+        cb.set_pssfp_launch(-1)
+
+
 # ------------------------------------------------------------------------------------------------
 # signal
 # ------------------------------------------------------------------------------------------------
