@@ -210,11 +210,11 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
         m[k].z = fmaf(m[k].z, E1_pr, 1.0f - E1_pr);
         if constexpr (TAN) {
             const float x1 = d1[k].x, y1 = d1[k].y, x2 = d2[k].x, y2 = d2[k].y;
-            d1[k].x = E2_pr * (c * x1 - s * y1);
-            d1[k].y = E2_pr * (c * y1 + s * x1);
+            d1[k].x = E2_pr * fmaf(c, x1, (-s) * y1);
+            d1[k].y = E2_pr * fmaf(c, y1, s * x1);
             d1[k].z = fmaf(d1[k].z, E1_pr, s1_pr * (m[k].z - 1.0f));
-            d2[k].x = fmaf(s2_pr, m[k].x, E2_pr * (c * x2 - s * y2));
-            d2[k].y = fmaf(s2_pr, m[k].y, E2_pr * (c * y2 + s * x2));
+            d2[k].x = fmaf(s2_pr, m[k].x, E2_pr * fmaf(c, x2, (-s) * y2));
+            d2[k].y = fmaf(s2_pr, m[k].y, E2_pr * fmaf(c, y2, s * x2));
             d2[k].z = d2[k].z * E1_pr;
         }
     };
@@ -280,13 +280,14 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
 }
 
 
-// Two-wide form of pssfp_tile (value only): a lane holds 2·ZP isochromats as ZP pairs, slot p in the
-// low and slot p + ZP in the high half of one register pair per component, and every operation of
-// the rotation, relaxation and precession is one sm_100 two-wide FP32 instruction on a pair, with
-// the RF sample's axis (ax, ay) and the per-voxel coefficients broadcast to both halves. The
-// operations are those of the scalar update in the same order, and the z sum runs over the slots in
-// the scalar order, so layout (ZP pairs, GZ lanes) gives the same bits as the scalar (2·ZP, GZ).
-template<int ZP, int GZ>
+// Two-wide form of pssfp_tile: a lane holds 2·ZP isochromats as ZP pairs, slot p in the low and
+// slot p + ZP in the high half of one register pair per component, and every operation of the
+// rotation, relaxation and precession is one sm_100 two-wide FP32 instruction on a pair, with the RF
+// sample's axis (ax, ay) and the per-voxel coefficients broadcast to both halves. The operations are
+// those of the scalar update in the same order, and the z sums run over the slots in the scalar
+// order, so layout (ZP pairs, GZ lanes) gives the same bits as the scalar (2·ZP, GZ), tangents (TAN)
+// included.
+template<int ZP, int GZ, bool TAN = false>
 __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int tile) {
     constexpr int ZT = 2 * ZP;
     const int lane = threadIdx.x & 31;
@@ -302,8 +303,15 @@ __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int 
     const float E1_ex = expf(-a.dt_ex * R1), E2_ex = expf(-a.dt_ex * R2);
     const float E1_pr = expf(-a.dt_pr * R1), E2_pr = expf(-a.dt_pr * R2);
     const float E1_inv = expf(-a.dt_inv * R1);
+    // tangent factors t/T1², t/T2² of each relaxation interval
+    const float s1_ex = a.dt_ex * R1 * R1, s2_ex = a.dt_ex * R2 * R2;
+    const float s1_pr = a.dt_pr * R1 * R1, s2_pr = a.dt_pr * R2 * R2;
+    const float s1_inv = a.dt_inv * R1 * R1;
 
     float2 mx[ZP], my[ZP], mz[ZP];      // the isochromats' magnetisation
+    constexpr int ZD = TAN ? ZP : 1;
+    float2 ax1[ZD], ay1[ZD], az1[ZD];   // ∂m/∂T1
+    float2 ax2[ZD], ay2[ZD], az2[ZD];   // ∂m/∂T2
     float2 az[ZP], naz[ZP];             // excitation axis z component and its negation
     float2 cpr[ZP], spr[ZP], nspr[ZP];  // precession over the prephasing interval
     bool valid[ZT];
@@ -327,12 +335,17 @@ __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int 
         nspr[p] = make_float2(-zs[0], -zs[1]);
         mx[p] = my[p] = bcast2(0.0f);
         mz[p] = bcast2(mz0);
+        if constexpr (TAN) {
+            ax1[p] = ay1[p] = ax2[p] = ay2[p] = az2[p] = bcast2(0.0f);
+            az1[p] = bcast2(s1_inv * (mz0 - 1.0f));
+        }
     }
 
     const RotRelax rr = make_rot_relax(E1_ex, E2_ex);
     const float2 S0 = bcast2(rr.s0), S1 = bcast2(rr.s1), S2 = bcast2(rr.s2), S3 = bcast2(rr.s3);
     const float2 H0 = bcast2(rr.h0), H1 = bcast2(rr.h1), H2 = bcast2(rr.h2), H3 = bcast2(rr.h3);
     const float2 E2X = bcast2(rr.E2), RX = bcast2(rr.r), ONE_E1X = bcast2(rr.oneE1);
+    const float2 S1EX = bcast2(s1_ex), S2EX = bcast2(s2_ex), NEG1 = bcast2(-1.0f);
     auto excite = [&](int row) {
         const float2* zr = a.zap + int64_t(row) * a.nRF;
         for (int i = 0; i < a.nRF; i++) {
@@ -362,15 +375,40 @@ __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int 
                 mx[p] = fma2(c, mx[p], fma2(sn, cx, mul2(hd, AX)));
                 my[p] = fma2(c, my[p], fma2(sn, cy, mul2(hd, AY)));
                 mz[p] = fma2(RX, fma2(c, mz[p], fma2(sn, cz, mul2(hd, az[p]))), ONE_E1X);
+                if constexpr (TAN) {
+                    // the same map on the tangents plus the explicit terms at the new state:
+                    // (0, 0, t/T1²·(m'_z - 1)) for T1, (t/T2²·m'_x, t/T2²·m'_y, 0) for T2
+                    auto rotate = [&](float2& x, float2& yv, float2& z, float2 px, float2 py, float2 pz) {
+                        const float2 tx = fma2(AY, z, mul2(naz[p], yv));
+                        const float2 ty = fma2(az[p], x, mul2(NAX, z));
+                        const float2 tz = fma2(AX, yv, mul2(NAY, x));
+                        const float2 td = mul2(h, fma2(AX, x, fma2(AY, yv, mul2(az[p], z))));
+                        x = fma2(c, x, fma2(sn, tx, fma2(td, AX, px)));
+                        yv = fma2(c, yv, fma2(sn, ty, fma2(td, AY, py)));
+                        z = fma2(RX, fma2(c, z, fma2(sn, tz, mul2(td, az[p]))), pz);
+                    };
+                    rotate(ax1[p], ay1[p], az1[p], bcast2(0.0f), bcast2(0.0f), mul2(S1EX, add2(mz[p], NEG1)));
+                    rotate(ax2[p], ay2[p], az2[p], mul2(S2EX, mx[p]), mul2(S2EX, my[p]), bcast2(0.0f));
+                }
             }
         }
     };
     const float2 E2P = bcast2(E2_pr), E1P = bcast2(E1_pr), ONE_E1P = bcast2(1.0f - E1_pr);
+    const float2 S1P = bcast2(s1_pr), S2P = bcast2(s2_pr);
     auto precess_by = [&](int p, float2 c, float2 sn, float2 nsn) {
         const float2 x = mx[p], y = my[p];
         mx[p] = mul2(E2P, fma2(c, x, mul2(nsn, y)));
         my[p] = mul2(E2P, fma2(c, y, mul2(sn, x)));
         mz[p] = fma2(mz[p], E1P, ONE_E1P);
+        if constexpr (TAN) {
+            const float2 x1 = ax1[p], y1 = ay1[p], x2 = ax2[p], y2 = ay2[p];
+            ax1[p] = mul2(E2P, fma2(c, x1, mul2(nsn, y1)));
+            ay1[p] = mul2(E2P, fma2(c, y1, mul2(sn, x1)));
+            az1[p] = fma2(az1[p], E1P, mul2(S1P, add2(mz[p], NEG1)));
+            ax2[p] = fma2(S2P, mx[p], mul2(E2P, fma2(c, x2, mul2(nsn, y2))));
+            ay2[p] = fma2(S2P, my[p], mul2(E2P, fma2(c, y2, mul2(sn, x2))));
+            az2[p] = mul2(az2[p], E1P);
+        }
     };
 
     // α/2 pulse, then re- and prephaser with twice the prephasing gradient (pssfp_kernels.cuh:73-80)
@@ -404,7 +442,31 @@ __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int 
             sx += __shfl_xor_sync(0xffffffffu, sx, d, GZ);
             sy += __shfl_xor_sync(0xffffffffu, sy, d, GZ);
         }
-        if (sub == 0 && vok) a.echo[int64_t(t) * a.echo_stride + a.voxel_begin + vloc] = make_float2(sx, sy);
+        const int64_t at = int64_t(t) * a.echo_stride + a.voxel_begin + vloc;
+        if (sub == 0 && vok) a.echo[at] = make_float2(sx, sy);
+        if constexpr (TAN) {
+            float t1x = 0.0f, t1y = 0.0f, t2x = 0.0f, t2y = 0.0f;
+#pragma unroll
+            for (int k = 0; k < ZT; k++) {
+                if (valid[k]) {
+                    t1x += k < ZP ? ax1[k].x : ax1[k - ZP].y;
+                    t1y += k < ZP ? ay1[k].x : ay1[k - ZP].y;
+                    t2x += k < ZP ? ax2[k].x : ax2[k - ZP].y;
+                    t2y += k < ZP ? ay2[k].x : ay2[k - ZP].y;
+                }
+            }
+#pragma unroll
+            for (int d = GZ / 2; d > 0; d /= 2) {
+                t1x += __shfl_xor_sync(0xffffffffu, t1x, d, GZ);
+                t1y += __shfl_xor_sync(0xffffffffu, t1y, d, GZ);
+                t2x += __shfl_xor_sync(0xffffffffu, t2x, d, GZ);
+                t2y += __shfl_xor_sync(0xffffffffu, t2y, d, GZ);
+            }
+            if (sub == 0 && vok) {
+                a.dT1[at] = make_float2(t1x, t1y);
+                a.dT2[at] = make_float2(t2x, t2y);
+            }
+        }
 #pragma unroll
         for (int p = 0; p < ZP; p++) precess_by(p, cpr[p], spr[p], nspr[p]);
     }
@@ -419,9 +481,10 @@ __global__ void __launch_bounds__(128) pssfp_kernel(PssfpArgs a) {
 }
 
 // One pSSFP simulation with its T1 and T2 tangents into a.echo, a.dT1, a.dT2.
-template<int ZT, int GZ>
+template<int ZT, int GZ, bool PACKED = false>
 __global__ void __launch_bounds__(128) pssfp_tangent_kernel(PssfpArgs a) {
-    pssfp_tile<ZT, GZ, true>(a, blockIdx.x);
+    if constexpr (PACKED) pssfp_tile_packed<ZT / 2, GZ, true>(a, blockIdx.x);
+    else pssfp_tile<ZT, GZ, true>(a, blockIdx.x);
 }
 
 // Persistent work-queue kernel for a batch of pSSFP simulations sharing one (ZT, GZ) layout:
@@ -441,7 +504,7 @@ __global__ void __launch_bounds__(128) pssfp_queue_kernel(const PssfpArgs* __res
         const int2 w = items[it];
         if (threadIdx.x == 0) job = jobs[w.x];
         __syncthreads();
-        if constexpr (PACKED) pssfp_tile_packed<ZT / 2, GZ>(job, w.y);
+        if constexpr (PACKED) pssfp_tile_packed<ZT / 2, GZ, TAN>(job, w.y);
         else pssfp_tile<ZT, GZ, TAN>(job, w.y);
         __syncthreads();
     }
@@ -458,12 +521,17 @@ struct PssfpConfig {
     PssfpQueueKernel queue;
     PssfpKernel tangent;
     PssfpQueueKernel tangent_queue;
-    bool packed;  // value kernels in the two-wide layout (ZT/2 pairs per lane); tangents scalar
+    bool packed;  // two-wide layout (ZT/2 pairs of isochromats per lane), value and tangent kernels
 };
 #define COMPAS_PSSFP(ZT, GZ)                                                                        \
     {ZT, GZ, kernels::pssfp_kernel<ZT, GZ>, kernels::pssfp_queue_kernel<ZT, GZ>,                 \
      kernels::pssfp_tangent_kernel<ZT, GZ>, kernels::pssfp_queue_kernel<ZT, GZ, true>, false}
 #define COMPAS_PSSFP_PACKED(ZT, GZ)                                                                 \
+    {ZT, GZ, kernels::pssfp_kernel<ZT, GZ, true>, kernels::pssfp_queue_kernel<ZT, GZ, false, true>, \
+     kernels::pssfp_tangent_kernel<ZT, GZ, true>, kernels::pssfp_queue_kernel<ZT, GZ, true, true>, true}
+// packed value kernels with the scalar tangent kernels (the same bits; for layouts whose three packed
+// vectors would not fit the registers)
+#define COMPAS_PSSFP_PACKED_VALUE(ZT, GZ)                                                           \
     {ZT, GZ, kernels::pssfp_kernel<ZT, GZ, true>, kernels::pssfp_queue_kernel<ZT, GZ, false, true>, \
      kernels::pssfp_tangent_kernel<ZT, GZ>, kernels::pssfp_queue_kernel<ZT, GZ, true>, true}
 const PssfpConfig kPssfpConfigs[] = {
@@ -473,7 +541,7 @@ const PssfpConfig kPssfpConfigs[] = {
     // the packed layouts come last, so the indices of the others (which a tuning table names) stay
     COMPAS_PSSFP_PACKED(2, 1), COMPAS_PSSFP_PACKED(4, 1), COMPAS_PSSFP_PACKED(10, 1), COMPAS_PSSFP_PACKED(2, 4),
     COMPAS_PSSFP_PACKED(4, 4), COMPAS_PSSFP_PACKED(6, 4), COMPAS_PSSFP_PACKED(10, 4), COMPAS_PSSFP_PACKED(6, 2),
-    COMPAS_PSSFP_PACKED(18, 2), COMPAS_PSSFP_PACKED(8, 8),
+    COMPAS_PSSFP_PACKED_VALUE(18, 2), COMPAS_PSSFP_PACKED(8, 8),
 };
 }  // namespace
 
