@@ -19,6 +19,7 @@
 // * The per-(position, TR) RF angle and phase table is built once per sequence and kept
 //   resident with it.
 #include <cfloat>
+#include <optional>
 #include <type_traits>
 
 #include "common.cuh"
@@ -484,11 +485,50 @@ constexpr int kFispChunk = (TAN && G > 1) ? 64 : 32;
 template<int K, int G, bool TAN, bool PACKED>
 using FispState = std::conditional_t<TAN, EPGTangent<K, G>, std::conditional_t<PACKED, EPGPacked<K / 2>, EPG<K, G>>>;
 
+// Balanced item split of the one-simulation kernel: the order of a CTA's items (at most
+// kFispBalancedItems) and its hand-off points, in shared memory
+constexpr int kFispBalancedItems = 2048;
+struct FispOrder {
+    int item[kFispBalancedItems];  // item of the u-th position in the CTA's order
+    int wait_u;                    // first u of the head part (positions of the shared first tile)
+    int publish_u;                 // u after the tail part (first positions of the shared last tile)
+    int cta;
+    int* handoff;                  // per-CTA flags, zero at launch
+    unsigned int* status;          // device status word
+};
+
+// Hand-off flags of the balanced item split: a CTA publishes the partial sums of its last, shared
+// tile, and the next CTA waits for them before it adds its positions of that tile. The wait is
+// bounded: one that gives up records STATUS_WAIT_TIMEOUT in the status word and returns.
+__device__ __forceinline__ void handoff_publish(int* flag) {
+    __threadfence();  // the CTA's partial-sum stores (ordered before by the barrier) are visible first
+    atomicExch(flag, 1);
+}
+__device__ __forceinline__ void handoff_wait(const int* flag, unsigned int* status) {
+    const long long t0 = clock64();
+    for (;;) {
+        int v;
+        asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+        if (v != 0) return;
+        if (clock64() - t0 > 4000000000LL) {
+            if (status) atomicOr(status, STATUS_WAIT_TIMEOUT);
+            return;
+        }
+        __nanosleep(256);
+    }
+}
+
 // TAN: also propagate ∂/∂T1 and ∂/∂T2 (EPGTangent) and write them to a.dT1, a.dT2; the
 // value goes through the same operations either way.
-template<int K, int G, bool TAN = false, bool PACKED = false>
+// BAL: items u = item_begin .. item_end-1 of the order `ord` (one-simulation kernel, balanced split):
+// the tail of the CTA's share (the first positions of its last tile, shared with CTA cta + 1), its
+// whole tiles, then the head (the last positions of its first tile, shared with CTA cta - 1); the
+// tail's partial sums are published as soon as they are written and the head waits for the
+// predecessor's. Every tile's positions are still added one at a time in increasing order, so the
+// echoes are the same bits as with whole tiles per CTA.
+template<int K, int G, bool TAN = false, bool PACKED = false, bool BAL = false>
 __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_begin, const int item_end,
-                                           float2* samples) {
+                                           float2* samples, const FispOrder* ord = nullptr) {
     static_assert(!PACKED || (G == 1 && K % 2 == 0 && !TAN), "packed layouts hold one voxel per lane");
     constexpr int VB = 32 / G;
     const int W = blockDim.x >> 5;
@@ -503,9 +543,16 @@ __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_beg
     const int plane = W * CH * VB;  // sample planes: value, ∂/∂T1, ∂/∂T2
     constexpr int NQ = TAN ? 3 : 1;
 
+    // item of position u of the order: the identity unless BAL
+    auto item_at = [&](int u) { return BAL ? ord->item[u] : u; };
     for (int base = item_begin; base < item_end; base += W) {
         const int nact = min(W, item_end - base);  // warps with an item this round
-        const int item = base + min(warp, nact - 1);
+        if (BAL && base <= ord->wait_u && ord->wait_u < base + nact) {
+            // this round reaches the head: its tile's first positions come from CTA cta - 1
+            if (threadIdx.x == 0) handoff_wait(ord->handoff + ord->cta - 1, ord->status);
+            __syncthreads();
+        }
+        const int item = item_at(base + min(warp, nact - 1));
         const bool pok = warp < nact;  // warp-uniform
         const int tile = item / P, p = item % P;
         const int vloc = tile * VB + (kSpareLanes ? min(grp, VB - 1) : grp);
@@ -540,7 +587,7 @@ __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_beg
         // warp w starts one); every thread derives the same mask
         unsigned starts = 0;
         for (int w = 0; w < nact; w++)
-            if (w == 0 || (base + w) / P != (base + w - 1) / P) starts |= 1u << w;
+            if (w == 0 || item_at(base + w) / P != item_at(base + w - 1) / P) starts |= 1u << w;
 
         const float4* tab = a.table + int64_t(p) * a.nTR;
         FispState<K, G, TAN, PACKED> st;
@@ -610,11 +657,11 @@ __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_beg
                     for (int w0 = 0; w0 < nact;) {
                         int w1 = w0 + 1;
                         while (w1 < nact && !(starts & (1u << w1))) w1++;
-                        const int seg_tile = (base + w0) / P;
-                        const bool first = (base + w0) % P == 0;
-                        // a partial sum is read again by a later round: keep it in L2; the
-                        // tile's final sum streams out
-                        const bool last = (base + w1 - 1) % P == P - 1;
+                        const int seg_tile = item_at(base + w0) / P;
+                        const bool first = item_at(base + w0) % P == 0;
+                        // a partial sum is read again by a later round (or the next CTA): keep it
+                        // in L2; the tile's final sum streams out
+                        const bool last = item_at(base + w1 - 1) % P == P - 1;
 #pragma unroll
                         for (int qn = 0; qn < NQ; qn++) {
                             float2* out = qn == 0 ? a.echo : qn == 1 ? a.dT1 : a.dT2;
@@ -624,7 +671,7 @@ __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_beg
                                 if (v >= a.nvoxels) continue;
                                 const float2* col = samples + qn * plane + j * VB + gv;
                                 float2* row0 = out + int64_t(t0 + j) * a.uf * a.echo_stride + a.voxel_begin + v;
-                                float2 acc = first ? col[w0 * CH * VB] : cadd(*row0, col[w0 * CH * VB]);
+                                float2 acc = first ? col[w0 * CH * VB] : cadd(__ldcg(row0), col[w0 * CH * VB]);
                                 for (int w = w0 + 1; w < w1; w++) acc = cadd(acc, col[w * CH * VB]);
                                 for (int q = 0; q < a.uf; q++) {
                                     float2* dst = row0 + int64_t(q) * a.echo_stride;
@@ -654,6 +701,10 @@ __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_beg
                 }
             }
         }
+        if (BAL && base < ord->publish_u && ord->publish_u <= base + nact) {
+            // the tail's partial sums are written (the summation ends with a barrier): hand them over
+            if (threadIdx.x == 0) handoff_publish(ord->handoff + ord->cta);
+        }
     }
 }
 
@@ -662,14 +713,44 @@ __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_beg
 __device__ __forceinline__ int2 cta_tile_range(int ntiles, int cta, int nctas) {
     return make_int2(int(int64_t(ntiles) * cta / nctas), int(int64_t(ntiles) * (cta + 1) / nctas));
 }
-// One FISP simulation: a persistent grid of CTAs, each running a contiguous range of whole voxel
-// tiles (cta_tile_range). PACKED: the two-wide layout EPGPacked<K/2> (one lane per voxel).
-template<int K, int G, bool PACKED = false>
-__global__ void __launch_bounds__(256, 1) fisp_epg_kernel(FispArgs a, int ntiles) {
+// One FISP simulation: a persistent grid of CTAs. Without `handoff` each CTA runs a contiguous
+// range of whole voxel tiles (cta_tile_range). With `handoff` (per-CTA flags, zero at launch; the
+// host asks for it when every CTA's
+// share spans at least two tiles, holds at most kFispBalancedItems items and all CTAs are resident
+// at once) each CTA runs an equal share of the (tile, position) items, sizes differing by at most
+// one item, in the order tail, whole tiles, head (fisp_items). PACKED: the two-wide layout
+// EPGPacked<K/2> (one lane per voxel).
+// BAL instantiates the balanced form (launched with non-null `handoff`), the others the whole-tile
+// form (`handoff` unused), so that each compiles to its own register allocation.
+template<int K, int G, bool PACKED = false, bool BAL = false>
+__global__ void __launch_bounds__(256, 1) fisp_epg_kernel(FispArgs a, int ntiles, int* handoff, unsigned int* status) {
     extern __shared__ float2 samples[];  // [W][32][VB]
     if (a.skip != nullptr && *a.skip != 0) return;  // uniform over the grid
-    const int2 r = cta_tile_range(ntiles, blockIdx.x, gridDim.x);
-    fisp_items<K, G, false, PACKED>(a, r.x * a.P, r.y * a.P, samples);
+    if constexpr (BAL) {
+        __shared__ FispOrder ord;
+        const int64_t total = int64_t(ntiles) * a.P;
+        const int i0 = int(total * blockIdx.x / gridDim.x), i1 = int(total * (blockIdx.x + 1) / gridDim.x);
+        const int P = a.P, n = i1 - i0;
+        const int h_end = min(i1, (i0 + P - 1) / P * P);  // end of the head: the first tile's last positions
+        const int t_start = max(h_end, i1 / P * P);        // start of the tail: the last tile's first positions
+        const int L0 = i1 - t_start, L01 = L0 + (t_start - h_end);
+        for (int u = threadIdx.x; u < n; u += blockDim.x)
+            ord.item[u] = u < L0 ? t_start + u : (u < L01 ? h_end + (u - L0) : i0 + (u - L01));
+        if (threadIdx.x == 0) {
+            ord.wait_u = i0 % P != 0 ? L01 : n;      // n: no head, nothing to wait for
+            ord.publish_u = i1 % P != 0 ? L0 : -1;   // -1: no tail, nothing to hand over
+            ord.cta = blockIdx.x;
+            ord.handoff = handoff;
+            ord.status = status;
+        }
+        __syncthreads();
+        fisp_items<K, G, false, PACKED, true>(a, 0, n, samples, &ord);
+    } else {
+        (void)handoff;
+        (void)status;
+        const int2 r = cta_tile_range(ntiles, blockIdx.x, gridDim.x);
+        fisp_items<K, G, false, PACKED>(a, r.x * a.P, r.y * a.P, samples);
+    }
 }
 
 // Persistent work-queue kernel for a batch of FISP simulations sharing one layout and W:
@@ -733,20 +814,24 @@ __global__ void __launch_bounds__(256, 1) fisp_tangent_queue_kernel(const FispAr
 namespace {
 
 using FispKernel = void (*)(kernels::FispArgs, int);
+using FispValueKernel = void (*)(kernels::FispArgs, int, int*, unsigned int*);
 using FispQueueKernel = void (*)(const kernels::FispArgs*, const int2*, int, int*);
 
 struct FispConfig {
     int K, G;
     bool packed;  // EPGPacked<K/2>: two states per two-wide instruction
-    FispKernel fn;
+    FispValueKernel fn;
     FispQueueKernel queue;
+    FispValueKernel balanced;  // the balanced item split (packed layouts), else null
 };
 
 // Instantiated layouts: (states per lane K, lanes per voxel/position G). Coverage K·G ≥ N.
 // The packed one-lane layouts come last, so the indices of the others (which a tuning table
 // names) keep their meaning.
-#define COMPAS_FISP(K, G) {K, G, false, kernels::fisp_epg_kernel<K, G>, kernels::fisp_queue_kernel<K, G>}
-#define COMPAS_FISP_PACKED(K) {K, 1, true, kernels::fisp_epg_kernel<K, 1, true>, kernels::fisp_queue_kernel<K, 1, true>}
+#define COMPAS_FISP(K, G) {K, G, false, kernels::fisp_epg_kernel<K, G>, kernels::fisp_queue_kernel<K, G>, nullptr}
+#define COMPAS_FISP_PACKED(K)                                                                         \
+    {K, 1, true, kernels::fisp_epg_kernel<K, 1, true>, kernels::fisp_queue_kernel<K, 1, true>,      \
+     kernels::fisp_epg_kernel<K, 1, true, true>}
 const FispConfig kFispConfigs[] = {
     COMPAS_FISP(1, 1), COMPAS_FISP(2, 1), COMPAS_FISP(4, 1), COMPAS_FISP(6, 1), COMPAS_FISP(8, 1),
     COMPAS_FISP(12, 1), COMPAS_FISP(16, 1), COMPAS_FISP(20, 1), COMPAS_FISP(25, 1),
@@ -939,7 +1024,8 @@ int fisp_tile_voxels(FispLaunch L) {
 }
 
 void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
-                 const FISPSequence& seq, cfloat* echo, int64_t echo_stride, FispLaunch L, const int* skip) {
+                 const FISPSequence& seq, cfloat* echo, int64_t echo_stride, FispLaunch L, const int* skip,
+                 bool balance) {
     const int nTR = int(seq.RF_train.size());
     const int P = int(seq.sliceprofiles.size(0));
     const int N = seq.max_state;
@@ -958,7 +1044,31 @@ void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int v
     DeviceGuard guard(ctx.device());
     allow_smem(reinterpret_cast<const void*>(cfg.fn), smem);
     const int grid = std::min(ntiles, resident_ctas(reinterpret_cast<const void*>(cfg.fn), 32 * W, smem, ctx.device()));
-    cfg.fn<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles);
+    // The balanced split needs every CTA's share to span at least two tiles (so a CTA waits only on
+    // its predecessor's first part, never on a chain), at most kFispBalancedItems items, and all
+    // CTAs resident at once (the grid is at most one resident wave). It saves the idle tail of the
+    // CTAs with one more whole tile: 1568 tiles x 35 positions on 148 CTAs of 8 warps run 47 rounds
+    // instead of 49.
+    const int64_t per_cta = (int64_t(ntiles) * P + grid - 1) / grid;
+    bool balanced = balance && cfg.balanced != nullptr && grid > 1 && int64_t(ntiles) >= 2 * int64_t(grid) &&
+                    per_cta <= kernels::kFispBalancedItems;
+    if (balanced) {
+        const void* bfn = reinterpret_cast<const void*>(cfg.balanced);
+        allow_smem(bfn, smem);
+        int per_sm = 0;
+        COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfn, 32 * W, smem));
+        int sms = 148;
+        COMPAS_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device()));
+        balanced = int64_t(per_sm) * sms >= grid;  // every CTA resident at once
+    }
+    std::optional<Array<int, 1>> flags;
+    if (balanced) {
+        flags.emplace(std::array<int64_t, 1> {grid}, ctx.device(), ctx.stream());
+        COMPAS_CUDA_CHECK(cudaMemsetAsync(flags->data(), 0, sizeof(int) * size_t(grid), ctx.stream()));
+        cfg.balanced<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles, flags->data(), ctx.status_word());
+    } else {
+        cfg.fn<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles, nullptr, nullptr);
+    }
     check_launch("fisp_epg_kernel");
 }
 
@@ -1066,7 +1176,8 @@ Array<cfloat, 2> simulate_magnetization(const CompasContext& context, TissuePara
     const int nvoxels = parameters.nvoxels;
     COMPAS_CHECK(sequence.undersampling_factor >= 1);
     Array<cfloat, 2> echos({nreadouts, nvoxels}, context.device(), context.stream());
-    launch_fisp(context, parameters, 0, nvoxels, sequence, echos.data(), nvoxels, tuned_fisp_launch(sequence.max_state, nvoxels, int(sequence.sliceprofiles.size(0))));
+    launch_fisp(context, parameters, 0, nvoxels, sequence, echos.data(), nvoxels,
+                tuned_fisp_launch(sequence.max_state, nvoxels, int(sequence.sliceprofiles.size(0))), nullptr, true);
     return echos;
 }
 

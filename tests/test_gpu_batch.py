@@ -114,3 +114,32 @@ def test_batch_tangent_jobs_match_one_job_calls_bitwise(ctx):
         if traj is not None:
             s_ref = cb.magnetization_to_signal(ctx, echos, params, traj, coils, method="MatmulFast").to_numpy()
             assert np.array_equal(batch.signal(j).to_numpy(), s_ref), (j, "signal")
+
+
+@pytest.mark.parametrize("P", [7, 35])
+def test_balanced_fisp_split_matches_whole_tiles_bitwise(ctx, P):
+    # With at least two voxel tiles per CTA, the one-simulation FISP kernel splits the (tile,
+    # position) items evenly over its CTAs: neighbours share a tile and the later one adds its
+    # positions to the earlier one's partial sums. The work-queue kernel of a batch runs whole tiles
+    # per item. Both add every tile's positions one at a time in increasing order: the same bits.
+    import compas_b200 as cb
+
+    rng = np.random.default_rng(40 + P)
+    nv, ntr = 13000, 48  # 407 tiles of 32 voxels on at most 148 CTAs
+    d = {"kind": "fisp", "params": W.tissue_voxels(rng, nv, 22.4),
+         "seq": W.fisp_sequence(W.smooth_flip_train(rng, ntr), W.gaussian_slice_profile(P, ntr), 8.7e-3, 4.35e-3,
+                                25e-3, 25),
+         "traj": None, "coils": np.ones((1, nv), np.complex64)}
+    packed = next(i for i, (k, g) in enumerate(cb.fisp_configs()) if (k, g) == (26, 1) and cb.fisp_config_packed(i))
+    cb.set_fisp_launch(packed, 8)
+    try:
+        params, seq, traj, coils = cb.job_from_dict(ctx, d)
+        single = cb.simulate_magnetization(ctx, params, seq).to_numpy()
+        batch = cb.SimulationBatch(ctx, [(params, seq, traj, coils)], method="MatmulFast")
+        batch.run()
+        ctx.synchronize()
+        assert np.array_equal(single, batch.echos(0).to_numpy())
+        again = cb.simulate_magnetization(ctx, params, seq).to_numpy()
+        assert np.array_equal(single, again)
+    finally:
+        cb.set_fisp_launch(-1, -1)

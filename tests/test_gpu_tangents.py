@@ -138,6 +138,35 @@ def test_pssfp_tangents_every_layout(cb, ctx, oracle, workloads, nz):
     assert tried > 0
 
 
+@pytest.mark.parametrize("scale", [1, 3])
+def test_pssfp_packed_tangents_match_scalar_bits(cb, ctx, workloads, scale):
+    # the two-wide tangent kernel runs the scalar tangent update's operations on pairs of isochromats:
+    # m, ∂m/∂T1 and ∂m/∂T2 are the bits of the scalar layout with as many isochromats per lane (at 3x
+    # the flip angles and 20x the off-resonance, some pairs take the sincos branch)
+    rng = np.random.default_rng(30 + scale)
+    seqd = workloads.pssfp_sequence(rng, 15, nrf=5, nz=3)
+    seqd["rf"] = (seqd["rf"] * scale).astype(np.complex64)
+    p = workloads.tissue(rng, 5, 20.0)
+    p[3] *= 1 if scale == 1 else 20
+    params = cb.TissueParameters.from_soa(ctx, p)
+    seq = cb.pSSFPSequence.from_dict(ctx, seqd)
+    configs = cb.pssfp_configs()
+    pairs = [(i, j) for i, c in enumerate(configs) if cb.pssfp_config_packed(i) and c[0] * c[1] >= 3
+             for j, d in enumerate(configs) if not cb.pssfp_config_packed(j) and tuple(d) == tuple(c)]
+    assert len(pairs) >= 3
+    try:
+        for i, j in pairs:
+            cb.set_pssfp_launch(i)
+            packed = cb.simulate_magnetization_tangents(ctx, params, seq)
+            packed = {k: packed[k].to_numpy() for k in ("echos", "T1", "T2")}
+            cb.set_pssfp_launch(j)
+            scalar = cb.simulate_magnetization_tangents(ctx, params, seq)
+            for k in ("echos", "T1", "T2"):
+                assert np.array_equal(packed[k], scalar[k].to_numpy()), (configs[i], k)
+    finally:
+        cb.set_pssfp_launch(-1)
+
+
 def test_pssfp_tangents_large_rotations(cb, ctx, oracle, workloads):
     # 3× the flip angles and 20× the off-resonance: the sincos branch of the rotation
     rng = np.random.default_rng(4)
