@@ -77,6 +77,21 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.window = (0, None)  # the lines sampled inside the timed region (mark_start / mark_end)
+
+    def _lines(self):
+        try:
+            return Path(self.path).read_text().count("\n")
+        except OSError:
+            return 0
+
+    def mark_start(self):
+        self.window = (self._lines(), None)
+
+    def mark_end(self):
+        # the sample in flight when the region ends belongs to it too
+        time.sleep(0.25)
+        self.window = (self.window[0], self._lines())
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -87,15 +102,12 @@ class ClockSampler:
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
-        # start timing only once nvidia-smi is polling: its start-up (NVML initialisation) occupies
-        # the NVIDIA kernel driver for up to a second and must not fall inside the timed region
+        # start timing only once nvidia-smi has been polling for a while: its start-up (NVML
+        # initialisation) and its first queries occupy the NVIDIA kernel driver for up to a second,
+        # and a driver call of the timed steps that waits on it leaves the GPU idle (a 0.5 s stall
+        # in one step was seen with timing started after the first sample)
         deadline = time.perf_counter() + 5.0
-        while self.proc is not None and time.perf_counter() < deadline:
-            try:
-                if Path(self.path).read_text().count("\n") >= 1:
-                    break
-            except OSError:
-                pass
+        while self.proc is not None and time.perf_counter() < deadline and self._lines() < 4:
             time.sleep(0.05)
         time.sleep(0.1)
         return self
@@ -112,7 +124,10 @@ class ClockSampler:
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         try:
-            for line in Path(self.path).read_text().splitlines():
+            lines = Path(self.path).read_text().splitlines()
+            lo, hi = self.window
+            timed = lines[lo:hi] if hi is not None and hi > lo else lines[lo:]
+            for line in timed or lines[-1:]:
                 f = [x.strip() for x in line.split(",")]
                 if len(f) < 9:
                     continue
@@ -299,10 +314,6 @@ def main():
             events[2].record(stream)
         return e, s
 
-    for _ in range(args.warmup):
-        step()
-    ctx.synchronize()
-
     def barrier():
         if world > 1:
             torch.distributed.barrier()
@@ -312,8 +323,14 @@ def main():
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     keep = []
+    # the clock sampler polls from before the warm-up on, so that its start-up is over before the
+    # timed steps; its summary covers the samples taken between mark_start and mark_end
     with ClockSampler(local) as clk:
+        for _ in range(args.warmup):
+            step()
+        ctx.synchronize()
         barrier()
+        clk.mark_start()
         launches0 = cb.launch_count()
         t_start.record(stream)
         for i in range(args.steps):
@@ -323,6 +340,7 @@ def main():
         t_end.record(stream)
         barrier()
         launches = cb.launch_count() - launches0
+        clk.mark_end()
     last_signal = keep[-1][1] if keep else None
     keep.clear()
     total_ms = t_start.elapsed_time(t_end)

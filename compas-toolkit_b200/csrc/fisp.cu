@@ -1025,7 +1025,7 @@ int fisp_tile_voxels(FispLaunch L) {
 
 void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
                  const FISPSequence& seq, cfloat* echo, int64_t echo_stride, FispLaunch L, const int* skip,
-                 bool balance) {
+                 bool balance, int* handoff, int handoff_capacity) {
     const int nTR = int(seq.RF_train.size());
     const int P = int(seq.sliceprofiles.size(0));
     const int N = seq.max_state;
@@ -1051,7 +1051,7 @@ void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int v
     // instead of 49.
     const int64_t per_cta = (int64_t(ntiles) * P + grid - 1) / grid;
     bool balanced = balance && cfg.balanced != nullptr && grid > 1 && int64_t(ntiles) >= 2 * int64_t(grid) &&
-                    per_cta <= kernels::kFispBalancedItems;
+                    per_cta <= kernels::kFispBalancedItems && (handoff == nullptr || grid <= handoff_capacity);
     if (balanced) {
         const void* bfn = reinterpret_cast<const void*>(cfg.balanced);
         allow_smem(bfn, smem);
@@ -1063,9 +1063,12 @@ void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int v
     }
     std::optional<Array<int, 1>> flags;
     if (balanced) {
-        flags.emplace(std::array<int64_t, 1> {grid}, ctx.device(), ctx.stream());
-        COMPAS_CUDA_CHECK(cudaMemsetAsync(flags->data(), 0, sizeof(int) * size_t(grid), ctx.stream()));
-        cfg.balanced<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles, flags->data(), ctx.status_word());
+        if (handoff == nullptr) {
+            flags.emplace(std::array<int64_t, 1> {grid}, ctx.device(), ctx.stream());
+            handoff = flags->data();
+        }
+        COMPAS_CUDA_CHECK(cudaMemsetAsync(handoff, 0, sizeof(int) * size_t(grid), ctx.stream()));
+        cfg.balanced<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles, handoff, ctx.status_word());
     } else {
         cfg.fn<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles, nullptr, nullptr);
     }

@@ -231,6 +231,8 @@ struct GaussNewtonStep::Impl {
     Array<cfloat, 2> trial_echos;   // m(trial)
     Array<cfloat, 3> trial_signal;  // s(trial)
     Array<int> flags;               // kernels::Flag
+    Array<int> handoff;             // per-CTA flags of the balanced FISP split (zeroed per simulation)
+    static constexpr int kHandoffCapacity = 4096;
 
     Array<cfloat, 2> echos, dT1, dT2;
     Array<cfloat, 3> signal, b, q;
@@ -246,7 +248,7 @@ struct GaussNewtonStep::Impl {
         const int V = p.nvoxels;
         if (const auto* f = std::get_if<FISPSequence>(&sequence)) {
             launch_fisp(ctx, p, 0, V, *f, out, V, tuned_fisp_launch(f->max_state, V, int(f->sliceprofiles.size(0))),
-                        skip);
+                        skip, true, handoff.data(), kHandoffCapacity);
         } else {
             const auto& s = std::get<pSSFPSequence>(sequence);
             launch_pssfp(ctx, p, 0, V, s, out, V, tuned_pssfp_launch(int(s.z.size()), V), skip);
@@ -446,6 +448,7 @@ GaussNewtonStep::GaussNewtonStep(const CompasContext& ctx, TissueParameters para
     im.d = Array<cfloat, 2>({4, V}, dev, ctx.stream());
     im.x = Array<float, 2>({4, V}, dev, ctx.stream());
     im.scalars = Array<float>({kernels::kNumScalars}, dev, ctx.stream());
+    im.handoff = Array<int>({Impl::kHandoffCapacity}, dev, ctx.stream());
     im.trial = Array<float, 2>({TissueParameterField::NUM_FIELDS, V}, dev, ctx.stream());
     COMPAS_CUDA_CHECK(cudaMemcpyAsync(im.trial.data(), own.data(), own.nbytes(), cudaMemcpyDeviceToDevice,
                                       ctx.stream()));

@@ -25,11 +25,12 @@ const Array<float, 3>& fisp_excite_table(const CompasContext& ctx, const FISPSeq
 // `skip` (device int, may be null): when it holds a nonzero value at run time the kernel returns
 // without writing (a step of a captured graph that is not needed this time)
 // `balance`: split the (tile, position) items evenly over the CTAs, neighbours handing over the
-// partial sums of the tile they share (one small stream-ordered allocation per call; the echoes
-// are the same bits either way); off: whole tiles per CTA, nothing allocated
+// partial sums of the tile they share (the echoes are the same bits either way); its per-CTA flags
+// live in `handoff` (`handoff_capacity` ints, owned by the caller, zeroed here on the stream) or,
+// without, in a small stream-ordered allocation per call. Off: whole tiles per CTA.
 void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
                  const FISPSequence& seq, cfloat* echo, int64_t echo_stride, FispLaunch L,
-                 const int* skip = nullptr, bool balance = false);
+                 const int* skip = nullptr, bool balance = false, int* handoff = nullptr, int handoff_capacity = 0);
 // argument block of one FISP simulation (validates the sequence, builds its table on first use)
 kernels::FispArgs fisp_args(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
                             const FISPSequence& seq, cfloat* echo, int64_t echo_stride);
