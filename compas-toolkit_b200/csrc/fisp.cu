@@ -30,7 +30,8 @@
 namespace compas {
 namespace kernels {
 
-// table[p][t] = {½·(π/180)·|sliceprofile[p][t]·RF[t]|, cos φ, sin φ, 0}
+// table[p][t] = {½·(π/180)·|sliceprofile[p][t]·RF[t]|, cos φ, sin φ, 0} for p < P, and in the extra
+// row P: table[P][0].x = 1 when some entry has sin φ ≠ 0, else 0 (the row is zeroed before the launch)
 __global__ void fisp_table_kernel(const float2* __restrict__ rf, const float2* __restrict__ slices, int nTR,
                                   int P, float4* __restrict__ table) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -46,6 +47,14 @@ __global__ void fisp_table_kernel(const float2* __restrict__ rf, const float2* _
         sp = im / a;
     }
     table[i] = make_float4(float(0.5 * (M_PI / 180.0) * a), float(cp), float(sp), 0.0f);
+    if (float(sp) != 0.0f) table[int64_t(P) * nTR].x = 1.0f;  // every writer stores the same value
+}
+
+// True when every phase of the sequence's table is real (sin φ = 0 exactly: a real RF train and real
+// slice profiles, as in the usual MR-STAT FISP sequences). The excitation coefficient d_re = sin φ·sin α·E1
+// and β·R13_re are then ±0, and the packed update leaves out their products (EPGPacked::excite<true>).
+__device__ __forceinline__ bool fisp_real_phases(const FispArgs& a) {
+    return __ldg(&a.table[int64_t(a.P) * a.nTR].x) == 0.0f;
 }
 
 
@@ -299,15 +308,20 @@ struct EPGPacked {
     // excite_state on a pair with Qn = -Im Q, zn = -Im Z and nQhi = -Im Qh:
     //   Qh_r = A4·Qr + A3·Qn + d_im·zn,   -Qh_i = A2·Qr + A1·Qn + d_re·zn,
     //   Z_r' = e_re·Pr - e_im·Pi + f·Z_r,   -Z_i' = e_re·Qn - e_im·Qr + f·zn
+    // REAL (every RF phase real, fisp_real_phases): d_re and β·R13_re are ±0, so d_re·Z_r, d_re·zn and
+    // the β·R13_re additions are left out: 24 instructions per pair instead of 26. An FMA that adds ±0
+    // to a product returns the rounded product, so the results are the same bits up to the sign of an
+    // exact zero.
+    template<bool REAL = false>
     __device__ __forceinline__ void excite(const ExciteCoefs2& k, int) {
 #pragma unroll
         for (int j = 0; j < KP; j++) {
             const float2 Pr = add2(ur[j], gr[j]), Pi = add2(ui[j], gi[j]);
             const float2 Qr = sub2(ur[j], gr[j]), Qn = sub2(gi[j], ui[j]);
-            const float2 Phr = fma2(k.A1, Pr, fma2(k.A2, Pi, mul2(k.dre, zr[j])));
+            const float2 Phr = REAL ? fma2(k.A1, Pr, mul2(k.A2, Pi)) : fma2(k.A1, Pr, fma2(k.A2, Pi, mul2(k.dre, zr[j])));
             const float2 Phi = fma2(k.A3, Pr, fma2(k.A4, Pi, mul2(k.dim, zr[j])));
             const float2 Qhr = fma2(k.A4, Qr, fma2(k.A3, Qn, mul2(k.dim, zn[j])));
-            const float2 nQhi = fma2(k.A2, Qr, fma2(k.A1, Qn, mul2(k.dre, zn[j])));
+            const float2 nQhi = REAL ? fma2(k.A2, Qr, mul2(k.A1, Qn)) : fma2(k.A2, Qr, fma2(k.A1, Qn, mul2(k.dre, zn[j])));
             const float2 nzr = fma2(k.ere, Pr, fma2(k.neim, Pi, mul2(k.f, zr[j])));
             const float2 nzn = fma2(k.ere, Qn, fma2(k.neim, Qr, mul2(k.f, zn[j])));
             ur[j] = add2(Phr, Qhr);
@@ -317,9 +331,11 @@ struct EPGPacked {
             zr[j] = nzr;
             zn[j] = nzn;
         }
-        ur[0].x += k.bre;
+        if constexpr (!REAL) {
+            ur[0].x += k.bre;
+            gr[0].x += k.bre;
+        }
         ui[0].x += k.bim;
-        gr[0].x += k.bre;
         gi[0].x += k.bim;
         zr[0].x += k.bz;
     }
@@ -526,10 +542,12 @@ __device__ __forceinline__ void handoff_wait(const int* flag, unsigned int* stat
 // tail's partial sums are published as soon as they are written and the head waits for the
 // predecessor's. Every tile's positions are still added one at a time in increasing order, so the
 // echoes are the same bits as with whole tiles per CTA.
-template<int K, int G, bool TAN = false, bool PACKED = false, bool BAL = false>
+// REAL (packed layouts only): every RF phase is real, the excitation without the d_re products.
+template<int K, int G, bool TAN = false, bool PACKED = false, bool BAL = false, bool REAL = false>
 __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_begin, const int item_end,
                                            float2* samples, const FispOrder* ord = nullptr) {
     static_assert(!PACKED || (G == 1 && K % 2 == 0 && !TAN), "packed layouts hold one voxel per lane");
+    static_assert(!REAL || PACKED, "the real-phase update is a packed-layout form");
     constexpr int VB = 32 / G;
     const int W = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -630,10 +648,10 @@ __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_beg
                         } else {
                             if constexpr (PACKED) {
                                 if (t == 0) {
-                                    st.excite(make_coefs2(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), sub);
+                                    st.template excite<REAL>(make_coefs2(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), sub);
                                 } else {
                                     st.shift(sub, a.N);
-                                    st.excite(make_coefs2(tv, B1, c_TR, E1_TR, beta), sub);
+                                    st.template excite<REAL>(make_coefs2(tv, B1, c_TR, E1_TR, beta), sub);
                                 }
                             } else {
                                 if (t == 0) {
@@ -722,10 +740,16 @@ __device__ __forceinline__ int2 cta_tile_range(int ntiles, int cta, int nctas) {
 // EPGPacked<K/2> (one lane per voxel).
 // BAL instantiates the balanced form (launched with non-null `handoff`), the others the whole-tile
 // form (`handoff` unused), so that each compiles to its own register allocation.
-template<int K, int G, bool PACKED = false, bool BAL = false>
+// REAL (packed layouts): the real-phase excitation. The host launches both forms of a packed layout;
+// each reads the sequence's phase flag and the one that does not match returns at once (a branch that
+// is uniform over the grid, so no host synchronisation picks the form and the pair can be captured).
+template<int K, int G, bool PACKED = false, bool BAL = false, bool REAL = false>
 __global__ void __launch_bounds__(256, 1) fisp_epg_kernel(FispArgs a, int ntiles, int* handoff, unsigned int* status) {
     extern __shared__ float2 samples[];  // [W][32][VB]
     if (a.skip != nullptr && *a.skip != 0) return;  // uniform over the grid
+    if constexpr (PACKED) {
+        if (fisp_real_phases(a) != REAL) return;
+    }
     if constexpr (BAL) {
         __shared__ FispOrder ord;
         const int64_t total = int64_t(ntiles) * a.P;
@@ -744,12 +768,12 @@ __global__ void __launch_bounds__(256, 1) fisp_epg_kernel(FispArgs a, int ntiles
             ord.status = status;
         }
         __syncthreads();
-        fisp_items<K, G, false, PACKED, true>(a, 0, n, samples, &ord);
+        fisp_items<K, G, false, PACKED, true, REAL>(a, 0, n, samples, &ord);
     } else {
         (void)handoff;
         (void)status;
         const int2 r = cta_tile_range(ntiles, blockIdx.x, gridDim.x);
-        fisp_items<K, G, false, PACKED>(a, r.x * a.P, r.y * a.P, samples);
+        fisp_items<K, G, false, PACKED, false, REAL>(a, r.x * a.P, r.y * a.P, samples);
     }
 }
 
@@ -823,15 +847,20 @@ struct FispConfig {
     FispValueKernel fn;
     FispQueueKernel queue;
     FispValueKernel balanced;  // the balanced item split (packed layouts), else null
+    // packed layouts: the real-phase forms of fn and balanced (launched beside them), else null
+    FispValueKernel fn_real;
+    FispValueKernel balanced_real;
 };
 
 // Instantiated layouts: (states per lane K, lanes per voxel/position G). Coverage K·G ≥ N.
 // The packed one-lane layouts come last, so the indices of the others (which a tuning table
 // names) keep their meaning.
-#define COMPAS_FISP(K, G) {K, G, false, kernels::fisp_epg_kernel<K, G>, kernels::fisp_queue_kernel<K, G>, nullptr}
+#define COMPAS_FISP(K, G) \
+    {K, G, false, kernels::fisp_epg_kernel<K, G>, kernels::fisp_queue_kernel<K, G>, nullptr, nullptr, nullptr}
 #define COMPAS_FISP_PACKED(K)                                                                         \
     {K, 1, true, kernels::fisp_epg_kernel<K, 1, true>, kernels::fisp_queue_kernel<K, 1, true>,      \
-     kernels::fisp_epg_kernel<K, 1, true, true>}
+     kernels::fisp_epg_kernel<K, 1, true, true>, kernels::fisp_epg_kernel<K, 1, true, false, true>,  \
+     kernels::fisp_epg_kernel<K, 1, true, true, true>}
 const FispConfig kFispConfigs[] = {
     COMPAS_FISP(1, 1), COMPAS_FISP(2, 1), COMPAS_FISP(4, 1), COMPAS_FISP(6, 1), COMPAS_FISP(8, 1),
     COMPAS_FISP(12, 1), COMPAS_FISP(16, 1), COMPAS_FISP(20, 1), COMPAS_FISP(25, 1),
@@ -930,9 +959,13 @@ const Array<float, 3>& fisp_excite_table(const CompasContext& ctx, const FISPSeq
         int nTR = int(seq.RF_train.size());
         int P = int(seq.sliceprofiles.size(0));
         COMPAS_CHECK(int(seq.sliceprofiles.size(1)) == nTR);
-        auto tab = std::make_shared<Array<float, 3>>(std::array<int64_t, 3> {P, nTR, 4}, ctx.device(), ctx.stream());
+        // rows 0..P-1: the entries; entry P·nTR (the start of row P): the flag of a complex phase
+        // (fisp_table_kernel). At least one entry per row, so the flag exists when nTR = 0.
+        auto tab = std::make_shared<Array<float, 3>>(std::array<int64_t, 3> {P + 1, std::max(nTR, 1), 4}, ctx.device(),
+                                                     ctx.stream());
         DeviceGuard guard(ctx.device());
         int n = nTR * P;
+        COMPAS_CUDA_CHECK(cudaMemsetAsync(tab->data() + int64_t(n) * 4, 0, sizeof(float4), ctx.stream()));
         if (n > 0) {
             kernels::fisp_table_kernel<<<div_ceil(n, 256), 256, 0, ctx.stream()>>>(
                 reinterpret_cast<const float2*>(seq.RF_train.data()),
@@ -1043,7 +1076,12 @@ void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int v
     const size_t smem = fisp_smem_bytes(cfg, W);
     DeviceGuard guard(ctx.device());
     allow_smem(reinterpret_cast<const void*>(cfg.fn), smem);
-    const int grid = std::min(ntiles, resident_ctas(reinterpret_cast<const void*>(cfg.fn), 32 * W, smem, ctx.device()));
+    int resident = resident_ctas(reinterpret_cast<const void*>(cfg.fn), 32 * W, smem, ctx.device());
+    if (cfg.fn_real != nullptr) {
+        allow_smem(reinterpret_cast<const void*>(cfg.fn_real), smem);
+        resident = std::min(resident, resident_ctas(reinterpret_cast<const void*>(cfg.fn_real), 32 * W, smem, ctx.device()));
+    }
+    const int grid = std::min(ntiles, resident);
     // The balanced split needs every CTA's share to span at least two tiles (so a CTA waits only on
     // its predecessor's first part, never on a chain), at most kFispBalancedItems items, and all
     // CTAs resident at once (the grid is at most one resident wave). It saves the idle tail of the
@@ -1053,13 +1091,16 @@ void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int v
     bool balanced = balance && cfg.balanced != nullptr && grid > 1 && int64_t(ntiles) >= 2 * int64_t(grid) &&
                     per_cta <= kernels::kFispBalancedItems && (handoff == nullptr || grid <= handoff_capacity);
     if (balanced) {
-        const void* bfn = reinterpret_cast<const void*>(cfg.balanced);
-        allow_smem(bfn, smem);
-        int per_sm = 0;
-        COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfn, 32 * W, smem));
         int sms = 148;
         COMPAS_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device()));
-        balanced = int64_t(per_sm) * sms >= grid;  // every CTA resident at once
+        for (FispValueKernel k : {cfg.balanced, cfg.balanced_real}) {
+            if (k == nullptr) continue;
+            const void* bfn = reinterpret_cast<const void*>(k);
+            allow_smem(bfn, smem);
+            int per_sm = 0;
+            COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfn, 32 * W, smem));
+            balanced = balanced && int64_t(per_sm) * sms >= grid;  // every CTA resident at once
+        }
     }
     std::optional<Array<int, 1>> flags;
     if (balanced) {
@@ -1068,11 +1109,21 @@ void launch_fisp(const CompasContext& ctx, const TissueParameters& params, int v
             handoff = flags->data();
         }
         COMPAS_CUDA_CHECK(cudaMemsetAsync(handoff, 0, sizeof(int) * size_t(grid), ctx.stream()));
+        // the form that does not match the sequence's phases returns without touching the flags
         cfg.balanced<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles, handoff, ctx.status_word());
+        check_launch("fisp_epg_kernel");
+        if (cfg.balanced_real != nullptr) {
+            cfg.balanced_real<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles, handoff, ctx.status_word());
+            check_launch("fisp_epg_kernel (real phases)");
+        }
     } else {
         cfg.fn<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles, nullptr, nullptr);
+        check_launch("fisp_epg_kernel");
+        if (cfg.fn_real != nullptr) {
+            cfg.fn_real<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles, nullptr, nullptr);
+            check_launch("fisp_epg_kernel (real phases)");
+        }
     }
-    check_launch("fisp_epg_kernel");
 }
 
 int fisp_tangent_config_count() {

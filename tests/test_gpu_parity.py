@@ -110,6 +110,41 @@ def test_fisp_deterministic(cb, ctx, workloads):
     assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("phase", [0.0, 0.3])
+def test_fisp_packed_layouts_match_scalar_bits(cb, ctx, workloads, phase):
+    # a packed layout runs the scalar update's operations on pairs of states. With real RF phases
+    # (phase 0: a real flip train and real slice profiles) it runs the form without the products of
+    # the coefficient d_re = sin φ·sin α·E1, which is then zero. Either way the echoes are the bits of
+    # the scalar layout (up to the sign of exact zeros, which array_equal ignores).
+    rng = np.random.default_rng(21)
+    ntr, P = 57, 4
+    rf = workloads.smooth_flip_train(rng, ntr) * np.exp(1j * phase * rng.uniform(-1, 1, ntr))
+    slices = workloads.gaussian_slice_profile(P, ntr)
+    p = workloads.tissue(rng, 9, 22.4)
+    p[3] = rng.uniform(-30, 30, p.shape[1])  # off-resonance: complex relaxation factors
+    params = cb.TissueParameters.from_soa(ctx, p)
+    configs = [tuple(c) for c in cb.fisp_configs()]
+    tried = 0
+    try:
+        for i, (k, g) in enumerate(configs):
+            if not cb.fisp_config_packed(i):
+                continue
+            scalar_ks = {c[0] for n, c in enumerate(configs) if c[1] == 1 and not cb.fisp_config_packed(n)}
+            twin = (k, 1) if k in scalar_ks else (k - 1, 1)  # 26 states packed, 25 scalar
+            j = next(n for n, c in enumerate(configs) if c == twin and not cb.fisp_config_packed(n))
+            for N in sorted({twin[0], twin[0] - 1}):
+                seq = cb.FispSequence.from_dict(ctx, workloads.fisp_sequence(rf, slices, 8.7e-3, 4.35e-3, 25e-3, N))
+                cb.set_fisp_launch(i, 4)
+                packed = cb.simulate_magnetization(ctx, params, seq).to_numpy()
+                cb.set_fisp_launch(j, 4)
+                scalar = cb.simulate_magnetization(ctx, params, seq).to_numpy()
+                assert np.array_equal(packed, scalar), (k, N, phase)
+                tried += 1
+    finally:
+        cb.set_fisp_launch(-1, -1)
+    assert tried >= 10
+
+
 def test_fisp_rejects_bad_state_count(cb, ctx, workloads):
     w = workloads.tiny()
     with pytest.raises(cb.CompasError):
