@@ -85,6 +85,7 @@ struct SimulationBatch::Impl {
         bool fisp;
         bool tangent;              // value and T1/T2 tangents (tangent layouts for FISP)
         int config, warps, cover;  // layout, warps (FISP), max_state / nz
+        bool real = false;         // FISP: every job's RF and slice-profile phases are real
         Array<unsigned char> args;
         Array<unsigned char> items;
         int nitems = 0;
@@ -124,9 +125,9 @@ struct SimulationBatch::Impl {
 void SimulationBatch::Impl::plan_simulation(Family& fam, bool fisp, const std::vector<int>& members) {
     // group by the launch the job would get alone
     struct Key {
-        int tangent, config, warps, cover;
+        int tangent, config, warps, cover, real;
         bool operator<(const Key& o) const {
-            return std::tie(tangent, config, warps, cover) < std::tie(o.tangent, o.config, o.warps, o.cover);
+            return std::tie(tangent, config, warps, cover, real) < std::tie(o.tangent, o.config, o.warps, o.cover, o.real);
         }
     };
     std::vector<std::pair<Key, int>> keyed;
@@ -145,13 +146,15 @@ void SimulationBatch::Impl::plan_simulation(Family& fam, bool fisp, const std::v
                 const FispLaunch L = tuned_fisp_launch(seq.max_state, V, P);
                 D = L.config < 0 ? fisp_default_launch(seq.max_state, V, P) : L;
             }
-            keyed.push_back({Key {tan, D.config, std::max(1, std::min(D.warps, 8)), seq.max_state}, j});
+            // jobs with real phases form their own groups, which a packed layout runs in its real-phase form
+            const int real = !tan && fisp_config_packed(D.config) && fisp_sequence_real_phases(ctx, seq) ? 1 : 0;
+            keyed.push_back({Key {tan, D.config, std::max(1, std::min(D.warps, 8)), seq.max_state, real}, j});
         } else {
             const auto& seq = std::get<pSSFPSequence>(job.sequence);
             const int nz = int(seq.z.size());
             const PssfpLaunch L = tuned_pssfp_launch(nz, job.parameters.nvoxels);
             const PssfpLaunch D = L.config < 0 ? pssfp_default_launch(nz, job.parameters.nvoxels) : L;
-            keyed.push_back({Key {tan, D.config, 0, nz}, j});
+            keyed.push_back({Key {tan, D.config, 0, nz, 0}, j});
         }
     }
     std::stable_sort(keyed.begin(), keyed.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
@@ -178,6 +181,7 @@ void SimulationBatch::Impl::plan_simulation(Family& fam, bool fisp, const std::v
         g.config = key.config;
         g.warps = key.warps;
         g.cover = key.cover;
+        g.real = key.real != 0;
         std::vector<int> items;
         if (fisp) {
             std::vector<kernels::FispArgs> args;
@@ -358,7 +362,7 @@ void SimulationBatch::Impl::enqueue(const Family& fam, cudaStream_t stream, int*
                                       as<kernels::FispArgs>(g.args), as<int2>(g.items), g.nitems, head_base + g.head);
         else if (g.fisp)
             launch_fisp_queue(stream, dev, FispLaunch {g.config, g.warps}, g.cover, as<kernels::FispArgs>(g.args),
-                              as<int2>(g.items), g.nitems, head_base + g.head);
+                              as<int2>(g.items), g.nitems, head_base + g.head, g.real);
         else if (g.tangent)
             launch_pssfp_tangent_queue(stream, dev, PssfpLaunch {g.config}, g.cover, as<kernels::PssfpArgs>(g.args),
                                        as<int2>(g.items), g.nitems, head_base + g.head);

@@ -780,7 +780,8 @@ __global__ void __launch_bounds__(256, 1) fisp_epg_kernel(FispArgs a, int ntiles
 // Persistent work-queue kernel for a batch of FISP simulations sharing one layout and W:
 // each CTA takes (job, tile) items from `items` in order through an atomic counter until the
 // queue is empty. Items are ordered longest job first, so the last wave is short.
-template<int K, int G, bool PACKED = false>
+// REAL (packed layouts): every job's phases are real, the real-phase excitation.
+template<int K, int G, bool PACKED = false, bool REAL = false>
 __global__ void __launch_bounds__(256, 1) fisp_queue_kernel(const FispArgs* __restrict__ jobs,
                                                             const int2* __restrict__ items, int nitems,
                                                             int* __restrict__ head) {
@@ -795,7 +796,7 @@ __global__ void __launch_bounds__(256, 1) fisp_queue_kernel(const FispArgs* __re
         const int2 w = items[it];
         if (threadIdx.x == 0) job = jobs[w.x];
         __syncthreads();
-        fisp_items<K, G, false, PACKED>(job, w.y * job.P, (w.y + 1) * job.P, samples);
+        fisp_items<K, G, false, PACKED, false, REAL>(job, w.y * job.P, (w.y + 1) * job.P, samples);
         __syncthreads();  // job and s_item are rewritten by the next item
     }
 }
@@ -847,20 +848,22 @@ struct FispConfig {
     FispValueKernel fn;
     FispQueueKernel queue;
     FispValueKernel balanced;  // the balanced item split (packed layouts), else null
-    // packed layouts: the real-phase forms of fn and balanced (launched beside them), else null
+    // packed layouts: the real-phase forms of fn and balanced (launched beside them) and of queue
+    // (launched instead of it for groups of real-phase jobs), else null
     FispValueKernel fn_real;
     FispValueKernel balanced_real;
+    FispQueueKernel queue_real;
 };
 
 // Instantiated layouts: (states per lane K, lanes per voxel/position G). Coverage K·G ≥ N.
 // The packed one-lane layouts come last, so the indices of the others (which a tuning table
 // names) keep their meaning.
 #define COMPAS_FISP(K, G) \
-    {K, G, false, kernels::fisp_epg_kernel<K, G>, kernels::fisp_queue_kernel<K, G>, nullptr, nullptr, nullptr}
+    {K, G, false, kernels::fisp_epg_kernel<K, G>, kernels::fisp_queue_kernel<K, G>, nullptr, nullptr, nullptr, nullptr}
 #define COMPAS_FISP_PACKED(K)                                                                         \
     {K, 1, true, kernels::fisp_epg_kernel<K, 1, true>, kernels::fisp_queue_kernel<K, 1, true>,      \
      kernels::fisp_epg_kernel<K, 1, true, true>, kernels::fisp_epg_kernel<K, 1, true, false, true>,  \
-     kernels::fisp_epg_kernel<K, 1, true, true, true>}
+     kernels::fisp_epg_kernel<K, 1, true, true, true>, kernels::fisp_queue_kernel<K, 1, true, true>}
 const FispConfig kFispConfigs[] = {
     COMPAS_FISP(1, 1), COMPAS_FISP(2, 1), COMPAS_FISP(4, 1), COMPAS_FISP(6, 1), COMPAS_FISP(8, 1),
     COMPAS_FISP(12, 1), COMPAS_FISP(16, 1), COMPAS_FISP(20, 1), COMPAS_FISP(25, 1),
@@ -976,8 +979,28 @@ const Array<float, 3>& fisp_excite_table(const CompasContext& ctx, const FISPSeq
         cache.table = tab;
         cache.key_rf = seq.RF_train.data();
         cache.key_sp = seq.sliceprofiles.data();
+        cache.real_phases = -1;
     }
     return *cache.table;
+}
+
+bool fisp_sequence_real_phases(const CompasContext& ctx, const FISPSequence& seq) {
+    const auto& tab = fisp_excite_table(ctx, seq);
+    auto& cache = *seq.cache;
+    std::lock_guard<std::mutex> lock(cache.mutex);
+    if (cache.real_phases < 0) {
+        cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+        COMPAS_CUDA_CHECK(cudaStreamIsCapturing(ctx.stream(), &capture));
+        if (capture != cudaStreamCaptureStatusNone) return false;  // the general form is right for every sequence
+        const int64_t flag_at = int64_t(seq.sliceprofiles.size(0)) * seq.RF_train.size() * 4;
+        float flag = 1.0f;
+        DeviceGuard guard(ctx.device());
+        COMPAS_CUDA_CHECK(cudaMemcpyAsync(&flag, tab.data() + flag_at, sizeof(float), cudaMemcpyDeviceToHost,
+                                          ctx.stream()));
+        COMPAS_CUDA_CHECK(cudaStreamSynchronize(ctx.stream()));
+        cache.real_phases = flag == 0.0f ? 1 : 0;
+    }
+    return cache.real_phases == 1;
 }
 
 kernels::FispArgs fisp_args(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
@@ -1208,18 +1231,19 @@ void launch_fisp_tangent_queue(cudaStream_t stream, int device, FispLaunch L, in
 }
 
 void launch_fisp_queue(cudaStream_t stream, int device, FispLaunch L, int max_state, const kernels::FispArgs* jobs,
-                       const int2* items, int nitems, int* head) {
+                       const int2* items, int nitems, int* head, bool real) {
     if (nitems <= 0) return;
     const auto& cfg = checked_config(L, max_state);
+    const FispQueueKernel fn = real && cfg.queue_real != nullptr ? cfg.queue_real : cfg.queue;
     const int W = std::max(1, std::min(L.warps, 8));
     const size_t smem = fisp_smem_bytes(cfg, W);
     DeviceGuard guard(device);
-    allow_smem(reinterpret_cast<const void*>(cfg.queue), smem);
+    allow_smem(reinterpret_cast<const void*>(fn), smem);
     int per_sm = 1, sms = 148;
-    COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.queue, 32 * W, smem));
+    COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * W, smem));
     COMPAS_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     const int grid = std::max(1, std::min(nitems, std::max(1, per_sm) * sms));
-    cfg.queue<<<grid, 32 * W, smem, stream>>>(jobs, items, nitems, head);
+    fn<<<grid, 32 * W, smem, stream>>>(jobs, items, nitems, head);
     check_launch("fisp_queue_kernel");
 }
 

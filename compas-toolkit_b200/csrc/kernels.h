@@ -20,6 +20,9 @@ bool fisp_config_packed(int index);  // EPGPacked layout (two states per FFMA2)
 FispLaunch fisp_default_launch(int N, int64_t nvoxels, int P);
 FispLaunch tuned_fisp_launch(int N, int64_t nvoxels, int P);
 const Array<float, 3>& fisp_excite_table(const CompasContext& ctx, const FISPSequence& seq);
+// whether every RF and slice-profile phase of the sequence is real (sin φ = 0), read back from its
+// excitation table: synchronises the context's stream the first time (not while it is captured)
+bool fisp_sequence_real_phases(const CompasContext& ctx, const FISPSequence& seq);
 // simulates voxels [voxel_begin, voxel_begin + nvoxels) of `params` into echo columns
 // voxel_begin.. of a [nTR*uf][echo_stride] complex array
 // `skip` (device int, may be null): when it holds a nonzero value at run time the kernel returns
@@ -36,9 +39,10 @@ kernels::FispArgs fisp_args(const CompasContext& ctx, const TissueParameters& pa
                             const FISPSequence& seq, cfloat* echo, int64_t echo_stride);
 int fisp_tile_voxels(FispLaunch L);  // voxels per work item (tile) of layout L
 // persistent work-queue launch over (job, tile) items of FISP jobs that all use layout L;
-// *head must be 0 when the kernel starts
+// *head must be 0 when the kernel starts. `real`: every job's phases are real
+// (fisp_sequence_real_phases), which a packed layout runs in its real-phase form.
 void launch_fisp_queue(cudaStream_t stream, int device, FispLaunch L, int max_state, const kernels::FispArgs* jobs,
-                       const int2* items, int nitems, int* head);
+                       const int2* items, int nitems, int* head, bool real = false);
 
 // value and T1/T2 tangents (forward mode) in one launch; L.config indexes the tangent layouts
 int fisp_tangent_config_count();

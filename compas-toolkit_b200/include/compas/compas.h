@@ -301,6 +301,7 @@ struct FISPSequence: public Object {
         const void* key_rf = nullptr;
         const void* key_sp = nullptr;
         std::shared_ptr<Array<float, 3>> table;
+        int real_phases = -1;  // host copy of the table's phase flag: -1 not read yet, else 0 / 1
     };
     std::shared_ptr<Cache> cache = std::make_shared<Cache>();
 };
