@@ -50,6 +50,7 @@ _SIGS = {
     "compas_destroy_array": ([_P], None),
     "compas_make_tissue_parameters": ([_P, _I] + [_P] * 9, _P),
     "compas_make_fisp_sequence": ([_P, _P, _F, _F, _F, _I, _F, _I, _I], _P),
+    "compas_b200_make_fisp_sequence_ex": ([_P, _P, _F, _F, _F, _I, _F, _I, _I, _I, _I], _P),
     "compas_make_pssfp_sequence": ([_P, _F, _P, _F, _F, _F, _F, _F, _F, _P], _P),
     "compas_make_cartesian_trajectory": ([_I, _I, _F, _P, _F], _P),
     "compas_make_spiral_trajectory": ([_I, _I, _F, _P, _P], _P),
@@ -314,14 +315,22 @@ class TissueParameters(_Object):
 
 
 class FispSequence(_Object):
-    """compas_make_fisp_sequence: RF train [nTR] (deg, phase), slice profiles [npos][nTR]."""
+    """compas_make_fisp_sequence: RF train [nTR] (deg, phase), slice profiles [npos][nTR]. Without the
+    inversion prepulse or the wait spoiling (both on in the reference's C ABI) it is built by
+    compas_b200_make_fisp_sequence_ex."""
 
     def __init__(self, context: Context, RF_train, slice_profiles, TR: float, TE: float, max_state: int, TI: float,
-                 undersampling_factor: int = 1, repetitions: int = 1, TW: float = 0.0):
+                 undersampling_factor: int = 1, repetitions: int = 1, TW: float = 0.0,
+                 inversion_prepulse: bool = True, wait_spoiling: bool = True):
         rf = _arr(context, np.asarray(RF_train, np.complex64))
         sp = _arr(context, np.asarray(slice_profiles, np.complex64).reshape(-1, rf.shape[0]))
-        ptr = library().compas_make_fisp_sequence(rf.ptr, sp.ptr, TR, TE, TW, int(max_state), TI,
-                                                  int(undersampling_factor), int(repetitions))
+        if inversion_prepulse and wait_spoiling:
+            ptr = library().compas_make_fisp_sequence(rf.ptr, sp.ptr, TR, TE, TW, int(max_state), TI,
+                                                      int(undersampling_factor), int(repetitions))
+        else:
+            ptr = library().compas_b200_make_fisp_sequence_ex(rf.ptr, sp.ptr, TR, TE, TW, int(max_state), TI,
+                                                              int(undersampling_factor), int(repetitions),
+                                                              int(bool(inversion_prepulse)), int(bool(wait_spoiling)))
         super().__init__(ptr, (rf, sp))
         self.nreadouts = rf.shape[0] * int(undersampling_factor)
         self.max_state = int(max_state)
@@ -330,7 +339,8 @@ class FispSequence(_Object):
     @staticmethod
     def from_dict(context: Context, s: dict) -> "FispSequence":
         return FispSequence(context, s["rf"], s["slices"], s["TR"], s["TE"], s["max_state"], s["TI"],
-                            s.get("uf", 1), s.get("reps", 1), s.get("TW", 0.0))
+                            s.get("uf", 1), s.get("reps", 1), s.get("TW", 0.0), bool(s.get("inversion", 1)),
+                            bool(s.get("wait_spoil", 1)))
 
 
 class pSSFPSequence(_Object):

@@ -241,17 +241,40 @@ const compas_object* compas_make_tissue_parameters(const compas_context* context
     });
 }
 
+namespace {
+
+// bindings.cpp:151-174 with the C++ sequence's two flags (compas/sequences/fisp.h:37-41)
+compas_object* make_fisp(const compas_array* RF_train, const compas_array* sliceprofiles, float TR, float TE, float TW,
+                         int max_state, float TI, int undersampling_factor, int repetitions, bool inversion_prepulse,
+                         bool wait_spoiling) {
+    const auto& rf = array_of<cfloat, 1>(RF_train, "RF_train");
+    const auto& sp = array_of<cfloat, 2>(sliceprofiles, "sliceprofiles");
+    if (sp.size(1) != rf.size(0)) throw compas::CompasException("sliceprofiles must be [npositions][nTR]");
+    if (max_state < 1 || max_state > 128) throw compas::CompasException("max_state must be in [1, 128]");
+    if (undersampling_factor < 1 || repetitions < 1)
+        throw compas::CompasException("undersampling_factor and repetitions must be >= 1");
+    return new_obj(compas::FISPSequence(rf, sp, TR, TE, TW, max_state, TI, undersampling_factor, repetitions,
+                                        inversion_prepulse, wait_spoiling));
+}
+
+}  // namespace
+
 compas_object* compas_make_fisp_sequence(const compas_array* RF_train, const compas_array* sliceprofiles, float TR,
                                          float TE, float TW, int max_state, float TI, int undersampling_factor,
                                          int repetitions) {
     return guarded([&]() -> compas_object* {
-        const auto& rf = array_of<cfloat, 1>(RF_train, "RF_train");
-        const auto& sp = array_of<cfloat, 2>(sliceprofiles, "sliceprofiles");
-        if (sp.size(1) != rf.size(0)) throw compas::CompasException("sliceprofiles must be [npositions][nTR]");
-        if (max_state < 1 || max_state > 128) throw compas::CompasException("max_state must be in [1, 128]");
-        if (undersampling_factor < 1 || repetitions < 1)
-            throw compas::CompasException("undersampling_factor and repetitions must be >= 1");
-        return new_obj(compas::FISPSequence(rf, sp, TR, TE, TW, max_state, TI, undersampling_factor, repetitions));
+        return make_fisp(RF_train, sliceprofiles, TR, TE, TW, max_state, TI, undersampling_factor, repetitions, true,
+                         true);
+    });
+}
+
+compas_object* compas_b200_make_fisp_sequence_ex(const compas_array* RF_train, const compas_array* sliceprofiles,
+                                                float TR, float TE, float TW, int max_state, float TI,
+                                                int undersampling_factor, int repetitions, int inversion_prepulse,
+                                                int wait_spoiling) {
+    return guarded([&]() -> compas_object* {
+        return make_fisp(RF_train, sliceprofiles, TR, TE, TW, max_state, TI, undersampling_factor, repetitions,
+                         inversion_prepulse != 0, wait_spoiling != 0);
     });
 }
 

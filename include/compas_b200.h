@@ -140,6 +140,15 @@ COMPAS_API int compas_b200_simulate_magnetization_tangents(const compas_context*
                                                 const compas_object* sequence, compas_array** echos,
                                                 compas_array** delta_echos_T1, compas_array** delta_echos_T2);
 
+/* compas_make_fisp_sequence with the two flags of the C++ FISPSequence that the reference's C ABI
+ * leaves at their defaults (compas/sequences/fisp.h:37-41; bindings.cpp:151-174 always builds the
+ * sequence with both true): the inversion prepulse at the start of every repetition and the spoiling
+ * before the wait TW. Nonzero = on. Same ownership and errors as compas_make_fisp_sequence. */
+COMPAS_API compas_object* compas_b200_make_fisp_sequence_ex(const compas_array* RF_train,
+                                                  const compas_array* sliceprofiles, float TR, float TE, float TW,
+                                                  int max_state, float TI, int undersampling_factor,
+                                                  int repetitions, int inversion_prepulse, int wait_spoiling);
+
 /* Explicit-method variants of the signal and Jacobian entry points: `method` takes the
  * reference's enum values SimulateSignalMethod {Naive=0, Direct, MatmulPedantic, Matmul,
  * MatmulFast, MatmulLow} (compas/trajectories/signal.h:14-44) and JacobianComputeMethod

@@ -145,6 +145,28 @@ def test_fisp_packed_layouts_match_scalar_bits(cb, ctx, workloads, phase):
     assert tried >= 10
 
 
+@pytest.mark.parametrize("inversion,wait_spoil", [(0, 1), (1, 0), (0, 0)])
+def test_fisp_sequence_flags(cb, ctx, oracle, workloads, inversion, wait_spoil):
+    # the C++ sequence's inversion prepulse and wait spoiling, off (compas_b200_make_fisp_sequence_ex),
+    # with repetitions so that the wait and the next repetition's start matter
+    w = workloads.tiny(n_side=6, ntr=31, P=3, max_state=9, seed=5)
+    w["seq"].update(reps=3, TW=0.04, inversion=inversion, wait_spoil=wait_spoil)
+    params, seq, _ = _upload(cb, ctx, w)
+    got = cb.simulate_magnetization(ctx, params, seq).to_numpy()
+    ref = oracle.fisp(w["params"], w["seq"])
+    assert oracle.rel_l2(got, ref) < TOL_FP32
+    both = oracle.fisp(w["params"], dict(w["seq"], inversion=1, wait_spoil=1))
+    if not inversion:
+        assert oracle.rel_l2(ref, both) > 1e-3  # the case differs from the C ABI's default sequence
+    # (with the inversion, which spoils, the wait spoiling changes nothing: F states do not feed Z
+    # without RF)
+    tan = cb.simulate_magnetization_tangents(ctx, params, seq)
+    assert oracle.rel_l2(tan["echos"].to_numpy(), got) < 1e-6
+    for f, field in (("T1", 0), ("T2", 1)):
+        d = oracle.derivative_central(oracle.fisp, w["params"], w["seq"], field)
+        assert oracle.rel_l2(tan[f].to_numpy(), d) < TOL_FP32, f
+
+
 def test_fisp_rejects_bad_state_count(cb, ctx, workloads):
     w = workloads.tiny()
     with pytest.raises(cb.CompasError):
@@ -161,17 +183,19 @@ def test_fisp_rejects_bad_state_count(cb, ctx, workloads):
 @pytest.mark.parametrize("kind", ["fisp", "pssfp"])
 def test_simulation_matches_reference_kernels(cb, ctx, ref_simulations, oracle, kind):
     # golden echoes of the reference's FISP / pSSFP kernels (run on the CPU in FP32); both FP32
-    # results lie within 1e-5 of the FP64 oracle, so they agree to 2e-5. The C ABI's FISP sequence
-    # always has the inversion prepulse and wait spoiling, so cases without them are skipped here.
-    tried = 0
+    # results lie within 1e-5 of the FP64 oracle, so they agree to 2e-5. FISP cases without the
+    # inversion prepulse or the wait spoiling (which the reference's C ABI always sets) are built
+    # through compas_b200_make_fisp_sequence_ex.
+    tried, flagless = 0, 0
     for i, (p, seq, echos) in enumerate(ref_simulations[kind]):
-        if kind == "fisp" and not (seq["inversion"] and seq["wait_spoil"]):
-            continue
         s = (cb.FispSequence if kind == "fisp" else cb.pSSFPSequence).from_dict(ctx, seq)
         got = cb.simulate_magnetization(ctx, cb.TissueParameters.from_soa(ctx, p), s).to_numpy()
         assert oracle.rel_l2(got, echos) < 2e-5, (kind, i)
         tried += 1
+        flagless += kind == "fisp" and not (seq["inversion"] and seq["wait_spoil"])
     assert tried >= 3
+    if kind == "fisp":
+        assert flagless >= 1
 
 
 def test_operators_match_reference_kernels(cb, ctx, ref_simulations, oracle):
