@@ -435,7 +435,10 @@ __global__ void __launch_bounds__(TS_THREADS, 1) tc_spiral_kernel(TsArgs a) {
 int spiral_table_chunk(int64_t per_readout_bytes, int R) {
     int64_t budget = int64_t(1) << 30;
     if (const char* e = std::getenv("COMPAS_B200_SPIRAL_TABLE_BYTES")) budget = std::max<int64_t>(1, std::atoll(e));
-    return int(std::max<int64_t>(1, std::min<int64_t>(R, budget / std::max<int64_t>(1, per_readout_bytes))));
+    const int64_t most = std::max<int64_t>(1, std::min<int64_t>(R, budget / std::max<int64_t>(1, per_readout_bytes)));
+    // as many chunks as the budget needs, of equal size (759 readouts: 380 + 379, not 559 + 200)
+    const int64_t nchunks = std::max<int64_t>(1, (int64_t(R) + most - 1) / most);
+    return int(std::max<int64_t>(1, (int64_t(R) + nchunks - 1) / nchunks));
 }
 
 // voxel splits of the spiral signal / J·v contraction: at least enough for ≤ 512 K16 steps each

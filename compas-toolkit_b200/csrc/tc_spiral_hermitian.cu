@@ -387,23 +387,38 @@ __global__ void __launch_bounds__(TX_THREADS, 1) tc_spiral_hermitian_kernel(TxAr
 }  // namespace kernels
 
 // readout splits within one readout chunk of the spiral Jᴴ·v contraction: the tuned count (at most
-// one readout each), else enough CTAs to fill the GPU twice (≥ 4 readouts each); returned as the
-// count the launch runs (every split non-empty). Each readout's accumulation is drained separately,
-// so the count changes only the partial sums.
+// one readout each), else the fewest splits, each of at least 4 readouts, whose grid of voxel tiles ×
+// coil groups × splits (one CTA per SM) spans two waves or more with the last wave at least 95 %
+// full, or failing that the best-filled grid of at most 16 splits (30000 voxels at 16 coils: 470
+// CTAs per split are 3.2 waves, 79 % of the SM time in use; 3 splits: 9.5 waves, 95 %). Returned as
+// the count the launches run (every split non-empty). Each readout's accumulation is drained
+// separately, so the count changes only the partial sums.
 int tc_spiral_hermitian_splits(int device, int nvoxels, int R, int S, int C) {
     const int T = div_ceil(std::max(S, 1), kernels::TX_M);
     const int chunk = spiral_table_chunk(int64_t(T) * nvoxels * int64_t(sizeof(float2)), R);
     const TcTuning tuning = tuned_tc(TcKind::SpiralHermitian, R, nvoxels, int64_t(C) * S);
-    int splits;
+    int splits = 1;
     if (tuning.splits > 0) {
         splits = std::max(1, std::min(tuning.splits, chunk));
     } else {
-        const int groups = div_ceil(C, kernels::TX_CTMAX);
-        const int vtiles = div_ceil(nvoxels, kernels::TX_M);
+        const int64_t base = int64_t(div_ceil(C, kernels::TX_CTMAX)) * div_ceil(std::max(nvoxels, 1), kernels::TX_M);
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        const int want = div_ceil(2 * sms, vtiles * groups);
-        splits = std::max(1, std::min(want, div_ceil(chunk, 4)));
+        const int most = std::max(1, std::min(16, div_ceil(chunk, 4)));
+        double best_fill = -1.0;
+        for (int s = 1; s <= most; s++) {
+            const int64_t ctas = base * s;
+            const int64_t waves = (ctas + sms - 1) / sms;
+            const double fill = double(ctas) / double(waves * sms);
+            if (ctas >= 2 * sms && fill >= 0.95) {
+                splits = s;
+                break;
+            }
+            if (fill > best_fill + 1e-9) {
+                best_fill = fill;
+                splits = s;
+            }
+        }
     }
     return div_ceil(chunk, div_ceil(chunk, splits));
 }
@@ -448,10 +463,16 @@ bool launch_jacobian_hermitian_spiral_tc(const CompasContext& ctx, const float* 
     const int chunk = spiral_table_chunk(int64_t(T) * nvoxels * int64_t(sizeof(float2)), nreadouts);
     const int nchunks = div_ceil(nreadouts, chunk);
     const int splits = tc_spiral_hermitian_splits(ctx.device(), nvoxels, nreadouts, ns, ncoils);
-    a.readouts_per_split = div_ceil(chunk, splits);
-    a.nsplit_launch = div_ceil(chunk, a.readouts_per_split);
-    const int partials_per_chunk = groups * a.nsplit_launch;
-    const int nparts = nchunks * partials_per_chunk;
+    // per chunk: its readouts in `splits` near-equal parts (the last chunk may be a readout shorter)
+    auto chunk_splits = [&](int rc, int* per_split) {
+        *per_split = div_ceil(rc, std::min(splits, rc));
+        return div_ceil(rc, *per_split);
+    };
+    int nparts = 0;
+    for (int ci = 0; ci < nchunks; ci++) {
+        int per_split = 0;
+        nparts += groups * chunk_splits(std::min(chunk, nreadouts - ci * chunk), &per_split);
+    }
     Array<cfloat, 2> partials({nparts > 1 ? nparts : 0, n}, ctx.device(), ctx.stream());
     a.out = reinterpret_cast<float2*>(nparts > 1 ? partials.data() : JHv);
     Array<cfloat, 2> table({std::min(chunk, nreadouts), int64_t(T) * nvoxels}, ctx.device(), ctx.stream());
@@ -461,17 +482,19 @@ bool launch_jacobian_hermitian_spiral_tc(const CompasContext& ctx, const float* 
         COMPAS_CUDA_CHECK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kernels::tc_spiral_hermitian_kernel),
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, kernels::TX_SMEM));
     });
+    a.partial0 = 0;
     for (int ci = 0; ci < nchunks; ci++) {
         a.r_first = ci * chunk;
         const int rc = std::min(chunk, nreadouts - a.r_first);
         a.r_end = a.r_first + rc;
-        a.partial0 = ci * partials_per_chunk;
+        a.nsplit_launch = chunk_splits(rc, &a.readouts_per_split);
         kernels::tc_spiral_hermitian_prep_kernel<<<dim3(div_ceil(nvoxels, 128), rc), 128, 0, ctx.stream()>>>(
             a, reinterpret_cast<float2*>(table.data()));
-        // splits past the chunk's last readout get no readouts and write zeros
+        // every split of the launch has readouts (chunk_splits)
         kernels::tc_spiral_hermitian_kernel<<<dim3(vtiles, groups, a.nsplit_launch), kernels::TX_THREADS,
                                               kernels::TX_SMEM, ctx.stream()>>>(a);
         check_launch("tc_spiral_hermitian_kernel");
+        a.partial0 += groups * a.nsplit_launch;
     }
     if (nparts > 1) sum_partials(ctx, partials.data(), nparts, n, JHv);
     return true;
