@@ -85,7 +85,7 @@ struct SimulationBatch::Impl {
         bool fisp;
         bool tangent;              // value and T1/T2 tangents (tangent layouts for FISP)
         int config, warps, cover;  // layout, warps (FISP), max_state / nz
-        bool real = false;         // FISP: every job's RF and slice-profile phases are real
+        bool real = false;         // every job's RF is real (FISP: RF and slice-profile phases)
         Array<unsigned char> args;
         Array<unsigned char> items;
         int nitems = 0;
@@ -154,7 +154,9 @@ void SimulationBatch::Impl::plan_simulation(Family& fam, bool fisp, const std::v
             const int nz = int(seq.z.size());
             const PssfpLaunch L = tuned_pssfp_launch(nz, job.parameters.nvoxels);
             const PssfpLaunch D = L.config < 0 ? pssfp_default_launch(nz, job.parameters.nvoxels) : L;
-            keyed.push_back({Key {tan, D.config, 0, nz, 0}, j});
+            // jobs with real RF form their own groups, which a packed layout runs in its real-RF form
+            const int real = pssfp_config_packed(D.config) && pssfp_sequence_real_rf(ctx, seq) ? 1 : 0;
+            keyed.push_back({Key {tan, D.config, 0, nz, real}, j});
         }
     }
     std::stable_sort(keyed.begin(), keyed.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
@@ -365,10 +367,10 @@ void SimulationBatch::Impl::enqueue(const Family& fam, cudaStream_t stream, int*
                               as<int2>(g.items), g.nitems, head_base + g.head, g.real);
         else if (g.tangent)
             launch_pssfp_tangent_queue(stream, dev, PssfpLaunch {g.config}, g.cover, as<kernels::PssfpArgs>(g.args),
-                                       as<int2>(g.items), g.nitems, head_base + g.head);
+                                       as<int2>(g.items), g.nitems, head_base + g.head, g.real);
         else
             launch_pssfp_queue(stream, dev, PssfpLaunch {g.config}, g.cover, as<kernels::PssfpArgs>(g.args),
-                               as<int2>(g.items), g.nitems, head_base + g.head);
+                               as<int2>(g.items), g.nitems, head_base + g.head, g.real);
     }
     for (int j : fam.empty_signals)
         COMPAS_CUDA_CHECK(cudaMemsetAsync(signals[size_t(j)].data(), 0, signals[size_t(j)].nbytes(), stream));

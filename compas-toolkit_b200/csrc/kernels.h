@@ -76,10 +76,16 @@ int pssfp_tile_voxels(PssfpLaunch L);
 void launch_pssfp_tangent(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
                           const pSSFPSequence& seq, cfloat* echo, cfloat* dT1, cfloat* dT2, int64_t echo_stride,
                           PssfpLaunch L);
+// work-queue launches over (job, tile) items of pSSFP jobs that all use layout L; `real`: every job's
+// RF is real (pssfp_sequence_real_rf), which a packed layout runs in its real-RF form
 void launch_pssfp_tangent_queue(cudaStream_t stream, int device, PssfpLaunch L, int nz,
-                                const kernels::PssfpArgs* jobs, const int2* items, int nitems, int* head);
+                                const kernels::PssfpArgs* jobs, const int2* items, int nitems, int* head,
+                                bool real = false);
 void launch_pssfp_queue(cudaStream_t stream, int device, PssfpLaunch L, int nz, const kernels::PssfpArgs* jobs,
-                        const int2* items, int nitems, int* head);
+                        const int2* items, int nitems, int* head, bool real = false);
+// whether every RF sample of the sequence (RF train × waveform) is real, read back from its rotation
+// table: synchronises the context's stream the first time (not while it is captured)
+bool pssfp_sequence_real_rf(const CompasContext& ctx, const pSSFPSequence& seq);
 
 // ---- signal / Jacobian products ----------------------------------------------------------
 enum class Precision { FP32, SplitBF16 };

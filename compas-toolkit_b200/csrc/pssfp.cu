@@ -29,13 +29,24 @@ namespace compas {
 namespace kernels {
 
 // zap[0][i] = -(RF[0]/2)·γΔtRF[i] (the α/2 pulse), zap[1+t][i] = RF[t]·γΔtRF[i]
+// zap[row][i] for rows 0..nTR, and after them, at entry (nTR + 1)·nRF, the flag of a complex RF
+// axis: x = 1 when some entry has Im zap ≠ 0, else 0 (zeroed before the launch)
 __global__ void pssfp_table_kernel(const float2* __restrict__ rf, int nTR, const float2* __restrict__ g, int nRF,
                                    float2* __restrict__ zap) {
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (nTR + 1) * nRF) return;
     int row = idx / nRF, i = idx % nRF;
     float2 th = row == 0 ? make_float2(-rf[0].x / 2.0f, -rf[0].y / 2.0f) : rf[row - 1];
-    zap[idx] = cmul(th, g[i]);
+    const float2 v = cmul(th, g[i]);
+    zap[idx] = v;
+    if (v.y != 0.0f) zap[int64_t(nTR + 1) * nRF].x = 1.0f;  // every writer stores the same value
+}
+
+// True when every RF sample of the sequence is real (Im zap = 0: a real RF train, as with 0-π phase
+// cycling, and a real waveform). The rotation axis then has a_y = ±0 and the packed update leaves
+// out its products (pssfp_tile_packed<…, REAL>).
+__device__ __forceinline__ bool pssfp_real_rf(const PssfpArgs& a) {
+    return __ldg(&a.zap[int64_t(a.nTR + 1) * a.nRF].x) == 0.0f;
 }
 
 
@@ -287,7 +298,11 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
 // those of the scalar update in the same order, and the z sums run over the slots in the scalar
 // order, so layout (ZP pairs, GZ lanes) gives the same bits as the scalar (2·ZP, GZ), tangents (TAN)
 // included.
-template<int ZP, int GZ, bool TAN = false>
+// REAL (every RF sample real, pssfp_real_rf): a_y = ±0, so the products a_y·m_z in the cross product's
+// x, a_y·m_x in its z, a_y·m_y in a·m and hd·a_y in the new m_y are left out: 23 instructions per pair
+// and RF sample instead of 27 (value; the same four per tangent). An FMA that adds ±0 to a product
+// returns the rounded product, so the results are the same bits up to the sign of an exact zero.
+template<int ZP, int GZ, bool TAN = false, bool REAL = false>
 __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int tile) {
     constexpr int ZT = 2 * ZP;
     const int lane = threadIdx.x & 31;
@@ -368,23 +383,26 @@ __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int 
                     sn = make_float2(q0.s, q1.s);
                     h = make_float2(q0.h, q1.h);
                 }
-                const float2 cx = fma2(AY, mz[p], mul2(naz[p], my[p]));
+                const float2 cx = REAL ? mul2(naz[p], my[p]) : fma2(AY, mz[p], mul2(naz[p], my[p]));
                 const float2 cy = fma2(az[p], mx[p], mul2(NAX, mz[p]));
-                const float2 cz = fma2(AX, my[p], mul2(NAY, mx[p]));
-                const float2 hd = mul2(h, fma2(AX, mx[p], fma2(AY, my[p], mul2(az[p], mz[p]))));
+                const float2 cz = REAL ? mul2(AX, my[p]) : fma2(AX, my[p], mul2(NAY, mx[p]));
+                const float2 hd = REAL ? mul2(h, fma2(AX, mx[p], mul2(az[p], mz[p])))
+                                       : mul2(h, fma2(AX, mx[p], fma2(AY, my[p], mul2(az[p], mz[p]))));
                 mx[p] = fma2(c, mx[p], fma2(sn, cx, mul2(hd, AX)));
-                my[p] = fma2(c, my[p], fma2(sn, cy, mul2(hd, AY)));
+                my[p] = REAL ? fma2(c, my[p], mul2(sn, cy)) : fma2(c, my[p], fma2(sn, cy, mul2(hd, AY)));
                 mz[p] = fma2(RX, fma2(c, mz[p], fma2(sn, cz, mul2(hd, az[p]))), ONE_E1X);
                 if constexpr (TAN) {
                     // the same map on the tangents plus the explicit terms at the new state:
                     // (0, 0, t/T1²·(m'_z - 1)) for T1, (t/T2²·m'_x, t/T2²·m'_y, 0) for T2
                     auto rotate = [&](float2& x, float2& yv, float2& z, float2 px, float2 py, float2 pz) {
-                        const float2 tx = fma2(AY, z, mul2(naz[p], yv));
+                        const float2 tx = REAL ? mul2(naz[p], yv) : fma2(AY, z, mul2(naz[p], yv));
                         const float2 ty = fma2(az[p], x, mul2(NAX, z));
-                        const float2 tz = fma2(AX, yv, mul2(NAY, x));
-                        const float2 td = mul2(h, fma2(AX, x, fma2(AY, yv, mul2(az[p], z))));
+                        const float2 tz = REAL ? mul2(AX, yv) : fma2(AX, yv, mul2(NAY, x));
+                        const float2 td = REAL ? mul2(h, fma2(AX, x, mul2(az[p], z)))
+                                               : mul2(h, fma2(AX, x, fma2(AY, yv, mul2(az[p], z))));
                         x = fma2(c, x, fma2(sn, tx, fma2(td, AX, px)));
-                        yv = fma2(c, yv, fma2(sn, ty, fma2(td, AY, py)));
+                        // REAL: fma2(td, ±0, py) is py exactly (py is a product or ±0)
+                        yv = REAL ? fma2(c, yv, fma2(sn, ty, py)) : fma2(c, yv, fma2(sn, ty, fma2(td, AY, py)));
                         z = fma2(RX, fma2(c, z, fma2(sn, tz, mul2(td, az[p]))), pz);
                     };
                     rotate(ax1[p], ay1[p], az1[p], bcast2(0.0f), bcast2(0.0f), mul2(S1EX, add2(mz[p], NEG1)));
@@ -472,25 +490,36 @@ __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int 
     }
 }
 
-// PACKED: ZT/2 pairs of isochromats per lane in the two-wide layout (pssfp_tile_packed)
-template<int ZT, int GZ, bool PACKED = false>
+// PACKED: ZT/2 pairs of isochromats per lane in the two-wide layout (pssfp_tile_packed). REAL: its
+// real-RF form; the host launches both forms of a packed layout back to back, each reads the table's
+// flag and the one that does not match returns at once (uniform over the grid).
+template<int ZT, int GZ, bool PACKED = false, bool REAL = false>
 __global__ void __launch_bounds__(128) pssfp_kernel(PssfpArgs a) {
     if (a.skip != nullptr && *a.skip != 0) return;  // uniform over the grid
-    if constexpr (PACKED) pssfp_tile_packed<ZT / 2, GZ>(a, blockIdx.x);
-    else pssfp_tile<ZT, GZ>(a, blockIdx.x);
+    if constexpr (PACKED) {
+        if (pssfp_real_rf(a) != REAL) return;
+        pssfp_tile_packed<ZT / 2, GZ, false, REAL>(a, blockIdx.x);
+    } else {
+        pssfp_tile<ZT, GZ>(a, blockIdx.x);
+    }
 }
 
 // One pSSFP simulation with its T1 and T2 tangents into a.echo, a.dT1, a.dT2.
-template<int ZT, int GZ, bool PACKED = false>
+template<int ZT, int GZ, bool PACKED = false, bool REAL = false>
 __global__ void __launch_bounds__(128) pssfp_tangent_kernel(PssfpArgs a) {
-    if constexpr (PACKED) pssfp_tile_packed<ZT / 2, GZ, true>(a, blockIdx.x);
-    else pssfp_tile<ZT, GZ, true>(a, blockIdx.x);
+    if constexpr (PACKED) {
+        if (pssfp_real_rf(a) != REAL) return;
+        pssfp_tile_packed<ZT / 2, GZ, true, REAL>(a, blockIdx.x);
+    } else {
+        pssfp_tile<ZT, GZ, true>(a, blockIdx.x);
+    }
 }
 
 // Persistent work-queue kernel for a batch of pSSFP simulations sharing one (ZT, GZ) layout:
 // CTAs of 128 threads take (job, tile) items, longest job first, through an atomic counter.
-// TAN: the value and T1/T2 tangents (pssfp_tangent_kernel's work).
-template<int ZT, int GZ, bool TAN = false, bool PACKED = false>
+// TAN: the value and T1/T2 tangents (pssfp_tangent_kernel's work). REAL: every job's RF is real (the
+// host groups jobs by their table's flag).
+template<int ZT, int GZ, bool TAN = false, bool PACKED = false, bool REAL = false>
 __global__ void __launch_bounds__(128) pssfp_queue_kernel(const PssfpArgs* __restrict__ jobs,
                                                           const int2* __restrict__ items, int nitems,
                                                           int* __restrict__ head) {
@@ -504,7 +533,7 @@ __global__ void __launch_bounds__(128) pssfp_queue_kernel(const PssfpArgs* __res
         const int2 w = items[it];
         if (threadIdx.x == 0) job = jobs[w.x];
         __syncthreads();
-        if constexpr (PACKED) pssfp_tile_packed<ZT / 2, GZ, TAN>(job, w.y);
+        if constexpr (PACKED) pssfp_tile_packed<ZT / 2, GZ, TAN, REAL>(job, w.y);
         else pssfp_tile<ZT, GZ, TAN>(job, w.y);
         __syncthreads();
     }
@@ -522,18 +551,29 @@ struct PssfpConfig {
     PssfpKernel tangent;
     PssfpQueueKernel tangent_queue;
     bool packed;  // two-wide layout (ZT/2 pairs of isochromats per lane), value and tangent kernels
+    // the real-RF forms (packed layouts, else null): fn_real and tangent_real launched beside fn and
+    // tangent, the queue forms instead of theirs for groups of real-RF jobs
+    PssfpKernel fn_real;
+    PssfpQueueKernel queue_real;
+    PssfpKernel tangent_real;
+    PssfpQueueKernel tangent_queue_real;
 };
 #define COMPAS_PSSFP(ZT, GZ)                                                                        \
     {ZT, GZ, kernels::pssfp_kernel<ZT, GZ>, kernels::pssfp_queue_kernel<ZT, GZ>,                 \
-     kernels::pssfp_tangent_kernel<ZT, GZ>, kernels::pssfp_queue_kernel<ZT, GZ, true>, false}
+     kernels::pssfp_tangent_kernel<ZT, GZ>, kernels::pssfp_queue_kernel<ZT, GZ, true>, false,     \
+     nullptr, nullptr, nullptr, nullptr}
 #define COMPAS_PSSFP_PACKED(ZT, GZ)                                                                 \
     {ZT, GZ, kernels::pssfp_kernel<ZT, GZ, true>, kernels::pssfp_queue_kernel<ZT, GZ, false, true>, \
-     kernels::pssfp_tangent_kernel<ZT, GZ, true>, kernels::pssfp_queue_kernel<ZT, GZ, true, true>, true}
+     kernels::pssfp_tangent_kernel<ZT, GZ, true>, kernels::pssfp_queue_kernel<ZT, GZ, true, true>, true, \
+     kernels::pssfp_kernel<ZT, GZ, true, true>, kernels::pssfp_queue_kernel<ZT, GZ, false, true, true>, \
+     kernels::pssfp_tangent_kernel<ZT, GZ, true, true>, kernels::pssfp_queue_kernel<ZT, GZ, true, true, true>}
 // packed value kernels with the scalar tangent kernels (the same bits; for layouts whose three packed
 // vectors would not fit the registers)
 #define COMPAS_PSSFP_PACKED_VALUE(ZT, GZ)                                                           \
     {ZT, GZ, kernels::pssfp_kernel<ZT, GZ, true>, kernels::pssfp_queue_kernel<ZT, GZ, false, true>, \
-     kernels::pssfp_tangent_kernel<ZT, GZ>, kernels::pssfp_queue_kernel<ZT, GZ, true>, true}
+     kernels::pssfp_tangent_kernel<ZT, GZ>, kernels::pssfp_queue_kernel<ZT, GZ, true>, true,      \
+     kernels::pssfp_kernel<ZT, GZ, true, true>, kernels::pssfp_queue_kernel<ZT, GZ, false, true, true>, \
+     nullptr, nullptr}
 const PssfpConfig kPssfpConfigs[] = {
     COMPAS_PSSFP(1, 1),  COMPAS_PSSFP(2, 1), COMPAS_PSSFP(4, 1),  COMPAS_PSSFP(8, 1),  COMPAS_PSSFP(9, 4),
     COMPAS_PSSFP(5, 8),  COMPAS_PSSFP(3, 16), COMPAS_PSSFP(2, 32), COMPAS_PSSFP(1, 32), COMPAS_PSSFP(18, 2),
@@ -600,8 +640,12 @@ kernels::PssfpArgs pssfp_args(const CompasContext& ctx, const TissueParameters& 
         auto& cache = *seq.cache;
         std::lock_guard<std::mutex> lock(cache.mutex);
         if (!cache.table || cache.key_rf != seq.RF_train.data() || cache.key_g != seq.gamma_dt_RF.data()) {
-            auto tab = std::make_shared<Array<cfloat, 2>>(std::array<int64_t, 2> {nTR + 1, nRF}, ctx.device(), ctx.stream());
+            // rows 0..nTR: the axes; entry (nTR + 1)·nRF: the flag of a complex axis
+            // (pssfp_table_kernel), at least one entry per row so that it exists when nRF = 0
+            auto tab = std::make_shared<Array<cfloat, 2>>(std::array<int64_t, 2> {nTR + 2, std::max(nRF, 1)},
+                                                          ctx.device(), ctx.stream());
             int n = (nTR + 1) * nRF;
+            COMPAS_CUDA_CHECK(cudaMemsetAsync(tab->data() + int64_t(n), 0, sizeof(cfloat), ctx.stream()));
             if (n > 0) {
                 kernels::pssfp_table_kernel<<<div_ceil(n, 256), 256, 0, ctx.stream()>>>(
                     reinterpret_cast<const float2*>(seq.RF_train.data()), nTR,
@@ -612,6 +656,7 @@ kernels::PssfpArgs pssfp_args(const CompasContext& ctx, const TissueParameters& 
             cache.table = tab;
             cache.key_rf = seq.RF_train.data();
             cache.key_g = seq.gamma_dt_RF.data();
+            cache.real_rf = -1;
         }
         zap = cache.table;
     }
@@ -662,34 +707,59 @@ void launch_pssfp(const CompasContext& ctx, const TissueParameters& params, int 
     const auto& cfg = checked_config(L, nz);
     const int64_t total = int64_t(nvoxels) * cfg.GZ;
     DeviceGuard guard(ctx.device());
-    cfg.fn<<<unsigned((total + kPssfpThreads - 1) / kPssfpThreads), kPssfpThreads, 0, ctx.stream()>>>(a);
+    const unsigned grid = unsigned((total + kPssfpThreads - 1) / kPssfpThreads);
+    cfg.fn<<<grid, kPssfpThreads, 0, ctx.stream()>>>(a);
     check_launch("pssfp_kernel");
+    if (cfg.fn_real != nullptr) {  // the form that does not match the sequence returns at once
+        cfg.fn_real<<<grid, kPssfpThreads, 0, ctx.stream()>>>(a);
+        check_launch("pssfp_kernel (real RF)");
+    }
 }
 
 void launch_pssfp_queue(cudaStream_t stream, int device, PssfpLaunch L, int nz, const kernels::PssfpArgs* jobs,
-                        const int2* items, int nitems, int* head) {
+                        const int2* items, int nitems, int* head, bool real) {
     if (nitems <= 0) return;
     const auto& cfg = checked_config(L, nz);
+    const PssfpQueueKernel fn = real && cfg.queue_real != nullptr ? cfg.queue_real : cfg.queue;
     DeviceGuard guard(device);
     int per_sm = 1, sms = 148;
-    COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.queue, kPssfpThreads, 0));
+    COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPssfpThreads, 0));
     COMPAS_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     const int grid = std::max(1, std::min(nitems, std::max(1, per_sm) * sms));
-    cfg.queue<<<grid, kPssfpThreads, 0, stream>>>(jobs, items, nitems, head);
+    fn<<<grid, kPssfpThreads, 0, stream>>>(jobs, items, nitems, head);
     check_launch("pssfp_queue_kernel");
 }
 
 void launch_pssfp_tangent_queue(cudaStream_t stream, int device, PssfpLaunch L, int nz,
-                                const kernels::PssfpArgs* jobs, const int2* items, int nitems, int* head) {
+                                const kernels::PssfpArgs* jobs, const int2* items, int nitems, int* head, bool real) {
     if (nitems <= 0) return;
     const auto& cfg = checked_config(L, nz);
+    const PssfpQueueKernel fn = real && cfg.tangent_queue_real != nullptr ? cfg.tangent_queue_real : cfg.tangent_queue;
     DeviceGuard guard(device);
     int per_sm = 1, sms = 148;
-    COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.tangent_queue, kPssfpThreads, 0));
+    COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPssfpThreads, 0));
     COMPAS_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     const int grid = std::max(1, std::min(nitems, std::max(1, per_sm) * sms));
-    cfg.tangent_queue<<<grid, kPssfpThreads, 0, stream>>>(jobs, items, nitems, head);
+    fn<<<grid, kPssfpThreads, 0, stream>>>(jobs, items, nitems, head);
     check_launch("pssfp_tangent_queue_kernel");
+}
+
+bool pssfp_sequence_real_rf(const CompasContext& ctx, const pSSFPSequence& seq) {
+    kernels::PssfpArgs a = pssfp_args(ctx, TissueParameters {}, 0, 0, seq, nullptr, 0);  // builds the table
+    auto& cache = *seq.cache;
+    std::lock_guard<std::mutex> lock(cache.mutex);
+    if (cache.real_rf < 0) {
+        cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+        COMPAS_CUDA_CHECK(cudaStreamIsCapturing(ctx.stream(), &capture));
+        if (capture != cudaStreamCaptureStatusNone) return false;  // the general form is right for every sequence
+        float2 flag = make_float2(1.0f, 0.0f);
+        DeviceGuard guard(ctx.device());
+        COMPAS_CUDA_CHECK(cudaMemcpyAsync(&flag, a.zap + int64_t(a.nTR + 1) * a.nRF, sizeof(float2),
+                                          cudaMemcpyDeviceToHost, ctx.stream()));
+        COMPAS_CUDA_CHECK(cudaStreamSynchronize(ctx.stream()));
+        cache.real_rf = flag.x == 0.0f ? 1 : 0;
+    }
+    return cache.real_rf == 1;
 }
 
 // Value and T1/T2 tangents in one launch, with the value kernel's layout L.
@@ -705,8 +775,13 @@ void launch_pssfp_tangent(const CompasContext& ctx, const TissueParameters& para
     a.dT2 = reinterpret_cast<float2*>(dT2);
     const int64_t total = int64_t(nvoxels) * cfg.GZ;
     DeviceGuard guard(ctx.device());
-    cfg.tangent<<<unsigned((total + kPssfpThreads - 1) / kPssfpThreads), kPssfpThreads, 0, ctx.stream()>>>(a);
+    const unsigned grid = unsigned((total + kPssfpThreads - 1) / kPssfpThreads);
+    cfg.tangent<<<grid, kPssfpThreads, 0, ctx.stream()>>>(a);
     check_launch("pssfp_tangent_kernel");
+    if (cfg.tangent_real != nullptr) {
+        cfg.tangent_real<<<grid, kPssfpThreads, 0, ctx.stream()>>>(a);
+        check_launch("pssfp_tangent_kernel (real RF)");
+    }
 }
 
 MagnetizationTangents simulate_magnetization_tangents(const CompasContext& context, TissueParameters parameters,

@@ -343,6 +343,7 @@ struct pSSFPSequence: public Object {
         const void* key_rf = nullptr;
         const void* key_g = nullptr;
         std::shared_ptr<Array<cfloat, 2>> table;
+        int real_rf = -1;  // host copy of the table's flag: -1 not read yet, 1 every RF sample real, else 0
     };
     std::shared_ptr<Cache> cache = std::make_shared<Cache>();
 };

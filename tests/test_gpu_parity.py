@@ -265,14 +265,16 @@ def test_pssfp_large_rotations(cb, ctx, oracle, workloads):
     assert oracle.rel_l2(got.to_numpy(), oracle.pssfp(p, seq)) < TOL_FP32
 
 
-@pytest.mark.parametrize("scale", [1, 3])
-def test_pssfp_packed_layouts_match_scalar_bits(cb, ctx, workloads, scale):
+@pytest.mark.parametrize("scale,phase", [(1, 0.0), (3, 0.0), (1, 0.4)])
+def test_pssfp_packed_layouts_match_scalar_bits(cb, ctx, workloads, scale, phase):
     # a two-wide layout runs the scalar update's operations on pairs of isochromats and sums them in
     # the scalar order: the same bits as the scalar layout with as many isochromats per lane; at 3x
-    # the flip angles (and 20x the off-resonance) some pairs take the sincos branch
+    # the flip angles (and 20x the off-resonance) some pairs take the sincos branch. With a real RF
+    # train (phase 0) the packed layouts run their real-RF form, without the products of the zero
+    # axis component a_y: still the scalar bits (up to the sign of exact zeros)
     rng = np.random.default_rng(12 + scale)
     seq = workloads.pssfp_sequence(rng, 19, nrf=5, nz=3)
-    seq["rf"] = (seq["rf"] * scale).astype(np.complex64)
+    seq["rf"] = (seq["rf"] * scale * np.exp(1j * phase * rng.uniform(-1, 1, len(seq["rf"])))).astype(np.complex64)
     p = workloads.tissue(rng, 5, 20.0)
     p[3] *= 1 if scale == 1 else 20
     params = cb.TissueParameters.from_soa(ctx, p)

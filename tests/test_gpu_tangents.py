@@ -138,14 +138,15 @@ def test_pssfp_tangents_every_layout(cb, ctx, oracle, workloads, nz):
     assert tried > 0
 
 
-@pytest.mark.parametrize("scale", [1, 3])
-def test_pssfp_packed_tangents_match_scalar_bits(cb, ctx, workloads, scale):
+@pytest.mark.parametrize("scale,phase", [(1, 0.0), (3, 0.0), (1, 0.4)])
+def test_pssfp_packed_tangents_match_scalar_bits(cb, ctx, workloads, scale, phase):
     # the two-wide tangent kernel runs the scalar tangent update's operations on pairs of isochromats:
     # m, ∂m/∂T1 and ∂m/∂T2 are the bits of the scalar layout with as many isochromats per lane (at 3x
-    # the flip angles and 20x the off-resonance, some pairs take the sincos branch)
+    # the flip angles and 20x the off-resonance, some pairs take the sincos branch; phase 0: the
+    # real-RF form)
     rng = np.random.default_rng(30 + scale)
     seqd = workloads.pssfp_sequence(rng, 15, nrf=5, nz=3)
-    seqd["rf"] = (seqd["rf"] * scale).astype(np.complex64)
+    seqd["rf"] = (seqd["rf"] * scale * np.exp(1j * phase * rng.uniform(-1, 1, len(seqd["rf"])))).astype(np.complex64)
     p = workloads.tissue(rng, 5, 20.0)
     p[3] *= 1 if scale == 1 else 20
     params = cb.TissueParameters.from_soa(ctx, p)
