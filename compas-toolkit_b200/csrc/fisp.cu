@@ -254,23 +254,29 @@ __device__ __forceinline__ ExciteCoefs2 make_coefs2(float4 tab, float B1, float2
     return q;
 }
 
-// Packed-pair EPG state (one lane per voxel/position, 2·KP state slots): pair j holds state j in
-// .x and state j + KP in .y, one register pair per real component (Re/Im of F+, of conj(F-), and
+// Packed-pair EPG state (one lane per voxel/position, 2·KP + EXTRA state slots): pair j holds state
+// j in .x and state j + KP in .y, one register pair per real component (Re/Im of F+, of conj(F-), and
 // Re Z and -Im Z). All states of a TR share the excitation coefficients, so every operation of
 // excite_state becomes one two-wide instruction (add2/mul2/fma2) on a pair: 26 issue slots per
 // two states instead of 52, with the same roundings as the scalar update (negating an operand or
 // a result is exact). Only the two states that cross the pair boundary in the dephasing shift
-// (KP-1 → KP for F+, KP → KP-1 for conj(F-)) move between halves.
-template<int KP>
+// (KP-1 → KP for F+, KP → KP-1 for conj(F-)) move between halves. EXTRA = 1 adds an unpaired slot
+// 2·KP (scalar registers, the same operations one-wide): an odd state count then needs no padding
+// slot (25 states: 12 pairs and one slot, where 13 pairs spend a twenty-sixth slot's update on a
+// state that is zeroed every TR).
+template<int KP, int EXTRA = 0>
 struct EPGPacked {
     static_assert(KP >= 2, "at least two pairs");
-    static constexpr int K = 2 * KP;
+    static_assert(EXTRA == 0 || EXTRA == 1, "at most one unpaired slot");
+    static constexpr int K = 2 * KP + EXTRA;
     float2 ur[KP], ui[KP], gr[KP], gi[KP], zr[KP], zn[KP];  // zn = -Im Z
+    float eur, eui, egr, egi, ezr, ezn;                      // the unpaired slot 2·KP (EXTRA)
 
     __device__ __forceinline__ void init(int) {
 #pragma unroll
         for (int j = 0; j < KP; j++) ur[j] = ui[j] = gr[j] = gi[j] = zr[j] = zn[j] = make_float2(0.f, 0.f);
         zr[0].x = 1.0f;
+        eur = eui = egr = egi = ezr = ezn = 0.f;
     }
 
     // dephasing (epg.cuh:229-298): conj(F-) one state down (state s ← s+1, zero at ≥ N-1), F+ one
@@ -283,11 +289,23 @@ struct EPGPacked {
             gr[j] = gr[j + 1];
             gi[j] = gi[j + 1];
         }
-        gr[KP - 1] = make_float2(cr, 0.f);
-        gi[KP - 1] = make_float2(ci, 0.f);
-        if (N == K - 1) {  // one padding slot (25 states in 26): state K-2 is pair KP-2, high half
-            gr[KP - 2].y = gi[KP - 2].y = 0.f;
-        } else if (N < K - 1) {
+        // state 2KP-1 takes the unpaired slot's conj(F-), or the zero beyond the layout; the unpaired
+        // slot takes the zero beyond the layout
+        gr[KP - 1] = make_float2(cr, EXTRA ? egr : 0.f);
+        gi[KP - 1] = make_float2(ci, EXTRA ? egi : 0.f);
+        egr = egi = 0.f;
+        if constexpr (EXTRA == 0) {
+            if (N == K - 1) {  // one padding slot (25 states in 26): state K-2 is pair KP-2, high half
+                gr[KP - 2].y = gi[KP - 2].y = 0.f;
+            } else if (N < K - 1) {
+                const unsigned cut = 1u << (N - 1);
+#pragma unroll
+                for (int j = 0; j < KP; j++) {
+                    if (cut & (1u << j)) gr[j].x = gi[j].x = 0.f;
+                    if (cut & (1u << (j + KP))) gr[j].y = gi[j].y = 0.f;
+                }
+            }
+        } else if (N < K) {  // state N-1 is a paired slot (N = K: the unpaired slot, zero already)
             const unsigned cut = 1u << (N - 1);
 #pragma unroll
             for (int j = 0; j < KP; j++) {
@@ -296,6 +314,10 @@ struct EPGPacked {
             }
         }
         const float ar = ur[KP - 1].x, ai = ui[KP - 1].x;  // F+ of state KP-1 → state KP
+        if constexpr (EXTRA) {  // F+ of state 2KP-1 → the unpaired slot (its old F+ leaves the layout)
+            eur = ur[KP - 1].y;
+            eui = ui[KP - 1].y;
+        }
 #pragma unroll
         for (int j = KP - 1; j > 0; j--) {
             ur[j] = ur[j - 1];
@@ -331,6 +353,22 @@ struct EPGPacked {
             zr[j] = nzr;
             zn[j] = nzn;
         }
+        if constexpr (EXTRA) {  // the unpaired slot: the same operations one-wide
+            const float Pr = eur + egr, Pi = eui + egi;
+            const float Qr = eur - egr, Qn = egi - eui;
+            const float Phr = REAL ? fmaf(k.A1.x, Pr, k.A2.x * Pi) : fmaf(k.A1.x, Pr, fmaf(k.A2.x, Pi, k.dre.x * ezr));
+            const float Phi = fmaf(k.A3.x, Pr, fmaf(k.A4.x, Pi, k.dim.x * ezr));
+            const float Qhr = fmaf(k.A4.x, Qr, fmaf(k.A3.x, Qn, k.dim.x * ezn));
+            const float nQhi = REAL ? fmaf(k.A2.x, Qr, k.A1.x * Qn) : fmaf(k.A2.x, Qr, fmaf(k.A1.x, Qn, k.dre.x * ezn));
+            const float nzr = fmaf(k.ere.x, Pr, fmaf(k.neim.x, Pi, k.f.x * ezr));
+            const float nzn = fmaf(k.ere.x, Qn, fmaf(k.neim.x, Qr, k.f.x * ezn));
+            eur = Phr + Qhr;
+            eui = Phi - nQhi;
+            egr = Phr - Qhr;
+            egi = Phi + nQhi;
+            ezr = nzr;
+            ezn = nzn;
+        }
         if constexpr (!REAL) {
             ur[0].x += k.bre;
             gr[0].x += k.bre;
@@ -354,6 +392,16 @@ struct EPGPacked {
             zr[j] = mul2(e1, zr[j]);
             zn[j] = mul2(e1, zn[j]);
         }
+        if constexpr (EXTRA) {
+            const float a = fmaf(eur, cx.x, eui * ncy.x), b = fmaf(eur, cy.x, eui * cx.x);
+            const float d = fmaf(egr, cx.x, egi * ncy.x), e = fmaf(egr, cy.x, egi * cx.x);
+            eur = a;
+            eui = b;
+            egr = d;
+            egi = e;
+            ezr = E1 * ezr;
+            ezn = E1 * ezn;
+        }
         zr[0].x += 1.0f - E1;
     }
 
@@ -364,11 +412,15 @@ struct EPGPacked {
             zr[j] = make_float2(-zr[j].x, -zr[j].y);
             zn[j] = make_float2(-zn[j].x, -zn[j].y);
         }
+        eur = eui = egr = egi = 0.f;
+        ezr = -ezr;
+        ezn = -ezn;
     }
 
     __device__ __forceinline__ void spoil() {
 #pragma unroll
         for (int j = 0; j < KP; j++) ur[j] = ui[j] = gr[j] = gi[j] = make_float2(0.f, 0.f);
+        eur = eui = egr = egi = 0.f;
     }
 
     __device__ __forceinline__ void invert_decay(float E1, int) {
@@ -379,6 +431,8 @@ struct EPGPacked {
             zr[j] = mul2(e1, zr[j]);
             zn[j] = mul2(e1, zn[j]);
         }
+        ezr = E1 * ezr;
+        ezn = E1 * ezn;
         zr[0].x += 1.0f - E1;
     }
 
@@ -497,9 +551,10 @@ struct EPGTangent {
 template<int G, bool TAN>
 constexpr int kFispChunk = (TAN && G > 1) ? 64 : 32;
 
-// state type of a layout: PACKED (G = 1, K even) → EPGPacked<K/2>; TAN → EPGTangent; else EPG
+// state type of a layout: PACKED (G = 1) → EPGPacked<K/2, K%2>; TAN → EPGTangent; else EPG
 template<int K, int G, bool TAN, bool PACKED>
-using FispState = std::conditional_t<TAN, EPGTangent<K, G>, std::conditional_t<PACKED, EPGPacked<K / 2>, EPG<K, G>>>;
+using FispState =
+    std::conditional_t<TAN, EPGTangent<K, G>, std::conditional_t<PACKED, EPGPacked<K / 2, K % 2>, EPG<K, G>>>;
 
 // Balanced item split of the one-simulation kernel: the order of a CTA's items (at most
 // kFispBalancedItems) and its hand-off points, in shared memory
@@ -546,7 +601,7 @@ __device__ __forceinline__ void handoff_wait(const int* flag, unsigned int* stat
 template<int K, int G, bool TAN = false, bool PACKED = false, bool BAL = false, bool REAL = false>
 __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_begin, const int item_end,
                                            float2* samples, const FispOrder* ord = nullptr) {
-    static_assert(!PACKED || (G == 1 && K % 2 == 0 && !TAN), "packed layouts hold one voxel per lane");
+    static_assert(!PACKED || (G == 1 && !TAN), "packed layouts hold one voxel per lane");
     static_assert(!REAL || PACKED, "the real-phase update is a packed-layout form");
     constexpr int VB = 32 / G;
     const int W = blockDim.x >> 5;
@@ -870,7 +925,7 @@ const FispConfig kFispConfigs[] = {
     COMPAS_FISP(2, 4), COMPAS_FISP(4, 2), COMPAS_FISP(4, 4), COMPAS_FISP(4, 8), COMPAS_FISP(7, 4),
     COMPAS_FISP(13, 2), COMPAS_FISP(8, 4), COMPAS_FISP(8, 8), COMPAS_FISP(8, 16), COMPAS_FISP(4, 32),
     COMPAS_FISP_PACKED(4), COMPAS_FISP_PACKED(8), COMPAS_FISP_PACKED(12), COMPAS_FISP_PACKED(16),
-    COMPAS_FISP_PACKED(20), COMPAS_FISP_PACKED(26),
+    COMPAS_FISP_PACKED(20), COMPAS_FISP_PACKED(26), COMPAS_FISP_PACKED(25),
 };
 #undef COMPAS_FISP
 #undef COMPAS_FISP_PACKED
@@ -922,8 +977,12 @@ FispLaunch fisp_default_launch(int N, int64_t nvoxels, int P) {
     const bool wide = pairs >= 148LL * 32 * 8;
     int best = -1;
     auto waste = [&](int i) { return kFispConfigs[i].K * kFispConfigs[i].G - N; };
-    // issue slots of the state update per lane and TR, in units of one state's 26 operations
-    auto cost = [&](int i) { return kFispConfigs[i].packed ? kFispConfigs[i].K / 2 : kFispConfigs[i].K; };
+    // FMA-pipe time of the state update per lane and TR, in units of one state's 26 one-wide
+    // operations: a two-wide instruction takes the pipe twice as long, so a pair of states costs two
+    // units, an unpaired state one, and a packed layout K/2 units for K states
+    auto cost = [&](int i) {
+        return kFispConfigs[i].packed ? 0.5 * kFispConfigs[i].K : double(kFispConfigs[i].K);
+    };
     for (int i = 0; i < fisp_config_count(); i++) {
         const auto& c = kFispConfigs[i];
         if (c.K * c.G < N) continue;

@@ -46,9 +46,9 @@ def test_builtin_choice_covers_the_states():
     for (cfg, warps), n in zip(out["fisp"], (25, 25, 8)):
         k, g = fc[cfg]
         assert k * g >= n and 1 <= warps <= 8
-    # 25 states x 35 positions at 50176 voxels: one lane per voxel in the packed layout (13 pairs of
-    # states, two states per two-wide instruction), 8 warps
-    assert tuple(fc[out["fisp"][0][0]]) == (26, 1) and out["fisp_packed"][out["fisp"][0][0]]
+    # 25 states x 35 positions at 50176 voxels: one lane per voxel in the packed layout (12 pairs of
+    # states, two states per two-wide instruction, and one unpaired state), 8 warps
+    assert tuple(fc[out["fisp"][0][0]]) == (25, 1) and out["fisp_packed"][out["fisp"][0][0]]
     assert out["fisp"][0][1] == 8
     assert fc[out["fisp"][2][0]][1] == 4  # few voxel/position pairs: states split over 4 lanes
     for cfg, nz in zip(out["pssfp"], (35, 5)):
