@@ -35,13 +35,21 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "compas-toolkit_b200"))
 
 METRIC = "EPG voxel·TR/s"
-# FMA-pipe lane operations the FISP kernel executes per (voxel, slice position, TR) at 25 states in
-# the packed 26-slot layout: 26 per state slot for the excitation update plus the per-TR
-# coefficients, dephasing moves and sample (ncu, profiles/fisp_epg_mrstat.txt). With real RF and
-# slice-profile phases the kernel runs the form without the d_re products: two FFMA2 fewer per pair
-# of states, 13 x 2 x 2 = 52 lane operations fewer.
-FISP_LANE_OPS_PER_ITEM = 732
-FISP_LANE_OPS_PER_ITEM_REAL_PHASES = 732 - 52
+# FMA-pipe lane operations the FISP kernel executes per (voxel, slice position, TR): every state
+# slot of the layout takes 26 one-wide operations for the excitation update (24 in the real-phase
+# form of the packed layouts, without the d_re products), and every lane 56 more for the per-TR
+# coefficients, dephasing moves and sample (ncu, profiles/fisp_epg_mrstat.txt: 732 for the 26-slot
+# packed layout in the general form)
+FISP_LANE_OPS_PER_LANE = 56
+
+
+def fisp_lane_ops_per_item(cb, N, V, P, real_phases):
+    cfg, _ = cb.fisp_launch_choice(N, V, P)
+    K, G = cb.fisp_configs()[cfg]
+    per_slot = 24 if real_phases and cb.fisp_config_packed(cfg) else 26
+    return K * G * per_slot + G * FISP_LANE_OPS_PER_LANE, f"{K}x{G}{' packed' if cb.fisp_config_packed(cfg) else ''}"
+
+
 UNIT = "voxel·TR/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "sm_max_mhz": 1965.0}
@@ -329,9 +337,16 @@ def main():
     # the clock sampler polls from before the warm-up on, so that its start-up is over before the
     # timed steps; its summary covers the samples taken between mark_start and mark_end
     with ClockSampler(local) as clk:
+        # the warm-up keeps results alive as the timed loop does (the last step's while the next
+        # one allocates), so that the memory pool has grown to two steps' worth before the timed
+        # region: growing it there maps memory and stalled a timed step by 225 ms
+        warm = []
         for _ in range(args.warmup):
-            step()
+            warm.append(step())
+            if len(warm) > 1:
+                warm.pop(0)
         ctx.synchronize()
+        warm.clear()
         barrier()
         clk.mark_start()
         launches0 = cb.launch_count()
@@ -371,13 +386,14 @@ def main():
     seqd = w["seq"]
     real_phases = not np.any(np.imag(np.asarray(seqd["slices"], np.complex128)
                                      * np.asarray(seqd["rf"], np.complex128)[None, :]))
-    per_item = FISP_LANE_OPS_PER_ITEM_REAL_PHASES if real_phases else FISP_LANE_OPS_PER_ITEM
+    per_item, layout = fisp_lane_ops_per_item(cb, N, Vl, P, real_phases)
     lane_ops = per_item * P * Vl * nTR
     exec_frac = lane_ops / (sim_ms / 1e3) / (148 * 128 * f_mhz * 1e6)
     roofline = {"bound": "fp32", "kernel": "fisp_epg_kernel", "achieved": epg_tf, "peak": fp32_peak_tf,
                 "unit": "TFLOP/s", "frac": epg_tf / fp32_peak_tf,
                 "traffic": profile_traffic("fisp_epg_mrstat"),
-                "executed": {"fp32_lane_ops_per_voxel_position_tr": per_item, "real_phase_form": real_phases,
+                "executed": {"fp32_lane_ops_per_voxel_position_tr": per_item, "layout": layout,
+                             "real_phase_form": real_phases,
                              "fp32_lane_ops": lane_ops, "frac_of_fp32_peak": exec_frac},
                 "note": f"FP32 SIMT peak 148 SM x 128 lanes x 2 x {f_mhz:.0f} MHz (median SM clock under load). "
                         "achieved/frac count the reference formulation's 86·N·P flops per voxel·TR; the kernel "
