@@ -89,6 +89,7 @@ _SIGS = {
     "compas_b200_set_fisp_tangent_launch": ([_I], None),
     "compas_b200_fisp_tangent_config_count": ([], _I),
     "compas_b200_fisp_tangent_config_info": ([_I, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
+    "compas_b200_fisp_tangent_config_packed": ([_I], _I),
     "compas_b200_make_batch": ([_P, _I, _P, _P, _P, _P, _I], _P),
     "compas_b200_make_batch_tangents": ([_P, _I, _P, _P, _P, _P, _I, _P], _P),
     "compas_b200_batch_derivative": ([_P, _I, _I], _P),
@@ -857,6 +858,11 @@ def fisp_configs() -> list:
         lib.compas_b200_fisp_config_info(i, C.byref(k), C.byref(g))
         out.append((k.value, g.value))
     return out
+
+
+def fisp_tangent_config_packed(index: int) -> bool:
+    """Whether FISP tangent layout `index` is packed (value and tangents as pairs of states)."""
+    return bool(library().compas_b200_fisp_tangent_config_packed(int(index)))
 
 
 def fisp_config_packed(index: int) -> bool:

@@ -147,7 +147,8 @@ void SimulationBatch::Impl::plan_simulation(Family& fam, bool fisp, const std::v
                 D = L.config < 0 ? fisp_default_launch(seq.max_state, V, P) : L;
             }
             // jobs with real phases form their own groups, which a packed layout runs in its real-phase form
-            const int real = !tan && fisp_config_packed(D.config) && fisp_sequence_real_phases(ctx, seq) ? 1 : 0;
+            const bool packed = tan ? fisp_tangent_config_packed(D.config) : fisp_config_packed(D.config);
+            const int real = packed && fisp_sequence_real_phases(ctx, seq) ? 1 : 0;
             keyed.push_back({Key {tan, D.config, std::max(1, std::min(D.warps, 8)), seq.max_state, real}, j});
         } else {
             const auto& seq = std::get<pSSFPSequence>(job.sequence);
@@ -361,7 +362,8 @@ void SimulationBatch::Impl::enqueue(const Family& fam, cudaStream_t stream, int*
     for (const auto& g : fam.sims) {
         if (g.fisp && g.tangent)
             launch_fisp_tangent_queue(stream, dev, FispLaunch {g.config, g.warps}, g.cover,
-                                      as<kernels::FispArgs>(g.args), as<int2>(g.items), g.nitems, head_base + g.head);
+                                      as<kernels::FispArgs>(g.args), as<int2>(g.items), g.nitems, head_base + g.head,
+                                      g.real);
         else if (g.fisp)
             launch_fisp_queue(stream, dev, FispLaunch {g.config, g.warps}, g.cover, as<kernels::FispArgs>(g.args),
                               as<int2>(g.items), g.nitems, head_base + g.head, g.real);

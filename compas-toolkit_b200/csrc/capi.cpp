@@ -686,6 +686,10 @@ int compas_b200_fisp_tangent_config_info(int index, int* states_per_lane, int* l
     return compas::fisp_tangent_config_info(index, states_per_lane, lanes) ? 1 : 0;
 }
 
+int compas_b200_fisp_tangent_config_packed(int index) {
+    return compas::fisp_tangent_config_packed(index) ? 1 : 0;
+}
+
 void compas_b200_set_pssfp_launch(int config) {
     guarded([&] { compas::set_pssfp_override(config); });
 }

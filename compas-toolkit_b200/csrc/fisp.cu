@@ -68,34 +68,71 @@ struct ExciteCoefs {
     float bre, bim, bz;     // β·R13 (added to F+0 and conj(F-0)), β·R33 (added to Z0)
 };
 
+// Every operation is written with an explicit rounding (no multiply-add left to the compiler to
+// fuse), so that the real-phase form below gives the same bits.
 __device__ __forceinline__ ExciteCoefs make_coefs(float4 tab, float B1, float2 c, float E1, float beta) {
     float s, co;
     __sincosf(tab.x * B1, &s, &co);  // x = α/2   (epg.cuh:41-51)
-    float s2 = s * s, c2 = co * co;
-    float sa = 2.0f * s * co;        // sin α
-    float ca = 2.0f * c2 - 1.0f;     // cos α
-    float cp = tab.y, sp = tab.z;
-    float cos2p = 2.0f * cp * cp - 1.0f, sin2p = 2.0f * cp * sp;
+    const float s2 = __fmul_rn(s, s), c2 = __fmul_rn(co, co);
+    const float sa = __fmul_rn(2.0f * s, co);      // sin α
+    const float ca = __fmaf_rn(2.0f, c2, -1.0f);   // cos α
+    const float cp = tab.y, sp = tab.z;
+    const float cos2p = __fmaf_rn(2.0f * cp, cp, -1.0f), sin2p = __fmul_rn(2.0f * cp, sp);
     // R11 = cos²(α/2), R12 = e^{2iφ} sin²(α/2), R13 = -i e^{iφ} sin α, R31 = -½ conj(R13), R33 = cos α
-    float r12re = cos2p * s2, r12im = sin2p * s2;
-    float r13re = sp * sa, r13im = -cp * sa;
-    float r31re = -0.5f * r13re, r31im = 0.5f * r13im;
+    const float r12re = __fmul_rn(cos2p, s2), r12im = __fmul_rn(sin2p, s2);
+    const float r13re = __fmul_rn(sp, sa), r13im = -__fmul_rn(cp, sa);
+    const float r31re = -0.5f * r13re, r31im = 0.5f * r13im;
     // a = R11·c, b = R12·c̄, d = R13·E1, e = R31·c, f = R33·E1
-    float are = c2 * c.x, aim = c2 * c.y;
-    float bre = r12re * c.x + r12im * c.y, bim = r12im * c.x - r12re * c.y;
+    const float are = __fmul_rn(c2, c.x), aim = __fmul_rn(c2, c.y);
+    const float bre = __fmaf_rn(r12re, c.x, __fmul_rn(r12im, c.y));
+    const float bim = __fmaf_rn(r12im, c.x, -__fmul_rn(r12re, c.y));
     ExciteCoefs k;
-    k.A1 = 0.5f * (are + bre);
-    k.A2 = 0.5f * (bim - aim);
-    k.A3 = 0.5f * (aim + bim);
-    k.A4 = 0.5f * (are - bre);
-    k.dre = r13re * E1;
-    k.dim = r13im * E1;
-    k.ere = r31re * c.x - r31im * c.y;
-    k.eim = r31re * c.y + r31im * c.x;
-    k.f = ca * E1;
-    k.bre = beta * r13re;
-    k.bim = beta * r13im;
-    k.bz = beta * ca;
+    k.A1 = 0.5f * __fadd_rn(are, bre);
+    k.A2 = 0.5f * __fsub_rn(bim, aim);
+    k.A3 = 0.5f * __fadd_rn(aim, bim);
+    k.A4 = 0.5f * __fsub_rn(are, bre);
+    k.dre = __fmul_rn(r13re, E1);
+    k.dim = __fmul_rn(r13im, E1);
+    k.ere = __fmaf_rn(r31re, c.x, -__fmul_rn(r31im, c.y));
+    k.eim = __fmaf_rn(r31re, c.y, __fmul_rn(r31im, c.x));
+    k.f = __fmul_rn(ca, E1);
+    k.bre = __fmul_rn(beta, r13re);
+    k.bim = __fmul_rn(beta, r13im);
+    k.bz = __fmul_rn(beta, ca);
+    return k;
+}
+
+// make_coefs for a real phase (sin φ = 0 and cos φ = ±1 exactly, as the table holds them when the
+// RF sample times the slice profile is real): cos 2φ = 1 and sin 2φ = ±0, so R12 = sin²(α/2) and
+// R13, R31 are imaginary. The products with those exact ones and zeros are left out; every other
+// operation is the general form's, so the coefficients it returns are the same bits (up to the sign
+// of an exact zero). d_re and β·R13_re, zero here, are not computed (the real-phase update does not
+// read them).
+__device__ __forceinline__ ExciteCoefs make_coefs_real(float4 tab, float B1, float2 c, float E1, float beta) {
+    float s, co;
+    __sincosf(tab.x * B1, &s, &co);
+    const float s2 = __fmul_rn(s, s), c2 = __fmul_rn(co, co);
+    const float sa = __fmul_rn(2.0f * s, co);
+    const float ca = __fmaf_rn(2.0f, c2, -1.0f);
+    const float cp = tab.y;
+    const float r13im = -__fmul_rn(cp, sa);
+    const float r31im = 0.5f * r13im;
+    const float are = __fmul_rn(c2, c.x), aim = __fmul_rn(c2, c.y);
+    const float bre = __fmul_rn(s2, c.x);
+    const float bim = -__fmul_rn(s2, c.y);
+    ExciteCoefs k;
+    k.A1 = 0.5f * __fadd_rn(are, bre);
+    k.A2 = 0.5f * __fsub_rn(bim, aim);
+    k.A3 = 0.5f * __fadd_rn(aim, bim);
+    k.A4 = 0.5f * __fsub_rn(are, bre);
+    k.dre = 0.0f;
+    k.dim = __fmul_rn(r13im, E1);
+    k.ere = -__fmul_rn(r31im, c.y);
+    k.eim = __fmul_rn(r31im, c.x);
+    k.f = __fmul_rn(ca, E1);
+    k.bre = 0.0f;
+    k.bim = __fmul_rn(beta, r13im);
+    k.bz = __fmul_rn(beta, ca);
     return k;
 }
 
@@ -236,8 +273,9 @@ struct ExciteCoefs2 {
     float bre, bim, bz;
 };
 
+template<bool REAL = false>
 __device__ __forceinline__ ExciteCoefs2 make_coefs2(float4 tab, float B1, float2 c, float E1, float beta) {
-    const ExciteCoefs k = make_coefs(tab, B1, c, E1, beta);
+    const ExciteCoefs k = REAL ? make_coefs_real(tab, B1, c, E1, beta) : make_coefs(tab, B1, c, E1, beta);
     ExciteCoefs2 q;
     q.A1 = bcast2(k.A1);
     q.A2 = bcast2(k.A2);
@@ -336,6 +374,24 @@ struct EPGPacked {
     // exact zero.
     template<bool REAL = false>
     __device__ __forceinline__ void excite(const ExciteCoefs2& k, int) {
+        // the unpaired slot first: the same operations one-wide (placed before the pairs, the
+        // 25-slot kernel ran 44.1 ms at the MR-STAT slice; after them 45.9 ms)
+        if constexpr (EXTRA) {
+            const float Pr = eur + egr, Pi = eui + egi;
+            const float Qr = eur - egr, Qn = egi - eui;
+            const float Phr = REAL ? fmaf(k.A1.x, Pr, k.A2.x * Pi) : fmaf(k.A1.x, Pr, fmaf(k.A2.x, Pi, k.dre.x * ezr));
+            const float Phi = fmaf(k.A3.x, Pr, fmaf(k.A4.x, Pi, k.dim.x * ezr));
+            const float Qhr = fmaf(k.A4.x, Qr, fmaf(k.A3.x, Qn, k.dim.x * ezn));
+            const float nQhi = REAL ? fmaf(k.A2.x, Qr, k.A1.x * Qn) : fmaf(k.A2.x, Qr, fmaf(k.A1.x, Qn, k.dre.x * ezn));
+            const float nzr = fmaf(k.ere.x, Pr, fmaf(k.neim.x, Pi, k.f.x * ezr));
+            const float nzn = fmaf(k.ere.x, Qn, fmaf(k.neim.x, Qr, k.f.x * ezn));
+            eur = Phr + Qhr;
+            eui = Phi - nQhi;
+            egr = Phr - Qhr;
+            egi = Phi + nQhi;
+            ezr = nzr;
+            ezn = nzn;
+        }
 #pragma unroll
         for (int j = 0; j < KP; j++) {
             const float2 Pr = add2(ur[j], gr[j]), Pi = add2(ui[j], gi[j]);
@@ -352,22 +408,6 @@ struct EPGPacked {
             gi[j] = add2(Phi, nQhi);
             zr[j] = nzr;
             zn[j] = nzn;
-        }
-        if constexpr (EXTRA) {  // the unpaired slot: the same operations one-wide
-            const float Pr = eur + egr, Pi = eui + egi;
-            const float Qr = eur - egr, Qn = egi - eui;
-            const float Phr = REAL ? fmaf(k.A1.x, Pr, k.A2.x * Pi) : fmaf(k.A1.x, Pr, fmaf(k.A2.x, Pi, k.dre.x * ezr));
-            const float Phi = fmaf(k.A3.x, Pr, fmaf(k.A4.x, Pi, k.dim.x * ezr));
-            const float Qhr = fmaf(k.A4.x, Qr, fmaf(k.A3.x, Qn, k.dim.x * ezn));
-            const float nQhi = REAL ? fmaf(k.A2.x, Qr, k.A1.x * Qn) : fmaf(k.A2.x, Qr, fmaf(k.A1.x, Qn, k.dre.x * ezn));
-            const float nzr = fmaf(k.ere.x, Pr, fmaf(k.neim.x, Pi, k.f.x * ezr));
-            const float nzn = fmaf(k.ere.x, Qn, fmaf(k.neim.x, Qr, k.f.x * ezn));
-            eur = Phr + Qhr;
-            eui = Phi - nQhi;
-            egr = Phr - Qhr;
-            egi = Phi + nQhi;
-            ezr = nzr;
-            ezn = nzn;
         }
         if constexpr (!REAL) {
             ur[0].x += k.bre;
@@ -529,6 +569,195 @@ struct EPGTangent {
         d1.spoil();
         d2.spoil();
     }
+
+    // F+ of state 0 (lane sub == 0) of the value (v = 0), ∂/∂T1 (1) or ∂/∂T2 (2)
+    __device__ __forceinline__ float2 f0(int v) const { return v == 0 ? x.u[0] : v == 1 ? d1.u[0] : d2.u[0]; }
+};
+
+// The excitation of one pair of states in the packed representation (EPGPacked::excite's update,
+// without the regrowth terms of state 0): every operation two-wide, in excite_state's order.
+template<bool REAL>
+__device__ __forceinline__ void excite_pair(const ExciteCoefs2& k, float2& ur, float2& ui, float2& gr, float2& gi,
+                                            float2& zr, float2& zn) {
+    const float2 Pr = add2(ur, gr), Pi = add2(ui, gi);
+    const float2 Qr = sub2(ur, gr), Qn = sub2(gi, ui);
+    const float2 Phr = REAL ? fma2(k.A1, Pr, mul2(k.A2, Pi)) : fma2(k.A1, Pr, fma2(k.A2, Pi, mul2(k.dre, zr)));
+    const float2 Phi = fma2(k.A3, Pr, fma2(k.A4, Pi, mul2(k.dim, zr)));
+    const float2 Qhr = fma2(k.A4, Qr, fma2(k.A3, Qn, mul2(k.dim, zn)));
+    const float2 nQhi = REAL ? fma2(k.A2, Qr, mul2(k.A1, Qn)) : fma2(k.A2, Qr, fma2(k.A1, Qn, mul2(k.dre, zn)));
+    const float2 nzr = fma2(k.ere, Pr, fma2(k.neim, Pi, mul2(k.f, zr)));
+    const float2 nzn = fma2(k.ere, Qn, fma2(k.neim, Qr, mul2(k.f, zn)));
+    ur = add2(Phr, Qhr);
+    ui = sub2(Phi, nQhi);
+    gr = sub2(Phr, Qhr);
+    gi = add2(Phi, nQhi);
+    zr = nzr;
+    zn = nzn;
+}
+
+// Two-wide form of EPGTangent: the value and its T1 and T2 tangents (vectors v = 0, 1, 2), each in
+// the packed representation of EPGPacked (pair j of a lane holds the lane's states j in .x and j + KP
+// in .y; Re Z and -Im Z), on G lanes of K = 2·KP states each (states sub·K .. sub·K + K-1 on lane sub).
+// The operations are EPGTangent's in the same order, so layout (K, G) gives the bits of the scalar
+// tangent layout (K, G). The dephasing shift exchanges the boundary states with the neighbour lanes
+// as EPG<K, G> does.
+template<int KP, int G>
+struct EPGPackedTangent {
+    static_assert(KP >= 2 && G >= 1 && G <= 32 && (G & (G - 1)) == 0, "pairs per lane, power-of-two lane groups");
+    static constexpr int K = 2 * KP;
+    float2 ur[3][KP], ui[3][KP], gr[3][KP], gi[3][KP], zr[3][KP], zn[3][KP];  // zn = -Im Z
+
+    __device__ __forceinline__ void init(int sub) {
+#pragma unroll
+        for (int v = 0; v < 3; v++)
+#pragma unroll
+            for (int j = 0; j < KP; j++) ur[v][j] = ui[v][j] = gr[v][j] = gi[v][j] = zr[v][j] = zn[v][j] = make_float2(0.f, 0.f);
+        if (sub == 0) zr[0][0].x = 1.0f;
+    }
+
+    __device__ __forceinline__ void shift_vector(int v, int sub, int N) {
+        const unsigned mask = 0xffffffffu;
+        // the neighbour lanes' boundary states, read before this lane shifts: conj(F-) of the next
+        // lane's first state, F+ of the previous lane's last state
+        float ngr = 0.f, ngi = 0.f, pur = 0.f, pui = 0.f;
+        if constexpr (G > 1) {
+            ngr = __shfl_down_sync(mask, gr[v][0].x, 1, G);
+            ngi = __shfl_down_sync(mask, gi[v][0].x, 1, G);
+            pur = __shfl_up_sync(mask, ur[v][KP - 1].y, 1, G);
+            pui = __shfl_up_sync(mask, ui[v][KP - 1].y, 1, G);
+        }
+        const float cr = gr[v][0].y, ci = gi[v][0].y;  // conj(F-) of state KP → state KP-1
+#pragma unroll
+        for (int j = 0; j < KP - 1; j++) {
+            gr[v][j] = gr[v][j + 1];
+            gi[v][j] = gi[v][j + 1];
+        }
+        const bool last = sub == G - 1;  // the last lane's top state takes the zero beyond the layout
+        gr[v][KP - 1] = make_float2(cr, last ? 0.f : ngr);
+        gi[v][KP - 1] = make_float2(ci, last ? 0.f : ngi);
+        if (sub == (N - 1) / K) {  // zero state N-1 (one-hot bit test per slot)
+            const unsigned cut = 1u << ((N - 1) % K);
+#pragma unroll
+            for (int j = 0; j < KP; j++) {
+                if (cut & (1u << j)) gr[v][j].x = gi[v][j].x = 0.f;
+                if (cut & (1u << (j + KP))) gr[v][j].y = gi[v][j].y = 0.f;
+            }
+        }
+        const float ar = ur[v][KP - 1].x, ai = ui[v][KP - 1].x;  // F+ of state KP-1 → state KP
+#pragma unroll
+        for (int j = KP - 1; j > 0; j--) {
+            ur[v][j] = ur[v][j - 1];
+            ui[v][j] = ui[v][j - 1];
+        }
+        ur[v][0] = make_float2(sub == 0 ? gr[v][0].x : pur, ar);  // F+0 = conj(F-0)
+        ui[v][0] = make_float2(sub == 0 ? gi[v][0].x : pui, ai);
+    }
+
+    __device__ __forceinline__ void shift(int sub, int N) {
+#pragma unroll
+        for (int v = 0; v < 3; v++) shift_vector(v, sub, N);
+    }
+
+    // EPGTangent::excite: the T1 tangent excites (F1, Z1 + s1·(Z - δ_{n0})), the T2 tangent
+    // (F2 + s2·F, Z2), both from the value before its own excitation
+    template<bool REAL = false>
+    __device__ __forceinline__ void excite(const ExciteCoefs2& k, float s1, float s2, int sub) {
+        const float2 S1 = bcast2(s1), S2 = bcast2(s2);
+#pragma unroll
+        for (int j = 0; j < KP; j++) {
+            float2 zs = zr[0][j];
+            if (j == 0 && sub == 0) zs.x = zr[0][0].x - 1.0f;
+            zr[1][j] = fma2(S1, zs, zr[1][j]);
+            zn[1][j] = fma2(S1, zn[0][j], zn[1][j]);
+            excite_pair<REAL>(k, ur[1][j], ui[1][j], gr[1][j], gi[1][j], zr[1][j], zn[1][j]);
+            ur[2][j] = fma2(S2, ur[0][j], ur[2][j]);
+            ui[2][j] = fma2(S2, ui[0][j], ui[2][j]);
+            gr[2][j] = fma2(S2, gr[0][j], gr[2][j]);
+            gi[2][j] = fma2(S2, gi[0][j], gi[2][j]);
+            excite_pair<REAL>(k, ur[2][j], ui[2][j], gr[2][j], gi[2][j], zr[2][j], zn[2][j]);
+        }
+#pragma unroll
+        for (int j = 0; j < KP; j++) excite_pair<REAL>(k, ur[0][j], ui[0][j], gr[0][j], gi[0][j], zr[0][j], zn[0][j]);
+        if (sub == 0) {  // the regrowth terms of state 0 (EPG::excite)
+            if constexpr (!REAL) {
+                ur[0][0].x += k.bre;
+                gr[0][0].x += k.bre;
+            }
+            ui[0][0].x += k.bim;
+            gi[0][0].x += k.bim;
+            zr[0][0].x += k.bz;
+        }
+    }
+
+    // EPGTangent::relax: F·c, Z·E1 on the value; the tangents as there
+    __device__ __forceinline__ void relax(float2 c, float E1, float s1, float s2, int sub) {
+        const float2 cx = bcast2(c.x), cy = bcast2(c.y), ncy = bcast2(-c.y), e1 = bcast2(E1);
+        const float2 S1 = bcast2(s1), S2 = bcast2(s2);
+        auto rot = [&](float2& re, float2& im) {
+            const float2 a = fma2(re, cx, mul2(im, ncy)), b = fma2(re, cy, mul2(im, cx));
+            re = a;
+            im = b;
+        };
+#pragma unroll
+        for (int j = 0; j < KP; j++) {
+            float2 zs = zr[0][j];
+            if (j == 0 && sub == 0) zs.x = zr[0][0].x - 1.0f;
+            rot(ur[1][j], ui[1][j]);
+            rot(gr[1][j], gi[1][j]);
+            zr[1][j] = mul2(e1, fma2(S1, zs, zr[1][j]));
+            zn[1][j] = mul2(e1, fma2(S1, zn[0][j], zn[1][j]));
+            ur[2][j] = fma2(S2, ur[0][j], ur[2][j]);
+            ui[2][j] = fma2(S2, ui[0][j], ui[2][j]);
+            gr[2][j] = fma2(S2, gr[0][j], gr[2][j]);
+            gi[2][j] = fma2(S2, gi[0][j], gi[2][j]);
+            rot(ur[2][j], ui[2][j]);
+            rot(gr[2][j], gi[2][j]);
+            zr[2][j] = mul2(e1, zr[2][j]);
+            zn[2][j] = mul2(e1, zn[2][j]);
+        }
+#pragma unroll
+        for (int j = 0; j < KP; j++) {
+            rot(ur[0][j], ui[0][j]);
+            rot(gr[0][j], gi[0][j]);
+            zr[0][j] = mul2(e1, zr[0][j]);
+            zn[0][j] = mul2(e1, zn[0][j]);
+        }
+        if (sub == 0) zr[0][0].x += 1.0f - E1;
+    }
+
+    __device__ __forceinline__ void spoil() {
+#pragma unroll
+        for (int v = 0; v < 3; v++)
+#pragma unroll
+            for (int j = 0; j < KP; j++) ur[v][j] = ui[v][j] = gr[v][j] = gi[v][j] = make_float2(0.f, 0.f);
+    }
+
+    // EPGTangent::invert_decay: inversion and spoiling of all three, then relaxation over TI
+    __device__ __forceinline__ void invert_decay(float E1, float s1, int sub) {
+        spoil();
+        const float2 e1 = bcast2(E1), S1 = bcast2(s1);
+#pragma unroll
+        for (int v = 0; v < 3; v++)
+#pragma unroll
+            for (int j = 0; j < KP; j++) {
+                zr[v][j] = make_float2(-zr[v][j].x, -zr[v][j].y);
+                zn[v][j] = make_float2(-zn[v][j].x, -zn[v][j].y);
+            }
+#pragma unroll
+        for (int j = 0; j < KP; j++) {
+            float2 zs = zr[0][j];
+            if (j == 0 && sub == 0) zs.x = zr[0][0].x - 1.0f;
+            zr[1][j] = mul2(e1, fma2(S1, zs, zr[1][j]));
+            zn[1][j] = mul2(e1, fma2(S1, zn[0][j], zn[1][j]));
+            zr[2][j] = mul2(e1, zr[2][j]);
+            zn[2][j] = mul2(e1, zn[2][j]);
+            zr[0][j] = mul2(e1, zr[0][j]);
+            zn[0][j] = mul2(e1, zn[0][j]);
+        }
+        if (sub == 0) zr[0][0].x += 1.0f - E1;
+    }
+
+    __device__ __forceinline__ float2 f0(int v) const { return make_float2(ur[v][0].x, ui[v][0].x); }
 };
 
 // The work of a FISP simulation is a list of items (voxel tile, slice position), tile-major:
@@ -551,10 +780,11 @@ struct EPGTangent {
 template<int G, bool TAN>
 constexpr int kFispChunk = (TAN && G > 1) ? 64 : 32;
 
-// state type of a layout: PACKED (G = 1) → EPGPacked<K/2, K%2>; TAN → EPGTangent; else EPG
+// state type of a layout: value PACKED (G = 1) → EPGPacked<K/2, K%2>; TAN → EPGTangent, or
+// EPGPackedTangent<K/2, G> when PACKED; else EPG
 template<int K, int G, bool TAN, bool PACKED>
-using FispState =
-    std::conditional_t<TAN, EPGTangent<K, G>, std::conditional_t<PACKED, EPGPacked<K / 2, K % 2>, EPG<K, G>>>;
+using FispState = std::conditional_t<TAN, std::conditional_t<PACKED, EPGPackedTangent<K / 2, G>, EPGTangent<K, G>>,
+                                     std::conditional_t<PACKED, EPGPacked<K / 2, K % 2>, EPG<K, G>>>;
 
 // Balanced item split of the one-simulation kernel: the order of a CTA's items (at most
 // kFispBalancedItems) and its hand-off points, in shared memory
@@ -601,7 +831,8 @@ __device__ __forceinline__ void handoff_wait(const int* flag, unsigned int* stat
 template<int K, int G, bool TAN = false, bool PACKED = false, bool BAL = false, bool REAL = false>
 __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_begin, const int item_end,
                                            float2* samples, const FispOrder* ord = nullptr) {
-    static_assert(!PACKED || (G == 1 && !TAN), "packed layouts hold one voxel per lane");
+    static_assert(!PACKED || TAN || G == 1, "packed value layouts hold one voxel per lane");
+    static_assert(!PACKED || !TAN || K % 2 == 0, "packed tangent layouts hold pairs of states");
     static_assert(!REAL || PACKED, "the real-phase update is a packed-layout form");
     constexpr int VB = 32 / G;
     const int W = blockDim.x >> 5;
@@ -687,26 +918,37 @@ __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_beg
                         const float4 tv = tv_next;
                         tv_next = __ldg(tab + min(t + 1, a.nTR - 1));
                         if constexpr (TAN) {
-                            if (t == 0) {
-                                st.excite(make_coefs(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), 0.0f, 0.0f, sub);
+                            if constexpr (PACKED) {
+                                if (t == 0) {
+                                    st.template excite<REAL>(make_coefs2<REAL>(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f),
+                                                             0.0f, 0.0f, sub);
+                                } else {
+                                    st.shift(sub, a.N);
+                                    st.template excite<REAL>(make_coefs2<REAL>(tv, B1, c_TR, E1_TR, beta), s1_TR, s2_TR,
+                                                             sub);
+                                }
                             } else {
-                                st.shift(sub, a.N);
-                                st.excite(make_coefs(tv, B1, c_TR, E1_TR, beta), s1_TR, s2_TR, sub);
+                                if (t == 0) {
+                                    st.excite(make_coefs(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), 0.0f, 0.0f, sub);
+                                } else {
+                                    st.shift(sub, a.N);
+                                    st.excite(make_coefs(tv, B1, c_TR, E1_TR, beta), s1_TR, s2_TR, sub);
+                                }
                             }
                             if (sampled && writer) {
                                 float2* q = samples + (warp * CH + j) * VB + grp;
-                                q[0] = cmul(c_TE, st.x.u[0]);
-                                q[plane] = cmul(c_TE, st.d1.u[0]);
-                                q[2 * plane] = cmul(c_TE, make_float2(fmaf(s2_TE, st.x.u[0].x, st.d2.u[0].x),
-                                                                      fmaf(s2_TE, st.x.u[0].y, st.d2.u[0].y)));
+                                const float2 f = st.f0(0), f2 = st.f0(2);
+                                q[0] = cmul(c_TE, f);
+                                q[plane] = cmul(c_TE, st.f0(1));
+                                q[2 * plane] = cmul(c_TE, make_float2(fmaf(s2_TE, f.x, f2.x), fmaf(s2_TE, f.y, f2.y)));
                             }
                         } else {
                             if constexpr (PACKED) {
                                 if (t == 0) {
-                                    st.template excite<REAL>(make_coefs2(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), sub);
+                                    st.template excite<REAL>(make_coefs2<REAL>(tv, B1, make_float2(1.f, 0.f), 1.0f, 0.0f), sub);
                                 } else {
                                     st.shift(sub, a.N);
-                                    st.template excite<REAL>(make_coefs2(tv, B1, c_TR, E1_TR, beta), sub);
+                                    st.template excite<REAL>(make_coefs2<REAL>(tv, B1, c_TR, E1_TR, beta), sub);
                                 }
                             } else {
                                 if (t == 0) {
@@ -857,15 +1099,21 @@ __global__ void __launch_bounds__(256, 1) fisp_queue_kernel(const FispArgs* __re
 }
 
 // One FISP simulation with its T1 and T2 tangents: value, ∂/∂T1, ∂/∂T2 into a.echo, a.dT1, a.dT2.
-template<int K, int G>
+// PACKED: the two-wide state EPGPackedTangent; REAL its real-phase form, launched beside the
+// general form (the one that does not match the sequence returns at once).
+template<int K, int G, bool PACKED = false, bool REAL = false>
 __global__ void __launch_bounds__(256, 1) fisp_tangent_kernel(FispArgs a, int ntiles) {
     extern __shared__ float2 samples[];  // [3][W][chunk][VB]
+    if constexpr (PACKED) {
+        if (fisp_real_phases(a) != REAL) return;
+    }
     const int2 r = cta_tile_range(ntiles, blockIdx.x, gridDim.x);
-    fisp_items<K, G, true>(a, r.x * a.P, r.y * a.P, samples);
+    fisp_items<K, G, true, PACKED, false, REAL>(a, r.x * a.P, r.y * a.P, samples);
 }
 
-// Work-queue form of fisp_tangent_kernel for batches (same items and order as fisp_queue_kernel).
-template<int K, int G>
+// Work-queue form of fisp_tangent_kernel for batches (same items and order as fisp_queue_kernel;
+// REAL: every job's phases are real).
+template<int K, int G, bool PACKED = false, bool REAL = false>
 __global__ void __launch_bounds__(256, 1) fisp_tangent_queue_kernel(const FispArgs* __restrict__ jobs,
                                                                     const int2* __restrict__ items, int nitems,
                                                                     int* __restrict__ head) {
@@ -880,7 +1128,7 @@ __global__ void __launch_bounds__(256, 1) fisp_tangent_queue_kernel(const FispAr
         const int2 w = items[it];
         if (threadIdx.x == 0) job = jobs[w.x];
         __syncthreads();
-        fisp_items<K, G, true>(job, w.y * job.P, (w.y + 1) * job.P, samples);
+        fisp_items<K, G, true, PACKED, false, REAL>(job, w.y * job.P, (w.y + 1) * job.P, samples);
         __syncthreads();
     }
 }
@@ -937,15 +1185,28 @@ struct FispTangentConfig {
     int K, G;
     FispKernel fn;
     FispQueueKernel queue;
+    bool packed;  // EPGPackedTangent<K/2, G>: two states per two-wide instruction
+    // packed layouts: the real-phase forms of fn (launched beside it) and queue (for groups of
+    // real-phase jobs), else null
+    FispKernel fn_real;
+    FispQueueKernel queue_real;
 };
-#define COMPAS_FISP_TANGENT(K, G) {K, G, kernels::fisp_tangent_kernel<K, G>, kernels::fisp_tangent_queue_kernel<K, G>}
+#define COMPAS_FISP_TANGENT(K, G) \
+    {K, G, kernels::fisp_tangent_kernel<K, G>, kernels::fisp_tangent_queue_kernel<K, G>, false, nullptr, nullptr}
+#define COMPAS_FISP_TANGENT_PACKED(K, G)                                                                     \
+    {K, G, kernels::fisp_tangent_kernel<K, G, true>, kernels::fisp_tangent_queue_kernel<K, G, true>, true, \
+     kernels::fisp_tangent_kernel<K, G, true, true>, kernels::fisp_tangent_queue_kernel<K, G, true, true>}
+// the packed layouts come last, so the indices of the others keep their meaning
 const FispTangentConfig kFispTangentConfigs[] = {
     COMPAS_FISP_TANGENT(1, 1), COMPAS_FISP_TANGENT(2, 1), COMPAS_FISP_TANGENT(4, 1), COMPAS_FISP_TANGENT(8, 1),
     COMPAS_FISP_TANGENT(2, 4), COMPAS_FISP_TANGENT(4, 4), COMPAS_FISP_TANGENT(5, 5), COMPAS_FISP_TANGENT(7, 4),
     COMPAS_FISP_TANGENT(8, 4),
     COMPAS_FISP_TANGENT(4, 8), COMPAS_FISP_TANGENT(8, 8), COMPAS_FISP_TANGENT(8, 16),
+    COMPAS_FISP_TANGENT_PACKED(8, 1), COMPAS_FISP_TANGENT_PACKED(4, 4), COMPAS_FISP_TANGENT_PACKED(8, 4),
+    COMPAS_FISP_TANGENT_PACKED(4, 8),
 };
 #undef COMPAS_FISP_TANGENT
+#undef COMPAS_FISP_TANGENT_PACKED
 constexpr int kFispTangentConfigCount = int(sizeof(kFispTangentConfigs) / sizeof(kFispTangentConfigs[0]));
 
 }  // namespace
@@ -1219,6 +1480,10 @@ bool fisp_tangent_config_info(int index, int* K, int* G) {
     return true;
 }
 
+bool fisp_tangent_config_packed(int index) {
+    return index >= 0 && index < kFispTangentConfigCount && kFispTangentConfigs[index].packed;
+}
+
 // Tangent layout for N states: with many (voxel, position) pairs and N ≤ 8 all states in one
 // lane; otherwise the covering layout with the least padding, fewer lanes on ties. The warps
 // per CTA are the value kernel's (tuned_fisp_launch): 8 for the MR-STAT slice, where 7 and 5
@@ -1261,9 +1526,18 @@ void launch_fisp_tangent(const CompasContext& ctx, const TissueParameters& param
     const size_t smem = fisp_tangent_smem_bytes(cfg.G, W);
     DeviceGuard guard(ctx.device());
     allow_smem(reinterpret_cast<const void*>(cfg.fn), smem);
-    const int grid = std::min(ntiles, resident_ctas(reinterpret_cast<const void*>(cfg.fn), 32 * W, smem, ctx.device()));
+    int resident = resident_ctas(reinterpret_cast<const void*>(cfg.fn), 32 * W, smem, ctx.device());
+    if (cfg.fn_real != nullptr) {
+        allow_smem(reinterpret_cast<const void*>(cfg.fn_real), smem);
+        resident = std::min(resident, resident_ctas(reinterpret_cast<const void*>(cfg.fn_real), 32 * W, smem, ctx.device()));
+    }
+    const int grid = std::min(ntiles, resident);
     cfg.fn<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles);
     check_launch("fisp_tangent_kernel");
+    if (cfg.fn_real != nullptr) {  // the form that does not match the sequence's phases returns at once
+        cfg.fn_real<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles);
+        check_launch("fisp_tangent_kernel (real phases)");
+    }
 }
 
 int fisp_tangent_tile_voxels(FispLaunch L) {
@@ -1272,20 +1546,21 @@ int fisp_tangent_tile_voxels(FispLaunch L) {
 }
 
 void launch_fisp_tangent_queue(cudaStream_t stream, int device, FispLaunch L, int max_state,
-                               const kernels::FispArgs* jobs, const int2* items, int nitems, int* head) {
+                               const kernels::FispArgs* jobs, const int2* items, int nitems, int* head, bool real) {
     if (nitems <= 0) return;
     COMPAS_CHECK(L.config >= 0 && L.config < kFispTangentConfigCount);
     const auto& cfg = kFispTangentConfigs[L.config];
     COMPAS_CHECK(cfg.K * cfg.G >= max_state);
+    const FispQueueKernel fn = real && cfg.queue_real != nullptr ? cfg.queue_real : cfg.queue;
     const int W = std::max(1, std::min(L.warps, 8));
     const size_t smem = fisp_tangent_smem_bytes(cfg.G, W);
     DeviceGuard guard(device);
-    allow_smem(reinterpret_cast<const void*>(cfg.queue), smem);
+    allow_smem(reinterpret_cast<const void*>(fn), smem);
     int per_sm = 1, sms = 148;
-    COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.queue, 32 * W, smem));
+    COMPAS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * W, smem));
     COMPAS_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     const int grid = std::max(1, std::min(nitems, std::max(1, per_sm) * sms));
-    cfg.queue<<<grid, 32 * W, smem, stream>>>(jobs, items, nitems, head);
+    fn<<<grid, 32 * W, smem, stream>>>(jobs, items, nitems, head);
     check_launch("fisp_tangent_queue_kernel");
 }
 

@@ -47,15 +47,18 @@ void launch_fisp_queue(cudaStream_t stream, int device, FispLaunch L, int max_st
 // value and T1/T2 tangents (forward mode) in one launch; L.config indexes the tangent layouts
 int fisp_tangent_config_count();
 bool fisp_tangent_config_info(int index, int* K, int* G);
+bool fisp_tangent_config_packed(int index);  // EPGPackedTangent layout
 FispLaunch fisp_tangent_default_launch(int N, int64_t nvoxels, int P);
 FispLaunch tuned_fisp_tangent_launch(int N, int64_t nvoxels, int P);  // honours the test override
 void launch_fisp_tangent(const CompasContext& ctx, const TissueParameters& params, int voxel_begin, int nvoxels,
                          const FISPSequence& seq, cfloat* echo, cfloat* dT1, cfloat* dT2, int64_t echo_stride,
                          FispLaunch L);
 int fisp_tangent_tile_voxels(FispLaunch L);  // voxels per work item of tangent layout L
-// work-queue launch over (job, tile) items of FISP tangent jobs (args with dT1 / dT2 set)
+// work-queue launch over (job, tile) items of FISP tangent jobs (args with dT1 / dT2 set); `real`:
+// every job's phases are real, which a packed layout runs in its real-phase form
 void launch_fisp_tangent_queue(cudaStream_t stream, int device, FispLaunch L, int max_state,
-                               const kernels::FispArgs* jobs, const int2* items, int nitems, int* head);
+                               const kernels::FispArgs* jobs, const int2* items, int nitems, int* head,
+                               bool real = false);
 
 // ---- pSSFP ------------------------------------------------------------------------------
 struct PssfpLaunch {

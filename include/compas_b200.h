@@ -216,6 +216,9 @@ COMPAS_API int compas_b200_pssfp_config_packed(int index);
 COMPAS_API void compas_b200_set_fisp_tangent_launch(int config);
 COMPAS_API int compas_b200_fisp_tangent_config_count(void);
 COMPAS_API int compas_b200_fisp_tangent_config_info(int index, int* states_per_lane, int* lanes);
+/* 1 when FISP tangent layout `index` is a two-wide layout (value, ∂/∂T1 and ∂/∂T2 of states_per_lane
+ * states as pairs; the same bits as the scalar tangent layout of that shape), else 0. */
+COMPAS_API int compas_b200_fisp_tangent_config_packed(int index);
 /* The layout a simulation of this shape gets (override, tuning table, or built-in choice). */
 COMPAS_API void compas_b200_fisp_launch_choice(int max_state, int64_t nvoxels, int npositions, int* config,
                                                int* warps);

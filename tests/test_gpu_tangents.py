@@ -66,6 +66,39 @@ def test_fisp_tangents_every_layout(cb, ctx, oracle, workloads, max_state):
     assert oracle.rel_l2(value, ref_value) < TOL_FP32
 
 
+@pytest.mark.parametrize("phase", [0.0, 0.3])
+def test_fisp_packed_tangents_match_scalar_bits(cb, ctx, workloads, phase):
+    # the two-wide tangent layouts run the scalar tangent update's operations on pairs of states
+    # (with real phases, phase 0, in the form without the d_re products): m, ∂m/∂T1 and ∂m/∂T2 are
+    # the bits of the scalar tangent layout of the same shape (up to the sign of exact zeros)
+    rng = np.random.default_rng(23)
+    ntr, P = 47, 3
+    rf = workloads.smooth_flip_train(rng, ntr) * np.exp(1j * phase * rng.uniform(-1, 1, ntr))
+    slices = workloads.gaussian_slice_profile(P, ntr)
+    p = workloads.tissue(rng, 9, 22.4)
+    params = cb.TissueParameters.from_soa(ctx, p)
+    configs = [tuple(c) for c in cb.fisp_tangent_configs()]
+    tried = 0
+    try:
+        for i, c in enumerate(configs):
+            if not cb.fisp_tangent_config_packed(i):
+                continue
+            j = next(n for n, d in enumerate(configs) if d == c and not cb.fisp_tangent_config_packed(n))
+            for N in sorted({c[0] * c[1], c[0] * c[1] - 3}):
+                seq = cb.FispSequence.from_dict(ctx, workloads.fisp_sequence(rf, slices, 8.7e-3, 4.35e-3, 25e-3, N))
+                cb.set_fisp_tangent_launch(i)
+                packed = cb.simulate_magnetization_tangents(ctx, params, seq)
+                packed = {k: packed[k].to_numpy() for k in ("echos", "T1", "T2")}
+                cb.set_fisp_tangent_launch(j)
+                scalar = cb.simulate_magnetization_tangents(ctx, params, seq)
+                for k in ("echos", "T1", "T2"):
+                    assert np.array_equal(packed[k], scalar[k].to_numpy()), (c, N, k, phase)
+                tried += 1
+    finally:
+        cb.set_fisp_tangent_launch(-1)
+    assert tried >= 6
+
+
 def test_fisp_tangents_repetitions_undersampling(cb, ctx, oracle, workloads):
     # repetitions carry the state (and its tangents) through the wait TW; the C ABI's FISP
     # sequence always has the inversion prepulse and wait spoiling (bindings.cpp:151-174)
