@@ -261,6 +261,9 @@ def main():
                     help="jobs of the batched uneven workload (0 skips it)")
     ap.add_argument("--batch-vmax", type=int, default=64000,
                     help="largest voxel count of a batched job (smaller values for profiler captures)")
+    ap.add_argument("--tangent-layout", type=int, default=-1,
+                    help="FISP tangent layout index for the derivatives block (-1: the built-in choice; "
+                         "for profiler comparisons of layouts)")
     ap.add_argument("--n-side", type=int, default=224,
                     help="voxel grid side (224 = the MR-STAT workload; smaller values for profiler captures)")
     args = ap.parse_args()
@@ -830,6 +833,9 @@ def derivatives(cb, ctx, stream, args, rank):
     import torch
     import workloads
 
+    if args.tangent_layout >= 0:
+        cb.set_fisp_tangent_launch(args.tangent_layout)
+
     def timed(fn, reps=2):
         warm = [fn() for _ in range(2)]  # two results alive, as in the timed loop (pool growth)
         ctx.synchronize()
@@ -864,6 +870,8 @@ def derivatives(cb, ctx, stream, args, rank):
             err[f] = float(torch.linalg.vector_norm((a - b).double()) / torch.linalg.vector_norm(b.double()))
         res[name] = {"voxels": int(params.shape[1]), "readouts": int(seq.nreadouts),
                      "forward_difference_ms": fd_ms, "tangent_ms": tan_ms, "fd_rel_error": err}
+    if args.tangent_layout >= 0:
+        cb.set_fisp_tangent_launch(-1)
     return res
 
 

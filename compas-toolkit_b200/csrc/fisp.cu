@@ -1484,13 +1484,23 @@ bool fisp_tangent_config_packed(int index) {
     return index >= 0 && index < kFispTangentConfigCount && kFispTangentConfigs[index].packed;
 }
 
-// Tangent layout for N states: with many (voxel, position) pairs and N ≤ 8 all states in one
-// lane; otherwise the covering layout with the least padding, fewer lanes on ties. The warps
+// Tangent layout for N states: with many (voxel, position) pairs and 25-32 states the two-wide
+// 4 x 8 layout, with N ≤ 8 all states in one lane; otherwise the covering layout with the least
+// padding, fewer lanes on ties. The warps
 // per CTA are the value kernel's (tuned_fisp_launch): 8 for the MR-STAT slice, where 7 and 5
 // measured 9 % and 54 % slower (one CTA of 255-register threads per SM).
 FispLaunch fisp_tangent_default_launch(int N, int64_t nvoxels, int P) {
     const bool wide = nvoxels * P >= 148LL * 32 * 8;
     int best = -1;
+    // 25 to 32 states on many (voxel, position) pairs: the two-wide layout of 4 lanes x 8 states
+    // (MR-STAT slice: 272.8 ms against 279.6 ms for the scalar 5 x 5 and 287 ms for 4 x 7; 96² voxels:
+    // 50.1 against 54.1 ms), although its 32 slots hold up to 7 padding states
+    if (wide && N > 24 && N <= 32) {
+        for (int i = 0; i < kFispTangentConfigCount; i++) {
+            const auto& c = kFispTangentConfigs[i];
+            if (c.packed && c.K == 8 && c.G == 4) return FispLaunch {i, tuned_fisp_launch(N, nvoxels, P).warps};
+        }
+    }
     for (int i = 0; i < kFispTangentConfigCount; i++) {
         const auto& c = kFispTangentConfigs[i];
         if (c.K * c.G < N || (c.G == 1) != (wide && N <= 8)) continue;
