@@ -122,27 +122,31 @@ __device__ __forceinline__ float precess_angle(const PssfpArgs& a, float g, floa
 // rotation coefficients and E1 enters as E1/E2 on the E2-scaled longitudinal result. Every
 // operation is written out (no contraction left to the compiler), in the form the packed update
 // repeats on pairs of isochromats, so both give the same bits.
+// REAL (a_y = ±0, pssfp_real_rf): the products with a_y are left out, as in the packed update; the
+// same bits up to the sign of an exact zero.
+template<bool REAL = false>
 __device__ __forceinline__ void rotate_relax(Iso& m, float ax, float ay, float az, const RotCoefs& q,
                                              const RotRelax& k) {
-    const float cx = fmaf(ay, m.z, (-az) * m.y);
+    const float cx = REAL ? (-az) * m.y : fmaf(ay, m.z, (-az) * m.y);
     const float cy = fmaf(az, m.x, (-ax) * m.z);
-    const float cz = fmaf(ax, m.y, (-ay) * m.x);
-    const float hd = q.h * fmaf(ax, m.x, fmaf(ay, m.y, az * m.z));
+    const float cz = REAL ? ax * m.y : fmaf(ax, m.y, (-ay) * m.x);
+    const float hd = REAL ? q.h * fmaf(ax, m.x, az * m.z) : q.h * fmaf(ax, m.x, fmaf(ay, m.y, az * m.z));
     m.x = fmaf(q.c, m.x, fmaf(q.s, cx, hd * ax));
-    m.y = fmaf(q.c, m.y, fmaf(q.s, cy, hd * ay));
+    m.y = REAL ? fmaf(q.c, m.y, q.s * cy) : fmaf(q.c, m.y, fmaf(q.s, cy, hd * ay));
     m.z = fmaf(k.r, fmaf(q.c, m.z, fmaf(q.s, cz, hd * az)), k.oneE1);
 }
 
 // Tangent of rotate_relax: the same linear map applied to d (without the regrowth 1 - E1) plus
 // the explicit derivative (px, py, pz) of the step at the current state.
+template<bool REAL = false>
 __device__ __forceinline__ void rotate_relax_tangent(Iso& d, float ax, float ay, float az, const RotCoefs& q,
                                                      const RotRelax& k, float px, float py, float pz) {
-    const float cx = fmaf(ay, d.z, (-az) * d.y);
+    const float cx = REAL ? (-az) * d.y : fmaf(ay, d.z, (-az) * d.y);
     const float cy = fmaf(az, d.x, (-ax) * d.z);
-    const float cz = fmaf(ax, d.y, (-ay) * d.x);
-    const float hd = q.h * fmaf(ax, d.x, fmaf(ay, d.y, az * d.z));
+    const float cz = REAL ? ax * d.y : fmaf(ax, d.y, (-ay) * d.x);
+    const float hd = REAL ? q.h * fmaf(ax, d.x, az * d.z) : q.h * fmaf(ax, d.x, fmaf(ay, d.y, az * d.z));
     d.x = fmaf(q.c, d.x, fmaf(q.s, cx, fmaf(hd, ax, px)));
-    d.y = fmaf(q.c, d.y, fmaf(q.s, cy, fmaf(hd, ay, py)));
+    d.y = REAL ? fmaf(q.c, d.y, fmaf(q.s, cy, py)) : fmaf(q.c, d.y, fmaf(q.s, cy, fmaf(hd, ay, py)));
     d.z = fmaf(k.r, fmaf(q.c, d.z, fmaf(q.s, cz, hd * az)), pz);
 }
 
@@ -302,9 +306,14 @@ __device__ __forceinline__ void pssfp_tile(const PssfpArgs& a, const int tile) {
 // x, a_y·m_x in its z, a_y·m_y in a·m and hd·a_y in the new m_y are left out: 23 instructions per pair
 // and RF sample instead of 27 (value; the same four per tangent). An FMA that adds ±0 to a product
 // returns the rounded product, so the results are the same bits up to the sign of an exact zero.
-template<int ZP, int GZ, bool TAN = false, bool REAL = false>
+// EXTRA = 1: one more isochromat, slot 2·ZP, in scalar registers with the scalar update (the same
+// operations one-wide), so that an odd count per lane needs no padding slot (35 z on 4 lanes of 9
+// instead of 10). Its update follows the pairs' (before them, ptxas spilled 40 B in the value kernel
+// and 196 B in the tangent kernel; after them 4 B and 28 B).
+template<int ZP, int GZ, bool TAN = false, bool REAL = false, int EXTRA = 0>
 __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int tile) {
-    constexpr int ZT = 2 * ZP;
+    static_assert(EXTRA == 0 || EXTRA == 1, "at most one unpaired isochromat");
+    constexpr int ZT = 2 * ZP + EXTRA;
     const int lane = threadIdx.x & 31;
     const int sub = lane % GZ;
     const int vloc = (tile * blockDim.x + threadIdx.x) / GZ;
@@ -354,6 +363,16 @@ __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int 
             ax1[p] = ay1[p] = ax2[p] = ay2[p] = az2[p] = bcast2(0.0f);
             az1[p] = bcast2(s1_inv * (mz0 - 1.0f));
         }
+    }
+    // the unpaired isochromat (EXTRA): magnetisation, tangents, axis z component, precession
+    Iso em {0.0f, 0.0f, mz0}, ed1 {0.0f, 0.0f, s1_inv * (mz0 - 1.0f)}, ed2 {0.0f, 0.0f, 0.0f};
+    float eaz = 0.0f, ecpr = 1.0f, espr = 0.0f;
+    if constexpr (EXTRA) {
+        const int k = 2 * ZP, zi = sub * ZT + k;
+        valid[k] = zi < a.nz;
+        const float z = valid[k] ? a.z[zi] : 0.0f;
+        eaz = excite_az(a, z, B0);
+        sincosf(precess_angle(a, 1.0f, z, B0), &espr, &ecpr);
     }
 
     const RotRelax rr = make_rot_relax(E1_ex, E2_ex);
@@ -409,6 +428,14 @@ __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int 
                     rotate(ax2[p], ay2[p], az2[p], mul2(S2EX, mx[p]), mul2(S2EX, my[p]), bcast2(0.0f));
                 }
             }
+            if constexpr (EXTRA) {  // the unpaired isochromat, with the scalar update (pssfp_tile)
+                const RotCoefs q = rot_coefs(fmaf(-eaz, eaz, naxy2), rr);
+                rotate_relax<REAL>(em, ax, ay, eaz, q, rr);
+                if constexpr (TAN) {
+                    rotate_relax_tangent<REAL>(ed1, ax, ay, eaz, q, rr, 0.0f, 0.0f, s1_ex * (em.z - 1.0f));
+                    rotate_relax_tangent<REAL>(ed2, ax, ay, eaz, q, rr, s2_ex * em.x, s2_ex * em.y, 0.0f);
+                }
+            }
         }
     };
     const float2 E2P = bcast2(E2_pr), E1P = bcast2(E1_pr), ONE_E1P = bcast2(1.0f - E1_pr);
@@ -428,6 +455,24 @@ __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int 
             az2[p] = mul2(az2[p], E1P);
         }
     };
+    // pssfp_tile's precession of the unpaired isochromat
+    auto precess_extra = [&](float c, float sn) {
+        if constexpr (EXTRA) {
+            const float x = em.x, y = em.y;
+            em.x = E2_pr * fmaf(c, x, (-sn) * y);
+            em.y = E2_pr * fmaf(c, y, sn * x);
+            em.z = fmaf(em.z, E1_pr, 1.0f - E1_pr);
+            if constexpr (TAN) {
+                const float x1 = ed1.x, y1 = ed1.y, x2 = ed2.x, y2 = ed2.y;
+                ed1.x = E2_pr * fmaf(c, x1, (-sn) * y1);
+                ed1.y = E2_pr * fmaf(c, y1, sn * x1);
+                ed1.z = fmaf(ed1.z, E1_pr, s1_pr * (em.z - 1.0f));
+                ed2.x = fmaf(s2_pr, em.x, E2_pr * fmaf(c, x2, (-sn) * y2));
+                ed2.y = fmaf(s2_pr, em.y, E2_pr * fmaf(c, y2, sn * x2));
+                ed2.z = ed2.z * E1_pr;
+            }
+        }
+    };
 
     // α/2 pulse, then re- and prephaser with twice the prephasing gradient (pssfp_kernels.cuh:73-80)
     excite(0);
@@ -442,17 +487,25 @@ __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int 
         }
         precess_by(p, make_float2(c2[0], c2[1]), make_float2(s2[0], s2[1]), make_float2(-s2[0], -s2[1]));
     }
+    if constexpr (EXTRA) {
+        const int zi = sub * ZT + 2 * ZP;
+        const float z = valid[2 * ZP] ? a.z[zi] : 0.0f;
+        float c2, s2;
+        sincosf(precess_angle(a, 2.0f, z, B0), &s2, &c2);
+        precess_extra(c2, s2);
+    }
 
     for (int t = 0; t < a.nTR; t++) {  // pssfp_kernels.cuh:83-107
         excite(t + 1);
 #pragma unroll
         for (int p = 0; p < ZP; p++) precess_by(p, cpr[p], spr[p], nspr[p]);
+        precess_extra(ecpr, espr);
         float sx = 0.0f, sy = 0.0f;
 #pragma unroll
         for (int k = 0; k < ZT; k++) {
             if (valid[k]) {
-                sx += k < ZP ? mx[k].x : mx[k - ZP].y;
-                sy += k < ZP ? my[k].x : my[k - ZP].y;
+                sx += k < ZP ? mx[k].x : k < 2 * ZP ? mx[k - ZP].y : em.x;
+                sy += k < ZP ? my[k].x : k < 2 * ZP ? my[k - ZP].y : em.y;
             }
         }
 #pragma unroll
@@ -467,10 +520,10 @@ __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int 
 #pragma unroll
             for (int k = 0; k < ZT; k++) {
                 if (valid[k]) {
-                    t1x += k < ZP ? ax1[k].x : ax1[k - ZP].y;
-                    t1y += k < ZP ? ay1[k].x : ay1[k - ZP].y;
-                    t2x += k < ZP ? ax2[k].x : ax2[k - ZP].y;
-                    t2y += k < ZP ? ay2[k].x : ay2[k - ZP].y;
+                    t1x += k < ZP ? ax1[k].x : k < 2 * ZP ? ax1[k - ZP].y : ed1.x;
+                    t1y += k < ZP ? ay1[k].x : k < 2 * ZP ? ay1[k - ZP].y : ed1.y;
+                    t2x += k < ZP ? ax2[k].x : k < 2 * ZP ? ax2[k - ZP].y : ed2.x;
+                    t2y += k < ZP ? ay2[k].x : k < 2 * ZP ? ay2[k - ZP].y : ed2.y;
                 }
             }
 #pragma unroll
@@ -487,6 +540,7 @@ __device__ __forceinline__ void pssfp_tile_packed(const PssfpArgs& a, const int 
         }
 #pragma unroll
         for (int p = 0; p < ZP; p++) precess_by(p, cpr[p], spr[p], nspr[p]);
+        precess_extra(ecpr, espr);
     }
 }
 
@@ -498,7 +552,7 @@ __global__ void __launch_bounds__(128) pssfp_kernel(PssfpArgs a) {
     if (a.skip != nullptr && *a.skip != 0) return;  // uniform over the grid
     if constexpr (PACKED) {
         if (pssfp_real_rf(a) != REAL) return;
-        pssfp_tile_packed<ZT / 2, GZ, false, REAL>(a, blockIdx.x);
+        pssfp_tile_packed<ZT / 2, GZ, false, REAL, ZT % 2>(a, blockIdx.x);
     } else {
         pssfp_tile<ZT, GZ>(a, blockIdx.x);
     }
@@ -509,7 +563,7 @@ template<int ZT, int GZ, bool PACKED = false, bool REAL = false>
 __global__ void __launch_bounds__(128) pssfp_tangent_kernel(PssfpArgs a) {
     if constexpr (PACKED) {
         if (pssfp_real_rf(a) != REAL) return;
-        pssfp_tile_packed<ZT / 2, GZ, true, REAL>(a, blockIdx.x);
+        pssfp_tile_packed<ZT / 2, GZ, true, REAL, ZT % 2>(a, blockIdx.x);
     } else {
         pssfp_tile<ZT, GZ, true>(a, blockIdx.x);
     }
@@ -533,7 +587,7 @@ __global__ void __launch_bounds__(128) pssfp_queue_kernel(const PssfpArgs* __res
         const int2 w = items[it];
         if (threadIdx.x == 0) job = jobs[w.x];
         __syncthreads();
-        if constexpr (PACKED) pssfp_tile_packed<ZT / 2, GZ, TAN, REAL>(job, w.y);
+        if constexpr (PACKED) pssfp_tile_packed<ZT / 2, GZ, TAN, REAL, ZT % 2>(job, w.y);
         else pssfp_tile<ZT, GZ, TAN>(job, w.y);
         __syncthreads();
     }
@@ -581,7 +635,7 @@ const PssfpConfig kPssfpConfigs[] = {
     // the packed layouts come last, so the indices of the others (which a tuning table names) stay
     COMPAS_PSSFP_PACKED(2, 1), COMPAS_PSSFP_PACKED(4, 1), COMPAS_PSSFP_PACKED(10, 1), COMPAS_PSSFP_PACKED(2, 4),
     COMPAS_PSSFP_PACKED(4, 4), COMPAS_PSSFP_PACKED(6, 4), COMPAS_PSSFP_PACKED(10, 4), COMPAS_PSSFP_PACKED(6, 2),
-    COMPAS_PSSFP_PACKED_VALUE(18, 2), COMPAS_PSSFP_PACKED(8, 8),
+    COMPAS_PSSFP_PACKED_VALUE(18, 2), COMPAS_PSSFP_PACKED(8, 8), COMPAS_PSSFP_PACKED(9, 4),
 };
 }  // namespace
 

@@ -54,8 +54,9 @@ def test_builtin_choice_covers_the_states():
     for cfg, nz in zip(out["pssfp"], (35, 5)):
         zt, gz = pc[cfg]
         assert zt * gz >= nz
-    # 35 z: the two-wide layout of 5 pairs on 4 lanes (40 slots); 5 z: 1 pair on 4 lanes (8 slots)
-    assert tuple(pc[out["pssfp"][0]]) == (10, 4) and out["pssfp_packed"][out["pssfp"][0]]
+    # 35 z: the two-wide layout of 4 pairs and one unpaired isochromat on 4 lanes (36 slots); 5 z:
+    # 1 pair on 4 lanes (8 slots)
+    assert tuple(pc[out["pssfp"][0]]) == (9, 4) and out["pssfp_packed"][out["pssfp"][0]]
     assert tuple(pc[out["pssfp"][1]]) == (2, 4) and out["pssfp_packed"][out["pssfp"][1]]
     # an override that does not cover the states is ignored; a covering one wins
     assert out["override_uncovered"] == out["fisp"][0]
