@@ -911,8 +911,10 @@ __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_beg
                     // two TRs per iteration, so the compiler can absorb one of the two dephasing
                     // shifts in register renaming (value kernel 63.6 -> 59.6 ms, tangent kernel
                     // 308 -> 281 ms on the 224² MR-STAT slice; 4 TRs per iteration spill and are
-                    // slower)
-#pragma unroll 2
+                    // slower); four for the two-wide tangent layouts, whose three shifted vectors
+                    // otherwise cost register moves on the FMA pipe (4 x 8 layout: 380 ms with one
+                    // TR per iteration, 272.6 with two, 250.0 with four; eight were not unrolled)
+#pragma unroll (TAN && PACKED ? 4 : 2)
                     for (int j = 0; j < nt; j++) {
                         const int t = t0 + j;
                         const float4 tv = tv_next;
