@@ -908,13 +908,14 @@ __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_beg
             for (int t0 = 0; t0 < a.nTR; t0 += CH) {
                 const int nt = min(CH, a.nTR - t0);
                 if (pok) {
-                    // two TRs per iteration, so the compiler can absorb one of the two dephasing
-                    // shifts in register renaming (value kernel 63.6 -> 59.6 ms, tangent kernel
-                    // 308 -> 281 ms on the 224² MR-STAT slice; 4 TRs per iteration spill and are
-                    // slower); four for the two-wide tangent layouts, whose three shifted vectors
-                    // otherwise cost register moves on the FMA pipe (4 x 8 layout: 380 ms with one
-                    // TR per iteration, 272.6 with two, 250.0 with four; eight were not unrolled)
-#pragma unroll (TAN && PACKED ? 4 : 2)
+                    // several TRs per iteration, so the compiler can absorb dephasing shifts in
+                    // register renaming instead of moving the state (moves the FMA pipe executes).
+                    // Measured on the 224² MR-STAT slice: the first scalar value kernel 63.6 -> 59.6
+                    // ms with two; the packed 25-slot value kernel 44.3 ms with two, 42.8 with three,
+                    // 42.5 with four, 44.0 / 44.4 / 48.5 with five / six / eight; the two-wide 4 x 8
+                    // tangent 380 ms with one, 272.6 with two, 250.0 with four; the scalar 5 x 5
+                    // tangent 278.7 with two, 272.4 with four. The scalar value layouts keep two.
+#pragma unroll ((PACKED || TAN) ? 4 : 2)
                     for (int j = 0; j < nt; j++) {
                         const int t = t0 + j;
                         const float4 tv = tv_next;
