@@ -774,11 +774,12 @@ struct EPGPackedTangent {
 // kernel.
 // TRs per sample chunk: the CTA's warps meet at a barrier once per chunk to sum their positions'
 // samples in shared memory ([W][chunk][VB] per sample plane). The split-lane tangent layouts use
-// 64 TRs, halving their barriers (271 -> 266 ms on the 224² MR-STAT slice); the value kernel keeps
-// 32 (64 measured 0.5 % slower), and so do the one-lane tangent layouts (three planes of 32 voxels
-// per warp would not fit in 227 KB at 64).
+// 64 TRs, halving their barriers (271 -> 266 ms on the 224² MR-STAT slice), and so do the one-lane
+// value layouts (with four TRs per loop iteration: 42.7 -> 41.8 ms; with two, 64 had measured 0.5 %
+// slower); the value layouts split over lanes and the one-lane tangent layouts keep 32 (three planes
+// of 32 voxels per warp would not fit in 227 KB at 64).
 template<int G, bool TAN>
-constexpr int kFispChunk = (TAN && G > 1) ? 64 : 32;
+constexpr int kFispChunk = ((TAN && G > 1) || (!TAN && G == 1)) ? 64 : 32;
 
 // state type of a layout: value PACKED (G = 1) → EPGPacked<K/2, K%2>; TAN → EPGTangent, or
 // EPGPackedTangent<K/2, G> when PACKED; else EPG
@@ -1371,7 +1372,9 @@ const FispConfig& checked_config(FispLaunch L, int N) {
 
 // samples of one chunk: [W][chunk][32 / G] complex per plane (kernels::kFispChunk)
 size_t fisp_smem_bytes(const FispConfig& cfg, int W) {
-    return size_t(W) * 32 * (32 / cfg.G) * sizeof(float2);  // ≤ 64 KB (W ≤ 8)
+    // [W][chunk][32 / G] samples: 64 TRs for one-lane layouts (≤ 128 KB at W ≤ 8), 32 for split ones
+    const int chunk = cfg.G == 1 ? kernels::kFispChunk<1, false> : kernels::kFispChunk<2, false>;
+    return size_t(W) * chunk * (32 / cfg.G) * sizeof(float2);
 }
 
 size_t fisp_tangent_smem_bytes(int G, int W) {
