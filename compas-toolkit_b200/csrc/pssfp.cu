@@ -636,6 +636,7 @@ const PssfpConfig kPssfpConfigs[] = {
     COMPAS_PSSFP_PACKED(2, 1), COMPAS_PSSFP_PACKED(4, 1), COMPAS_PSSFP_PACKED(10, 1), COMPAS_PSSFP_PACKED(2, 4),
     COMPAS_PSSFP_PACKED(4, 4), COMPAS_PSSFP_PACKED(6, 4), COMPAS_PSSFP_PACKED(10, 4), COMPAS_PSSFP_PACKED(6, 2),
     COMPAS_PSSFP_PACKED_VALUE(18, 2), COMPAS_PSSFP_PACKED(8, 8), COMPAS_PSSFP_PACKED(9, 4),
+    COMPAS_PSSFP_PACKED(9, 1),
 };
 }  // namespace
 
