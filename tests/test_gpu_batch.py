@@ -35,6 +35,13 @@ def _mixed_jobs():
     ps["kind"] = "pssfp"
     ps["seq"] = W.pssfp_sequence(np.random.default_rng(5), 25, nrf=4, nz=3)
     jobs.append(ps)
+    # a FISP and a pSSFP job with complex RF samples: they run the general forms of the packed
+    # layouts, in work-queue groups of their own beside the real-RF jobs of the same layouts
+    for kind, seed in (("fisp", 13), ("pssfp", 14)):
+        d = next(j for j in jobs if j["kind"] == kind and j["traj"] is not None)
+        rf = np.asarray(d["seq"]["rf"])
+        phase = np.exp(1j * np.random.default_rng(seed).uniform(-0.5, 0.5, rf.shape[0]))
+        jobs.append({**d, "seq": {**d["seq"], "rf": (rf * phase).astype(np.complex64)}})
     return jobs
 
 
