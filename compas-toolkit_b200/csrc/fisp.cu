@@ -601,7 +601,11 @@ __device__ __forceinline__ void excite_pair(const ExciteCoefs2& k, float2& ur, f
 // The operations are EPGTangent's in the same order, so layout (K, G) gives the bits of the scalar
 // tangent layout (K, G). The dephasing shift exchanges the boundary states with the neighbour lanes
 // as EPG<K, G> does.
-template<int KP, int G>
+// CUT0: state N-1 is the first state of its lane ((N-1) % K == 0, as for 25 states on 4 lanes of 8),
+// so the truncation zeroes one known slot; otherwise a one-hot bit test per slot finds it. The
+// bit tests and their selects sat between every shifted state and its next excitation (the ALU pipe
+// 22 % busy at 25 states on 4 x 8). Zeroing is exact either way: the same bits.
+template<int KP, int G, bool CUT0 = false>
 struct EPGPackedTangent {
     static_assert(KP >= 2 && G >= 1 && G <= 32 && (G & (G - 1)) == 0, "pairs per lane, power-of-two lane groups");
     static constexpr int K = 2 * KP;
@@ -635,7 +639,9 @@ struct EPGPackedTangent {
         const bool last = sub == G - 1;  // the last lane's top state takes the zero beyond the layout
         gr[v][KP - 1] = make_float2(cr, last ? 0.f : ngr);
         gi[v][KP - 1] = make_float2(ci, last ? 0.f : ngi);
-        if (sub == (N - 1) / K) {  // zero state N-1 (one-hot bit test per slot)
+        if constexpr (CUT0) {
+            if (sub == (N - 1) / K) gr[v][0].x = gi[v][0].x = 0.f;  // state N-1 = this lane's slot 0
+        } else if (sub == (N - 1) / K) {  // zero state N-1 (one-hot bit test per slot)
             const unsigned cut = 1u << ((N - 1) % K);
 #pragma unroll
             for (int j = 0; j < KP; j++) {
@@ -782,10 +788,11 @@ template<int G, bool TAN>
 constexpr int kFispChunk = ((TAN && G > 1) || (!TAN && G == 1)) ? 64 : 32;
 
 // state type of a layout: value PACKED (G = 1) → EPGPacked<K/2, K%2>; TAN → EPGTangent, or
-// EPGPackedTangent<K/2, G> when PACKED; else EPG
-template<int K, int G, bool TAN, bool PACKED>
-using FispState = std::conditional_t<TAN, std::conditional_t<PACKED, EPGPackedTangent<K / 2, G>, EPGTangent<K, G>>,
-                                     std::conditional_t<PACKED, EPGPacked<K / 2, K % 2>, EPG<K, G>>>;
+// EPGPackedTangent<K/2, G, CUT0> when PACKED; else EPG
+template<int K, int G, bool TAN, bool PACKED, bool CUT0 = false>
+using FispState =
+    std::conditional_t<TAN, std::conditional_t<PACKED, EPGPackedTangent<K / 2, G, CUT0>, EPGTangent<K, G>>,
+                       std::conditional_t<PACKED, EPGPacked<K / 2, K % 2>, EPG<K, G>>>;
 
 // Balanced item split of the one-simulation kernel: the order of a CTA's items (at most
 // kFispBalancedItems) and its hand-off points, in shared memory
@@ -829,12 +836,15 @@ __device__ __forceinline__ void handoff_wait(const int* flag, unsigned int* stat
 // predecessor's. Every tile's positions are still added one at a time in increasing order, so the
 // echoes are the same bits as with whole tiles per CTA.
 // REAL (packed layouts only): every RF phase is real, the excitation without the d_re products.
-template<int K, int G, bool TAN = false, bool PACKED = false, bool BAL = false, bool REAL = false>
+// CUT0 (packed tangent layouts only): state N-1 is the first state of its lane (EPGPackedTangent).
+template<int K, int G, bool TAN = false, bool PACKED = false, bool BAL = false, bool REAL = false,
+         bool CUT0 = false>
 __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_begin, const int item_end,
                                            float2* samples, const FispOrder* ord = nullptr) {
     static_assert(!PACKED || TAN || G == 1, "packed value layouts hold one voxel per lane");
     static_assert(!PACKED || !TAN || K % 2 == 0, "packed tangent layouts hold pairs of states");
     static_assert(!REAL || PACKED, "the real-phase update is a packed-layout form");
+    static_assert(!CUT0 || (PACKED && TAN), "the slot-0 truncation is a packed tangent form");
     constexpr int VB = 32 / G;
     const int W = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -895,7 +905,7 @@ __device__ __forceinline__ void fisp_items(const FispArgs& a, const int item_beg
             if (w == 0 || item_at(base + w) / P != item_at(base + w - 1) / P) starts |= 1u << w;
 
         const float4* tab = a.table + int64_t(p) * a.nTR;
-        FispState<K, G, TAN, PACKED> st;
+        FispState<K, G, TAN, PACKED, CUT0> st;
         st.init(sub);
         for (int rep = a.reps; rep >= 1; rep--) {
             const bool sampled = (rep == 1);
@@ -1104,20 +1114,21 @@ __global__ void __launch_bounds__(256, 1) fisp_queue_kernel(const FispArgs* __re
 
 // One FISP simulation with its T1 and T2 tangents: value, ∂/∂T1, ∂/∂T2 into a.echo, a.dT1, a.dT2.
 // PACKED: the two-wide state EPGPackedTangent; REAL its real-phase form, launched beside the
-// general form (the one that does not match the sequence returns at once).
-template<int K, int G, bool PACKED = false, bool REAL = false>
+// general form (the one that does not match the sequence returns at once); CUT0 its form for
+// (N-1) % K == 0, which the host launches for those N.
+template<int K, int G, bool PACKED = false, bool REAL = false, bool CUT0 = false>
 __global__ void __launch_bounds__(256, 1) fisp_tangent_kernel(FispArgs a, int ntiles) {
     extern __shared__ float2 samples[];  // [3][W][chunk][VB]
     if constexpr (PACKED) {
         if (fisp_real_phases(a) != REAL) return;
     }
     const int2 r = cta_tile_range(ntiles, blockIdx.x, gridDim.x);
-    fisp_items<K, G, true, PACKED, false, REAL>(a, r.x * a.P, r.y * a.P, samples);
+    fisp_items<K, G, true, PACKED, false, REAL, CUT0>(a, r.x * a.P, r.y * a.P, samples);
 }
 
 // Work-queue form of fisp_tangent_kernel for batches (same items and order as fisp_queue_kernel;
-// REAL: every job's phases are real).
-template<int K, int G, bool PACKED = false, bool REAL = false>
+// REAL: every job's phases are real; CUT0: every job has (N-1) % K == 0).
+template<int K, int G, bool PACKED = false, bool REAL = false, bool CUT0 = false>
 __global__ void __launch_bounds__(256, 1) fisp_tangent_queue_kernel(const FispArgs* __restrict__ jobs,
                                                                     const int2* __restrict__ items, int nitems,
                                                                     int* __restrict__ head) {
@@ -1132,7 +1143,7 @@ __global__ void __launch_bounds__(256, 1) fisp_tangent_queue_kernel(const FispAr
         const int2 w = items[it];
         if (threadIdx.x == 0) job = jobs[w.x];
         __syncthreads();
-        fisp_items<K, G, true, PACKED, false, REAL>(job, w.y * job.P, (w.y + 1) * job.P, samples);
+        fisp_items<K, G, true, PACKED, false, REAL, CUT0>(job, w.y * job.P, (w.y + 1) * job.P, samples);
         __syncthreads();
     }
 }
@@ -1194,12 +1205,19 @@ struct FispTangentConfig {
     // real-phase jobs), else null
     FispKernel fn_real;
     FispQueueKernel queue_real;
+    // packed layouts: the four kernels above in their form for (N-1) % K == 0 (state N-1 is the
+    // first state of its lane), else null
+    FispKernel fn_cut0, fn_real_cut0;
+    FispQueueKernel queue_cut0, queue_real_cut0;
 };
-#define COMPAS_FISP_TANGENT(K, G) \
-    {K, G, kernels::fisp_tangent_kernel<K, G>, kernels::fisp_tangent_queue_kernel<K, G>, false, nullptr, nullptr}
+#define COMPAS_FISP_TANGENT(K, G)                                                                              \
+    {K, G, kernels::fisp_tangent_kernel<K, G>, kernels::fisp_tangent_queue_kernel<K, G>, false, nullptr, nullptr, \
+     nullptr, nullptr, nullptr, nullptr}
 #define COMPAS_FISP_TANGENT_PACKED(K, G)                                                                     \
     {K, G, kernels::fisp_tangent_kernel<K, G, true>, kernels::fisp_tangent_queue_kernel<K, G, true>, true, \
-     kernels::fisp_tangent_kernel<K, G, true, true>, kernels::fisp_tangent_queue_kernel<K, G, true, true>}
+     kernels::fisp_tangent_kernel<K, G, true, true>, kernels::fisp_tangent_queue_kernel<K, G, true, true>, \
+     kernels::fisp_tangent_kernel<K, G, true, false, true>, kernels::fisp_tangent_kernel<K, G, true, true, true>, \
+     kernels::fisp_tangent_queue_kernel<K, G, true, false, true>, kernels::fisp_tangent_queue_kernel<K, G, true, true, true>}
 // the packed layouts come last, so the indices of the others keep their meaning
 const FispTangentConfig kFispTangentConfigs[] = {
     COMPAS_FISP_TANGENT(1, 1), COMPAS_FISP_TANGENT(2, 1), COMPAS_FISP_TANGENT(4, 1), COMPAS_FISP_TANGENT(8, 1),
@@ -1540,18 +1558,21 @@ void launch_fisp_tangent(const CompasContext& ctx, const TissueParameters& param
     const int W = std::max(1, std::min(L.warps, 8));
     const int ntiles = div_ceil(nvoxels, VB);
     const size_t smem = fisp_tangent_smem_bytes(cfg.G, W);
+    const bool cut0 = cfg.fn_cut0 != nullptr && (N - 1) % cfg.K == 0;
+    const FispKernel fn = cut0 ? cfg.fn_cut0 : cfg.fn;
+    const FispKernel fn_real = cut0 ? cfg.fn_real_cut0 : cfg.fn_real;
     DeviceGuard guard(ctx.device());
-    allow_smem(reinterpret_cast<const void*>(cfg.fn), smem);
-    int resident = resident_ctas(reinterpret_cast<const void*>(cfg.fn), 32 * W, smem, ctx.device());
-    if (cfg.fn_real != nullptr) {
-        allow_smem(reinterpret_cast<const void*>(cfg.fn_real), smem);
-        resident = std::min(resident, resident_ctas(reinterpret_cast<const void*>(cfg.fn_real), 32 * W, smem, ctx.device()));
+    allow_smem(reinterpret_cast<const void*>(fn), smem);
+    int resident = resident_ctas(reinterpret_cast<const void*>(fn), 32 * W, smem, ctx.device());
+    if (fn_real != nullptr) {
+        allow_smem(reinterpret_cast<const void*>(fn_real), smem);
+        resident = std::min(resident, resident_ctas(reinterpret_cast<const void*>(fn_real), 32 * W, smem, ctx.device()));
     }
     const int grid = std::min(ntiles, resident);
-    cfg.fn<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles);
+    fn<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles);
     check_launch("fisp_tangent_kernel");
-    if (cfg.fn_real != nullptr) {  // the form that does not match the sequence's phases returns at once
-        cfg.fn_real<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles);
+    if (fn_real != nullptr) {  // the form that does not match the sequence's phases returns at once
+        fn_real<<<grid, 32 * W, smem, ctx.stream()>>>(a, ntiles);
         check_launch("fisp_tangent_kernel (real phases)");
     }
 }
@@ -1567,7 +1588,11 @@ void launch_fisp_tangent_queue(cudaStream_t stream, int device, FispLaunch L, in
     COMPAS_CHECK(L.config >= 0 && L.config < kFispTangentConfigCount);
     const auto& cfg = kFispTangentConfigs[L.config];
     COMPAS_CHECK(cfg.K * cfg.G >= max_state);
-    const FispQueueKernel fn = real && cfg.queue_real != nullptr ? cfg.queue_real : cfg.queue;
+    // every job of the launch has max_state states (the batch groups jobs by it), so the
+    // slot-0 truncation form holds for all of them or for none
+    const bool cut0 = cfg.queue_cut0 != nullptr && (max_state - 1) % cfg.K == 0;
+    const bool use_real = real && cfg.queue_real != nullptr;
+    const FispQueueKernel fn = use_real ? (cut0 ? cfg.queue_real_cut0 : cfg.queue_real) : (cut0 ? cfg.queue_cut0 : cfg.queue);
     const int W = std::max(1, std::min(L.warps, 8));
     const size_t smem = fisp_tangent_smem_bytes(cfg.G, W);
     DeviceGuard guard(device);

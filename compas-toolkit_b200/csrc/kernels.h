@@ -54,8 +54,9 @@ void launch_fisp_tangent(const CompasContext& ctx, const TissueParameters& param
                          const FISPSequence& seq, cfloat* echo, cfloat* dT1, cfloat* dT2, int64_t echo_stride,
                          FispLaunch L);
 int fisp_tangent_tile_voxels(FispLaunch L);  // voxels per work item of tangent layout L
-// work-queue launch over (job, tile) items of FISP tangent jobs (args with dT1 / dT2 set); `real`:
-// every job's phases are real, which a packed layout runs in its real-phase form
+// work-queue launch over (job, tile) items of FISP tangent jobs (args with dT1 / dT2 set), every
+// job with max_state states; `real`: every job's phases are real, which a packed layout runs in its
+// real-phase form
 void launch_fisp_tangent_queue(cudaStream_t stream, int device, FispLaunch L, int max_state,
                                const kernels::FispArgs* jobs, const int2* items, int nitems, int* head,
                                bool real = false);

@@ -90,12 +90,26 @@ def test_batch_rejects_mismatched_trajectory(ctx):
         cb.SimulationBatch(ctx, [(params, seq, wrong, coils)])
 
 
-def test_batch_tangent_jobs_match_one_job_calls_bitwise(ctx):
+@pytest.mark.parametrize("layout", ["default", "packed4x8"])
+def test_batch_tangent_jobs_match_one_job_calls_bitwise(ctx, layout):
     # jobs flagged for tangents run on the tangent work-queue kernels in groups of their own; their
     # echoes and derivatives are the bits of simulate_magnetization_tangents for each alone, the
-    # other jobs keep the bits of simulate_magnetization
+    # other jobs keep the bits of simulate_magnetization. packed4x8: every tangent job on the
+    # two-wide layout of 4 lanes x 8 states, the 25-state job in its slot-0 truncation form
+    # ((25 - 1) % 8 == 0), the 8-state jobs in the bit-test form
     import compas_b200 as cb
 
+    if layout == "packed4x8":
+        configs = [tuple(c) for c in cb.fisp_tangent_configs()]
+        cb.set_fisp_tangent_launch(next(i for i, c in enumerate(configs)
+                                        if c == (8, 4) and cb.fisp_tangent_config_packed(i)))
+    try:
+        _check_tangent_batch(cb, ctx)
+    finally:
+        cb.set_fisp_tangent_launch(-1)
+
+
+def _check_tangent_batch(cb, ctx):
     dicts = _mixed_jobs()
     # the MR-STAT sequence (25 states, 35 positions: 8 warps, 48 KB of dynamic shared memory in the
     # tangent queue kernel beside its static argument block) on a few voxels

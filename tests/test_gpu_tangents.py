@@ -84,7 +84,9 @@ def test_fisp_packed_tangents_match_scalar_bits(cb, ctx, workloads, phase):
             if not cb.fisp_tangent_config_packed(i):
                 continue
             j = next(n for n, d in enumerate(configs) if d == c and not cb.fisp_tangent_config_packed(n))
-            for N in sorted({c[0] * c[1], c[0] * c[1] - 3}):
+            # N = K·(G-1) + 1 puts state N-1 in the first slot of the last lane: the packed layout
+            # runs its slot-0 truncation form there, the scalar one its bit tests
+            for N in sorted({c[0] * c[1], c[0] * c[1] - 3, c[0] * (c[1] - 1) + 1}):
                 seq = cb.FispSequence.from_dict(ctx, workloads.fisp_sequence(rf, slices, 8.7e-3, 4.35e-3, 25e-3, N))
                 cb.set_fisp_tangent_launch(i)
                 packed = cb.simulate_magnetization_tangents(ctx, params, seq)
@@ -96,7 +98,7 @@ def test_fisp_packed_tangents_match_scalar_bits(cb, ctx, workloads, phase):
                 tried += 1
     finally:
         cb.set_fisp_tangent_launch(-1)
-    assert tried >= 6
+    assert tried >= 10
 
 
 def test_fisp_tangents_repetitions_undersampling(cb, ctx, oracle, workloads):
