@@ -116,13 +116,11 @@ def _cn32(rng, shape):
 
 
 def _builtin_tile(R):
-    """the library's built-in Cartesian readout tile: the multiple of 16 up to 256 that pads R least"""
-    best, padded = 256, -(-max(R, 1) // 256) * 256
-    for nr in range(240, 15, -16):
-        p = -(-max(R, 1) // nr) * nr
-        if p < padded:
-            best, padded = nr, p
-    return best
+    """the library's built-in Cartesian readout tile: the fewest tiles of at most 256 readouts, then
+    the least padding (a multiple of 16)"""
+    r = max(R, 1)
+    tiles = -(-r // 256)
+    return -(-(-(-r // tiles)) // 16) * 16
 
 
 def _tc_call(ctx, kind, nv, R, S, C, seed):

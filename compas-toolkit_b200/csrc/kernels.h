@@ -147,7 +147,8 @@ struct TcPlan {
     int nr;                              // readouts per tile
     int64_t ctas;                        // CTAs of the contraction (CTA pairs × 2)
 };
-// readouts per tile of the Cartesian contraction: the multiple of 16 up to 256 that pads R least
+// readouts per tile of the Cartesian contraction: a multiple of 16 up to 256, the fewest tiles,
+// then the least padding
 int tc_readout_tile(int R);
 
 // ---- tensor-core launch knobs searched by the autotuner -----------------------------------

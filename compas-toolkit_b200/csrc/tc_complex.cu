@@ -18,8 +18,8 @@
 // streamed operand once as the split, swizzled shared-memory images the contraction consumes.
 // The contraction runs on CTA pairs (cluster of 2, tcgen05 cta_group::2): one MMA spans both SMs'
 // tensor cores with M = 256 generated rows (128 (coil, sample) pairs × re/im; each CTA generates
-// its 128) and N = nr readouts (each CTA holds nr/2; nr is the multiple of 16 up to 256 that pads R
-// least, e.g. 224 for 1120 readouts).
+// its 128) and N = nr readouts (each CTA holds nr/2; nr, a multiple of 16 up to 256, gives the fewest
+// readout tiles and then the least padding, e.g. 224 for 1120 readouts).
 // CTA organisation (576 threads, 1 CTA/SM, 192 KB shared memory in 3 stages of 64 KB):
 //   warps 0-15  generate this CTA's 128 rows (64 pairs × 64 K per stage): thread = (2 voxels,
 //               group of TC_PPG pairs); a group starts from the exact E_k table value × coil·w and
@@ -574,17 +574,15 @@ __global__ void tc_pack_batch_kernel(const TcArgs* __restrict__ jobs, const int*
 
 }  // namespace kernels
 
+// The fewest readout tiles of at most 256, then the least padding at that count: nr = ⌈R / tiles⌉
+// rounded up to 16 (224 for 1120 readouts, 256 for 743, 208 for 400). Every readout tile generates
+// the (coil, sample) operand over all voxels again, and a narrow tile's MMAs no longer cover that
+// generation: the earlier rule (the multiple of 16 that pads R least, ties to the wider tile) took
+// 16-readout tiles for 743 readouts (752 rows instead of 768) and ran 10× slower than 256.
 int tc_readout_tile(int R) {
-    int best = 256;
-    int64_t padded = int64_t(div_ceil(std::max(R, 1), 256)) * 256;
-    for (int nr = 240; nr >= 16; nr -= 16) {
-        const int64_t p = int64_t(div_ceil(std::max(R, 1), nr)) * nr;
-        if (p < padded) {
-            padded = p;
-            best = nr;
-        }
-    }
-    return best;
+    const int r = std::max(R, 1);
+    const int tiles = div_ceil(r, 256);
+    return div_ceil(div_ceil(r, tiles), 16) * 16;
 }
 
 namespace {

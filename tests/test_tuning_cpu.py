@@ -114,13 +114,15 @@ def _tc_probe(env_extra=None):
 
 def test_tensor_core_builtin_choice_and_overrides():
     out = _tc_probe()
-    # Cartesian: the readout tile that pads R least (224 divides 1120); voxel splits only to fill
-    # the GPU (the kernel bounds its accumulation length itself), at most 64
+    # Cartesian: the fewest readout tiles of at most 256, then the least padding (5 tiles of 224
+    # for 1120); voxel splits only to fill the GPU (the kernel bounds its accumulation length
+    # itself), at most 64
     tile, splits = out["cartesian_signal"]
     assert tile == 224 and 1 <= splits <= 64
     tile, splits = out["cartesian_jacobian"]
     assert tile == 224 and 1 <= splits <= 64
-    assert out["ragged"][0] == 144  # 1000 readouts: 7 tiles of 144 (1008 rows) pad least
+    # 1000 readouts: 4 tiles of 256 (1024 rows), not the 7 tiles of 144 (1008 rows) that pad least
+    assert out["ragged"][0] == 256
     assert out["cartesian_hermitian"][0] == 0 and out["cartesian_hermitian"][1] >= 1
     assert out["spiral_signal"][1] >= 13 and out["spiral_jacobian"][1] >= 25
     # a Cartesian override of one split is taken as it is; the spiral J·v kernel raises a split
