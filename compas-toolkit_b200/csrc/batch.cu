@@ -199,7 +199,10 @@ void SimulationBatch::Impl::plan_simulation(Family& fam, bool fisp, const std::v
                     args.back().dT1 = reinterpret_cast<float2*>(dT1[size_t(js[q])].data());
                     args.back().dT2 = reinterpret_cast<float2*>(dT2[size_t(js[q])].data());
                 }
-                for (int t = 0; t < div_ceil(V, vb); t++) {
+                // items of fisp_queue_tiles_per_item tiles: the queue kernels run an item's
+                // (tile, position) pairs in rounds of the CTA's warps
+                const int tpi = kernels::fisp_queue_tiles_per_item(args.back().P, g.warps);
+                for (int t = 0; t < div_ceil(V, vb); t += tpi) {
                     items.push_back(int(q));
                     items.push_back(t);
                 }

@@ -1107,7 +1107,10 @@ __global__ void __launch_bounds__(256, 1) fisp_queue_kernel(const FispArgs* __re
         const int2 w = items[it];
         if (threadIdx.x == 0) job = jobs[w.x];
         __syncthreads();
-        fisp_items<K, G, false, PACKED, false, REAL>(job, w.y * job.P, (w.y + 1) * job.P, samples);
+        // tiles w.y .. of the job, as many as the batch put in one item
+        const int tiles = (job.nvoxels + 32 / G - 1) / (32 / G);
+        const int t_end = min(w.y + fisp_queue_tiles_per_item(job.P, blockDim.x >> 5), tiles);
+        fisp_items<K, G, false, PACKED, false, REAL>(job, w.y * job.P, t_end * job.P, samples);
         __syncthreads();  // job and s_item are rewritten by the next item
     }
 }
@@ -1143,7 +1146,9 @@ __global__ void __launch_bounds__(256, 1) fisp_tangent_queue_kernel(const FispAr
         const int2 w = items[it];
         if (threadIdx.x == 0) job = jobs[w.x];
         __syncthreads();
-        fisp_items<K, G, true, PACKED, false, REAL, CUT0>(job, w.y * job.P, (w.y + 1) * job.P, samples);
+        const int tiles = (job.nvoxels + 32 / G - 1) / (32 / G);
+        const int t_end = min(w.y + fisp_queue_tiles_per_item(job.P, blockDim.x >> 5), tiles);
+        fisp_items<K, G, true, PACKED, false, REAL, CUT0>(job, w.y * job.P, t_end * job.P, samples);
         __syncthreads();
     }
 }

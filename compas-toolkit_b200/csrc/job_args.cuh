@@ -27,6 +27,25 @@ struct FispArgs {
     const int* skip;       // one-simulation kernel: returns at once when *skip != 0 (null: never)
 };
 
+// Voxel tiles per item of the FISP work-queue kernels, for a job of P slice positions on CTAs of W
+// warps: an item's (tile, position) pairs run in rounds of W warps, and one tile of 35 positions on
+// 8 warps leaves the last of 5 rounds with 3 warps busy (35 of 40 warp slots), two tiles fill 70 of
+// 72. The count up to 4 with the fullest rounds, the fewest on ties. The batch builds its items and
+// the kernel reads them with this same count; the summation order, and so every bit, does not
+// depend on it.
+__host__ __device__ inline int fisp_queue_tiles_per_item(int P, int W) {
+    int best = 1, best_pairs = P, best_slots = ((P + W - 1) / W) * W;
+    for (int n = 2; n <= 4; n++) {
+        const int pairs = n * P, slots = ((pairs + W - 1) / W) * W;
+        if (int64_t(pairs) * best_slots > int64_t(best_pairs) * slots) {
+            best = n;
+            best_pairs = pairs;
+            best_slots = slots;
+        }
+    }
+    return best;
+}
+
 struct PssfpArgs {
     const float* params;
     int64_t param_stride;
