@@ -407,6 +407,22 @@ def test_jacobian(cb, ctx, oracle, workloads, method):
     assert oracle.rel_l2(got, ref) < (TOL_BF16X3 if method in TC_JAC else TOL_FP32)
 
 
+@pytest.mark.parametrize("nr", [257, 400, 743])
+def test_cartesian_ragged_readout_counts(cb, ctx, oracle, workloads, nr):
+    # readout counts that do not fill whole 256-readout tiles: the tensor-core contractions take
+    # the fewest tiles, ceil(R / ceil(R / 256)) readouts each rounded up to 16 (743: 3 tiles of 256,
+    # the last holding 231 readouts); split-BF16 signal and J·v against the FP64 oracle
+    rng = np.random.default_rng(nr)
+    p, traj, coils, e, d1, d2 = _jac_case(workloads, rng, nr=nr)
+    params = cb.TissueParameters.from_soa(ctx, p)
+    t = cb.trajectory_from_dict(ctx, traj)
+    sig = cb.magnetization_to_signal(ctx, e, params, t, coils, method="MatmulFast").to_numpy()
+    assert oracle.rel_l2(sig, oracle.signal_cartesian(e, p, traj, coils)) < TOL_BF16X3
+    v = workloads.cn(rng, (4, p.shape[1]))
+    jv = cb.compute_jacobian(ctx, e, {"T1": d1, "T2": d2}, params, t, coils, v, method="GemmFast").to_numpy()
+    assert oracle.rel_l2(jv, oracle.jacobian(e, d1, d2, p, traj, coils, v)) < TOL_BF16X3
+
+
 @pytest.mark.parametrize("method", PLAIN_JAC + TC_JAC)
 @pytest.mark.parametrize("nc", [1, 5])
 def test_jacobian_hermitian(cb, ctx, oracle, workloads, method, nc):
